@@ -1,0 +1,75 @@
+"""Regenerate the golden fixtures under tests/golden/ from the reference tree.
+
+Run once, in a container where the TeNeS source tree is mounted:
+
+    python tests/golden/make_fixtures.py /root/reference
+
+It copies the numbers of the reference's own test fixtures (not its sources)
+into compact JSON / TOML files so that the tests never read the reference
+tree at run time:
+
+* simple_update_kat.json  <- test/data/simple_update.dat
+  (known answer of core::Simple_update_bond, test/simple_update.cpp:28-160)
+* te_tfi_input.toml       <- test/data/TE_TFI.toml (expert input file)
+* te_tfi_expected.json    <- test/data/output_TE_TFI/TE_{density,onesite_obs,
+  twosite_obs,multisite_obs_4,correlation_length}.dat
+* mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
+  produced by oracle/mt19937_draws.cpp compiled with the system g++
+"""
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def _rows(path):
+    out = []
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if not line or line.startswith("#"):
+                continue
+            out.append([float(x) for x in line.split()])
+    return out
+
+
+def main(ref):
+    data = os.path.join(ref, "test", "data")
+    vals = [float(x) for x in open(os.path.join(data, "simple_update.dat")).read().split()]
+    n = 2 * 2 * 2 * 2 * 2
+    kat = {"T1": vals[:n], "T2": vals[n:2 * n], "lambda": vals[2 * n:2 * n + 2],
+           "D": 2, "ldof": 2, "connect": 2, "tol": 1e-8,
+           "source": "test/data/simple_update.dat; inputs test/simple_update.cpp:34-71"}
+    with open(os.path.join(HERE, "simple_update_kat.json"), "w") as f:
+        json.dump(kat, f, indent=1)
+
+    shutil.copyfile(os.path.join(data, "TE_TFI.toml"), os.path.join(HERE, "te_tfi_input.toml"))
+    out = os.path.join(data, "output_TE_TFI")
+    exp = {}
+    for key, fname in (("density", "TE_density.dat"), ("onesite", "TE_onesite_obs.dat"),
+                       ("twosite", "TE_twosite_obs.dat"), ("multisite", "TE_multisite_obs_4.dat"),
+                       ("correlation_length", "TE_correlation_length.dat")):
+        exp[key] = _rows(os.path.join(out, fname))
+    exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
+    with open(os.path.join(HERE, "te_tfi_expected.json"), "w") as f:
+        json.dump(exp, f)
+
+    with tempfile.TemporaryDirectory() as td:
+        exe = os.path.join(td, "mt")
+        subprocess.check_call(["g++", "-O2", "-o", exe, os.path.join(REPO, "oracle", "mt19937_draws.cpp")])
+        txt = subprocess.check_output([exe, "11", "64"]).decode()
+    draws = [float(x) for x in txt.split()]
+    with open(os.path.join(HERE, "mt19937_seed11.json"), "w") as f:
+        json.dump({"seed": 11, "uniform_pm1": draws,
+                   "generator": "oracle/mt19937_draws.cpp (std::mt19937, "
+                                "std::uniform_real_distribution<double>(-1, 1))"}, f)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
