@@ -1,0 +1,152 @@
+/*
+ * tenes_gpu.h -- C ABI of libtenes_gpu.so, the B200 (sm_100a) implementation
+ * of TeNeS's iTPS CTMRG environment path.
+ *
+ * Every entry point returns a tg_status and never throws or aborts across the
+ * ABI (the reference lets C++ exceptions escape tenes_itps_main,
+ * src/iTPS/main.cpp:33-39; here they are turned into status codes).  The
+ * message of the last failure is available from tg_last_error().
+ *
+ * Tensor layouts on the host side of the ABI are row-major (last leg fastest)
+ * in the reference's leg order:
+ *   site tensor Tn  [left, up, right, bottom, phys]   (D0, D1, D2, D3, d)
+ *   corners C1..C4  [chi, chi]  legs (previous, next) going clockwise
+ *   edges  eT*      [chi, chi, D, D]  (previous, next, ket, bra)
+ * (src/iTPS/iTPS.hpp:301-318, src/iTPS/core/ctm.cpp:44-53).  Complex tensors
+ * are interleaved (re, im) pairs of doubles.  Environment legs are padded to
+ * chi with zeros; the reference's shrinking of a leg below chi when fewer
+ * than chi singular values pass the cutoff is represented by zero rows and
+ * columns, which leaves every contraction unchanged.
+ *
+ * Threading: a context is used by one host thread at a time.  All work is
+ * issued on the context's own CUDA stream; every call returns after its work
+ * is complete unless its name ends in _async.
+ */
+#ifndef TENES_GPU_H_
+#define TENES_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tg_status {
+  TG_OK = 0,
+  TG_E_INPUT = 1,    /* bad argument, shape or parameter (tenes::input_error) */
+  TG_E_LOAD = 2,     /* bad tensor data (tenes::load_error) */
+  TG_E_RUNTIME = 3,  /* numerical failure, e.g. SVD did not converge */
+  TG_E_NOCONV = 4,   /* CTMRG hit iteration_max without converging (warning-level) */
+  TG_E_CUDA = 5,     /* CUDA / cuSOLVER error */
+  TG_E_STATE = 6     /* call made in the wrong order (e.g. move before init) */
+} tg_status;
+
+typedef struct tg_ctx tg_ctx;
+
+/* Unit cell (SquareLattice, src/SquareLattice.hpp:54-163). */
+typedef struct tg_lattice_desc {
+  int LX;
+  int LY;
+  int skew;
+  const int* physical_dims; /* [LX*LY] */
+  const int* virtual_dims;  /* [LX*LY][4]: left, up, right, bottom */
+} tg_lattice_desc;
+
+/* CTMRG / simple-update parameters (PEPS_Parameters,
+ * src/iTPS/PEPS_Parameters.cpp:30-77, keys of [parameter.ctm] in
+ * src/iTPS/load_toml.cpp:383-398). */
+typedef struct tg_params {
+  int chi;                          /* ctm.dimension */
+  double inverse_projector_cut;     /* ctm.projector_cutoff (1e-12) */
+  double ctm_convergence_epsilon;   /* ctm.convergence_epsilon (1e-6) */
+  int max_ctm_iteration;            /* ctm.iteration_max (100) */
+  int projector_corner;             /* ctm.projector_corner (1) */
+  int use_rsvd;                     /* ctm.use_rsvd (0) */
+  double rsvd_oversampling_factor;  /* ctm.rsvd_oversampling_factor (2.0) */
+  int rsvd_oversample_abs;          /* >= 0: k = cut + this, overrides the factor */
+  int rsvd_power_iters;             /* power iterations of the rSVD range finder (2) */
+  uint64_t rsvd_seed;               /* key of the counter-based rSVD test matrix */
+  double inverse_lambda_cut;        /* simple_update.lambda_cutoff (1e-12) */
+} tg_params;
+
+/* Fill *p with the reference defaults. */
+void tg_params_default(tg_params* p);
+
+/* Human-readable message of the last failing call on this thread. */
+const char* tg_last_error(void);
+
+/* Library version string. */
+const char* tg_version(void);
+
+/* Create / destroy a context on CUDA device `device`.  is_complex selects
+ * complex128 tensors (TeNeS complex_tensor) instead of float64 (real_tensor). */
+tg_status tg_ctx_create(const tg_lattice_desc* lattice, const tg_params* params,
+                        int is_complex, int device, tg_ctx** out);
+tg_status tg_ctx_destroy(tg_ctx* ctx);
+
+/* Site tensors and simple-update weights (iTPS::Tn, lambda_tensor,
+ * src/iTPS/iTPS.hpp:301-306).  `host` holds D0*D1*D2*D3*d values (twice as
+ * many doubles when complex). */
+tg_status tg_set_site_tensor(tg_ctx* ctx, int site, const double* host);
+tg_status tg_get_site_tensor(tg_ctx* ctx, int site, double* host);
+tg_status tg_set_lambda(tg_ctx* ctx, int site, int leg, const double* host);
+tg_status tg_get_lambda(tg_ctx* ctx, int site, int leg, double* host);
+
+/* Environment tensors.  which: 0..3 = C1..C4, 4..7 = eTt, eTr, eTb, eTl. */
+tg_status tg_set_env(tg_ctx* ctx, int which, int site, const double* host);
+tg_status tg_get_env(tg_ctx* ctx, int which, int site, double* host);
+
+/* Environment initialisation from the site tensors
+ * (core::Calc_CTM_Environment initialize branch, ctm.cpp:984-1193). */
+tg_status tg_ctm_init(tg_ctx* ctx);
+
+/* One directional move absorbing column ix / row iy
+ * (core::Left_move / Right_move / Top_move / Bottom_move, ctm.cpp:562-813).
+ * dir: 0 = left, 1 = right, 2 = top, 3 = bottom. */
+tg_status tg_ctm_move(tg_ctx* ctx, int dir, int line);
+
+/* One CTMRG iteration: all left, right, top, bottom moves (ctm.cpp:1205-1228). */
+tg_status tg_ctm_sweep(tg_ctx* ctx);
+
+/* Check_Convergence_CTM (ctm.cpp:815-969) against the corners saved by the
+ * previous call (or by tg_ctm_init); saves the current corners. */
+tg_status tg_ctm_check_convergence(tg_ctx* ctx, int* converged, double* sig_max);
+
+/* core::Calc_CTM_Environment (ctm.cpp:971-1253): optional init, then sweeps
+ * until converged or max_ctm_iteration.  Returns TG_OK also when not
+ * converged (the reference only warns); *converged tells which. */
+tg_status tg_ctm_run(tg_ctx* ctx, int initialize, int* iterations, int* converged,
+                     double* sig_max);
+
+/* L2-normalised singular values of corner `which` (0..3) of `site`
+ * (the spectrum Check_Convergence_CTM compares, ctm.cpp:830-847); chi values. */
+tg_status tg_corner_spectrum(tg_ctx* ctx, int which, int site, double* host);
+
+/* <op> through the environment.  Results are (re, im) pairs.
+ * One site: Contract_one_site_iTPS_CTM (contract_itps_ctm/ctm.cpp:89-113),
+ *   op is d x d, applied as sum_{p,q} Tn[..p] op[p,q] conj(Tn[..q]).
+ * Nearest-neighbour op12 (d1,d2,d1,d2): Contract_two_sites_{horizontal,vertical}_op12
+ *   (ctm.cpp:213-319); source/target as in twosite_obs.cpp:189-222. */
+tg_status tg_measure_onesite(tg_ctx* ctx, int site, const double* op, double* out);
+tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const double* op,
+                               double* out);
+
+/* Simple update (src/iTPS/simple_update.cpp:25-46).
+ * One-site: Tn[site] <- tensordot(Tn[site], op, 4, 0).
+ * Bond: core::Simple_update_bond (core/simple_update.cpp:50-198) between
+ * `source` and its neighbour on `source_leg`; op is (d1, d2, d1, d2). */
+tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op);
+tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op);
+
+/* Synchronise the context's stream; report asynchronous CUDA errors. */
+tg_status tg_sync(tg_ctx* ctx);
+
+/* Count of kernels this library has launched in the calling process. */
+uint64_t tg_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENES_GPU_H_ */

@@ -1,0 +1,185 @@
+// C ABI of libtenes_gpu (declared in include/tenes_gpu.h).  Every entry point
+// converts C++ exceptions into tg_status codes; nothing is thrown across it.
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "engine.hpp"
+#include "tenes_gpu.h"
+
+struct tg_ctx {
+  tg::Engine* eng = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+tg_status guard(F&& f) {
+  try {
+    f();
+    return TG_OK;
+  } catch (const tg::Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return TG_E_RUNTIME;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return TG_E_RUNTIME;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return TG_E_RUNTIME;
+  }
+}
+
+tg::Engine* E(tg_ctx* c) {
+  if (!c || !c->eng) tg::fail(TG_E_STATE, "null context");
+  return c->eng;
+}
+
+void need(const void* p, const char* what) {
+  if (!p) tg::fail(TG_E_INPUT, std::string("null pointer: ") + what);
+}
+
+}  // namespace
+
+extern "C" {
+
+void tg_params_default(tg_params* p) {
+  if (!p) return;
+  p->chi = 2;
+  p->inverse_projector_cut = 1e-12;
+  p->ctm_convergence_epsilon = 1e-6;
+  p->max_ctm_iteration = 100;
+  p->projector_corner = 1;
+  p->use_rsvd = 0;
+  p->rsvd_oversampling_factor = 2.0;
+  p->rsvd_oversample_abs = -1;
+  p->rsvd_power_iters = 2;
+  p->rsvd_seed = 0;
+  p->inverse_lambda_cut = 1e-12;
+}
+
+const char* tg_last_error(void) { return g_last_error.c_str(); }
+
+const char* tg_version(void) { return "tenes_gpu 0.1.0 (sm_100a)"; }
+
+tg_status tg_ctx_create(const tg_lattice_desc* lattice, const tg_params* params, int is_complex, int device,
+                        tg_ctx** out) {
+  return guard([&] {
+    need(out, "out");
+    *out = nullptr;
+    auto* c = new tg_ctx;
+    try {
+      c->eng = tg::make_engine(lattice, params, is_complex, device);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+tg_status tg_ctx_destroy(tg_ctx* ctx) {
+  return guard([&] {
+    if (!ctx) return;
+    delete ctx->eng;
+    delete ctx;
+  });
+}
+
+tg_status tg_set_site_tensor(tg_ctx* ctx, int site, const double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->set_site_tensor(site, host);
+  });
+}
+tg_status tg_get_site_tensor(tg_ctx* ctx, int site, double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->get_site_tensor(site, host);
+  });
+}
+tg_status tg_set_lambda(tg_ctx* ctx, int site, int leg, const double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->set_lambda(site, leg, host);
+  });
+}
+tg_status tg_get_lambda(tg_ctx* ctx, int site, int leg, double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->get_lambda(site, leg, host);
+  });
+}
+tg_status tg_set_env(tg_ctx* ctx, int which, int site, const double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->set_env(which, site, host);
+  });
+}
+tg_status tg_get_env(tg_ctx* ctx, int which, int site, double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->get_env(which, site, host);
+  });
+}
+tg_status tg_ctm_init(tg_ctx* ctx) {
+  return guard([&] { E(ctx)->ctm_init(); });
+}
+tg_status tg_ctm_move(tg_ctx* ctx, int dir, int line) {
+  return guard([&] {
+    E(ctx)->ctm_move(dir, line);
+    E(ctx)->sync();
+  });
+}
+tg_status tg_ctm_sweep(tg_ctx* ctx) {
+  return guard([&] { E(ctx)->ctm_sweep(); });
+}
+tg_status tg_ctm_check_convergence(tg_ctx* ctx, int* converged, double* sig_max) {
+  return guard([&] { E(ctx)->check_convergence(converged, sig_max); });
+}
+tg_status tg_ctm_run(tg_ctx* ctx, int initialize, int* iterations, int* converged, double* sig_max) {
+  return guard([&] { E(ctx)->ctm_run(initialize, iterations, converged, sig_max); });
+}
+tg_status tg_corner_spectrum(tg_ctx* ctx, int which, int site, double* host) {
+  return guard([&] {
+    need(host, "host");
+    E(ctx)->corner_spectrum(which, site, host);
+  });
+}
+tg_status tg_measure_onesite(tg_ctx* ctx, int site, const double* op, double* out) {
+  return guard([&] {
+    need(op, "op");
+    need(out, "out");
+    E(ctx)->measure_onesite(site, op, out);
+  });
+}
+tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const double* op, double* out) {
+  return guard([&] {
+    need(op, "op");
+    need(out, "out");
+    E(ctx)->measure_bond_op12(source, dx, dy, op, out);
+  });
+}
+tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op) {
+  return guard([&] {
+    need(op, "op");
+    E(ctx)->su_onesite(site, op);
+  });
+}
+tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op) {
+  return guard([&] {
+    need(op, "op");
+    E(ctx)->su_bond(source, source_leg, op);
+  });
+}
+tg_status tg_sync(tg_ctx* ctx) {
+  return guard([&] { E(ctx)->sync(); });
+}
+uint64_t tg_kernel_launch_count(void) { return tg::launch_count(); }
+
+}  // extern "C"

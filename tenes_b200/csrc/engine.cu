@@ -1,0 +1,871 @@
+// CTMRG environment engine of libtenes_gpu.
+//
+// The driver mirrors src/iTPS/core/ctm.cpp contraction by contraction
+// (same tensordot sequences, same leg orders), so every intermediate can be
+// compared one to one with the reference algorithm.  All tensors stay on the
+// device; contractions run on the hand-written DMMA kernels of kernels.cu,
+// the dense projector SVD and the simple-update QR / SVD on cuSOLVER.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dtensor.hpp"
+#include "engine.hpp"
+#include "kernels.cuh"
+
+namespace tg {
+
+namespace {
+
+void check_sol(cusolverStatus_t s, const char* what) {
+  if (s != CUSOLVER_STATUS_SUCCESS) fail(TG_E_CUDA, std::string(what) + ": cuSOLVER status " + std::to_string(static_cast<int>(s)));
+}
+
+using V = std::vector<int>;
+
+}  // namespace
+
+template <typename T>
+struct EngineT final : Engine {
+  static constexpr bool CPLX = is_cplx<T>::value;
+  static constexpr int NW = CPLX ? 2 : 1;  // doubles per element
+
+  Lattice lat;
+  tg_params P;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  cusolverDnHandle_t sol = nullptr;
+
+  std::vector<DT<T>> Tn;
+  std::vector<std::array<DT<T>, 3>> Trot;  // right (2,3,0,1,4), top (1,2,3,0,4), bottom (3,0,1,2,4)
+  std::vector<bool> rot_ok;
+  std::array<std::vector<DT<T>>, 4> C;  // C1..C4
+  std::array<std::vector<DT<T>>, 4> E;  // eTt, eTr, eTb, eTl
+  std::vector<std::array<std::vector<double>, 4>> lambda;
+  bool env_ready = false;
+  DT<double> spec_old;
+  bool spec_old_ok = false;
+
+  unsigned long long* d_max = nullptr;
+  int* d_info = nullptr;
+  int* d_cut = nullptr;
+  const T** d_ptrs = nullptr;
+  const T** h_ptrs = nullptr;  // pinned
+  double* h_sig = nullptr;     // pinned
+
+  EngineT(const tg_lattice_desc* ld, const tg_params* p, int device) : P(*p), dev(device) {
+    if (!ld || !ld->physical_dims || !ld->virtual_dims) fail(TG_E_INPUT, "lattice description is incomplete");
+    lat = Lattice(ld->LX, ld->LY, ld->skew);
+    lat.pdim.resize(lat.N);
+    lat.vdim.resize(lat.N);
+    for (int i = 0; i < lat.N; ++i) {
+      lat.pdim[i] = ld->physical_dims[i];
+      for (int l = 0; l < 4; ++l) lat.vdim[i][l] = ld->virtual_dims[4 * i + l];
+    }
+    lat.check_dims();
+    if (P.chi < 1) fail(TG_E_INPUT, "chi must be positive");
+    if (P.rsvd_oversampling_factor < 1.0) fail(TG_E_INPUT, "rsvd_oversampling_factor must be >= 1.0");
+    TG_CUDA(cudaSetDevice(dev));
+    TG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaMemPool_t pool;
+    TG_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = UINT64_MAX;
+    TG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    check_sol(cusolverDnCreate(&sol), "cusolverDnCreate");
+    check_sol(cusolverDnSetStream(sol, st), "cusolverDnSetStream");
+    TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long)));
+    TG_CUDA(cudaMalloc(&d_info, sizeof(int) * 4));
+    TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * 4));
+    TG_CUDA(cudaMalloc(&d_ptrs, sizeof(T*) * 4 * lat.N));
+    TG_CUDA(cudaMallocHost(&h_ptrs, sizeof(T*) * 4 * lat.N));
+    TG_CUDA(cudaMallocHost(&h_sig, sizeof(double) * 4 * lat.N));
+    Tn.resize(lat.N);
+    Trot.resize(lat.N);
+    rot_ok.assign(lat.N, false);
+    lambda.resize(lat.N);
+    for (int i = 0; i < lat.N; ++i) {
+      const auto& v = lat.vdim[i];
+      Tn[i] = zeros<T>({v[0], v[1], v[2], v[3], lat.pdim[i]}, st);
+      for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+    }
+    const int64_t chi = P.chi;
+    for (int k = 0; k < 4; ++k) {
+      C[k].resize(lat.N);
+      E[k].resize(lat.N);
+    }
+    for (int i = 0; i < lat.N; ++i) {
+      for (int k = 0; k < 4; ++k) C[k][i] = zeros<T>({chi, chi}, st);
+      // eTt: vdim[1], eTr: vdim[2], eTb: vdim[3], eTl: vdim[0] (tensors.cpp:57-60)
+      const int64_t dt = lat.vdim[i][1], dr = lat.vdim[i][2], db = lat.vdim[i][3], dl = lat.vdim[i][0];
+      E[0][i] = zeros<T>({chi, chi, dt, dt}, st);
+      E[1][i] = zeros<T>({chi, chi, dr, dr}, st);
+      E[2][i] = zeros<T>({chi, chi, db, db}, st);
+      E[3][i] = zeros<T>({chi, chi, dl, dl}, st);
+    }
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  ~EngineT() override {
+    // release device tensors before the stream goes away
+    Tn.clear();
+    Trot.clear();
+    for (auto& v : C) v.clear();
+    for (auto& v : E) v.clear();
+    spec_old = DT<double>();
+    if (st) cudaStreamSynchronize(st);
+    if (sol) cusolverDnDestroy(sol);
+    cudaFree(d_max);
+    cudaFree(d_info);
+    cudaFree(d_cut);
+    cudaFree(d_ptrs);
+    cudaFreeHost(h_ptrs);
+    cudaFreeHost(h_sig);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  // ---------------------------------------------------------------- helpers
+  DT<T> td(const DT<T>& a, const DT<T>& b, const V& x, const V& y, bool ca = false, bool cb = false) {
+    return tensordot<T>(a, b, x, y, st, ca, cb);
+  }
+  DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
+  void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.size(), d_max, st); }
+
+  void upload(DT<T>& t, const double* host) {
+    TG_CUDA(cudaMemcpyAsync(t.p, host, sizeof(T) * t.size(), cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+  void download(const DT<T>& t, double* host) {
+    TG_CUDA(cudaMemcpyAsync(host, t.p, sizeof(T) * t.size(), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+  T scalar(const DT<T>& t) {
+    T v;
+    TG_CUDA(cudaMemcpyAsync(&v, t.p, sizeof(T), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    return v;
+  }
+  DT<T> from_host(const Shape& s, const double* host) {
+    DT<T> t(s, st);
+    TG_CUDA(cudaMemcpyAsync(t.p, host, sizeof(T) * t.size(), cudaMemcpyHostToDevice, st));
+    return t;
+  }
+
+  void check_site(int site) const {
+    if (site < 0 || site >= lat.N) fail(TG_E_INPUT, "site index out of range: " + std::to_string(site));
+  }
+
+  const DT<T>& rot(int site, int which) {
+    if (!rot_ok[site]) {
+      Trot[site][0] = tr(Tn[site], {2, 3, 0, 1, 4});
+      Trot[site][1] = tr(Tn[site], {1, 2, 3, 0, 4});
+      Trot[site][2] = tr(Tn[site], {3, 0, 1, 2, 4});
+      rot_ok[site] = true;
+    }
+    return Trot[site][which];
+  }
+
+  // Singular value decomposition of a row-major m x n matrix A (consumed):
+  // U (m x k), s (k), VT (k x n), k = min(m, n).  cuSOLVER gesvd works on
+  // column-major data with rows >= cols; for m <= n the row-major buffer is
+  // the column-major A^T and the factors of A^T give those of A without any
+  // transposition (U_A = conj(V_{A^T}), VT_A = U_{A^T}^T).
+  void svd(DT<T>& A, int64_t m, int64_t n, DT<T>& U, DT<double>& s, DT<T>& VT) {
+    if (m > n) {
+      // work on the transpose: A^T (n x m), n < m
+      DT<T> At = tr(reshape(A, {m, n}), {1, 0});
+      DT<T> Ut, VTt;
+      svd(At, n, m, Ut, s, VTt);  // A^T = Ut s VTt  ->  A = VTt^T s Ut^T
+      const int64_t k = n;
+      // U_A = (VTt)^T (m x k) without conj; VT_A = (Ut)^T (k x n)
+      U = tr(reshape(VTt, {k, m}), {1, 0});
+      VT = tr(reshape(Ut, {n, k}), {1, 0});
+      return;
+    }
+    const int64_t k = m;  // m <= n
+    // column-major view: B = A^T is n x m (rows >= cols)
+    const int rows = static_cast<int>(n), cols = static_cast<int>(m);
+    s = DT<double>({k}, st);
+    DT<T> Ub({k, n}, st);   // U_B: n x k column-major  == VT_A row-major (k x n)
+    DT<T> VTb({k, k}, st);  // VT_B: k x k column-major == U_A row-major (m x k)
+    int lwork = 0;
+    if constexpr (CPLX) {
+      check_sol(cusolverDnZgesvd_bufferSize(sol, rows, cols, &lwork), "Zgesvd_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
+      DT<double> rwork({std::max<int64_t>(5 * k, 1)}, st);
+      check_sol(cusolverDnZgesvd(sol, 'S', 'S', rows, cols, reinterpret_cast<cuDoubleComplex*>(A.p), rows, s.p,
+                                 reinterpret_cast<cuDoubleComplex*>(Ub.p), rows,
+                                 reinterpret_cast<cuDoubleComplex*>(VTb.p), cols,
+                                 reinterpret_cast<cuDoubleComplex*>(work.p), lwork, rwork.p, d_info),
+                "Zgesvd");
+    } else {
+      check_sol(cusolverDnDgesvd_bufferSize(sol, rows, cols, &lwork), "Dgesvd_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
+      check_sol(cusolverDnDgesvd(sol, 'S', 'S', rows, cols, A.p, rows, s.p, Ub.p, rows, VTb.p, cols, work.p,
+                                 lwork, nullptr, d_info),
+                "Dgesvd");
+    }
+    U = reshape(VTb, {m, k});
+    VT = reshape(Ub, {k, n});
+    if constexpr (CPLX) {
+      // U_A = conj(V_B) = (VT_B)^T read row-major without conj -> conj needed
+      // only on the value: VT_B holds V_B^H, whose row-major reading is
+      // conj(V_B) already; VT_A = U_B^T has no conjugation.
+    }
+    check_info("gesvd");
+  }
+
+  void check_info(const char* what) {
+    int info = 0;
+    TG_CUDA(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (info != 0) fail(TG_E_RUNTIME, std::string(what) + " failed, info = " + std::to_string(info));
+  }
+
+  // QR of a row-major m x n matrix: Q (m x k), R (k x n), k = min(m, n)
+  // (Householder, cuSOLVER geqrf + orgqr on a column-major copy).
+  void qr(const DT<T>& A, int64_t m, int64_t n, DT<T>& Q, DT<T>& R) {
+    const int64_t k = std::min(m, n);
+    DT<T> Ac = tr(reshape(A, {m, n}), {1, 0});  // row-major (n, m) == column-major (m, n)
+    DT<T> tau({std::max<int64_t>(k, 1)}, st);
+    int lwork = 0, lwork2 = 0;
+    const int im = static_cast<int>(m), in = static_cast<int>(n), ik = static_cast<int>(k);
+    if constexpr (CPLX) {
+      auto* a = reinterpret_cast<cuDoubleComplex*>(Ac.p);
+      auto* t = reinterpret_cast<cuDoubleComplex*>(tau.p);
+      check_sol(cusolverDnZgeqrf_bufferSize(sol, im, in, a, im, &lwork), "Zgeqrf_bufferSize");
+      check_sol(cusolverDnZungqr_bufferSize(sol, im, ik, ik, a, im, t, &lwork2), "Zungqr_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
+      auto* w = reinterpret_cast<cuDoubleComplex*>(work.p);
+      check_sol(cusolverDnZgeqrf(sol, im, in, a, im, t, w, std::max(lwork, lwork2), d_info), "Zgeqrf");
+      // R: upper k x n of the factored matrix (column-major (m, n))
+      R = DT<T>({n, k}, st);  // fill as row-major (n, k) == column-major (k, n)
+      extract_r(Ac, m, n, k, R);
+      check_sol(cusolverDnZungqr(sol, im, ik, ik, a, im, t, w, std::max(lwork, lwork2), d_info), "Zungqr");
+    } else {
+      check_sol(cusolverDnDgeqrf_bufferSize(sol, im, in, Ac.p, im, &lwork), "Dgeqrf_bufferSize");
+      check_sol(cusolverDnDorgqr_bufferSize(sol, im, ik, ik, Ac.p, im, tau.p, &lwork2), "Dorgqr_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
+      check_sol(cusolverDnDgeqrf(sol, im, in, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), d_info), "Dgeqrf");
+      R = DT<T>({n, k}, st);
+      extract_r(Ac, m, n, k, R);
+      check_sol(cusolverDnDorgqr(sol, im, ik, ik, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), d_info),
+                "Dorgqr");
+    }
+    check_info("qr");
+    // Q: first k columns of the column-major (m, *) buffer -> row-major (m, k)
+    DT<T> Qc = DT<T>({k, m}, st);
+    TG_CUDA(cudaMemcpyAsync(Qc.p, Ac.p, sizeof(T) * k * m, cudaMemcpyDeviceToDevice, st));
+    Q = tr(Qc, {1, 0});
+    R = tr(R, {1, 0});  // column-major (k, n) -> row-major (k, n)
+  }
+
+  // copy the upper-trapezoidal k x n block of a column-major (m, n) matrix
+  // into column-major (k, n) storage (row-major (n, k)), zeroing below the diagonal
+  void extract_r(const DT<T>& Ac, int64_t m, int64_t n, int64_t k, DT<T>& R) {
+    std::vector<T> h(static_cast<size_t>(m * n)), r(static_cast<size_t>(k * n));
+    TG_CUDA(cudaMemcpyAsync(h.data(), Ac.p, sizeof(T) * m * n, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    for (int64_t c = 0; c < n; ++c)
+      for (int64_t rr = 0; rr < k; ++rr) {
+        T v = h[static_cast<size_t>(rr + c * m)];
+        if (rr > c) std::memset(&v, 0, sizeof(T));
+        r[static_cast<size_t>(rr + c * k)] = v;
+      }
+    TG_CUDA(cudaMemcpyAsync(R.p, r.data(), sizeof(T) * k * n, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ------------------------------------------------------------ CTM pieces
+  // LT = Tn1*(((C1*eT1)*eT8)*conj(Tn1)), legs (t12,t41,e12,e78,tc12,tc41)  (ctm.cpp:207-212)
+  DT<T> block_LT(const DT<T>& C1, const DT<T>& eT1, const DT<T>& eT8, const DT<T>& T1) {
+    DT<T> X = td(td(td(C1, eT1, {1}, {0}), eT8, {0}, {1}), T1, {2, 5}, {1, 0}, false, true);
+    return td(T1, X, {0, 1, 4}, {3, 1, 6});
+  }
+  // LB = Tn4*(((C4*eT7)*eT6)*conj(Tn4)), legs (t41,t34,e78,e56,tc41,tc34)  (ctm.cpp:222-227)
+  DT<T> block_LB(const DT<T>& C4, const DT<T>& eT7, const DT<T>& eT6, const DT<T>& T4) {
+    DT<T> X = td(td(td(C4, eT7, {1}, {0}), eT6, {0}, {1}), T4, {2, 5}, {0, 3}, false, true);
+    return td(T4, X, {0, 3, 4}, {1, 3, 6});
+  }
+
+  // Truncated projectors from M (nrow x ncol, consumed):
+  // U_c (nrow x w), VT_c (w x ncol) scaled by 1/sqrt(s), w = min(k, chi)
+  void truncated_factors(DT<T>& M, int64_t nrow, int64_t ncol, DT<T>& Uc, DT<T>& VTc) {
+    DT<T> U, VT;
+    DT<double> s;
+    svd(M, nrow, ncol, U, s, VT);
+    const int64_t k = std::min(nrow, ncol);
+    const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
+    DT<double> sinv({w}, st);
+    truncation(s.p, k, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut, st);
+    Uc = DT<T>({nrow, w}, st);
+    scale_cols<T>(U.p, k, nrow, w, sinv.p, false, Uc.p, st);
+    VTc = DT<T>({w, ncol}, st);
+    scale_rows<T>(VT.p, ncol, ncol, w, sinv.p, false, VTc.p, st);
+  }
+
+  // Calc_projector_left_block (ctm.cpp:174-318)
+  void proj_left_block(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT6,
+                       const DT<T>& eT7, const DT<T>& eT8, const DT<T>& T1, const DT<T>& T4, DT<T>& PU,
+                       DT<T>& PL) {
+    const int64_t e12 = eT1.dim(1), e56 = eT6.dim(0), e78 = eT8.dim(0);
+    const int64_t t12 = T1.dim(2), t41 = T1.dim(3), t34 = T4.dim(2);
+    if (t41 != 1) {
+      DT<T> LT = block_LT(C1, eT1, eT8, T1);
+      DT<T> LB = block_LB(C4, eT7, eT6, T4);
+      const int64_t nrow = t12 * e12 * t12, ncol = t34 * e56 * t34;
+      DT<T> Uc, VTc;
+      if ((t12 != 1 && t34 != 1) && P.use_rsvd) {
+        fail(TG_E_INPUT, "use_rsvd is not available in this build of the FP64 path");
+      } else {
+        DT<T> M = td(LT, LB, {1, 3, 5}, {0, 2, 4});
+        truncated_factors(M, nrow, ncol, Uc, VTc);
+      }
+      const int64_t w = Uc.dim(1);
+      DT<T> VTc4 = reshape(VTc, {w, t34, e56, t34});
+      DT<T> Uc4 = reshape(Uc, {t12, e12, t12, w});
+      PU = tr(td(LB, VTc4, {1, 3, 5}, {1, 2, 3}, false, true), {1, 0, 2, 3});
+      PL = tr(td(LT, Uc4, {0, 2, 4}, {0, 1, 2}, false, true), {1, 0, 2, 3});
+    } else {
+      PU = DT<T>({e78, 1, 1, e78}, st);
+      identity<T>(PU.p, e78, st);
+      PL = clone(PU, st);
+    }
+  }
+
+  // Calc_projector_updown_blocks (ctm.cpp:320-491), full-SVD branch
+  void proj_updown(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                   const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                   const DT<T>& eT7, const DT<T>& eT8, const DT<T>& T1, const DT<T>& T2, const DT<T>& T3,
+                   const DT<T>& T4, DT<T>& PU, DT<T>& PL) {
+    const int64_t e78 = eT7.dim(1);
+    const int64_t t23 = T2.dim(3), t41 = T4.dim(1);
+    (void)t23;
+    if (t41 != 1) {
+      DT<T> LT = block_LT(C1, eT1, eT8, T1);
+      DT<T> X = td(td(td(C2, eT3, {1}, {0}), eT2, {0}, {1}), T2, {2, 5}, {2, 1}, false, true);
+      DT<T> RT = td(T2, X, {1, 2, 4}, {3, 1, 6});
+      X = td(td(td(C3, eT5, {1}, {0}), eT4, {0}, {1}), T3, {2, 5}, {3, 2}, false, true);
+      DT<T> RB = td(T3, X, {2, 3, 4}, {3, 1, 6});
+      DT<T> LB = block_LB(C4, eT7, eT6, T4);
+      if (t23 != 1 && P.use_rsvd) fail(TG_E_INPUT, "use_rsvd is not available in this build of the FP64 path");
+      DT<T> R1 = td(RT, LT, {0, 3, 4}, {0, 2, 4});
+      DT<T> R2 = td(RB, LB, {0, 2, 4}, {1, 3, 5});
+      DT<T> M = td(R1, R2, {3, 4, 5}, {3, 4, 5});
+      const int64_t nrow = M.dim(0) * M.dim(1) * M.dim(2), ncol = M.dim(3) * M.dim(4) * M.dim(5);
+      DT<T> Uc, VTc;
+      const Shape ms = M.sh;
+      truncated_factors(M, nrow, ncol, Uc, VTc);
+      const int64_t w = Uc.dim(1);
+      DT<T> VTc4 = reshape(VTc, {w, ms[3], ms[4], ms[5]});
+      DT<T> Uc4 = reshape(Uc, {ms[0], ms[1], ms[2], w});
+      PU = tr(td(R2, VTc4, {0, 1, 2}, {1, 2, 3}, false, true), {1, 0, 2, 3});
+      PL = tr(td(R1, Uc4, {0, 1, 2}, {0, 1, 2}, false, true), {1, 0, 2, 3});
+    } else {
+      PU = DT<T>({e78, 1, 1, e78}, st);
+      identity<T>(PU.p, e78, st);
+      PL = clone(PU, st);
+    }
+  }
+
+  // Calc_Next_CTM (ctm.cpp:493-518)
+  void next_ctm(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT6, const DT<T>& PU,
+                const DT<T>& PL, DT<T>& C1o, DT<T>& C4o) {
+    C1o = td(PU, td(C1, eT1, {1}, {0}), {0, 1, 2}, {0, 2, 3});
+    C4o = td(td(eT6, C4, {1}, {0}), PL, {3, 1, 2}, {0, 1, 2});
+    normalize(C1o);
+    normalize(C4o);
+  }
+
+  // Calc_Next_eT (ctm.cpp:520-552)
+  DT<T> next_et(const DT<T>& eT8, const DT<T>& T1, const DT<T>& PU, const DT<T>& PL) {
+    DT<T> X = td(T1, td(eT8, PL, {1}, {0}), {0, 1}, {2, 4}, true, false);
+    X = td(T1, X, {0, 1, 4}, {4, 5, 2});
+    DT<T> e = tr(td(X, PU, {1, 3, 4}, {1, 2, 0}), {3, 2, 0, 1});
+    normalize(e);
+    return e;
+  }
+
+  // ------------------------------------------------------------- the moves
+  void left_move(int ix) {
+    auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
+    auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
+    const int LY = lat.LY_noskew;
+    std::vector<DT<T>> PUs(LY), PLs(LY);
+    for (int iy = 0; iy < LY; ++iy) {
+      const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
+      if (P.projector_corner)
+        proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
+      else
+        proj_updown(C1[i], C2[j], C3[k], C4[l], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i],
+                    Tn[i], Tn[j], Tn[k], Tn[l], PUs[iy], PLs[iy]);
+    }
+    auto C1b = C1, C4b = C4, eTlb = eTl;
+    for (int iy = 0; iy < LY; ++iy) {
+      const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
+      const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
+      next_ctm(C1b[i], C4b[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
+      eTl[j] = next_et(eTlb[i], Tn[i], PUs[iy], PLs[up]);
+      eTl[k] = next_et(eTlb[l], Tn[l], PUs[dn], PLs[iy]);
+    }
+  }
+
+  void right_move(int ix) {
+    auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
+    auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
+    const int LY = lat.LY_noskew;
+    std::vector<DT<T>> PUs(LY), PLs(LY);
+    for (int iy = 0; iy < LY; ++iy) {
+      const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
+      if (P.projector_corner)
+        proj_left_block(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], rot(k, 0), rot(j, 0), PUs[iy], PLs[iy]);
+      else
+        proj_updown(C3[k], C4[l], C1[i], C2[j], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k],
+                    rot(k, 0), rot(l, 0), rot(i, 0), rot(j, 0), PUs[iy], PLs[iy]);
+    }
+    auto C2b = C2, C3b = C3, eTrb = eTr;
+    for (int iy = 0; iy < LY; ++iy) {
+      const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
+      const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
+      next_ctm(C3b[k], C2b[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
+      eTr[l] = next_et(eTrb[k], rot(k, 0), PUs[iy], PLs[dn]);
+      eTr[i] = next_et(eTrb[j], rot(j, 0), PUs[up], PLs[iy]);
+    }
+  }
+
+  void top_move(int iy) {
+    auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
+    auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
+    const int LX = lat.LX_noskew;
+    std::vector<DT<T>> PUs(LX), PLs(LX);
+    for (int ix = 0; ix < LX; ++ix) {
+      const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
+      if (P.projector_corner)
+        proj_left_block(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], rot(j, 1), rot(i, 1), PUs[ix], PLs[ix]);
+      else
+        proj_updown(C2[j], C3[k], C4[l], C1[i], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j],
+                    rot(j, 1), rot(k, 1), rot(l, 1), rot(i, 1), PUs[ix], PLs[ix]);
+    }
+    auto C1b = C1, C2b = C2, eTtb = eTt;
+    for (int ix = 0; ix < LX; ++ix) {
+      const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
+      const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
+      next_ctm(C2b[j], C1b[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
+      eTt[k] = next_et(eTtb[j], rot(j, 1), PUs[ix], PLs[rt]);
+      eTt[l] = next_et(eTtb[i], rot(i, 1), PUs[lf], PLs[ix]);
+    }
+  }
+
+  void bottom_move(int iy) {
+    auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
+    auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
+    const int LX = lat.LX_noskew;
+    std::vector<DT<T>> PUs(LX), PLs(LX);
+    for (int ix = 0; ix < LX; ++ix) {
+      const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
+      if (P.projector_corner)
+        proj_left_block(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], rot(l, 2), rot(k, 2), PUs[ix], PLs[ix]);
+      else
+        proj_updown(C4[l], C1[i], C2[j], C3[k], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l],
+                    rot(l, 2), rot(i, 2), rot(j, 2), rot(k, 2), PUs[ix], PLs[ix]);
+    }
+    auto C3b = C3, C4b = C4, eTbb = eTb;
+    for (int ix = 0; ix < LX; ++ix) {
+      const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
+      const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
+      next_ctm(C4b[l], C3b[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
+      eTb[i] = next_et(eTbb[l], rot(l, 2), PUs[ix], PLs[lf]);
+      eTb[j] = next_et(eTbb[k], rot(k, 2), PUs[rt], PLs[ix]);
+    }
+  }
+
+  // ------------------------------------------------------ initialisation
+  DT<T> fit(const DT<T>& X, int64_t d1, int64_t d2, int64_t rest) {
+    const int64_t chi = P.chi;
+    Shape s = rest == 1 ? Shape{chi, chi} : Shape{chi, chi, X.dim(4), X.dim(5)};
+    DT<T> out(s, st);
+    fit_chi<T>(X.p, d1, d2, rest, out.p, chi, st);
+    return out;
+  }
+
+  void ctm_init() override {
+    for (int i = 0; i < lat.N; ++i) {
+      int num = lat.top(lat.left(i));
+      const DT<T>* t = &Tn[num];
+      DT<T> X = tr(td(*t, *t, {0, 1, 4}, {0, 1, 4}, false, true), {1, 3, 0, 2});
+      C[0][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      num = lat.top(lat.right(i));
+      t = &Tn[num];
+      X = tr(td(*t, *t, {1, 2, 4}, {1, 2, 4}, false, true), {0, 2, 1, 3});
+      C[1][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      num = lat.bottom(lat.right(i));
+      t = &Tn[num];
+      X = tr(td(*t, *t, {2, 3, 4}, {2, 3, 4}, false, true), {1, 3, 0, 2});
+      C[2][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      num = lat.bottom(lat.left(i));
+      t = &Tn[num];
+      X = tr(td(*t, *t, {0, 3, 4}, {0, 3, 4}, false, true), {1, 3, 0, 2});
+      C[3][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      num = lat.top(i);
+      t = &Tn[num];
+      X = tr(td(*t, *t, {1, 4}, {1, 4}, false, true), {0, 3, 1, 4, 2, 5});
+      E[0][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      num = lat.right(i);
+      t = &Tn[num];
+      X = tr(td(*t, *t, {2, 4}, {2, 4}, false, true), {1, 4, 2, 5, 0, 3});
+      E[1][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      num = lat.bottom(i);
+      t = &Tn[num];
+      X = tr(td(*t, *t, {3, 4}, {3, 4}, false, true), {2, 5, 0, 3, 1, 4});
+      E[2][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      num = lat.left(i);
+      t = &Tn[num];
+      X = tr(td(*t, *t, {0, 4}, {0, 4}, false, true), {2, 5, 0, 3, 1, 4});
+      E[3][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+    }
+    env_ready = true;
+    spec_old = spectra();
+    spec_old_ok = true;
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  void require_env() const {
+    if (!env_ready) fail(TG_E_STATE, "environment not initialised (call tg_ctm_init or tg_set_env first)");
+  }
+
+  void ctm_move(int dir, int line) override {
+    require_env();
+    const int L = (dir <= 1) ? lat.LX_noskew : lat.LY_noskew;
+    if (line < 0 || line >= L) fail(TG_E_INPUT, "move line out of range");
+    switch (dir) {
+      case 0: left_move(line); break;
+      case 1: right_move(line); break;
+      case 2: top_move(line); break;
+      case 3: bottom_move(line); break;
+      default: fail(TG_E_INPUT, "move direction must be 0..3");
+    }
+  }
+
+  void sweep_impl() {
+    const int LX = lat.LX_noskew, LY = lat.LY_noskew;
+    for (int ix = 0; ix < LX; ++ix) left_move(ix);
+    for (int ix = 0; ix > -LX; --ix) right_move((ix + 1 + LX) % LX);
+    for (int iy = 0; iy > -LY; --iy) top_move((iy + 1 + LY) % LY);
+    for (int iy = 0; iy < LY; ++iy) bottom_move(iy);
+  }
+
+  void ctm_sweep() override {
+    require_env();
+    sweep_impl();
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // normalised corner spectra of every site, ordered (site, corner)
+  DT<double> spectra() {
+    const int cnt = 4 * lat.N;
+    TG_CUDA(cudaStreamSynchronize(st));  // h_ptrs is reused
+    for (int i = 0; i < lat.N; ++i)
+      for (int k = 0; k < 4; ++k) h_ptrs[4 * i + k] = C[k][i].p;
+    TG_CUDA(cudaMemcpyAsync(d_ptrs, h_ptrs, sizeof(T*) * cnt, cudaMemcpyHostToDevice, st));
+    DT<double> out({cnt, static_cast<int64_t>(P.chi)}, st);
+    batched_spectrum<T>(d_ptrs, cnt, P.chi, out.p, nullptr, st);
+    return out;
+  }
+
+  void check_convergence(int* converged, double* sig_max) override {
+    require_env();
+    if (!spec_old_ok) fail(TG_E_STATE, "no previous corner spectra");
+    DT<double> now = spectra();
+    const int cnt = 4 * lat.N;
+    DT<double> sig({cnt}, st);
+    spectrum_distance(now.p, spec_old.p, cnt, P.chi, sig.p, st);
+    TG_CUDA(cudaMemcpyAsync(h_sig, sig.p, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    // early break on the first corner above epsilon, in the reference's
+    // order (site-major, C1..C4), ctm.cpp:828-967
+    double smax = 0.0;
+    bool conv = true;
+    for (int b = 0; b < cnt; ++b) {
+      const double s = h_sig[b];
+      if (s > P.ctm_convergence_epsilon) {
+        smax = s;
+        conv = false;
+        break;
+      } else if (s > smax) {
+        smax = s;
+      }
+    }
+    spec_old = now;
+    if (converged) *converged = conv ? 1 : 0;
+    if (sig_max) *sig_max = smax;
+  }
+
+  void ctm_run(int initialize, int* iterations, int* converged, double* sig_max) override {
+    if (initialize) ctm_init();
+    require_env();
+    if (!initialize || !spec_old_ok) {
+      spec_old = spectra();
+      spec_old_ok = true;
+    }
+    int count = 0, conv = 0;
+    double smax = 0.0;
+    while (!conv && count < P.max_ctm_iteration) {
+      sweep_impl();
+      check_convergence(&conv, &smax);
+      ++count;
+    }
+    if (iterations) *iterations = count;
+    if (converged) *converged = conv;
+    if (sig_max) *sig_max = smax;
+  }
+
+  void corner_spectrum(int which, int site, double* host) override {
+    require_env();
+    check_site(site);
+    if (which < 0 || which > 3) fail(TG_E_INPUT, "corner index must be 0..3");
+    DT<double> sp = spectra();
+    TG_CUDA(cudaMemcpyAsync(host, sp.p + (4 * site + which) * P.chi, sizeof(double) * P.chi,
+                            cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ---------------------------------------------------------- observables
+  // Contract_one_site_iTPS_CTM (contract_itps_ctm/ctm.cpp:89-113)
+  T one_site(int i, const DT<T>& op) {
+    const DT<T>&C1 = C[0][i], &C2 = C[1][i], &C3 = C[2][i], &C4 = C[3][i];
+    const DT<T>&eT1 = E[0][i], &eT2 = E[1][i], &eT3 = E[2][i], &eT4 = E[3][i];
+    const DT<T>& T1 = Tn[i];
+    DT<T> X = td(td(C2, td(C3, eT2, {0}, {1}), {1}, {1}), td(C1, eT1, {1}, {0}), {0}, {1});
+    DT<T> Y = td(td(td(C4, eT4, {1}, {0}), eT3, {0}, {1}), T1, {2, 5}, {0, 3}, false, true);
+    DT<T> Z = td(X, Y, {0, 2, 3, 5}, {2, 5, 0, 4});
+    DT<T> W = td(Z, T1, {0, 1, 2, 3}, {2, 1, 0, 3});
+    return scalar(td(W, op, {0, 1}, {1, 0}));
+  }
+
+  void measure_onesite(int site, const double* op, double* out) override {
+    require_env();
+    check_site(site);
+    const int64_t d = lat.pdim[site];
+    DT<T> o = from_host({d, d}, op);
+    T v = one_site(site, o);
+    std::memcpy(out, &v, sizeof(T));
+    if constexpr (!CPLX) out[1] = 0.0;
+  }
+
+  // Contract_two_sites_horizontal_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:213-264)
+  T two_sites_h(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+    DT<T> A = td(eT5, td(C1, td(C4, eT6, {1}, {0}), {0}, {1}), {1}, {1});
+    A = td(T1, A, {0, 3}, {5, 2}, true, false);
+    A = td(T1, A, {0, 3}, {6, 4});
+    A = td(eT1, A, {0, 2, 3}, {7, 0, 3});
+    DT<T> B = td(eT4, td(C2, td(C3, eT3, {0}, {1}), {1}, {1}), {0}, {1});
+    B = td(T2, B, {2, 3}, {5, 2}, true, false);
+    B = td(T2, B, {2, 3}, {6, 4});
+    B = td(eT2, B, {1, 2, 3}, {7, 1, 4});
+    DT<T> X = td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+    return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
+  }
+
+  // Contract_two_sites_vertical_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:266-319)
+  T two_sites_v(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+    DT<T> A = td(eT6, td(C1, td(C2, eT1, {0}, {1}), {1}, {1}), {1}, {0});
+    A = td(T1, A, {0, 1}, {2, 5}, true, false);
+    A = td(T1, A, {0, 1}, {4, 6});
+    A = td(eT2, A, {0, 2, 3}, {7, 0, 3});
+    DT<T> B = td(eT5, td(C3, td(C4, eT4, {0}, {1}), {1}, {1}), {0}, {1});
+    B = td(T2, B, {0, 3}, {2, 5}, true, false);
+    B = td(T2, B, {0, 3}, {4, 6});
+    B = td(eT3, B, {1, 2, 3}, {7, 1, 4});
+    DT<T> X = td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+    return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
+  }
+
+  // twosite_obs.cpp:186-222: nearest-neighbour op12 with the source/target
+  // orientation rule
+  void measure_bond_op12(int source, int dx, int dy, const double* op, double* out) override {
+    require_env();
+    check_site(source);
+    if (std::abs(dx) + std::abs(dy) != 1) fail(TG_E_INPUT, "op12 bond must be a nearest-neighbour bond");
+    const int target = lat.other(source, dx, dy);
+    const int64_t d1 = lat.pdim[source], d2 = lat.pdim[target];
+    T v;
+    auto swapped = [&](int64_t a, int64_t b) {
+      // transpose(op, {1,0,3,2}) on the host
+      std::vector<double> h(static_cast<size_t>(a * b * a * b * NW));
+      for (int64_t i = 0; i < b; ++i)
+        for (int64_t j = 0; j < a; ++j)
+          for (int64_t k = 0; k < b; ++k)
+            for (int64_t l = 0; l < a; ++l) {
+              const int64_t src = ((j * b + i) * a + l) * b + k;
+              const int64_t dst = ((i * a + j) * b + k) * a + l;
+              for (int w = 0; w < NW; ++w) h[static_cast<size_t>(dst * NW + w)] = op[src * NW + w];
+            }
+      return from_host({b, a, b, a}, h.data());
+    };
+    if (dy == 0) {
+      const int source_col = dx >= 0 ? 0 : 1;
+      const int left = lat.other(source, -source_col, 0), right = lat.other(source, 1 - source_col, 0);
+      DT<T> o = (left == source) ? from_host({d1, d2, d1, d2}, op) : swapped(d1, d2);
+      v = two_sites_h(C[0][left], C[1][right], C[2][right], C[3][left], E[0][left], E[0][right], E[1][right],
+                      E[2][right], E[2][left], E[3][left], Tn[left], Tn[right], o);
+    } else {
+      const int source_row = dy >= 0 ? 1 : 0;
+      const int top = lat.other(source, 0, source_row), bottom = lat.other(source, 0, source_row - 1);
+      DT<T> o = (top == source) ? from_host({d1, d2, d1, d2}, op) : swapped(d1, d2);
+      v = two_sites_v(C[0][top], C[1][top], C[2][bottom], C[3][bottom], E[0][top], E[1][top], E[1][bottom],
+                      E[2][bottom], E[3][bottom], E[3][top], Tn[top], Tn[bottom], o);
+    }
+    std::memcpy(out, &v, sizeof(T));
+    if constexpr (!CPLX) out[1] = 0.0;
+  }
+
+  // -------------------------------------------------------- simple update
+  void su_onesite(int site, const double* op) override {
+    check_site(site);
+    const int64_t d = lat.pdim[site];
+    DT<T> o = from_host({d, d}, op);
+    Tn[site] = td(Tn[site], o, {4}, {0});
+    rot_ok[site] = false;
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  DT<double> dvec(const std::vector<double>& h) {
+    DT<double> t({static_cast<int64_t>(h.size())}, st);
+    TG_CUDA(cudaMemcpyAsync(t.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaStreamSynchronize(st));  // h may be a temporary
+    return t;
+  }
+
+  // multiply leg `ax` of tensor t by v (multiply_vector)
+  void mulvec(DT<T>& t, int ax, const std::vector<double>& v) {
+    int64_t outer = 1, inner = 1;
+    for (int i = 0; i < ax; ++i) outer *= t.dim(i);
+    for (int i = ax + 1; i < t.rank(); ++i) inner *= t.dim(i);
+    DT<double> dv = dvec(v);
+    scale_leg<T>(t.p, outer, t.dim(ax), inner, dv.p, st);
+  }
+
+  // core::Simple_update_bond (core/simple_update.cpp:50-198)
+  void su_bond(int source, int connect1, const double* op) override {
+    check_site(source);
+    if (connect1 < 0 || connect1 > 3) fail(TG_E_INPUT, "source_leg must be 0..3");
+    const int target = lat.neighbor(source, connect1);
+    const int connect2 = (connect1 + 2) % 4;
+    static const int outer[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+    static const int to_last[4][5] = {{1, 2, 3, 0, 4}, {0, 2, 3, 1, 4}, {0, 1, 3, 2, 4}, {0, 1, 2, 3, 4}};
+    static const int back1[4][5] = {{4, 0, 1, 2, 3}, {0, 4, 1, 2, 3}, {0, 1, 4, 2, 3}, {0, 1, 2, 4, 3}};
+    static const int back2[4][5] = {{3, 0, 1, 2, 4}, {0, 3, 1, 2, 4}, {0, 1, 3, 2, 4}, {0, 1, 2, 3, 4}};
+    auto& lam1 = lambda[source];
+    auto& lam2 = lambda[target];
+    auto inv = [&](const std::vector<double>& l) {
+      std::vector<double> r(l.size());
+      for (size_t j = 0; j < l.size(); ++j) r[j] = l[j] > P.inverse_lambda_cut ? 1.0 / l[j] : 0.0;
+      return r;
+    };
+    const int64_t dc = Tn[source].dim(connect1);
+    DT<T> T1 = clone(Tn[source], st);
+    for (int a = 0; a < 3; ++a) mulvec(T1, outer[connect1][a], lam1[outer[connect1][a]]);
+    T1 = tr(T1, V(to_last[connect1], to_last[connect1] + 5));
+    DT<T> T2 = clone(Tn[target], st);
+    for (int a = 0; a < 3; ++a) mulvec(T2, outer[connect2][a], lam2[outer[connect2][a]]);
+    T2 = tr(T2, V(to_last[connect2], to_last[connect2] + 5));
+    DT<T> Q1, R1, Q2, R2;
+    const int64_t m1 = T1.dim(0) * T1.dim(1) * T1.dim(2), n1 = T1.dim(3) * T1.dim(4);
+    const int64_t m2 = T2.dim(0) * T2.dim(1) * T2.dim(2), n2 = T2.dim(3) * T2.dim(4);
+    qr(T1, m1, n1, Q1, R1);
+    qr(T2, m2, n2, Q2, R2);
+    const int64_t k1 = std::min(m1, n1), k2 = std::min(m2, n2);
+    Q1 = reshape(Q1, {T1.dim(0), T1.dim(1), T1.dim(2), k1});
+    R1 = reshape(R1, {k1, T1.dim(3), T1.dim(4)});
+    Q2 = reshape(Q2, {T2.dim(0), T2.dim(1), T2.dim(2), k2});
+    R2 = reshape(R2, {k2, T2.dim(3), T2.dim(4)});
+    const int64_t d1 = T1.dim(4), d2 = T2.dim(4);
+    DT<T> op12 = from_host({d1, d2, d1, d2}, op);
+    DT<T> Theta = td(td(R1, R2, {1}, {1}), op12, {1, 3}, {0, 1});  // (c1, c2, m1o, m2o)
+    DT<T> Th = tr(Theta, {0, 2, 1, 3});
+    DT<T> U, VT;
+    DT<double> s;
+    const int64_t rows = k1 * d1, cols = k2 * d2;
+    svd(Th, rows, cols, U, s, VT);
+    const int64_t kk = std::min(rows, cols);
+    std::vector<double> hs(static_cast<size_t>(kk));
+    TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * kk, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (dc > kk) fail(TG_E_RUNTIME, "simple update: bond dimension exceeds the rank of Theta");
+    std::vector<double> lc(hs.begin(), hs.begin() + dc);
+    double nrm = 0.0;
+    for (double x : lc) nrm += x * x;
+    nrm = std::sqrt(nrm);
+    for (double& x : lc) x = std::sqrt(x / nrm);
+    DT<double> dlc = dvec(lc);
+    DT<T> Uc({rows, dc}, st);
+    scale_cols<T>(U.p, kk, rows, static_cast<int>(dc), dlc.p, false, Uc.p, st);
+    DT<T> VTc({dc, cols}, st);
+    scale_rows<T>(VT.p, cols, cols, static_cast<int>(dc), dlc.p, false, VTc.p, st);
+    Uc = reshape(Uc, {k1, d1, dc});
+    VTc = reshape(VTc, {dc, k2, d2});
+    auto il1 = lam1, il2 = lam2;
+    for (int a = 0; a < 3; ++a) mulvec(Q1, a, inv(lam1[outer[connect1][a]]));
+    for (int a = 0; a < 3; ++a) mulvec(Q2, a, inv(lam2[outer[connect2][a]]));
+    Tn[source] = tr(td(Q1, Uc, {3}, {0}), V(back1[connect1], back1[connect1] + 5));
+    Tn[target] = tr(td(Q2, VTc, {3}, {1}), V(back2[connect2], back2[connect2] + 5));
+    lambda[source][connect1] = lc;
+    lambda[target][connect2] = lc;
+    rot_ok[source] = rot_ok[target] = false;
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ------------------------------------------------------------- host I/O
+  void set_site_tensor(int site, const double* host) override {
+    check_site(site);
+    upload(Tn[site], host);
+    rot_ok[site] = false;
+  }
+  void get_site_tensor(int site, double* host) override {
+    check_site(site);
+    download(Tn[site], host);
+  }
+  void set_lambda(int site, int leg, const double* host) override {
+    check_site(site);
+    if (leg < 0 || leg > 3) fail(TG_E_INPUT, "leg must be 0..3");
+    auto& l = lambda[site][leg];
+    std::copy(host, host + l.size(), l.begin());
+  }
+  void get_lambda(int site, int leg, double* host) override {
+    check_site(site);
+    if (leg < 0 || leg > 3) fail(TG_E_INPUT, "leg must be 0..3");
+    const auto& l = lambda[site][leg];
+    std::copy(l.begin(), l.end(), host);
+  }
+  DT<T>& env_ref(int which, int site) {
+    check_site(site);
+    if (which < 0 || which > 7) fail(TG_E_INPUT, "environment index must be 0..7");
+    return which < 4 ? C[which][site] : E[which - 4][site];
+  }
+  void set_env(int which, int site, const double* host) override {
+    DT<T>& t = env_ref(which, site);
+    DT<T> n(t.sh, st);
+    upload(n, host);
+    t = n;
+    env_ready = true;
+    spec_old_ok = false;
+  }
+  void get_env(int which, int site, double* host) override { download(env_ref(which, site), host); }
+  void sync() override { TG_CUDA(cudaStreamSynchronize(st)); }
+};
+
+Engine* make_engine(const tg_lattice_desc* lat, const tg_params* p, int is_complex, int device) {
+  if (!lat || !p) fail(TG_E_INPUT, "null lattice or params");
+  if (is_complex) return new EngineT<cplx>(lat, p, device);
+  return new EngineT<double>(lat, p, device);
+}
+
+}  // namespace tg

@@ -1,0 +1,39 @@
+// The per-context engine: device-resident iTPS state and the CTMRG driver.
+#pragma once
+
+#include <cusolverDn.h>
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "dtensor.hpp"
+#include "lattice.hpp"
+
+namespace tg {
+
+struct Engine {
+  virtual ~Engine() = default;
+  virtual void set_site_tensor(int site, const double* host) = 0;
+  virtual void get_site_tensor(int site, double* host) = 0;
+  virtual void set_lambda(int site, int leg, const double* host) = 0;
+  virtual void get_lambda(int site, int leg, double* host) = 0;
+  virtual void set_env(int which, int site, const double* host) = 0;
+  virtual void get_env(int which, int site, double* host) = 0;
+  virtual void ctm_init() = 0;
+  virtual void ctm_move(int dir, int line) = 0;
+  virtual void ctm_sweep() = 0;
+  virtual void check_convergence(int* converged, double* sig_max) = 0;
+  virtual void ctm_run(int initialize, int* iterations, int* converged, double* sig_max) = 0;
+  virtual void corner_spectrum(int which, int site, double* host) = 0;
+  virtual void measure_onesite(int site, const double* op, double* out) = 0;
+  virtual void measure_bond_op12(int source, int dx, int dy, const double* op, double* out) = 0;
+  virtual void su_onesite(int site, const double* op) = 0;
+  virtual void su_bond(int source, int leg, const double* op) = 0;
+  virtual void sync() = 0;
+};
+
+Engine* make_engine(const tg_lattice_desc* lat, const tg_params* p, int is_complex, int device);
+
+}  // namespace tg

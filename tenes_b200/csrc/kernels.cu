@@ -1,0 +1,668 @@
+// Hand-written sm_100a kernels of the CTMRG path: FP64 tensor-core (DMMA)
+// strided batched matrix product, leg permutation, max-abs normalisation,
+// projector truncation helpers and a batched one-sided Jacobi spectrum.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+
+#include "kernels.cuh"
+
+namespace tg {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+__device__ __forceinline__ double re_of(double x) { return x; }
+__device__ __forceinline__ double re_of(cplx x) { return x.x; }
+__device__ __forceinline__ double im_of(double) { return 0.0; }
+__device__ __forceinline__ double im_of(cplx x) { return x.y; }
+__device__ __forceinline__ double abs_of(double x) { return fabs(x); }
+__device__ __forceinline__ double abs_of(cplx x) { return hypot(x.x, x.y); }
+__device__ __forceinline__ double conj_of(double x) { return x; }
+__device__ __forceinline__ cplx conj_of(cplx x) { return make_double2(x.x, -x.y); }
+__device__ __forceinline__ double mul_real(double x, double a) { return x * a; }
+__device__ __forceinline__ cplx mul_real(cplx x, double a) { return make_double2(x.x * a, x.y * a); }
+template <typename T>
+__device__ __forceinline__ T zero_of();
+template <>
+__device__ __forceinline__ double zero_of<double>() { return 0.0; }
+template <>
+__device__ __forceinline__ cplx zero_of<cplx>() { return make_double2(0.0, 0.0); }
+template <typename T>
+__device__ __forceinline__ T one_of();
+template <>
+__device__ __forceinline__ double one_of<double>() { return 1.0; }
+template <>
+__device__ __forceinline__ cplx one_of<cplx>() { return make_double2(1.0, 0.0); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+int num_blocks(int64_t n, int threads, int64_t cap = 148 * 32) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return static_cast<int>(std::min<int64_t>(b, cap));
+}
+
+// ---------------------------------------------------------------------------
+// GEMM: 64 x 64 x 16 CTA tile, 4 warps of 32 x 32, register-staged double
+// buffering of the global loads, DMMA m8n8k4 on the FP64 tensor pipe.
+// Complex operands are split into real / imaginary planes in shared memory
+// and multiplied with four real DMMAs per complex MAC.
+// ---------------------------------------------------------------------------
+constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 4;
+constexpr int GLD = GBM + GPAD;  // row length of the k-major smem tiles
+
+template <typename T>
+struct GemmParams {
+  const T* A;
+  const T* B;
+  T* C;
+  GemmDesc d;
+};
+
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
+  constexpr int NP = CPLX ? 2 : 1;  // planes
+  extern __shared__ double smem[];
+  // layout: As[stage][plane][GBK][GLD], Bs[stage][plane][GBK][GLD]
+  double* As = smem;
+  double* Bs = smem + 2 * NP * GBK * GLD;
+  const GemmDesc& d = p.d;
+  const int64_t bz = blockIdx.z;
+  const T* A = p.A + bz * d.bA;
+  const T* B = p.B + bz * d.bB;
+  T* C = p.C + bz * d.bC;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * GBM;
+  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * GBN;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int wm = (warp & 1) * 32;
+  const int wn = (warp >> 1) * 32;
+  const bool a_kc = (d.sAk == 1);  // A contiguous along k
+  const bool b_nc = (d.sBn == 1);  // B contiguous along n
+
+  T ra[8], rb[8];
+  auto load_tiles = [&](int64_t k0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
+      int mm, kk;
+      if (a_kc) {
+        kk = idx % GBK;
+        mm = idx / GBK;
+      } else {
+        mm = idx % GBM;
+        kk = idx / GBM;
+      }
+      const int64_t gm = m0 + mm, gk = k0 + kk;
+      ra[i] = (gm < d.M && gk < d.K) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
+      int nn, kb;
+      if (b_nc) {
+        nn = idx % GBN;
+        kb = idx / GBN;
+      } else {
+        kb = idx % GBK;
+        nn = idx / GBK;
+      }
+      const int64_t gn = n0 + nn, gkb = k0 + kb;
+      rb[i] = (gn < d.N && gkb < d.K) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
+    }
+  };
+  auto store_tiles = [&](int stage) {
+    double* as = As + stage * NP * GBK * GLD;
+    double* bs = Bs + stage * NP * GBK * GLD;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
+      int mm, kk;
+      if (a_kc) {
+        kk = idx % GBK;
+        mm = idx / GBK;
+      } else {
+        mm = idx % GBM;
+        kk = idx / GBM;
+      }
+      as[kk * GLD + mm] = re_of(ra[i]);
+      if constexpr (CPLX) as[GBK * GLD + kk * GLD + mm] = d.conjA ? -im_of(ra[i]) : im_of(ra[i]);
+      int nn, kb;
+      if (b_nc) {
+        nn = idx % GBN;
+        kb = idx / GBN;
+      } else {
+        kb = idx % GBK;
+        nn = idx / GBK;
+      }
+      bs[kb * GLD + nn] = re_of(rb[i]);
+      if constexpr (CPLX) bs[GBK * GLD + kb * GLD + nn] = d.conjB ? -im_of(rb[i]) : im_of(rb[i]);
+    }
+  };
+
+  double acc_r[4][4][2];
+  double acc_i[CPLX ? 4 : 1][CPLX ? 4 : 1][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc_r[i][j][0] = acc_r[i][j][1] = 0.0;
+  if constexpr (CPLX) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc_i[i][j][0] = acc_i[i][j][1] = 0.0;
+  }
+
+  const int64_t nk = (d.K + GBK - 1) / GBK;
+  load_tiles(0);
+  store_tiles(0);
+  __syncthreads();
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int stage = static_cast<int>(kt & 1);
+    if (kt + 1 < nk) load_tiles((kt + 1) * GBK);
+    const double* as = As + stage * NP * GBK * GLD;
+    const double* bs = Bs + stage * NP * GBK * GLD;
+#pragma unroll
+    for (int k4 = 0; k4 < GBK; k4 += 4) {
+      const int kr = k4 + (lane & 3);
+      double a_r[4], b_r[4], a_i[CPLX ? 4 : 1], b_i[CPLX ? 4 : 1];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a_r[i] = as[kr * GLD + wm + i * 8 + (lane >> 2)];
+        b_r[i] = bs[kr * GLD + wn + i * 8 + (lane >> 2)];
+        if constexpr (CPLX) {
+          a_i[i] = as[GBK * GLD + kr * GLD + wm + i * 8 + (lane >> 2)];
+          b_i[i] = bs[GBK * GLD + kr * GLD + wn + i * 8 + (lane >> 2)];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(acc_r[i][j][0], acc_r[i][j][1], a_r[i], b_r[j]);
+          if constexpr (CPLX) {
+            dmma(acc_r[i][j][0], acc_r[i][j][1], -a_i[i], b_i[j]);
+            dmma(acc_i[i][j][0], acc_i[i][j][1], a_r[i], b_i[j]);
+            dmma(acc_i[i][j][0], acc_i[i][j][1], a_i[i], b_r[j]);
+          }
+        }
+    }
+    if (kt + 1 < nk) {
+      store_tiles(stage ^ 1);
+    }
+    __syncthreads();
+  }
+
+  // epilogue
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t gm = m0 + wm + i * 8 + (lane >> 2);
+        const int64_t gn = n0 + wn + j * 8 + 2 * (lane & 3) + h;
+        if (gm < d.M && gn < d.N) {
+          T* c = C + gm * d.sCm + gn * d.sCn;
+          if constexpr (CPLX) {
+            cplx v = make_double2(acc_r[i][j][h], acc_i[i][j][h]);
+            if (d.accumulate) {
+              v.x += c->x;
+              v.y += c->y;
+            }
+            *c = v;
+          } else {
+            double v = acc_r[i][j][h];
+            if (d.accumulate) v += *c;
+            *c = v;
+          }
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Permutation: one thread per output element, output-coalesced.
+// ---------------------------------------------------------------------------
+struct PermParams {
+  int rank;
+  int64_t total;
+  int64_t out_dims[8];
+  int64_t src_stride[8];  // stride in `in` of output axis i
+  bool conj;
+};
+
+template <typename T>
+__global__ void permute_kernel(const T* __restrict__ in, T* __restrict__ out, PermParams p) {
+  for (int64_t lin = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; lin < p.total;
+       lin += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t rem = lin, off = 0;
+    for (int i = p.rank - 1; i >= 0; --i) {
+      const int64_t q = rem / p.out_dims[i];
+      off += (rem - q * p.out_dims[i]) * p.src_stride[i];
+      rem = q;
+    }
+    T v = in[off];
+    out[lin] = p.conj ? conj_of(v) : v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// max |x| then x /= max
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void maxabs_kernel(const T* __restrict__ x, int64_t n, unsigned long long* out) {
+  double m = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    m = fmax(m, abs_of(x[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double wmax[32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = (threadIdx.x < (blockDim.x >> 5)) ? wmax[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative doubles order like their bit patterns
+    if (threadIdx.x == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+template <typename T>
+__global__ void divide_kernel(T* __restrict__ x, int64_t n, const unsigned long long* mx) {
+  const double m = __longlong_as_double(static_cast<long long>(*mx));
+  const double inv = 1.0 / m;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] = mul_real(x[i], inv);
+}
+
+template <typename T>
+__global__ void scale_kernel(T* __restrict__ x, int64_t n, double a) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] = mul_real(x[i], a);
+}
+
+template <typename T>
+__global__ void scale_leg_kernel(T* __restrict__ x, int64_t outer, int64_t dim, int64_t inner,
+                                 const double* __restrict__ v) {
+  const int64_t n = outer * dim * inner;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = (i / inner) % dim;
+    x[i] = mul_real(x[i], v[k]);
+  }
+}
+
+template <typename T>
+__global__ void fit_chi_kernel(const T* __restrict__ in, int64_t d1, int64_t d2, int64_t rest,
+                               T* __restrict__ out, int64_t chi) {
+  const int64_t n = chi * chi * rest;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i % rest;
+    const int64_t b = (i / rest) % chi;
+    const int64_t a = i / (rest * chi);
+    out[i] = (a < d1 && b < d2) ? in[(a * d2 + b) * rest + r] : zero_of<T>();
+  }
+}
+
+__global__ void truncation_kernel(const double* __restrict__ s, int64_t n, int chi_cap,
+                                  double cutoff, double* __restrict__ sinv, int chi_out,
+                                  int* cut_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int cut = static_cast<int>(n < chi_cap ? n : chi_cap);
+  const double denom = s[0];
+  for (int i = 0; i < cut; ++i) {
+    if (s[i] / denom > cutoff) {
+      sinv[i] = 1.0 / sqrt(s[i]);
+    } else {
+      cut = i;
+      break;
+    }
+  }
+  for (int i = cut; i < chi_out; ++i) sinv[i] = 0.0;
+  if (cut_out) *cut_out = cut;
+}
+
+template <typename T>
+__global__ void scale_cols_kernel(const T* __restrict__ U, int64_t ldu, int64_t rows, int kc,
+                                  const double* __restrict__ sinv, bool conj, T* __restrict__ out) {
+  const int64_t n = rows * kc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / kc;
+    const int k = static_cast<int>(i - r * kc);
+    T v = U[r * ldu + k];
+    if (conj) v = conj_of(v);
+    out[i] = mul_real(v, sinv[k]);
+  }
+}
+
+template <typename T>
+__global__ void scale_rows_kernel(const T* __restrict__ VT, int64_t ldv, int64_t cols, int kc,
+                                  const double* __restrict__ sinv, bool conj, T* __restrict__ out) {
+  const int64_t n = cols * kc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = i / cols;
+    const int64_t c = i - k * cols;
+    T v = VT[k * ldv + c];
+    if (conj) v = conj_of(v);
+    out[i] = mul_real(v, sinv[k]);
+  }
+}
+
+template <typename T>
+__global__ void identity_kernel(T* __restrict__ out, int64_t e) {
+  const int64_t n = e * e;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[i] = (i / e == i % e) ? one_of<T>() : zero_of<T>();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-sided (Hestenes) Jacobi singular values, one CTA per n x n matrix.
+// Columns live in shared memory (column-major); each warp orthogonalises
+// disjoint column pairs of a round-robin schedule.  Converged when no pair of
+// a sweep needed a rotation (|a_p^H a_q| <= 1e-15 sqrt(|a_p|^2 |a_q|^2)), or
+// after 60 sweeps (the count is reported back).
+// ---------------------------------------------------------------------------
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* mats, int n,
+                                                                double* out, int* sweeps_used) {
+  extern __shared__ double sm[];
+  double* re = sm;                      // n*n column-major
+  double* im = sm + (CPLX ? n * n : 0);  // n*n (complex only)
+  double* nrm = sm + (CPLX ? 2 : 1) * n * n;  // n
+  __shared__ int rotated;
+  const T* M = mats[blockIdx.x];
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx % n;  // row-major source
+    const T v = M[idx];
+    re[c * n + r] = re_of(v);
+    if constexpr (CPLX) im[c * n + r] = im_of(v);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int np = n + (n & 1);
+  int sweep = 0;
+  for (; sweep < 60; ++sweep) {
+    if (threadIdx.x == 0) rotated = 0;
+    __syncthreads();
+    for (int rnd = 0; rnd < np - 1; ++rnd) {
+      for (int pr = warp; pr < np / 2; pr += nw) {
+        auto player = [&](int k) { return k == 0 ? 0 : ((k - 1 + rnd) % (np - 1)) + 1; };
+        int p = player(pr), q = player(np - 1 - pr);
+        if (p >= n || q >= n) continue;
+        if (p > q) {
+          int t = p;
+          p = q;
+          q = t;
+        }
+        double al = 0, be = 0, gr = 0, gi = 0;
+        for (int r = lane; r < n; r += 32) {
+          const double pr_ = re[p * n + r], qr_ = re[q * n + r];
+          al += pr_ * pr_;
+          be += qr_ * qr_;
+          gr += pr_ * qr_;
+          if constexpr (CPLX) {
+            const double pi_ = im[p * n + r], qi_ = im[q * n + r];
+            al += pi_ * pi_;
+            be += qi_ * qi_;
+            gr += pi_ * qi_;
+            gi += pr_ * qi_ - pi_ * qr_;  // Im(conj(a_p) a_q)
+          }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o);
+          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
+        }
+        const double g = CPLX ? hypot(gr, gi) : fabs(gr);
+        if (g == 0.0 || g <= 1e-15 * sqrt(al * be)) continue;
+        // phase e^{-i phi} with gamma = |gamma| e^{i phi}
+        const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
+        const double ph_i = CPLX ? -gi / g : 0.0;
+        const double zeta = (be - al) / (2.0 * g);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        for (int r = lane; r < n; r += 32) {
+          const double apr = re[p * n + r];
+          const double api = CPLX ? im[p * n + r] : 0.0;
+          const double aqr = re[q * n + r];
+          const double aqi = CPLX ? im[q * n + r] : 0.0;
+          // b_q = a_q * e^{-i phi}
+          const double bqr = aqr * ph_r - aqi * ph_i;
+          const double bqi = aqr * ph_i + aqi * ph_r;
+          re[p * n + r] = c * apr - s * bqr;
+          re[q * n + r] = s * apr + c * bqr;
+          if constexpr (CPLX) {
+            im[p * n + r] = c * api - s * bqi;
+            im[q * n + r] = s * api + c * bqi;
+          }
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+    const int any = rotated;
+    __syncthreads();
+    if (!any) break;
+  }
+  // column norms, normalised, sorted descending
+  for (int c = warp; c < n; c += nw) {
+    double a = 0;
+    for (int r = lane; r < n; r += 32) {
+      a += re[c * n + r] * re[c * n + r];
+      if constexpr (CPLX) a += im[c * n + r] * im[c * n + r];
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) nrm[c] = sqrt(a);
+  }
+  __syncthreads();
+  __shared__ double tot;
+  if (threadIdx.x < 32) {
+    double a = 0;
+    for (int c = lane; c < n; c += 32) a += nrm[c] * nrm[c];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) tot = sqrt(a);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const double v = nrm[c];
+    int pos = 0;
+    for (int o = 0; o < n; ++o) {
+      const double w = nrm[o];
+      pos += (w > v) || (w == v && o < c);
+    }
+    out[static_cast<int64_t>(blockIdx.x) * n + pos] = tot > 0 ? v / tot : 0.0;
+  }
+  if (threadIdx.x == 0 && sweeps_used) sweeps_used[blockIdx.x] = sweep;
+}
+
+__global__ void spectrum_distance_kernel(const double* a, const double* c, int count, int n,
+                                         double* sig) {
+  const int b = blockIdx.x;
+  if (b >= count) return;
+  double acc = 0;
+  for (int i = threadIdx.x; i < n; i += 32) {
+    const double d = a[static_cast<int64_t>(b) * n + i] - c[static_cast<int64_t>(b) * n + i];
+    acc += d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (threadIdx.x == 0) sig[b] = sqrt(acc);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T>
+void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
+  if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return;
+  if (d.K <= 0) fail(TG_E_INPUT, "gemm: K must be positive");
+  constexpr bool CPLX = is_cplx<T>::value;
+  constexpr int NP = CPLX ? 2 : 1;
+  const size_t smem = sizeof(double) * 2 * 2 * NP * GBK * GLD;
+  static bool attr_set = false;
+  if (!attr_set) {
+    TG_CUDA(cudaFuncSetAttribute(gemm_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    attr_set = true;
+  }
+  if (d.batch > 65535) fail(TG_E_INPUT, "gemm: batch too large");
+  dim3 grid(static_cast<unsigned>((d.N + GBN - 1) / GBN), static_cast<unsigned>((d.M + GBM - 1) / GBM),
+            static_cast<unsigned>(d.batch));
+  if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
+  GemmParams<T> p{A, B, C, d};
+  gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(p);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>& perm, bool conj,
+             cudaStream_t st) {
+  const int r = static_cast<int>(in_shape.size());
+  if (r > 8) fail(TG_E_INPUT, "permute: rank > 8");
+  PermParams p{};
+  p.rank = r;
+  p.conj = conj;
+  p.total = numel(in_shape);
+  if (p.total == 0) return;
+  int64_t strides[8];
+  int64_t s = 1;
+  for (int i = r - 1; i >= 0; --i) {
+    strides[i] = s;
+    s *= in_shape[i];
+  }
+  for (int i = 0; i < r; ++i) {
+    p.out_dims[i] = in_shape[perm[i]];
+    p.src_stride[i] = strides[perm[i]];
+  }
+  permute_kernel<T><<<num_blocks(p.total, 256), 256, 0, st>>>(in, out, p);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void normalize_max_abs(T* x, int64_t n, unsigned long long* scratch, cudaStream_t st) {
+  TG_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), st));
+  const int nb = num_blocks(n, 256, 148 * 4);
+  maxabs_kernel<T><<<nb, 256, 0, st>>>(x, n, scratch);
+  TG_CHECK_LAUNCH();
+  divide_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(x, n, scratch);
+  TG_CHECK_LAUNCH();
+  count_launch(2);
+}
+
+template <typename T>
+void fit_chi(const T* in, int64_t d1, int64_t d2, int64_t rest, T* out, int64_t chi,
+             cudaStream_t st) {
+  fit_chi_kernel<T><<<num_blocks(chi * chi * rest, 256), 256, 0, st>>>(in, d1, d2, rest, out, chi);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+void truncation(const double* s, int64_t n, int chi_cap, double cutoff, double* sinv, int chi_out,
+                int* cut_out, cudaStream_t st) {
+  truncation_kernel<<<1, 32, 0, st>>>(s, n, chi_cap, cutoff, sinv, chi_out, cut_out);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void scale_cols(const T* U, int64_t ldu, int64_t rows, int kc, const double* sinv, bool conj,
+                T* out, cudaStream_t st) {
+  scale_cols_kernel<T><<<num_blocks(rows * kc, 256), 256, 0, st>>>(U, ldu, rows, kc, sinv, conj, out);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void scale_rows(const T* VT, int64_t ldv, int64_t cols, int kc, const double* sinv, bool conj,
+                T* out, cudaStream_t st) {
+  scale_rows_kernel<T><<<num_blocks(cols * kc, 256), 256, 0, st>>>(VT, ldv, cols, kc, sinv, conj, out);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void identity(T* out, int64_t e, cudaStream_t st) {
+  identity_kernel<T><<<num_blocks(e * e, 256), 256, 0, st>>>(out, e);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void batched_spectrum(const T* const* mats, int count, int n, double* out, int* sweeps_used,
+                      cudaStream_t st) {
+  if (count <= 0) return;
+  if (n > 128 || n < 1) fail(TG_E_INPUT, "batched_spectrum: 1 <= n <= 128 required");
+  constexpr bool CPLX = is_cplx<T>::value;
+  const size_t smem = sizeof(double) * ((CPLX ? 2 : 1) * n * n + n);
+  static bool attr_set = false;
+  if (!attr_set) {
+    TG_CUDA(cudaFuncSetAttribute(jacobi_spectrum_kernel<T, CPLX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(double) * (2 * 128 * 128 + 128))));
+    attr_set = true;
+  }
+  jacobi_spectrum_kernel<T, CPLX><<<count, 256, smem, st>>>(mats, n, out, sweeps_used);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+void spectrum_distance(const double* a, const double* c, int count, int n, double* sig,
+                       cudaStream_t st) {
+  if (count <= 0) return;
+  spectrum_distance_kernel<<<count, 32, 0, st>>>(a, c, count, n, sig);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void scale(T* x, int64_t n, double alpha, cudaStream_t st) {
+  scale_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(x, n, alpha);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void scale_leg(T* x, int64_t outer, int64_t dim, int64_t inner, const double* v, cudaStream_t st) {
+  scale_leg_kernel<T><<<num_blocks(outer * dim * inner, 256), 256, 0, st>>>(x, outer, dim, inner, v);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+#define TG_INST(T)                                                                               \
+  template void gemm<T>(const T*, const T*, T*, const GemmDesc&, cudaStream_t);                  \
+  template void permute<T>(const T*, T*, const Shape&, const std::vector<int>&, bool,            \
+                           cudaStream_t);                                                        \
+  template void normalize_max_abs<T>(T*, int64_t, unsigned long long*, cudaStream_t);            \
+  template void fit_chi<T>(const T*, int64_t, int64_t, int64_t, T*, int64_t, cudaStream_t);      \
+  template void scale_cols<T>(const T*, int64_t, int64_t, int, const double*, bool, T*,          \
+                              cudaStream_t);                                                     \
+  template void scale_rows<T>(const T*, int64_t, int64_t, int, const double*, bool, T*,          \
+                              cudaStream_t);                                                     \
+  template void identity<T>(T*, int64_t, cudaStream_t);                                          \
+  template void batched_spectrum<T>(const T* const*, int, int, double*, int*, cudaStream_t);     \
+  template void scale<T>(T*, int64_t, double, cudaStream_t);                                     \
+  template void scale_leg<T>(T*, int64_t, int64_t, int64_t, const double*, cudaStream_t);
+
+TG_INST(double)
+TG_INST(cplx)
+
+}  // namespace tg

@@ -1,0 +1,77 @@
+// Launchers of the hand-written sm_100a kernels used by the CTMRG driver.
+#pragma once
+
+#include "common.hpp"
+
+namespace tg {
+
+// Strided batched matrix product C[b] (+)= op(A[b]) * op(B[b]) on the FP64
+// tensor cores (DMMA m8n8k4).  Element (m,k) of A is A[m*sAm + k*sAk]; one of
+// sAm / sAk must be 1 for coalesced tile loads, the other stride is free.
+struct GemmDesc {
+  int64_t M, N, K, batch;
+  int64_t sAm, sAk, sBk, sBn, sCm, sCn;
+  int64_t bA, bB, bC;
+  bool conjA, conjB, accumulate;
+};
+
+template <typename T>
+void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st);
+
+// out[i0..i_{r-1}] = in[...] with out.shape[i] = in.shape[perm[i]] (row-major),
+// optionally conjugated.
+template <typename T>
+void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>& perm, bool conj,
+             cudaStream_t st);
+
+// x /= max_i |x_i|  (the max_abs normalisation of ctm.cpp:514-517, 550-551).
+// `scratch` holds one uint64 on the device.
+template <typename T>
+void normalize_max_abs(T* x, int64_t n, unsigned long long* scratch, cudaStream_t st);
+
+// out(chi, chi, r...) = zero-padded / sliced in(d1, d2, r...)  (extend / slice
+// of the environment initialisation, ctm.cpp:998-1012).
+template <typename T>
+void fit_chi(const T* in, int64_t d1, int64_t d2, int64_t rest, T* out, int64_t chi,
+             cudaStream_t st);
+
+// Projector truncation (ctm.cpp:245-256, 275-288): given descending singular
+// values s[0..n), keep cut = min(n, chi_cap) values, stopping at the first
+// s_i / s_0 <= cutoff; sinv[k] = 1/sqrt(s_k) for k < cut, 0 for cut <= k < chi_out.
+// cut is written to *cut_out (device int).
+void truncation(const double* s, int64_t n, int chi_cap, double cutoff, double* sinv,
+                int chi_out, int* cut_out, cudaStream_t st);
+
+// U_c[i, k] = U[i*ldu + k] * sinv[k], k < kc (conj optional)  -> (rows x kc)
+template <typename T>
+void scale_cols(const T* U, int64_t ldu, int64_t rows, int kc, const double* sinv, bool conj,
+                T* out, cudaStream_t st);
+// VT_c[k, j] = VT[k*ldv + j] * sinv[k], k < kc  -> (kc x cols)
+template <typename T>
+void scale_rows(const T* VT, int64_t ldv, int64_t cols, int kc, const double* sinv, bool conj,
+                T* out, cudaStream_t st);
+
+// Identity projector reshaped to (e, 1, 1, e) (ctm.cpp:303-317).
+template <typename T>
+void identity(T* out, int64_t e, cudaStream_t st);
+
+// Batched L2-normalised singular values of `count` n x n matrices by one-sided
+// Jacobi (one CTA per matrix, matrix resident in shared memory).  Values are
+// written descending to out[b*n + i].  n <= 128.
+template <typename T>
+void batched_spectrum(const T* const* mats, int count, int n, double* out, int* sweeps_used,
+                      cudaStream_t st);
+
+// sig[b] = || a[b*n : (b+1)*n] - c[b*n : (b+1)*n] ||_2
+void spectrum_distance(const double* a, const double* c, int count, int n, double* sig,
+                       cudaStream_t st);
+
+// x *= alpha (scalar, real)
+template <typename T>
+void scale(T* x, int64_t n, double alpha, cudaStream_t st);
+
+// multiply leg `ax` of a tensor viewed as (outer, dim, inner) by v[dim]
+template <typename T>
+void scale_leg(T* x, int64_t outer, int64_t dim, int64_t inner, const double* v, cudaStream_t st);
+
+}  // namespace tg

@@ -1,0 +1,198 @@
+"""Python mirror of TeNeS's iTPS environment interface on top of the C ABI.
+
+``Environment`` owns one libtenes_gpu context (device-resident site tensors,
+simple-update weights and CTM environment) and exposes the reference's
+operations under the reference's names:
+
+=====================================  =============================================
+reference (src/iTPS/...)               here
+=====================================  =============================================
+core::Calc_CTM_Environment (ctm.cpp)   ``Environment.calc_ctm_environment``
+core::Left/Right/Top/Bottom_move        ``Environment.move``
+core::Check_Convergence_CTM             ``Environment.check_convergence``
+core::Simple_update_bond / tensordot    ``Environment.simple_update``
+Contract_one_site_iTPS_CTM              ``Environment.contract_one_site``
+Contract_two_sites_*_op12_iTPS_CTM      ``Environment.contract_bond_op12``
+=====================================  =============================================
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr
+
+
+@dataclass
+class CTMParams:
+    """[parameter.ctm] / [parameter.simple_update] knobs (PEPS_Parameters)."""
+    chi: int = 2
+    inverse_projector_cut: float = 1e-12
+    ctm_convergence_epsilon: float = 1e-6
+    max_ctm_iteration: int = 100
+    projector_corner: bool = True
+    use_rsvd: bool = False
+    rsvd_oversampling_factor: float = 2.0
+    rsvd_oversample_abs: int = -1
+    rsvd_power_iters: int = 2
+    rsvd_seed: int = 0
+    inverse_lambda_cut: float = 1e-12
+
+    def to_c(self) -> _lib.Params:
+        p = _lib.Params()
+        for f in self.__dataclass_fields__:
+            setattr(p, f, int(getattr(self, f)) if isinstance(getattr(self, f), bool) else getattr(self, f))
+        return p
+
+
+ENV_NAMES = ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")
+
+
+class Environment:
+    """Device-resident iTPS + CTM environment of one unit cell."""
+
+    def __init__(self, LX: int, LY: int, physical_dims: Sequence[int],
+                 virtual_dims: Sequence[Sequence[int]], params: CTMParams, is_complex: bool,
+                 skew: int = 0, device: int = 0):
+        self.lib = _lib.load()
+        self.LX, self.LY, self.skew = LX, LY, skew
+        self.N = LX * LY
+        self.pdim = [int(x) for x in physical_dims]
+        self.vdim = [[int(x) for x in v] for v in virtual_dims]
+        self.params = params
+        self.is_complex = bool(is_complex)
+        self.dtype = np.complex128 if is_complex else np.float64
+        pd = (C.c_int * self.N)(*self.pdim)
+        vd = (C.c_int * (4 * self.N))(*[x for v in self.vdim for x in v])
+        self._keep = (pd, vd)
+        desc = _lib.LatticeDesc(LX, LY, skew, pd, vd)
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        check(self.lib.tg_ctx_create(C.byref(desc), C.byref(self._cp), int(is_complex), device, C.byref(h)))
+        self.ctx = h
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.tg_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------- tensors
+    def site_shape(self, i: int) -> Tuple[int, ...]:
+        v = self.vdim[i]
+        return (v[0], v[1], v[2], v[3], self.pdim[i])
+
+    def env_shape(self, which: int, i: int) -> Tuple[int, ...]:
+        chi = self.params.chi
+        if which < 4:
+            return (chi, chi)
+        leg = {4: 1, 5: 2, 6: 3, 7: 0}[which]
+        d = self.vdim[i][leg]
+        return (chi, chi, d, d)
+
+    def set_site_tensor(self, i: int, T: np.ndarray) -> None:
+        a = _lib.as_host(T, self.is_complex)
+        if a.shape != self.site_shape(i):
+            raise ValueError(f"site {i}: shape {a.shape} != {self.site_shape(i)}")
+        check(self.lib.tg_set_site_tensor(self.ctx, i, dptr(a.view(np.float64))))
+
+    def get_site_tensor(self, i: int) -> np.ndarray:
+        a = np.empty(self.site_shape(i), dtype=self.dtype)
+        check(self.lib.tg_get_site_tensor(self.ctx, i, dptr(a.view(np.float64))))
+        return a
+
+    def set_lambda(self, i: int, leg: int, lam: np.ndarray) -> None:
+        a = np.ascontiguousarray(lam, dtype=np.float64)
+        if a.shape != (self.vdim[i][leg],):
+            raise ValueError("lambda length mismatch")
+        check(self.lib.tg_set_lambda(self.ctx, i, leg, dptr(a)))
+
+    def get_lambda(self, i: int, leg: int) -> np.ndarray:
+        a = np.empty(self.vdim[i][leg], dtype=np.float64)
+        check(self.lib.tg_get_lambda(self.ctx, i, leg, dptr(a)))
+        return a
+
+    def set_env(self, which: int, i: int, T: np.ndarray) -> None:
+        a = _lib.as_host(T, self.is_complex)
+        if a.shape != self.env_shape(which, i):
+            raise ValueError(f"{ENV_NAMES[which]}[{i}]: shape {a.shape} != {self.env_shape(which, i)}")
+        check(self.lib.tg_set_env(self.ctx, which, i, dptr(a.view(np.float64))))
+
+    def get_env(self, which: int, i: int) -> np.ndarray:
+        a = np.empty(self.env_shape(which, i), dtype=self.dtype)
+        check(self.lib.tg_get_env(self.ctx, which, i, dptr(a.view(np.float64))))
+        return a
+
+    # --------------------------------------------------------------- CTMRG
+    def init_env(self) -> None:
+        check(self.lib.tg_ctm_init(self.ctx))
+
+    def move(self, direction: int, line: int) -> None:
+        """0 = Left_move, 1 = Right_move, 2 = Top_move, 3 = Bottom_move."""
+        check(self.lib.tg_ctm_move(self.ctx, direction, line))
+
+    def sweep(self) -> None:
+        check(self.lib.tg_ctm_sweep(self.ctx))
+
+    def check_convergence(self) -> Tuple[bool, float]:
+        conv = C.c_int()
+        sig = C.c_double()
+        check(self.lib.tg_ctm_check_convergence(self.ctx, C.byref(conv), C.byref(sig)))
+        return bool(conv.value), sig.value
+
+    def calc_ctm_environment(self, initialize: bool = True) -> Tuple[int, bool, float]:
+        it = C.c_int()
+        conv = C.c_int()
+        sig = C.c_double()
+        check(self.lib.tg_ctm_run(self.ctx, int(initialize), C.byref(it), C.byref(conv), C.byref(sig)))
+        return it.value, bool(conv.value), sig.value
+
+    def corner_spectrum(self, which: int, i: int) -> np.ndarray:
+        a = np.empty(self.params.chi, dtype=np.float64)
+        check(self.lib.tg_corner_spectrum(self.ctx, which, i, dptr(a)))
+        return a
+
+    # --------------------------------------------------------- observables
+    def contract_one_site(self, i: int, op: np.ndarray) -> complex:
+        o = np.ascontiguousarray(op, dtype=self.dtype)
+        out = np.zeros(2)
+        check(self.lib.tg_measure_onesite(self.ctx, i, dptr(o.view(np.float64)), dptr(out)))
+        return complex(out[0], out[1])
+
+    def contract_bond_op12(self, source: int, dx: int, dy: int, op12: np.ndarray) -> complex:
+        o = np.ascontiguousarray(op12, dtype=self.dtype)
+        out = np.zeros(2)
+        check(self.lib.tg_measure_bond_op12(self.ctx, source, dx, dy, dptr(o.view(np.float64)), dptr(out)))
+        return complex(out[0], out[1])
+
+    # ------------------------------------------------------- simple update
+    def simple_update(self, source: int, source_leg: int, op: np.ndarray) -> None:
+        """iTPS::simple_update(EvolutionOperator) (src/iTPS/simple_update.cpp:25-46)."""
+        o = _lib.as_host(op, self.is_complex)
+        if source_leg < 0:
+            check(self.lib.tg_su_onesite(self.ctx, source, dptr(o.view(np.float64))))
+        else:
+            check(self.lib.tg_su_bond(self.ctx, source, source_leg, dptr(o.view(np.float64))))
+
+    def sync(self) -> None:
+        check(self.lib.tg_sync(self.ctx))
+
+
+def kernel_launch_count() -> int:
+    return int(_lib.load().tg_kernel_launch_count())

@@ -1,0 +1,115 @@
+"""CTMRG parity: the CUDA path against the FP64 oracle on the same seeded
+tensors.  Gauge-invariant quantities are compared (|entries| after one move,
+corner spectra, observables); the tolerance is 1e-10 relative."""
+import numpy as np
+import pytest
+
+from oracle import tenes_oracle as O
+from tests._helpers import (SX, SZ, gpu_env, load_env, make_lattice, oracle_params,
+                            random_tensors, rel)
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_init_env_matches_oracle(is_complex):
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 1, is_complex)
+    chi = 6
+    oe = O.init_env(Tn, oracle_params(chi), lat)
+    ge = gpu_env(lat, Tn, chi, is_complex)
+    ge.init_env()
+    for w, name in enumerate(("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(ge.get_env(w, i), getattr(oe, name)[i], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("direction", [0, 1, 2, 3])
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_single_move_matches_oracle(direction, is_complex):
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 7, is_complex)
+    chi = 8
+    p = oracle_params(chi)
+    oe = O.init_env(Tn, p, lat)
+    O.sweep(oe, Tn, p, lat)  # a non-trivial environment
+    ge = gpu_env(lat, Tn, chi, is_complex)
+    load_env(ge, oe)
+    move = (O.left_move, O.right_move, O.top_move, O.bottom_move)[direction]
+    move(oe, Tn, 0, p, lat)
+    ge.move(direction, 0)
+    # sign / phase gauge of the SVD leaves |entries| unchanged
+    for w, name in enumerate(("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")):
+        for i in range(lat.N_UNIT):
+            g = np.abs(ge.get_env(w, i))
+            o = np.abs(getattr(oe, name)[i])
+            np.testing.assert_allclose(g, o, rtol=1e-9, atol=1e-11, err_msg=f"{name}[{i}]")
+
+
+def _observables_oracle(oe, Tn, lat):
+    out = []
+    for i in range(lat.N_UNIT):
+        nrm = O.contract_one_site(oe.C1[i], oe.C2[i], oe.C3[i], oe.C4[i], oe.eTt[i], oe.eTr[i],
+                                  oe.eTb[i], oe.eTl[i], Tn[i], np.eye(2))
+        for op in (SZ, SX):
+            v = O.contract_one_site(oe.C1[i], oe.C2[i], oe.C3[i], oe.C4[i], oe.eTt[i], oe.eTr[i],
+                                    oe.eTb[i], oe.eTl[i], Tn[i], op)
+            out.append((v / nrm).real)
+    return out
+
+
+def _observables_gpu(ge, lat):
+    out = []
+    for i in range(lat.N_UNIT):
+        nrm = ge.contract_one_site(i, np.eye(2))
+        for op in (SZ, SX):
+            out.append((ge.contract_one_site(i, op) / nrm).real)
+    return out
+
+
+@pytest.mark.parametrize("D,chi,iters,corner", [(2, 10, 10, True), (3, 12, 6, True), (2, 8, 5, False)])
+def test_ctm_run_matches_oracle(D, chi, iters, corner):
+    lat = make_lattice(2, 2, D)
+    Tn = random_tensors(lat, 11 + D, False)
+    p = oracle_params(chi, Max_CTM_Iteration=iters, CTM_Projector_corner=corner)
+    oe, ocnt, oconv, osig = O.calc_ctm_environment(Tn, p, lat)
+    ge = gpu_env(lat, Tn, chi, False, max_ctm_iteration=iters, projector_corner=corner)
+    gcnt, gconv, gsig = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt and gconv == oconv
+    assert rel(gsig, osig) < 1e-6 or abs(gsig - osig) < 1e-12
+    for w, name in enumerate(("C1", "C2", "C3", "C4")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i]),
+                                       rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
+    # nearest-neighbour <SzSz> through the op12 contractions
+    op12 = np.einsum("ac,bd->abcd", SZ, SZ)
+    for i in range(lat.N_UNIT):
+        for dx, dy in ((1, 0), (0, 1)):
+            g = ge.contract_bond_op12(i, dx, dy, op12) / ge.contract_bond_op12(i, dx, dy, np.einsum(
+                "ac,bd->abcd", np.eye(2), np.eye(2)))
+            if dy == 0:
+                j = lat.right(i)
+                args = (oe.C1[i], oe.C2[j], oe.C3[j], oe.C4[i], oe.eTt[i], oe.eTt[j], oe.eTr[j],
+                        oe.eTb[j], oe.eTb[i], oe.eTl[i], Tn[i], Tn[j])
+                f = O.contract_two_sites_horizontal_op12
+            else:
+                j = lat.top(i)
+                args = (oe.C1[j], oe.C2[j], oe.C3[i], oe.C4[i], oe.eTt[j], oe.eTr[j], oe.eTr[i],
+                        oe.eTb[i], oe.eTl[i], oe.eTl[j], Tn[j], Tn[i])
+                f = O.contract_two_sites_vertical_op12
+            o = f(*args, op12) / f(*args, np.einsum("ac,bd->abcd", np.eye(2), np.eye(2)))
+            assert rel(g.real, o.real) < TOL or abs(g.real - o.real) < 1e-12
+
+
+def test_complex_ctm_run_matches_oracle():
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 5, True)
+    chi = 8
+    p = oracle_params(chi, Max_CTM_Iteration=4)
+    oe, ocnt, _, _ = O.calc_ctm_environment(Tn, p, lat)
+    ge = gpu_env(lat, Tn, chi, True, max_ctm_iteration=4)
+    gcnt, _, _ = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt
+    np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
