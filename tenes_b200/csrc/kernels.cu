@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <string>
 
 #include "kernels.cuh"
 
@@ -610,15 +611,17 @@ template <typename T>
 void batched_spectrum(const T* const* mats, int count, int n, double* out, int* sweeps_used,
                       cudaStream_t st) {
   if (count <= 0) return;
-  if (n > 128 || n < 1) fail(TG_E_INPUT, "batched_spectrum: 1 <= n <= 128 required");
   constexpr bool CPLX = is_cplx<T>::value;
+  // the matrix lives in shared memory: n <= 160 (real), 112 (complex)
+  const int nmax = CPLX ? 112 : 160;
+  if (n > nmax || n < 1)
+    fail(TG_E_INPUT, "batched_spectrum: 1 <= chi <= " + std::to_string(nmax) + " required");
   const size_t smem = sizeof(double) * ((CPLX ? 2 : 1) * n * n + n);
-  static bool attr_set = false;
-  if (!attr_set) {
+  static size_t attr_bytes = 0;
+  if (smem > attr_bytes) {
     TG_CUDA(cudaFuncSetAttribute(jacobi_spectrum_kernel<T, CPLX>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sizeof(double) * (2 * 128 * 128 + 128))));
-    attr_set = true;
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr_bytes = smem;
   }
   jacobi_spectrum_kernel<T, CPLX><<<count, 256, smem, st>>>(mats, n, out, sweeps_used);
   TG_CHECK_LAUNCH();

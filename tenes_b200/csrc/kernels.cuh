@@ -57,7 +57,7 @@ void identity(T* out, int64_t e, cudaStream_t st);
 
 // Batched L2-normalised singular values of `count` n x n matrices by one-sided
 // Jacobi (one CTA per matrix, matrix resident in shared memory).  Values are
-// written descending to out[b*n + i].  n <= 128.
+// written descending to out[b*n + i].  n <= 160 (real), 112 (complex).
 template <typename T>
 void batched_spectrum(const T* const* mats, int count, int n, double* out, int* sweeps_used,
                       cudaStream_t st);

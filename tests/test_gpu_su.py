@@ -72,24 +72,23 @@ def test_te_tfi_golden_on_gpu():
     exp = expected()
     Tn = O.initialize_tensors(lat, inp.params.seed, inp.is_real)
     env = gpu_env(lat, Tn, inp.params.CHI, not inp.is_real, max_ctm_iteration=inp.params.Max_CTM_Iteration)
-    names1 = {o.group: o.name for o in one}
     sz = [o for o in one if o.name == "Sz"]
 
     def measure(t):
         env.calc_ctm_environment(True)
         for o in sz:
-            nrm = env.contract_one_site(o.source_site, np.eye(2))
-            v = (env.contract_one_site(o.source_site, o.op) / nrm).real
+            nrm = env.contract_one_site(o.site, np.eye(2))
+            v = (env.contract_one_site(o.site, o.op) / nrm).real
             ref = [r for r in exp["onesite"] if abs(r[0] - t) < 1e-9 and int(r[1]) == o.group
-                   and int(r[2]) == o.source_site][0]
+                   and int(r[2]) == o.site][0]
             assert abs(v - ref[3]) < 1e-10 * max(1, abs(ref[3]))
         E = 0.0
         for o in two:
             if o.name != "bond_hamiltonian":
                 continue
             ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
-            E += (env.contract_bond_op12(o.source_site, o.dx[0], o.dy[0], o.op)
-                  / env.contract_bond_op12(o.source_site, o.dx[0], o.dy[0], ident)).real
+            E += (env.contract_bond_op12(o.source, o.dx, o.dy, o.op)
+                  / env.contract_bond_op12(o.source, o.dx, o.dy, ident)).real
         E /= lat.N_UNIT
         ref = [r for r in exp["density"] if abs(r[0] - t) < 1e-9 and int(r[1]) == 0][0]
         assert abs(E - ref[2]) < 1e-10
