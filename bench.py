@@ -1,0 +1,381 @@
+"""CTMRG throughput on B200: sweeps/s of the iTPS corner-transfer-matrix
+environment (one sweep = Left, Right, Top, Bottom moves of
+core::Calc_CTM_Environment, src/iTPS/core/ctm.cpp:1203-1243).
+
+Workload (default): spin-1/2 antiferromagnetic Heisenberg model, 2x2 unit
+cell, D=6, chi=72, FP64, site tensors from 300 seeded simple-update steps at
+tau=0.01 run through the library itself, Neel initial state + noise 1e-2
+(seed 11).  Data are synthetic; the reference publishes no benchmark suite.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs N independent replicas (one per GPU, different seeds; the CTMRG of
+one unit cell does not shard) and reports the summed sweeps/s.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = {
+    # name: (D, chi, su_steps, description)
+    "c3": (6, 72, 300, "afh_square_2x2_D6_chi72_fp64"),
+    "c2": (4, 32, 200, "afh_square_2x2_D4_chi32_fp64"),
+    "c1": (2, 10, 100, "afh_square_2x2_D2_chi10_fp64"),
+}
+TAU = 0.01
+SEED = 11
+L2_BYTES = 126 * 1024 * 1024
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ workload
+def lattice_spec(D):
+    LX = LY = 2
+    N = LX * LY
+    pd = [2] * N
+    vd = [[D] * 4 for _ in range(N)]
+    # Neel pattern: sublattice A up, B down (parity of x + y)
+    dirs = [[1.0, 0.0] if ((i % LX) + (i // LX)) % 2 == 0 else [0.0, 1.0] for i in range(N)]
+    noises = [1e-2] * N
+    return LX, LY, pd, vd, dirs, noises
+
+
+def bonds(LX, LY):
+    N = LX * LY
+    return [(s, 2) for s in range(N)] + [(s, 1) for s in range(N)]
+
+
+def heisenberg_op():
+    from tenes_b200.std_ops import evolution_twosite, heisenberg_bond, real_if_close
+    return real_if_close(evolution_twosite(heisenberg_bond(1.0), TAU))
+
+
+# ------------------------------------------------------------------ our arm
+def make_env(cfg, seed, device):
+    from tenes_b200.env import CTMParams, Environment
+    D, chi, su_steps, _ = CONFIGS[cfg]
+    LX, LY, pd, vd, dirs, noises = lattice_spec(D)
+    env = Environment(LX, LY, pd, vd, CTMParams(chi=chi, max_ctm_iteration=1), False, device=device)
+    env.init_tensors(seed, dirs, noises)
+    op = heisenberg_op()
+    t0 = time.perf_counter()
+    for _ in range(su_steps):
+        for (s, leg) in bonds(LX, LY):
+            env.simple_update(s, leg, op)
+    log(f"[bench] {su_steps} simple-update steps in {time.perf_counter() - t0:.1f}s")
+    env.init_env()
+    return env
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_peak_tflops(device):
+    """Measured FP64 dense GEMM peak of this GPU (cuBLAS DGEMM 8192^3)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize(device)
+    best = 1e30
+    for _ in range(3):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize(device)
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def traffic_from_profile(cfg):
+    """DRAM bytes per DMMA-GEMM launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"gemm_dmma_{cfg}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch\s*=\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from tenes_b200.env import (PROFILE_KINDS, kernel_launch_count, profile_enable, profile_query,
+                                profile_reset)
+    device = local_rank
+    torch.cuda.set_device(device)
+    env = make_env(args.config, SEED + rank, device)
+    stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
+
+    for _ in range(args.warmup):
+        env.sweep()
+    if args.profile_sweep:
+        # one sweep inside cudaProfilerStart/Stop for `ncu --profile-from-start off`
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.start()
+        env.sweep()
+        env.sync()
+        torch.cuda.profiler.stop()
+    times = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    clocks = Clocks(device)
+    clocks.start()
+    l0 = kernel_launch_count()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # L2 flush outside the timed window
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        env.sweep()
+        e.record(stream)
+        e.synchronize()
+        times.append(s.elapsed_time(e))
+    launches = kernel_launch_count() - l0
+    torch.cuda.synchronize(device)
+    ck = clocks.stop()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers (set Tn + env, sweep, get env)
+    host_T = [env.get_site_tensor(i) for i in range(env.N)]
+    host_env = [[env.get_env(w, i) for i in range(env.N)] for w in range(8)]
+    h2d = sum(t.nbytes for t in host_T) + sum(t.nbytes for ws in host_env for t in ws)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for i, T in enumerate(host_T):
+            env.set_site_tensor(i, T)
+        for w in range(8):
+            for i in range(env.N):
+                env.set_env(w, i, host_env[w][i])
+        env.sweep()
+        host_env = [[env.get_env(w, i) for i in range(env.N)] for w in range(8)]
+        e.record(stream)
+        e.synchronize()
+        e2e_ms += s.elapsed_time(e)
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "sweeps/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(t.nbytes for ws in host_env for t in ws)}
+
+    # ---- per-family device time of one instrumented sweep (roofline)
+    profile_enable(True)
+    profile_reset()
+    env.sweep()
+    env.sync()
+    fam = {PROFILE_KINDS[k]: profile_query(k) for k in range(len(PROFILE_KINDS))}
+    profile_enable(False)
+    n_g, ms_g, fl_g, _ = fam["gemm_dmma"]
+    peak = fp64_peak_tflops(device) if rank == 0 else None
+    achieved = fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0
+    traffic = traffic_from_profile(args.config)
+    roofline = {"bound": "tensor", "kernel": "gemm_kernel (FP64 DMMA m8n8k4)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None,
+                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (no FP64 entry in MEASURED_PEAKS.json)",
+                "traffic": traffic, "launches_per_sweep": n_g, "avg_launch_us": 1e3 * ms_g / max(n_g, 1),
+                "flops_per_launch": fl_g / max(n_g, 1),
+                "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}}
+    env.close()
+    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roofline,
+            "clocks": ck, "gpu_launches": launches}
+
+
+# -------------------------------------------------------- CPU oracle (reference arm)
+def oracle_sample(cfg, rank=0):
+    """Time one Left_move of the CPU oracle on the same workload; one sweep is
+    4*LX... = 8 moves of this size for a 2x2 cell."""
+    from oracle import tenes_oracle as O
+    D, chi, su_steps, _ = CONFIGS[cfg]
+    LX, LY, pd, vd, dirs, noises = lattice_spec(D)
+    lat = O.Lattice(LX, LY)
+    lat.physical_dims = pd
+    lat.virtual_dims = vd
+    lat.initial_dirs = dirs
+    lat.noises = noises
+    Tn = O.initialize_tensors(lat, SEED + rank, True)
+    lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
+    p = O.Params(CHI=chi)
+    op = heisenberg_op()
+    for _ in range(su_steps):
+        for (s, leg) in bonds(LX, LY):
+            tg = lat.neighbor(s, leg)
+            a, b, lc = O.simple_update_bond(Tn[s], Tn[tg], lam[s], lam[tg], op, leg, p)
+            lam[s][leg] = lc
+            lam[tg][(leg + 2) % 4] = lc
+            Tn[s], Tn[tg] = a, b
+    env = O.init_env(Tn, p, lat)
+    return lat, Tn, p, env
+
+
+def time_oracle_move(lat, Tn, p, env):
+    from oracle import tenes_oracle as O
+    t0 = time.perf_counter()
+    O.left_move(env, Tn, 0, p, lat)
+    return time.perf_counter() - t0
+
+
+def moves_per_sweep(lat):
+    return 2 * lat.LX_noskew + 2 * lat.LY_noskew
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    lat, Tn, p, env = oracle_sample(args.config)
+    for _ in range(args.warmup):
+        time_oracle_move(lat, Tn, p, env)
+    tot = 0.0
+    for _ in range(args.steps):
+        tot += time_oracle_move(lat, Tn, p, env)
+    per_sweep = tot / args.steps * moves_per_sweep(lat)
+    v = 1.0 / per_sweep
+    cores = os.cpu_count()
+    D, chi, _, name = CONFIGS[args.config]
+    return {"metric": "ctmrg_sweeps_per_s", "value": v, "unit": "sweeps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_sweep * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": name, "D": D, "chi": chi, "unit_cell": "2x2", "projector": "full SVD"},
+            "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": cores, "kind": "port",
+                             "sample": "one Left_move (2 projector rows, full SVD) of the CPU oracle per step, "
+                                       f"x{moves_per_sweep(lat)} moves per sweep"},
+            "e2e": {"value": v, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-sweep", action="store_true",
+                    help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    res = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        D, chi, su, name = CONFIGS[args.config]
+        cpu = None
+        if not args.no_cpu_baseline:
+            lat, Tn, p, env = oracle_sample(args.config)
+            t = time_oracle_move(lat, Tn, p, env)
+            v = 1.0 / (t * moves_per_sweep(lat))
+            cpu = {"value": v, "unit": "sweeps/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"one Left_move of the CPU oracle (numpy FP64, full SVD), x{moves_per_sweep(lat)} "
+                             "moves per sweep"}
+        line = {"metric": "ctmrg_sweeps_per_s", "value": res["value"], "unit": "sweeps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": name, "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
+                           "projector": "full SVD (reference default)", "parallelism": f"replicas{world}",
+                           "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},
+                "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
+                "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

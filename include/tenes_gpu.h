@@ -139,11 +139,34 @@ tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const do
 tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op);
 tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op);
 
+/* iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137): per site,
+ * Tn[0,0,0,0,:] = initial state (random when all entries are zero) and every
+ * other entry noise * U(-1,1) from std::mt19937(seed) (real part) and
+ * std::mt19937(seed*11+137) (imaginary part), drawn first-leg-fastest.
+ * initial_dirs concatenates the per-site initial states (dir_len[i] values
+ * each); noises has one value per site.  Resets the lambdas to one. */
+tg_status tg_init_tensors(tg_ctx* ctx, int seed, const double* initial_dirs, const int* dir_len,
+                          const double* noises);
+
 /* Synchronise the context's stream; report asynchronous CUDA errors. */
 tg_status tg_sync(tg_ctx* ctx);
 
 /* Count of kernels this library has launched in the calling process. */
 uint64_t tg_kernel_launch_count(void);
+
+/* The CUDA stream (cudaStream_t) all work of the context is issued on, so a
+ * caller can order its own work or timing events against it. */
+tg_status tg_ctx_stream(tg_ctx* ctx, void** stream);
+
+/* Per-launch CUDA-event profiling of the library's kernel families
+ * (0 = DMMA matrix product, 1 = leg permutation, 2 = max-abs normalisation,
+ * 3 = Jacobi corner spectra, 4 = cuSOLVER factorisations, 5 = other).
+ * Adds two events per launch; off by default.  query returns the number of
+ * launches, their summed device time in ms and the algorithmic flops and
+ * bytes they were issued for since the last reset. */
+tg_status tg_profile_enable(int on);
+tg_status tg_profile_reset(void);
+tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes);
 
 #ifdef __cplusplus
 }

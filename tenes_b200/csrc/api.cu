@@ -177,9 +177,34 @@ tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op) 
     E(ctx)->su_bond(source, source_leg, op);
   });
 }
+tg_status tg_init_tensors(tg_ctx* ctx, int seed, const double* initial_dirs, const int* dir_len,
+                          const double* noises) {
+  return guard([&] {
+    need(initial_dirs, "initial_dirs");
+    need(dir_len, "dir_len");
+    need(noises, "noises");
+    E(ctx)->init_tensors(seed, initial_dirs, dir_len, noises);
+  });
+}
 tg_status tg_sync(tg_ctx* ctx) {
   return guard([&] { E(ctx)->sync(); });
 }
 uint64_t tg_kernel_launch_count(void) { return tg::launch_count(); }
+
+tg_status tg_ctx_stream(tg_ctx* ctx, void** stream) {
+  return guard([&] {
+    need(stream, "stream");
+    *stream = E(ctx)->stream();
+  });
+}
+tg_status tg_profile_enable(int on) {
+  return guard([&] { tg::profile_enable(on != 0); });
+}
+tg_status tg_profile_reset(void) {
+  return guard([&] { tg::profile_reset(); });
+}
+tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes) {
+  return guard([&] { tg::profile_query(kind, launches, ms, flops, bytes); });
+}
 
 }  // extern "C"

@@ -46,6 +46,33 @@ inline void check_cuda(cudaError_t e, const char* what, const char* file, int li
 void count_launch(uint64_t n = 1);
 uint64_t launch_count();
 
+// Optional per-launch CUDA-event profiling, grouped by kernel family.  When
+// enabled, every launch of the family is bracketed by two events on its
+// stream; the totals (launches, device ms, algorithmic flops / bytes) are
+// read back by tg_profile_query.
+enum ProfKind {
+  PK_GEMM = 0,       // DMMA strided batched matrix product
+  PK_PERMUTE = 1,    // leg permutation
+  PK_NORMALIZE = 2,  // max-abs normalisation
+  PK_SPECTRUM = 3,   // batched Jacobi corner spectra
+  PK_SOLVER = 4,     // cuSOLVER factorisations (SVD, QR)
+  PK_OTHER = 5,      // small helpers
+  PK_COUNT = 6
+};
+void profile_enable(bool on);
+bool profile_enabled();
+void profile_reset();
+void profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes);
+
+struct ProfScope {
+  int kind;
+  cudaStream_t st;
+  double flops, bytes;
+  cudaEvent_t e0 = nullptr;
+  ProfScope(int k, cudaStream_t s, double f, double b);
+  ~ProfScope();
+};
+
 using Shape = std::vector<int64_t>;
 
 inline int64_t numel(const Shape& s) {

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -189,6 +190,7 @@ struct EngineT final : Engine {
     const int64_t k = m;  // m <= n
     // column-major view: B = A^T is n x m (rows >= cols)
     const int rows = static_cast<int>(n), cols = static_cast<int>(m);
+    ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 22.0 * static_cast<double>(m) * m * n, 0.0);
     s = DT<double>({k}, st);
     DT<T> Ub({k, n}, st);   // U_B: n x k column-major  == VT_A row-major (k x n)
     DT<T> VTb({k, k}, st);  // VT_B: k x k column-major == U_A row-major (m x k)
@@ -231,6 +233,7 @@ struct EngineT final : Engine {
   void qr(const DT<T>& A, int64_t m, int64_t n, DT<T>& Q, DT<T>& R) {
     const int64_t k = std::min(m, n);
     DT<T> Ac = tr(reshape(A, {m, n}), {1, 0});  // row-major (n, m) == column-major (m, n)
+    ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 4.0 * static_cast<double>(m) * n * k, 0.0);
     DT<T> tau({std::max<int64_t>(k, 1)}, st);
     int lwork = 0, lwork2 = 0;
     const int im = static_cast<int>(m), in = static_cast<int>(n), ik = static_cast<int>(k);
@@ -823,6 +826,64 @@ struct EngineT final : Engine {
     TG_CUDA(cudaStreamSynchronize(st));
   }
 
+  // iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137): Tn[0,0,0,0,p] =
+  // initial_state[p] (random when all zero), every other entry noise*U(-1,1)
+  // drawn in first-leg-fastest order from mt19937(seed) (real part) and
+  // mt19937(seed*11+137) (imaginary part); lambdas reset to one.
+  void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) override {
+    std::mt19937 gen(static_cast<unsigned>(seed));
+    std::mt19937 gen_im(static_cast<unsigned>(seed * 11 + 137));
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    int off = 0;
+    for (int i = 0; i < lat.N; ++i) {
+      const auto& v = lat.vdim[i];
+      const int pd = lat.pdim[i];
+      const size_t ndim = static_cast<size_t>(v[0]) * v[1] * v[2] * v[3] * pd;
+      std::vector<double> re(ndim), im(ndim);
+      for (size_t j = 0; j < ndim; ++j) {
+        re[j] = dist(gen);
+        im[j] = dist(gen_im);
+      }
+      std::vector<double> d(dirs + off, dirs + off + dir_len[i]);
+      off += dir_len[i];
+      std::vector<double> d_im(pd, 0.0);
+      if (std::all_of(d.begin(), d.end(), [](double x) { return x == 0.0; })) {
+        d.assign(pd, 0.0);
+        for (int j = 0; j < pd; ++j) {
+          d[j] = dist(gen);
+          d_im[j] = dist(gen_im);
+        }
+      }
+      std::vector<T> h(ndim);
+      for (int a = 0; a < v[0]; ++a)
+        for (int b = 0; b < v[1]; ++b)
+          for (int c = 0; c < v[2]; ++c)
+            for (int e = 0; e < v[3]; ++e)
+              for (int p = 0; p < pd; ++p) {
+                const size_t rm = ((((static_cast<size_t>(a) * v[1] + b) * v[2] + c) * v[3] + e) * pd + p);
+                double xr, xi;
+                if (a == 0 && b == 0 && c == 0 && e == 0) {
+                  xr = p < static_cast<int>(d.size()) ? d[p] : 0.0;
+                  xi = d_im[p];
+                } else {
+                  const size_t nr = a + static_cast<size_t>(b) * v[0] + static_cast<size_t>(c) * v[0] * v[1] +
+                                    static_cast<size_t>(e) * v[0] * v[1] * v[2] +
+                                    static_cast<size_t>(p) * v[0] * v[1] * v[2] * v[3];
+                  xr = noises[i] * re[nr];
+                  xi = noises[i] * im[nr];
+                }
+                if constexpr (CPLX) {
+                  h[rm] = make_double2(xr, xi);
+                } else {
+                  h[rm] = xr;
+                }
+              }
+      upload(Tn[i], reinterpret_cast<const double*>(h.data()));
+      rot_ok[i] = false;
+      for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+    }
+  }
+
   // ------------------------------------------------------------- host I/O
   void set_site_tensor(int site, const double* host) override {
     check_site(site);
@@ -860,6 +921,7 @@ struct EngineT final : Engine {
   }
   void get_env(int which, int site, double* host) override { download(env_ref(which, site), host); }
   void sync() override { TG_CUDA(cudaStreamSynchronize(st)); }
+  void* stream() override { return static_cast<void*>(st); }
 };
 
 Engine* make_engine(const tg_lattice_desc* lat, const tg_params* p, int is_complex, int device) {

@@ -31,7 +31,9 @@ struct Engine {
   virtual void measure_bond_op12(int source, int dx, int dy, const double* op, double* out) = 0;
   virtual void su_onesite(int site, const double* op) = 0;
   virtual void su_bond(int source, int leg, const double* op) = 0;
+  virtual void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) = 0;
   virtual void sync() = 0;
+  virtual void* stream() = 0;
 };
 
 Engine* make_engine(const tg_lattice_desc* lat, const tg_params* p, int is_complex, int device);

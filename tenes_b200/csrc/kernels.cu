@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <vector>
 #include <cmath>
 #include <string>
 
@@ -15,6 +17,75 @@ namespace tg {
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+struct ProfRec {
+  int kind;
+  cudaEvent_t a, b;
+  double flops, bytes;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+struct ProfTot {
+  uint64_t n = 0;
+  double ms = 0, flops = 0, bytes = 0;
+};
+ProfTot g_tot[PK_COUNT];
+
+void prof_drain() {
+  for (auto& r : g_prof) {
+    float ms = 0.f;
+    cudaEventSynchronize(r.b);
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    auto& t = g_tot[r.kind];
+    t.n += 1;
+    t.ms += ms;
+    t.flops += r.flops;
+    t.bytes += r.bytes;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_prof.clear();
+}
+}  // namespace
+
+void profile_enable(bool on) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  g_prof_on = on;
+}
+bool profile_enabled() { return g_prof_on; }
+void profile_reset() {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  prof_drain();
+  for (auto& t : g_tot) t = ProfTot{};
+}
+void profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  prof_drain();
+  if (kind < 0 || kind >= PK_COUNT) fail(TG_E_INPUT, "profile kind out of range");
+  const auto& t = g_tot[kind];
+  if (launches) *launches = t.n;
+  if (ms) *ms = t.ms;
+  if (flops) *flops = t.flops;
+  if (bytes) *bytes = t.bytes;
+}
+
+ProfScope::ProfScope(int k, cudaStream_t s, double f, double b) : kind(k), st(s), flops(f), bytes(b) {
+  if (g_prof_on) {
+    TG_CUDA(cudaEventCreate(&e0));
+    TG_CUDA(cudaEventRecord(e0, st));
+  }
+}
+ProfScope::~ProfScope() {
+  if (!e0) return;
+  cudaEvent_t e1;
+  if (cudaEventCreate(&e1) != cudaSuccess) return;
+  cudaEventRecord(e1, st);
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  g_prof.push_back(ProfRec{kind, e0, e1, flops, bytes});
+  if (g_prof.size() > 4096) prof_drain();
+}
 
 namespace {
 
@@ -528,6 +599,9 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
             static_cast<unsigned>(d.batch));
   if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
   GemmParams<T> p{A, B, C, d};
+  const double macs = static_cast<double>(d.M) * d.N * d.K * d.batch;
+  ProfScope ps(PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
+               sizeof(T) * static_cast<double>(d.batch) * (d.M * d.K + d.K * d.N + d.M * d.N));
   gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(p);
   TG_CHECK_LAUNCH();
   count_launch();
@@ -553,6 +627,7 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
     p.out_dims[i] = in_shape[perm[i]];
     p.src_stride[i] = strides[perm[i]];
   }
+  ProfScope ps(PK_PERMUTE, st, 0.0, 2.0 * sizeof(T) * static_cast<double>(p.total));
   permute_kernel<T><<<num_blocks(p.total, 256), 256, 0, st>>>(in, out, p);
   TG_CHECK_LAUNCH();
   count_launch();
@@ -560,6 +635,7 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
 
 template <typename T>
 void normalize_max_abs(T* x, int64_t n, unsigned long long* scratch, cudaStream_t st) {
+  ProfScope ps(PK_NORMALIZE, st, 0.0, 3.0 * sizeof(T) * static_cast<double>(n));
   TG_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), st));
   const int nb = num_blocks(n, 256, 148 * 4);
   maxabs_kernel<T><<<nb, 256, 0, st>>>(x, n, scratch);
@@ -623,6 +699,7 @@ void batched_spectrum(const T* const* mats, int count, int n, double* out, int* 
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     attr_bytes = smem;
   }
+  ProfScope ps(PK_SPECTRUM, st, 0.0, sizeof(T) * static_cast<double>(count) * n * n);
   jacobi_spectrum_kernel<T, CPLX><<<count, 256, smem, st>>>(mats, n, out, sweeps_used);
   TG_CHECK_LAUNCH();
   count_launch();

@@ -190,9 +190,43 @@ class Environment:
         else:
             check(self.lib.tg_su_bond(self.ctx, source, source_leg, dptr(o.view(np.float64))))
 
+    def init_tensors(self, seed: int, initial_dirs: Sequence[Sequence[float]],
+                     noises: Sequence[float]) -> None:
+        """iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137)."""
+        flat = np.ascontiguousarray([x for d in initial_dirs for x in d] or [0.0], dtype=np.float64)
+        lens = (C.c_int * self.N)(*[len(d) for d in initial_dirs])
+        nz = np.ascontiguousarray(noises, dtype=np.float64)
+        check(self.lib.tg_init_tensors(self.ctx, int(seed), dptr(flat), lens, dptr(nz)))
+
     def sync(self) -> None:
         check(self.lib.tg_sync(self.ctx))
 
 
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (for events / ordering)."""
+        h = C.c_void_p()
+        check(self.lib.tg_ctx_stream(self.ctx, C.byref(h)))
+        return int(h.value or 0)
+
+
 def kernel_launch_count() -> int:
     return int(_lib.load().tg_kernel_launch_count())
+
+
+PROFILE_KINDS = ("gemm_dmma", "permute", "normalize", "jacobi_spectrum", "cusolver", "other")
+
+
+def profile_enable(on: bool) -> None:
+    check(_lib.load().tg_profile_enable(int(on)))
+
+
+def profile_reset() -> None:
+    check(_lib.load().tg_profile_reset())
+
+
+def profile_query(kind: int):
+    """(launches, device_ms, flops, bytes) summed since the last reset."""
+    n = C.c_uint64()
+    ms, fl, by = C.c_double(), C.c_double(), C.c_double()
+    check(_lib.load().tg_profile_query(kind, C.byref(n), C.byref(ms), C.byref(fl), C.byref(by)))
+    return int(n.value), ms.value, fl.value, by.value
