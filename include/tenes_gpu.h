@@ -168,6 +168,30 @@ tg_status tg_profile_enable(int on);
 tg_status tg_profile_reset(void);
 tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes);
 
+/* Allocation-free corner spectra.  No counterpart in the reference: it exists
+ * for callers that must not allocate device memory where they need the
+ * spectra -- code that runs under a fixed device-memory budget, hosts that
+ * hand out every device byte through their own pool, or a convergence check
+ * slotted between other GPU work where a cudaMalloc could stall the device.
+ *
+ * Computes the same L2-normalised, descending singular values as
+ * tg_corner_spectrum for `count` n x n matrices that already live in device
+ * memory: device_mats is a HOST array of `count` DEVICE pointers (row-major
+ * float64, or interleaved complex128 when is_complex), device_out is a device
+ * buffer of count*n doubles.  Work is queued on `stream` (a cudaStream_t, NULL
+ * for the legacy default stream); the call returns once it is queued.
+ *
+ * It allocates nothing: the device-side copy of the pointer table goes into a
+ * fixed 8 KiB array inside the library (at most 1024 matrices; n <= 160 real,
+ * n <= 112 complex; larger requests fail with TG_E_INPUT).  Every GPU that
+ * loads the library keeps that array until the process exits.  The first call
+ * on each device looks up the array's device address (call it once before
+ * any stream capture).  All calls share the array and it keeps the last
+ * call's contents, so calls whose GPU work overlaps race on it: order them
+ * on one stream, or synchronise between them. */
+tg_status tg_corner_spectra_noalloc(const void* const* device_mats, int count, int n, int is_complex,
+                                    double* device_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,10 @@ void need(const void* p, const char* what) {
 
 }  // namespace
 
+namespace tg {
+void set_last_error(const std::string& m) { g_last_error = m; }
+}  // namespace tg
+
 extern "C" {
 
 void tg_params_default(tg_params* p) {

@@ -30,6 +30,9 @@ struct Error : std::runtime_error {
   Error(tg_status c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// Message returned by tg_last_error() on this thread.
+void set_last_error(const std::string& m);
+
 [[noreturn]] inline void fail(tg_status c, const std::string& m) { throw Error(c, m); }
 
 inline void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
