@@ -69,11 +69,21 @@ def heisenberg_op():
 
 
 # ------------------------------------------------------------------ our arm
-def make_env(cfg, seed, device):
-    from tenes_b200.env import CTMParams, Environment
+def ctm_params(cfg, projector):
+    from tenes_b200.env import CTMParams
+    D, chi, _, _ = CONFIGS[cfg]
+    if projector == "rsvd":
+        # rSVD projectors, oversampling chi+10, 2 power iterations
+        return CTMParams(chi=chi, max_ctm_iteration=1, use_rsvd=True, rsvd_oversample_abs=10,
+                         rsvd_power_iters=2)
+    return CTMParams(chi=chi, max_ctm_iteration=1)
+
+
+def make_env(cfg, seed, device, projector="svd"):
+    from tenes_b200.env import Environment
     D, chi, su_steps, _ = CONFIGS[cfg]
     LX, LY, pd, vd, dirs, noises = lattice_spec(D)
-    env = Environment(LX, LY, pd, vd, CTMParams(chi=chi, max_ctm_iteration=1), False, device=device)
+    env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector), False, device=device)
     env.init_tensors(seed, dirs, noises)
     op = heisenberg_op()
     t0 = time.perf_counter()
@@ -169,7 +179,7 @@ def run_ours(args, rank, world, local_rank):
                                 profile_reset)
     device = local_rank
     torch.cuda.set_device(device)
-    env = make_env(args.config, SEED + rank, device)
+    env = make_env(args.config, SEED + rank, device, args.projector)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
@@ -329,6 +339,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--projector", default="svd", choices=["svd", "rsvd"],
+                    help="svd: full SVD (reference default); rsvd: k = chi+10, 2 power iterations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-sweep", action="store_true",
                     help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")
@@ -367,7 +379,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": name, "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
-                           "projector": "full SVD (reference default)", "parallelism": f"replicas{world}",
+                           "projector": ("full SVD (reference default)" if args.projector == "svd"
+                                         else "rSVD k=chi+10, q=2"), "parallelism": f"replicas{world}",
                            "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}

@@ -53,7 +53,9 @@ struct EngineT final : Engine {
   bool spec_old_ok = false;
 
   unsigned long long* d_max = nullptr;
-  int* d_info = nullptr;
+  static constexpr int kInfoSlots = 4096;
+  int* d_info = nullptr;  // one slot per cuSOLVER call, checked at sync points
+  int info_used = 0;
   int* d_cut = nullptr;
   const T** d_ptrs = nullptr;
   const T** h_ptrs = nullptr;  // pinned
@@ -80,7 +82,8 @@ struct EngineT final : Engine {
     check_sol(cusolverDnCreate(&sol), "cusolverDnCreate");
     check_sol(cusolverDnSetStream(sol, st), "cusolverDnSetStream");
     TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long)));
-    TG_CUDA(cudaMalloc(&d_info, sizeof(int) * 4));
+    TG_CUDA(cudaMalloc(&d_info, sizeof(int) * kInfoSlots));
+    TG_CUDA(cudaMemset(d_info, 0, sizeof(int) * kInfoSlots));
     TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * 4));
     TG_CUDA(cudaMalloc(&d_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_ptrs, sizeof(T*) * 4 * lat.N));
@@ -202,13 +205,13 @@ struct EngineT final : Engine {
       check_sol(cusolverDnZgesvd(sol, 'S', 'S', rows, cols, reinterpret_cast<cuDoubleComplex*>(A.p), rows, s.p,
                                  reinterpret_cast<cuDoubleComplex*>(Ub.p), rows,
                                  reinterpret_cast<cuDoubleComplex*>(VTb.p), cols,
-                                 reinterpret_cast<cuDoubleComplex*>(work.p), lwork, rwork.p, d_info),
+                                 reinterpret_cast<cuDoubleComplex*>(work.p), lwork, rwork.p, info_slot()),
                 "Zgesvd");
     } else {
       check_sol(cusolverDnDgesvd_bufferSize(sol, rows, cols, &lwork), "Dgesvd_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
       check_sol(cusolverDnDgesvd(sol, 'S', 'S', rows, cols, A.p, rows, s.p, Ub.p, rows, VTb.p, cols, work.p,
-                                 lwork, nullptr, d_info),
+                                 lwork, nullptr, info_slot()),
                 "Dgesvd");
     }
     U = reshape(VTb, {m, k});
@@ -218,14 +221,26 @@ struct EngineT final : Engine {
       // only on the value: VT_B holds V_B^H, whose row-major reading is
       // conj(V_B) already; VT_A = U_B^T has no conjugation.
     }
-    check_info("gesvd");
   }
 
-  void check_info(const char* what) {
-    int info = 0;
-    TG_CUDA(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int* info_slot() {
+    if (info_used == kInfoSlots) check_infos();
+    return d_info + info_used++;
+  }
+  // Every cuSOLVER call reports into its own device slot; a non-zero value
+  // (illegal argument or non-convergence) is turned into an error here.
+  void check_infos() {
+    if (info_used == 0) return;
+    std::vector<int> h(static_cast<size_t>(info_used));
+    TG_CUDA(cudaMemcpyAsync(h.data(), d_info, sizeof(int) * info_used, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
-    if (info != 0) fail(TG_E_RUNTIME, std::string(what) + " failed, info = " + std::to_string(info));
+    const int n = info_used;
+    info_used = 0;
+    for (int i = 0; i < n; ++i)
+      if (h[static_cast<size_t>(i)] != 0) {
+        TG_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int) * n, st));
+        fail(TG_E_RUNTIME, "cuSOLVER factorisation failed, info = " + std::to_string(h[static_cast<size_t>(i)]));
+      }
   }
 
   // QR of a row-major m x n matrix: Q (m x k), R (k x n), k = min(m, n)
@@ -244,22 +259,21 @@ struct EngineT final : Engine {
       check_sol(cusolverDnZungqr_bufferSize(sol, im, ik, ik, a, im, t, &lwork2), "Zungqr_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
       auto* w = reinterpret_cast<cuDoubleComplex*>(work.p);
-      check_sol(cusolverDnZgeqrf(sol, im, in, a, im, t, w, std::max(lwork, lwork2), d_info), "Zgeqrf");
+      check_sol(cusolverDnZgeqrf(sol, im, in, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zgeqrf");
       // R: upper k x n of the factored matrix (column-major (m, n))
       R = DT<T>({n, k}, st);  // fill as row-major (n, k) == column-major (k, n)
       extract_r(Ac, m, n, k, R);
-      check_sol(cusolverDnZungqr(sol, im, ik, ik, a, im, t, w, std::max(lwork, lwork2), d_info), "Zungqr");
+      check_sol(cusolverDnZungqr(sol, im, ik, ik, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zungqr");
     } else {
       check_sol(cusolverDnDgeqrf_bufferSize(sol, im, in, Ac.p, im, &lwork), "Dgeqrf_bufferSize");
       check_sol(cusolverDnDorgqr_bufferSize(sol, im, ik, ik, Ac.p, im, tau.p, &lwork2), "Dorgqr_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
-      check_sol(cusolverDnDgeqrf(sol, im, in, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), d_info), "Dgeqrf");
+      check_sol(cusolverDnDgeqrf(sol, im, in, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()), "Dgeqrf");
       R = DT<T>({n, k}, st);
       extract_r(Ac, m, n, k, R);
-      check_sol(cusolverDnDorgqr(sol, im, ik, ik, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), d_info),
+      check_sol(cusolverDnDorgqr(sol, im, ik, ik, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()),
                 "Dorgqr");
     }
-    check_info("qr");
     // Q: first k columns of the column-major (m, *) buffer -> row-major (m, k)
     DT<T> Qc = DT<T>({k, m}, st);
     TG_CUDA(cudaMemcpyAsync(Qc.p, Ac.p, sizeof(T) * k * m, cudaMemcpyDeviceToDevice, st));
@@ -295,6 +309,140 @@ struct EngineT final : Engine {
     return td(T4, X, {0, 3, 4}, {1, 3, 6});
   }
 
+  // ------------------------------------------------ matrix-view products
+  // element (i, j) of a view is p[i*rs + j*cs]; one of rs / cs must be 1
+  struct MV {
+    const T* p;
+    int64_t rows, cols, rs, cs;
+    bool conj;
+  };
+  static MV rm(const T* p, int64_t r, int64_t c) { return MV{p, r, c, c, 1, false}; }      // row-major
+  static MV cm(const T* p, int64_t r, int64_t c) { return MV{p, r, c, 1, r, false}; }      // column-major
+  static MV tp(MV a) { return MV{a.p, a.cols, a.rows, a.cs, a.rs, a.conj}; }               // transpose
+  static MV ht(MV a) { return MV{a.p, a.cols, a.rows, a.cs, a.rs, !a.conj}; }              // conj transpose
+  // C (rows x cols at C[i*crs + j*ccs]) = A B
+  void mm(const MV& A, const MV& B, T* C, int64_t crs, int64_t ccs) {
+    if (A.cols != B.rows) fail(TG_E_INPUT, "mm: inner dimensions differ");
+    GemmDesc g{};
+    g.M = A.rows;
+    g.N = B.cols;
+    g.K = A.cols;
+    g.batch = 1;
+    g.sAm = A.rs;
+    g.sAk = A.cs;
+    g.sBk = B.rs;
+    g.sBn = B.cs;
+    g.sCm = crs;
+    g.sCn = ccs;
+    g.conjA = A.conj;
+    g.conjB = B.conj;
+    g.accumulate = false;
+    gemm<T>(A.p, B.p, C, g, st);
+  }
+  DT<T> mm_rm(const MV& A, const MV& B) {  // row-major result
+    DT<T> C({A.rows, B.cols}, st);
+    mm(A, B, C.p, B.cols, 1);
+    return C;
+  }
+  DT<T> mm_cm(const MV& A, const MV& B) {  // column-major result (stored as (cols, rows) row-major)
+    DT<T> C({B.cols, A.rows}, st);
+    mm(A, B, C.p, 1, A.rows);
+    return C;
+  }
+
+  // Householder QR of a column-major n x k panel, in place (cuSOLVER geqrf):
+  // R in the upper triangle, reflectors below; tau returned.
+  DT<T> geqrf_cm(DT<T>& Y, int64_t n, int64_t k) {
+    DT<T> tau({std::max<int64_t>(k, 1)}, st);
+    int lwork = 0;
+    const int in = static_cast<int>(n), ik = static_cast<int>(k);
+    ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * n * k * k, 0.0);
+    if constexpr (CPLX) {
+      auto* a = reinterpret_cast<cuDoubleComplex*>(Y.p);
+      check_sol(cusolverDnZgeqrf_bufferSize(sol, in, ik, a, in, &lwork), "Zgeqrf_bufferSize");
+      DT<T> work({std::max<int64_t>(lwork, 1)}, st);
+      check_sol(cusolverDnZgeqrf(sol, in, ik, a, in, reinterpret_cast<cuDoubleComplex*>(tau.p),
+                                 reinterpret_cast<cuDoubleComplex*>(work.p), lwork, info_slot()),
+                "Zgeqrf");
+    } else {
+      check_sol(cusolverDnDgeqrf_bufferSize(sol, in, ik, Y.p, in, &lwork), "Dgeqrf_bufferSize");
+      DT<T> work({std::max<int64_t>(lwork, 1)}, st);
+      check_sol(cusolverDnDgeqrf(sol, in, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dgeqrf");
+    }
+    return tau;
+  }
+  // form the explicit Q (n x k, column-major) from geqrf's output, in place
+  void orgqr_cm(DT<T>& Y, int64_t n, int64_t k, const DT<T>& tau) {
+    int lwork = 0;
+    const int in = static_cast<int>(n), ik = static_cast<int>(k);
+    ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * n * k * k, 0.0);
+    if constexpr (CPLX) {
+      auto* a = reinterpret_cast<cuDoubleComplex*>(Y.p);
+      auto* t = reinterpret_cast<const cuDoubleComplex*>(tau.p);
+      check_sol(cusolverDnZungqr_bufferSize(sol, in, ik, ik, a, in, t, &lwork), "Zungqr_bufferSize");
+      DT<T> work({std::max<int64_t>(lwork, 1)}, st);
+      check_sol(cusolverDnZungqr(sol, in, ik, ik, a, in, t, reinterpret_cast<cuDoubleComplex*>(work.p), lwork,
+                                 info_slot()),
+                "Zungqr");
+    } else {
+      check_sol(cusolverDnDorgqr_bufferSize(sol, in, ik, ik, Y.p, in, tau.p, &lwork), "Dorgqr_bufferSize");
+      DT<T> work({std::max<int64_t>(lwork, 1)}, st);
+      check_sol(cusolverDnDorgqr(sol, in, ik, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dorgqr");
+    }
+  }
+  void orth_cm(DT<T>& Y, int64_t n, int64_t k) {
+    DT<T> tau = geqrf_cm(Y, n, k);
+    orgqr_cm(Y, n, k, tau);
+  }
+
+  // Randomized SVD of M = LTm * LBm (Halko, Martinsson & Tropp 2011,
+  // Alg. 4.4 with q power iterations, then the SVD of B = Q^H M through a QR
+  // of B^H and a one-sided Jacobi SVD of the k x k factor).  The test matrix
+  // is the counter-based Gaussian stream shared with the CPU oracle.  Outputs
+  // the truncated, 1/sqrt(s)-scaled factors Uc (nrow x w, row-major) and
+  // Vc (ncol x w, row-major), w = min(k, chi); columns past `cut` are zero.
+  // Stands in for mptensor::rsvd (src/iTPS/core/ctm.cpp:243-244).
+  void rsvd_factors(const DT<T>& LTm, const DT<T>& LBm, int64_t nrow, int64_t nmid, int64_t ncol, int cut,
+                    int64_t k, DT<T>& Uc, DT<T>& Vc) {
+    const MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
+    auto apply_M = [&](const DT<T>& Xcm) {  // (ncol x k) col-major -> (nrow x k) col-major
+      DT<T> t = mm_cm(lb, cm(Xcm.p, ncol, k));
+      return mm_cm(lt, cm(t.p, nmid, k));
+    };
+    auto apply_MH = [&](const DT<T>& Ycm) {  // (nrow x k) -> (ncol x k), both col-major
+      DT<T> t = mm_cm(ht(lt), cm(Ycm.p, nrow, k));
+      return mm_cm(ht(lb), cm(t.p, nmid, k));
+    };
+    DT<T> Om({k, ncol}, st);
+    counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
+    DT<T> Q = apply_M(Om);
+    orth_cm(Q, nrow, k);
+    for (int it = 0; it < P.rsvd_power_iters; ++it) {
+      DT<T> Z = apply_MH(Q);
+      orth_cm(Z, ncol, k);
+      Q = apply_M(Z);
+      orth_cm(Q, nrow, k);
+    }
+    DT<T> Z = apply_MH(Q);  // M^H Q = B^H (ncol x k)
+    DT<T> tau = geqrf_cm(Z, ncol, k);
+    DT<T> Rh({k, k}, st);
+    upper_to_rh<T>(Z.p, ncol, k, Rh.p, st);  // Rz^H (k x k, row-major)
+    orgqr_cm(Z, ncol, k, tau);               // Qz
+    DT<T> Ur({k, k}, st), Wr({k, k}, st);
+    DT<double> s({k}, st);
+    jacobi_svd<T>(Rh.p, k, Ur.p, s.p, Wr.p, st);  // Rz^H Wr = Ur S
+    // B = Rz^H Qz^H = Ur S (Qz Wr)^H:  U = Q Ur,  V = Qz Wr
+    DT<T> U = mm_rm(cm(Q.p, nrow, k), rm(Ur.p, k, k));
+    DT<T> V = mm_rm(cm(Z.p, ncol, k), rm(Wr.p, k, k));
+    const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
+    DT<double> sinv({w}, st);
+    truncation(s.p, k, cut, P.inverse_projector_cut, sinv.p, w, d_cut, st);
+    Uc = DT<T>({nrow, w}, st);
+    scale_cols<T>(U.p, k, nrow, w, sinv.p, false, Uc.p, st);
+    Vc = DT<T>({ncol, w}, st);
+    scale_cols<T>(V.p, k, ncol, w, sinv.p, false, Vc.p, st);
+  }
+
   // Truncated projectors from M (nrow x ncol, consumed):
   // U_c (nrow x w), VT_c (w x ncol) scaled by 1/sqrt(s), w = min(k, chi)
   void truncated_factors(DT<T>& M, int64_t nrow, int64_t ncol, DT<T>& Uc, DT<T>& VTc) {
@@ -318,21 +466,38 @@ struct EngineT final : Engine {
     const int64_t e12 = eT1.dim(1), e56 = eT6.dim(0), e78 = eT8.dim(0);
     const int64_t t12 = T1.dim(2), t41 = T1.dim(3), t34 = T4.dim(2);
     if (t41 != 1) {
-      DT<T> LT = block_LT(C1, eT1, eT8, T1);
-      DT<T> LB = block_LB(C4, eT7, eT6, T4);
-      const int64_t nrow = t12 * e12 * t12, ncol = t34 * e56 * t34;
-      DT<T> Uc, VTc;
+      // LT as the matrix [(t12,e12,tc12), (t41,e78,tc41)], LB as [(t41,e78,tc41), (t34,e56,tc34)]:
+      // M = LTm LBm is tensordot(LT, LB, Axes(1,3,5), Axes(0,2,4)) of ctm.cpp:273
+      DT<T> LTm = tr(block_LT(C1, eT1, eT8, T1), {0, 2, 4, 1, 3, 5});
+      DT<T> LBm = tr(block_LB(C4, eT7, eT6, T4), {0, 2, 4, 1, 3, 5});
+      const int64_t nrow = t12 * e12 * t12, nmid = t41 * e78 * t41, ncol = t34 * e56 * t34;
+      const MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
+      DT<T> Uc, Vrow;  // Uc: nrow x w;  PU = LBm * Vc where Vc = (VT_c)^H
+      MV vc{nullptr, 0, 0, 0, 0, false};
       if ((t12 != 1 && t34 != 1) && P.use_rsvd) {
-        fail(TG_E_INPUT, "use_rsvd is not available in this build of the FP64 path");
+        // cut = min(chi, e78 t41^2, e12 t12^2, e56 t34^2), k = factor * cut (ctm.cpp:242-244)
+        const int cut = static_cast<int>(std::min<int64_t>(std::min<int64_t>(P.chi, nmid), std::min(nrow, ncol)));
+        int64_t k = P.rsvd_oversample_abs >= 0 ? cut + P.rsvd_oversample_abs
+                                               : static_cast<int64_t>(P.rsvd_oversampling_factor * cut);
+        k = std::min<int64_t>(std::min(k, nrow), ncol);
+        if (k > jacobi_svd_max_k<T>())
+          fail(TG_E_INPUT, "rSVD sketch size " + std::to_string(k) + " exceeds " +
+                               std::to_string(jacobi_svd_max_k<T>()) +
+                               " (lower rsvd_oversampling_factor or set rsvd_oversample_abs)");
+        rsvd_factors(LTm, LBm, nrow, nmid, ncol, cut, k, Uc, Vrow);
+        vc = rm(Vrow.p, ncol, Vrow.dim(1));
       } else {
-        DT<T> M = td(LT, LB, {1, 3, 5}, {0, 2, 4});
-        truncated_factors(M, nrow, ncol, Uc, VTc);
+        DT<T> M = mm_rm(lt, lb);
+        truncated_factors(M, nrow, ncol, Uc, Vrow);  // Vrow = VT_c (w x ncol)
+        vc = ht(rm(Vrow.p, Vrow.dim(0), ncol));
       }
       const int64_t w = Uc.dim(1);
-      DT<T> VTc4 = reshape(VTc, {w, t34, e56, t34});
-      DT<T> Uc4 = reshape(Uc, {t12, e12, t12, w});
-      PU = tr(td(LB, VTc4, {1, 3, 5}, {1, 2, 3}, false, true), {1, 0, 2, 3});
-      PL = tr(td(LT, Uc4, {0, 2, 4}, {0, 1, 2}, false, true), {1, 0, 2, 3});
+      // PU = tensordot(LB, conj(VT_c), Axes(1,3,5), Axes(1,2,3)).transpose(1,0,2,3)  (ctm.cpp:263-266)
+      PU = tr(reshape(mm_rm(lb, vc), {t41, e78, t41, w}), {1, 0, 2, 3});
+      // PL = tensordot(LT, conj(U_c), Axes(0,2,4), Axes(0,1,2)).transpose(1,0,2,3)
+      MV uc = rm(Uc.p, nrow, w);
+      uc.conj = true;
+      PL = tr(reshape(mm_rm(tp(lt), uc), {t41, e78, t41, w}), {1, 0, 2, 3});
     } else {
       PU = DT<T>({e78, 1, 1, e78}, st);
       identity<T>(PU.p, e78, st);
@@ -551,6 +716,7 @@ struct EngineT final : Engine {
       case 3: bottom_move(line); break;
       default: fail(TG_E_INPUT, "move direction must be 0..3");
     }
+    check_infos();
   }
 
   void sweep_impl() {
@@ -564,6 +730,7 @@ struct EngineT final : Engine {
   void ctm_sweep() override {
     require_env();
     sweep_impl();
+    check_infos();
     TG_CUDA(cudaStreamSynchronize(st));
   }
 
@@ -587,7 +754,7 @@ struct EngineT final : Engine {
     DT<double> sig({cnt}, st);
     spectrum_distance(now.p, spec_old.p, cnt, P.chi, sig.p, st);
     TG_CUDA(cudaMemcpyAsync(h_sig, sig.p, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st));
-    TG_CUDA(cudaStreamSynchronize(st));
+    check_infos();
     // early break on the first corner above epsilon, in the reference's
     // order (site-major, C1..C4), ctm.cpp:828-967
     double smax = 0.0;
@@ -823,7 +990,7 @@ struct EngineT final : Engine {
     lambda[source][connect1] = lc;
     lambda[target][connect2] = lc;
     rot_ok[source] = rot_ok[target] = false;
-    TG_CUDA(cudaStreamSynchronize(st));
+    check_infos();
   }
 
   // iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137): Tn[0,0,0,0,p] =
@@ -920,7 +1087,10 @@ struct EngineT final : Engine {
     spec_old_ok = false;
   }
   void get_env(int which, int site, double* host) override { download(env_ref(which, site), host); }
-  void sync() override { TG_CUDA(cudaStreamSynchronize(st)); }
+  void sync() override {
+    check_infos();
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
   void* stream() override { return static_cast<void*>(st); }
 };
 

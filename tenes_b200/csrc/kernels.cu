@@ -563,6 +563,183 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
   if (threadIdx.x == 0 && sweeps_used) sweeps_used[blockIdx.x] = sweep;
 }
 
+// splitmix64 finaliser on a Weyl sequence; the CPU oracle's counter_normal
+// (oracle/tenes_oracle.py) computes the same numbers.
+__device__ __forceinline__ double counter_uniform(uint64_t idx, uint64_t key) {
+  uint64_t z = idx * 0x9E3779B97F4A7C15ull + key;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (static_cast<double>(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ double counter_gauss(uint64_t n, uint64_t key) {
+  const double u1 = counter_uniform(2 * n, key);
+  const double u2 = counter_uniform(2 * n + 1, key);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+template <typename T>
+__global__ void counter_normal_kernel(T* __restrict__ out, int64_t rows, int64_t cols, uint64_t key_re,
+                                      uint64_t key_im) {
+  const int64_t total = rows * cols;
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < total;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = n / cols, j = n - i * cols;
+    const double re = counter_gauss(static_cast<uint64_t>(n), key_re);
+    T v;
+    if constexpr (is_cplx<T>::value) {
+      v = make_double2(re, counter_gauss(static_cast<uint64_t>(n), key_im));
+    } else {
+      v = re;
+    }
+    out[i + j * rows] = v;
+  }
+}
+
+template <typename T>
+__global__ void upper_to_rh_kernel(const T* __restrict__ acm, int64_t lda, int64_t k, T* __restrict__ out) {
+  const int64_t total = k * k;
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < total;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t a = n / k, b = n - a * k;  // out[a, b] = conj(R[b, a]), R upper
+    out[n] = (b <= a) ? conj_of(acm[b + a * lda]) : zero_of<T>();
+  }
+}
+
+// One-sided Jacobi SVD with vectors; see jacobi_svd() in kernels.cuh.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
+                                                          double* __restrict__ S, T* __restrict__ Wout) {
+  extern __shared__ double sm[];
+  const int nn = n * n;
+  double* ar = sm;
+  double* ai = sm + nn;                       // complex only
+  double* wr = sm + (CPLX ? 2 : 1) * nn;
+  double* wi = wr + nn;                       // complex only
+  double* nrm = sm + (CPLX ? 4 : 2) * nn;     // n
+  int* pos = reinterpret_cast<int*>(nrm + n);  // n
+  __shared__ int rotated;
+  for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    const int r = idx / n, c = idx % n;
+    const T v = A[idx];
+    ar[c * n + r] = re_of(v);
+    wr[c * n + r] = (r == c) ? 1.0 : 0.0;
+    if constexpr (CPLX) {
+      ai[c * n + r] = im_of(v);
+      wi[c * n + r] = 0.0;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int np = n + (n & 1);
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    if (threadIdx.x == 0) rotated = 0;
+    __syncthreads();
+    for (int rnd = 0; rnd < np - 1; ++rnd) {
+      for (int pr = warp; pr < np / 2; pr += nw) {
+        auto player = [&](int kk) { return kk == 0 ? 0 : ((kk - 1 + rnd) % (np - 1)) + 1; };
+        int p = player(pr), q = player(np - 1 - pr);
+        if (p >= n || q >= n) continue;
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        double al = 0, be = 0, gr = 0, gi = 0;
+        for (int r = lane; r < n; r += 32) {
+          const double pr_ = ar[p * n + r], qr_ = ar[q * n + r];
+          al += pr_ * pr_;
+          be += qr_ * qr_;
+          gr += pr_ * qr_;
+          if constexpr (CPLX) {
+            const double pi_ = ai[p * n + r], qi_ = ai[q * n + r];
+            al += pi_ * pi_;
+            be += qi_ * qi_;
+            gr += pi_ * qi_;
+            gi += pr_ * qi_ - pi_ * qr_;
+          }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o);
+          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
+        }
+        const double g = CPLX ? hypot(gr, gi) : fabs(gr);
+        if (g == 0.0 || g <= 1e-15 * sqrt(al * be)) continue;
+        const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
+        const double ph_i = CPLX ? -gi / g : 0.0;
+        const double zeta = (be - al) / (2.0 * g);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        for (int r = lane; r < n; r += 32) {
+          {
+            const double xpr = ar[p * n + r], xqr = ar[q * n + r];
+            const double xpi = CPLX ? ai[p * n + r] : 0.0, xqi = CPLX ? ai[q * n + r] : 0.0;
+            const double bqr = xqr * ph_r - xqi * ph_i, bqi = xqr * ph_i + xqi * ph_r;
+            ar[p * n + r] = c * xpr - s * bqr;
+            ar[q * n + r] = s * xpr + c * bqr;
+            if constexpr (CPLX) {
+              ai[p * n + r] = c * xpi - s * bqi;
+              ai[q * n + r] = s * xpi + c * bqi;
+            }
+          }
+          {
+            const double xpr = wr[p * n + r], xqr = wr[q * n + r];
+            const double xpi = CPLX ? wi[p * n + r] : 0.0, xqi = CPLX ? wi[q * n + r] : 0.0;
+            const double bqr = xqr * ph_r - xqi * ph_i, bqi = xqr * ph_i + xqi * ph_r;
+            wr[p * n + r] = c * xpr - s * bqr;
+            wr[q * n + r] = s * xpr + c * bqr;
+            if constexpr (CPLX) {
+              wi[p * n + r] = c * xpi - s * bqi;
+              wi[q * n + r] = s * xpi + c * bqi;
+            }
+          }
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    const int any = rotated;
+    __syncthreads();
+    if (!any) break;
+  }
+  for (int c = warp; c < n; c += nw) {
+    double a = 0;
+    for (int r = lane; r < n; r += 32) {
+      a += ar[c * n + r] * ar[c * n + r];
+      if constexpr (CPLX) a += ai[c * n + r] * ai[c * n + r];
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) nrm[c] = sqrt(a);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const double v = nrm[c];
+    int p = 0;
+    for (int o = 0; o < n; ++o) {
+      const double w = nrm[o];
+      p += (w > v) || (w == v && o < c);
+    }
+    pos[c] = p;
+    S[p] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    const int r = idx / n, c = idx % n;  // source column c -> output column pos[c]
+    const double inv = nrm[c] > 0.0 ? 1.0 / nrm[c] : 0.0;
+    const int64_t o = static_cast<int64_t>(r) * n + pos[c];
+    if constexpr (CPLX) {
+      U[o] = make_double2(ar[c * n + r] * inv, ai[c * n + r] * inv);
+      Wout[o] = make_double2(wr[c * n + r], wi[c * n + r]);
+    } else {
+      U[o] = ar[c * n + r] * inv;
+      Wout[o] = wr[c * n + r];
+    }
+  }
+}
+
 __global__ void spectrum_distance_kernel(const double* a, const double* c, int count, int n,
                                          double* sig) {
   const int b = blockIdx.x;
@@ -727,7 +904,50 @@ void scale_leg(T* x, int64_t outer, int64_t dim, int64_t inner, const double* v,
   count_launch();
 }
 
+template <typename T>
+void counter_normal(T* out, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream, cudaStream_t st) {
+  const uint64_t k_re = seed * 0x9E3779B97F4A7C15ull + stream * 0xBF58476D1CE4E5B9ull;
+  const uint64_t k_im = seed * 0x9E3779B97F4A7C15ull + (stream + 1) * 0xBF58476D1CE4E5B9ull;
+  counter_normal_kernel<T><<<num_blocks(rows * cols, 256), 256, 0, st>>>(out, rows, cols, k_re, k_im);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void upper_to_rh(const T* acm, int64_t lda, int64_t k, T* out, cudaStream_t st) {
+  upper_to_rh_kernel<T><<<num_blocks(k * k, 256), 256, 0, st>>>(acm, lda, k, out);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+int jacobi_svd_max_k() {
+  // A and W (re [, im]) plus norms / positions must fit in 227 KB of smem
+  return is_cplx<T>::value ? 84 : 119;
+}
+
+template <typename T>
+void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st) {
+  constexpr bool CPLX = is_cplx<T>::value;
+  if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "jacobi_svd: k out of range");
+  const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k) + sizeof(int) * k;
+  static size_t attr_bytes = 0;
+  if (smem > attr_bytes) {
+    TG_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    attr_bytes = smem;
+  }
+  ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
+  jacobi_svd_kernel<T, CPLX><<<1, 512, smem, st>>>(A, static_cast<int>(k), U, S, W);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
 #define TG_INST(T)                                                                               \
+  template void counter_normal<T>(T*, int64_t, int64_t, uint64_t, uint64_t, cudaStream_t);       \
+  template void upper_to_rh<T>(const T*, int64_t, int64_t, T*, cudaStream_t);                    \
+  template int jacobi_svd_max_k<T>();                                                            \
+  template void jacobi_svd<T>(const T*, int64_t, T*, double*, T*, cudaStream_t);                 \
   template void gemm<T>(const T*, const T*, T*, const GemmDesc&, cudaStream_t);                  \
   template void permute<T>(const T*, T*, const Shape&, const std::vector<int>&, bool,            \
                            cudaStream_t);                                                        \

@@ -66,6 +66,28 @@ void batched_spectrum(const T* const* mats, int count, int n, double* out, int* 
 void spectrum_distance(const double* a, const double* c, int count, int n, double* sig,
                        cudaStream_t st);
 
+// Counter-based standard normals (splitmix64 hash + Box-Muller) in a
+// column-major rows x cols array: element (i, j) uses counters 2n, 2n+1 of the
+// row-major index n = i*cols + j under key (seed, stream); complex arrays take
+// their imaginary parts from stream + 1.  The CPU oracle draws the same numbers.
+template <typename T>
+void counter_normal(T* out_colmajor, int64_t rows, int64_t cols, uint64_t seed, uint64_t stream,
+                    cudaStream_t st);
+
+// out (row-major k x k) = R^H, R = upper triangle of the first k rows of the
+// column-major factored matrix `acm` (leading dimension lda) left by geqrf.
+template <typename T>
+void upper_to_rh(const T* acm, int64_t lda, int64_t k, T* out, cudaStream_t st);
+
+// SVD of one row-major k x k matrix by one-sided Jacobi with accumulated
+// right vectors, in one CTA with A and W resident in shared memory:
+// A W = U S, singular values descending.  U, W written row-major (k x k,
+// column j = j-th singular vector), S (k).  k <= jacobi_svd_max_k<T>().
+template <typename T>
+void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st);
+template <typename T>
+int jacobi_svd_max_k();
+
 // x *= alpha (scalar, real)
 template <typename T>
 void scale(T* x, int64_t n, double alpha, cudaStream_t st);

@@ -113,3 +113,27 @@ def test_complex_ctm_run_matches_oracle():
     gcnt, _, _ = ge.calc_ctm_environment(True)
     assert gcnt == ocnt
     np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+@pytest.mark.parametrize("oversample", [-1, 4])
+def test_rsvd_ctm_run_matches_oracle(is_complex, oversample):
+    """rSVD projectors (ctm.cpp:231-266) with the shared counter-based test
+    matrix: the GPU rSVD and the oracle's see identical random inputs, so the
+    environments agree to rounding."""
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 21, is_complex)
+    chi, iters = 8, 4
+    kw = dict(Use_RSVD=True, Max_CTM_Iteration=iters, rsvd_power_iters=2)
+    if oversample >= 0:
+        kw["rsvd_oversample_abs"] = oversample
+    oe, ocnt, _, _ = O.calc_ctm_environment(Tn, oracle_params(chi, **kw), lat)
+    ge = gpu_env(lat, Tn, chi, is_complex, max_ctm_iteration=iters, use_rsvd=True,
+                 rsvd_oversample_abs=oversample, rsvd_power_iters=2)
+    gcnt, _, _ = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt
+    for w, name in enumerate(("C1", "C2", "C3", "C4")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i]),
+                                       rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
