@@ -56,6 +56,8 @@ struct EngineT final : Engine {
   static constexpr int kInfoSlots = 4096;
   int* d_info = nullptr;  // one slot per cuSOLVER call, checked at sync points
   int info_used = 0;
+  int* d_flag = nullptr;  // set by device kernels on a numerical failure
+  uint64_t noise_stream = 0;  // key sequence of the orthonormalisation perturbations
   int* d_cut = nullptr;
   const T** d_ptrs = nullptr;
   const T** h_ptrs = nullptr;  // pinned
@@ -84,6 +86,8 @@ struct EngineT final : Engine {
     TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long)));
     TG_CUDA(cudaMalloc(&d_info, sizeof(int) * kInfoSlots));
     TG_CUDA(cudaMemset(d_info, 0, sizeof(int) * kInfoSlots));
+    TG_CUDA(cudaMalloc(&d_flag, sizeof(int)));
+    TG_CUDA(cudaMemset(d_flag, 0, sizeof(int)));
     TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * 4));
     TG_CUDA(cudaMalloc(&d_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_ptrs, sizeof(T*) * 4 * lat.N));
@@ -125,6 +129,7 @@ struct EngineT final : Engine {
     if (sol) cusolverDnDestroy(sol);
     cudaFree(d_max);
     cudaFree(d_info);
+    cudaFree(d_flag);
     cudaFree(d_cut);
     cudaFree(d_ptrs);
     cudaFreeHost(h_ptrs);
@@ -230,6 +235,13 @@ struct EngineT final : Engine {
   // Every cuSOLVER call reports into its own device slot; a non-zero value
   // (illegal argument or non-convergence) is turned into an error here.
   void check_infos() {
+    int flag = 0;
+    TG_CUDA(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (flag) {
+      TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+      fail(TG_E_RUNTIME, "CholeskyQR orthonormalisation met a non-positive pivot (rank-deficient panel)");
+    }
     if (info_used == 0) return;
     std::vector<int> h(static_cast<size_t>(info_used));
     TG_CUDA(cudaMemcpyAsync(h.data(), d_info, sizeof(int) * info_used, cudaMemcpyDeviceToHost, st));
@@ -395,6 +407,66 @@ struct EngineT final : Engine {
     orgqr_cm(Y, n, k, tau);
   }
 
+  // G = Y^H Y (k x k, row-major) of a column-major n x k panel: split-K DMMA
+  // products into partial Gram matrices, then one summation pass.
+  DT<T> gram(const DT<T>& Y, int64_t n, int64_t k) {
+    const int64_t chunk = std::max<int64_t>(64, (n + 63) / 64);
+    const int64_t nfull = n / chunk, rem = n - nfull * chunk;
+    const int nparts = static_cast<int>(nfull + (rem > 0 ? 1 : 0));
+    DT<T> parts({nparts, k, k}, st);
+    GemmDesc g{};
+    g.M = k;
+    g.N = k;
+    g.sAm = n;  // A = Y^H: element (i, j) = conj(Y[j + i n])
+    g.sAk = 1;
+    g.sBk = 1;  // B = Y: element (j, c) = Y[j + c n]
+    g.sBn = n;
+    g.sCm = k;
+    g.sCn = 1;
+    g.conjA = true;
+    g.conjB = false;
+    g.accumulate = false;
+    if (nfull > 0) {
+      g.K = chunk;
+      g.batch = nfull;
+      g.bA = chunk;
+      g.bB = chunk;
+      g.bC = k * k;
+      gemm<T>(Y.p, Y.p, parts.p, g, st);
+    }
+    if (rem > 0) {
+      g.K = rem;
+      g.batch = 1;
+      gemm<T>(Y.p + nfull * chunk, Y.p + nfull * chunk, parts.p + nfull * k * k, g, st);
+    }
+    DT<T> G({k, k}, st);
+    sum_partials<T>(parts.p, nparts, k * k, G.p, st);
+    return G;
+  }
+
+  // Shifted CholeskyQR3 with column equilibration (Fukaya, Kannan,
+  // Nakatsukasa, Yamamoto, Yanagisawa 2020): three Gram / Cholesky /
+  // triangular-solve passes, the first shifted, orthonormal to O(u) for
+  // panels with condition number up to ~1/u.  Y (column-major n x k) is
+  // replaced by Q; if R is given, Y = Q R on return (R upper, row-major).
+  //
+  // Only the span of Q is used.  A panel may be rank deficient (zero-padded
+  // environment legs give exactly-zero rows), so after the first shifted pass
+  // -- whose output has columns of norm <= 1 -- a counter-based Gaussian
+  // perturbation of norm ~1e-14 per column is added: it turns the missing
+  // directions into independent ones, which the following shifted pass and
+  // two plain passes orthonormalise.  The perturbation moves the span by
+  // ~1e-14, below the rounding of the products that produced the panel.
+  void orth_chol(DT<T>& Y, int64_t n, int64_t k) {
+    for (int pass = 0; pass < 4; ++pass) {
+      DT<T> G = gram(Y, n, k);
+      DT<T> Rp({k, k}, st), Ri({k, k}, st);
+      chol_rinv<T>(G.p, k, n, pass <= 1 ? 1 : 0, Rp.p, Ri.p, d_flag, st);
+      Y = mm_cm(cm(Y.p, n, k), rm(Ri.p, k, k));
+      if (pass == 0) add_noise<T>(Y.p, n * k, 1e-14 / std::sqrt(static_cast<double>(n)), ++noise_stream, st);
+    }
+  }
+
   // Randomized SVD of M = LTm * LBm (Halko, Martinsson & Tropp 2011,
   // Alg. 4.4 with q power iterations, then the SVD of B = Q^H M through a QR
   // of B^H and a one-sided Jacobi SVD of the k x k factor).  The test matrix
@@ -416,24 +488,25 @@ struct EngineT final : Engine {
     DT<T> Om({k, ncol}, st);
     counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
     DT<T> Q = apply_M(Om);
-    orth_cm(Q, nrow, k);
+    orth_chol(Q, nrow, k);
     for (int it = 0; it < P.rsvd_power_iters; ++it) {
       DT<T> Z = apply_MH(Q);
-      orth_cm(Z, ncol, k);
+      orth_chol(Z, ncol, k);
       Q = apply_M(Z);
-      orth_cm(Q, nrow, k);
+      orth_chol(Q, nrow, k);
     }
-    DT<T> Z = apply_MH(Q);  // M^H Q = B^H (ncol x k)
-    DT<T> tau = geqrf_cm(Z, ncol, k);
-    DT<T> Rh({k, k}, st);
-    upper_to_rh<T>(Z.p, ncol, k, Rh.p, st);  // Rz^H (k x k, row-major)
-    orgqr_cm(Z, ncol, k, tau);               // Qz
+    // B = Q^H M = Z^H with Z = M^H Q.  With Qz an orthonormal basis of
+    // range(Z), B = (Z^H Qz) Qz^H, so the SVD of the k x k matrix T = Z^H Qz,
+    // T = Ut S Wt^H, gives B = Ut S (Qz Wt)^H.
+    DT<T> Z = apply_MH(Q);  // ncol x k, column-major
+    DT<T> Qz = clone(Z, st);
+    orth_chol(Qz, ncol, k);
+    DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, k)), cm(Qz.p, ncol, k));  // k x k row-major
     DT<T> Ur({k, k}, st), Wr({k, k}, st);
     DT<double> s({k}, st);
-    jacobi_svd<T>(Rh.p, k, Ur.p, s.p, Wr.p, st);  // Rz^H Wr = Ur S
-    // B = Rz^H Qz^H = Ur S (Qz Wr)^H:  U = Q Ur,  V = Qz Wr
+    jacobi_svd<T>(Tm.p, k, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
     DT<T> U = mm_rm(cm(Q.p, nrow, k), rm(Ur.p, k, k));
-    DT<T> V = mm_rm(cm(Z.p, ncol, k), rm(Wr.p, k, k));
+    DT<T> V = mm_rm(cm(Qz.p, ncol, k), rm(Wr.p, k, k));
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
     DT<double> sinv({w}, st);
     truncation(s.p, k, cut, P.inverse_projector_cut, sinv.p, w, d_cut, st);

@@ -740,6 +740,141 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
   }
 }
 
+template <typename T>
+__global__ void add_noise_kernel(T* __restrict__ x, int64_t len, double scale, uint64_t key_re, uint64_t key_im) {
+  for (int64_t n = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; n < len;
+       n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    T v = x[n];
+    if constexpr (is_cplx<T>::value) {
+      v.x += scale * counter_gauss(static_cast<uint64_t>(n), key_re);
+      v.y += scale * counter_gauss(static_cast<uint64_t>(n), key_im);
+    } else {
+      v += scale * counter_gauss(static_cast<uint64_t>(n), key_re);
+    }
+    x[n] = v;
+  }
+}
+
+template <typename T>
+__global__ void sum_partials_kernel(const T* __restrict__ parts, int nparts, int64_t len, T* __restrict__ out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < len;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int p = 0; p < nparts; ++p) {
+      const T v = parts[p * len + i];
+      re += re_of(v);
+      im += im_of(v);
+    }
+    if constexpr (is_cplx<T>::value) {
+      out[i] = make_double2(re, im);
+    } else {
+      out[i] = re;
+    }
+  }
+}
+
+// Cholesky factor and its inverse of an equilibrated (optionally shifted)
+// Gram matrix, one CTA, everything in shared memory.  See chol_rinv().
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ G, int k, double shift,
+                                                         T* __restrict__ R, T* __restrict__ Rinv, int* flag) {
+  extern __shared__ double sm[];
+  const int kk = k * k;
+  double* ar = sm;                          // A' then R' (upper), row-major
+  double* ai = sm + kk;                     // complex only
+  double* xr = sm + (CPLX ? 2 : 1) * kk;    // X = R'^{-1} (upper), row-major
+  double* xi = xr + kk;                     // complex only
+  double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    const double g = re_of(G[static_cast<int64_t>(i) * k + i]);
+    d[i] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kk; idx += blockDim.x) {
+    const int r = idx / k, c = idx % k;
+    const T v = G[idx];
+    ar[idx] = re_of(v) * d[r] * d[c] + ((r == c) ? shift : 0.0);
+    if constexpr (CPLX) ai[idx] = im_of(v) * d[r] * d[c];
+  }
+  __syncthreads();
+  __shared__ double piv;
+  for (int j = 0; j < k; ++j) {
+    if (threadIdx.x == 0) {
+      double s = ar[j * k + j];
+      for (int i = 0; i < j; ++i) {
+        s -= ar[i * k + j] * ar[i * k + j];
+        if constexpr (CPLX) s -= ai[i * k + j] * ai[i * k + j];
+      }
+      if (!(s > 0.0)) {
+        if (flag) atomicExch(flag, 1);
+        s = 1.0;
+      }
+      piv = sqrt(s);
+      ar[j * k + j] = piv;
+      if constexpr (CPLX) ai[j * k + j] = 0.0;
+    }
+    __syncthreads();
+    const double p = piv;
+    for (int c = j + 1 + threadIdx.x; c < k; c += blockDim.x) {
+      // R'_jc = (A'_jc - sum_{i<j} conj(R'_ij) R'_ic) / R'_jj
+      double sr = ar[j * k + c], si = CPLX ? ai[j * k + c] : 0.0;
+      for (int i = 0; i < j; ++i) {
+        const double ur = ar[i * k + j], vr = ar[i * k + c];
+        if constexpr (CPLX) {
+          const double ui = ai[i * k + j], vi = ai[i * k + c];
+          sr -= ur * vr + ui * vi;
+          si -= ur * vi - ui * vr;
+        } else {
+          sr -= ur * vr;
+        }
+      }
+      ar[j * k + c] = sr / p;
+      if constexpr (CPLX) ai[j * k + c] = si / p;
+    }
+    __syncthreads();
+  }
+  // X = R'^{-1}: column c by back substitution (one thread per column)
+  for (int c = threadIdx.x; c < k; c += blockDim.x) {
+    for (int i = c + 1; i < k; ++i) {
+      xr[i * k + c] = 0.0;
+      if constexpr (CPLX) xi[i * k + c] = 0.0;
+    }
+    xr[c * k + c] = 1.0 / ar[c * k + c];
+    if constexpr (CPLX) xi[c * k + c] = 0.0;
+    for (int i = c - 1; i >= 0; --i) {
+      double sr = 0.0, si = 0.0;
+      for (int l = i + 1; l <= c; ++l) {
+        const double rr = ar[i * k + l], xr_ = xr[l * k + c];
+        if constexpr (CPLX) {
+          const double ri = ai[i * k + l], xi_ = xi[l * k + c];
+          sr += rr * xr_ - ri * xi_;
+          si += rr * xi_ + ri * xr_;
+        } else {
+          sr += rr * xr_;
+        }
+      }
+      const double inv = 1.0 / ar[i * k + i];
+      xr[i * k + c] = -sr * inv;
+      if constexpr (CPLX) xi[i * k + c] = -si * inv;
+    }
+  }
+  __syncthreads();
+  // R = R' D^{-1}, Rinv = D X
+  for (int idx = threadIdx.x; idx < kk; idx += blockDim.x) {
+    const int r = idx / k, c = idx % k;
+    const bool up = c >= r;
+    const double rr = up ? ar[idx] / d[c] : 0.0;
+    const double xr_ = up ? xr[idx] * d[r] : 0.0;
+    if constexpr (CPLX) {
+      R[idx] = make_double2(rr, up ? ai[idx] / d[c] : 0.0);
+      Rinv[idx] = make_double2(xr_, up ? xi[idx] * d[r] : 0.0);
+    } else {
+      R[idx] = rr;
+      Rinv[idx] = xr_;
+    }
+  }
+}
+
 __global__ void spectrum_distance_kernel(const double* a, const double* c, int count, int n,
                                          double* sig) {
   const int b = blockIdx.x;
@@ -943,7 +1078,48 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st) {
   count_launch();
 }
 
+template <typename T>
+void add_noise(T* x, int64_t len, double scale, uint64_t stream, cudaStream_t st) {
+  const uint64_t base = 0xD1B54A32D192ED03ull;  // keys disjoint from the rSVD test matrices
+  const uint64_t k_re = base + (2 * stream) * 0xBF58476D1CE4E5B9ull;
+  const uint64_t k_im = base + (2 * stream + 1) * 0xBF58476D1CE4E5B9ull;
+  add_noise_kernel<T><<<num_blocks(len, 256), 256, 0, st>>>(x, len, scale, k_re, k_im);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t st) {
+  sum_partials_kernel<T><<<num_blocks(len, 256), 256, 0, st>>>(parts, nparts, len, out);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* flag, cudaStream_t st) {
+  constexpr bool CPLX = is_cplx<T>::value;
+  if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
+  const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k);
+  static size_t attr_bytes = 0;
+  if (smem > attr_bytes) {
+    TG_CUDA(cudaFuncSetAttribute(chol_rinv_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+    attr_bytes = smem;
+  }
+  // shifted CholeskyQR (Fukaya et al., SIAM J. Sci. Comput. 42 (2020) A477):
+  // s = 11 (m n + n (n+1)) u ||X||_2^2 with ||X||_2^2 <= k for unit columns
+  const double u = 1.1102230246251565e-16;
+  const double s = shift ? 11.0 * (static_cast<double>(n) * k + static_cast<double>(k) * (k + 1)) * u * k : 0.0;
+  ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * static_cast<double>(k) * k * k / 3.0, 0.0);
+  chol_rinv_kernel<T, CPLX><<<1, 256, smem, st>>>(G, static_cast<int>(k), s, R, Rinv, flag);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
 #define TG_INST(T)                                                                               \
+  template void sum_partials<T>(const T*, int, int64_t, T*, cudaStream_t);                       \
+  template void add_noise<T>(T*, int64_t, double, uint64_t, cudaStream_t);                    \
+  template void chol_rinv<T>(const T*, int64_t, int64_t, int, T*, T*, int*, cudaStream_t);       \
   template void counter_normal<T>(T*, int64_t, int64_t, uint64_t, uint64_t, cudaStream_t);       \
   template void upper_to_rh<T>(const T*, int64_t, int64_t, T*, cudaStream_t);                    \
   template int jacobi_svd_max_k<T>();                                                            \

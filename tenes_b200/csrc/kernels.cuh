@@ -88,6 +88,23 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st);
 template <typename T>
 int jacobi_svd_max_k();
 
+// x[i] += scale * N(0,1) (counter-based, key derived from `stream`; complex
+// entries get independent real and imaginary parts)
+template <typename T>
+void add_noise(T* x, int64_t len, double scale, uint64_t stream, cudaStream_t st);
+
+// out[i] = sum_p parts[p*len + i]
+template <typename T>
+void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t st);
+
+// One CTA: from the Gram matrix G = Y^H Y (row-major k x k) of an n-row panel,
+// the Cholesky factor of the column-equilibrated (and, when shift != 0,
+// shifted by shift * 11 (n k + k (k+1)) u) matrix, returned unscaled as
+// R (upper, row-major, Y = Q R) and Rinv = R^{-1} (upper, row-major).
+// flag[0] is set to 1 if a pivot is not positive.  k <= jacobi_svd_max_k<T>().
+template <typename T>
+void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* flag, cudaStream_t st);
+
 // x *= alpha (scalar, real)
 template <typename T>
 void scale(T* x, int64_t n, double alpha, cudaStream_t st);

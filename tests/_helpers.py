@@ -54,3 +54,24 @@ def load_env(genv, oenv):
 
 def rel(a, b):
     return abs(a - b) / max(abs(b), 1e-300)
+
+
+def physical_tensors(lat, D, steps=40, tau=0.05, seed=3, is_complex=False):
+    """Site tensors from `steps` simple-update steps of the spin-1/2 Heisenberg
+    model (oracle), from a seeded random start: spectra decay like a physical
+    state's, unlike i.i.d. random tensors."""
+    from tenes_b200.std_ops import evolution_twosite, heisenberg_bond
+    op = evolution_twosite(heisenberg_bond(1.0), tau)
+    op = op if is_complex else op.real
+    Tn = random_tensors(lat, seed, is_complex)
+    lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
+    p = O.Params()
+    for _ in range(steps):
+        for s in range(lat.N_UNIT):
+            for leg in (2, 1):
+                tg = lat.neighbor(s, leg)
+                a, b, lc = O.simple_update_bond(Tn[s], Tn[tg], lam[s], lam[tg], op, leg, p)
+                lam[s][leg] = lc
+                lam[tg][(leg + 2) % 4] = lc
+                Tn[s], Tn[tg] = a, b
+    return [T / np.max(np.abs(T)) for T in Tn]

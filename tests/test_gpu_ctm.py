@@ -6,7 +6,7 @@ import pytest
 
 from oracle import tenes_oracle as O
 from tests._helpers import (SX, SZ, gpu_env, load_env, make_lattice, oracle_params,
-                            random_tensors, rel)
+                            physical_tensors, random_tensors, rel)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
@@ -120,9 +120,11 @@ def test_complex_ctm_run_matches_oracle():
 def test_rsvd_ctm_run_matches_oracle(is_complex, oversample):
     """rSVD projectors (ctm.cpp:231-266) with the shared counter-based test
     matrix: the GPU rSVD and the oracle's see identical random inputs, so the
-    environments agree to rounding."""
+    environments agree to rounding.  Physical (simple-update) tensors: with
+    i.i.d. random tensors the spectrum is flat at the sketch size and the rSVD
+    iteration amplifies rounding differences."""
     lat = make_lattice(2, 2, 2)
-    Tn = random_tensors(lat, 21, is_complex)
+    Tn = physical_tensors(lat, 2, is_complex=is_complex)
     chi, iters = 8, 4
     kw = dict(Use_RSVD=True, Max_CTM_Iteration=iters, rsvd_power_iters=2)
     if oversample >= 0:
@@ -137,3 +139,24 @@ def test_rsvd_ctm_run_matches_oracle(is_complex, oversample):
             np.testing.assert_allclose(ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i]),
                                        rtol=1e-9, atol=1e-12)
     np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_rsvd_single_move_matches_oracle(is_complex):
+    """One Left_move with rSVD projectors from a full-rank environment."""
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 31, is_complex)
+    chi = 8
+    p_full = oracle_params(chi)
+    oe = O.init_env(Tn, p_full, lat)
+    for _ in range(2):
+        O.sweep(oe, Tn, p_full, lat)
+    p = oracle_params(chi, Use_RSVD=True, rsvd_power_iters=2, rsvd_oversample_abs=4)
+    ge = gpu_env(lat, Tn, chi, is_complex, use_rsvd=True, rsvd_oversample_abs=4, rsvd_power_iters=2)
+    load_env(ge, oe)
+    O.left_move(oe, Tn, 0, p, lat)
+    ge.move(0, 0)
+    for w, name in enumerate(("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(np.abs(ge.get_env(w, i)), np.abs(getattr(oe, name)[i]), rtol=1e-8,
+                                       atol=1e-10, err_msg=f"{name}[{i}]")
