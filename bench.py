@@ -79,9 +79,10 @@ def ctm_params(cfg, projector):
     return CTMParams(chi=chi, max_ctm_iteration=1)
 
 
-def make_env(cfg, seed, device, projector="svd"):
+def make_env(cfg, seed, device, projector="svd", su_steps=None):
     from tenes_b200.env import Environment
-    D, chi, su_steps, _ = CONFIGS[cfg]
+    D, chi, su_default, _ = CONFIGS[cfg]
+    su_steps = su_default if su_steps is None else su_steps
     LX, LY, pd, vd, dirs, noises = lattice_spec(D)
     env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector), False, device=device)
     env.init_tensors(seed, dirs, noises)
@@ -179,7 +180,7 @@ def run_ours(args, rank, world, local_rank):
                                 profile_reset)
     device = local_rank
     torch.cuda.set_device(device)
-    env = make_env(args.config, SEED + rank, device, args.projector)
+    env = make_env(args.config, SEED + rank, device, args.projector, args.su_steps)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
@@ -341,6 +342,8 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--projector", default="svd", choices=["svd", "rsvd"],
                     help="svd: full SVD (reference default); rsvd: k = chi+10, 2 power iterations")
+    ap.add_argument("--su-steps", type=int, default=None,
+                    help="override the simple-update steps that prepare the tensors (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-sweep", action="store_true",
                     help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")

@@ -407,9 +407,9 @@ struct EngineT final : Engine {
     orgqr_cm(Y, n, k, tau);
   }
 
-  // G = Y^H Y (k x k, row-major) of a column-major n x k panel: split-K DMMA
-  // products into partial Gram matrices, then one summation pass.
-  DT<T> gram(const DT<T>& Y, int64_t n, int64_t k) {
+  // Partial Gram matrices G_p = Y_p^H Y_p (k x k, row-major) of row chunks of
+  // a column-major n x k panel (split-K DMMA products); sum_p G_p = Y^H Y.
+  DT<T> gram_parts(const DT<T>& Y, int64_t n, int64_t k, int* nparts_out) {
     const int64_t chunk = std::max<int64_t>(64, (n + 63) / 64);
     const int64_t nfull = n / chunk, rem = n - nfull * chunk;
     const int nparts = static_cast<int>(nfull + (rem > 0 ? 1 : 0));
@@ -439,16 +439,14 @@ struct EngineT final : Engine {
       g.batch = 1;
       gemm<T>(Y.p + nfull * chunk, Y.p + nfull * chunk, parts.p + nfull * k * k, g, st);
     }
-    DT<T> G({k, k}, st);
-    sum_partials<T>(parts.p, nparts, k * k, G.p, st);
-    return G;
+    *nparts_out = nparts;
+    return parts;
   }
 
-  // Shifted CholeskyQR3 with column equilibration (Fukaya, Kannan,
-  // Nakatsukasa, Yamamoto, Yanagisawa 2020): three Gram / Cholesky /
-  // triangular-solve passes, the first shifted, orthonormal to O(u) for
-  // panels with condition number up to ~1/u.  Y (column-major n x k) is
-  // replaced by Q; if R is given, Y = Q R on return (R upper, row-major).
+  // Shifted CholeskyQR with column equilibration (Fukaya, Kannan,
+  // Nakatsukasa, Yamamoto, Yanagisawa 2020): Gram / Cholesky / triangular
+  // solve passes, orthonormal to O(u) for panels with condition number up to
+  // ~1/u.  Y (column-major n x k) is replaced by an orthonormal Q.
   //
   // Only the span of Q is used.  A panel may be rank deficient (zero-padded
   // environment legs give exactly-zero rows), so after the first shifted pass
@@ -459,9 +457,10 @@ struct EngineT final : Engine {
   // ~1e-14, below the rounding of the products that produced the panel.
   void orth_chol(DT<T>& Y, int64_t n, int64_t k) {
     for (int pass = 0; pass < 4; ++pass) {
-      DT<T> G = gram(Y, n, k);
-      DT<T> Rp({k, k}, st), Ri({k, k}, st);
-      chol_rinv<T>(G.p, k, n, pass <= 1 ? 1 : 0, Rp.p, Ri.p, d_flag, st);
+      int nparts = 0;
+      DT<T> G = gram_parts(Y, n, k, &nparts);
+      DT<T> Ri({k, k}, st);
+      chol_rinv<T>(G.p, nparts, k, n, pass <= 1 ? 1 : 0, Ri.p, d_flag, st);
       Y = mm_cm(cm(Y.p, n, k), rm(Ri.p, k, k));
       if (pass == 0) add_noise<T>(Y.p, n * k, 1e-14 / std::sqrt(static_cast<double>(n)), ++noise_stream, st);
     }

@@ -773,104 +773,103 @@ __global__ void sum_partials_kernel(const T* __restrict__ parts, int nparts, int
   }
 }
 
-// Cholesky factor and its inverse of an equilibrated (optionally shifted)
-// Gram matrix, one CTA, everything in shared memory.  See chol_rinv().
+// Inverse Cholesky factor of an equilibrated (optionally shifted) Gram
+// matrix summed from split-K partials; one CTA, everything in shared memory.
+// Right-looking Cholesky (A' = R'^H R', R' upper) and right-looking
+// triangular inverse, each k steps with the trailing work spread over the CTA.
+// See chol_rinv() in kernels.cuh.
 template <typename T, bool CPLX>
-__global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ G, int k, double shift,
-                                                         T* __restrict__ R, T* __restrict__ Rinv, int* flag) {
+__global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ parts, int nparts, int k,
+                                                         double shift, T* __restrict__ Rinv, int* flag) {
   extern __shared__ double sm[];
   const int kk = k * k;
-  double* ar = sm;                          // A' then R' (upper), row-major
+  double* ar = sm;                          // A' -> R' (upper), row-major
   double* ai = sm + kk;                     // complex only
   double* xr = sm + (CPLX ? 2 : 1) * kk;    // X = R'^{-1} (upper), row-major
   double* xi = xr + kk;                     // complex only
-  double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration
-  for (int i = threadIdx.x; i < k; i += blockDim.x) {
-    const double g = re_of(G[static_cast<int64_t>(i) * k + i]);
+  double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration D
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int idx = tid; idx < kk; idx += nt) {
+    double sr = 0.0, si = 0.0;
+    for (int p = 0; p < nparts; ++p) {
+      const T v = parts[static_cast<int64_t>(p) * kk + idx];
+      sr += re_of(v);
+      si += im_of(v);
+    }
+    ar[idx] = sr;
+    if constexpr (CPLX) ai[idx] = si;
+  }
+  __syncthreads();
+  for (int i = tid; i < k; i += nt) {
+    const double g = ar[i * k + i];
     d[i] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < kk; idx += blockDim.x) {
-    const int r = idx / k, c = idx % k;
-    const T v = G[idx];
-    ar[idx] = re_of(v) * d[r] * d[c] + ((r == c) ? shift : 0.0);
-    if constexpr (CPLX) ai[idx] = im_of(v) * d[r] * d[c];
+  for (int idx = tid; idx < kk; idx += nt) {
+    const int r = idx / k, c = idx - r * k;
+    ar[idx] = ar[idx] * d[r] * d[c] + ((r == c) ? shift : 0.0);
+    if constexpr (CPLX) ai[idx] *= d[r] * d[c];
+    xr[idx] = (r == c) ? 1.0 : 0.0;
+    if constexpr (CPLX) xi[idx] = 0.0;
   }
   __syncthreads();
-  __shared__ double piv;
+  // Cholesky, right-looking on the upper triangle
   for (int j = 0; j < k; ++j) {
-    if (threadIdx.x == 0) {
-      double s = ar[j * k + j];
-      for (int i = 0; i < j; ++i) {
-        s -= ar[i * k + j] * ar[i * k + j];
-        if constexpr (CPLX) s -= ai[i * k + j] * ai[i * k + j];
-      }
-      if (!(s > 0.0)) {
-        if (flag) atomicExch(flag, 1);
-        s = 1.0;
-      }
-      piv = sqrt(s);
-      ar[j * k + j] = piv;
-      if constexpr (CPLX) ai[j * k + j] = 0.0;
+    const double a = ar[j * k + j];
+    const double piv = (a > 0.0) ? sqrt(a) : 1.0;
+    if (!(a > 0.0) && tid == 0 && flag) atomicExch(flag, 1);
+    __syncthreads();  // everyone has read A'_jj
+    for (int c = j + tid; c < k; c += nt) {
+      ar[j * k + c] /= piv;
+      if constexpr (CPLX) ai[j * k + c] /= piv;
     }
     __syncthreads();
-    const double p = piv;
-    for (int c = j + 1 + threadIdx.x; c < k; c += blockDim.x) {
-      // R'_jc = (A'_jc - sum_{i<j} conj(R'_ij) R'_ic) / R'_jj
-      double sr = ar[j * k + c], si = CPLX ? ai[j * k + c] : 0.0;
-      for (int i = 0; i < j; ++i) {
-        const double ur = ar[i * k + j], vr = ar[i * k + c];
-        if constexpr (CPLX) {
-          const double ui = ai[i * k + j], vi = ai[i * k + c];
-          sr -= ur * vr + ui * vi;
-          si -= ur * vi - ui * vr;
-        } else {
-          sr -= ur * vr;
-        }
+    const int m = k - j - 1;
+    for (int t = tid; t < m * m; t += nt) {
+      const int r = j + 1 + t / m, c = j + 1 + t % m;
+      if (c < r) continue;
+      // A'_rc -= conj(R'_jr) R'_jc
+      const double ur = ar[j * k + r], vr = ar[j * k + c];
+      if constexpr (CPLX) {
+        const double ui = ai[j * k + r], vi = ai[j * k + c];
+        ar[r * k + c] -= ur * vr + ui * vi;
+        ai[r * k + c] -= ur * vi - ui * vr;
+      } else {
+        ar[r * k + c] -= ur * vr;
       }
-      ar[j * k + c] = sr / p;
-      if constexpr (CPLX) ai[j * k + c] = si / p;
     }
     __syncthreads();
   }
-  // X = R'^{-1}: column c by back substitution (one thread per column)
-  for (int c = threadIdx.x; c < k; c += blockDim.x) {
-    for (int i = c + 1; i < k; ++i) {
-      xr[i * k + c] = 0.0;
-      if constexpr (CPLX) xi[i * k + c] = 0.0;
+  // X = R'^{-1}: for i = k-1 .. 0: X[i,:] /= R'_ii; X[r,:] -= R'_ri X[i,:] (r < i)
+  for (int i = k - 1; i >= 0; --i) {
+    const double inv = 1.0 / ar[i * k + i];
+    for (int c = i + tid; c < k; c += nt) {
+      xr[i * k + c] *= inv;
+      if constexpr (CPLX) xi[i * k + c] *= inv;
     }
-    xr[c * k + c] = 1.0 / ar[c * k + c];
-    if constexpr (CPLX) xi[c * k + c] = 0.0;
-    for (int i = c - 1; i >= 0; --i) {
-      double sr = 0.0, si = 0.0;
-      for (int l = i + 1; l <= c; ++l) {
-        const double rr = ar[i * k + l], xr_ = xr[l * k + c];
-        if constexpr (CPLX) {
-          const double ri = ai[i * k + l], xi_ = xi[l * k + c];
-          sr += rr * xr_ - ri * xi_;
-          si += rr * xi_ + ri * xr_;
-        } else {
-          sr += rr * xr_;
-        }
+    __syncthreads();
+    const int w = k - i;  // columns i .. k-1
+    for (int t = tid; t < i * w; t += nt) {
+      const int r = t / w, c = i + t % w;
+      const double rr = ar[r * k + i], x_r = xr[i * k + c];
+      if constexpr (CPLX) {
+        const double ri = ai[r * k + i], x_i = xi[i * k + c];
+        xr[r * k + c] -= rr * x_r - ri * x_i;
+        xi[r * k + c] -= rr * x_i + ri * x_r;
+      } else {
+        xr[r * k + c] -= rr * x_r;
       }
-      const double inv = 1.0 / ar[i * k + i];
-      xr[i * k + c] = -sr * inv;
-      if constexpr (CPLX) xi[i * k + c] = -si * inv;
     }
+    __syncthreads();
   }
-  __syncthreads();
-  // R = R' D^{-1}, Rinv = D X
-  for (int idx = threadIdx.x; idx < kk; idx += blockDim.x) {
-    const int r = idx / k, c = idx % k;
+  // Rinv = D X (upper)
+  for (int idx = tid; idx < kk; idx += nt) {
+    const int r = idx / k, c = idx - r * k;
     const bool up = c >= r;
-    const double rr = up ? ar[idx] / d[c] : 0.0;
-    const double xr_ = up ? xr[idx] * d[r] : 0.0;
     if constexpr (CPLX) {
-      R[idx] = make_double2(rr, up ? ai[idx] / d[c] : 0.0);
-      Rinv[idx] = make_double2(xr_, up ? xi[idx] * d[r] : 0.0);
+      Rinv[idx] = make_double2(up ? xr[idx] * d[r] : 0.0, up ? xi[idx] * d[r] : 0.0);
     } else {
-      R[idx] = rr;
-      Rinv[idx] = xr_;
+      Rinv[idx] = up ? xr[idx] * d[r] : 0.0;
     }
   }
 }
@@ -1096,7 +1095,7 @@ void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t 
 }
 
 template <typename T>
-void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* flag, cudaStream_t st) {
+void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st) {
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
   const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k);
@@ -1111,7 +1110,7 @@ void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* 
   const double u = 1.1102230246251565e-16;
   const double s = shift ? 11.0 * (static_cast<double>(n) * k + static_cast<double>(k) * (k + 1)) * u * k : 0.0;
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * static_cast<double>(k) * k * k / 3.0, 0.0);
-  chol_rinv_kernel<T, CPLX><<<1, 256, smem, st>>>(G, static_cast<int>(k), s, R, Rinv, flag);
+  chol_rinv_kernel<T, CPLX><<<1, 512, smem, st>>>(parts, nparts, static_cast<int>(k), s, Rinv, flag);
   TG_CHECK_LAUNCH();
   count_launch();
 }
@@ -1119,7 +1118,7 @@ void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* 
 #define TG_INST(T)                                                                               \
   template void sum_partials<T>(const T*, int, int64_t, T*, cudaStream_t);                       \
   template void add_noise<T>(T*, int64_t, double, uint64_t, cudaStream_t);                    \
-  template void chol_rinv<T>(const T*, int64_t, int64_t, int, T*, T*, int*, cudaStream_t);       \
+  template void chol_rinv<T>(const T*, int, int64_t, int64_t, int, T*, int*, cudaStream_t);        \
   template void counter_normal<T>(T*, int64_t, int64_t, uint64_t, uint64_t, cudaStream_t);       \
   template void upper_to_rh<T>(const T*, int64_t, int64_t, T*, cudaStream_t);                    \
   template int jacobi_svd_max_k<T>();                                                            \

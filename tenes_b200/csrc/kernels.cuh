@@ -97,13 +97,14 @@ void add_noise(T* x, int64_t len, double scale, uint64_t stream, cudaStream_t st
 template <typename T>
 void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t st);
 
-// One CTA: from the Gram matrix G = Y^H Y (row-major k x k) of an n-row panel,
-// the Cholesky factor of the column-equilibrated (and, when shift != 0,
-// shifted by shift * 11 (n k + k (k+1)) u) matrix, returned unscaled as
-// R (upper, row-major, Y = Q R) and Rinv = R^{-1} (upper, row-major).
+// One CTA: sums the nparts partial Gram matrices (row-major k x k each) of an
+// n-row panel Y into G = Y^H Y, equilibrates its columns (D = diag(G)^-1/2),
+// adds shift * 11 (n k + k (k+1)) u * k to the diagonal when shift != 0, and
+// writes Rinv = D R'^{-1} (upper, row-major) with D G D (+shift) = R'^H R',
+// so that Y Rinv has orthonormal columns up to the CholeskyQR error.
 // flag[0] is set to 1 if a pivot is not positive.  k <= jacobi_svd_max_k<T>().
 template <typename T>
-void chol_rinv(const T* G, int64_t k, int64_t n, int shift, T* R, T* Rinv, int* flag, cudaStream_t st);
+void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st);
 
 // x *= alpha (scalar, real)
 template <typename T>
