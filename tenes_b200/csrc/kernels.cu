@@ -445,7 +445,7 @@ __global__ void identity_kernel(T* __restrict__ out, int64_t e) {
 // One-sided (Hestenes) Jacobi singular values, one CTA per n x n matrix.
 // Columns live in shared memory (column-major); each warp orthogonalises
 // disjoint column pairs of a round-robin schedule.  Converged when no pair of
-// a sweep needed a rotation (|a_p^H a_q| <= 1e-15 sqrt(|a_p|^2 |a_q|^2)), or
+// a sweep needed a rotation (|a_p^H a_q| <= n u sqrt(|a_p|^2 |a_q|^2)), or
 // after 60 sweeps (the count is reported back).
 // ---------------------------------------------------------------------------
 template <typename T, bool CPLX>
@@ -466,6 +466,7 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int np = n + (n & 1);
+  const double tol = static_cast<double>(n) * 2.220446049250313e-16;
   int sweep = 0;
   for (; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (g == 0.0 || g <= 1e-15 * sqrt(al * be)) continue;
+        if (g == 0.0 || g <= tol * sqrt(al * be)) continue;
         // phase e^{-i phi} with gamma = |gamma| e^{i phi}
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
@@ -633,6 +634,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int np = n + (n & 1);
+  const double tol = static_cast<double>(n) * 2.220446049250313e-16;
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
@@ -667,7 +669,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (g == 0.0 || g <= 1e-15 * sqrt(al * be)) continue;
+        if (g == 0.0 || g <= tol * sqrt(al * be)) continue;
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
         const double zeta = (be - al) / (2.0 * g);
@@ -789,6 +791,7 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
   double* xi = xr + kk;                     // complex only
   double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration D
   const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
   for (int idx = tid; idx < kk; idx += nt) {
     double sr = 0.0, si = 0.0;
     for (int p = 0; p < nparts; ++p) {
@@ -824,18 +827,19 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
       if constexpr (CPLX) ai[j * k + c] /= piv;
     }
     __syncthreads();
-    const int m = k - j - 1;
-    for (int t = tid; t < m * m; t += nt) {
-      const int r = j + 1 + t / m, c = j + 1 + t % m;
-      if (c < r) continue;
-      // A'_rc -= conj(R'_jr) R'_jc
-      const double ur = ar[j * k + r], vr = ar[j * k + c];
-      if constexpr (CPLX) {
-        const double ui = ai[j * k + r], vi = ai[j * k + c];
-        ar[r * k + c] -= ur * vr + ui * vi;
-        ai[r * k + c] -= ur * vi - ui * vr;
-      } else {
-        ar[r * k + c] -= ur * vr;
+    // A'_rc -= conj(R'_jr) R'_jc for j < r <= c: warps over rows, lanes over columns
+    for (int r = j + 1 + warp; r < k; r += nwarp) {
+      const double ur = ar[j * k + r];
+      const double ui = CPLX ? ai[j * k + r] : 0.0;
+      for (int c = r + lane; c < k; c += 32) {
+        const double vr = ar[j * k + c];
+        if constexpr (CPLX) {
+          const double vi = ai[j * k + c];
+          ar[r * k + c] -= ur * vr + ui * vi;
+          ai[r * k + c] -= ur * vi - ui * vr;
+        } else {
+          ar[r * k + c] -= ur * vr;
+        }
       }
     }
     __syncthreads();
@@ -848,16 +852,18 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
       if constexpr (CPLX) xi[i * k + c] *= inv;
     }
     __syncthreads();
-    const int w = k - i;  // columns i .. k-1
-    for (int t = tid; t < i * w; t += nt) {
-      const int r = t / w, c = i + t % w;
-      const double rr = ar[r * k + i], x_r = xr[i * k + c];
-      if constexpr (CPLX) {
-        const double ri = ai[r * k + i], x_i = xi[i * k + c];
-        xr[r * k + c] -= rr * x_r - ri * x_i;
-        xi[r * k + c] -= rr * x_i + ri * x_r;
-      } else {
-        xr[r * k + c] -= rr * x_r;
+    for (int r = warp; r < i; r += nwarp) {  // rows above i, columns i .. k-1
+      const double rr = ar[r * k + i];
+      const double ri = CPLX ? ai[r * k + i] : 0.0;
+      for (int c = i + lane; c < k; c += 32) {
+        const double x_r = xr[i * k + c];
+        if constexpr (CPLX) {
+          const double x_i = xi[i * k + c];
+          xr[r * k + c] -= rr * x_r - ri * x_i;
+          xi[r * k + c] -= rr * x_i + ri * x_r;
+        } else {
+          xr[r * k + c] -= rr * x_r;
+        }
       }
     }
     __syncthreads();
