@@ -458,9 +458,11 @@ struct EngineT final : Engine {
   void orth_chol(DT<T>& Y, int64_t n, int64_t k) {
     for (int pass = 0; pass < 4; ++pass) {
       int nparts = 0;
-      DT<T> G = gram_parts(Y, n, k, &nparts);
+      DT<T> parts = gram_parts(Y, n, k, &nparts);
+      DT<T> G({k, k}, st);
+      sum_partials<T>(parts.p, nparts, k * k, G.p, st);
       DT<T> Ri({k, k}, st);
-      chol_rinv<T>(G.p, nparts, k, n, pass <= 1 ? 1 : 0, Ri.p, d_flag, st);
+      chol_rinv<T>(G.p, 1, k, n, pass <= 1 ? 1 : 0, Ri.p, d_flag, st);
       Y = mm_cm(cm(Y.p, n, k), rm(Ri.p, k, k));
       if (pass == 0) add_noise<T>(Y.p, n * k, 1e-14 / std::sqrt(static_cast<double>(n)), ++noise_stream, st);
     }

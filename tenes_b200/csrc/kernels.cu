@@ -299,6 +299,34 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
       }
 }
 
+// C[m*sCm + n*sCn] (+)= sum_p parts[p][m*N + n]  (split-K epilogue)
+template <typename T>
+__global__ void splitk_reduce_kernel(const T* __restrict__ parts, int nparts, int64_t M, int64_t N, T* C,
+                                     int64_t sCm, int64_t sCn, bool accumulate) {
+  const int64_t len = M * N;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < len;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int p = 0; p < nparts; ++p) {
+      const T v = parts[p * len + i];
+      re += re_of(v);
+      im += im_of(v);
+    }
+    const int64_t m = i / N, n = i - m * N;
+    T* c = C + m * sCm + n * sCn;
+    if constexpr (is_cplx<T>::value) {
+      if (accumulate) {
+        re += c->x;
+        im += c->y;
+      }
+      *c = make_double2(re, im);
+    } else {
+      if (accumulate) re += *c;
+      *c = re;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Permutation: one thread per output element, output-coalesced.
 // ---------------------------------------------------------------------------
@@ -448,6 +476,28 @@ __global__ void identity_kernel(T* __restrict__ out, int64_t e) {
 // a sweep needed a rotation (|a_p^H a_q| <= n u sqrt(|a_p|^2 |a_q|^2)), or
 // after 60 sweeps (the count is reported back).
 // ---------------------------------------------------------------------------
+// sum of |x|^2 over a shared-memory array (re [, im] planes), whole CTA
+template <bool CPLX>
+__device__ double block_sumsq(const double* re, const double* im, int len) {
+  __shared__ double wsum[32];
+  __shared__ double total;
+  double a = 0.0;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) {
+    a += re[i] * re[i];
+    if constexpr (CPLX) a += im[i] * im[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double b = (threadIdx.x < (blockDim.x >> 5)) ? wsum[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+    if (threadIdx.x == 0) total = b;
+  }
+  __syncthreads();
+  return total;
+}
+
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* mats, int n,
                                                                 double* out, int* sweeps_used) {
@@ -467,6 +517,7 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int np = n + (n & 1);
   const double tol = static_cast<double>(n) * 2.220446049250313e-16;
+  const double small2 = tol * tol * block_sumsq<CPLX>(re, im, n * n);  // rounding-noise columns
   int sweep = 0;
   for (; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
@@ -502,7 +553,7 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (g == 0.0 || g <= tol * sqrt(al * be)) continue;
+        if (g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
         // phase e^{-i phi} with gamma = |gamma| e^{i phi}
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
@@ -635,6 +686,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int np = n + (n & 1);
   const double tol = static_cast<double>(n) * 2.220446049250313e-16;
+  const double small2 = tol * tol * block_sumsq<CPLX>(ar, ai, nn);  // rounding-noise columns
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
@@ -669,7 +721,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (g == 0.0 || g <= tol * sqrt(al * be)) continue;
+        if (g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
         const double zeta = (be - al) / (2.0 * g);
@@ -915,13 +967,53 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   dim3 grid(static_cast<unsigned>((d.N + GBN - 1) / GBN), static_cast<unsigned>((d.M + GBM - 1) / GBM),
             static_cast<unsigned>(d.batch));
   if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
-  GemmParams<T> p{A, B, C, d};
   const double macs = static_cast<double>(d.M) * d.N * d.K * d.batch;
   ProfScope ps(PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
                sizeof(T) * static_cast<double>(d.batch) * (d.M * d.K + d.K * d.N + d.M * d.N));
-  gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(p);
+  // Split-K for products whose output tiles cannot fill the 148 SMs (tall-
+  // skinny rSVD panels): K is cut into equal chunks written to partial
+  // buffers, then summed into C.
+  const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
+  int64_t split = 1;
+  if (d.batch == 1 && tiles < 148 && d.K >= 1024)
+    split = std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 512);
+  if (split <= 1) {
+    GemmParams<T> p{A, B, C, d};
+    gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(p);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    return;
+  }
+  const int64_t chunk = (d.K / split + GBK - 1) / GBK * GBK;  // multiple of the k tile
+  const int64_t nfull = d.K / chunk, rem = d.K - nfull * chunk;
+  const int64_t nparts = nfull + (rem > 0 ? 1 : 0);
+  void* buf = nullptr;
+  TG_CUDA(cudaMallocAsync(&buf, sizeof(T) * nparts * d.M * d.N, st));
+  T* parts = static_cast<T*>(buf);
+  GemmDesc g = d;
+  g.sCm = d.N;
+  g.sCn = 1;
+  g.accumulate = false;
+  g.K = chunk;
+  g.batch = nfull;
+  g.bA = chunk * d.sAk;
+  g.bB = chunk * d.sBk;
+  g.bC = d.M * d.N;
+  dim3 g1(grid.x, grid.y, static_cast<unsigned>(nfull));
+  gemm_kernel<T, CPLX><<<g1, 128, smem, st>>>(GemmParams<T>{A, B, parts, g});
   TG_CHECK_LAUNCH();
-  count_launch();
+  if (rem > 0) {
+    g.K = rem;
+    g.batch = 1;
+    gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(
+        GemmParams<T>{A + nfull * chunk * d.sAk, B + nfull * chunk * d.sBk, parts + nfull * d.M * d.N, g});
+    TG_CHECK_LAUNCH();
+  }
+  splitk_reduce_kernel<T><<<num_blocks(d.M * d.N, 256), 256, 0, st>>>(parts, static_cast<int>(nparts), d.M, d.N,
+                                                                       C, d.sCm, d.sCn, d.accumulate);
+  TG_CHECK_LAUNCH();
+  count_launch(rem > 0 ? 3 : 2);
+  TG_CUDA(cudaFreeAsync(buf, st));
 }
 
 template <typename T>
