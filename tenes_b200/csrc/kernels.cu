@@ -687,47 +687,57 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
   const int np = n + (n & 1);
   const double tol = static_cast<double>(n) * 2.220446049250313e-16;
   const double small2 = tol * tol * block_sumsq<CPLX>(ar, ai, nn);  // rounding-noise columns
+  // each column pair is handled by a group of 8 lanes (4 pairs per warp)
+  const int grp = lane >> 3, gl = lane & 7;
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
     for (int rnd = 0; rnd < np - 1; ++rnd) {
-      for (int pr = warp; pr < np / 2; pr += nw) {
+      for (int base = warp * 4; base < np / 2; base += nw * 4) {
+        const int pr = base + grp;
         auto player = [&](int kk) { return kk == 0 ? 0 : ((kk - 1 + rnd) % (np - 1)) + 1; };
-        int p = player(pr), q = player(np - 1 - pr);
-        if (p >= n || q >= n) continue;
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
-        double al = 0, be = 0, gr = 0, gi = 0;
-        for (int r = lane; r < n; r += 32) {
-          const double pr_ = ar[p * n + r], qr_ = ar[q * n + r];
-          al += pr_ * pr_;
-          be += qr_ * qr_;
-          gr += pr_ * qr_;
-          if constexpr (CPLX) {
-            const double pi_ = ai[p * n + r], qi_ = ai[q * n + r];
-            al += pi_ * pi_;
-            be += qi_ * qi_;
-            gr += pi_ * qi_;
-            gi += pr_ * qi_ - pi_ * qr_;
+        int p = 0, q = 0;
+        bool valid = pr < np / 2;
+        if (valid) {
+          p = player(pr);
+          q = player(np - 1 - pr);
+          valid = p < n && q < n;
+          if (p > q) {
+            const int t = p;
+            p = q;
+            q = t;
           }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          gr += __shfl_xor_sync(0xffffffffu, gr, o);
-          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o);
+        double al = 0, be = 0, gr = 0, gi = 0;
+        if (valid) {
+          for (int r = gl; r < n; r += 8) {
+            const double pr_ = ar[p * n + r], qr_ = ar[q * n + r];
+            al += pr_ * pr_;
+            be += qr_ * qr_;
+            gr += pr_ * qr_;
+            if constexpr (CPLX) {
+              const double pi_ = ai[p * n + r], qi_ = ai[q * n + r];
+              al += pi_ * pi_;
+              be += qi_ * qi_;
+              gr += pi_ * qi_;
+              gi += pr_ * qi_ - pi_ * qr_;
+            }
+          }
+        }
+        for (int o = 4; o > 0; o >>= 1) {  // reduce within the 8-lane group
+          al += __shfl_xor_sync(0xffffffffu, al, o, 8);
+          be += __shfl_xor_sync(0xffffffffu, be, o, 8);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o, 8);
+          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o, 8);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
+        if (!valid || g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
         const double zeta = (be - al) / (2.0 * g);
         const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-        for (int r = lane; r < n; r += 32) {
+        for (int r = gl; r < n; r += 8) {
           {
             const double xpr = ar[p * n + r], xqr = ar[q * n + r];
             const double xpi = CPLX ? ai[p * n + r] : 0.0, xqi = CPLX ? ai[q * n + r] : 0.0;
@@ -751,7 +761,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
             }
           }
         }
-        if (lane == 0) rotated = 1;
+        if (gl == 0) rotated = 1;
       }
       __syncthreads();
     }
