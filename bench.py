@@ -199,6 +199,9 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(device)
     clocks = Clocks(device)
     clocks.start()
+    if args.profile_timed:
+        profile_enable(True)
+        profile_reset()
     l0 = kernel_launch_count()
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
@@ -213,6 +216,11 @@ def run_ours(args, rank, world, local_rank):
     launches = kernel_launch_count() - l0
     torch.cuda.synchronize(device)
     ck = clocks.stop()
+    timed_breakdown = None
+    if args.profile_timed:
+        timed_breakdown = {PROFILE_KINDS[k]: round(profile_query(k)[1] / args.steps, 3)
+                           for k in range(len(PROFILE_KINDS))}
+        profile_enable(False)
     total_ms = sum(times)
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device=device)
@@ -268,7 +276,8 @@ def run_ours(args, rank, world, local_rank):
                 "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}}
     env.close()
     return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roofline,
-            "clocks": ck, "gpu_launches": launches}
+            "clocks": ck, "gpu_launches": launches, "sweep_ms": [round(t, 3) for t in times],
+            "timed_breakdown_ms": timed_breakdown}
 
 
 # -------------------------------------------------------- CPU oracle (reference arm)
@@ -345,6 +354,8 @@ def main():
     ap.add_argument("--su-steps", type=int, default=None,
                     help="override the simple-update steps that prepare the tensors (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-timed", action="store_true",
+                    help="CUDA-event profile of the library kernels during the timed sweeps (diagnostic)")
     ap.add_argument("--profile-sweep", action="store_true",
                     help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")
     args = ap.parse_args()
@@ -386,7 +397,9 @@ def main():
                                          else "rSVD k=chi+10, q=2"), "parallelism": f"replicas{world}",
                            "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
-                "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]}
+                "clocks": res["clocks"], "gpu_launches": res["gpu_launches"], "sweep_ms": res["sweep_ms"]}
+        if res["timed_breakdown_ms"] is not None:
+            line["timed_breakdown_ms"] = res["timed_breakdown_ms"]
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
