@@ -69,22 +69,23 @@ def heisenberg_op():
 
 
 # ------------------------------------------------------------------ our arm
-def ctm_params(cfg, projector):
+def ctm_params(cfg, projector, precision="fp64"):
     from tenes_b200.env import CTMParams
     D, chi, _, _ = CONFIGS[cfg]
+    mixed = precision == "mixed"
     if projector == "rsvd":
         # rSVD projectors, oversampling chi+10, 2 power iterations
         return CTMParams(chi=chi, max_ctm_iteration=1, use_rsvd=True, rsvd_oversample_abs=10,
-                         rsvd_power_iters=2)
-    return CTMParams(chi=chi, max_ctm_iteration=1)
+                         rsvd_power_iters=2, mixed=mixed)
+    return CTMParams(chi=chi, max_ctm_iteration=1, mixed=mixed)
 
 
-def make_env(cfg, seed, device, projector="svd", su_steps=None):
+def make_env(cfg, seed, device, projector="svd", su_steps=None, precision="fp64"):
     from tenes_b200.env import Environment
     D, chi, su_default, _ = CONFIGS[cfg]
     su_steps = su_default if su_steps is None else su_steps
     LX, LY, pd, vd, dirs, noises = lattice_spec(D)
-    env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector), False, device=device)
+    env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector, precision), False, device=device)
     env.init_tensors(seed, dirs, noises)
     op = heisenberg_op()
     t0 = time.perf_counter()
@@ -180,7 +181,7 @@ def run_ours(args, rank, world, local_rank):
                                 profile_reset)
     device = local_rank
     torch.cuda.set_device(device)
-    env = make_env(args.config, SEED + rank, device, args.projector, args.su_steps)
+    env = make_env(args.config, SEED + rank, device, args.projector, args.su_steps, args.precision)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
@@ -351,6 +352,8 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--projector", default="svd", choices=["svd", "rsvd"],
                     help="svd: full SVD (reference default); rsvd: k = chi+10, 2 power iterations")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: 3xTF32 tensor-core contractions, FP64 projector algebra")
     ap.add_argument("--su-steps", type=int, default=None,
                     help="override the simple-update steps that prepare the tensors (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -390,9 +393,10 @@ def main():
                              "moves per sweep"}
         line = {"metric": "ctmrg_sweeps_per_s", "value": res["value"], "unit": "sweeps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64",
                 "data": "synthetic",
-                "config": {"workload": name, "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
+                "config": {"workload": name, "precision": args.precision, "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
                            "projector": ("full SVD (reference default)" if args.projector == "svd"
                                          else "rSVD k=chi+10, q=2"), "parallelism": f"replicas{world}",
                            "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},

@@ -68,6 +68,10 @@ typedef struct tg_params {
   int rsvd_power_iters;             /* power iterations of the rSVD range finder (2) */
   uint64_t rsvd_seed;               /* key of the counter-based rSVD test matrix */
   double inverse_lambda_cut;        /* simple_update.lambda_cutoff (1e-12) */
+  int mixed;                        /* 1: CTMRG absorption contractions and rSVD panel products as
+                                       3xTF32 tensor-core products (FP64 tile accumulation); the
+                                       orthonormalisation, SVDs and observables stay FP64.  Real
+                                       tensors only.  0 (default): everything FP64. */
 } tg_params;
 
 /* Fill *p with the reference defaults. */

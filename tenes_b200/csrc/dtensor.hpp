@@ -99,7 +99,7 @@ DT<T> reshape(const DT<T>& a, const Shape& s) {
 template <typename T>
 DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
                 const std::vector<int>& axB, cudaStream_t st, bool conjA = false,
-                bool conjB = false) {
+                bool conjB = false, int prec = 0) {
   if (axA.size() != axB.size()) fail(TG_E_INPUT, "tensordot: axes length mismatch");
   std::vector<int> freeA, freeB;
   for (int i = 0; i < A.rank(); ++i)
@@ -128,6 +128,7 @@ DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
   g.conjA = conjA;
   g.conjB = conjB;
   g.accumulate = false;
+  g.prec = prec;
   // A as (M, K) or (K, M)
   DT<T> Ause = A;
   std::vector<int> pa(freeA);

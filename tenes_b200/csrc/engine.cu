@@ -75,6 +75,8 @@ struct EngineT final : Engine {
     lat.check_dims();
     if (P.chi < 1) fail(TG_E_INPUT, "chi must be positive");
     if (P.rsvd_oversampling_factor < 1.0) fail(TG_E_INPUT, "rsvd_oversampling_factor must be >= 1.0");
+    if (P.mixed && CPLX) fail(TG_E_INPUT, "mixed precision is available for real tensors only");
+    abs_prec = P.mixed ? 1 : 0;
     TG_CUDA(cudaSetDevice(dev));
     TG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     cudaMemPool_t pool;
@@ -138,8 +140,20 @@ struct EngineT final : Engine {
   }
 
   // ---------------------------------------------------------------- helpers
+  // precision of the contraction products issued now: the absorption
+  // contractions of a move run in `abs_prec` (3xTF32 when params.mixed),
+  // everything else (initialisation, measurements, simple update) in FP64
+  int cur_prec = 0;
+  int abs_prec = 0;
+  struct PrecScope {
+    EngineT* e;
+    int saved;
+    PrecScope(EngineT* e_, int p) : e(e_), saved(e_->cur_prec) { e->cur_prec = p; }
+    ~PrecScope() { e->cur_prec = saved; }
+  };
+
   DT<T> td(const DT<T>& a, const DT<T>& b, const V& x, const V& y, bool ca = false, bool cb = false) {
-    return tensordot<T>(a, b, x, y, st, ca, cb);
+    return tensordot<T>(a, b, x, y, st, ca, cb, cur_prec);
   }
   DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
   void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.size(), d_max, st); }
@@ -349,6 +363,7 @@ struct EngineT final : Engine {
     g.conjA = A.conj;
     g.conjB = B.conj;
     g.accumulate = false;
+    g.prec = cur_prec;
     gemm<T>(A.p, B.p, C, g, st);
   }
   DT<T> mm_rm(const MV& A, const MV& B) {  // row-major result
@@ -456,6 +471,7 @@ struct EngineT final : Engine {
   // two plain passes orthonormalise.  The perturbation moves the span by
   // ~1e-14, below the rounding of the products that produced the panel.
   void orth_chol(DT<T>& Y, int64_t n, int64_t k) {
+    PrecScope fp64(this, 0);
     for (int pass = 0; pass < 4; ++pass) {
       int nparts = 0;
       DT<T> parts = gram_parts(Y, n, k, &nparts);
@@ -502,6 +518,7 @@ struct EngineT final : Engine {
     DT<T> Z = apply_MH(Q);  // ncol x k, column-major
     DT<T> Qz = clone(Z, st);
     orth_chol(Qz, ncol, k);
+    PrecScope fp64(this, 0);  // the core SVD and its basis changes stay FP64
     DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, k)), cm(Qz.p, ncol, k));  // k x k row-major
     DT<T> Ur({k, k}, st), Wr({k, k}, st);
     DT<double> s({k}, st);
@@ -781,6 +798,7 @@ struct EngineT final : Engine {
 
   void ctm_move(int dir, int line) override {
     require_env();
+    PrecScope prec(this, abs_prec);
     const int L = (dir <= 1) ? lat.LX_noskew : lat.LY_noskew;
     if (line < 0 || line >= L) fail(TG_E_INPUT, "move line out of range");
     switch (dir) {
@@ -794,6 +812,7 @@ struct EngineT final : Engine {
   }
 
   void sweep_impl() {
+    PrecScope prec(this, abs_prec);
     const int LX = lat.LX_noskew, LY = lat.LY_noskew;
     for (int ix = 0; ix < LX; ++ix) left_move(ix);
     for (int ix = 0; ix > -LX; --ix) right_move((ix + 1 + LX) % LX);

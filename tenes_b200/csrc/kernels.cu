@@ -299,6 +299,153 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
       }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed precision: 3xTF32 product on the TF32 tensor pipe (mma.sync
+// m16n8k8).  Each FP64 operand a is rounded to FP32 and split as
+// a = hi + lo with hi = tf32(a), lo = tf32(a - hi); a*b ~ hi*hi + hi*lo +
+// lo*hi.  Products accumulate in FP32 inside one 16-deep k tile and the tile
+// sums are added into FP64 accumulators, so the accumulation error does not
+// grow with K.  64 x 64 x 16 CTA tile, 4 warps of 32 x 32.
+// ---------------------------------------------------------------------------
+constexpr int XBM = 64, XBN = 64, XBK = 16, XLD = 64 + 8;  // XLD: conflict-free fragment loads
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) gemm_tf32x3_kernel(GemmParams<double> p) {
+  __shared__ uint32_t sA[2][2][XBK * XLD];  // [stage][hi/lo][k][m]
+  __shared__ uint32_t sB[2][2][XBK * XLD];  // [stage][hi/lo][k][n]
+  const GemmDesc& d = p.d;
+  const int64_t bz = blockIdx.z;
+  const double* A = p.A + bz * d.bA;
+  const double* B = p.B + bz * d.bB;
+  double* C = p.C + bz * d.bC;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * XBM;
+  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * XBN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int gid = lane >> 2, tig = lane & 3;
+  const bool a_kc = (d.sAk == 1), b_nc = (d.sBn == 1);
+  double ra[8], rb[8];
+  auto load = [&](int64_t k0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
+      int mm, kk, nn, kb;
+      if (a_kc) { kk = idx % XBK; mm = idx / XBK; } else { mm = idx % XBM; kk = idx / XBM; }
+      if (b_nc) { nn = idx % XBN; kb = idx / XBN; } else { kb = idx % XBK; nn = idx / XBK; }
+      const int64_t gm = m0 + mm, gk = k0 + kk, gn = n0 + nn, gkb = k0 + kb;
+      ra[i] = (gm < d.M && gk < d.K) ? A[gm * d.sAm + gk * d.sAk] : 0.0;
+      rb[i] = (gn < d.N && gkb < d.K) ? B[gkb * d.sBk + gn * d.sBn] : 0.0;
+    }
+  };
+  auto store = [&](int s) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
+      int mm, kk, nn, kb;
+      if (a_kc) { kk = idx % XBK; mm = idx / XBK; } else { mm = idx % XBM; kk = idx / XBM; }
+      if (b_nc) { nn = idx % XBN; kb = idx / XBN; } else { kb = idx % XBK; nn = idx / XBK; }
+      const float fa = static_cast<float>(ra[i]);
+      const uint32_t ha = to_tf32(fa);
+      sA[s][0][kk * XLD + mm] = ha;
+      sA[s][1][kk * XLD + mm] = to_tf32(fa - __uint_as_float(ha));
+      const float fb = static_cast<float>(rb[i]);
+      const uint32_t hb = to_tf32(fb);
+      sB[s][0][kb * XLD + nn] = hb;
+      sB[s][1][kb * XLD + nn] = to_tf32(fb - __uint_as_float(hb));
+    }
+  };
+  double acc64[2][4][4];
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc64[i][j][r] = 0.0;
+  const int64_t nk = (d.K + XBK - 1) / XBK;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    const int s = static_cast<int>(kt & 1);
+    if (kt + 1 < nk) load((kt + 1) * XBK);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+#pragma unroll
+    for (int k8 = 0; k8 < XBK; k8 += 8) {
+      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int mb = wm + i * 16 + gid;
+        const int o0 = (k8 + tig) * XLD + mb, o1 = (k8 + tig + 4) * XLD + mb;
+        ah[i][0] = sA[s][0][o0];
+        ah[i][1] = sA[s][0][o0 + 8];
+        ah[i][2] = sA[s][0][o1];
+        ah[i][3] = sA[s][0][o1 + 8];
+        al[i][0] = sA[s][1][o0];
+        al[i][1] = sA[s][1][o0 + 8];
+        al[i][2] = sA[s][1][o1];
+        al[i][3] = sA[s][1][o1 + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int nb = wn + j * 8 + gid;
+        bh[j][0] = sB[s][0][(k8 + tig) * XLD + nb];
+        bh[j][1] = sB[s][0][(k8 + tig + 4) * XLD + nb];
+        bl[j][0] = sB[s][1][(k8 + tig) * XLD + nb];
+        bl[j][1] = sB[s][1][(k8 + tig + 4) * XLD + nb];
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma_tf32(acc[i][j], al[i], bh[j]);
+          mma_tf32(acc[i][j], ah[i], bl[j]);
+          mma_tf32(acc[i][j], ah[i], bh[j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc64[i][j][r] += static_cast<double>(acc[i][j][r]);
+    if (kt + 1 < nk) store(s ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int64_t gm = m0 + wm + i * 16 + gid + ((r & 2) ? 8 : 0);
+        const int64_t gn = n0 + wn + j * 8 + 2 * tig + (r & 1);
+        if (gm < d.M && gn < d.N) {
+          double* c = C + gm * d.sCm + gn * d.sCn;
+          const double v = acc64[i][j][r];
+          *c = d.accumulate ? *c + v : v;
+        }
+      }
+}
+
 // C[m*sCm + n*sCn] (+)= sum_p parts[p][m*N + n]  (split-K epilogue)
 template <typename T>
 __global__ void splitk_reduce_kernel(const T* __restrict__ parts, int nparts, int64_t M, int64_t N, T* C,
@@ -983,13 +1130,22 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   // Split-K for products whose output tiles cannot fill the 148 SMs (tall-
   // skinny rSVD panels): K is cut into equal chunks written to partial
   // buffers, then summed into C.
+  if (CPLX && d.prec != 0) fail(TG_E_INPUT, "gemm: the 3xTF32 product is real-only");
+  auto launch = [&](dim3 gr, const GemmParams<T>& gp) {
+    if constexpr (!CPLX) {
+      if (gp.d.prec == 1) {
+        gemm_tf32x3_kernel<<<gr, 128, 0, st>>>(gp);
+        return;
+      }
+    }
+    gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp);
+  };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
   if (d.batch == 1 && tiles < 148 && d.K >= 1024)
     split = std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 512);
   if (split <= 1) {
-    GemmParams<T> p{A, B, C, d};
-    gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(p);
+    launch(grid, GemmParams<T>{A, B, C, d});
     TG_CHECK_LAUNCH();
     count_launch();
     return;
@@ -1010,13 +1166,12 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   g.bB = chunk * d.sBk;
   g.bC = d.M * d.N;
   dim3 g1(grid.x, grid.y, static_cast<unsigned>(nfull));
-  gemm_kernel<T, CPLX><<<g1, 128, smem, st>>>(GemmParams<T>{A, B, parts, g});
+  launch(g1, GemmParams<T>{A, B, parts, g});
   TG_CHECK_LAUNCH();
   if (rem > 0) {
     g.K = rem;
     g.batch = 1;
-    gemm_kernel<T, CPLX><<<grid, 128, smem, st>>>(
-        GemmParams<T>{A + nfull * chunk * d.sAk, B + nfull * chunk * d.sBk, parts + nfull * d.M * d.N, g});
+    launch(grid, GemmParams<T>{A + nfull * chunk * d.sAk, B + nfull * chunk * d.sBk, parts + nfull * d.M * d.N, g});
     TG_CHECK_LAUNCH();
   }
   splitk_reduce_kernel<T><<<num_blocks(d.M * d.N, 256), 256, 0, st>>>(parts, static_cast<int>(nparts), d.M, d.N,

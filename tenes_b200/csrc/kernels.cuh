@@ -13,6 +13,7 @@ struct GemmDesc {
   int64_t sAm, sAk, sBk, sBn, sCm, sCn;
   int64_t bA, bB, bC;
   bool conjA, conjB, accumulate;
+  int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 tensor cores with FP64 tile accumulation (real only)
 };
 
 template <typename T>

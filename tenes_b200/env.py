@@ -42,6 +42,7 @@ class CTMParams:
     rsvd_power_iters: int = 2
     rsvd_seed: int = 0
     inverse_lambda_cut: float = 1e-12
+    mixed: bool = False
 
     def to_c(self) -> _lib.Params:
         p = _lib.Params()
