@@ -172,6 +172,12 @@ tg_status tg_profile_enable(int on);
 tg_status tg_profile_reset(void);
 tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes);
 
+/* Microbenchmark of the library's contraction kernel: average device time of
+ * one M x N x K real product (prec 0: FP64 DMMA, 1: 3xTF32), B row-major
+ * (layout 0) or column-major (layout 1).  Allocates its own buffers; not part
+ * of the CTMRG path. */
+tg_status tg_bench_gemm(int64_t M, int64_t N, int64_t K, int layout, int prec, int iters, double* avg_ms);
+
 /* Allocation-free corner spectra.  No counterpart in the reference: it exists
  * for callers that must not allocate device memory where they need the
  * spectra -- code that runs under a fixed device-memory budget, hosts that

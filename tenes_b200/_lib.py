@@ -27,6 +27,7 @@ EXPORTED = [
     "tg_ctm_run", "tg_corner_spectrum", "tg_measure_onesite", "tg_measure_bond_op12",
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
+    "tg_bench_gemm",
 ]
 
 
@@ -94,6 +95,7 @@ def load() -> C.CDLL:
         "tg_profile_reset": (C.c_int, []),
         "tg_profile_query": (C.c_int, [C.c_int, P(C.c_uint64), dp, dp, dp]),
         "tg_corner_spectra_noalloc": (C.c_int, [P(vp), C.c_int, C.c_int, C.c_int, dp, vp]),
+        "tg_bench_gemm": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "engine.hpp"
+#include "kernels.cuh"
 #include "tenes_gpu.h"
 
 struct tg_ctx {
@@ -213,3 +214,56 @@ tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Microbenchmark of the contraction kernel on one product shape (device
+// buffers allocated and freed here; not used by the CTMRG path).
+extern "C" tg_status tg_bench_gemm(int64_t M, int64_t N, int64_t K, int layout, int prec, int iters,
+                                   double* avg_ms) {
+  return guard([&] {
+    if (M < 1 || N < 1 || K < 1 || iters < 1 || !avg_ms) tg::fail(TG_E_INPUT, "bad gemm benchmark arguments");
+    cudaStream_t st;
+    TG_CUDA(cudaStreamCreate(&st));
+    double *A = nullptr, *B = nullptr, *C = nullptr;
+    TG_CUDA(cudaMalloc(&A, sizeof(double) * M * K));
+    TG_CUDA(cudaMalloc(&B, sizeof(double) * K * N));
+    TG_CUDA(cudaMalloc(&C, sizeof(double) * M * N));
+    TG_CUDA(cudaMemset(A, 0, sizeof(double) * M * K));
+    TG_CUDA(cudaMemset(B, 0, sizeof(double) * K * N));
+    tg::GemmDesc g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.batch = 1;
+    // layout 0: A row-major (M,K), B row-major (K,N); 1: B column-major (panel products)
+    g.sAm = K;
+    g.sAk = 1;
+    if (layout == 1) {
+      g.sBk = 1;
+      g.sBn = K;
+    } else {
+      g.sBk = N;
+      g.sBn = 1;
+    }
+    g.sCm = N;
+    g.sCn = 1;
+    g.prec = prec;
+    tg::gemm<double>(A, B, C, g, st);
+    cudaEvent_t e0, e1;
+    TG_CUDA(cudaEventCreate(&e0));
+    TG_CUDA(cudaEventCreate(&e1));
+    TG_CUDA(cudaEventRecord(e0, st));
+    for (int i = 0; i < iters; ++i) tg::gemm<double>(A, B, C, g, st);
+    TG_CUDA(cudaEventRecord(e1, st));
+    TG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    TG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *avg_ms = ms / iters;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(A);
+    cudaFree(B);
+    cudaFree(C);
+    cudaStreamDestroy(st);
+  });
+}
