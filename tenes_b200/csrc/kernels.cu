@@ -300,154 +300,6 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
 }
 
 // ---------------------------------------------------------------------------
-// Pipelined FP64 / complex128 product: the same 64 x 64 x 16 CTA tile and
-// DMMA m8n8k4 warp tiles as gemm_kernel, but the global->shared copies are
-// asynchronous (cp.async, zero-filled outside the matrix) with PSTAGES tiles
-// in flight, so the load latency of small-K / skinny products is hidden.
-// Conjugation is applied when fragments are read.
-// ---------------------------------------------------------------------------
-constexpr int PSTAGES = 4;
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0));
-}
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-template <typename T, bool CPLX>
-__global__ void __launch_bounds__(128) gemm_pipe_kernel(GemmParams<T> p) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* As = reinterpret_cast<T*>(smraw);                 // [PSTAGES][GBK][GLD]
-  T* Bs = As + PSTAGES * GBK * GLD;                     // [PSTAGES][GBK][GLD]
-  const GemmDesc& d = p.d;
-  const int64_t bz = blockIdx.z;
-  const T* A = p.A + bz * d.bA;
-  const T* B = p.B + bz * d.bB;
-  T* C = p.C + bz * d.bC;
-  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * GBM;
-  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * GBN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  const bool a_kc = (d.sAk == 1), b_nc = (d.sBn == 1);
-  const int64_t nk = (d.K + GBK - 1) / GBK;
-
-  auto issue = [&](int stage, int64_t kt) {
-    T* as = As + stage * GBK * GLD;
-    T* bs = Bs + stage * GBK * GLD;
-    const int64_t k0 = kt * GBK;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int idx = tid + i * 128;
-      int mm, kk, nn, kb;
-      if (a_kc) { kk = idx % GBK; mm = idx / GBK; } else { mm = idx % GBM; kk = idx / GBM; }
-      if (b_nc) { nn = idx % GBN; kb = idx / GBN; } else { kb = idx % GBK; nn = idx / GBK; }
-      const int64_t gm = m0 + mm, gk = k0 + kk, gn = n0 + nn, gkb = k0 + kb;
-      const bool va = gm < d.M && gk < d.K, vb = gn < d.N && gkb < d.K;
-      const T* ga = va ? A + gm * d.sAm + gk * d.sAk : A;
-      const T* gb = vb ? B + gkb * d.sBk + gn * d.sBn : B;
-      if constexpr (CPLX) {
-        cp_async16(as + kk * GLD + mm, ga, va);
-        cp_async16(bs + kb * GLD + nn, gb, vb);
-      } else {
-        cp_async8(as + kk * GLD + mm, ga, va);
-        cp_async8(bs + kb * GLD + nn, gb, vb);
-      }
-    }
-  };
-
-  double acc_r[4][4][2];
-  double acc_i[CPLX ? 4 : 1][CPLX ? 4 : 1][2];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc_r[i][j][0] = acc_r[i][j][1] = 0.0;
-  if constexpr (CPLX) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc_i[i][j][0] = acc_i[i][j][1] = 0.0;
-  }
-  const double sa = d.conjA ? -1.0 : 1.0, sb = d.conjB ? -1.0 : 1.0;
-
-#pragma unroll
-  for (int s = 0; s < PSTAGES - 1; ++s) {
-    if (s < nk) issue(s, s);
-    cp_async_commit();
-  }
-  for (int64_t kt = 0; kt < nk; ++kt) {
-    cp_async_wait<PSTAGES - 2>();
-    __syncthreads();
-    const int stage = static_cast<int>(kt % PSTAGES);
-    const T* as = As + stage * GBK * GLD;
-    const T* bs = Bs + stage * GBK * GLD;
-#pragma unroll
-    for (int k4 = 0; k4 < GBK; k4 += 4) {
-      const int kr = k4 + (lane & 3);
-      double a_r[4], b_r[4], a_i[CPLX ? 4 : 1], b_i[CPLX ? 4 : 1];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const T va = as[kr * GLD + wm + i * 8 + (lane >> 2)];
-        const T vb = bs[kr * GLD + wn + i * 8 + (lane >> 2)];
-        a_r[i] = re_of(va);
-        b_r[i] = re_of(vb);
-        if constexpr (CPLX) {
-          a_i[i] = sa * im_of(va);
-          b_i[i] = sb * im_of(vb);
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          dmma(acc_r[i][j][0], acc_r[i][j][1], a_r[i], b_r[j]);
-          if constexpr (CPLX) {
-            dmma(acc_r[i][j][0], acc_r[i][j][1], -a_i[i], b_i[j]);
-            dmma(acc_i[i][j][0], acc_i[i][j][1], a_r[i], b_i[j]);
-            dmma(acc_i[i][j][0], acc_i[i][j][1], a_i[i], b_r[j]);
-          }
-        }
-    }
-    const int64_t next = kt + PSTAGES - 1;
-    if (next < nk) issue(static_cast<int>(next % PSTAGES), next);
-    cp_async_commit();
-  }
-  cp_async_wait<0>();
-
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int64_t gm = m0 + wm + i * 8 + (lane >> 2);
-        const int64_t gn = n0 + wn + j * 8 + 2 * (lane & 3) + h;
-        if (gm < d.M && gn < d.N) {
-          T* c = C + gm * d.sCm + gn * d.sCn;
-          if constexpr (CPLX) {
-            cplx v = make_double2(acc_r[i][j][h], acc_i[i][j][h]);
-            if (d.accumulate) {
-              v.x += c->x;
-              v.y += c->y;
-            }
-            *c = v;
-          } else {
-            double v = acc_r[i][j][h];
-            if (d.accumulate) v += *c;
-            *c = v;
-          }
-        }
-      }
-}
-
-// ---------------------------------------------------------------------------
 // Mixed precision: 3xTF32 product on the TF32 tensor pipe (mma.sync
 // m16n8k8).  Each FP64 operand a is rounded to FP32 and split as
 // a = hi + lo with hi = tf32(a), lo = tf32(a - hi); a*b ~ hi*hi + hi*lo +
@@ -1279,14 +1131,6 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   // skinny rSVD panels): K is cut into equal chunks written to partial
   // buffers, then summed into C.
   if (CPLX && d.prec != 0) fail(TG_E_INPUT, "gemm: the 3xTF32 product is real-only");
-  const size_t psmem = sizeof(T) * 2 * PSTAGES * GBK * GLD;
-  static bool pattr_set = false;
-  if (!pattr_set) {
-    TG_CUDA(cudaFuncSetAttribute(gemm_pipe_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(psmem)));
-    pattr_set = true;
-  }
-  (void)smem;
   auto launch = [&](dim3 gr, const GemmParams<T>& gp) {
     if constexpr (!CPLX) {
       if (gp.d.prec == 1) {
@@ -1294,7 +1138,7 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
         return;
       }
     }
-    gemm_pipe_kernel<T, CPLX><<<gr, 128, psmem, st>>>(gp);
+    gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp);
   };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
