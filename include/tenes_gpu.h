@@ -136,6 +136,25 @@ tg_status tg_measure_onesite(tg_ctx* ctx, int site, const double* op, double* ou
 tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const double* op,
                                double* out);
 
+/* <prod of one-site ops> on an nrow x ncol window (1..4 each), unnormalised:
+ * Contract_RxC_iTPS_CTM (contract_itps_ctm/ctm.cpp:45-87).  The window holds
+ * site lat.other(source, c - source_col, source_row - r) at (r, c), row 0 on
+ * top (twosite_obs.cpp:123-149); nops operators sit at (op_row[i], op_col[i]),
+ * each d x d for that site's d, concatenated in `ops`; identity elsewhere.
+ * The norm is the call with nops = 0. */
+tg_status tg_measure_window(tg_ctx* ctx, int source, int nrow, int ncol, int source_row, int source_col, int nops,
+                            const int* op_row, const int* op_col, const double* ops, double* out);
+
+/* Leading eigenvalues (largest modulus first, (re, im) pairs) of the row
+ * (dir 0, row y = fixed) or column (dir 1, column x = fixed) transfer matrix
+ * built from the edge tensors: TransferMatrix::eigenvalues
+ * (transfer_matrix.cpp:84-142) -- a dense eigensolver when chi^2 <=
+ * maxdim_dense, else Arnoldi (arnoldi.cpp) with the given dimensions,
+ * restarts and tolerance; *nev receives min(num_eigvals, chi^2). */
+tg_status tg_tm_eigenvalues(tg_ctx* ctx, int dir, int fixed, int num_eigvals, int maxdim_dense, int arnoldi_maxdim,
+                            int arnoldi_restartdim, int arnoldi_maxiter, double arnoldi_rtol, double* out,
+                            int* nev);
+
 /* Simple update (src/iTPS/simple_update.cpp:25-46).
  * One-site: Tn[site] <- tensordot(Tn[site], op, 4, 0).
  * Bond: core::Simple_update_bond (core/simple_update.cpp:50-198) between

@@ -25,7 +25,8 @@ EXPORTED = [
     "tg_set_site_tensor", "tg_get_site_tensor", "tg_set_lambda", "tg_get_lambda", "tg_set_env",
     "tg_get_env", "tg_ctm_init", "tg_ctm_move", "tg_ctm_sweep", "tg_ctm_check_convergence",
     "tg_ctm_run", "tg_corner_spectrum", "tg_measure_onesite", "tg_measure_bond_op12",
-    "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_kernel_launch_count", "tg_ctx_stream",
+    "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
+    "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
     "tg_bench_gemm",
 ]
@@ -86,6 +87,10 @@ def load() -> C.CDLL:
         "tg_measure_onesite": (C.c_int, [vp, C.c_int, dp, dp]),
         "tg_measure_bond_op12": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, dp]),
         "tg_su_onesite": (C.c_int, [vp, C.c_int, dp]),
+        "tg_measure_window": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int),
+                                        P(C.c_int), dp, dp]),
+        "tg_tm_eigenvalues": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_double, dp, P(C.c_int)]),
         "tg_su_bond": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "tg_init_tensors": (C.c_int, [vp, C.c_int, dp, P(C.c_int), dp]),
         "tg_sync": (C.c_int, [vp]),

@@ -171,6 +171,28 @@ tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const do
     E(ctx)->measure_bond_op12(source, dx, dy, op, out);
   });
 }
+tg_status tg_measure_window(tg_ctx* ctx, int source, int nrow, int ncol, int source_row, int source_col, int nops,
+                            const int* op_row, const int* op_col, const double* ops, double* out) {
+  return guard([&] {
+    need(out, "out");
+    if (nops > 0) {
+      need(op_row, "op_row");
+      need(op_col, "op_col");
+      need(ops, "ops");
+    }
+    E(ctx)->measure_window(source, nrow, ncol, source_row, source_col, nops, op_row, op_col, ops, out);
+  });
+}
+tg_status tg_tm_eigenvalues(tg_ctx* ctx, int dir, int fixed, int num_eigvals, int maxdim_dense, int arnoldi_maxdim,
+                            int arnoldi_restartdim, int arnoldi_maxiter, double arnoldi_rtol, double* out,
+                            int* nev) {
+  return guard([&] {
+    need(out, "out");
+    if (num_eigvals < 1 || arnoldi_maxdim < 2 || arnoldi_maxiter < 1) tg::fail(TG_E_INPUT, "bad transfer-matrix parameters");
+    E(ctx)->tm_eigenvalues(dir, fixed, num_eigvals, maxdim_dense, arnoldi_maxdim, arnoldi_restartdim,
+                           arnoldi_maxiter, arnoldi_rtol, out, nev);
+  });
+}
 tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op) {
   return guard([&] {
     need(op, "op");

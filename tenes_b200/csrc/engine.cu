@@ -990,6 +990,421 @@ struct EngineT final : Engine {
     if constexpr (!CPLX) out[1] = 0.0;
   }
 
+  // ------------------------------------------------- N x M window <op...>
+  static V moved_to_end(int rank, int pos, int cnt) {  // legs pos..pos+cnt-1 to the end
+    V p;
+    for (int i = 0; i < rank; ++i)
+      if (i < pos || i >= pos + cnt) p.push_back(i);
+    for (int i = 0; i < cnt; ++i) p.push_back(pos + i);
+    return p;
+  }
+  static V moved_from_end(int rank, int pos, int cnt) {  // inverse of moved_to_end
+    V p;
+    const int keep = rank - cnt;
+    for (int i = 0; i < rank; ++i) {
+      if (i < pos) p.push_back(i);
+      else if (i < pos + cnt) p.push_back(keep + (i - pos));
+      else p.push_back(i - cnt);
+    }
+    return p;
+  }
+
+  // Contract_RxC_iTPS_CTM (contract_itps_ctm/ctm.cpp:45-87, ctm_RxC.cpp) for
+  // the window whose source site sits at (source_row, source_col), row 0 on
+  // top; ops[r*ncol + c] is the operator of that site (empty = identity),
+  // applied as sum_{p,q} Tn[..p] op[p,q] conj(Tn[..q]).  Contracted row by
+  // row through a boundary tensor (a, k0, kb0, ..., r).
+  T window(int source, int nrow, int ncol, int source_row, int source_col, const std::vector<DT<T>>& ops) {
+    if (nrow < 1 || ncol < 1 || nrow > 4 || ncol > 4) fail(TG_E_INPUT, "window must be 1..4 x 1..4");
+    std::vector<std::vector<int>> idx(nrow, std::vector<int>(ncol));
+    for (int r = 0; r < nrow; ++r)
+      for (int c = 0; c < ncol; ++c) idx[r][c] = lat.other(source, c - source_col, source_row - r);
+    DT<T> B = C[0][idx[0][0]];
+    for (int c = 0; c < ncol; ++c) {
+      B = td(B, E[0][idx[0][c]], {B.rank() - 1}, {0});  // (..., b', k, kb)
+      B = tr(B, moved_to_end(B.rank(), B.rank() - 3, 1));
+    }
+    B = td(B, C[1][idx[0][ncol - 1]], {B.rank() - 1}, {0});
+    for (int r = 0; r < nrow; ++r) {
+      B = td(E[3][idx[r][0]], B, {1}, {0});  // (a', y, yb, k0, kb0, ..., r)
+      for (int c = 0; c < ncol; ++c) {
+        const DT<T>& Tc = Tn[idx[r][c]];
+        const int pos = 1 + 2 * c;
+        B = tr(B, moved_to_end(B.rank(), pos, 4));  // (..., y, yb, k, kb)
+        int n = B.rank();
+        B = td(B, Tc, {n - 4, n - 2}, {0, 1});  // (..., yb, kb, y', z, p)
+        const DT<T>& o = ops[static_cast<size_t>(r * ncol + c)];
+        if (!o.empty()) B = td(B, o, {B.rank() - 1}, {0});
+        n = B.rank();
+        B = td(B, Tc, {n - 5, n - 4, n - 1}, {0, 1, 4}, false, true);  // (..., y', z, yb', zb)
+        n = B.rank();
+        V p;
+        for (int i = 0; i < n - 4; ++i) p.push_back(i);
+        p.insert(p.end(), {n - 3, n - 1, n - 4, n - 2});  // (..., z, zb, y', yb')
+        B = tr(B, p);
+        B = tr(B, moved_from_end(B.rank(), pos, 4));
+      }
+      const int n = B.rank();
+      B = td(B, E[1][idx[r][ncol - 1]], {n - 1, n - 3, n - 2}, {0, 2, 3});  // (a', z..., r')
+    }
+    DT<T> X = td(C[3][idx[nrow - 1][0]], B, {1}, {0});
+    for (int c = 0; c < ncol; ++c) X = td(E[2][idx[nrow - 1][c]], X, {1, 2, 3}, {0, 1, 2});
+    return scalar(td(X, C[2][idx[nrow - 1][ncol - 1]], {0, X.rank() - 1}, {1, 0}));
+  }
+
+  void measure_window(int source, int nrow, int ncol, int source_row, int source_col, int nops,
+                      const int* op_row, const int* op_col, const double* ops, double* out) override {
+    require_env();
+    check_site(source);
+    if (nrow < 1 || ncol < 1 || nrow > 4 || ncol > 4) fail(TG_E_INPUT, "window must be 1..4 x 1..4");
+    if (source_row < 0 || source_row >= nrow || source_col < 0 || source_col >= ncol)
+      fail(TG_E_INPUT, "source position outside the window");
+    std::vector<DT<T>> grid(static_cast<size_t>(nrow * ncol));
+    int64_t off = 0;
+    for (int i = 0; i < nops; ++i) {
+      const int r = op_row[i], c = op_col[i];
+      if (r < 0 || r >= nrow || c < 0 || c >= ncol) fail(TG_E_INPUT, "operator position outside the window");
+      const int site = lat.other(source, c - source_col, source_row - r);
+      const int64_t d = lat.pdim[site];
+      grid[static_cast<size_t>(r * ncol + c)] = from_host({d, d}, ops + off * NW);
+      off += d * d;
+    }
+    T v = window(source, nrow, ncol, source_row, source_col, grid);
+    std::memcpy(out, &v, sizeof(T));
+    if constexpr (!CPLX) out[1] = 0.0;
+  }
+
+  // ----------------------------------------- transfer matrix eigenvalues
+  // TransferMatrix_ctm::matvec_horizontal / matvec_vertical
+  // (transfer_matrix.cpp:187-308) on a batch of vectors v (chi, chi, nb).
+  DT<T> tm_apply(int dir, int fixed, DT<T> v) {
+    if (dir == 0) {
+      for (int x = 0; x < lat.LX; ++x) {
+        const int site = lat.index(x, fixed);
+        v = td(E[0][site], td(E[2][lat.top(site)], v, {1}, {1}), {0, 2, 3}, {3, 1, 2});
+      }
+    } else {
+      int x = fixed;
+      const int x0 = fixed;
+      do {
+        for (int y = 0; y < lat.LY; ++y) {
+          const int site = lat.index(x, y);
+          v = td(E[3][site], td(E[1][lat.left(site)], v, {1}, {1}), {0, 2, 3}, {3, 1, 2});
+        }
+        x = (x + lat.skew + lat.LX) % lat.LX;
+      } while (x != x0);
+    }
+    return v;
+  }
+
+  // eigenvalues of a dense n x n matrix (row-major, device), by cuSOLVER
+  // Xgeev in complex arithmetic; returned unsorted
+  std::vector<cplx> dense_eigvals(const DT<T>& Mrow, int64_t n) {
+    // complex column-major copy: transpose of the row-major matrix
+    std::vector<T> h(static_cast<size_t>(n * n));
+    TG_CUDA(cudaMemcpyAsync(h.data(), Mrow.p, sizeof(T) * n * n, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    std::vector<cplx> a(static_cast<size_t>(n * n));
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t j = 0; j < n; ++j) {
+        const T v = h[static_cast<size_t>(i * n + j)];
+        cplx z;
+        if constexpr (CPLX) z = v; else z = make_double2(v, 0.0);
+        a[static_cast<size_t>(i + j * n)] = z;
+      }
+    return geev_host_matrix(a, n, nullptr);
+  }
+
+  // Xgeev of a column-major complex n x n matrix given on the host; when
+  // vr_last is given it receives the last component of each right eigenvector
+  std::vector<cplx> geev_host_matrix(const std::vector<cplx>& a, int64_t n, std::vector<cplx>* vr_last) {
+    DT<cplx> A({n, n}, st), W({n}, st), VR({vr_last ? n * n : 1}, st);
+    TG_CUDA(cudaMemcpyAsync(A.p, a.data(), sizeof(cplx) * n * n, cudaMemcpyHostToDevice, st));
+    cusolverDnParams_t prm;
+    check_sol(cusolverDnCreateParams(&prm), "cusolverDnCreateParams");
+    size_t dws = 0, hws = 0;
+    const cusolverEigMode_t jr = vr_last ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+    check_sol(cusolverDnXgeev_bufferSize(sol, prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F,
+                                         W.p, CUDA_C_64F, nullptr, 1, CUDA_C_64F, VR.p, vr_last ? n : 1,
+                                         CUDA_C_64F, &dws, &hws),
+              "Xgeev_bufferSize");
+    DT<unsigned char> dw({static_cast<int64_t>(std::max<size_t>(dws, 1))}, st);
+    std::vector<unsigned char> hw(std::max<size_t>(hws, 1));
+    ProfScope ps(PK_SOLVER, st, 10.0 * n * n * n, 0.0);
+    check_sol(cusolverDnXgeev(sol, prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F, W.p,
+                              CUDA_C_64F, nullptr, 1, CUDA_C_64F, VR.p, vr_last ? n : 1, CUDA_C_64F, dw.p, dws,
+                              hw.data(), hws, info_slot()),
+              "Xgeev");
+    cusolverDnDestroyParams(prm);
+    std::vector<cplx> w(static_cast<size_t>(n));
+    TG_CUDA(cudaMemcpyAsync(w.data(), W.p, sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
+    if (vr_last) {
+      std::vector<cplx> vr(static_cast<size_t>(n * n));
+      TG_CUDA(cudaMemcpyAsync(vr.data(), VR.p, sizeof(cplx) * n * n, cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaStreamSynchronize(st));
+      vr_last->assign(static_cast<size_t>(n), cplx{});
+      for (int64_t i = 0; i < n; ++i) (*vr_last)[static_cast<size_t>(i)] = vr[static_cast<size_t>(n - 1 + i * n)];
+    }
+    check_infos();
+    return w;
+  }
+
+  // eigen() of src/tensor.cpp:91-112: the nev eigenvalues of largest modulus
+  static std::vector<size_t> largest(const std::vector<cplx>& w, size_t nev) {
+    std::vector<size_t> order(w.size());
+    std::iota(order.begin(), order.end(), 0);
+    auto a2 = [&](size_t i) { return w[i].x * w[i].x + w[i].y * w[i].y; };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return a2(a) > a2(b); });
+    order.resize(std::min(nev, order.size()));
+    return order;
+  }
+
+  // TransferMatrix::eigenvalues (transfer_matrix.cpp:84-142) with the
+  // Arnoldi of arnoldi.cpp:45-181 (classical Gram-Schmidt applied twice;
+  // the Krylov space and its Ritz values are those of the reference's
+  // modified Gram-Schmidt).
+  void tm_eigenvalues(int dir, int fixed, int num_eigvals, int maxdim_dense, int maxdim, int restartdim,
+                      int maxiter, double rtol, double* out, int* nev_out) override {
+    require_env();
+    if (dir != 0 && dir != 1) fail(TG_E_INPUT, "direction must be 0 (+x) or 1 (+y)");
+    if (fixed < 0 || fixed >= (dir == 0 ? lat.LY : lat.LX)) fail(TG_E_INPUT, "fixed coordinate out of range");
+    const int64_t chi = P.chi, N = chi * chi;
+    const int64_t nev = std::min<int64_t>(num_eigvals, N);
+    std::vector<cplx> ev;
+    if (N <= maxdim_dense) {
+      DT<T> I({chi, chi, N}, st);
+      identity<T>(I.p, N, st);  // (N x N) identity viewed as (chi, chi, N)
+      DT<T> Mt = tm_apply(dir, fixed, I);  // (chi, chi, N): column j = T e_j
+      std::vector<cplx> w = dense_eigvals(Mt, N);
+      for (size_t i : largest(w, static_cast<size_t>(nev))) ev.push_back(w[i]);
+    } else {
+      ev = arnoldi(dir, fixed, static_cast<size_t>(nev), maxdim, restartdim, maxiter, rtol, N);
+    }
+    for (size_t i = 0; i < ev.size(); ++i) {
+      out[2 * i] = ev[i].x;
+      out[2 * i + 1] = ev[i].y;
+    }
+    if (nev_out) *nev_out = static_cast<int>(ev.size());
+  }
+
+  std::vector<cplx> hess_eigs(const std::vector<T>& H, int ldh, int64_t k, std::vector<cplx>* last) {
+    std::vector<cplx> a(static_cast<size_t>(k * k));
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) {
+        const T v = H[static_cast<size_t>(i * ldh + j)];
+        cplx z;
+        if constexpr (CPLX) z = v; else z = make_double2(v, 0.0);
+        a[static_cast<size_t>(i + j * k)] = z;
+      }
+    return geev_host_matrix(a, k, last);
+  }
+
+  std::vector<cplx> arnoldi(int dir, int fixed, size_t nev, int maxvec_in, int mindim, int maxiter, double rtol,
+                            int64_t N) {
+    int64_t maxvec = maxvec_in;
+    if (N < maxvec) {
+      maxvec = N;
+      maxiter = 1;
+    }
+    if (mindim < static_cast<int>(nev)) mindim = static_cast<int>(nev);
+    const int ldh = static_cast<int>(maxvec);
+    std::vector<T> H(static_cast<size_t>((maxvec + 1) * maxvec));
+    std::memset(H.data(), 0, sizeof(T) * H.size());
+    DT<T> Q = zeros<T>({maxvec + 1, N}, st);  // row j = Krylov vector j
+    // initial vector: C1[site] . C4[top(site)] (dir 0) or C4[site] . C3[left(site)]
+    // (transfer_matrix.cpp:161-185)
+    {
+      DT<T> v0;
+      if (dir == 0) {
+        const int site = lat.index(0, fixed);
+        v0 = td(C[0][site], C[3][lat.top(site)], {0}, {1});
+      } else {
+        const int site = lat.index(fixed, 0);
+        v0 = td(C[3][site], C[2][lat.left(site)], {0}, {1});
+      }
+      TG_CUDA(cudaMemcpyAsync(Q.p, v0.p, sizeof(T) * N, cudaMemcpyDeviceToDevice, st));
+    }
+    auto row = [&](int64_t j) { return Q.p + j * N; };
+    // h[0..k) = Q[:k] q_k (conj), q_k -= Q[:k]^T h  -- twice; then normalise
+    auto orthonormalize = [&](int64_t k) {
+      PrecScope fp64(this, 0);
+      std::vector<T> hacc(static_cast<size_t>(std::max<int64_t>(k, 1)));
+      std::memset(hacc.data(), 0, sizeof(T) * hacc.size());
+      for (int pass = 0; pass < (k > 0 ? 2 : 0); ++pass) {
+        DT<T> h({k, 1}, st);
+        MV qh{Q.p, k, N, N, 1, true};  // conj(Q[:k]) as k x N
+        mm(qh, MV{row(k), N, 1, 1, N, false}, h.p, 1, 1);
+        DT<T> proj({N, 1}, st);
+        mm(MV{Q.p, N, k, 1, N, false}, MV{h.p, k, 1, 1, k, false}, proj.p, 1, 1);  // Q[:k]^T h
+        axpy_neg(row(k), proj.p, N);
+        std::vector<T> hh(static_cast<size_t>(k));
+        TG_CUDA(cudaMemcpyAsync(hh.data(), h.p, sizeof(T) * k, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+        for (int64_t j = 0; j < k; ++j) add_to(hacc[static_cast<size_t>(j)], hh[static_cast<size_t>(j)]);
+      }
+      for (int64_t j = 0; j < k; ++j) H[static_cast<size_t>(j * ldh + (k - 1))] = hacc[static_cast<size_t>(j)];
+      const double nrm = norm2(row(k), N);
+      if (!(nrm > 0.0)) fail(TG_E_RUNTIME, "Arnoldi: Krylov space exhausted (zero vector)");
+      scale<T>(row(k), N, 1.0 / nrm, st);
+      if (k > 0) set_real(H[static_cast<size_t>(k * ldh + (k - 1))], nrm);
+    };
+    auto apply = [&](int64_t k) {  // q_k = T q_{k-1}
+      DT<T> v({chi_(), chi_(), 1}, st);
+      TG_CUDA(cudaMemcpyAsync(v.p, row(k - 1), sizeof(T) * N, cudaMemcpyDeviceToDevice, st));
+      DT<T> w = tm_apply(dir, fixed, v);
+      TG_CUDA(cudaMemcpyAsync(row(k), w.p, sizeof(T) * N, cudaMemcpyDeviceToDevice, st));
+    };
+    auto residue = [&](int64_t k) {  // arnoldi.cpp:170-181
+      std::vector<cplx> last;
+      std::vector<cplx> w = hess_eigs(H, ldh, k, &last);
+      std::vector<size_t> ord = largest(w, nev);
+      const T hk = H[static_cast<size_t>(k * ldh + (k - 1))];
+      double hkr, hki;
+      if constexpr (CPLX) { hkr = hk.x; hki = hk.y; } else { hkr = hk; hki = 0.0; }
+      std::vector<double> res;
+      for (size_t i : ord) {
+        const cplx e = last[i];
+        const double pr = hkr * e.x - hki * e.y, pi = hkr * e.y + hki * e.x;
+        res.push_back(std::hypot(pr, pi) / std::hypot(w[i].x, w[i].y));
+      }
+      return res;
+    };
+    orthonormalize(0);
+    for (size_t k = 1; k <= nev; ++k) {
+      apply(static_cast<int64_t>(k));
+      orthonormalize(static_cast<int64_t>(k));
+    }
+    double res_nev = 1.0;
+    for (int iter = 1; iter <= maxiter; ++iter) {
+      for (int64_t k = static_cast<int64_t>(nev) + 1; k <= maxvec; ++k) {
+        apply(k);
+        orthonormalize(k);
+        res_nev = residue(k)[nev - 1];
+        if (res_nev <= rtol) break;
+      }
+      if (res_nev <= rtol || iter == maxiter) break;
+      restart(Q, H, ldh, maxvec, mindim, N);
+    }
+    std::vector<cplx> w = hess_eigs(H, ldh, maxvec, nullptr);
+    std::vector<cplx> out;
+    for (size_t i : largest(w, nev)) out.push_back(w[i]);
+    return out;
+  }
+
+  // implicitly shifted restart (arnoldi.cpp:117-167): for the k - minvec
+  // largest Ritz values sigma, h <- q^H h q with (h - sigma I) = q r, and the
+  // basis rotated by q; then tiny entries of h dropped
+  void restart(DT<T>& Q, std::vector<T>& H, int ldh, int64_t k, int minvec, int64_t N) {
+    std::vector<cplx> w = hess_eigs(H, ldh, k, nullptr);
+    std::vector<size_t> ord = largest(w, static_cast<size_t>(k));
+    std::vector<cplx> h(static_cast<size_t>(k * k));
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) {
+        const T v = H[static_cast<size_t>(i * ldh + j)];
+        if constexpr (CPLX) h[static_cast<size_t>(i * k + j)] = v; else h[static_cast<size_t>(i * k + j)] = make_double2(v, 0.0);
+      }
+    for (int64_t s = 0; s < k - minvec; ++s) {
+      cplx sigma = w[ord[static_cast<size_t>(s)]];
+      if constexpr (!CPLX) sigma.y = 0.0;  // real_if_real (arnoldi.cpp:113-114)
+      std::vector<cplx> q = small_qr_q(h, k, sigma);
+      h = cmatmul(cmatmul(q, h, k, true), q, k, false);  // q^H h q
+      // Q (rows = vectors) <- q^T Q  i.e. new vector j = sum_i Q_i q[i][j]
+      rotate_basis(Q, q, k, N);
+    }
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) {
+        cplx z = h[static_cast<size_t>(i * k + j)];
+        if (z.x * z.x + z.y * z.y < 1e-28) z = make_double2(0.0, 0.0);
+        T v;
+        if constexpr (CPLX) v = z; else v = z.x;
+        H[static_cast<size_t>(i * ldh + j)] = v;
+      }
+  }
+
+  // Q factor of (h - sigma I) (k x k, row-major, complex) by Householder
+  // QR on the host-visible small matrix, computed with cuSOLVER
+  std::vector<cplx> small_qr_q(const std::vector<cplx>& h, int64_t k, cplx sigma) {
+    std::vector<cplx> a(static_cast<size_t>(k * k));  // column-major
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) {
+        cplx z = h[static_cast<size_t>(i * k + j)];
+        if (i == j) {
+          z.x -= sigma.x;
+          z.y -= sigma.y;
+        }
+        a[static_cast<size_t>(i + j * k)] = z;
+      }
+    DT<cplx> A({k, k}, st), tau({k}, st);
+    TG_CUDA(cudaMemcpyAsync(A.p, a.data(), sizeof(cplx) * k * k, cudaMemcpyHostToDevice, st));
+    int lw1 = 0, lw2 = 0;
+    auto* ap = reinterpret_cast<cuDoubleComplex*>(A.p);
+    auto* tp = reinterpret_cast<cuDoubleComplex*>(tau.p);
+    const int ik = static_cast<int>(k);
+    check_sol(cusolverDnZgeqrf_bufferSize(sol, ik, ik, ap, ik, &lw1), "Zgeqrf_bufferSize");
+    check_sol(cusolverDnZungqr_bufferSize(sol, ik, ik, ik, ap, ik, tp, &lw2), "Zungqr_bufferSize");
+    const int lw = std::max(std::max(lw1, lw2), 1);
+    DT<cplx> work({lw}, st);
+    auto* wp = reinterpret_cast<cuDoubleComplex*>(work.p);
+    check_sol(cusolverDnZgeqrf(sol, ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zgeqrf");
+    check_sol(cusolverDnZungqr(sol, ik, ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zungqr");
+    TG_CUDA(cudaMemcpyAsync(a.data(), A.p, sizeof(cplx) * k * k, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    check_infos();
+    std::vector<cplx> q(static_cast<size_t>(k * k));  // row-major
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) q[static_cast<size_t>(i * k + j)] = a[static_cast<size_t>(i + j * k)];
+    return q;
+  }
+
+  static std::vector<cplx> cmatmul(const std::vector<cplx>& a, const std::vector<cplx>& b, int64_t k, bool adj_a) {
+    std::vector<cplx> c(static_cast<size_t>(k * k), make_double2(0.0, 0.0));
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t l = 0; l < k; ++l) {
+        cplx x = adj_a ? a[static_cast<size_t>(l * k + i)] : a[static_cast<size_t>(i * k + l)];
+        if (adj_a) x.y = -x.y;
+        for (int64_t j = 0; j < k; ++j) {
+          const cplx y = b[static_cast<size_t>(l * k + j)];
+          c[static_cast<size_t>(i * k + j)].x += x.x * y.x - x.y * y.y;
+          c[static_cast<size_t>(i * k + j)].y += x.x * y.y + x.y * y.x;
+        }
+      }
+    return c;
+  }
+
+  void rotate_basis(DT<T>& Q, const std::vector<cplx>& q, int64_t k, int64_t N) {
+    std::vector<T> qt(static_cast<size_t>(k * k));  // qt[j][i] = q[i][j]
+    for (int64_t i = 0; i < k; ++i)
+      for (int64_t j = 0; j < k; ++j) {
+        const cplx z = q[static_cast<size_t>(i * k + j)];
+        T v;
+        if constexpr (CPLX) v = z; else v = z.x;
+        qt[static_cast<size_t>(j * k + i)] = v;
+      }
+    DT<T> qd = from_host({k, k}, reinterpret_cast<const double*>(qt.data()));
+    DT<T> newQ({k, N}, st);
+    PrecScope fp64(this, 0);
+    mm(rm(qd.p, k, k), rm(Q.p, k, N), newQ.p, N, 1);
+    TG_CUDA(cudaMemcpyAsync(Q.p, newQ.p, sizeof(T) * k * N, cudaMemcpyDeviceToDevice, st));
+  }
+
+  int64_t chi_() const { return P.chi; }
+  static void add_to(double& a, double b) { a += b; }
+  static void add_to(cplx& a, cplx b) {
+    a.x += b.x;
+    a.y += b.y;
+  }
+  static void set_real(double& a, double v) { a = v; }
+  static void set_real(cplx& a, double v) { a = make_double2(v, 0.0); }
+  void axpy_neg(T* y, const T* x, int64_t n) { axpy<T>(y, x, -1.0, n, st); }
+  double norm2(const T* x, int64_t n) {
+    DT<T> h({1, 1}, st);
+    PrecScope fp64(this, 0);
+    MV xc{x, 1, n, n, 1, true};
+    mm(xc, MV{x, n, 1, 1, n, false}, h.p, 1, 1);
+    T v = scalar(h);
+    if constexpr (CPLX) return std::sqrt(v.x); else return std::sqrt(v);
+  }
+
   // -------------------------------------------------------- simple update
   void su_onesite(int site, const double* op) override {
     check_site(site);

@@ -531,6 +531,18 @@ __global__ void divide_kernel(T* __restrict__ x, int64_t n, const unsigned long 
 }
 
 template <typename T>
+__global__ void axpy_kernel(T* __restrict__ y, const T* __restrict__ x, double a, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if constexpr (is_cplx<T>::value) {
+      y[i] = make_double2(y[i].x + a * x[i].x, y[i].y + a * x[i].y);
+    } else {
+      y[i] += a * x[i];
+    }
+  }
+}
+
+template <typename T>
 __global__ void scale_kernel(T* __restrict__ x, int64_t n, double a) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -1288,6 +1300,13 @@ void spectrum_distance(const double* a, const double* c, int count, int n, doubl
 }
 
 template <typename T>
+void axpy(T* y, const T* x, double alpha, int64_t n, cudaStream_t st) {
+  axpy_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(y, x, alpha, n);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
 void scale(T* x, int64_t n, double alpha, cudaStream_t st) {
   scale_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(x, n, alpha);
   TG_CHECK_LAUNCH();
@@ -1398,6 +1417,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   template void identity<T>(T*, int64_t, cudaStream_t);                                          \
   template void batched_spectrum<T>(const T* const*, int, int, double*, int*, cudaStream_t);     \
   template void scale<T>(T*, int64_t, double, cudaStream_t);                                     \
+  template void axpy<T>(T*, const T*, double, int64_t, cudaStream_t);                            \
   template void scale_leg<T>(T*, int64_t, int64_t, int64_t, const double*, cudaStream_t);
 
 TG_INST(double)

@@ -107,6 +107,10 @@ void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t 
 template <typename T>
 void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st);
 
+// y += alpha x (alpha real)
+template <typename T>
+void axpy(T* y, const T* x, double alpha, int64_t n, cudaStream_t st);
+
 // x *= alpha (scalar, real)
 template <typename T>
 void scale(T* x, int64_t n, double alpha, cudaStream_t st);

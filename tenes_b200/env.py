@@ -182,6 +182,34 @@ class Environment:
         check(self.lib.tg_measure_bond_op12(self.ctx, source, dx, dy, dptr(o.view(np.float64)), dptr(out)))
         return complex(out[0], out[1])
 
+    def contract_window(self, source: int, nrow: int, ncol: int, source_row: int, source_col: int,
+                        ops: Optional[dict] = None) -> complex:
+        """Contract_RxC_iTPS_CTM: <prod ops> on an nrow x ncol window (unnormalised).
+        ops maps (row, col) -> d x d operator; identity elsewhere."""
+        ops = ops or {}
+        keys = sorted(ops)
+        rows = (C.c_int * max(len(keys), 1))(*[k[0] for k in keys])
+        cols = (C.c_int * max(len(keys), 1))(*[k[1] for k in keys])
+        flat = np.concatenate([np.ascontiguousarray(ops[k], dtype=self.dtype).reshape(-1) for k in keys]) \
+            if keys else np.zeros(1, dtype=self.dtype)
+        flat = np.ascontiguousarray(flat, dtype=self.dtype)
+        out = np.zeros(2)
+        check(self.lib.tg_measure_window(self.ctx, source, nrow, ncol, source_row, source_col, len(keys), rows,
+                                         cols, dptr(flat.view(np.float64)), dptr(out)))
+        return complex(out[0], out[1])
+
+    def tm_eigenvalues(self, direction: int, fixed: int, num_eigvals: int = 4, maxdim_dense: int = 200,
+                       arnoldi_maxdim: int = 50, arnoldi_restartdim: int = 20, arnoldi_maxiter: int = 1,
+                       arnoldi_rtol: float = 1e-10) -> np.ndarray:
+        """TransferMatrix::eigenvalues (transfer_matrix.cpp:84-142)."""
+        out = np.zeros(2 * num_eigvals)
+        nev = C.c_int()
+        check(self.lib.tg_tm_eigenvalues(self.ctx, direction, fixed, num_eigvals, maxdim_dense, arnoldi_maxdim,
+                                         arnoldi_restartdim, arnoldi_maxiter, arnoldi_rtol, dptr(out),
+                                         C.byref(nev)))
+        v = out[: 2 * nev.value]
+        return v[0::2] + 1j * v[1::2]
+
     # ------------------------------------------------------- simple update
     def simple_update(self, source: int, source_leg: int, op: np.ndarray) -> None:
         """iTPS::simple_update(EvolutionOperator) (src/iTPS/simple_update.cpp:25-46)."""
