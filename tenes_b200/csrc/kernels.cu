@@ -477,11 +477,13 @@ __global__ void splitk_reduce_kernel(const T* __restrict__ parts, int nparts, in
 // ---------------------------------------------------------------------------
 // Permutation: one thread per output element, output-coalesced.
 // ---------------------------------------------------------------------------
+constexpr int kMaxRank = 16;  // N x M window boundaries reach rank 2 + 2 M + 4
+
 struct PermParams {
   int rank;
   int64_t total;
-  int64_t out_dims[8];
-  int64_t src_stride[8];  // stride in `in` of output axis i
+  int64_t out_dims[kMaxRank];
+  int64_t src_stride[kMaxRank];  // stride in `in` of output axis i
   bool conj;
 };
 
@@ -1197,13 +1199,13 @@ template <typename T>
 void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>& perm, bool conj,
              cudaStream_t st) {
   const int r = static_cast<int>(in_shape.size());
-  if (r > 8) fail(TG_E_INPUT, "permute: rank > 8");
+  if (r > kMaxRank) fail(TG_E_INPUT, "permute: rank > " + std::to_string(kMaxRank));
   PermParams p{};
   p.rank = r;
   p.conj = conj;
   p.total = numel(in_shape);
   if (p.total == 0) return;
-  int64_t strides[8];
+  int64_t strides[kMaxRank];
   int64_t s = 1;
   for (int i = r - 1; i >= 0; --i) {
     strides[i] = s;
