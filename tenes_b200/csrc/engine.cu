@@ -1097,24 +1097,6 @@ struct EngineT final : Engine {
     return v;
   }
 
-  // eigenvalues of a dense n x n matrix (row-major, device), by cuSOLVER
-  // Xgeev in complex arithmetic; returned unsorted
-  std::vector<cplx> dense_eigvals(const DT<T>& Mrow, int64_t n) {
-    // complex column-major copy: transpose of the row-major matrix
-    std::vector<T> h(static_cast<size_t>(n * n));
-    TG_CUDA(cudaMemcpyAsync(h.data(), Mrow.p, sizeof(T) * n * n, cudaMemcpyDeviceToHost, st));
-    TG_CUDA(cudaStreamSynchronize(st));
-    std::vector<cplx> a(static_cast<size_t>(n * n));
-    for (int64_t i = 0; i < n; ++i)
-      for (int64_t j = 0; j < n; ++j) {
-        const T v = h[static_cast<size_t>(i * n + j)];
-        cplx z;
-        if constexpr (CPLX) z = v; else z = make_double2(v, 0.0);
-        a[static_cast<size_t>(i + j * n)] = z;
-      }
-    return geev_host_matrix(a, n, nullptr);
-  }
-
   // Xgeev of a column-major complex n x n matrix given on the host; when
   // vr_last is given it receives the last component of each right eigenvector
   std::vector<cplx> geev_host_matrix(const std::vector<cplx>& a, int64_t n, std::vector<cplx>* vr_last) {
@@ -1159,26 +1141,75 @@ struct EngineT final : Engine {
     return order;
   }
 
+  // Extent of leg `leg` (0 or 1) of an environment tensor (chi, chi, D, D)
+  // that carries nonzero entries.  The environment is kept at the static
+  // size chi with exact zeros beyond each projector's cut; the reference
+  // stores the cut-sized tensors, so this is its shape()[leg].
+  int64_t used_extent(const DT<T>& e, int leg) {
+    std::vector<T> h(static_cast<size_t>(e.size()));
+    TG_CUDA(cudaMemcpyAsync(h.data(), e.p, sizeof(T) * h.size(), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    const int64_t n0 = e.dim(0), n1 = e.dim(1), inner = e.size() / (n0 * n1);
+    int64_t used = 0;
+    for (int64_t i = 0; i < n0; ++i)
+      for (int64_t j = 0; j < n1; ++j)
+        for (int64_t k = 0; k < inner; ++k)
+          if (!is_zero(h[static_cast<size_t>((i * n1 + j) * inner + k)])) {
+            used = std::max(used, (leg == 0 ? i : j) + 1);
+            break;
+          }
+    return used;
+  }
+  static bool is_zero(double v) { return v == 0.0; }
+  static bool is_zero(cplx v) { return v.x == 0.0 && v.y == 0.0; }
+
   // TransferMatrix::eigenvalues (transfer_matrix.cpp:84-142) with the
   // Arnoldi of arnoldi.cpp:45-181 (classical Gram-Schmidt applied twice;
   // the Krylov space and its Ritz values are those of the reference's
-  // modified Gram-Schmidt).
+  // modified Gram-Schmidt).  The matrix dimension N (dim(), which picks the
+  // N = 1 shortcut, the dense solver for N <= maxdim_dense and the Krylov
+  // size) is the product of the used extents of the boundary legs; the
+  // zero-padded remainder of the chi x chi space is an invariant null block.
   void tm_eigenvalues(int dir, int fixed, int num_eigvals, int maxdim_dense, int maxdim, int restartdim,
                       int maxiter, double rtol, double* out, int* nev_out) override {
     require_env();
     if (dir != 0 && dir != 1) fail(TG_E_INPUT, "direction must be 0 (+x) or 1 (+y)");
     if (fixed < 0 || fixed >= (dir == 0 ? lat.LY : lat.LX)) fail(TG_E_INPUT, "fixed coordinate out of range");
-    const int64_t chi = P.chi, N = chi * chi;
+    const int64_t chi = P.chi, Npad = chi * chi;
+    const int s0 = dir == 0 ? lat.index(0, fixed) : lat.index(fixed, 0);
+    const int64_t ea = dir == 0 ? used_extent(E[0][s0], 0) : used_extent(E[3][s0], 0);
+    const int64_t eb = dir == 0 ? used_extent(E[2][lat.top(s0)], 1) : used_extent(E[1][lat.left(s0)], 1);
+    const int64_t N = ea * eb;
+    if (N == 0) fail(TG_E_RUNTIME, "transfer matrix: boundary tensors are zero");
     const int64_t nev = std::min<int64_t>(num_eigvals, N);
     std::vector<cplx> ev;
-    if (N <= maxdim_dense) {
+    if (N == 1) {
+      ev.push_back(make_double2(1.0, 0.0));
+    } else if (N <= maxdim_dense) {
+      // T applied to the unit vectors of the used block, rows of the block kept
+      std::vector<T> basis(static_cast<size_t>(Npad * N));
+      std::memset(basis.data(), 0, sizeof(T) * basis.size());
+      for (int64_t i = 0; i < ea; ++i)
+        for (int64_t j = 0; j < eb; ++j) set_real(basis[static_cast<size_t>((i * chi + j) * N + i * eb + j)], 1.0);
       DT<T> I({chi, chi, N}, st);
-      identity<T>(I.p, N, st);  // (N x N) identity viewed as (chi, chi, N)
-      DT<T> Mt = tm_apply(dir, fixed, I);  // (chi, chi, N): column j = T e_j
-      std::vector<cplx> w = dense_eigvals(Mt, N);
+      TG_CUDA(cudaMemcpyAsync(I.p, basis.data(), sizeof(T) * basis.size(), cudaMemcpyHostToDevice, st));
+      DT<T> Mt = tm_apply(dir, fixed, I);  // (chi, chi, N): column c = T e_c
+      std::vector<T> full(static_cast<size_t>(Npad * N));
+      TG_CUDA(cudaMemcpyAsync(full.data(), Mt.p, sizeof(T) * full.size(), cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaStreamSynchronize(st));
+      std::vector<cplx> a(static_cast<size_t>(N * N));
+      for (int64_t i = 0; i < ea; ++i)
+        for (int64_t j = 0; j < eb; ++j)
+          for (int64_t c = 0; c < N; ++c) {
+            const T v = full[static_cast<size_t>((i * chi + j) * N + c)];
+            cplx z;
+            if constexpr (CPLX) z = v; else z = make_double2(v, 0.0);
+            a[static_cast<size_t>((i * eb + j) + c * N)] = z;  // column-major
+          }
+      std::vector<cplx> w = geev_host_matrix(a, N, nullptr);
       for (size_t i : largest(w, static_cast<size_t>(nev))) ev.push_back(w[i]);
     } else {
-      ev = arnoldi(dir, fixed, static_cast<size_t>(nev), maxdim, restartdim, maxiter, rtol, N);
+      ev = arnoldi(dir, fixed, static_cast<size_t>(nev), maxdim, restartdim, maxiter, rtol, Npad, N);
     }
     for (size_t i = 0; i < ev.size(); ++i) {
       out[2 * i] = ev[i].x;
@@ -1199,11 +1230,13 @@ struct EngineT final : Engine {
     return geev_host_matrix(a, k, last);
   }
 
+  // N: length of the (zero-padded) vectors; n_used: the matrix dimension
+  // of the reference, which bounds the Krylov size
   std::vector<cplx> arnoldi(int dir, int fixed, size_t nev, int maxvec_in, int mindim, int maxiter, double rtol,
-                            int64_t N) {
+                            int64_t N, int64_t n_used) {
     int64_t maxvec = maxvec_in;
-    if (N < maxvec) {
-      maxvec = N;
+    if (n_used < maxvec) {
+      maxvec = n_used;
       maxiter = 1;
     }
     if (mindim < static_cast<int>(nev)) mindim = static_cast<int>(nev);

@@ -70,6 +70,29 @@ class LatticeSpec:
     initial_dirs: List[List[float]]
     noises: List[float]
 
+    def neighbors(self) -> List[List[int]]:
+        """Neighbour table [left, top, right, bottom] of every site, skew
+        boundary included (SquareLattice::calc_neighbors, SquareLattice.cpp:48-90)."""
+        LX, LY, N = self.LX, self.LY, self.LX * self.LY
+        nn = [[(ix - 1) % LX + iy * LX, ix + ((iy + 1) % LY) * LX, (ix + 1) % LX + iy * LX,
+               ix + ((iy - 1) % LY) * LX] for iy in range(LY) for ix in range(LX)]
+        skew = int(np.fmod(self.skew, LX))
+        if skew != 0:
+            for ix in range(LX):
+                nn[ix][3] = int(np.fmod(ix + LX + skew, LX)) + (LY - 1) * LX
+                nn[N + ix - LX][1] = int(np.fmod(ix + LX - skew, LX))
+        return nn
+
+    def other(self, i: int, dx: int, dy: int) -> int:
+        """Site reached from i by dx steps right and dy steps up
+        (SquareLattice::other, SquareLattice.cpp:116-137)."""
+        nn = self.neighbors()
+        for _ in range(abs(dx)):
+            i = nn[i][2 if dx > 0 else 0]
+        for _ in range(abs(dy)):
+            i = nn[i][1 if dy > 0 else 3]
+        return i
+
 
 @dataclass
 class Operator:

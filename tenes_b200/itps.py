@@ -1,0 +1,473 @@
+"""Drop-in driver for TeNeS's iTPS ground-state / time-evolution runs on the
+GPU path: ``python -m tenes_b200 input.toml`` in place of ``tenes input.toml``.
+
+Mirrors the reference's driver (src/iTPS/main.cpp:141-199, iTPS.cpp,
+optimize.cpp:24-37, simple_update.cpp:103-138, time_evolution.cpp:21-90,
+measure.cpp:30-79) and its output files (onesite_obs.cpp:125-200,
+twosite_obs.cpp:288-340, multisite_obs.cpp:250-300, correlation_length.cpp:57-125,
+density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
+of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
+
+Out of scope (raises InputError): full update (num_step > 0 of
+[parameter.full_update]), finite-temperature mode, the mean-field environment;
+long-range correlation functions ([correlation]) are skipped with a warning.
+"""
+
+from __future__ import annotations
+
+import math
+import os
+import sys
+import time as _time
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .env import CTMParams, Environment
+from .input import Input, InputError, load_input
+
+
+def _fmt(x: float) -> str:
+    return f"{x:.17e}"
+
+
+class ITPS:
+    """iTPS<tensor> (src/iTPS/iTPS.hpp:97-234) over a device-resident Environment."""
+
+    def __init__(self, inp: Input, device: int = 0, mixed: bool = False, print_level: int = 1):
+        p = inp.params
+        if p.calcmode == "finite_temperature":
+            raise InputError("finite-temperature (iTPO) mode is not part of this library")
+        if p.MeanField_Env:
+            raise InputError("the mean-field environment is not part of this library")
+        self.inp = inp
+        self.p = p
+        self.print_level = print_level
+        ls = inp.lattice
+        self.LX, self.LY, self.N = ls.LX, ls.LY, ls.LX * ls.LY
+        self.is_real = inp.is_real
+        cp = CTMParams(chi=p.CHI, inverse_projector_cut=p.Inverse_projector_cut,
+                       ctm_convergence_epsilon=p.CTM_Convergence_Epsilon,
+                       max_ctm_iteration=p.Max_CTM_Iteration, projector_corner=p.CTM_Projector_corner,
+                       use_rsvd=p.Use_RSVD, rsvd_oversampling_factor=p.RSVD_Oversampling_factor,
+                       inverse_lambda_cut=p.Inverse_lambda_cut, mixed=mixed)
+        self.env = Environment(ls.LX, ls.LY, ls.physical_dims, ls.virtual_dims, cp, not self.is_real,
+                               skew=ls.skew, device=device)
+        self.env.init_tensors(p.seed, ls.initial_dirs, ls.noises)
+        if p.Simple_Gauge_Fix:
+            raise InputError("simple_update.gauge_fix is not part of this library")
+        self.outdir = p.outdir
+        os.makedirs(self.outdir, exist_ok=True)
+        n1 = self._names(inp.onesite, "onesite", False)
+        n2 = self._names(inp.twosite, "twosite", False)
+        nm = self._names(inp.multisite, "multisite", True)
+        width = max([len("Energy")] + [len(s) for s in n1 + n2 + nm])
+        self.names1, self.names2, self.namesm = ([s.ljust(width) for s in n] for n in (n1, n2, nm))
+        self._first: Dict[str, bool] = {}
+        self.t_su = self.t_env = self.t_obs = 0.0
+        self.t0 = _time.perf_counter()
+        if p.CHI < max(max(v) for v in ls.virtual_dims) ** 2 and print_level > 0:
+            print("WARNING: CTM may be too small (chi < D*D) for iTPS", file=sys.stderr)
+
+    @staticmethod
+    def _names(ops, kind: str, default_name: bool) -> List[str]:
+        """Group names (iTPS.cpp:310-415): one name per group, an error when a
+        group carries two; only multisite groups get a generated default name."""
+        if not ops:
+            return []
+        names = [""] * (max(o.group for o in ops) + 1)
+        for o in ops:
+            name = o.name or f"{kind}[{o.group}]"
+            if not names[o.group]:
+                names[o.group] = name if default_name else o.name
+            elif names[o.group] != (name if default_name else o.name):
+                raise InputError(f"{kind} operator group {o.group} has two different names: "
+                                 f"{name} and {names[o.group]}")
+        return names
+
+    def _op(self, a: np.ndarray) -> np.ndarray:
+        return a.real.copy() if self.is_real else a
+
+    # ----------------------------------------------------- simple update
+    def simple_update_step(self, group: int = 0) -> None:
+        """One Trotter step: every op of `group` in input order (simple_update.cpp:113-119)."""
+        for up in self.inp.simple_updates:
+            if up.group != group:
+                continue
+            self.env.simple_update(up.source_site, up.source_leg, self._op(up.op))
+
+    def optimize(self) -> None:
+        """optimize() (optimize.cpp:24-37): simple update, then (full update: not built)."""
+        if any(n > 0 for n in self.p.num_full_step):
+            raise InputError("full update is not part of this library (set full_update.num_step = 0)")
+        t = _time.perf_counter()
+        nsteps = self.p.num_simple_step[0]
+        for _ in range(nsteps):
+            self.simple_update_step(0)
+        self.env.sync()
+        self.t_su += _time.perf_counter() - t
+
+    # ------------------------------------------------------ environment
+    def update_ctm(self) -> Tuple[int, bool, float]:
+        t = _time.perf_counter()
+        it, conv, sig = self.env.calc_ctm_environment(True)
+        self.t_env += _time.perf_counter() - t
+        if not conv and self.print_level > 0:
+            print(f"Warning: CTM did not converge! count, sig_max = {it} {sig}")
+        return it, conv, sig
+
+    # ------------------------------------------------------- observables
+    def measure_onesite(self):
+        """measure_onesite (onesite_obs.cpp:35-123)."""
+        ng = len(self.names1)
+        vals = [[complex("nan")] * self.N for _ in range(ng)]
+        norm = []
+        for i in range(self.N):
+            d = self.inp.lattice.physical_dims[i]
+            norm.append(self.env.contract_one_site(i, np.eye(d)))
+        for o in self.inp.onesite:
+            v = self.env.contract_one_site(o.source_site, self._op(o.op))
+            vals[o.group][o.source_site] = o.coeff * v / norm[o.source_site]
+        self._norm_warnings(norm, strict=False)
+        return vals, norm
+
+    def _norm_warnings(self, norms, strict: bool) -> None:
+        if not norms or self.print_level <= 0:
+            return
+        re_min = min(n.real for n in norms)
+        im_max = max(abs(n.imag) for n in norms)
+        if (re_min <= 0.0) if not strict else (re_min < 0.0):
+            print(f"WARNING: Norm is negative [min(real(NORM)) = {re_min}].", file=sys.stderr)
+        if im_max > 1e-6:
+            print(f"WARNING: Norm is not real [max(abs(imag(NORM))) = {im_max} > 1e-6].", file=sys.stderr)
+
+    def _site_op(self, site: int, group: int) -> np.ndarray:
+        for o in self.inp.onesite:
+            if o.source_site == site and o.group == group:
+                return self._op(o.op)
+        raise InputError(f"no onesite operator of group {group} on site {site}")
+
+    def measure_twosite(self):
+        """measure_twosite (twosite_obs.cpp:31-260)."""
+        lat_other = self._other
+        ng = len(self.names2)
+        ret: List[Dict] = [dict() for _ in range(ng)]
+        norms: Dict = {}
+        for o in self.inp.twosite:
+            dx, dy = o.dx[0], o.dy[0]
+            ncol, nrow = abs(dx) + 1, abs(dy) + 1
+            if ncol > 4 or nrow > 4:
+                print("Warning: now version of TeNeS does not support too long-ranged operator", file=sys.stderr)
+                continue
+            sc, tc = (0, ncol - 1) if dx >= 0 else (ncol - 1, 0)
+            sr, tr = (nrow - 1, 0) if dy >= 0 else (0, nrow - 1)
+            origin = lat_other(o.source_site, -sc, sr)  # site at (row 0, col 0)
+            bottom_left = lat_other(origin, 0, -(nrow - 1))
+            key = (bottom_left, nrow - 1, ncol - 1)
+            if key not in norms:
+                norms[key] = self.env.contract_window(o.source_site, nrow, ncol, sr, sc)
+            norm = norms[key]
+            if not o.ops_indices:
+                op = self._op(o.op)
+                if nrow * ncol == 2:
+                    value = self.env.contract_bond_op12(o.source_site, dx, dy, op)
+                else:
+                    sh = op.shape
+                    U, s, VT = np.linalg.svd(op.transpose(0, 2, 1, 3).reshape(sh[0] * sh[2], -1),
+                                             full_matrices=False)
+                    U = U.reshape(sh[0], sh[2], -1)
+                    VT = VT.reshape(-1, sh[1], sh[3])
+                    value = 0.0
+                    for si in range(len(s)):
+                        value += s[si] * self.env.contract_window(
+                            o.source_site, nrow, ncol, sr, sc,
+                            {(sr, sc): self._op(U[:, :, si]), (tr, tc): self._op(VT[si])})
+            else:
+                tgt = lat_other(o.source_site, dx, dy)
+                value = self.env.contract_window(o.source_site, nrow, ncol, sr, sc,
+                                                 {(sr, sc): self._site_op(o.source_site, o.ops_indices[0]),
+                                                  (tr, tc): self._site_op(tgt, o.ops_indices[1])})
+            ret[o.group][(o.source_site, dx, dy)] = o.coeff * value / norm
+        self._norm_warnings(list(norms.values()), strict=True)
+        return ret, norms
+
+    def measure_multisite(self):
+        """measure_multisite (multisite_obs.cpp:31-232)."""
+        ng = len(self.namesm)
+        ret: List[Dict] = [dict() for _ in range(ng)]
+        norms: Dict = {}
+        for o in self.inp.multisite:
+            mindx, maxdx = min(0, *o.dx), max(0, *o.dx)
+            mindy, maxdy = min(0, *o.dy), max(0, *o.dy)
+            ncol, nrow = maxdx - mindx + 1, maxdy - mindy + 1
+            if ncol > 4 or nrow > 4:
+                print("Warning: now version of TeNeS does not support too long-ranged operator", file=sys.stderr)
+                continue
+            if not o.ops_indices:
+                raise InputError("Empty op.ops_indices is not supported for multisites observable")
+            sc, sr = -mindx, maxdy
+            origin = self._other(o.source_site, -sc, sr)
+            key = (self._other(origin, 0, -(nrow - 1)), nrow - 1, ncol - 1)
+            if key not in norms:
+                norms[key] = self.env.contract_window(o.source_site, nrow, ncol, sr, sc)
+            ops = {(sr, sc): self._site_op(o.source_site, o.ops_indices[0])}
+            for n, (dx, dy) in enumerate(zip(o.dx, o.dy)):
+                tgt = self._other(o.source_site, dx, dy)
+                ops[(sr - dy, sc + dx)] = self._site_op(tgt, o.ops_indices[n + 1])
+            value = self.env.contract_window(o.source_site, nrow, ncol, sr, sc, ops)
+            ret[o.group][(o.source_site, tuple(o.dx), tuple(o.dy))] = o.coeff * value / norms[key]
+        self._norm_warnings(list(norms.values()), strict=True)
+        return ret
+
+    def measure_transfer_matrix(self):
+        """measure_transfer_matrix_eigenvalues (correlation_length.cpp:24-55)."""
+        tp = self.inp.tm_params
+        res = []
+        for d in (0, 1):
+            W = self.LY if d == 0 else self.LX
+            for fixed in range(W):
+                ev = self.env.tm_eigenvalues(d, fixed, tp.num_eigvals, tp.maxdim_dense_eigensolver,
+                                             tp.arnoldi_maxdim, tp.arnoldi_restartdim, tp.arnoldi_maxiter,
+                                             tp.arnoldi_rtol)
+                res.append((d, fixed, ev))
+        return res
+
+    def _other(self, i: int, dx: int, dy: int) -> int:
+        return self.inp.lattice.other(i, dx, dy)
+
+    # ----------------------------------------------------------- writers
+    def _open(self, name: str, header: List[str]):
+        path = os.path.join(self.outdir, name)
+        if not self._first.get(name):
+            self._first[name] = True
+            with open(path, "w") as f:
+                f.write("\n".join(header) + "\n\n")
+        return open(path, "a")
+
+    def _time_header(self, time: Optional[float]) -> List[str]:
+        if time is None:
+            return []
+        return ["time" if self.p.calcmode == "time_evolution" else "inverse temperature"]
+
+    @staticmethod
+    def _cols(cols: List[str]) -> List[str]:
+        out = ["# The meaning of each column is the following: "]
+        out += [f"# ${i + 1}: {c}" for i, c in enumerate(cols)]
+        return out
+
+    def save_onesite(self, vals, norm, time, prefix):
+        hdr = self._cols(self._time_header(time) + ["op_group", "site_index", "real", "imag"])
+        hdr += ["# The names of op_group are the following: "]
+        hdr += [f"# {g}: {n}" for g, n in enumerate(self.names1)] + ["# -1: norm"]
+        with self._open(prefix + "onesite_obs.dat", hdr) as f:
+            tp = "" if time is None else _fmt(time) + " "
+            for g, row in enumerate(vals):
+                for i, v in enumerate(row):
+                    if not math.isnan(v.real):
+                        f.write(f"{tp}{g} {i} {_fmt(v.real)} {_fmt(v.imag)}\n")
+            for i, v in enumerate(norm):
+                f.write(f"{tp}-1 {i} {_fmt(v.real)} {_fmt(v.imag)}\n")
+
+    def save_twosite(self, ret, norms, time, prefix):
+        hdr = self._cols(self._time_header(time) + ["op_group", "source_site", "dx", "dy", "real", "imag"])
+        hdr += ["# The names of op_group are the following: "]
+        hdr += [f"# {g}: {n}" for g, n in enumerate(self.names2)] + ["# -1: norm"]
+        with self._open(prefix + "twosite_obs.dat", hdr) as f:
+            tp = "" if time is None else _fmt(time) + " "
+            for g, d in enumerate(ret):
+                for (s, dx, dy), v in sorted(d.items()):
+                    f.write(f"{tp}{g} {s} {dx} {dy} {_fmt(v.real)} {_fmt(v.imag)}\n")
+            # norm keys are Bond{bottom-left site, nrow - 1, ncol - 1} (twosite_obs.cpp:166)
+            for (s, a, b), v in sorted(norms.items()):
+                f.write(f"{tp}-1 {s} {a} {b} {_fmt(v.real)} {_fmt(v.imag)}\n")
+
+    def save_multisite(self, ret, time, prefix):
+        nsites_of = {}
+        for o in self.inp.multisite:
+            if nsites_of.setdefault(o.group, len(o.dx) + 1) != len(o.dx) + 1:
+                raise InputError(f"multisite operator group {o.group} mixes different numbers of sites")
+        for nsites in sorted(set(nsites_of.values())):
+            cols = self._time_header(time) + ["op_group", "source_site"]
+            for k in range(1, nsites):
+                cols += [f"dx[{k}]", f"dy[{k}]"]
+            hdr = self._cols(cols + ["real", "imag"]) + ["# The names of op_group are the following: "]
+            hdr += [f"# {g}: {n}" for g, n in enumerate(self.namesm) if nsites_of.get(g) == nsites]
+            with self._open(prefix + f"multisite_obs_{nsites}.dat", hdr) as f:
+                tp = "" if time is None else _fmt(time) + " "
+                for g, d in enumerate(ret):
+                    for (s, dxs, dys), v in sorted(d.items()):
+                        if len(dxs) + 1 != nsites:
+                            continue
+                        pos = " ".join(f"{a} {b}" for a, b in zip(dxs, dys))
+                        f.write(f"{tp}{g} {s} {pos} {_fmt(v.real)} {_fmt(v.imag)}\n")
+
+    def save_correlation_length(self, res, time, prefix):
+        hdr = ["# The meaning of each column is the following: "]
+        idx = 1
+        if time is not None:
+            hdr.append(f"# ${idx}: time")
+            idx += 1
+        hdr += [f"# ${idx}: direction 0: +x, 1: +y", f"# ${idx + 1}: y (dir=0) or x (dir=1) coorinates",
+                f"# ${idx + 2}: correlation length xi = 1/e_1 ",
+                f"# ${idx + 3}-: eigenvalues e_i = -log|t_i/t_0|",
+                "#      where i > 0 and t_i is i-th largest eigenvalue of T"]
+        with self._open(prefix + "correlation_length.dat", hdr) as f:
+            tp = "" if time is None else _fmt(time) + " "
+            lat = self.inp.lattice
+            for (d, x, ev) in res:
+                if len(ev) == 1:
+                    f.write(f"{tp}{d} {x} {_fmt(0.0)}\n")
+                    continue
+                L = lat.LX if d == 0 else self._ly_noskew()
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    e = np.abs(np.asarray(ev)) / abs(ev[0])
+                    xi = -L / np.log(e[1])
+                    es = -np.log(e[1:]) / L
+                f.write(f"{tp}{d} {x} {_fmt(xi)} " + " ".join(_fmt(v) for v in es) + "\n")
+
+    def _ly_noskew(self) -> int:
+        ls = self.inp.lattice
+        if ls.skew == 0:
+            return ls.LY
+        s = ls.skew % ls.LX
+        return ls.LY * ((ls.LX * s // math.gcd(ls.LX, s)) // s)
+
+    def save_density(self, vals, two, multi, time, prefix):
+        nsites = sum(1 for d in self.inp.lattice.physical_dims if d > 1)
+        # sites without an operator of a group hold NaN and make that group's sum NaN, as in
+        # the reference; energy compares the width-padded names (density.cpp:61-72)
+        loc = [sum((row[i] for i in range(self.N) if self.inp.lattice.physical_dims[i] > 1), 0j)
+               for row in vals]
+        tw = [sum(d.values(), 0j) for d in two]
+        mu = [sum(d.values(), 0j) for d in multi]
+        energy = sum(loc[g].real for g, n in enumerate(self.names1) if n == "site_hamiltonian")
+        energy += sum(tw[g].real for g, n in enumerate(self.names2) if n == "bond_hamiltonian")
+        inv = 1.0 / nsites
+        energy *= inv
+        cnt1 = {o.group for o in self.inp.onesite}
+        cnt2 = {o.group for o in self.inp.twosite}
+        cntm = {o.group for o in self.inp.multisite}
+        path = os.path.join(self.outdir, prefix + "density.dat")
+
+        def num(v: float) -> str:
+            return (" " if v >= 0.0 else "") + _fmt(v)
+
+        if time is not None:
+            if not self._first.get("density"):
+                self._first["density"] = True
+                hdr = self._cols(self._time_header(time) + ["observable ID", "real", "imag"])
+                hdr += ["# The meaning of observable IDs are the following: ", "# 0: Energy"]
+                k = 1
+                for names, cnt in ((self.names1, cnt1), (self.names2, cnt2), (self.namesm, cntm)):
+                    for g, n in enumerate(names):
+                        if g in cnt:
+                            hdr.append(f"# {k}: {n}")
+                            k += 1
+                with open(path, "w") as f:
+                    f.write("\n".join(hdr) + "\n\n")
+            with open(path, "a") as f:
+                f.write(f"{_fmt(time)} 0 {num(energy)}  {_fmt(0.0)}\n")
+                k = 1
+                for arr, names, cnt in ((loc, self.names1, cnt1), (tw, self.names2, cnt2),
+                                        (mu, self.namesm, cntm)):
+                    for g, n in enumerate(names):
+                        if g in cnt:
+                            v = complex(arr[g]) * inv
+                            f.write(f"{_fmt(time)} {k} {num(v.real)} {num(v.imag)}\n")
+                            k += 1
+        else:
+            width = len((self.names1 + self.names2 + self.namesm + ["Energy"])[0])
+            with open(path, "w") as f:
+                f.write(f"{'Energy'.ljust(width)} = {num(energy)}  {_fmt(0.0)}\n")
+                for arr, names, cnt in ((loc, self.names1, cnt1), (tw, self.names2, cnt2),
+                                        (mu, self.namesm, cntm)):
+                    for g, n in enumerate(names):
+                        if g in cnt:
+                            v = complex(arr[g]) * inv
+                            f.write(f"{n} = {num(v.real)} {num(v.imag)}\n")
+        return energy
+
+    # ----------------------------------------------------------- measure
+    def measure(self, time: Optional[float] = None, prefix: str = ""):
+        """iTPS::measure (measure.cpp:30-79)."""
+        self.update_ctm()
+        t = _time.perf_counter()
+        vals, norm = self.measure_onesite()
+        self.save_onesite(vals, norm, time, prefix)
+        two, norms = self.measure_twosite()
+        self.save_twosite(two, norms, time, prefix)
+        multi = self.measure_multisite()
+        if self.inp.multisite:
+            self.save_multisite(multi, time, prefix)
+        if self.inp.tm_params.to_calculate:
+            self.save_correlation_length(self.measure_transfer_matrix(), time, prefix)
+        energy = self.save_density(vals, two, multi, time, prefix)
+        self.t_obs += _time.perf_counter() - t
+        return energy
+
+    def time_evolution(self) -> None:
+        """iTPS::time_evolution (time_evolution.cpp:21-90), simple-update based."""
+        p = self.p
+        if p.num_simple_step[0] <= 0:
+            raise InputError("full-update time evolution is not part of this library")
+        if p.num_full_step[0] > 0:
+            raise InputError("While mode is not ground state calculation,\n"
+                             "       simple update and full update are both required.")
+        groups = {u.group for u in self.inp.simple_updates}
+        ngroups = max(groups) + 1 if groups else 1
+        for g in range(ngroups):
+            if groups and g not in groups:
+                raise InputError(f"no simple update with group number {g}")
+
+        def per_group(v: List, what: str) -> List:
+            if len(v) == ngroups:
+                return list(v)
+            if len(v) == 1:
+                return list(v) * ngroups
+            raise InputError(f"size of {what} {len(v)} is not equal to the number of simple update groups.")
+
+        nss = per_group(p.num_simple_step, "num_step")
+        tau = per_group(p.tau_simple_step, "tau")
+        mi = list(p.measure_interval)
+        while len(mi) < ngroups:
+            mi.append(mi[-1])
+        t = 0.0
+        self.measure(t, "TE_")
+        for g in range(ngroups):
+            for step in range(nss[g]):
+                t0 = _time.perf_counter()
+                self.simple_update_step(g)
+                self.env.sync()
+                self.t_su += _time.perf_counter() - t0
+                t += tau[g]
+                if (step + 1) % mi[g] == 0:
+                    self.measure(t, "TE_")
+            if nss[g] % mi[g] != 0:
+                self.measure(t, "TE_")
+
+    def summary(self) -> None:
+        """summary() (measure.cpp:81-107): time.dat."""
+        with open(os.path.join(self.outdir, "time.dat"), "w") as f:
+            f.write(f"time all           = {_time.perf_counter() - self.t0}\n")
+            f.write(f"time simple update = {self.t_su}\n")
+            f.write(f"time full update   = 0\n")
+            f.write(f"time environment  = {self.t_env}\n")
+            f.write(f"time observable    = {self.t_obs}\n")
+
+
+def run(path: str, device: int = 0, mixed: bool = False, print_level: int = 1,
+        outdir: Optional[str] = None) -> ITPS:
+    """tenes_itps_main for one expert input file; `outdir` overrides
+    parameter.general.output."""
+    inp = load_input(path)
+    if outdir is not None:
+        inp.params.outdir = outdir
+    it = ITPS(inp, device=device, mixed=mixed, print_level=print_level)
+    if inp.params.calcmode == "time_evolution":
+        it.time_evolution()
+    else:
+        it.optimize()
+        if inp.params.to_measure:
+            it.measure()
+    it.summary()
+    return it

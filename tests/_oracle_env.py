@@ -1,0 +1,82 @@
+"""CPU stand-in for tenes_b200.env.Environment built on the oracle.
+
+Test infrastructure only: it lets the front-end's driver loop and writers run
+here (no GPU) against the golden output files.  The product never imports it."""
+import numpy as np
+
+from oracle import tenes_oracle as O
+
+
+class OracleEnvironment:
+    def __init__(self, LX, LY, physical_dims, virtual_dims, params, is_complex, skew=0, device=0):
+        self.lat = O.Lattice(LX, LY, skew)
+        self.lat.physical_dims = list(physical_dims)
+        self.lat.virtual_dims = [list(v) for v in virtual_dims]
+        self.N = LX * LY
+        self.is_complex = is_complex
+        self.p = O.Params(CHI=params.chi, Inverse_projector_cut=params.inverse_projector_cut,
+                          CTM_Convergence_Epsilon=params.ctm_convergence_epsilon,
+                          Max_CTM_Iteration=params.max_ctm_iteration,
+                          CTM_Projector_corner=params.projector_corner, Use_RSVD=params.use_rsvd,
+                          RSVD_Oversampling_factor=params.rsvd_oversampling_factor,
+                          Inverse_lambda_cut=params.inverse_lambda_cut)
+        self.env = None
+        self.lam = [[np.ones(v[l]) for l in range(4)] for v in virtual_dims]
+
+    def init_tensors(self, seed, initial_dirs, noises):
+        self.lat.initial_dirs = [list(d) for d in initial_dirs]
+        self.lat.noises = list(noises)
+        self.Tn = O.initialize_tensors(self.lat, seed, not self.is_complex)
+
+    def simple_update(self, source, leg, op):
+        if leg < 0:
+            self.Tn[source] = np.tensordot(self.Tn[source], op, ([4], [0]))
+            return
+        tg = self.lat.neighbor(source, leg)
+        a, b, lc = O.simple_update_bond(self.Tn[source], self.Tn[tg], self.lam[source], self.lam[tg], op, leg,
+                                        self.p)
+        self.lam[source][leg] = lc
+        self.lam[tg][(leg + 2) % 4] = lc
+        self.Tn[source], self.Tn[tg] = a, b
+
+    def sync(self):
+        pass
+
+    def calc_ctm_environment(self, initialize=True):
+        self.env, it, conv, sig = O.calc_ctm_environment(self.Tn, self.p, self.lat)
+        return it, conv, sig
+
+    def contract_one_site(self, i, op):
+        e = self.env
+        return complex(O.contract_one_site(e.C1[i], e.C2[i], e.C3[i], e.C4[i], e.eTt[i], e.eTr[i], e.eTb[i],
+                                           e.eTl[i], self.Tn[i], op))
+
+    def contract_bond_op12(self, source, dx, dy, op):
+        e, lat, Tn = self.env, self.lat, self.Tn
+        if dy == 0:
+            sc = 0 if dx >= 0 else 1
+            l, r = lat.other(source, -sc, 0), lat.other(source, 1 - sc, 0)
+            o = op if l == source else op.transpose(1, 0, 3, 2)
+            return complex(O.contract_two_sites_horizontal_op12(
+                e.C1[l], e.C2[r], e.C3[r], e.C4[l], e.eTt[l], e.eTt[r], e.eTr[r], e.eTb[r], e.eTb[l], e.eTl[l],
+                Tn[l], Tn[r], o))
+        sr = 1 if dy >= 0 else 0
+        t, b = lat.other(source, 0, sr), lat.other(source, 0, sr - 1)
+        o = op if t == source else op.transpose(1, 0, 3, 2)
+        return complex(O.contract_two_sites_vertical_op12(
+            e.C1[t], e.C2[t], e.C3[b], e.C4[b], e.eTt[t], e.eTr[t], e.eTr[b], e.eTb[b], e.eTl[b], e.eTl[t],
+            Tn[t], Tn[b], o))
+
+    def contract_window(self, source, nrow, ncol, source_row, source_col, ops=None):
+        ops = ops or {}
+        idx, Cs, eTt, eTr, eTb, eTl, T = O._window(self.env, self.Tn, self.lat, source, source_col, source_row,
+                                                    nrow, ncol)
+        grid = [[ops.get((r, c), np.eye(self.lat.physical_dims[idx[r][c]])) for c in range(ncol)]
+                for r in range(nrow)]
+        return complex(O.contract_window(Cs, eTt, eTr, eTb, eTl, T, grid))
+
+    def tm_eigenvalues(self, direction, fixed, num_eigvals=4, maxdim_dense=200, arnoldi_maxdim=50,
+                       arnoldi_restartdim=20, arnoldi_maxiter=1, arnoldi_rtol=1e-10):
+        tp = O.TMParams(num_eigvals, maxdim_dense, arnoldi_maxdim, arnoldi_restartdim, arnoldi_maxiter,
+                        arnoldi_rtol)
+        return O.tm_eigenvalues(self.env, self.lat, direction, fixed, tp)

@@ -1,0 +1,59 @@
+"""End-to-end run of the reference's TE_TFI test input through
+``python -m tenes_b200`` on the GPU, checked the way the reference checks its
+own runs (test/fulltest.py.in:55-88, rtol 1e-3, atol 1e-4) against the
+committed TE_* output fixtures."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from tests._te_tfi import GOLDEN, expected
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _read(path):
+    rows = []
+    with open(path) as f:
+        for line in f:
+            line = line.split("#")[0].strip()
+            if line:
+                rows.append([float(w) for w in line.split()])
+    return rows
+
+
+@pytest.fixture(scope="module")
+def te_tfi_run(tmp_path_factory):
+    out = tmp_path_factory.mktemp("te_tfi")
+    r = subprocess.run([sys.executable, "-m", "tenes_b200", os.path.join(GOLDEN, "te_tfi_input.toml"),
+                        "--outdir", str(out), "--quiet"], cwd=REPO, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return out
+
+
+@pytest.mark.parametrize("name,key", [("TE_density.dat", "density"), ("TE_onesite_obs.dat", "onesite"),
+                                      ("TE_twosite_obs.dat", "twosite"),
+                                      ("TE_multisite_obs_4.dat", "multisite"),
+                                      ("TE_correlation_length.dat", "correlation_length")])
+def test_te_tfi_outputs(te_tfi_run, name, key):
+    exp = expected()
+    tol = exp["tolerance"]
+    res = _read(os.path.join(te_tfi_run, name))
+    ref = exp[key]
+    assert len(res) == len(ref), (name, len(res), len(ref))
+    bad = []
+    for i, (rs, rf) in enumerate(zip(res, ref)):
+        if not all(np.isclose(s, f, rtol=tol["rtol"], atol=tol["atol"]) for s, f in zip(rs, rf)):
+            bad.append((i, rs, rf))
+    assert not bad, bad[:5]
+
+
+def test_te_tfi_time_dat(te_tfi_run):
+    lines = open(os.path.join(te_tfi_run, "time.dat")).read().splitlines()
+    assert [l.split("=")[0].strip() for l in lines] == [
+        "time all", "time simple update", "time full update", "time environment", "time observable"]
