@@ -72,6 +72,9 @@ typedef struct tg_params {
                                        3xTF32 tensor-core products (FP64 tile accumulation); the
                                        orthonormalisation, SVDs and observables stay FP64.  Real
                                        tensors only.  0 (default): everything FP64. */
+  int cuda_graph;                   /* 1 (default): with rSVD corner projectors, replay each CTMRG
+                                       sweep from a captured CUDA graph (same kernels, same results);
+                                       0: launch every kernel from the host. */
 } tg_params;
 
 /* Fill *p with the reference defaults. */

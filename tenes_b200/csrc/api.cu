@@ -67,6 +67,7 @@ void tg_params_default(tg_params* p) {
   p->rsvd_seed = 0;
   p->inverse_lambda_cut = 1e-12;
   p->mixed = 0;
+  p->cuda_graph = 1;
 }
 
 const char* tg_last_error(void) { return g_last_error.c_str(); }

@@ -45,8 +45,11 @@ inline void check_cuda(cudaError_t e, const char* what, const char* file, int li
 #define TG_CUDA(x) ::tg::check_cuda((x), #x, __FILE__, __LINE__)
 #define TG_CHECK_LAUNCH() ::tg::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
-// Number of kernels launched by this library (host-side counter).
+// Number of kernels launched by this library (host-side counter).  Kernels
+// recorded into a CUDA graph are taken back off with uncount_launch and
+// counted again at every launch of the graph.
 void count_launch(uint64_t n = 1);
+void uncount_launch(uint64_t n);
 uint64_t launch_count();
 
 // Optional per-launch CUDA-event profiling, grouped by kernel family.  When

@@ -121,6 +121,7 @@ struct EngineT final : Engine {
   }
 
   ~EngineT() override {
+    drop_graph();
     // release device tensors before the stream goes away
     Tn.clear();
     Trot.clear();
@@ -128,6 +129,7 @@ struct EngineT final : Engine {
     for (auto& v : E) v.clear();
     spec_old = DT<double>();
     if (st) cudaStreamSynchronize(st);
+    cudaDeviceGraphMemTrim(dev);
     if (sol) cusolverDnDestroy(sol);
     cudaFree(d_max);
     cudaFree(d_info);
@@ -156,7 +158,12 @@ struct EngineT final : Engine {
     return tensordot<T>(a, b, x, y, st, ca, cb, cur_prec);
   }
   DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
-  void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.size(), d_max, st); }
+  void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.p, a.size(), d_max, st); }
+  // dst = a / max|a|, written into the existing storage of dst
+  void normalize_into(const DT<T>& a, DT<T>& dst) {
+    if (dst.size() != a.size()) fail(TG_E_RUNTIME, "normalize_into: size mismatch");
+    normalize_max_abs<T>(a.p, dst.p, a.size(), d_max, st);
+  }
 
   void upload(DT<T>& t, const double* host) {
     TG_CUDA(cudaMemcpyAsync(t.p, host, sizeof(T) * t.size(), cudaMemcpyHostToDevice, st));
@@ -184,9 +191,15 @@ struct EngineT final : Engine {
 
   const DT<T>& rot(int site, int which) {
     if (!rot_ok[site]) {
-      Trot[site][0] = tr(Tn[site], {2, 3, 0, 1, 4});
-      Trot[site][1] = tr(Tn[site], {1, 2, 3, 0, 4});
-      Trot[site][2] = tr(Tn[site], {3, 0, 1, 2, 4});
+      static const std::vector<int> perms[3] = {{2, 3, 0, 1, 4}, {1, 2, 3, 0, 4}, {3, 0, 1, 2, 4}};
+      for (int w = 0; w < 3; ++w) {
+        if (Trot[site][w].empty()) {
+          Shape s(5);
+          for (int a = 0; a < 5; ++a) s[a] = Tn[site].dim(perms[w][a]);
+          Trot[site][w] = DT<T>(s, st);  // allocated once, rewritten when Tn changes
+        }
+        permute<T>(Tn[site].p, Trot[site][w].p, Tn[site].sh, perms[w], false, st);
+      }
       rot_ok[site] = true;
     }
     return Trot[site][which];
@@ -631,25 +644,51 @@ struct EngineT final : Engine {
     }
   }
 
-  // Calc_Next_CTM (ctm.cpp:493-518)
+  // Calc_Next_CTM (ctm.cpp:493-518); the results are written into the
+  // storage of C1o / C4o
   void next_ctm(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT6, const DT<T>& PU,
                 const DT<T>& PL, DT<T>& C1o, DT<T>& C4o) {
-    C1o = td(PU, td(C1, eT1, {1}, {0}), {0, 1, 2}, {0, 2, 3});
-    C4o = td(td(eT6, C4, {1}, {0}), PL, {3, 1, 2}, {0, 1, 2});
-    normalize(C1o);
-    normalize(C4o);
+    normalize_into(td(PU, td(C1, eT1, {1}, {0}), {0, 1, 2}, {0, 2, 3}), C1o);
+    normalize_into(td(td(eT6, C4, {1}, {0}), PL, {3, 1, 2}, {0, 1, 2}), C4o);
   }
 
-  // Calc_Next_eT (ctm.cpp:520-552)
-  DT<T> next_et(const DT<T>& eT8, const DT<T>& T1, const DT<T>& PU, const DT<T>& PL) {
+  // Calc_Next_eT (ctm.cpp:520-552), written into the storage of `out`
+  void next_et(const DT<T>& eT8, const DT<T>& T1, const DT<T>& PU, const DT<T>& PL, DT<T>& out) {
     DT<T> X = td(T1, td(eT8, PL, {1}, {0}), {0, 1}, {2, 4}, true, false);
     X = td(T1, X, {0, 1, 4}, {4, 5, 2});
-    DT<T> e = tr(td(X, PU, {1, 3, 4}, {1, 2, 0}), {3, 2, 0, 1});
-    normalize(e);
-    return e;
+    normalize_into(tr(td(X, PU, {1, 3, 4}, {1, 2, 0}), {3, 2, 0, 1}), out);
   }
 
   // ------------------------------------------------------------- the moves
+  //
+  // Each move has the two passes of Left_move (ctm.cpp:562-616): all the
+  // projectors of the line, then the new corners and edges of the next line.
+  // The reference writes into copies (C1_bak, ...) and copies back; here the
+  // results go straight into the environment storage, which is safe because
+  // every row reads the current line and writes the next one (for a line
+  // count of 1 both are the same line, and then every tensor is read and
+  // written by one row only).  The reference computes every new edge tensor
+  // twice -- row iy's eT[k] and row iy-1's eT[j] are the same Calc_Next_eT
+  // of the same inputs -- so each distinct (output, inputs) job runs once;
+  // when two jobs write one output the later one wins, as in the reference.
+  struct EtJob {
+    int out, src, site, pu, pl;
+    bool same_inputs(const EtJob& o) const { return src == o.src && site == o.site && pu == o.pu && pl == o.pl; }
+  };
+  static std::vector<EtJob> final_jobs(const std::vector<EtJob>& jobs) {
+    std::vector<EtJob> out;
+    for (size_t a = 0; a < jobs.size(); ++a) {
+      bool superseded = false;
+      for (size_t b = a + 1; b < jobs.size(); ++b)
+        if (jobs[b].out == jobs[a].out && !jobs[b].same_inputs(jobs[a])) superseded = true;
+      bool repeated = false;
+      for (const EtJob& o : out)
+        if (o.out == jobs[a].out && o.same_inputs(jobs[a])) repeated = true;
+      if (!superseded && !repeated) out.push_back(jobs[a]);
+    }
+    return out;
+  }
+
   void left_move(int ix) {
     auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
@@ -663,14 +702,15 @@ struct EngineT final : Engine {
         proj_updown(C1[i], C2[j], C3[k], C4[l], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i],
                     Tn[i], Tn[j], Tn[k], Tn[l], PUs[iy], PLs[iy]);
     }
-    auto C1b = C1, C4b = C4, eTlb = eTl;
+    std::vector<EtJob> jobs;
     for (int iy = 0; iy < LY; ++iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C1b[i], C4b[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
-      eTl[j] = next_et(eTlb[i], Tn[i], PUs[iy], PLs[up]);
-      eTl[k] = next_et(eTlb[l], Tn[l], PUs[dn], PLs[iy]);
+      next_ctm(C1[i], C4[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
+      jobs.push_back({j, i, i, iy, up});
+      jobs.push_back({k, l, l, dn, iy});
     }
+    for (const EtJob& b : final_jobs(jobs)) next_et(eTl[b.src], Tn[b.site], PUs[b.pu], PLs[b.pl], eTl[b.out]);
   }
 
   void right_move(int ix) {
@@ -686,14 +726,15 @@ struct EngineT final : Engine {
         proj_updown(C3[k], C4[l], C1[i], C2[j], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k],
                     rot(k, 0), rot(l, 0), rot(i, 0), rot(j, 0), PUs[iy], PLs[iy]);
     }
-    auto C2b = C2, C3b = C3, eTrb = eTr;
+    std::vector<EtJob> jobs;
     for (int iy = 0; iy < LY; ++iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C3b[k], C2b[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
-      eTr[l] = next_et(eTrb[k], rot(k, 0), PUs[iy], PLs[dn]);
-      eTr[i] = next_et(eTrb[j], rot(j, 0), PUs[up], PLs[iy]);
+      next_ctm(C3[k], C2[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
+      jobs.push_back({l, k, k, iy, dn});
+      jobs.push_back({i, j, j, up, iy});
     }
+    for (const EtJob& b : final_jobs(jobs)) next_et(eTr[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
   }
 
   void top_move(int iy) {
@@ -709,14 +750,15 @@ struct EngineT final : Engine {
         proj_updown(C2[j], C3[k], C4[l], C1[i], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j],
                     rot(j, 1), rot(k, 1), rot(l, 1), rot(i, 1), PUs[ix], PLs[ix]);
     }
-    auto C1b = C1, C2b = C2, eTtb = eTt;
+    std::vector<EtJob> jobs;
     for (int ix = 0; ix < LX; ++ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C2b[j], C1b[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
-      eTt[k] = next_et(eTtb[j], rot(j, 1), PUs[ix], PLs[rt]);
-      eTt[l] = next_et(eTtb[i], rot(i, 1), PUs[lf], PLs[ix]);
+      next_ctm(C2[j], C1[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
+      jobs.push_back({k, j, j, ix, rt});
+      jobs.push_back({l, i, i, lf, ix});
     }
+    for (const EtJob& b : final_jobs(jobs)) next_et(eTt[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
   }
 
   void bottom_move(int iy) {
@@ -732,23 +774,24 @@ struct EngineT final : Engine {
         proj_updown(C4[l], C1[i], C2[j], C3[k], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l],
                     rot(l, 2), rot(i, 2), rot(j, 2), rot(k, 2), PUs[ix], PLs[ix]);
     }
-    auto C3b = C3, C4b = C4, eTbb = eTb;
+    std::vector<EtJob> jobs;
     for (int ix = 0; ix < LX; ++ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C4b[l], C3b[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
-      eTb[i] = next_et(eTbb[l], rot(l, 2), PUs[ix], PLs[lf]);
-      eTb[j] = next_et(eTbb[k], rot(k, 2), PUs[rt], PLs[ix]);
+      next_ctm(C4[l], C3[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
+      jobs.push_back({i, l, l, ix, lf});
+      jobs.push_back({j, k, k, rt, ix});
     }
+    for (const EtJob& b : final_jobs(jobs)) next_et(eTb[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
   }
 
   // ------------------------------------------------------ initialisation
-  DT<T> fit(const DT<T>& X, int64_t d1, int64_t d2, int64_t rest) {
+  // zero-pad / slice X to the static environment shape, into `out`'s storage
+  void fit(const DT<T>& X, int64_t d1, int64_t d2, int64_t rest, DT<T>& out) {
     const int64_t chi = P.chi;
     Shape s = rest == 1 ? Shape{chi, chi} : Shape{chi, chi, X.dim(4), X.dim(5)};
-    DT<T> out(s, st);
+    if (s != out.sh) fail(TG_E_RUNTIME, "environment initialisation: shape mismatch");
     fit_chi<T>(X.p, d1, d2, rest, out.p, chi, st);
-    return out;
   }
 
   void ctm_init() override {
@@ -756,35 +799,35 @@ struct EngineT final : Engine {
       int num = lat.top(lat.left(i));
       const DT<T>* t = &Tn[num];
       DT<T> X = tr(td(*t, *t, {0, 1, 4}, {0, 1, 4}, false, true), {1, 3, 0, 2});
-      C[0][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1, C[0][i]);
       num = lat.top(lat.right(i));
       t = &Tn[num];
       X = tr(td(*t, *t, {1, 2, 4}, {1, 2, 4}, false, true), {0, 2, 1, 3});
-      C[1][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1, C[1][i]);
       num = lat.bottom(lat.right(i));
       t = &Tn[num];
       X = tr(td(*t, *t, {2, 3, 4}, {2, 3, 4}, false, true), {1, 3, 0, 2});
-      C[2][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1, C[2][i]);
       num = lat.bottom(lat.left(i));
       t = &Tn[num];
       X = tr(td(*t, *t, {0, 3, 4}, {0, 3, 4}, false, true), {1, 3, 0, 2});
-      C[3][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1);
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), 1, C[3][i]);
       num = lat.top(i);
       t = &Tn[num];
       X = tr(td(*t, *t, {1, 4}, {1, 4}, false, true), {0, 3, 1, 4, 2, 5});
-      E[0][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5), E[0][i]);
       num = lat.right(i);
       t = &Tn[num];
       X = tr(td(*t, *t, {2, 4}, {2, 4}, false, true), {1, 4, 2, 5, 0, 3});
-      E[1][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5), E[1][i]);
       num = lat.bottom(i);
       t = &Tn[num];
       X = tr(td(*t, *t, {3, 4}, {3, 4}, false, true), {2, 5, 0, 3, 1, 4});
-      E[2][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5), E[2][i]);
       num = lat.left(i);
       t = &Tn[num];
       X = tr(td(*t, *t, {0, 4}, {0, 4}, false, true), {2, 5, 0, 3, 1, 4});
-      E[3][i] = fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5));
+      fit(X, X.dim(0) * X.dim(1), X.dim(2) * X.dim(3), X.dim(4) * X.dim(5), E[3][i]);
     }
     env_ready = true;
     spec_old = spectra();
@@ -813,6 +856,7 @@ struct EngineT final : Engine {
 
   void sweep_impl() {
     PrecScope prec(this, abs_prec);
+    noise_stream = 0;  // the same perturbation keys in every sweep, eager or replayed
     const int LX = lat.LX_noskew, LY = lat.LY_noskew;
     for (int ix = 0; ix < LX; ++ix) left_move(ix);
     for (int ix = 0; ix > -LX; --ix) right_move((ix + 1 + LX) % LX);
@@ -820,9 +864,104 @@ struct EngineT final : Engine {
     for (int iy = 0; iy < LY; ++iy) bottom_move(iy);
   }
 
+  // ------------------------------------------------ CUDA-graph sweep
+  //
+  // With rSVD corner projectors a sweep has no host synchronisation and all
+  // shapes are static (the environment is kept at chi), so one sweep is
+  // captured into a CUDA graph and replayed: ~4000 launches become one
+  // graph launch.  The graph bakes in the addresses of the site tensors,
+  // their rotations and the environment; it is re-captured when any of them
+  // changes.  The first sweep after a change runs eagerly (it also fixes the
+  // kernels' shared-memory attributes), the second is captured.
+  cudaGraphExec_t g_exec = nullptr;
+  std::vector<const void*> g_addr;
+  uint64_t g_kernels = 0;
+  bool g_warm = false, g_broken = false;
+
+  std::vector<const void*> state_addresses() {
+    std::vector<const void*> a;
+    for (int i = 0; i < lat.N; ++i) {
+      a.push_back(Tn[i].p);
+      for (int w = 0; w < 3; ++w) a.push_back(rot(i, w).p);
+      for (int k = 0; k < 4; ++k) {
+        a.push_back(C[k][i].p);
+        a.push_back(E[k][i].p);
+      }
+    }
+    a.push_back(reinterpret_cast<const void*>(static_cast<intptr_t>(abs_prec)));
+    return a;
+  }
+
+  bool graph_capable() const {
+    if (!P.cuda_graph || g_broken || !P.use_rsvd || !P.projector_corner || profile_enabled()) return false;
+    for (int i = 0; i < lat.N; ++i)
+      for (int l = 0; l < 4; ++l)
+        if (lat.vdim[i][l] == 1) return false;  // D = 1 legs can select the full-SVD branch
+    return true;
+  }
+
+  void drop_graph() {
+    if (g_exec) cudaGraphExecDestroy(g_exec);
+    g_exec = nullptr;
+    g_addr.clear();
+    g_warm = false;
+  }
+
+  void capture_sweep() {
+    drop_graph();
+    const uint64_t before = launch_count();
+    TG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+      sweep_impl();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      g_broken = true;  // eager sweeps from now on
+      uncount_launch(launch_count() - before);
+      return;
+    }
+    TG_CUDA(cudaStreamEndCapture(st, &g));
+    g_kernels = launch_count() - before;
+    uncount_launch(g_kernels);  // recorded, not run
+    const cudaError_t e = cudaGraphInstantiate(&g_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      g_exec = nullptr;
+      g_broken = true;
+      return;
+    }
+    g_addr = state_addresses();
+  }
+
+  void run_sweep() {
+    if (!graph_capable()) {
+      sweep_impl();
+      return;
+    }
+    const std::vector<const void*> addr = state_addresses();  // also refreshes the rotations
+    if (!g_exec || addr != g_addr) {
+      if (g_exec) drop_graph();
+      if (!g_warm) {
+        sweep_impl();
+        g_warm = true;
+        return;
+      }
+      capture_sweep();
+      if (!g_exec) {
+        sweep_impl();
+        return;
+      }
+    }
+    TG_CUDA(cudaGraphLaunch(g_exec, st));
+    count_launch(g_kernels);
+  }
+
   void ctm_sweep() override {
     require_env();
-    sweep_impl();
+    run_sweep();
     check_infos();
     TG_CUDA(cudaStreamSynchronize(st));
   }
@@ -877,7 +1016,7 @@ struct EngineT final : Engine {
     int count = 0, conv = 0;
     double smax = 0.0;
     while (!conv && count < P.max_ctm_iteration) {
-      sweep_impl();
+      run_sweep();
       check_convergence(&conv, &smax);
       ++count;
     }
@@ -1620,10 +1759,7 @@ struct EngineT final : Engine {
     return which < 4 ? C[which][site] : E[which - 4][site];
   }
   void set_env(int which, int site, const double* host) override {
-    DT<T>& t = env_ref(which, site);
-    DT<T> n(t.sh, st);
-    upload(n, host);
-    t = n;
+    upload(env_ref(which, site), host);  // into the existing storage (captured sweeps hold its address)
     env_ready = true;
     spec_old_ok = false;
   }

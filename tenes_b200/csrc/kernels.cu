@@ -16,6 +16,7 @@ namespace tg {
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launch(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {
@@ -524,12 +525,12 @@ __global__ void maxabs_kernel(const T* __restrict__ x, int64_t n, unsigned long 
 }
 
 template <typename T>
-__global__ void divide_kernel(T* __restrict__ x, int64_t n, const unsigned long long* mx) {
+__global__ void divide_kernel(const T* x, T* out, int64_t n, const unsigned long long* mx) {
   const double m = __longlong_as_double(static_cast<long long>(*mx));
   const double inv = 1.0 / m;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    x[i] = mul_real(x[i], inv);
+    out[i] = mul_real(x[i], inv);
 }
 
 template <typename T>
@@ -1222,13 +1223,13 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
 }
 
 template <typename T>
-void normalize_max_abs(T* x, int64_t n, unsigned long long* scratch, cudaStream_t st) {
+void normalize_max_abs(const T* x, T* out, int64_t n, unsigned long long* scratch, cudaStream_t st) {
   ProfScope ps(PK_NORMALIZE, st, 0.0, 3.0 * sizeof(T) * static_cast<double>(n));
   TG_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), st));
   const int nb = num_blocks(n, 256, 148 * 4);
   maxabs_kernel<T><<<nb, 256, 0, st>>>(x, n, scratch);
   TG_CHECK_LAUNCH();
-  divide_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(x, n, scratch);
+  divide_kernel<T><<<num_blocks(n, 256), 256, 0, st>>>(x, out, n, scratch);
   TG_CHECK_LAUNCH();
   count_launch(2);
 }
@@ -1410,7 +1411,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   template void gemm<T>(const T*, const T*, T*, const GemmDesc&, cudaStream_t);                  \
   template void permute<T>(const T*, T*, const Shape&, const std::vector<int>&, bool,            \
                            cudaStream_t);                                                        \
-  template void normalize_max_abs<T>(T*, int64_t, unsigned long long*, cudaStream_t);            \
+  template void normalize_max_abs<T>(const T*, T*, int64_t, unsigned long long*, cudaStream_t);            \
   template void fit_chi<T>(const T*, int64_t, int64_t, int64_t, T*, int64_t, cudaStream_t);      \
   template void scale_cols<T>(const T*, int64_t, int64_t, int, const double*, bool, T*,          \
                               cudaStream_t);                                                     \

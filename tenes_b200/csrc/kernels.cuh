@@ -25,10 +25,10 @@ template <typename T>
 void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>& perm, bool conj,
              cudaStream_t st);
 
-// x /= max_i |x_i|  (the max_abs normalisation of ctm.cpp:514-517, 550-551).
-// `scratch` holds one uint64 on the device.
+// out = x / max_i |x_i|  (the max_abs normalisation of ctm.cpp:514-517,
+// 550-551); out may be x.  `scratch` holds one uint64 on the device.
 template <typename T>
-void normalize_max_abs(T* x, int64_t n, unsigned long long* scratch, cudaStream_t st);
+void normalize_max_abs(const T* x, T* out, int64_t n, unsigned long long* scratch, cudaStream_t st);
 
 // out(chi, chi, r...) = zero-padded / sliced in(d1, d2, r...)  (extend / slice
 // of the environment initialisation, ctm.cpp:998-1012).

@@ -43,6 +43,7 @@ class CTMParams:
     rsvd_seed: int = 0
     inverse_lambda_cut: float = 1e-12
     mixed: bool = False
+    cuda_graph: bool = True
 
     def to_c(self) -> _lib.Params:
         p = _lib.Params()

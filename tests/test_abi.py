@@ -35,6 +35,7 @@ def test_params_default_matches_reference():
     assert p.inverse_projector_cut == 1e-12 and p.ctm_convergence_epsilon == 1e-6
     assert p.projector_corner == 1 and p.use_rsvd == 0 and p.rsvd_oversampling_factor == 2.0
     assert p.inverse_lambda_cut == 1e-12
+    assert p.mixed == 0 and p.cuda_graph == 1
     assert lib.tg_version().decode().startswith("tenes_gpu")
 
 

@@ -160,3 +160,34 @@ def test_rsvd_single_move_matches_oracle(is_complex):
         for i in range(lat.N_UNIT):
             np.testing.assert_allclose(np.abs(ge.get_env(w, i)), np.abs(getattr(oe, name)[i]), rtol=1e-8,
                                        atol=1e-10, err_msg=f"{name}[{i}]")
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_graph_sweeps_equal_eager_sweeps(is_complex):
+    """Sweeps replayed from the captured CUDA graph give the same environment as
+    sweeps launched kernel by kernel, re-capture after the site tensors change,
+    and count the same kernels."""
+    from tenes_b200.env import kernel_launch_count
+    lat = make_lattice(2, 2, 2)
+    Tn = physical_tensors(lat, 2, is_complex=is_complex)
+    kw = dict(use_rsvd=True, rsvd_oversample_abs=4, rsvd_power_iters=2, max_ctm_iteration=5,
+              ctm_convergence_epsilon=1e-30)
+    envs = {g: gpu_env(lat, Tn, 8, is_complex, cuda_graph=g, **kw) for g in (False, True)}
+    counts = {}
+    for g, e in envs.items():
+        e.init_env()
+        n0 = kernel_launch_count()
+        for _ in range(5):
+            e.sweep()
+        counts[g] = kernel_launch_count() - n0
+    assert counts[True] == counts[False] > 0
+    for rnd in range(2):
+        for w in range(8):
+            for i in range(lat.N_UNIT):
+                a, b = envs[False].get_env(w, i), envs[True].get_env(w, i)
+                np.testing.assert_allclose(b, a, rtol=0, atol=1e-13 * np.abs(a).max())
+        if rnd == 0:
+            for e in envs.values():
+                e.set_site_tensor(0, Tn[1] if Tn[1].shape == Tn[0].shape else Tn[0])
+                for _ in range(3):
+                    e.sweep()
