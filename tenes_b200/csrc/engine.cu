@@ -52,7 +52,18 @@ struct EngineT final : Engine {
   DT<double> spec_old;
   bool spec_old_ok = false;
 
-  unsigned long long* d_max = nullptr;
+  // The rows of a move are independent (ctm.cpp:577-593, 603-615): with rSVD
+  // projectors each row runs on its own stream, forked from and joined back
+  // into `st` with events (inside a captured sweep these become parallel
+  // branches of the graph).  `st` and `slot` name the stream in use; every
+  // stream slot has its own device scratch.
+  static constexpr int kRowStreams = 4;
+  cudaStream_t main_st = nullptr;
+  cudaStream_t row_st[kRowStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kRowStreams] = {};
+  int slot = 0;  // 0: main stream, 1..kRowStreams: row streams
+
+  unsigned long long* d_max = nullptr;  // one per stream slot
   static constexpr int kInfoSlots = 4096;
   int* d_info = nullptr;  // one slot per cuSOLVER call, checked at sync points
   int info_used = 0;
@@ -85,12 +96,18 @@ struct EngineT final : Engine {
     TG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     check_sol(cusolverDnCreate(&sol), "cusolverDnCreate");
     check_sol(cusolverDnSetStream(sol, st), "cusolverDnSetStream");
-    TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long)));
+    main_st = st;
+    for (int r = 0; r < kRowStreams; ++r) {
+      TG_CUDA(cudaStreamCreateWithFlags(&row_st[r], cudaStreamNonBlocking));
+      TG_CUDA(cudaEventCreateWithFlags(&ev_join[r], cudaEventDisableTiming));
+    }
+    TG_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long) * (kRowStreams + 1)));
     TG_CUDA(cudaMalloc(&d_info, sizeof(int) * kInfoSlots));
     TG_CUDA(cudaMemset(d_info, 0, sizeof(int) * kInfoSlots));
     TG_CUDA(cudaMalloc(&d_flag, sizeof(int)));
     TG_CUDA(cudaMemset(d_flag, 0, sizeof(int)));
-    TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * 4));
+    TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * (kRowStreams + 1)));
     TG_CUDA(cudaMalloc(&d_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_sig, sizeof(double) * 4 * lat.N));
@@ -138,6 +155,11 @@ struct EngineT final : Engine {
     cudaFree(d_ptrs);
     cudaFreeHost(h_ptrs);
     cudaFreeHost(h_sig);
+    for (int r = 0; r < kRowStreams; ++r) {
+      if (row_st[r]) cudaStreamDestroy(row_st[r]);
+      if (ev_join[r]) cudaEventDestroy(ev_join[r]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -158,12 +180,55 @@ struct EngineT final : Engine {
     return tensordot<T>(a, b, x, y, st, ca, cb, cur_prec);
   }
   DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
-  void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.p, a.size(), d_max, st); }
+  void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.p, a.size(), d_max + slot, st); }
   // dst = a / max|a|, written into the existing storage of dst
   void normalize_into(const DT<T>& a, DT<T>& dst) {
     if (dst.size() != a.size()) fail(TG_E_RUNTIME, "normalize_into: size mismatch");
-    normalize_max_abs<T>(a.p, dst.p, a.size(), d_max, st);
+    normalize_max_abs<T>(a.p, dst.p, a.size(), d_max + slot, st);
   }
+
+  // Run body(r) for r = 0 .. n-1, row r on row stream r % kRowStreams when
+  // `parallel`, else in order on the current stream.  Tensors that a row
+  // creates and that outlive it must be handed to `st` with keep() before
+  // they are released, so that their release is ordered after every row.
+  template <typename F>
+  void for_rows(int n, bool parallel, F&& body) {
+    if (!parallel || n < 2) {
+      for (int r = 0; r < n; ++r) body(r);
+      return;
+    }
+    const int ns = std::min(n, kRowStreams);
+    TG_CUDA(cudaEventRecord(ev_fork, st));
+    for (int s = 0; s < ns; ++s) TG_CUDA(cudaStreamWaitEvent(row_st[s], ev_fork, 0));
+    cudaStream_t saved = st;
+    const int saved_slot = slot;
+    auto join = [&]() {
+      st = saved;
+      slot = saved_slot;
+      for (int s = 0; s < ns; ++s) {
+        cudaEventRecord(ev_join[s], row_st[s]);
+        cudaStreamWaitEvent(st, ev_join[s], 0);
+      }
+    };
+    try {
+      for (int r = 0; r < n; ++r) {
+        st = row_st[r % ns];
+        slot = 1 + r % ns;
+        body(r);
+      }
+    } catch (...) {
+      join();
+      throw;
+    }
+    join();
+    TG_CUDA(cudaGetLastError());
+  }
+  // release `v`'s storage in stream order on `st` (after a join)
+  void keep(std::vector<DT<T>>& v) {
+    for (auto& t : v)
+      if (t.mem) t.mem->st = st;
+  }
+  bool rows_parallel() const { return graph_capable(); }
 
   void upload(DT<T>& t, const double* host) {
     TG_CUDA(cudaMemcpyAsync(t.p, host, sizeof(T) * t.size(), cudaMemcpyHostToDevice, st));
@@ -203,6 +268,9 @@ struct EngineT final : Engine {
       rot_ok[site] = true;
     }
     return Trot[site][which];
+  }
+  void prepare_rotations() {
+    for (int i = 0; i < lat.N; ++i) rot(i, 0);
   }
 
   // Singular value decomposition of a row-major m x n matrix A (consumed):
@@ -483,9 +551,14 @@ struct EngineT final : Engine {
   // directions into independent ones, which the following shifted pass and
   // two plain passes orthonormalise.  The perturbation moves the span by
   // ~1e-14, below the rounding of the products that produced the panel.
-  void orth_chol(DT<T>& Y, int64_t n, int64_t k) {
+  //
+  // passes = 4: two shifted and two plain passes, orthonormal to O(u).
+  // passes = 2: the two shifted passes only, a basis of the same span with
+  // condition number ~1e4 -- enough for the intermediate bases of the power
+  // iteration, whose next product and orthonormalisation only use the span.
+  void orth_chol(DT<T>& Y, int64_t n, int64_t k, int passes = 4) {
     PrecScope fp64(this, 0);
-    for (int pass = 0; pass < 4; ++pass) {
+    for (int pass = 0; pass < passes; ++pass) {
       int nparts = 0;
       DT<T> parts = gram_parts(Y, n, k, &nparts);
       DT<T> G({k, k}, st);
@@ -518,12 +591,12 @@ struct EngineT final : Engine {
     DT<T> Om({k, ncol}, st);
     counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
     DT<T> Q = apply_M(Om);
-    orth_chol(Q, nrow, k);
+    orth_chol(Q, nrow, k, P.rsvd_power_iters > 0 ? 2 : 4);
     for (int it = 0; it < P.rsvd_power_iters; ++it) {
       DT<T> Z = apply_MH(Q);
-      orth_chol(Z, ncol, k);
+      orth_chol(Z, ncol, k, 2);
       Q = apply_M(Z);
-      orth_chol(Q, nrow, k);
+      orth_chol(Q, nrow, k, it + 1 < P.rsvd_power_iters ? 2 : 4);
     }
     // B = Q^H M = Z^H with Z = M^H Q.  With Qz an orthonormal basis of
     // range(Z), B = (Z^H Qz) Qz^H, so the SVD of the k x k matrix T = Z^H Qz,
@@ -540,7 +613,7 @@ struct EngineT final : Engine {
     DT<T> V = mm_rm(cm(Qz.p, ncol, k), rm(Wr.p, k, k));
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
     DT<double> sinv({w}, st);
-    truncation(s.p, k, cut, P.inverse_projector_cut, sinv.p, w, d_cut, st);
+    truncation(s.p, k, cut, P.inverse_projector_cut, sinv.p, w, d_cut + slot, st);
     Uc = DT<T>({nrow, w}, st);
     scale_cols<T>(U.p, k, nrow, w, sinv.p, false, Uc.p, st);
     Vc = DT<T>({ncol, w}, st);
@@ -556,7 +629,7 @@ struct EngineT final : Engine {
     const int64_t k = std::min(nrow, ncol);
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
     DT<double> sinv({w}, st);
-    truncation(s.p, k, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut, st);
+    truncation(s.p, k, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut + slot, st);
     Uc = DT<T>({nrow, w}, st);
     scale_cols<T>(U.p, k, nrow, w, sinv.p, false, Uc.p, st);
     VTc = DT<T>({w, ncol}, st);
@@ -693,96 +766,143 @@ struct EngineT final : Engine {
     auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
     const int LY = lat.LY_noskew;
+    const bool par = rows_parallel();
     std::vector<DT<T>> PUs(LY), PLs(LY);
-    for (int iy = 0; iy < LY; ++iy) {
+    for_rows(LY, par, [&](int iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       if (P.projector_corner)
         proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
       else
         proj_updown(C1[i], C2[j], C3[k], C4[l], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i],
                     Tn[i], Tn[j], Tn[k], Tn[l], PUs[iy], PLs[iy]);
-    }
+    });
     std::vector<EtJob> jobs;
     for (int iy = 0; iy < LY; ++iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C1[i], C4[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
       jobs.push_back({j, i, i, iy, up});
       jobs.push_back({k, l, l, dn, iy});
     }
-    for (const EtJob& b : final_jobs(jobs)) next_et(eTl[b.src], Tn[b.site], PUs[b.pu], PLs[b.pl], eTl[b.out]);
+    const std::vector<EtJob> fin = final_jobs(jobs);
+    for_rows(LY, par, [&](int iy) {
+      const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
+      const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
+      next_ctm(C1[i], C4[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
+      for (size_t q = iy; q < fin.size(); q += LY) {
+        const EtJob& b = fin[q];
+        next_et(eTl[b.src], Tn[b.site], PUs[b.pu], PLs[b.pl], eTl[b.out]);
+      }
+    });
+    keep(PUs);
+    keep(PLs);
   }
 
   void right_move(int ix) {
     auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
     const int LY = lat.LY_noskew;
+    const bool par = rows_parallel();
+    prepare_rotations();  // before the rows fork
     std::vector<DT<T>> PUs(LY), PLs(LY);
-    for (int iy = 0; iy < LY; ++iy) {
+    for_rows(LY, par, [&](int iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       if (P.projector_corner)
         proj_left_block(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], rot(k, 0), rot(j, 0), PUs[iy], PLs[iy]);
       else
         proj_updown(C3[k], C4[l], C1[i], C2[j], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k],
                     rot(k, 0), rot(l, 0), rot(i, 0), rot(j, 0), PUs[iy], PLs[iy]);
-    }
+    });
     std::vector<EtJob> jobs;
     for (int iy = 0; iy < LY; ++iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C3[k], C2[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
       jobs.push_back({l, k, k, iy, dn});
       jobs.push_back({i, j, j, up, iy});
     }
-    for (const EtJob& b : final_jobs(jobs)) next_et(eTr[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
+    const std::vector<EtJob> fin = final_jobs(jobs);
+    for_rows(LY, par, [&](int iy) {
+      const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
+      const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
+      next_ctm(C3[k], C2[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
+      for (size_t q = iy; q < fin.size(); q += LY) {
+        const EtJob& b = fin[q];
+        next_et(eTr[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
+      }
+    });
+    keep(PUs);
+    keep(PLs);
   }
 
   void top_move(int iy) {
     auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
     const int LX = lat.LX_noskew;
+    const bool par = rows_parallel();
+    prepare_rotations();
     std::vector<DT<T>> PUs(LX), PLs(LX);
-    for (int ix = 0; ix < LX; ++ix) {
+    for_rows(LX, par, [&](int ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       if (P.projector_corner)
         proj_left_block(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], rot(j, 1), rot(i, 1), PUs[ix], PLs[ix]);
       else
         proj_updown(C2[j], C3[k], C4[l], C1[i], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j],
                     rot(j, 1), rot(k, 1), rot(l, 1), rot(i, 1), PUs[ix], PLs[ix]);
-    }
+    });
     std::vector<EtJob> jobs;
     for (int ix = 0; ix < LX; ++ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C2[j], C1[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
       jobs.push_back({k, j, j, ix, rt});
       jobs.push_back({l, i, i, lf, ix});
     }
-    for (const EtJob& b : final_jobs(jobs)) next_et(eTt[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
+    const std::vector<EtJob> fin = final_jobs(jobs);
+    for_rows(LX, par, [&](int ix) {
+      const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
+      const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
+      next_ctm(C2[j], C1[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
+      for (size_t q = ix; q < fin.size(); q += LX) {
+        const EtJob& b = fin[q];
+        next_et(eTt[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
+      }
+    });
+    keep(PUs);
+    keep(PLs);
   }
 
   void bottom_move(int iy) {
     auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
     const int LX = lat.LX_noskew;
+    const bool par = rows_parallel();
+    prepare_rotations();
     std::vector<DT<T>> PUs(LX), PLs(LX);
-    for (int ix = 0; ix < LX; ++ix) {
+    for_rows(LX, par, [&](int ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       if (P.projector_corner)
         proj_left_block(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], rot(l, 2), rot(k, 2), PUs[ix], PLs[ix]);
       else
         proj_updown(C4[l], C1[i], C2[j], C3[k], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l],
                     rot(l, 2), rot(i, 2), rot(j, 2), rot(k, 2), PUs[ix], PLs[ix]);
-    }
+    });
     std::vector<EtJob> jobs;
     for (int ix = 0; ix < LX; ++ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C4[l], C3[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
       jobs.push_back({i, l, l, ix, lf});
       jobs.push_back({j, k, k, rt, ix});
     }
-    for (const EtJob& b : final_jobs(jobs)) next_et(eTb[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
+    const std::vector<EtJob> fin = final_jobs(jobs);
+    for_rows(LX, par, [&](int ix) {
+      const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
+      const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
+      next_ctm(C4[l], C3[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
+      for (size_t q = ix; q < fin.size(); q += LX) {
+        const EtJob& b = fin[q];
+        next_et(eTb[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
+      }
+    });
+    keep(PUs);
+    keep(PLs);
   }
 
   // ------------------------------------------------------ initialisation

@@ -1005,7 +1005,7 @@ __global__ void sum_partials_kernel(const T* __restrict__ parts, int nparts, int
 // triangular inverse, each k steps with the trailing work spread over the CTA.
 // See chol_rinv() in kernels.cuh.
 template <typename T, bool CPLX>
-__global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ parts, int nparts, int k,
+__global__ void __launch_bounds__(1024) chol_rinv_kernel(const T* __restrict__ parts, int nparts, int k,
                                                          double shift, T* __restrict__ Rinv, int* flag) {
   extern __shared__ double sm[];
   const int kk = k * k;
@@ -1014,6 +1014,7 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
   double* xr = sm + (CPLX ? 2 : 1) * kk;    // X = R'^{-1} (upper), row-major
   double* xi = xr + kk;                     // complex only
   double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration D
+  double* rs = d + k;                       // 1 / sqrt of the Cholesky pivots
   const int tid = threadIdx.x, nt = blockDim.x;
   const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
   for (int idx = tid; idx < kk; idx += nt) {
@@ -1040,21 +1041,20 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
     if constexpr (CPLX) xi[idx] = 0.0;
   }
   __syncthreads();
-  // Cholesky, right-looking on the upper triangle
+  // Cholesky on the upper triangle, one barrier per step: step j subtracts
+  // conj(A'_jr) A'_jc / A'_jj from the trailing rows r > j (row j itself is
+  // left unscaled and only read); the rows are scaled by 1/sqrt(A'_jj) at
+  // the end.  Warps over rows, lanes over columns.
   for (int j = 0; j < k; ++j) {
     const double a = ar[j * k + j];
-    const double piv = (a > 0.0) ? sqrt(a) : 1.0;
-    if (!(a > 0.0) && tid == 0 && flag) atomicExch(flag, 1);
-    __syncthreads();  // everyone has read A'_jj
-    for (int c = j + tid; c < k; c += nt) {
-      ar[j * k + c] /= piv;
-      if constexpr (CPLX) ai[j * k + c] /= piv;
+    if (!(a > 0.0)) {
+      if (tid == 0 && flag) atomicExch(flag, 1);
+      continue;  // same decision in every thread: the row stays as it is
     }
-    __syncthreads();
-    // A'_rc -= conj(R'_jr) R'_jc for j < r <= c: warps over rows, lanes over columns
+    const double inv_a = 1.0 / a;
     for (int r = j + 1 + warp; r < k; r += nwarp) {
-      const double ur = ar[j * k + r];
-      const double ui = CPLX ? ai[j * k + r] : 0.0;
+      const double ur = ar[j * k + r] * inv_a;
+      const double ui = CPLX ? ai[j * k + r] * inv_a : 0.0;
       for (int c = r + lane; c < k; c += 32) {
         const double vr = ar[j * k + c];
         if constexpr (CPLX) {
@@ -1068,17 +1068,27 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
     }
     __syncthreads();
   }
-  // X = R'^{-1}: for i = k-1 .. 0: X[i,:] /= R'_ii; X[r,:] -= R'_ri X[i,:] (r < i)
-  for (int i = k - 1; i >= 0; --i) {
+  // R'_jc = A'_jc / sqrt(A'_jj) (a non-positive pivot counts as 1)
+  for (int i = tid; i < k; i += nt) {
+    const double a = ar[i * k + i];
+    rs[i] = (a > 0.0) ? 1.0 / sqrt(a) : 1.0;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kk; idx += nt) {
+    const int r = idx / k, c = idx - r * k;
+    if (c < r) continue;
+    ar[idx] *= rs[r];
+    if constexpr (CPLX) ai[idx] *= rs[r];
+  }
+  __syncthreads();
+  // X = R'^{-1} by backward substitution, one barrier per step: once row i of
+  // the accumulator is final, X[i,:] = acc[i,:] / R'_ii and every row r < i
+  // takes off R'_ri X[i,:]; rows are divided by their diagonal at the end.
+  for (int i = k - 1; i > 0; --i) {
     const double inv = 1.0 / ar[i * k + i];
-    for (int c = i + tid; c < k; c += nt) {
-      xr[i * k + c] *= inv;
-      if constexpr (CPLX) xi[i * k + c] *= inv;
-    }
-    __syncthreads();
     for (int r = warp; r < i; r += nwarp) {  // rows above i, columns i .. k-1
-      const double rr = ar[r * k + i];
-      const double ri = CPLX ? ai[r * k + i] : 0.0;
+      const double rr = ar[r * k + i] * inv;
+      const double ri = CPLX ? ai[r * k + i] * inv : 0.0;
       for (int c = i + lane; c < k; c += 32) {
         const double x_r = xr[i * k + c];
         if constexpr (CPLX) {
@@ -1092,14 +1102,15 @@ __global__ void __launch_bounds__(512) chol_rinv_kernel(const T* __restrict__ pa
     }
     __syncthreads();
   }
-  // Rinv = D X (upper)
+  // Rinv = D X (upper), X[r,:] = acc[r,:] / R'_rr
   for (int idx = tid; idx < kk; idx += nt) {
     const int r = idx / k, c = idx - r * k;
     const bool up = c >= r;
+    const double s = d[r] / ar[r * k + r];
     if constexpr (CPLX) {
-      Rinv[idx] = make_double2(up ? xr[idx] * d[r] : 0.0, up ? xi[idx] * d[r] : 0.0);
+      Rinv[idx] = make_double2(up ? xr[idx] * s : 0.0, up ? xi[idx] * s : 0.0);
     } else {
-      Rinv[idx] = up ? xr[idx] * d[r] : 0.0;
+      Rinv[idx] = up ? xr[idx] * s : 0.0;
     }
   }
 }
@@ -1383,7 +1394,7 @@ template <typename T>
 void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st) {
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
-  const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k);
+  const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + 2 * k);
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
     TG_CUDA(cudaFuncSetAttribute(chol_rinv_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1395,7 +1406,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   const double u = 1.1102230246251565e-16;
   const double s = shift ? 11.0 * (static_cast<double>(n) * k + static_cast<double>(k) * (k + 1)) * u * k : 0.0;
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * static_cast<double>(k) * k * k / 3.0, 0.0);
-  chol_rinv_kernel<T, CPLX><<<1, 512, smem, st>>>(parts, nparts, static_cast<int>(k), s, Rinv, flag);
+  chol_rinv_kernel<T, CPLX><<<1, 1024, smem, st>>>(parts, nparts, static_cast<int>(k), s, Rinv, flag);
   TG_CHECK_LAUNCH();
   count_launch();
 }
