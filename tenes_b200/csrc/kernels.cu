@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <numeric>
 #include <vector>
 #include <cmath>
 #include <string>
@@ -503,6 +504,80 @@ __global__ void permute_kernel(const T* __restrict__ in, T* __restrict__ out, Pe
   }
 }
 
+// The same gather with 32-bit index arithmetic (total < 2^31), for
+// permutations that keep the innermost axis innermost: consecutive threads
+// read consecutive elements within each contiguous run.
+struct PermParams32 {
+  int rank;
+  uint32_t total;
+  uint32_t out_dims[kMaxRank];
+  uint32_t src_stride[kMaxRank];
+  bool conj;
+};
+
+template <typename T>
+__global__ void permute32_kernel(const T* __restrict__ in, T* __restrict__ out, PermParams32 p) {
+  for (uint32_t lin = blockIdx.x * blockDim.x + threadIdx.x; lin < p.total; lin += gridDim.x * blockDim.x) {
+    uint32_t rem = lin, off = 0;
+    for (int i = p.rank - 1; i > 0; --i) {
+      const uint32_t q = rem / p.out_dims[i];
+      off += (rem - q * p.out_dims[i]) * p.src_stride[i];
+      rem = q;
+    }
+    off += rem * p.src_stride[0];
+    const T v = in[off];
+    out[lin] = p.conj ? conj_of(v) : v;
+  }
+}
+
+// Permutations that move the innermost axis: batched 32 x 32 tile
+// transposes through shared memory between input axis b (innermost in the
+// input) and input axis a (innermost in the output), so that reads and
+// writes are both coalesced.  The other axes index the batch of tiles.
+struct TransParams {
+  int nbatch_dims;
+  uint32_t na, nb;                      // extents of axes a and b
+  uint32_t in_a, out_b;                 // input stride of a, output stride of b
+  uint32_t tiles_a, tiles_b, ntiles;    // tiles per batch entry, in total
+  uint32_t bdims[kMaxRank];             // extents of the batch axes
+  uint32_t bin[kMaxRank], bout[kMaxRank];  // their input / output strides
+  bool conj;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) transpose_tiles_kernel(const T* __restrict__ in, T* __restrict__ out,
+                                                              TransParams p) {
+  __shared__ T tile[32][33];
+  for (uint32_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+    uint32_t rem = t / (p.tiles_a * p.tiles_b);
+    const uint32_t tt = t - rem * (p.tiles_a * p.tiles_b);
+    const uint32_t ta = tt / p.tiles_b, tb = tt - ta * p.tiles_b;
+    uint32_t ibase = 0, obase = 0;
+    for (int i = p.nbatch_dims - 1; i >= 0; --i) {
+      const uint32_t q = rem / p.bdims[i];
+      const uint32_t idx = rem - q * p.bdims[i];
+      ibase += idx * p.bin[i];
+      obase += idx * p.bout[i];
+      rem = q;
+    }
+    const uint32_t a0 = ta * 32, b0 = tb * 32;
+    const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    for (uint32_t r = ty; r < 32; r += 8) {  // read rows of a, coalesced along b
+      const uint32_t a = a0 + r, b = b0 + tx;
+      if (a < p.na && b < p.nb) tile[r][tx] = in[ibase + a * p.in_a + b];
+    }
+    __syncthreads();
+    for (uint32_t r = ty; r < 32; r += 8) {  // write rows of b, coalesced along a
+      const uint32_t b = b0 + r, a = a0 + tx;
+      if (a < p.na && b < p.nb) {
+        const T v = tile[tx][r];
+        out[obase + b * p.out_b + a] = p.conj ? conj_of(v) : v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // max |x| then x /= max
 // ---------------------------------------------------------------------------
@@ -823,7 +898,7 @@ __global__ void upper_to_rh_kernel(const T* __restrict__ acm, int64_t lda, int64
 
 // One-sided Jacobi SVD with vectors; see jacobi_svd() in kernels.cuh.
 template <typename T, bool CPLX>
-__global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
                                                           double* __restrict__ S, T* __restrict__ Wout) {
   extern __shared__ double sm[];
   const int nn = n * n;
@@ -849,13 +924,14 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
   const int np = n + (n & 1);
   const double tol = static_cast<double>(n) * 2.220446049250313e-16;
   const double small2 = tol * tol * block_sumsq<CPLX>(ar, ai, nn);  // rounding-noise columns
-  // each column pair is handled by a group of 8 lanes (4 pairs per warp)
-  const int grp = lane >> 3, gl = lane & 7;
+  // each column pair is handled by a group of kJG lanes (32 / kJG pairs per warp)
+  constexpr int kJG = 16;
+  const int grp = lane / kJG, gl = lane % kJG;
   for (int sweep = 0; sweep < 60; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
     for (int rnd = 0; rnd < np - 1; ++rnd) {
-      for (int base = warp * 4; base < np / 2; base += nw * 4) {
+      for (int base = warp * (32 / kJG); base < np / 2; base += nw * (32 / kJG)) {
         const int pr = base + grp;
         auto player = [&](int kk) { return kk == 0 ? 0 : ((kk - 1 + rnd) % (np - 1)) + 1; };
         int p = 0, q = 0;
@@ -872,7 +948,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
         }
         double al = 0, be = 0, gr = 0, gi = 0;
         if (valid) {
-          for (int r = gl; r < n; r += 8) {
+          for (int r = gl; r < n; r += kJG) {
             const double pr_ = ar[p * n + r], qr_ = ar[q * n + r];
             al += pr_ * pr_;
             be += qr_ * qr_;
@@ -886,11 +962,11 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
             }
           }
         }
-        for (int o = 4; o > 0; o >>= 1) {  // reduce within the 8-lane group
-          al += __shfl_xor_sync(0xffffffffu, al, o, 8);
-          be += __shfl_xor_sync(0xffffffffu, be, o, 8);
-          gr += __shfl_xor_sync(0xffffffffu, gr, o, 8);
-          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o, 8);
+        for (int o = kJG / 2; o > 0; o >>= 1) {  // reduce within the lane group
+          al += __shfl_xor_sync(0xffffffffu, al, o, kJG);
+          be += __shfl_xor_sync(0xffffffffu, be, o, kJG);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o, kJG);
+          if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o, kJG);
         }
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
         if (!valid || g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
@@ -899,7 +975,7 @@ __global__ void __launch_bounds__(512) jacobi_svd_kernel(const T* __restrict__ A
         const double zeta = (be - al) / (2.0 * g);
         const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
         const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-        for (int r = gl; r < n; r += 8) {
+        for (int r = gl; r < n; r += kJG) {
           {
             const double xpr = ar[p * n + r], xqr = ar[q * n + r];
             const double xpi = CPLX ? ai[p * n + r] : 0.0, xqi = CPLX ? ai[q * n + r] : 0.0;
@@ -1212,23 +1288,120 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
              cudaStream_t st) {
   const int r = static_cast<int>(in_shape.size());
   if (r > kMaxRank) fail(TG_E_INPUT, "permute: rank > " + std::to_string(kMaxRank));
-  PermParams p{};
-  p.rank = r;
+  const int64_t total = numel(in_shape);
+  if (total == 0) return;
+  ProfScope ps(PK_PERMUTE, st, 0.0, 2.0 * sizeof(T) * static_cast<double>(total));
+  // Canonical form: drop unit axes, then merge input axes that stay adjacent
+  // and in order in the output.
+  std::vector<int> newax(static_cast<size_t>(r), -1);
+  std::vector<int64_t> sh;
+  for (int i = 0; i < r; ++i)
+    if (in_shape[i] != 1) {
+      newax[i] = static_cast<int>(sh.size());
+      sh.push_back(in_shape[i]);
+    }
+  std::vector<int> pm;
+  for (int i = 0; i < r; ++i)
+    if (newax[perm[i]] >= 0) pm.push_back(newax[perm[i]]);
+  std::vector<std::vector<int>> groups;  // runs of input axes, in output order
+  for (int a : pm) {
+    if (!groups.empty() && a == groups.back().back() + 1) groups.back().push_back(a);
+    else groups.push_back({a});
+  }
+  std::vector<int> order(groups.size());  // groups sorted by their first input axis
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return groups[x][0] < groups[y][0]; });
+  const int m = static_cast<int>(groups.size());
+  std::vector<int64_t> ms(static_cast<size_t>(m));  // merged input shape
+  std::vector<int> rank_of(static_cast<size_t>(m));
+  for (int q = 0; q < m; ++q) {
+    int64_t e = 1;
+    for (int a : groups[order[q]]) e *= sh[a];
+    ms[q] = e;
+    rank_of[order[q]] = q;
+  }
+  std::vector<int> mp(static_cast<size_t>(m));  // merged permutation
+  for (int g = 0; g < m; ++g) mp[g] = rank_of[g];
+  if (m <= 1) {  // a plain copy
+    if (!conj) {
+      TG_CUDA(cudaMemcpyAsync(out, in, sizeof(T) * static_cast<size_t>(total), cudaMemcpyDeviceToDevice, st));
+      return;
+    }
+  }
+  std::vector<int64_t> istr(static_cast<size_t>(std::max(m, 1))), od(static_cast<size_t>(std::max(m, 1))),
+      ostr(static_cast<size_t>(std::max(m, 1)));
+  std::vector<int> pos(static_cast<size_t>(std::max(m, 1)));
+  {
+    int64_t s = 1;
+    for (int i = m - 1; i >= 0; --i) {
+      istr[i] = s;
+      s *= ms[i];
+    }
+    for (int i = 0; i < m; ++i) {
+      od[i] = ms[mp[i]];
+      pos[mp[i]] = i;
+    }
+    s = 1;
+    for (int i = m - 1; i >= 0; --i) {
+      ostr[i] = s;
+      s *= od[i];
+    }
+  }
+  if (total >= (int64_t{1} << 31)) {
+    PermParams p{};
+    p.rank = m;
+    p.conj = conj;
+    p.total = total;
+    for (int i = 0; i < m; ++i) {
+      p.out_dims[i] = od[i];
+      p.src_stride[i] = istr[mp[i]];
+    }
+    permute_kernel<T><<<num_blocks(total, 256), 256, 0, st>>>(in, out, p);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    return;
+  }
+  const int a = m >= 1 ? mp[m - 1] : 0, b = m - 1;
+  if (m >= 2 && a != b && ms[a] >= 16 && ms[b] >= 16) {
+    TransParams p{};
+    p.conj = conj;
+    p.na = static_cast<uint32_t>(ms[a]);
+    p.nb = static_cast<uint32_t>(ms[b]);
+    p.in_a = static_cast<uint32_t>(istr[a]);
+    p.out_b = static_cast<uint32_t>(ostr[pos[b]]);
+    p.tiles_a = (p.na + 31) / 32;
+    p.tiles_b = (p.nb + 31) / 32;
+    uint64_t nt = static_cast<uint64_t>(p.tiles_a) * p.tiles_b;
+    int nbd = 0;
+    for (int d = 0; d < m; ++d) {
+      if (d == a || d == b) continue;
+      p.bdims[nbd] = static_cast<uint32_t>(ms[d]);
+      p.bin[nbd] = static_cast<uint32_t>(istr[d]);
+      p.bout[nbd] = static_cast<uint32_t>(ostr[pos[d]]);
+      nt *= static_cast<uint64_t>(ms[d]);
+      ++nbd;
+    }
+    p.nbatch_dims = nbd;
+    p.ntiles = static_cast<uint32_t>(nt);
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(nt, 148 * 16));
+    transpose_tiles_kernel<T><<<grid, 256, 0, st>>>(in, out, p);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    return;
+  }
+  PermParams32 p{};
+  p.rank = std::max(m, 1);
   p.conj = conj;
-  p.total = numel(in_shape);
-  if (p.total == 0) return;
-  int64_t strides[kMaxRank];
-  int64_t s = 1;
-  for (int i = r - 1; i >= 0; --i) {
-    strides[i] = s;
-    s *= in_shape[i];
+  p.total = static_cast<uint32_t>(total);
+  if (m == 0) {
+    p.out_dims[0] = 1;
+    p.src_stride[0] = 1;
   }
-  for (int i = 0; i < r; ++i) {
-    p.out_dims[i] = in_shape[perm[i]];
-    p.src_stride[i] = strides[perm[i]];
+  for (int i = 0; i < m; ++i) {
+    p.out_dims[i] = static_cast<uint32_t>(od[i]);
+    p.src_stride[i] = static_cast<uint32_t>(istr[mp[i]]);
   }
-  ProfScope ps(PK_PERMUTE, st, 0.0, 2.0 * sizeof(T) * static_cast<double>(p.total));
-  permute_kernel<T><<<num_blocks(p.total, 256), 256, 0, st>>>(in, out, p);
+  permute32_kernel<T><<<num_blocks(total, 256, 148 * 16), 256, 0, st>>>(in, out, p);
   TG_CHECK_LAUNCH();
   count_launch();
 }
@@ -1368,7 +1541,7 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st) {
     attr_bytes = smem;
   }
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
-  jacobi_svd_kernel<T, CPLX><<<1, 512, smem, st>>>(A, static_cast<int>(k), U, S, W);
+  jacobi_svd_kernel<T, CPLX><<<1, 1024, smem, st>>>(A, static_cast<int>(k), U, S, W);
   TG_CHECK_LAUNCH();
   count_launch();
 }
