@@ -200,6 +200,16 @@ tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flo
  * of the CTMRG path. */
 tg_status tg_bench_gemm(int64_t M, int64_t N, int64_t K, int layout, int prec, int iters, double* avg_ms);
 
+/* One real product C = A B through the library's contraction kernels, with
+ * host buffers and element strides: A(m,k) = A[m*sAm + k*sAk], B(k,n) =
+ * B[k*sBk + n*sBn], C(m,n) = C[m*sCm + n*sCn] (one of each operand's strides
+ * must be 1).  prec 0: FP64 DMMA; 1: 3xTF32 on tcgen05.  The buffers hold
+ * the extents the strides reach.  For tests of the kernels; not part of the
+ * CTMRG path. */
+tg_status tg_gemm_host(int64_t M, int64_t N, int64_t K, const double* A, int64_t sAm, int64_t sAk,
+                       const double* B, int64_t sBk, int64_t sBn, double* C, int64_t sCm, int64_t sCn,
+                       int prec);
+
 /* Allocation-free corner spectra.  No counterpart in the reference: it exists
  * for callers that must not allocate device memory where they need the
  * spectra -- code that runs under a fixed device-memory budget, hosts that

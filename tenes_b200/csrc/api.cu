@@ -241,6 +241,50 @@ tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flo
 // ---------------------------------------------------------------------------
 // Microbenchmark of the contraction kernel on one product shape (device
 // buffers allocated and freed here; not used by the CTMRG path).
+extern "C" tg_status tg_gemm_host(int64_t M, int64_t N, int64_t K, const double* A, int64_t sAm, int64_t sAk,
+                                  const double* B, int64_t sBk, int64_t sBn, double* C, int64_t sCm, int64_t sCn,
+                                  int prec) {
+  return guard([&] {
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C) tg::fail(TG_E_INPUT, "bad gemm arguments");
+    if ((sAm != 1 && sAk != 1) || (sBk != 1 && sBn != 1) || sAm < 1 || sAk < 1 || sBk < 1 || sBn < 1 || sCm < 1 ||
+        sCn < 1)
+      tg::fail(TG_E_INPUT, "gemm: one unit stride per operand required");
+    if (prec != 0 && prec != 1) tg::fail(TG_E_INPUT, "prec must be 0 or 1");
+    const int64_t na = (M - 1) * sAm + (K - 1) * sAk + 1, nb = (K - 1) * sBk + (N - 1) * sBn + 1,
+                  nc = (M - 1) * sCm + (N - 1) * sCn + 1;
+    cudaStream_t st;
+    TG_CUDA(cudaStreamCreate(&st));
+    double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    TG_CUDA(cudaMalloc(&dA, sizeof(double) * na));
+    TG_CUDA(cudaMalloc(&dB, sizeof(double) * nb));
+    TG_CUDA(cudaMalloc(&dC, sizeof(double) * nc));
+    TG_CUDA(cudaMemcpyAsync(dA, A, sizeof(double) * na, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(dB, B, sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(dC, C, sizeof(double) * nc, cudaMemcpyHostToDevice, st));
+    tg::GemmDesc g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.batch = 1;
+    g.sAm = sAm;
+    g.sAk = sAk;
+    g.sBk = sBk;
+    g.sBn = sBn;
+    g.sCm = sCm;
+    g.sCn = sCn;
+    g.prec = prec;
+    tg::gemm<double>(dA, dB, dC, g, st);
+    TG_CUDA(cudaMemcpyAsync(C, dC, sizeof(double) * nc, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    const bool fault = prec == 1 && tg::tc_fault_take();
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaStreamDestroy(st);
+    if (fault) tg::fail(TG_E_RUNTIME, "tensor-core product stopped waiting for its MMAs");
+  });
+}
+
 extern "C" tg_status tg_bench_gemm(int64_t M, int64_t N, int64_t K, int layout, int prec, int iters,
                                    double* avg_ms) {
   return guard([&] {

@@ -337,6 +337,8 @@ struct EngineT final : Engine {
       TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
       fail(TG_E_RUNTIME, "CholeskyQR orthonormalisation met a non-positive pivot (rank-deficient panel)");
     }
+    if (P.mixed && tc_fault_take())
+      fail(TG_E_RUNTIME, "tensor-core product stopped waiting for its MMAs (results discarded)");
     if (info_used == 0) return;
     std::vector<int> h(static_cast<size_t>(info_used));
     TG_CUDA(cudaMemcpyAsync(h.data(), d_info, sizeof(int) * info_used, cudaMemcpyDeviceToHost, st));

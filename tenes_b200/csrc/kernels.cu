@@ -302,150 +302,210 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision: 3xTF32 product on the TF32 tensor pipe (mma.sync
-// m16n8k8).  Each FP64 operand a is rounded to FP32 and split as
-// a = hi + lo with hi = tf32(a), lo = tf32(a - hi); a*b ~ hi*hi + hi*lo +
-// lo*hi.  Products accumulate in FP32 inside one 16-deep k tile and the tile
-// sums are added into FP64 accumulators, so the accumulation error does not
-// grow with K.  64 x 64 x 16 CTA tile, 4 warps of 32 x 32.
+// Mixed precision: 3xTF32 product on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, accumulator in tensor memory).
+//
+// Each FP64 operand element a is split as a = hi + lo, hi = tf32(a),
+// lo = tf32(a - hi) (residual taken in FP64), and a*b ~ hi*hi + hi*lo + lo*hi:
+// three MMAs into one FP32 accumulator.  The split-K chunks of the launcher
+// are summed in FP64, so FP32 accumulation runs over one chunk only.
+//
+// CTA: 128 threads, tile 128 (M, the TMEM lanes) x TC_BN (N, TMEM columns),
+// K staged 16 at a time through two shared-memory stages.  All threads load
+// their FP64 row (A) / column (B) of the next stage into registers, split it
+// and store hi / lo in the K-major no-swizzle canonical layout: 8-row x
+// 16-byte core matrices, K-adjacent core matrices 128 B apart (LBO), 8-row
+// groups 512 B apart (SBO).  One thread issues the MMAs of a stage (two K=8
+// steps x three products) and commits them to the stage's mbarrier, which
+// gates the reuse of that stage.  The epilogue reads the accumulator with
+// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31).  Every mbarrier wait is
+// bounded (2 s of %globaltimer); a timeout sets g_tc_fault, skips the rest of
+// the work and still releases the tensor memory.
 // ---------------------------------------------------------------------------
-constexpr int XBM = 64, XBN = 64, XBK = 16, XLD = 64 + 8;  // XLD: conflict-free fragment loads
-
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return r;
 }
 
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
+__device__ int g_tc_fault = 0;
 
-__global__ void __launch_bounds__(128) gemm_tf32x3_kernel(GemmParams<double> p) {
-  __shared__ uint32_t sA[2][2][XBK * XLD];  // [stage][hi/lo][k][m]
-  __shared__ uint32_t sB[2][2][XBK * XLD];  // [stage][hi/lo][k][n]
+namespace tc {
+constexpr int BM = 128, BK = 16, STAGES = 2, THREADS = 128;
+constexpr uint32_t LBO = 128, SBO = (BK / 4) * 128;  // bytes
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// byte offset of element (r, k) of an R x BK K-major canonical tile
+__device__ __forceinline__ uint32_t tile_off(int r, int k) {
+  return static_cast<uint32_t>((r >> 3) * SBO + (k >> 2) * LBO + (r & 7) * 16 + (k & 3) * 4);
+}
+__device__ __forceinline__ uint64_t desc(uint32_t addr) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (static_cast<uint64_t>((LBO >> 4) & 0x3FFF) << 16) |
+         (static_cast<uint64_t>((SBO >> 4) & 0x3FFF) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+// kind::tf32, F32 accumulator, A and B K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t idesc(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) | ((BM >> 4) << 24);
+}
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = now_ns();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (now_ns() - t0 > 2000000000ull) return false;
+  }
+}
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem), "l"(a), "l"(b), "r"(id), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+}  // namespace tc
+
+template <int BN>
+__global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<double> p) {
+  using namespace tc;
+  constexpr int TILE_A = BM * BK * 4, TILE_B = BN * BK * 4;     // bytes of one hi or lo tile
+  constexpr int STAGE = 2 * TILE_A + 2 * TILE_B;                // A hi, A lo, B hi, B lo
+  constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t mbar[STAGES];
+  __shared__ uint32_t tmem_slot;
   const GemmDesc& d = p.d;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t bz = blockIdx.z;
   const double* A = p.A + bz * d.bA;
   const double* B = p.B + bz * d.bB;
   double* C = p.C + bz * d.bC;
-  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * XBM;
-  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * XBN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  const int gid = lane >> 2, tig = lane & 3;
-  const bool a_kc = (d.sAk == 1), b_nc = (d.sBn == 1);
-  double ra[8], rb[8];
-  auto load = [&](int64_t k0) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int idx = tid + i * 128;
-      int mm, kk, nn, kb;
-      if (a_kc) { kk = idx % XBK; mm = idx / XBK; } else { mm = idx % XBM; kk = idx / XBM; }
-      if (b_nc) { nn = idx % XBN; kb = idx / XBN; } else { kb = idx % XBK; nn = idx / XBK; }
-      const int64_t gm = m0 + mm, gk = k0 + kk, gn = n0 + nn, gkb = k0 + kb;
-      ra[i] = (gm < d.M && gk < d.K) ? A[gm * d.sAm + gk * d.sAk] : 0.0;
-      rb[i] = (gn < d.N && gkb < d.K) ? B[gkb * d.sBk + gn * d.sBn] : 0.0;
-    }
-  };
-  auto store = [&](int s) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int idx = tid + i * 128;
-      int mm, kk, nn, kb;
-      if (a_kc) { kk = idx % XBK; mm = idx / XBK; } else { mm = idx % XBM; kk = idx / XBM; }
-      if (b_nc) { nn = idx % XBN; kb = idx / XBN; } else { kb = idx % XBK; nn = idx / XBK; }
-      const float fa = static_cast<float>(ra[i]);
-      const uint32_t ha = to_tf32(fa);
-      sA[s][0][kk * XLD + mm] = ha;
-      sA[s][1][kk * XLD + mm] = to_tf32(fa - __uint_as_float(ha));
-      const float fb = static_cast<float>(rb[i]);
-      const uint32_t hb = to_tf32(fb);
-      sB[s][0][kb * XLD + nn] = hb;
-      sB[s][1][kb * XLD + nn] = to_tf32(fb - __uint_as_float(hb));
-    }
-  };
-  double acc64[2][4][4];
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc64[i][j][r] = 0.0;
-  const int64_t nk = (d.K + XBK - 1) / XBK;
-  load(0);
-  store(0);
-  __syncthreads();
-  for (int64_t kt = 0; kt < nk; ++kt) {
-    const int s = static_cast<int>(kt & 1);
-    if (kt + 1 < nk) load((kt + 1) * XBK);
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
-#pragma unroll
-    for (int k8 = 0; k8 < XBK; k8 += 8) {
-      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int mb = wm + i * 16 + gid;
-        const int o0 = (k8 + tig) * XLD + mb, o1 = (k8 + tig + 4) * XLD + mb;
-        ah[i][0] = sA[s][0][o0];
-        ah[i][1] = sA[s][0][o0 + 8];
-        ah[i][2] = sA[s][0][o1];
-        ah[i][3] = sA[s][0][o1 + 8];
-        al[i][0] = sA[s][1][o0];
-        al[i][1] = sA[s][1][o0 + 8];
-        al[i][2] = sA[s][1][o1];
-        al[i][3] = sA[s][1][o1 + 8];
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int nb = wn + j * 8 + gid;
-        bh[j][0] = sB[s][0][(k8 + tig) * XLD + nb];
-        bh[j][1] = sB[s][0][(k8 + tig + 4) * XLD + nb];
-        bl[j][0] = sB[s][1][(k8 + tig) * XLD + nb];
-        bl[j][1] = sB[s][1][(k8 + tig + 4) * XLD + nb];
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          mma_tf32(acc[i][j], al[i], bh[j]);
-          mma_tf32(acc[i][j], ah[i], bl[j]);
-          mma_tf32(acc[i][j], ah[i], bh[j]);
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc64[i][j][r] += static_cast<double>(acc[i][j][r]);
-    if (kt + 1 < nk) store(s ^ 1);
-    __syncthreads();
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * BM, n0 = static_cast<int64_t>(blockIdx.x) * BN;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar[s])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t sbase = smem_addr(tc_smem);
+
+  const int64_t nk = (d.K + BK - 1) / BK;
+  const int64_t gm = m0 + tid, gn = n0 + tid;
+  const bool row_ok = gm < d.M, col_ok = tid < BN && gn < d.N;
+  double ra[BK], rb[BK];
+  auto load = [&](int64_t kt) {
+    const int64_t k0 = kt * BK;
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < BK; ++j) {
+      const int64_t k = k0 + j;
+      ra[j] = (row_ok && k < d.K) ? A[gm * d.sAm + k * d.sAk] : 0.0;
+      rb[j] = (col_ok && k < d.K) ? B[k * d.sBk + gn * d.sBn] : 0.0;
+    }
+  };
+  auto split_store = [&](uint8_t* hi, uint8_t* lo, const double (&v)[BK], int r) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int c = 0; c < BK / 4; ++c) {
+      uint32_t h[4], l[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int64_t gm = m0 + wm + i * 16 + gid + ((r & 2) ? 8 : 0);
-        const int64_t gn = n0 + wn + j * 8 + 2 * tig + (r & 1);
-        if (gm < d.M && gn < d.N) {
-          double* c = C + gm * d.sCm + gn * d.sCn;
-          const double v = acc64[i][j][r];
-          *c = d.accumulate ? *c + v : v;
+      for (int e = 0; e < 4; ++e) {
+        const double x = v[4 * c + e];
+        h[e] = to_tf32(static_cast<float>(x));
+        l[e] = to_tf32(static_cast<float>(x - static_cast<double>(__uint_as_float(h[e]))));
+      }
+      const uint32_t o = tile_off(r, 4 * c);
+      *reinterpret_cast<uint4*>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+  };
+  bool ok = true;
+  int64_t issued = 0;  // stages whose MMAs have been issued (the same in every thread)
+  load(0);
+  for (int64_t kt = 0; kt < nk && ok; ++kt) {
+    const int s = static_cast<int>(kt % STAGES);
+    uint8_t* st = tc_smem + s * STAGE;
+    if (kt >= STAGES) ok = mbar_wait(smem_addr(&mbar[s]), static_cast<uint32_t>((kt / STAGES - 1) & 1));
+    split_store(st, st + TILE_A, ra, tid);
+    if (tid < BN) split_store(st + 2 * TILE_A, st + 2 * TILE_A + TILE_B, rb, tid);
+    if (kt + 1 < nk) load(kt + 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    issued = kt + 1;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_hi = sbase + s * STAGE, a_lo = a_hi + TILE_A, b_hi = a_hi + 2 * TILE_A, b_lo = b_hi + TILE_B;
+#pragma unroll
+      for (int kk = 0; kk < BK / 8; ++kk) {
+        const uint32_t off = kk * 2 * LBO;
+        mma(tmem, desc(a_hi + off), desc(b_hi + off), idesc(BN), (kt > 0 || kk > 0) ? 1u : 0u);
+        mma(tmem, desc(a_hi + off), desc(b_lo + off), idesc(BN), 1u);
+        mma(tmem, desc(a_lo + off), desc(b_hi + off), idesc(BN), 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&mbar[s]))
+                   : "memory");
+    }
+  }
+  if (issued > 0) {  // the last commit covers every MMA issued before it; also waited for on failure
+    const int s = static_cast<int>((issued - 1) % STAGES);
+    ok = mbar_wait(smem_addr(&mbar[s]), static_cast<uint32_t>(((issued - 1) / STAGES) & 1)) && ok;
+  }
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int64_t m = m0 + warp * 32 + lane;
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < d.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int64_t n = n0 + c0 + j;
+          if (c0 + j < BN && n < d.N) {
+            double* c = C + m * d.sCm + n * d.sCn;
+            const double r = static_cast<double>(__uint_as_float(v[j]));
+            *c = d.accumulate ? *c + r : r;
+          }
         }
       }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_tc_fault, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
 }
 
 // C[m*sCm + n*sCn] (+)= sum_p parts[p][m*N + n]  (split-K epilogue)
@@ -1209,6 +1269,103 @@ __global__ void spectrum_distance_kernel(const double* a, const double* c, int c
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+template <int BN>
+void launch_tc_bn(dim3 grid, const GemmParams<double>& gp, cudaStream_t st) {
+  constexpr int bytes = tc::STAGES * (2 * tc::BM * tc::BK * 4 + 2 * BN * tc::BK * 4);
+  static bool attr_set = false;
+  if (!attr_set) {
+    TG_CUDA(cudaFuncSetAttribute(gemm_tc_tf32x3_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    attr_set = true;
+  }
+  gemm_tc_tf32x3_kernel<BN><<<grid, tc::THREADS, bytes, st>>>(gp);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+void launch_tc(int bn, dim3 grid, const GemmParams<double>& gp, cudaStream_t st) {
+  switch (bn) {
+    case 32: launch_tc_bn<32>(grid, gp, st); break;
+    case 48: launch_tc_bn<48>(grid, gp, st); break;
+    case 64: launch_tc_bn<64>(grid, gp, st); break;
+    case 96: launch_tc_bn<96>(grid, gp, st); break;
+    default: launch_tc_bn<128>(grid, gp, st); break;
+  }
+}
+
+// 3xTF32 product on tcgen05 (real).  The longer of M and N goes on the
+// 128-row side of the tile (C^T = B^T A^T when N > M); K is split so that
+// the CTAs fill the GPU and no FP32 accumulation runs over more than 1024
+// of K, the chunks being summed in FP64.
+void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream_t st) {
+  if (d.N > d.M) {
+    GemmDesc s = d;
+    s.M = d.N;
+    s.N = d.M;
+    s.sAm = d.sBn;
+    s.sAk = d.sBk;
+    s.sBk = d.sAk;
+    s.sBn = d.sAm;
+    s.sCm = d.sCn;
+    s.sCn = d.sCm;
+    s.bA = d.bB;
+    s.bB = d.bA;
+    std::swap(A, B);
+    d = s;
+  }
+  const int bn = d.N <= 32 ? 32 : d.N <= 48 ? 48 : d.N <= 64 ? 64 : d.N <= 96 ? 96 : 128;
+  dim3 grid(static_cast<unsigned>((d.N + bn - 1) / bn), static_cast<unsigned>((d.M + tc::BM - 1) / tc::BM),
+            static_cast<unsigned>(d.batch));
+  if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
+  const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
+  int64_t split = 1;
+  if (d.batch == 1) {
+    split = (d.K + 1023) / 1024;
+    if (tiles < 148 && d.K >= 512) split = std::max<int64_t>(split, std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 256));
+  }
+  if (split <= 1) {
+    launch_tc(bn, grid, GemmParams<double>{A, B, C, d}, st);
+    return;
+  }
+  const int64_t chunk = (d.K / split + tc::BK - 1) / tc::BK * tc::BK;
+  const int64_t nfull = d.K / chunk, rem = d.K - nfull * chunk;
+  const int64_t nparts = nfull + (rem > 0 ? 1 : 0);
+  void* buf = nullptr;
+  TG_CUDA(cudaMallocAsync(&buf, sizeof(double) * nparts * d.M * d.N, st));
+  double* parts = static_cast<double*>(buf);
+  GemmDesc g = d;
+  g.sCm = d.N;
+  g.sCn = 1;
+  g.accumulate = false;
+  g.K = chunk;
+  g.batch = nfull;
+  g.bA = chunk * d.sAk;
+  g.bB = chunk * d.sBk;
+  g.bC = d.M * d.N;
+  launch_tc(bn, dim3(grid.x, grid.y, static_cast<unsigned>(nfull)), GemmParams<double>{A, B, parts, g}, st);
+  if (rem > 0) {
+    g.K = rem;
+    g.batch = 1;
+    launch_tc(bn, grid,
+              GemmParams<double>{A + nfull * chunk * d.sAk, B + nfull * chunk * d.sBk, parts + nfull * d.M * d.N, g},
+              st);
+  }
+  splitk_reduce_kernel<double><<<num_blocks(d.M * d.N, 256), 256, 0, st>>>(parts, static_cast<int>(nparts), d.M,
+                                                                           d.N, C, d.sCm, d.sCn, d.accumulate);
+  TG_CHECK_LAUNCH();
+  count_launch();
+  TG_CUDA(cudaFreeAsync(buf, st));
+}
+
+bool tc_fault_take() {
+  int f = 0;
+  TG_CUDA(cudaMemcpyFromSymbol(&f, g_tc_fault, sizeof(int)));
+  if (f) {
+    const int z = 0;
+    TG_CUDA(cudaMemcpyToSymbol(g_tc_fault, &z, sizeof(int)));
+  }
+  return f != 0;
+}
+
 template <typename T>
 void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return;
@@ -1233,19 +1390,22 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   // skinny rSVD panels): K is cut into equal chunks written to partial
   // buffers, then summed into C.
   if (CPLX && d.prec != 0) fail(TG_E_INPUT, "gemm: the 3xTF32 product is real-only");
-  auto launch = [&](dim3 gr, const GemmParams<T>& gp) {
-    if constexpr (!CPLX) {
-      if (gp.d.prec == 1) {
-        gemm_tf32x3_kernel<<<gr, 128, 0, st>>>(gp);
-        return;
-      }
+  if constexpr (!CPLX) {
+    if (d.prec == 1) {
+      gemm_tc(A, B, C, d, st);
+      return;
     }
-    gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp);
-  };
+  }
+  auto launch = [&](dim3 gr, const GemmParams<T>& gp) { gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp); };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
   if (d.batch == 1 && tiles < 148 && d.K >= 1024)
     split = std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 512);
+#ifdef TG_GEMM_TRACE  // shape log for tuning builds (off in the library)
+  fprintf(stderr, "gemm M=%lld N=%lld K=%lld batch=%lld sAm=%lld sAk=%lld sBk=%lld sBn=%lld split=%lld prec=%d\n",
+          (long long)d.M, (long long)d.N, (long long)d.K, (long long)d.batch, (long long)d.sAm, (long long)d.sAk,
+          (long long)d.sBk, (long long)d.sBn, (long long)split, d.prec);
+#endif
   if (split <= 1) {
     launch(grid, GemmParams<T>{A, B, C, d});
     TG_CHECK_LAUNCH();

@@ -13,11 +13,16 @@ struct GemmDesc {
   int64_t sAm, sAk, sBk, sBn, sCm, sCn;
   int64_t bA, bB, bC;
   bool conjA, conjB, accumulate;
-  int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 tensor cores with FP64 tile accumulation (real only)
+  int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 on tcgen05, FP32 accumulation over K chunks <= 1024
+                 //    summed in FP64 (real only; conjugation flags are ignored)
 };
 
 template <typename T>
 void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st);
+
+// True (and cleared) when a tcgen05 product gave up waiting for its tensor
+// cores since the last call.  Synchronises the device.
+bool tc_fault_take();
 
 // out[i0..i_{r-1}] = in[...] with out.shape[i] = in.shape[perm[i]] (row-major),
 // optionally conjugated.

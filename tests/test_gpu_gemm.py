@@ -1,0 +1,58 @@
+"""The contraction kernels against numpy FP64: the FP64 DMMA product to
+rounding, and the 3xTF32 tcgen05 product (FP32 accumulation over K chunks of
+at most 1024, summed in FP64) to the accuracy of an FP32 product:
+|C - C_ref| <= 2e-6 * (|A| |B|) elementwise."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from tenes_b200 import _lib
+from tenes_b200._lib import check, dptr
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(A, B, layout_a, layout_b, layout_c, prec, seed_c=None):
+    """C = A B through tg_gemm_host with the requested row/column-major layouts."""
+    M, K = A.shape
+    N = B.shape[1]
+    a = np.ascontiguousarray(A if layout_a == "r" else A.T)
+    sAm, sAk = (K, 1) if layout_a == "r" else (1, M)
+    b = np.ascontiguousarray(B if layout_b == "r" else B.T)
+    sBk, sBn = (N, 1) if layout_b == "r" else (1, K)
+    c = np.zeros((M, N) if layout_c == "r" else (N, M))
+    sCm, sCn = (N, 1) if layout_c == "r" else (1, M)
+    check(_lib.load().tg_gemm_host(M, N, K, dptr(a), sAm, sAk, dptr(b), sBk, sBn, dptr(c), sCm, sCn, prec))
+    return c if layout_c == "r" else c.T
+
+
+SHAPES = [(128, 128, 16), (200, 37, 100), (36, 1000, 72), (1000, 36, 72), (2592, 82, 2592), (130, 257, 1030),
+          (1, 1, 1), (17, 300, 5)]
+
+
+@pytest.mark.parametrize("M,N,K", SHAPES)
+@pytest.mark.parametrize("prec", [0, 1])
+def test_gemm_matches_numpy(M, N, K, prec):
+    rng = np.random.default_rng(M * 7 + N * 3 + K)
+    A = rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N))
+    ref = A @ B
+    bound = np.abs(A) @ np.abs(B)
+    for la, lb, lc in [("r", "r", "r"), ("c", "c", "c"), ("r", "c", "r"), ("c", "r", "c")]:
+        got = _run(A, B, la, lb, lc, prec)
+        err = np.abs(got - ref)
+        if prec == 0:
+            assert np.all(err <= 1e-13 * bound + 1e-300), (la, lb, lc, err.max())
+        else:
+            assert np.all(err <= 2e-6 * bound), (la, lb, lc, (err / bound).max())
+
+
+def test_tf32x3_is_more_accurate_than_one_tf32_product():
+    """The hi/lo split recovers ~FP32 accuracy: far below TF32's 2^-11."""
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((256, 512))
+    B = rng.standard_normal((512, 96))
+    got = _run(A, B, "r", "r", "r", 1)
+    rel = np.abs(got - A @ B) / (np.abs(A) @ np.abs(B))
+    assert rel.max() < 1e-6
