@@ -310,29 +310,44 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
 // three MMAs into one FP32 accumulator.  The split-K chunks of the launcher
 // are summed in FP64, so FP32 accumulation runs over one chunk only.
 //
-// CTA: 128 threads, tile 128 (M, the TMEM lanes) x TC_BN (N, TMEM columns),
-// K staged 16 at a time through two shared-memory stages.  All threads load
-// their FP64 row (A) / column (B) of the next stage into registers, split it
-// and store hi / lo in the K-major no-swizzle canonical layout: 8-row x
-// 16-byte core matrices, K-adjacent core matrices 128 B apart (LBO), 8-row
-// groups 512 B apart (SBO).  One thread issues the MMAs of a stage (two K=8
-// steps x three products) and commits them to the stage's mbarrier, which
-// gates the reuse of that stage.  The epilogue reads the accumulator with
-// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31).  Every mbarrier wait is
-// bounded (2 s of %globaltimer); a timeout sets g_tc_fault, skips the rest of
-// the work and still releases the tensor memory.
+// CTA: 256 threads, tile 128 (M, the TMEM lanes) x BN (N, TMEM columns), K
+// staged 16 at a time through three shared-memory stages.  Each thread keeps
+// two stages of its FP64 half-row of A (and half-column of B) in flight in
+// registers, splits them with integer ALU work and stores hi / lo in the
+// K-major no-swizzle canonical layout: 8-row x 16-byte core matrices,
+// K-adjacent core matrices 128 B apart (LBO), 8-row groups 512 B apart (SBO).
+// One thread issues the MMAs of a stage (two K=8 steps x three products) and
+// commits them to the stage's mbarrier, which gates the reuse of that stage.
+// The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes
+// 32 (w % 4) and one half of the columns).  Every mbarrier wait is bounded
+// (2 s of %globaltimer); a timeout sets g_tc_fault, skips the rest of the
+// work and still releases the tensor memory.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-  return r;
-}
-
 __device__ int g_tc_fault = 0;
 
 namespace tc {
-constexpr int BM = 128, BK = 16, STAGES = 2, THREADS = 128;
+constexpr int BM = 128, BK = 16, STAGES = 3, THREADS = 256;
 constexpr uint32_t LBO = 128, SBO = (BK / 4) * 128;  // bytes
+
+// FP32 bit pattern of a double whose mantissa has at most 10 bits (exact);
+// values below the FP32 normal range become 0
+__device__ __forceinline__ uint32_t tf32_bits_of(unsigned long long b) {
+  const uint32_t hw = static_cast<uint32_t>(b >> 32);
+  const int e = static_cast<int>((hw >> 20) & 0x7FF) - 896;  // FP64 bias 1023 -> FP32 bias 127
+  const uint32_t f = (hw & 0x80000000u) | (static_cast<uint32_t>(e) << 23) | ((hw & 0x000FFC00u) << 3);
+  return e > 0 ? f : 0u;
+}
+// x = hi + lo + O(2^-22 |x|), hi and lo TF32 values given as FP32 bits:
+// round-to-nearest to 10 mantissa bits on the FP64 pattern, the residual
+// x - hi is exact in FP64.  Integer ALU work only (no conversion unit).
+__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
+  constexpr unsigned long long half = 1ull << 41, keep = 0xFFFFFC0000000000ull;
+  const unsigned long long hb = (static_cast<unsigned long long>(__double_as_longlong(x)) + half) & keep;
+  const double l = x - __longlong_as_double(static_cast<long long>(hb));
+  const unsigned long long lb = (static_cast<unsigned long long>(__double_as_longlong(l)) + half) & keep;
+  hi = tf32_bits_of(hb);
+  lo = tf32_bits_of(lb);
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -413,46 +428,48 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
   const uint32_t sbase = smem_addr(tc_smem);
 
   const int64_t nk = (d.K + BK - 1) / BK;
-  const int64_t gm = m0 + tid, gn = n0 + tid;
-  const bool row_ok = gm < d.M, col_ok = tid < BN && gn < d.N;
-  double ra[BK], rb[BK];
-  auto load = [&](int64_t kt) {
-    const int64_t k0 = kt * BK;
+  // thread t loads K half (t >> 7) of row (t & 127) of A and, for t & 127 < BN, of column t & 127 of B
+  constexpr int KH = BK / 2;
+  const int r = tid & (BM - 1), kh = (tid >> 7) * KH;
+  const int64_t gm = m0 + r, gn = n0 + r;
+  const bool row_ok = gm < d.M, col_ok = r < BN && gn < d.N;
+  const double* pa = A + gm * d.sAm;
+  const double* pb = B + gn * d.sBn;
+  double ra0[KH], rb0[KH], ra1[KH], rb1[KH];
+  auto load = [&](int64_t kt, double (&va)[KH], double (&vb)[KH]) {
+    const int64_t k0 = kt * BK + kh;
 #pragma unroll
-    for (int j = 0; j < BK; ++j) {
+    for (int j = 0; j < KH; ++j) {
       const int64_t k = k0 + j;
-      ra[j] = (row_ok && k < d.K) ? A[gm * d.sAm + k * d.sAk] : 0.0;
-      rb[j] = (col_ok && k < d.K) ? B[k * d.sBk + gn * d.sBn] : 0.0;
+      va[j] = (row_ok && k < d.K) ? pa[k * d.sAk] : 0.0;
+      vb[j] = (col_ok && k < d.K) ? pb[k * d.sBk] : 0.0;
     }
   };
-  auto split_store = [&](uint8_t* hi, uint8_t* lo, const double (&v)[BK], int r) {
+  auto split_store = [&](uint8_t* hi, uint8_t* lo, const double (&v)[KH]) {
 #pragma unroll
-    for (int c = 0; c < BK / 4; ++c) {
+    for (int c = 0; c < KH / 4; ++c) {
       uint32_t h[4], l[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const double x = v[4 * c + e];
-        h[e] = to_tf32(static_cast<float>(x));
-        l[e] = to_tf32(static_cast<float>(x - static_cast<double>(__uint_as_float(h[e]))));
-      }
-      const uint32_t o = tile_off(r, 4 * c);
+      for (int e = 0; e < 4; ++e) split_tf32(v[4 * c + e], h[e], l[e]);
+      const uint32_t o = tile_off(r, kh + 4 * c);
       *reinterpret_cast<uint4*>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
       *reinterpret_cast<uint4*>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
     }
   };
   bool ok = true;
   int64_t issued = 0;  // stages whose MMAs have been issued (the same in every thread)
-  load(0);
-  for (int64_t kt = 0; kt < nk && ok; ++kt) {
+  // one pipeline step: stage kt from registers (va, vb) into shared memory,
+  // refill (va, vb) with stage kt + 2, hand stage kt to the tensor cores
+  auto step = [&](int64_t kt, double (&va)[KH], double (&vb)[KH]) {
     const int s = static_cast<int>(kt % STAGES);
     uint8_t* st = tc_smem + s * STAGE;
     if (kt >= STAGES) ok = mbar_wait(smem_addr(&mbar[s]), static_cast<uint32_t>((kt / STAGES - 1) & 1));
-    split_store(st, st + TILE_A, ra, tid);
-    if (tid < BN) split_store(st + 2 * TILE_A, st + 2 * TILE_A + TILE_B, rb, tid);
-    if (kt + 1 < nk) load(kt + 1);
+    split_store(st, st + TILE_A, va);
+    if (r < BN) split_store(st + 2 * TILE_A, st + 2 * TILE_A + TILE_B, vb);
+    if (kt + 2 < nk) load(kt + 2, va, vb);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     ok = __syncthreads_and(ok);
-    if (!ok) break;
+    if (!ok) return;
     issued = kt + 1;
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -468,6 +485,12 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
                        smem_addr(&mbar[s]))
                    : "memory");
     }
+  };
+  load(0, ra0, rb0);
+  if (nk > 1) load(1, ra1, rb1);
+  for (int64_t kt = 0; kt < nk && ok; kt += 2) {
+    step(kt, ra0, rb0);
+    if (kt + 1 < nk && ok) step(kt + 1, ra1, rb1);
   }
   if (issued > 0) {  // the last commit covers every MMA issued before it; also waited for on failure
     const int s = static_cast<int>((issued - 1) % STAGES);
@@ -476,22 +499,25 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
   ok = __syncthreads_and(ok);
   if (ok) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int64_t m = m0 + warp * 32 + lane;
+    // warp w reads TMEM lanes 32 (w % 4) ...; warps 0-3 take the first half of the columns, 4-7 the second
+    const int quarter = warp & 3, half = warp >> 2;
+    const int64_t m = m0 + quarter * 32 + lane;
 #pragma unroll
-    for (int c0 = 0; c0 < BN; c0 += 16) {
+    for (int cc = 0; cc < BN / 2; cc += 16) {
+      const int c0 = half * (BN / 2) + cc;
       uint32_t v[16];
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
           "%14, %15}, [%16];"
           : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+          : "r"(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(c0)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (m < d.M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int64_t n = n0 + c0 + j;
-          if (c0 + j < BN && n < d.N) {
+          if (n < d.N) {
             double* c = C + m * d.sCm + n * d.sCn;
             const double r = static_cast<double>(__uint_as_float(v[j]));
             *c = d.accumulate ? *c + r : r;
@@ -1285,7 +1311,6 @@ void launch_tc_bn(dim3 grid, const GemmParams<double>& gp, cudaStream_t st) {
 void launch_tc(int bn, dim3 grid, const GemmParams<double>& gp, cudaStream_t st) {
   switch (bn) {
     case 32: launch_tc_bn<32>(grid, gp, st); break;
-    case 48: launch_tc_bn<48>(grid, gp, st); break;
     case 64: launch_tc_bn<64>(grid, gp, st); break;
     case 96: launch_tc_bn<96>(grid, gp, st); break;
     default: launch_tc_bn<128>(grid, gp, st); break;
@@ -1312,7 +1337,7 @@ void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream
     std::swap(A, B);
     d = s;
   }
-  const int bn = d.N <= 32 ? 32 : d.N <= 48 ? 48 : d.N <= 64 ? 64 : d.N <= 96 ? 96 : 128;
+  const int bn = d.N <= 32 ? 32 : d.N <= 64 ? 64 : d.N <= 96 ? 96 : 128;
   dim3 grid(static_cast<unsigned>((d.N + bn - 1) / bn), static_cast<unsigned>((d.M + tc::BM - 1) / tc::BM),
             static_cast<unsigned>(d.batch));
   if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
@@ -1320,7 +1345,8 @@ void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream
   int64_t split = 1;
   if (d.batch == 1) {
     split = (d.K + 1023) / 1024;
-    if (tiles < 148 && d.K >= 512) split = std::max<int64_t>(split, std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 256));
+    if (tiles < 296 && d.K >= 512)  // two CTAs per SM
+      split = std::max<int64_t>(split, std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 256));
   }
   if (split <= 1) {
     launch_tc(bn, grid, GemmParams<double>{A, B, C, d}, st);
