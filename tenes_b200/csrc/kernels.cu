@@ -329,24 +329,15 @@ namespace tc {
 constexpr int BM = 128, BK = 16, STAGES = 3, THREADS = 256;
 constexpr uint32_t LBO = 128, SBO = (BK / 4) * 128;  // bytes
 
-// FP32 bit pattern of a double whose mantissa has at most 10 bits (exact);
-// values below the FP32 normal range become 0
-__device__ __forceinline__ uint32_t tf32_bits_of(unsigned long long b) {
-  const uint32_t hw = static_cast<uint32_t>(b >> 32);
-  const int e = static_cast<int>((hw >> 20) & 0x7FF) - 896;  // FP64 bias 1023 -> FP32 bias 127
-  const uint32_t f = (hw & 0x80000000u) | (static_cast<uint32_t>(e) << 23) | ((hw & 0x000FFC00u) << 3);
-  return e > 0 ? f : 0u;
-}
-// x = hi + lo + O(2^-22 |x|), hi and lo TF32 values given as FP32 bits:
-// round-to-nearest to 10 mantissa bits on the FP64 pattern, the residual
-// x - hi is exact in FP64.  Integer ALU work only (no conversion unit).
+// x = hi + lo + O(2^-23 |x|), hi and lo TF32 values given as FP32 bits:
+// one FP64 -> FP32 conversion, then round-to-nearest to 10 mantissa bits on
+// the FP32 pattern; the residual xf - hi is exact in FP32.
 __device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
-  constexpr unsigned long long half = 1ull << 41, keep = 0xFFFFFC0000000000ull;
-  const unsigned long long hb = (static_cast<unsigned long long>(__double_as_longlong(x)) + half) & keep;
-  const double l = x - __longlong_as_double(static_cast<long long>(hb));
-  const unsigned long long lb = (static_cast<unsigned long long>(__double_as_longlong(l)) + half) & keep;
-  hi = tf32_bits_of(hb);
-  lo = tf32_bits_of(lb);
+  const float xf = __double2float_rn(x);
+  const uint32_t hb = (__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u;
+  const float l = xf - __uint_as_float(hb);
+  hi = hb;
+  lo = (__float_as_uint(l) + 0x1000u) & 0xFFFFE000u;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -428,30 +419,52 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
   const uint32_t sbase = smem_addr(tc_smem);
 
   const int64_t nk = (d.K + BK - 1) / BK;
-  // thread t loads K half (t >> 7) of row (t & 127) of A and, for t & 127 < BN, of column t & 127 of B
+  // Each thread moves two pieces of four K-consecutive values per operand and
+  // stage.  When the operand's rows are contiguous in memory (stride 1 along
+  // M or N) piece p is row t & 127 at k = 8 (t >> 7) + 4p, so a warp reads
+  // consecutive rows; when K is contiguous piece p is row (t >> 2) + 64p at
+  // k = 4 (t & 3), so four threads read one row's 16 consecutive values.
   constexpr int KH = BK / 2;
-  const int r = tid & (BM - 1), kh = (tid >> 7) * KH;
-  const int64_t gm = m0 + r, gn = n0 + r;
-  const bool row_ok = gm < d.M, col_ok = r < BN && gn < d.N;
-  const double* pa = A + gm * d.sAm;
-  const double* pb = B + gn * d.sBn;
+  struct Pieces {
+    int row[2], k[2];
+    bool ok[2];
+    const double* base[2];
+    int64_t sk;
+  };
+  auto pieces = [&](const double* X, int64_t row0, int64_t nrows_valid, int nrows_tile, int64_t s_row,
+                    int64_t s_k) {
+    Pieces P;
+    const bool rows_contig = (s_row == 1 && s_k != 1);
+    for (int q = 0; q < 2; ++q) {
+      P.row[q] = rows_contig ? (tid & (BM - 1)) : (tid >> 2) + 64 * q;
+      P.k[q] = rows_contig ? (tid >> 7) * KH + 4 * q : 4 * (tid & 3);
+      P.ok[q] = P.row[q] < nrows_tile && row0 + P.row[q] < nrows_valid;
+      P.base[q] = X + (row0 + P.row[q]) * s_row;
+    }
+    P.sk = s_k;
+    return P;
+  };
+  const Pieces PA = pieces(A, m0, d.M, BM, d.sAm, d.sAk);
+  const Pieces PB = pieces(B, n0, d.N, BN, d.sBn, d.sBk);
   double ra0[KH], rb0[KH], ra1[KH], rb1[KH];
   auto load = [&](int64_t kt, double (&va)[KH], double (&vb)[KH]) {
-    const int64_t k0 = kt * BK + kh;
 #pragma unroll
-    for (int j = 0; j < KH; ++j) {
-      const int64_t k = k0 + j;
-      va[j] = (row_ok && k < d.K) ? pa[k * d.sAk] : 0.0;
-      vb[j] = (col_ok && k < d.K) ? pb[k * d.sBk] : 0.0;
-    }
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t ka = kt * BK + PA.k[q] + j, kb = kt * BK + PB.k[q] + j;
+        va[4 * q + j] = (PA.ok[q] && ka < d.K) ? PA.base[q][ka * PA.sk] : 0.0;
+        vb[4 * q + j] = (PB.ok[q] && kb < d.K) ? PB.base[q][kb * PB.sk] : 0.0;
+      }
   };
-  auto split_store = [&](uint8_t* hi, uint8_t* lo, const double (&v)[KH]) {
+  auto split_store = [&](uint8_t* hi, uint8_t* lo, const double (&v)[KH], const Pieces& P, int nrows_tile) {
 #pragma unroll
-    for (int c = 0; c < KH / 4; ++c) {
+    for (int q = 0; q < 2; ++q) {
+      if (P.row[q] >= nrows_tile) continue;
       uint32_t h[4], l[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) split_tf32(v[4 * c + e], h[e], l[e]);
-      const uint32_t o = tile_off(r, kh + 4 * c);
+      for (int e = 0; e < 4; ++e) split_tf32(v[4 * q + e], h[e], l[e]);
+      const uint32_t o = tile_off(P.row[q], P.k[q]);
       *reinterpret_cast<uint4*>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
       *reinterpret_cast<uint4*>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
     }
@@ -464,8 +477,8 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
     const int s = static_cast<int>(kt % STAGES);
     uint8_t* st = tc_smem + s * STAGE;
     if (kt >= STAGES) ok = mbar_wait(smem_addr(&mbar[s]), static_cast<uint32_t>((kt / STAGES - 1) & 1));
-    split_store(st, st + TILE_A, va);
-    if (r < BN) split_store(st + 2 * TILE_A, st + 2 * TILE_A + TILE_B, vb);
+    split_store(st, st + TILE_A, va, PA, BM);
+    split_store(st + 2 * TILE_A, st + 2 * TILE_A + TILE_B, vb, PB, BN);
     if (kt + 2 < nk) load(kt + 2, va, vb);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     ok = __syncthreads_and(ok);
