@@ -1,6 +1,8 @@
 // Hand-written sm_100a kernels of the CTMRG path: FP64 tensor-core (DMMA)
 // strided batched matrix product, leg permutation, max-abs normalisation,
 // projector truncation helpers and a batched one-sided Jacobi spectrum.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -545,6 +547,215 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_tf32x3_kernel(GemmParams<
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+}
+
+// ---------------------------------------------------------------------------
+// 3xTF32 with TMA-fed operands.
+//
+// split_pack_kernel: an FP64 matrix view X(r, k) = X[r*s_r + k*s_k] becomes
+// two FP32 arrays hi, lo of shape [rows_pad][kpad] (K contiguous, zero
+// padding), x = hi + lo + O(2^-23 |x|).  32 x 32 tiles through shared memory
+// keep both the read (along whichever stride is 1) and the write coalesced.
+//
+// gemm_tma_kernel: 128 threads.  Lane 0 of warp 0 streams the hi / lo tiles
+// of A (128 rows x 32 K) and B (BN rows x 32 K) with cp.async.bulk.tensor
+// into a three-stage ring (128-byte swizzle), each stage completing a "full"
+// mbarrier by its transaction bytes; lane 0 of warp 1 issues, per stage,
+// four K=8 steps x three tcgen05.mma (hi*hi, hi*lo, lo*hi) into the TMEM
+// accumulator and commits them to the stage's "empty" mbarrier, which the
+// producer waits on before refilling the slot; the last commit arrives on
+// "done", after which all four warps move the accumulator out through
+// tcgen05.ld (warp w: TMEM lanes 32w..32w+31) as FP64.  blockIdx.z selects
+// a K chunk; with more than one chunk the CTA writes an FP64 partial tile.
+// Waits are bounded (2 s); a timeout sets g_tc_fault and the CTA still
+// releases its tensor memory after a bounded wait for its own MMAs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) split_pack_kernel(const double* __restrict__ X, int64_t rows, int64_t K,
+                                                         int64_t s_r, int64_t s_k, int64_t kpad,
+                                                         float* __restrict__ hi, float* __restrict__ lo) {
+  __shared__ double t[32][33];
+  const int64_t k0 = static_cast<int64_t>(blockIdx.x) * 32, r0 = static_cast<int64_t>(blockIdx.y) * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const bool k_contig = (s_k == 1);
+  for (int i = ty; i < 32; i += 8) {
+    // element (r0 + a, k0 + b) with the thread index on the contiguous axis
+    const int a = k_contig ? i : tx, b = k_contig ? tx : i;
+    const int64_t r = r0 + a, k = k0 + b;
+    t[a][b] = (r < rows && k < K) ? X[r * s_r + k * s_k] : 0.0;
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    uint32_t h, l;
+    tc::split_tf32(t[i][tx], h, l);
+    const int64_t o = (r0 + i) * kpad + k0 + tx;
+    hi[o] = __uint_as_float(h);
+    lo[o] = __uint_as_float(l);
+  }
+}
+
+namespace tma {
+constexpr int BM = 128, BK = 32, STAGES = 3, THREADS = 128;
+constexpr uint32_t A_TILE = BM * BK * 4;  // 16 KB, one hi or lo tile
+__device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = tc::now_ns();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (tc::now_ns() - t0 > 2000000000ull) return false;
+  }
+}
+// K-major operand tile with 128-byte swizzle: rows of 128 B, 8-row atoms
+// 1024 B apart (SBO); the leading offset is unused for this layout (1)
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFF) | (1ull << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+__device__ __forceinline__ void load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      :
+      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+}  // namespace tma
+
+struct TmaGemm {
+  int64_t M, N;
+  int ktiles_per_chunk, ktiles;  // K tiles of 32 per CTA chunk, in total
+  double* C;                     // output (nchunks == 1) or partials [chunk][M][N]
+  int64_t sCm, sCn;
+  int nchunks;
+  bool accumulate;
+};
+
+template <int BN>
+__global__ void __launch_bounds__(tma::THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap mAh,
+                                                                const __grid_constant__ CUtensorMap mAl,
+                                                                const __grid_constant__ CUtensorMap mBh,
+                                                                const __grid_constant__ CUtensorMap mBl, TmaGemm g) {
+  using namespace tma;
+  constexpr uint32_t B_TILE = BN * BK * 4;
+  constexpr uint32_t STAGE = 2 * A_TILE + 2 * B_TILE;
+  constexpr uint32_t TX = STAGE;  // bytes each stage's four loads deliver
+  constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);
+  extern __shared__ __align__(1024) uint8_t tma_smem[];
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, chunk = blockIdx.z;
+  const int kt0 = chunk * g.ktiles_per_chunk;
+  const int nk = min(g.ktiles_per_chunk, g.ktiles - kt0);
+  // 1024-byte aligned ring (the 128-byte swizzle repeats every 8 rows of 128 B)
+  const uint32_t raw = tc::smem_addr(tma_smem);
+  const uint32_t ring = (raw + 1023u) & ~1023u;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_addr(&tmem_slot)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_addr(&full[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_addr(&empty[s])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_addr(&done)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  bool ok = true;
+  int issued = 0;  // stages handed to the tensor cores (MMA thread only)
+  if (tid == 0) {
+    // producer
+    for (int i = 0; i < nk && ok; ++i) {
+      const int s = i % STAGES;
+      if (i >= STAGES) ok = wait(tc::smem_addr(&empty[s]), static_cast<uint32_t>((i / STAGES - 1) & 1));
+      if (!ok) break;
+      const uint32_t st = ring + s * STAGE, bar = tc::smem_addr(&full[s]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(TX) : "memory");
+      const int x = (kt0 + i) * BK;
+      load_2d(st, &mAh, bar, x, m0);
+      load_2d(st + A_TILE, &mAl, bar, x, m0);
+      load_2d(st + 2 * A_TILE, &mBh, bar, x, n0);
+      load_2d(st + 2 * A_TILE + B_TILE, &mBl, bar, x, n0);
+    }
+  } else if (tid == 32) {
+    // MMA issuer
+    constexpr uint32_t id = tc::idesc(BN);
+    for (int i = 0; i < nk && ok; ++i) {
+      const int s = i % STAGES;
+      ok = wait(tc::smem_addr(&full[s]), static_cast<uint32_t>((i / STAGES) & 1));
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_hi = ring + s * STAGE, a_lo = a_hi + A_TILE, b_hi = a_hi + 2 * A_TILE, b_lo = b_hi + B_TILE;
+#pragma unroll
+      for (int kk = 0; kk < BK / 8; ++kk) {
+        const uint32_t off = kk * 32;  // 8 TF32 values of a 128-byte swizzled row
+        tc::mma(tmem, desc_sw128(a_hi + off), desc_sw128(b_hi + off), id, (i > 0 || kk > 0) ? 1u : 0u);
+        tc::mma(tmem, desc_sw128(a_hi + off), desc_sw128(b_lo + off), id, 1u);
+        tc::mma(tmem, desc_sw128(a_lo + off), desc_sw128(b_hi + off), id, 1u);
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       tc::smem_addr(&empty[s]))
+                   : "memory");
+      issued = i + 1;
+    }
+    // "done" follows every issued MMA (also after a failure, so that the
+    // other warps stop waiting)
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     tc::smem_addr(&done))
+                 : "memory");
+  }
+  __syncwarp();
+  const bool mma_done = wait(tc::smem_addr(&done), 0u);
+  ok = __syncthreads_and(ok && mma_done && (nk > 0));
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int64_t m = m0 + warp * 32 + lane;
+    double* out = g.nchunks > 1 ? g.C + static_cast<int64_t>(chunk) * g.M * g.N : g.C;
+    const int64_t sm_ = g.nchunks > 1 ? g.N : g.sCm, sn_ = g.nchunks > 1 ? 1 : g.sCn;
+    const bool acc = g.nchunks == 1 && g.accumulate;
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < g.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int64_t n = n0 + c0 + j;
+          if (n < g.N) {
+            double* c = out + m * sm_ + n * sn_;
+            const double r = static_cast<double>(__uint_as_float(v[j]));
+            *c = acc ? *c + r : r;
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_tc_fault, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+  (void)issued;
 }
 
 // C[m*sCm + n*sCn] (+)= sum_p parts[p][m*N + n]  (split-K epilogue)
@@ -1330,10 +1541,106 @@ void launch_tc(int bn, dim3 grid, const GemmParams<double>& gp, cudaStream_t st)
   }
 }
 
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    TG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess) fail(TG_E_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 2D map over a [rows][kpad] FP32 array: boxes of 32 K x box_rows rows with
+// the 128-byte swizzle the tcgen05 descriptors expect
+CUtensorMap tf32_map(const float* base, int64_t rows, int64_t kpad, int box_rows) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(kpad), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(kpad) * 4};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(tma::BK), static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims,
+                                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(TG_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")");
+  return m;
+}
+
+template <int BN>
+void launch_tma_bn(dim3 grid, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
+                   const CUtensorMap& bl, const TmaGemm& g, cudaStream_t st) {
+  constexpr int bytes = tma::STAGES * (2 * tma::A_TILE + 2 * BN * tma::BK * 4) + 1024;
+  static bool attr_set = false;
+  if (!attr_set) {
+    TG_CUDA(cudaFuncSetAttribute(gemm_tma_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    attr_set = true;
+  }
+  gemm_tma_kernel<BN><<<grid, tma::THREADS, bytes, st>>>(ah, al, bh, bl, g);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+// C = A B for one real product: both operands split into padded hi / lo TF32
+// arrays (split_pack_kernel), then the TMA-fed tcgen05 kernel over 128 x bn
+// tiles; K chunks (<= 1024 of K, enough of them to give every SM a CTA) are
+// reduced in FP64.
+void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, int bn, cudaStream_t st) {
+  const int64_t kpad = (d.K + tma::BK - 1) / tma::BK * tma::BK, ktiles = kpad / tma::BK;
+  const int64_t mpad = (d.M + tma::BM - 1) / tma::BM * tma::BM, npad = (d.N + bn - 1) / bn * bn;
+  if (mpad / tma::BM > 65535 || ktiles > (int64_t{1} << 30)) fail(TG_E_INPUT, "gemm: problem too large");
+  void* sbuf = nullptr;
+  TG_CUDA(cudaMallocAsync(&sbuf, sizeof(float) * 2 * (mpad + npad) * kpad, st));
+  float* ah = static_cast<float*>(sbuf);
+  float* al = ah + mpad * kpad;
+  float* bh = al + mpad * kpad;
+  float* bl = bh + npad * kpad;
+  split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(mpad / 32)), 256, 0, st>>>(
+      A, d.M, d.K, d.sAm, d.sAk, kpad, ah, al);
+  TG_CHECK_LAUNCH();
+  split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(npad / 32)), 256, 0, st>>>(
+      B, d.N, d.K, d.sBn, d.sBk, kpad, bh, bl);
+  TG_CHECK_LAUNCH();
+  count_launch(2);
+  const CUtensorMap mah = tf32_map(ah, mpad, kpad, tma::BM), mal = tf32_map(al, mpad, kpad, tma::BM);
+  const CUtensorMap mbh = tf32_map(bh, npad, kpad, bn), mbl = tf32_map(bl, npad, kpad, bn);
+  const int64_t tiles = (mpad / tma::BM) * (npad / bn);
+  int64_t nch = (ktiles + 31) / 32;
+  if (tiles < 148) nch = std::max<int64_t>(nch, std::min<int64_t>((148 + tiles - 1) / tiles, ktiles / 8));
+  nch = std::max<int64_t>(1, std::min<int64_t>(nch, ktiles));
+  const int64_t per = (ktiles + nch - 1) / nch;
+  nch = (ktiles + per - 1) / per;
+  TmaGemm g{d.M, d.N, static_cast<int>(per), static_cast<int>(ktiles), C, d.sCm, d.sCn, static_cast<int>(nch),
+            d.accumulate};
+  void* pbuf = nullptr;
+  if (nch > 1) {
+    TG_CUDA(cudaMallocAsync(&pbuf, sizeof(double) * nch * d.M * d.N, st));
+    g.C = static_cast<double*>(pbuf);
+  }
+  const dim3 grid(static_cast<unsigned>(npad / bn), static_cast<unsigned>(mpad / tma::BM), static_cast<unsigned>(nch));
+  switch (bn) {
+    case 32: launch_tma_bn<32>(grid, mah, mal, mbh, mbl, g, st); break;
+    case 64: launch_tma_bn<64>(grid, mah, mal, mbh, mbl, g, st); break;
+    case 96: launch_tma_bn<96>(grid, mah, mal, mbh, mbl, g, st); break;
+    default: launch_tma_bn<128>(grid, mah, mal, mbh, mbl, g, st); break;
+  }
+  if (nch > 1) {
+    splitk_reduce_kernel<double><<<num_blocks(d.M * d.N, 256), 256, 0, st>>>(
+        static_cast<double*>(pbuf), static_cast<int>(nch), d.M, d.N, C, d.sCm, d.sCn, d.accumulate);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    TG_CUDA(cudaFreeAsync(pbuf, st));
+  }
+  TG_CUDA(cudaFreeAsync(sbuf, st));
+}
+
 // 3xTF32 product on tcgen05 (real).  The longer of M and N goes on the
 // 128-row side of the tile (C^T = B^T A^T when N > M); K is split so that
 // the CTAs fill the GPU and no FP32 accumulation runs over more than 1024
-// of K, the chunks being summed in FP64.
+// of K, the chunks being summed in FP64.  Single products take the TMA-fed
+// kernel, batched ones the register-staged kernel.
 void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream_t st) {
   if (d.N > d.M) {
     GemmDesc s = d;
@@ -1351,6 +1658,10 @@ void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream
     d = s;
   }
   const int bn = d.N <= 32 ? 32 : d.N <= 64 ? 64 : d.N <= 96 ? 96 : 128;
+  if (d.batch == 1) {
+    gemm_tma(A, B, C, d, bn, st);
+    return;
+  }
   dim3 grid(static_cast<unsigned>((d.N + bn - 1) / bn), static_cast<unsigned>((d.M + tc::BM - 1) / tc::BM),
             static_cast<unsigned>(d.batch));
   if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
