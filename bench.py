@@ -1,11 +1,16 @@
 """CTMRG throughput on B200: sweeps/s of the iTPS corner-transfer-matrix
 environment (one sweep = Left, Right, Top, Bottom moves of
-core::Calc_CTM_Environment, src/iTPS/core/ctm.cpp:1203-1243).
+core::Calc_CTM_Environment, src/iTPS/core/ctm.cpp:1203-1243) and the time to
+a converged environment, mixed precision against the FP64 path.
 
 Workload (default): spin-1/2 antiferromagnetic Heisenberg model, 2x2 unit
-cell, D=6, chi=72, FP64, site tensors from 300 seeded simple-update steps at
+cell, D=6, chi=72, site tensors from 300 seeded simple-update steps at
 tau=0.01 run through the library itself, Neel initial state + noise 1e-2
 (seed 11).  Data are synthetic; the reference publishes no benchmark suite.
+`value` is the chosen form: 3xTF32 tcgen05 contractions with FP64 rSVD
+projectors (k = chi+10, q = 2).  `time_to_converge` runs the chosen form, the
+FP64 rSVD path and the FP64 full-SVD path (the reference's default projector)
+from the same tensors until the energy per site moves by <= 1e-7 per sweep.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -174,6 +179,70 @@ def traffic_from_profile(cfg):
     return float(m.group(1)) if m else None
 
 
+def bond_energy(env):
+    """Energy per site: <S.S> over the horizontal and vertical bond of every
+    site, each normalised by the same contraction with the identity
+    (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225)."""
+    from tenes_b200.std_ops import heisenberg_bond, real_if_close
+    h = real_if_close(heisenberg_bond(1.0))
+    ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    tot = 0.0
+    for s in range(env.N):
+        for dx, dy in ((1, 0), (0, 1)):
+            tot += (env.contract_bond_op12(s, dx, dy, h) / env.contract_bond_op12(s, dx, dy, ident)).real
+    return tot / env.N
+
+
+def prepare_tensors(cfg, seed, device, su_steps=None):
+    """Site tensors from the seeded simple update, run by the library."""
+    env = make_env(cfg, seed, device, "svd", su_steps, "fp64")
+    T = [env.get_site_tensor(i) for i in range(env.N)]
+    env.close()
+    return T
+
+
+def env_for(cfg, T, device, projector, precision, max_iter=1):
+    from tenes_b200.env import Environment
+    D, chi, _, _ = CONFIGS[cfg]
+    LX, LY, pd, vd, _, _ = lattice_spec(D)
+    p = ctm_params(cfg, projector, precision)
+    p.max_ctm_iteration = max_iter
+    env = Environment(LX, LY, pd, vd, p, False, device=device)
+    for i, t in enumerate(T):
+        env.set_site_tensor(i, t)
+    env.init_env()
+    return env
+
+
+def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
+    """Time to a converged environment: sweeps until the energy per site
+    changes by at most `tol` between successive sweeps (energy evaluations
+    included in the wall time); the sweep at which the reference's own
+    corner-spectrum criterion (eps = 1e-6, ctm.cpp:815-969) first holds is
+    recorded too."""
+    env = env_for(cfg, T, device, projector, precision)
+    env.sync()
+    t0 = time.perf_counter()
+    e_prev, n, ref_conv, conv = None, 0, None, False
+    e = float("nan")
+    while n < max_sweeps:
+        env.sweep()
+        n += 1
+        c, _ = env.check_convergence()
+        if c and ref_conv is None:
+            ref_conv = n
+        e = bond_energy(env)
+        if e_prev is not None and abs(e - e_prev) <= tol:
+            conv = True
+            break
+        e_prev = e
+    secs = time.perf_counter() - t0
+    env.close()
+    return {"sweeps": n, "seconds": secs, "converged": conv, "energy_per_site": e,
+            "last_delta_e": (abs(e - e_prev) if e_prev is not None else None),
+            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -181,7 +250,8 @@ def run_ours(args, rank, world, local_rank):
                                 profile_reset)
     device = local_rank
     torch.cuda.set_device(device)
-    env = make_env(args.config, SEED + rank, device, args.projector, args.su_steps, args.precision)
+    T = prepare_tensors(args.config, SEED + rank, device, args.su_steps)
+    env = env_for(args.config, T, device, args.projector, args.precision)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
@@ -240,8 +310,8 @@ def run_ours(args, rank, world, local_rank):
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        for i, T in enumerate(host_T):
-            env.set_site_tensor(i, T)
+        for i, Ti in enumerate(host_T):
+            env.set_site_tensor(i, Ti)
         for w in range(8):
             for i in range(env.N):
                 env.set_env(w, i, host_env[w][i])
@@ -257,28 +327,59 @@ def run_ours(args, rank, world, local_rank):
     e2e = {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "sweeps/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(t.nbytes for ws in host_env for t in ws)}
 
-    # ---- per-family device time of one instrumented sweep (roofline)
+    # ---- per-family device time of one instrumented sweep (roofline of the dominant product kernel)
     profile_enable(True)
     profile_reset()
     env.sweep()
     env.sync()
     fam = {PROFILE_KINDS[k]: profile_query(k) for k in range(len(PROFILE_KINDS))}
     profile_enable(False)
-    n_g, ms_g, fl_g, _ = fam["gemm_dmma"]
-    peak = fp64_peak_tflops(device) if rank == 0 else None
-    achieved = fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0
-    traffic = traffic_from_profile(args.config)
-    roofline = {"bound": "tensor", "kernel": "gemm_kernel (FP64 DMMA m8n8k4)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None,
-                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (no FP64 entry in MEASURED_PEAKS.json)",
-                "traffic": traffic, "launches_per_sweep": n_g, "avg_launch_us": 1e3 * ms_g / max(n_g, 1),
-                "flops_per_launch": fl_g / max(n_g, 1),
-                "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}}
     env.close()
-    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roofline,
+    peaks = measured_peaks()
+    if fam["gemm_tcgen05"][1] >= fam["gemm_dmma"][1]:
+        n_g, ms_g, fl_g, _ = fam["gemm_tcgen05"]
+        issued = 3.0 * fl_g  # three TF32 products per multiply-add
+        peak = peaks.get("bf16_tflops_sustained", 1411.5) / 2.0
+        roof = {"bound": "tensor", "kernel": "gemm_tma_kernel (tcgen05 kind::tf32, 3 products; split/pack included)",
+                "achieved": issued / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0, "peak": peak,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained / 2 (dense TF32 rate, of measured)",
+                "algorithmic_tflops": fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0}
+    else:
+        n_g, ms_g, fl_g, _ = fam["gemm_dmma"]
+        peak = fp64_peak_tflops(device) if rank == 0 else None
+        roof = {"bound": "tensor", "kernel": "gemm_kernel (FP64 DMMA m8n8k4)",
+                "achieved": fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0, "peak": peak,
+                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (MEASURED_PEAKS.json has no FP64 entry)"}
+    roof.update({"unit": "TFLOP/s", "frac": (roof["achieved"] / roof["peak"]) if roof["peak"] else None,
+                 "traffic": traffic_from_profile(args.config), "launches_per_sweep": n_g,
+                 "avg_launch_us": 1e3 * ms_g / max(n_g, 1), "flops_per_launch": fl_g / max(n_g, 1),
+                 "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}})
+
+    # ---- time to a converged environment: the chosen form against the FP64 plain path
+    conv = None
+    if args.converge != "none":
+        conv = {"criterion": "|E/site(sweep t) - E/site(sweep t-1)| <= 1e-7 (energy evaluations timed too)"}
+        conv["mixed_rsvd"] = converge(args.config, T, device, "rsvd", "mixed")
+        conv["fp64_rsvd"] = converge(args.config, T, device, "rsvd", "fp64")
+        if args.converge == "full":
+            conv["fp64_full_svd"] = converge(args.config, T, device, "svd", "fp64", max_sweeps=30)
+        base = conv.get("fp64_full_svd") or conv["fp64_rsvd"]
+        conv["speedup_mixed_vs_fp64_full_svd"] = (conv["fp64_full_svd"]["seconds"] / conv["mixed_rsvd"]["seconds"]
+                                                  if "fp64_full_svd" in conv else None)
+        conv["speedup_mixed_vs_fp64_rsvd"] = conv["fp64_rsvd"]["seconds"] / conv["mixed_rsvd"]["seconds"]
+        conv["abs_delta_e_mixed_vs_fp64"] = abs(conv["mixed_rsvd"]["energy_per_site"] - base["energy_per_site"])
+    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roof,
             "clocks": ck, "gpu_launches": launches, "sweep_ms": [round(t, 3) for t in times],
-            "timed_breakdown_ms": timed_breakdown}
+            "timed_breakdown_ms": timed_breakdown, "converge": conv}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 # -------------------------------------------------------- CPU oracle (reference arm)
@@ -350,10 +451,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
-    ap.add_argument("--projector", default="svd", choices=["svd", "rsvd"],
+    ap.add_argument("--projector", default="rsvd", choices=["svd", "rsvd"],
                     help="svd: full SVD (reference default); rsvd: k = chi+10, 2 power iterations")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
-                    help="mixed: 3xTF32 tensor-core contractions, FP64 projector algebra")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="mixed: 3xTF32 tcgen05 contractions, FP64 projector algebra")
+    ap.add_argument("--converge", default="full", choices=["full", "fast", "none"],
+                    help="time-to-converge arms: full = mixed rSVD, FP64 rSVD and FP64 full SVD; "
+                         "fast = without the FP64 full-SVD arm")
     ap.add_argument("--su-steps", type=int, default=None,
                     help="override the simple-update steps that prepare the tensors (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -395,13 +499,16 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64",
-                "data": "synthetic",
-                "config": {"workload": name, "precision": args.precision, "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
+                "data": "synthetic (seeded simple-update tensors of the workload's shapes)",
+                "config": {"workload": f"{name}_{args.precision}_{args.projector}", "precision": args.precision,
+                           "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
                            "projector": ("full SVD (reference default)" if args.projector == "svd"
                                          else "rSVD k=chi+10, q=2"), "parallelism": f"replicas{world}",
                            "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"], "sweep_ms": res["sweep_ms"]}
+        if res["converge"] is not None:
+            line["time_to_converge"] = res["converge"]
         if res["timed_breakdown_ms"] is not None:
             line["timed_breakdown_ms"] = res["timed_breakdown_ms"]
         print(json.dumps(line), flush=True)

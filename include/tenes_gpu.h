@@ -185,8 +185,10 @@ uint64_t tg_kernel_launch_count(void);
 tg_status tg_ctx_stream(tg_ctx* ctx, void** stream);
 
 /* Per-launch CUDA-event profiling of the library's kernel families
- * (0 = DMMA matrix product, 1 = leg permutation, 2 = max-abs normalisation,
- * 3 = Jacobi corner spectra, 4 = cuSOLVER factorisations, 5 = other).
+ * (0 = FP64 DMMA matrix product, 1 = leg permutation, 2 = max-abs
+ * normalisation, 3 = Jacobi corner spectra, 4 = dense factorisations
+ * (cuSOLVER, CholeskyQR, Jacobi SVD), 5 = other, 6 = 3xTF32 tcgen05 product
+ * including its split / pack pre-pass).
  * Adds two events per launch; off by default.  query returns the number of
  * launches, their summed device time in ms and the algorithmic flops and
  * bytes they were issued for since the last reset. */

@@ -57,13 +57,14 @@ uint64_t launch_count();
 // stream; the totals (launches, device ms, algorithmic flops / bytes) are
 // read back by tg_profile_query.
 enum ProfKind {
-  PK_GEMM = 0,       // DMMA strided batched matrix product
+  PK_GEMM = 0,       // FP64 DMMA strided batched matrix product
   PK_PERMUTE = 1,    // leg permutation
   PK_NORMALIZE = 2,  // max-abs normalisation
   PK_SPECTRUM = 3,   // batched Jacobi corner spectra
-  PK_SOLVER = 4,     // cuSOLVER factorisations (SVD, QR)
+  PK_SOLVER = 4,     // dense factorisations: cuSOLVER, CholeskyQR, Jacobi SVD of the rSVD core
   PK_OTHER = 5,      // small helpers
-  PK_COUNT = 6
+  PK_GEMM_TC = 6,    // 3xTF32 tcgen05 product, split / pack pre-pass included (flops: 2 M N K)
+  PK_COUNT = 7
 };
 void profile_enable(bool on);
 bool profile_enabled();

@@ -1734,7 +1734,7 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
             static_cast<unsigned>(d.batch));
   if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
   const double macs = static_cast<double>(d.M) * d.N * d.K * d.batch;
-  ProfScope ps(PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
+  ProfScope ps(d.prec == 1 ? PK_GEMM_TC : PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
                sizeof(T) * static_cast<double>(d.batch) * (d.M * d.K + d.K * d.N + d.M * d.N));
   // Split-K for products whose output tiles cannot fill the 148 SMs (tall-
   // skinny rSVD panels): K is cut into equal chunks written to partial

@@ -243,7 +243,8 @@ def kernel_launch_count() -> int:
     return int(_lib.load().tg_kernel_launch_count())
 
 
-PROFILE_KINDS = ("gemm_dmma", "permute", "normalize", "jacobi_spectrum", "cusolver", "other")
+PROFILE_KINDS = ("gemm_dmma", "permute", "normalize", "jacobi_spectrum", "factorisations", "other",
+                 "gemm_tcgen05")
 
 
 def profile_enable(on: bool) -> None:
