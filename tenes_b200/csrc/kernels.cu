@@ -1585,8 +1585,9 @@ void launch_tma_bn(dim3 grid, const CUtensorMap& ah, const CUtensorMap& al, cons
 
 // C = A B for one real product: both operands split into padded hi / lo TF32
 // arrays (split_pack_kernel), then the TMA-fed tcgen05 kernel over 128 x bn
-// tiles; K chunks (<= 1024 of K, enough of them to give every SM a CTA) are
-// reduced in FP64.
+// tiles; K chunks (<= 256 of K, enough of them to give every SM a CTA) are
+// reduced in FP64, which keeps the FP32 accumulation error at the level of
+// the dropped lo*lo term.
 void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, int bn, cudaStream_t st) {
   const int64_t kpad = (d.K + tma::BK - 1) / tma::BK * tma::BK, ktiles = kpad / tma::BK;
   const int64_t mpad = (d.M + tma::BM - 1) / tma::BM * tma::BM, npad = (d.N + bn - 1) / bn * bn;
@@ -1607,7 +1608,7 @@ void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, in
   const CUtensorMap mah = tf32_map(ah, mpad, kpad, tma::BM), mal = tf32_map(al, mpad, kpad, tma::BM);
   const CUtensorMap mbh = tf32_map(bh, npad, kpad, bn), mbl = tf32_map(bl, npad, kpad, bn);
   const int64_t tiles = (mpad / tma::BM) * (npad / bn);
-  int64_t nch = (ktiles + 31) / 32;
+  int64_t nch = (ktiles + 7) / 8;  // FP32 accumulation over at most 256 of K
   if (tiles < 148) nch = std::max<int64_t>(nch, std::min<int64_t>((148 + tiles - 1) / tiles, ktiles / 8));
   nch = std::max<int64_t>(1, std::min<int64_t>(nch, ktiles));
   const int64_t per = (ktiles + nch - 1) / nch;
@@ -1638,9 +1639,10 @@ void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, in
 
 // 3xTF32 product on tcgen05 (real).  The longer of M and N goes on the
 // 128-row side of the tile (C^T = B^T A^T when N > M); K is split so that
-// the CTAs fill the GPU and no FP32 accumulation runs over more than 1024
-// of K, the chunks being summed in FP64.  Single products take the TMA-fed
-// kernel, batched ones the register-staged kernel.
+// the CTAs fill the GPU and FP32 accumulation runs over short K chunks, the
+// chunks being summed in FP64 (256 of K for single products, 1024 for
+// batched ones).  Single products take the TMA-fed kernel, batched ones the
+// register-staged kernel.
 void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream_t st) {
   if (d.N > d.M) {
     GemmDesc s = d;

@@ -13,7 +13,7 @@ struct GemmDesc {
   int64_t sAm, sAk, sBk, sBn, sCm, sCn;
   int64_t bA, bB, bC;
   bool conjA, conjB, accumulate;
-  int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 on tcgen05, FP32 accumulation over K chunks <= 1024
+  int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 on tcgen05, FP32 accumulation over K chunks <= 256
                  //    summed in FP64 (real only; conjugation flags are ignored)
 };
 
