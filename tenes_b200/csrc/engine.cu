@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <random>
 #include <string>
@@ -140,6 +141,7 @@ struct EngineT final : Engine {
   ~EngineT() override {
     drop_graph();
     // release device tensors before the stream goes away
+    core_w.clear();
     Tn.clear();
     Trot.clear();
     for (auto& v : C) v.clear();
@@ -180,6 +182,24 @@ struct EngineT final : Engine {
     return tensordot<T>(a, b, x, y, st, ca, cb, cur_prec);
   }
   DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
+  // Warm-start bases of the rSVD core SVD, one per projector row of a sweep
+  // (key: direction, line, row; set by the moves), identity at first use.
+  std::map<int64_t, DT<T>> core_w;
+  int64_t core_key = -1;
+  static int64_t row_key(int dir, int line, int row) {
+    return (static_cast<int64_t>(dir) << 40) | (static_cast<int64_t>(line) << 20) | row;
+  }
+  DT<T>& core_basis(int64_t k) {
+    auto it = core_w.find(core_key);
+    if (it == core_w.end() || it->second.dim(0) != k) {
+      DT<T> w({k, k}, st);
+      identity<T>(w.p, k, st);
+      w.mem->st = main_st;  // lives as long as the context
+      it = core_w.insert_or_assign(core_key, w).first;
+    }
+    return it->second;
+  }
+
   void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.p, a.size(), d_max + slot, st); }
   // dst = a / max|a|, written into the existing storage of dst
   void normalize_into(const DT<T>& a, DT<T>& dst) {
@@ -424,11 +444,29 @@ struct EngineT final : Engine {
     const T* p;
     int64_t rows, cols, rs, cs;
     bool conj;
+    // for a left operand: its TF32 split (rows x cols); for a right operand:
+    // the split of its transpose (cols x rows).  Used by 3xTF32 products only.
+    const SplitOperand* split = nullptr;
   };
   static MV rm(const T* p, int64_t r, int64_t c) { return MV{p, r, c, c, 1, false}; }      // row-major
   static MV cm(const T* p, int64_t r, int64_t c) { return MV{p, r, c, 1, r, false}; }      // column-major
   static MV tp(MV a) { return MV{a.p, a.cols, a.rows, a.cs, a.rs, a.conj}; }               // transpose
   static MV ht(MV a) { return MV{a.p, a.cols, a.rows, a.cs, a.rs, !a.conj}; }              // conj transpose
+  static MV with_split(MV a, const SplitOperand* s) {
+    a.split = s;
+    return a;
+  }
+  // TF32 split of the left-operand view X (rows x cols), for reuse by several products
+  struct Split {
+    DT<float> buf;
+    SplitOperand op;
+  };
+  Split split_of(const MV& X) {
+    Split s;
+    s.buf = DT<float>({split_operand_floats(X.rows, X.cols)}, st);
+    split_operand(reinterpret_cast<const double*>(X.p), X.rows, X.cols, X.rs, X.cs, s.buf.p, &s.op, st);
+    return s;
+  }
   // C (rows x cols at C[i*crs + j*ccs]) = A B
   void mm(const MV& A, const MV& B, T* C, int64_t crs, int64_t ccs) {
     if (A.cols != B.rows) fail(TG_E_INPUT, "mm: inner dimensions differ");
@@ -447,6 +485,10 @@ struct EngineT final : Engine {
     g.conjB = B.conj;
     g.accumulate = false;
     g.prec = cur_prec;
+    if (cur_prec == 1) {
+      g.preA = A.split;
+      g.preB = B.split;
+    }
     gemm<T>(A.p, B.p, C, g, st);
   }
   DT<T> mm_rm(const MV& A, const MV& B) {  // row-major result
@@ -579,16 +621,17 @@ struct EngineT final : Engine {
   // the truncated, 1/sqrt(s)-scaled factors Uc (nrow x w, row-major) and
   // Vc (ncol x w, row-major), w = min(k, chi); columns past `cut` are zero.
   // Stands in for mptensor::rsvd (src/iTPS/core/ctm.cpp:243-244).
-  void rsvd_factors(const DT<T>& LTm, const DT<T>& LBm, int64_t nrow, int64_t nmid, int64_t ncol, int cut,
-                    int64_t k, DT<T>& Uc, DT<T>& Vc) {
-    const MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
+  // lt, lb: LT, LB as row-major matrices; lth, lbh: their conjugate
+  // transposes (the views may carry TF32 splits for 3xTF32 products)
+  void rsvd_factors(const MV& lt, const MV& lth, const MV& lb, const MV& lbh, int64_t nrow, int64_t nmid,
+                    int64_t ncol, int cut, int64_t k, DT<T>& Uc, DT<T>& Vc) {
     auto apply_M = [&](const DT<T>& Xcm) {  // (ncol x k) col-major -> (nrow x k) col-major
       DT<T> t = mm_cm(lb, cm(Xcm.p, ncol, k));
       return mm_cm(lt, cm(t.p, nmid, k));
     };
     auto apply_MH = [&](const DT<T>& Ycm) {  // (nrow x k) -> (ncol x k), both col-major
-      DT<T> t = mm_cm(ht(lt), cm(Ycm.p, nrow, k));
-      return mm_cm(ht(lb), cm(t.p, nmid, k));
+      DT<T> t = mm_cm(lth, cm(Ycm.p, nrow, k));
+      return mm_cm(lbh, cm(t.p, nmid, k));
     };
     DT<T> Om({k, ncol}, st);
     counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
@@ -610,7 +653,13 @@ struct EngineT final : Engine {
     DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, k)), cm(Qz.p, ncol, k));  // k x k row-major
     DT<T> Ur({k, k}, st), Wr({k, k}, st);
     DT<double> s({k}, st);
-    jacobi_svd<T>(Tm.p, k, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
+    // Jacobi from the right singular vectors this projector row had in the
+    // previous sweep: the environment changes little from sweep to sweep, so
+    // T W0 is nearly diagonal and a few Jacobi sweeps finish the SVD of T.
+    DT<T>& W0 = core_basis(k);
+    DT<T> Tw = mm_rm(rm(Tm.p, k, k), rm(W0.p, k, k));
+    jacobi_svd<T>(Tw.p, k, Ur.p, s.p, Wr.p, st, W0.p);  // T Wr = Ur S
+    TG_CUDA(cudaMemcpyAsync(W0.p, Wr.p, sizeof(T) * static_cast<size_t>(k * k), cudaMemcpyDeviceToDevice, st));
     DT<T> U = mm_rm(cm(Q.p, nrow, k), rm(Ur.p, k, k));
     DT<T> V = mm_rm(cm(Qz.p, ncol, k), rm(Wr.p, k, k));
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
@@ -650,7 +699,23 @@ struct EngineT final : Engine {
       DT<T> LTm = tr(block_LT(C1, eT1, eT8, T1), {0, 2, 4, 1, 3, 5});
       DT<T> LBm = tr(block_LB(C4, eT7, eT6, T4), {0, 2, 4, 1, 3, 5});
       const int64_t nrow = t12 * e12 * t12, nmid = t41 * e78 * t41, ncol = t34 * e56 * t34;
-      const MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
+      MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
+      MV lth = ht(lt), lbh = ht(lb);
+      // 3xTF32: LT, LB and their transposes are the left operands of every
+      // product below (six range-finder products, PU, PL); split them once
+      Split s_lt, s_lth, s_lb, s_lbh;
+      if constexpr (!CPLX) {
+        if (cur_prec == 1 && (t12 != 1 && t34 != 1) && P.use_rsvd) {
+          s_lt = split_of(lt);
+          s_lth = split_of(lth);
+          s_lb = split_of(lb);
+          s_lbh = split_of(lbh);
+          lt.split = &s_lt.op;
+          lth.split = &s_lth.op;
+          lb.split = &s_lb.op;
+          lbh.split = &s_lbh.op;
+        }
+      }
       DT<T> Uc, Vrow;  // Uc: nrow x w;  PU = LBm * Vc where Vc = (VT_c)^H
       MV vc{nullptr, 0, 0, 0, 0, false};
       if ((t12 != 1 && t34 != 1) && P.use_rsvd) {
@@ -663,7 +728,7 @@ struct EngineT final : Engine {
           fail(TG_E_INPUT, "rSVD sketch size " + std::to_string(k) + " exceeds " +
                                std::to_string(jacobi_svd_max_k<T>()) +
                                " (lower rsvd_oversampling_factor or set rsvd_oversample_abs)");
-        rsvd_factors(LTm, LBm, nrow, nmid, ncol, cut, k, Uc, Vrow);
+        rsvd_factors(lt, lth, lb, lbh, nrow, nmid, ncol, cut, k, Uc, Vrow);
         vc = rm(Vrow.p, ncol, Vrow.dim(1));
       } else {
         DT<T> M = mm_rm(lt, lb);
@@ -676,7 +741,9 @@ struct EngineT final : Engine {
       // PL = tensordot(LT, conj(U_c), Axes(0,2,4), Axes(0,1,2)).transpose(1,0,2,3)
       MV uc = rm(Uc.p, nrow, w);
       uc.conj = true;
-      PL = tr(reshape(mm_rm(tp(lt), uc), {t41, e78, t41, w}), {1, 0, 2, 3});
+      MV ltt = tp(lt);
+      ltt.split = lth.split;  // real operands: transpose = conjugate transpose
+      PL = tr(reshape(mm_rm(ltt, uc), {t41, e78, t41, w}), {1, 0, 2, 3});
     } else {
       PU = DT<T>({e78, 1, 1, e78}, st);
       identity<T>(PU.p, e78, st);
@@ -772,6 +839,7 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
+      core_key = row_key(0, ix, iy);
       if (P.projector_corner)
         proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
       else
@@ -808,6 +876,7 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
+      core_key = row_key(1, ix, iy);
       if (P.projector_corner)
         proj_left_block(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], rot(k, 0), rot(j, 0), PUs[iy], PLs[iy]);
       else
@@ -844,6 +913,7 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
+      core_key = row_key(2, iy, ix);
       if (P.projector_corner)
         proj_left_block(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], rot(j, 1), rot(i, 1), PUs[ix], PLs[ix]);
       else
@@ -880,6 +950,7 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
+      core_key = row_key(3, iy, ix);
       if (P.projector_corner)
         proj_left_block(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], rot(l, 2), rot(k, 2), PUs[ix], PLs[ix]);
       else

@@ -1209,7 +1209,8 @@ __global__ void upper_to_rh_kernel(const T* __restrict__ acm, int64_t lda, int64
 // One-sided Jacobi SVD with vectors; see jacobi_svd() in kernels.cuh.
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
-                                                          double* __restrict__ S, T* __restrict__ Wout) {
+                                                          double* __restrict__ S, T* __restrict__ Wout,
+                                                          const T* __restrict__ Winit) {
   extern __shared__ double sm[];
   const int nn = n * n;
   double* ar = sm;
@@ -1223,10 +1224,11 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
     const int r = idx / n, c = idx % n;
     const T v = A[idx];
     ar[c * n + r] = re_of(v);
-    wr[c * n + r] = (r == c) ? 1.0 : 0.0;
+    const T w0 = Winit ? Winit[idx] : ((r == c) ? one_of<T>() : zero_of<T>());
+    wr[c * n + r] = re_of(w0);
     if constexpr (CPLX) {
       ai[c * n + r] = im_of(v);
-      wi[c * n + r] = 0.0;
+      wi[c * n + r] = im_of(w0);
     }
   }
   __syncthreads();
@@ -1385,119 +1387,163 @@ __global__ void sum_partials_kernel(const T* __restrict__ parts, int nparts, int
   }
 }
 
+
+// Complex-or-real arithmetic for the blocked factorisation below.
+__device__ __forceinline__ double vmul(double a, double b) { return a * b; }
+__device__ __forceinline__ cplx vmul(cplx a, cplx b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double vadd(double a, double b) { return a + b; }
+__device__ __forceinline__ cplx vadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double vsub(double a, double b) { return a - b; }
+__device__ __forceinline__ cplx vsub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double vneg(double a) { return -a; }
+__device__ __forceinline__ cplx vneg(cplx a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double shfl_v(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ cplx shfl_v(cplx v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
 // Inverse Cholesky factor of an equilibrated (optionally shifted) Gram
-// matrix summed from split-K partials; one CTA, everything in shared memory.
-// Right-looking Cholesky (A' = R'^H R', R' upper) and right-looking
-// triangular inverse, each k steps with the trailing work spread over the CTA.
-// See chol_rinv() in kernels.cuh.
+// matrix summed from split-K partials, one CTA, blocked by 8: kp = k rounded up to 8,
+// the padding being the identity.  Cholesky (upper, A' = R'^H R'), three
+// barriers per 8-column block: warp 0 factors the 8 x 8 diagonal block in
+// registers (lane c holds column c, rows exchanged by shuffles), one thread
+// per column solves the block row R'_JK = R'_JJ^{-H} A'_JK, all threads
+// update the trailing triangle.  Then R' is inverted in place, two barriers
+// per block: warp 0 inverts the diagonal block, the column block above it
+// becomes -X[0:j0, 0:j0] R'[0:j0, J] X_JJ.  Rinv = D X as before.  One copy
+// of the matrix lives in shared memory (kp^2 values), plus an 8 x kp panel.
 template <typename T, bool CPLX>
-__global__ void __launch_bounds__(1024) chol_rinv_kernel(const T* __restrict__ parts, int nparts, int k,
-                                                         double shift, T* __restrict__ Rinv, int* flag) {
-  extern __shared__ double sm[];
+__global__ void __launch_bounds__(512) chol_rinv_blocked_kernel(const T* __restrict__ parts, int nparts, int k,
+                                                                 double shift, T* __restrict__ Rinv, int* flag) {
+  extern __shared__ __align__(16) unsigned char chol_smem[];
+  const int kp = (k + 7) & ~7, nb = kp / 8;
+  T* A = reinterpret_cast<T*>(chol_smem);  // kp x kp, row-major
+  T* P = A + kp * kp;                      // panel, kp x 8
+  double* d = reinterpret_cast<double*>(P + 8 * kp);
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int kk = k * k;
-  double* ar = sm;                          // A' -> R' (upper), row-major
-  double* ai = sm + kk;                     // complex only
-  double* xr = sm + (CPLX ? 2 : 1) * kk;    // X = R'^{-1} (upper), row-major
-  double* xi = xr + kk;                     // complex only
-  double* d = sm + (CPLX ? 4 : 2) * kk;     // equilibration D
-  double* rs = d + k;                       // 1 / sqrt of the Cholesky pivots
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
-  for (int idx = tid; idx < kk; idx += nt) {
-    double sr = 0.0, si = 0.0;
-    for (int p = 0; p < nparts; ++p) {
-      const T v = parts[static_cast<int64_t>(p) * kk + idx];
-      sr += re_of(v);
-      si += im_of(v);
+  for (int idx = tid; idx < kp * kp; idx += nt) {
+    const int r = idx / kp, c = idx - r * kp;
+    T v = (r == c) ? one_of<T>() : zero_of<T>();
+    if (r < k && c < k) {
+      v = zero_of<T>();
+      for (int p = 0; p < nparts; ++p) v = vadd(v, parts[static_cast<int64_t>(p) * kk + r * k + c]);
     }
-    ar[idx] = sr;
-    if constexpr (CPLX) ai[idx] = si;
+    A[idx] = v;
   }
   __syncthreads();
-  for (int i = tid; i < k; i += nt) {
-    const double g = ar[i * k + i];
-    d[i] = g > 0.0 ? 1.0 / sqrt(g) : 1.0;
+  for (int i = tid; i < kp; i += nt) {
+    const double g = re_of(A[i * kp + i]);
+    d[i] = (i < k && g > 0.0) ? 1.0 / sqrt(g) : 1.0;
   }
   __syncthreads();
-  for (int idx = tid; idx < kk; idx += nt) {
-    const int r = idx / k, c = idx - r * k;
-    ar[idx] = ar[idx] * d[r] * d[c] + ((r == c) ? shift : 0.0);
-    if constexpr (CPLX) ai[idx] *= d[r] * d[c];
-    xr[idx] = (r == c) ? 1.0 : 0.0;
-    if constexpr (CPLX) xi[idx] = 0.0;
-  }
-  __syncthreads();
-  // Cholesky on the upper triangle, one barrier per step: step j subtracts
-  // conj(A'_jr) A'_jc / A'_jj from the trailing rows r > j (row j itself is
-  // left unscaled and only read); the rows are scaled by 1/sqrt(A'_jj) at
-  // the end.  Warps over rows, lanes over columns.
-  for (int j = 0; j < k; ++j) {
-    const double a = ar[j * k + j];
-    if (!(a > 0.0)) {
-      if (tid == 0 && flag) atomicExch(flag, 1);
-      continue;  // same decision in every thread: the row stays as it is
+  for (int idx = tid; idx < kp * kp; idx += nt) {
+    const int r = idx / kp, c = idx - r * kp;
+    if (r < k && c < k) {
+      T v = mul_real(A[idx], d[r] * d[c]);
+      if (r == c) v = vadd(v, mul_real(one_of<T>(), shift));
+      A[idx] = v;
     }
-    const double inv_a = 1.0 / a;
-    for (int r = j + 1 + warp; r < k; r += nwarp) {
-      const double ur = ar[j * k + r] * inv_a;
-      const double ui = CPLX ? ai[j * k + r] * inv_a : 0.0;
-      for (int c = r + lane; c < k; c += 32) {
-        const double vr = ar[j * k + c];
-        if constexpr (CPLX) {
-          const double vi = ai[j * k + c];
-          ar[r * k + c] -= ur * vr + ui * vi;
-          ai[r * k + c] -= ur * vi - ui * vr;
-        } else {
-          ar[r * k + c] -= ur * vr;
+  }
+  __syncthreads();
+  // ---- blocked Cholesky
+  for (int J = 0; J < nb; ++J) {
+    const int j0 = 8 * J;
+    if (warp == 0) {
+      const int c = lane & 7;
+      T col[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) col[r] = (r <= c) ? A[(j0 + r) * kp + j0 + c] : zero_of<T>();
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        double p = __shfl_sync(0xffffffffu, re_of(col[j]), j);
+        if (!(p > 0.0)) {
+          if (lane == 0 && flag) atomicExch(flag, 1);
+          p = 1.0;
         }
+        const double inv = 1.0 / sqrt(p);
+        if (c >= j) col[j] = mul_real(col[j], inv);
+#pragma unroll
+        for (int r = j + 1; r < 8; ++r) {
+          const T rjr = shfl_v(col[j], r);  // R'_{j0+j, j0+r}
+          if (c >= r) col[r] = vsub(col[r], vmul(conj_of(rjr), col[j]));
+        }
+      }
+      if (lane < 8) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (r <= c) A[(j0 + r) * kp + j0 + c] = col[r];
       }
     }
     __syncthreads();
-  }
-  // R'_jc = A'_jc / sqrt(A'_jj) (a non-positive pivot counts as 1)
-  for (int i = tid; i < k; i += nt) {
-    const double a = ar[i * k + i];
-    rs[i] = (a > 0.0) ? 1.0 / sqrt(a) : 1.0;
-  }
-  __syncthreads();
-  for (int idx = tid; idx < kk; idx += nt) {
-    const int r = idx / k, c = idx - r * k;
-    if (c < r) continue;
-    ar[idx] *= rs[r];
-    if constexpr (CPLX) ai[idx] *= rs[r];
-  }
-  __syncthreads();
-  // X = R'^{-1} by backward substitution, one barrier per step: once row i of
-  // the accumulator is final, X[i,:] = acc[i,:] / R'_ii and every row r < i
-  // takes off R'_ri X[i,:]; rows are divided by their diagonal at the end.
-  for (int i = k - 1; i > 0; --i) {
-    const double inv = 1.0 / ar[i * k + i];
-    for (int r = warp; r < i; r += nwarp) {  // rows above i, columns i .. k-1
-      const double rr = ar[r * k + i] * inv;
-      const double ri = CPLX ? ai[r * k + i] * inv : 0.0;
-      for (int c = i + lane; c < k; c += 32) {
-        const double x_r = xr[i * k + c];
-        if constexpr (CPLX) {
-          const double x_i = xi[i * k + c];
-          xr[r * k + c] -= rr * x_r - ri * x_i;
-          xi[r * k + c] -= rr * x_i + ri * x_r;
-        } else {
-          xr[r * k + c] -= rr * x_r;
-        }
+    for (int c = j0 + 8 + tid; c < kp; c += nt) {  // block row: solve R'_JJ^H x = a
+      T x[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) x[r] = A[(j0 + r) * kp + c];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+#pragma unroll
+        for (int m = 0; m < r; ++m) x[r] = vsub(x[r], vmul(conj_of(A[(j0 + m) * kp + j0 + r]), x[m]));
+        x[r] = mul_real(x[r], 1.0 / re_of(A[(j0 + r) * kp + j0 + r]));
       }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) A[(j0 + r) * kp + c] = x[r];
+    }
+    __syncthreads();
+    const int n2 = kp - j0 - 8;
+    for (int idx = tid; idx < n2 * n2; idx += nt) {  // trailing triangle
+      const int r = j0 + 8 + idx / n2, c = j0 + 8 + idx % n2;
+      if (c < r) continue;
+      T acc = zero_of<T>();
+#pragma unroll
+      for (int m = 0; m < 8; ++m) acc = vadd(acc, vmul(conj_of(A[(j0 + m) * kp + r]), A[(j0 + m) * kp + c]));
+      A[r * kp + c] = vsub(A[r * kp + c], acc);
     }
     __syncthreads();
   }
-  // Rinv = D X (upper), X[r,:] = acc[r,:] / R'_rr
-  for (int idx = tid; idx < kk; idx += nt) {
-    const int r = idx / k, c = idx - r * k;
-    const bool up = c >= r;
-    const double s = d[r] / ar[r * k + r];
-    if constexpr (CPLX) {
-      Rinv[idx] = make_double2(up ? xr[idx] * s : 0.0, up ? xi[idx] * s : 0.0);
-    } else {
-      Rinv[idx] = up ? xr[idx] * s : 0.0;
+  // ---- in-place blocked inverse of the upper triangle
+  for (int J = 0; J < nb; ++J) {
+    const int j0 = 8 * J;
+    // Y = X[0:j0, 0:j0] R'[0:j0, J]  (X upper, already inverted)
+    for (int idx = tid; idx < j0 * 8; idx += nt) {
+      const int i = idx >> 3, c = idx & 7;
+      T acc = zero_of<T>();
+      for (int m = i; m < j0; ++m) acc = vadd(acc, vmul(A[i * kp + m], A[m * kp + j0 + c]));
+      P[idx] = acc;
     }
+    if (warp == 0) {  // X_JJ = R'_JJ^{-1}: lane c solves R'_JJ x = e_c
+      const int c = lane & 7;
+      T x[8];
+#pragma unroll
+      for (int r = 7; r >= 0; --r) {
+        T s = (r == c) ? one_of<T>() : zero_of<T>();
+#pragma unroll
+        for (int m = r + 1; m < 8; ++m)
+          if (m <= c) s = vsub(s, vmul(A[(j0 + r) * kp + j0 + m], x[m]));
+        x[r] = (r <= c) ? mul_real(s, 1.0 / re_of(A[(j0 + r) * kp + j0 + r])) : zero_of<T>();
+      }
+      __syncwarp();
+      if (lane < 8) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+          if (r <= c) A[(j0 + r) * kp + j0 + c] = x[r];
+      }
+    }
+    __syncthreads();
+    // X[0:j0, J] = -Y X_JJ
+    for (int idx = tid; idx < j0 * 8; idx += nt) {
+      const int i = idx >> 3, c = idx & 7;
+      T acc = zero_of<T>();
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m <= c) acc = vadd(acc, vmul(P[i * 8 + m], A[(j0 + m) * kp + j0 + c]));
+      A[i * kp + j0 + c] = vneg(acc);
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < kk; idx += nt) {  // Rinv = D X (upper)
+    const int r = idx / k, c = idx - r * k;
+    Rinv[idx] = (c >= r) ? mul_real(A[r * kp + c], d[r]) : zero_of<T>();
   }
 }
 
@@ -1592,21 +1638,41 @@ void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, in
   const int64_t kpad = (d.K + tma::BK - 1) / tma::BK * tma::BK, ktiles = kpad / tma::BK;
   const int64_t mpad = (d.M + tma::BM - 1) / tma::BM * tma::BM, npad = (d.N + bn - 1) / bn * bn;
   if (mpad / tma::BM > 65535 || ktiles > (int64_t{1} << 30)) fail(TG_E_INPUT, "gemm: problem too large");
+  // operands split by the caller are used as they are; the others are split here
+  auto usable = [&](const SplitOperand* s, int64_t rows, int64_t rows_pad_needed) {
+    return s && s->hi && s->rows == rows && s->K == d.K && s->kpad == kpad && s->rows_pad >= rows_pad_needed;
+  };
+  const bool pa = usable(d.preA, d.M, mpad), pb = usable(d.preB, d.N, npad);
   void* sbuf = nullptr;
-  TG_CUDA(cudaMallocAsync(&sbuf, sizeof(float) * 2 * (mpad + npad) * kpad, st));
+  const int64_t na = pa ? 0 : mpad * kpad, nbf = pb ? 0 : npad * kpad;
+  if (na + nbf > 0) TG_CUDA(cudaMallocAsync(&sbuf, sizeof(float) * 2 * (na + nbf), st));
   float* ah = static_cast<float*>(sbuf);
-  float* al = ah + mpad * kpad;
-  float* bh = al + mpad * kpad;
-  float* bl = bh + npad * kpad;
-  split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(mpad / 32)), 256, 0, st>>>(
-      A, d.M, d.K, d.sAm, d.sAk, kpad, ah, al);
-  TG_CHECK_LAUNCH();
-  split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(npad / 32)), 256, 0, st>>>(
-      B, d.N, d.K, d.sBn, d.sBk, kpad, bh, bl);
-  TG_CHECK_LAUNCH();
-  count_launch(2);
-  const CUtensorMap mah = tf32_map(ah, mpad, kpad, tma::BM), mal = tf32_map(al, mpad, kpad, tma::BM);
-  const CUtensorMap mbh = tf32_map(bh, npad, kpad, bn), mbl = tf32_map(bl, npad, kpad, bn);
+  float* al = ah + na;
+  float* bh = al + na;
+  float* bl = bh + nbf;
+  int64_t arows = mpad, brows = npad;
+  if (pa) {
+    ah = const_cast<float*>(d.preA->hi);
+    al = const_cast<float*>(d.preA->lo);
+    arows = d.preA->rows_pad;
+  } else {
+    split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(mpad / 32)), 256, 0, st>>>(
+        A, d.M, d.K, d.sAm, d.sAk, kpad, ah, al);
+    TG_CHECK_LAUNCH();
+    count_launch();
+  }
+  if (pb) {
+    bh = const_cast<float*>(d.preB->hi);
+    bl = const_cast<float*>(d.preB->lo);
+    brows = d.preB->rows_pad;
+  } else {
+    split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(npad / 32)), 256, 0, st>>>(
+        B, d.N, d.K, d.sBn, d.sBk, kpad, bh, bl);
+    TG_CHECK_LAUNCH();
+    count_launch();
+  }
+  const CUtensorMap mah = tf32_map(ah, arows, kpad, tma::BM), mal = tf32_map(al, arows, kpad, tma::BM);
+  const CUtensorMap mbh = tf32_map(bh, brows, kpad, bn), mbl = tf32_map(bl, brows, kpad, bn);
   const int64_t tiles = (mpad / tma::BM) * (npad / bn);
   int64_t nch = (ktiles + 7) / 8;  // FP32 accumulation over at most 256 of K
   if (tiles < 148) nch = std::max<int64_t>(nch, std::min<int64_t>((148 + tiles - 1) / tiles, ktiles / 8));
@@ -1634,7 +1700,28 @@ void gemm_tma(const double* A, const double* B, double* C, const GemmDesc& d, in
     count_launch();
     TG_CUDA(cudaFreeAsync(pbuf, st));
   }
-  TG_CUDA(cudaFreeAsync(sbuf, st));
+  if (sbuf) TG_CUDA(cudaFreeAsync(sbuf, st));
+}
+
+int64_t split_operand_floats(int64_t rows, int64_t K) {
+  const int64_t kpad = (K + tma::BK - 1) / tma::BK * tma::BK, rpad = (rows + tma::BM - 1) / tma::BM * tma::BM;
+  return 2 * rpad * kpad;
+}
+
+void split_operand(const double* X, int64_t rows, int64_t K, int64_t s_r, int64_t s_k, float* buf,
+                   SplitOperand* out, cudaStream_t st) {
+  const int64_t kpad = (K + tma::BK - 1) / tma::BK * tma::BK, rpad = (rows + tma::BM - 1) / tma::BM * tma::BM;
+  ProfScope ps(PK_GEMM_TC, st, 0.0, 16.0 * static_cast<double>(rows) * K);
+  split_pack_kernel<<<dim3(static_cast<unsigned>(kpad / 32), static_cast<unsigned>(rpad / 32)), 256, 0, st>>>(
+      X, rows, K, s_r, s_k, kpad, buf, buf + rpad * kpad);
+  TG_CHECK_LAUNCH();
+  count_launch();
+  out->hi = buf;
+  out->lo = buf + rpad * kpad;
+  out->rows = rows;
+  out->K = K;
+  out->rows_pad = rpad;
+  out->kpad = kpad;
 }
 
 // 3xTF32 product on tcgen05 (real).  The longer of M and N goes on the
@@ -1656,6 +1743,8 @@ void gemm_tc(const double* A, const double* B, double* C, GemmDesc d, cudaStream
     s.sCn = d.sCm;
     s.bA = d.bB;
     s.bB = d.bA;
+    s.preA = d.preB;
+    s.preB = d.preA;
     std::swap(A, B);
     d = s;
   }
@@ -2042,7 +2131,7 @@ int jacobi_svd_max_k() {
 }
 
 template <typename T>
-void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st) {
+void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, const T* Winit) {
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "jacobi_svd: k out of range");
   const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k) + sizeof(int) * k;
@@ -2053,7 +2142,7 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st) {
     attr_bytes = smem;
   }
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
-  jacobi_svd_kernel<T, CPLX><<<1, 1024, smem, st>>>(A, static_cast<int>(k), U, S, W);
+  jacobi_svd_kernel<T, CPLX><<<1, 1024, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
   TG_CHECK_LAUNCH();
   count_launch();
 }
@@ -2079,10 +2168,11 @@ template <typename T>
 void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st) {
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
-  const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + 2 * k);
+  const int64_t kp = (k + 7) / 8 * 8;
+  const size_t smem = sizeof(T) * static_cast<size_t>(kp * kp + 8 * kp) + sizeof(double) * static_cast<size_t>(kp);
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(chol_rinv_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TG_CUDA(cudaFuncSetAttribute(chol_rinv_blocked_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     attr_bytes = smem;
   }
@@ -2091,7 +2181,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   const double u = 1.1102230246251565e-16;
   const double s = shift ? 11.0 * (static_cast<double>(n) * k + static_cast<double>(k) * (k + 1)) * u * k : 0.0;
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * static_cast<double>(k) * k * k / 3.0, 0.0);
-  chol_rinv_kernel<T, CPLX><<<1, 1024, smem, st>>>(parts, nparts, static_cast<int>(k), s, Rinv, flag);
+  chol_rinv_blocked_kernel<T, CPLX><<<1, 512, smem, st>>>(parts, nparts, static_cast<int>(k), s, Rinv, flag);
   TG_CHECK_LAUNCH();
   count_launch();
 }
@@ -2103,7 +2193,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   template void counter_normal<T>(T*, int64_t, int64_t, uint64_t, uint64_t, cudaStream_t);       \
   template void upper_to_rh<T>(const T*, int64_t, int64_t, T*, cudaStream_t);                    \
   template int jacobi_svd_max_k<T>();                                                            \
-  template void jacobi_svd<T>(const T*, int64_t, T*, double*, T*, cudaStream_t);                 \
+  template void jacobi_svd<T>(const T*, int64_t, T*, double*, T*, cudaStream_t, const T*);       \
   template void gemm<T>(const T*, const T*, T*, const GemmDesc&, cudaStream_t);                  \
   template void permute<T>(const T*, T*, const Shape&, const std::vector<int>&, bool,            \
                            cudaStream_t);                                                        \

@@ -5,6 +5,19 @@
 
 namespace tg {
 
+// An FP64 operand X(r, k) = X[r*s_r + k*s_k] split once into TF32 hi / lo
+// arrays of shape [rows_pad][kpad] (rows padded to 128, K to 32), for
+// operands that several 3xTF32 products share.
+struct SplitOperand {
+  const float* hi = nullptr;
+  const float* lo = nullptr;
+  int64_t rows = 0, K = 0, rows_pad = 0, kpad = 0;
+};
+// floats of buffer split_operand needs for rows x K
+int64_t split_operand_floats(int64_t rows, int64_t K);
+void split_operand(const double* X, int64_t rows, int64_t K, int64_t s_r, int64_t s_k, float* buf,
+                   SplitOperand* out, cudaStream_t st);
+
 // Strided batched matrix product C[b] (+)= op(A[b]) * op(B[b]) on the FP64
 // tensor cores (DMMA m8n8k4).  Element (m,k) of A is A[m*sAm + k*sAk]; one of
 // sAm / sAk must be 1 for coalesced tile loads, the other stride is free.
@@ -15,6 +28,9 @@ struct GemmDesc {
   bool conjA, conjB, accumulate;
   int prec = 0;  // 0: FP64 DMMA; 1: 3xTF32 on tcgen05, FP32 accumulation over K chunks <= 256
                  //    summed in FP64 (real only; conjugation flags are ignored)
+  // prec 1, single products: already-split copies of A (rows M) / B (rows N, i.e. B^T), if any
+  const SplitOperand* preA = nullptr;
+  const SplitOperand* preB = nullptr;
 };
 
 template <typename T>
@@ -89,8 +105,11 @@ void upper_to_rh(const T* acm, int64_t lda, int64_t k, T* out, cudaStream_t st);
 // right vectors, in one CTA with A and W resident in shared memory:
 // A W = U S, singular values descending.  U, W written row-major (k x k,
 // column j = j-th singular vector), S (k).  k <= jacobi_svd_max_k<T>().
+// With Winit the accumulated rotations start from Winit instead of the
+// identity: pass A = B Winit (Winit unitary) and the result is the SVD of B,
+// B W = U S -- a warm start when Winit already nearly diagonalises B.
 template <typename T>
-void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st);
+void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, const T* Winit = nullptr);
 template <typename T>
 int jacobi_svd_max_k();
 
