@@ -141,7 +141,6 @@ struct EngineT final : Engine {
   ~EngineT() override {
     drop_graph();
     // release device tensors before the stream goes away
-    core_w.clear();
     Tn.clear();
     Trot.clear();
     for (auto& v : C) v.clear();
@@ -182,24 +181,6 @@ struct EngineT final : Engine {
     return tensordot<T>(a, b, x, y, st, ca, cb, cur_prec);
   }
   DT<T> tr(const DT<T>& a, const V& p) { return transpose<T>(a, p, st); }
-  // Warm-start bases of the rSVD core SVD, one per projector row of a sweep
-  // (key: direction, line, row; set by the moves), identity at first use.
-  std::map<int64_t, DT<T>> core_w;
-  int64_t core_key = -1;
-  static int64_t row_key(int dir, int line, int row) {
-    return (static_cast<int64_t>(dir) << 40) | (static_cast<int64_t>(line) << 20) | row;
-  }
-  DT<T>& core_basis(int64_t k) {
-    auto it = core_w.find(core_key);
-    if (it == core_w.end() || it->second.dim(0) != k) {
-      DT<T> w({k, k}, st);
-      identity<T>(w.p, k, st);
-      w.mem->st = main_st;  // lives as long as the context
-      it = core_w.insert_or_assign(core_key, w).first;
-    }
-    return it->second;
-  }
-
   void normalize(DT<T>& a) { normalize_max_abs<T>(a.p, a.p, a.size(), d_max + slot, st); }
   // dst = a / max|a|, written into the existing storage of dst
   void normalize_into(const DT<T>& a, DT<T>& dst) {
@@ -653,13 +634,10 @@ struct EngineT final : Engine {
     DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, k)), cm(Qz.p, ncol, k));  // k x k row-major
     DT<T> Ur({k, k}, st), Wr({k, k}, st);
     DT<double> s({k}, st);
-    // Jacobi from the right singular vectors this projector row had in the
-    // previous sweep: the environment changes little from sweep to sweep, so
-    // T W0 is nearly diagonal and a few Jacobi sweeps finish the SVD of T.
-    DT<T>& W0 = core_basis(k);
-    DT<T> Tw = mm_rm(rm(Tm.p, k, k), rm(W0.p, k, k));
-    jacobi_svd<T>(Tw.p, k, Ur.p, s.p, Wr.p, st, W0.p);  // T Wr = Ur S
-    TG_CUDA(cudaMemcpyAsync(W0.p, Wr.p, sizeof(T) * static_cast<size_t>(k * k), cudaMemcpyDeviceToDevice, st));
+    // (The previous sweep's right singular vectors are no warm start here: T
+    // is expressed in the CholeskyQR basis of Z, which rotates within the
+    // kept subspace from sweep to sweep, so a cold start needs fewer sweeps.)
+    jacobi_svd<T>(Tm.p, k, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
     DT<T> U = mm_rm(cm(Q.p, nrow, k), rm(Ur.p, k, k));
     DT<T> V = mm_rm(cm(Qz.p, ncol, k), rm(Wr.p, k, k));
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
@@ -839,7 +817,6 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
-      core_key = row_key(0, ix, iy);
       if (P.projector_corner)
         proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
       else
@@ -876,7 +853,6 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
-      core_key = row_key(1, ix, iy);
       if (P.projector_corner)
         proj_left_block(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], rot(k, 0), rot(j, 0), PUs[iy], PLs[iy]);
       else
@@ -913,7 +889,6 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
-      core_key = row_key(2, iy, ix);
       if (P.projector_corner)
         proj_left_block(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], rot(j, 1), rot(i, 1), PUs[ix], PLs[ix]);
       else
@@ -950,7 +925,6 @@ struct EngineT final : Engine {
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
-      core_key = row_key(3, iy, ix);
       if (P.projector_corner)
         proj_left_block(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], rot(l, 2), rot(k, 2), PUs[ix], PLs[ix]);
       else

@@ -1220,6 +1220,10 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
   double* nrm = sm + (CPLX ? 4 : 2) * nn;     // n
   int* pos = reinterpret_cast<int*>(nrm + n);  // n
   __shared__ int rotated;
+#ifdef TG_JACOBI_TRACE
+  __shared__ int trace_rot;
+  if (threadIdx.x == 0) trace_rot = 0;
+#endif
   for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
     const int r = idx / n, c = idx % n;
     const T v = A[idx];
@@ -1312,11 +1316,19 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
           }
         }
         if (gl == 0) rotated = 1;
+#ifdef TG_JACOBI_TRACE
+        if (gl == 0) atomicAdd(&trace_rot, 1);
+#endif
       }
       __syncthreads();
     }
     const int any = rotated;
     __syncthreads();
+#ifdef TG_JACOBI_TRACE  // sweep log for tuning builds (off in the library)
+    if (threadIdx.x == 0) printf("jacobi_svd n=%d sweep=%d rotations=%d\n", n, sweep, trace_rot);
+    __syncthreads();
+    if (threadIdx.x == 0) trace_rot = 0;
+#endif
     if (!any) break;
   }
   for (int c = warp; c < n; c += nw) {
@@ -1420,6 +1432,7 @@ __global__ void __launch_bounds__(512) chol_rinv_blocked_kernel(const T* __restr
   T* A = reinterpret_cast<T*>(chol_smem);  // kp x kp, row-major
   T* P = A + kp * kp;                      // panel, kp x 8
   double* d = reinterpret_cast<double*>(P + 8 * kp);
+  double* dinv = d + kp;  // 1 / R'_ii
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int kk = k * k;
   for (int idx = tid; idx < kp * kp; idx += nt) {
@@ -1461,7 +1474,8 @@ __global__ void __launch_bounds__(512) chol_rinv_blocked_kernel(const T* __restr
           if (lane == 0 && flag) atomicExch(flag, 1);
           p = 1.0;
         }
-        const double inv = 1.0 / sqrt(p);
+        const double inv = rsqrt(p);  // 1 / R'_jj, kept for the solves below
+        if (lane == j) dinv[j0 + j] = inv;
         if (c >= j) col[j] = mul_real(col[j], inv);
 #pragma unroll
         for (int r = j + 1; r < 8; ++r) {
@@ -1484,7 +1498,7 @@ __global__ void __launch_bounds__(512) chol_rinv_blocked_kernel(const T* __restr
       for (int r = 0; r < 8; ++r) {
 #pragma unroll
         for (int m = 0; m < r; ++m) x[r] = vsub(x[r], vmul(conj_of(A[(j0 + m) * kp + j0 + r]), x[m]));
-        x[r] = mul_real(x[r], 1.0 / re_of(A[(j0 + r) * kp + j0 + r]));
+        x[r] = mul_real(x[r], dinv[j0 + r]);
       }
 #pragma unroll
       for (int r = 0; r < 8; ++r) A[(j0 + r) * kp + c] = x[r];
@@ -1520,7 +1534,7 @@ __global__ void __launch_bounds__(512) chol_rinv_blocked_kernel(const T* __restr
 #pragma unroll
         for (int m = r + 1; m < 8; ++m)
           if (m <= c) s = vsub(s, vmul(A[(j0 + r) * kp + j0 + m], x[m]));
-        x[r] = (r <= c) ? mul_real(s, 1.0 / re_of(A[(j0 + r) * kp + j0 + r])) : zero_of<T>();
+        x[r] = (r <= c) ? mul_real(s, dinv[j0 + r]) : zero_of<T>();
       }
       __syncwarp();
       if (lane < 8) {
@@ -2169,7 +2183,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
   const int64_t kp = (k + 7) / 8 * 8;
-  const size_t smem = sizeof(T) * static_cast<size_t>(kp * kp + 8 * kp) + sizeof(double) * static_cast<size_t>(kp);
+  const size_t smem = sizeof(T) * static_cast<size_t>(kp * kp + 8 * kp) + sizeof(double) * static_cast<size_t>(2 * kp);
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
     TG_CUDA(cudaFuncSetAttribute(chol_rinv_blocked_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
