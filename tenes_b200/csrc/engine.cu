@@ -956,7 +956,8 @@ struct EngineT final : Engine {
   // zero-pad / slice X to the static environment shape, into `out`'s storage
   void fit(const DT<T>& X, int64_t d1, int64_t d2, int64_t rest, DT<T>& out) {
     const int64_t chi = P.chi;
-    Shape s = rest == 1 ? Shape{chi, chi} : Shape{chi, chi, X.dim(4), X.dim(5)};
+    // corners are rank 2; edges keep their two physical-bond legs even when those are 1
+    Shape s = out.rank() == 2 ? Shape{chi, chi} : Shape{chi, chi, X.dim(4), X.dim(5)};
     if (s != out.sh) fail(TG_E_RUNTIME, "environment initialisation: shape mismatch");
     fit_chi<T>(X.p, d1, d2, rest, out.p, chi, st);
   }
