@@ -166,6 +166,8 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
   const int wn = (warp >> 1) * 32;
   const bool a_kc = (d.sAk == 1);  // A contiguous along k
   const bool b_nc = (d.sBn == 1);  // B contiguous along n
+  // split-K launches: the last chunk may be shorter
+  const int64_t Kz = (d.klast > 0 && blockIdx.z == gridDim.z - 1) ? d.klast : d.K;
 
   T ra[8], rb[8];
   auto load_tiles = [&](int64_t k0) {
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
         kk = idx / GBM;
       }
       const int64_t gm = m0 + mm, gk = k0 + kk;
-      ra[i] = (gm < d.M && gk < d.K) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
+      ra[i] = (gm < d.M && gk < Kz) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
       int nn, kb;
       if (b_nc) {
         nn = idx % GBN;
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
         nn = idx / GBK;
       }
       const int64_t gn = n0 + nn, gkb = k0 + kb;
-      rb[i] = (gn < d.N && gkb < d.K) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
+      rb[i] = (gn < d.N && gkb < Kz) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
     }
   };
   auto store_tiles = [&](int stage) {
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
       for (int j = 0; j < 4; ++j) acc_i[i][j][0] = acc_i[i][j][1] = 0.0;
   }
 
-  const int64_t nk = (d.K + GBK - 1) / GBK;
+  const int64_t nk = (Kz + GBK - 1) / GBK;
   load_tiles(0);
   store_tiles(0);
   __syncthreads();
@@ -1854,8 +1856,9 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   auto launch = [&](dim3 gr, const GemmParams<T>& gp) { gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp); };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
-  if (d.batch == 1 && tiles < 148 && d.K >= 1024)
-    split = std::min<int64_t>((296 + tiles - 1) / tiles, d.K / 512);
+  // up to two CTAs per SM (the kernel's occupancy), K chunks of at least 128
+  if (d.batch == 1 && tiles < 148 && d.K >= 256)
+    split = std::min<int64_t>(std::max<int64_t>(1, 296 / tiles), (d.K + 127) / 128);
 #ifdef TG_GEMM_TRACE  // shape log for tuning builds (off in the library)
   fprintf(stderr, "gemm M=%lld N=%lld K=%lld batch=%lld sAm=%lld sAk=%lld sBk=%lld sBn=%lld split=%lld prec=%d\n",
           (long long)d.M, (long long)d.N, (long long)d.K, (long long)d.batch, (long long)d.sAm, (long long)d.sAk,
@@ -1867,9 +1870,10 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
     count_launch();
     return;
   }
-  const int64_t chunk = (d.K / split + GBK - 1) / GBK * GBK;  // multiple of the k tile
-  const int64_t nfull = d.K / chunk, rem = d.K - nfull * chunk;
-  const int64_t nparts = nfull + (rem > 0 ? 1 : 0);
+  // all chunks in one launch (z = chunk, the last one possibly shorter), then an FP64 sum
+  const int64_t chunk = (d.K + split - 1) / split;
+  const int64_t chunk16 = (chunk + GBK - 1) / GBK * GBK;  // multiple of the k tile
+  const int64_t nparts = (d.K + chunk16 - 1) / chunk16;
   void* buf = nullptr;
   TG_CUDA(cudaMallocAsync(&buf, sizeof(T) * nparts * d.M * d.N, st));
   T* parts = static_cast<T*>(buf);
@@ -1877,24 +1881,18 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   g.sCm = d.N;
   g.sCn = 1;
   g.accumulate = false;
-  g.K = chunk;
-  g.batch = nfull;
-  g.bA = chunk * d.sAk;
-  g.bB = chunk * d.sBk;
+  g.K = chunk16;
+  g.klast = d.K - (nparts - 1) * chunk16;
+  g.batch = nparts;
+  g.bA = chunk16 * d.sAk;
+  g.bB = chunk16 * d.sBk;
   g.bC = d.M * d.N;
-  dim3 g1(grid.x, grid.y, static_cast<unsigned>(nfull));
-  launch(g1, GemmParams<T>{A, B, parts, g});
+  launch(dim3(grid.x, grid.y, static_cast<unsigned>(nparts)), GemmParams<T>{A, B, parts, g});
   TG_CHECK_LAUNCH();
-  if (rem > 0) {
-    g.K = rem;
-    g.batch = 1;
-    launch(grid, GemmParams<T>{A + nfull * chunk * d.sAk, B + nfull * chunk * d.sBk, parts + nfull * d.M * d.N, g});
-    TG_CHECK_LAUNCH();
-  }
   splitk_reduce_kernel<T><<<num_blocks(d.M * d.N, 256), 256, 0, st>>>(parts, static_cast<int>(nparts), d.M, d.N,
                                                                        C, d.sCm, d.sCn, d.accumulate);
   TG_CHECK_LAUNCH();
-  count_launch(rem > 0 ? 3 : 2);
+  count_launch(2);
   TG_CUDA(cudaFreeAsync(buf, st));
 }
 

@@ -31,6 +31,8 @@ struct GemmDesc {
   // prec 1, single products: already-split copies of A (rows M) / B (rows N, i.e. B^T), if any
   const SplitOperand* preA = nullptr;
   const SplitOperand* preB = nullptr;
+  // FP64 product, > 0: the last batch entry contracts only klast of its K (split-K chunks of one launch)
+  int64_t klast = 0;
 };
 
 template <typename T>
