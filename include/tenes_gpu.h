@@ -212,6 +212,14 @@ tg_status tg_gemm_host(int64_t M, int64_t N, int64_t K, const double* A, int64_t
                        const double* B, int64_t sBk, int64_t sBn, double* C, int64_t sCm, int64_t sCn,
                        int prec);
 
+/* Orthonormal basis of the span of a real column-major n x k host panel Y
+ * (in place) by the engine's shifted CholeskyQR: `passes` passes, the first
+ * two shifted, a perturbation of relative size 1e-14 after the first, all in
+ * one launch of one thread-block cluster.  *pivot_flag = 1 if a Cholesky
+ * pivot was not positive.  k <= 96.  For tests of the kernel; the CTMRG path
+ * calls it inside the rSVD projectors (src/iTPS/core/ctm.cpp:243-244). */
+tg_status tg_cholqr_host(int64_t n, int64_t k, double* Y, int passes, int* pivot_flag);
+
 /* Allocation-free corner spectra.  No counterpart in the reference: it exists
  * for callers that must not allocate device memory where they need the
  * spectra -- code that runs under a fixed device-memory budget, hosts that

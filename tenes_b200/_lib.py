@@ -28,7 +28,7 @@ EXPORTED = [
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
-    "tg_bench_gemm", "tg_gemm_host",
+    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host",
 ]
 
 
@@ -103,6 +103,7 @@ def load() -> C.CDLL:
         "tg_bench_gemm": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int, dp]),
         "tg_gemm_host": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, dp, C.c_int64, C.c_int64, dp, C.c_int64,
                                    C.c_int64, dp, C.c_int64, C.c_int64, C.c_int]),
+        "tg_cholqr_host": (C.c_int, [C.c_int64, C.c_int64, dp, C.c_int, P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

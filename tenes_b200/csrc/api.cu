@@ -1,5 +1,6 @@
 // C ABI of libtenes_gpu (declared in include/tenes_gpu.h).  Every entry point
 // converts C++ exceptions into tg_status codes; nothing is thrown across it.
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -282,6 +283,30 @@ extern "C" tg_status tg_gemm_host(int64_t M, int64_t N, int64_t K, const double*
     cudaFree(dC);
     cudaStreamDestroy(st);
     if (fault) tg::fail(TG_E_RUNTIME, "tensor-core product stopped waiting for its MMAs");
+  });
+}
+
+extern "C" tg_status tg_cholqr_host(int64_t n, int64_t k, double* Y, int passes, int* pivot_flag) {
+  return guard([&] {
+    if (n < 1 || k < 1 || k > n || passes < 1 || !Y) tg::fail(TG_E_INPUT, "bad CholeskyQR arguments");
+    if (!tg::cholqr_cluster_supported(n, k)) tg::fail(TG_E_INPUT, "CholeskyQR panel shape not supported");
+    cudaStream_t st;
+    TG_CUDA(cudaStreamCreate(&st));
+    double* dY = nullptr;
+    int* dflag = nullptr;
+    TG_CUDA(cudaMalloc(&dY, sizeof(double) * n * k));
+    TG_CUDA(cudaMalloc(&dflag, sizeof(int)));
+    TG_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), st));
+    TG_CUDA(cudaMemcpyAsync(dY, Y, sizeof(double) * n * k, cudaMemcpyHostToDevice, st));
+    tg::cholqr_cluster(dY, n, k, passes, 2, 1, 1e-14 / std::sqrt(static_cast<double>(n)), dflag, st);
+    int flag = 0;
+    TG_CUDA(cudaMemcpyAsync(Y, dY, sizeof(double) * n * k, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaMemcpyAsync(&flag, dflag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dY);
+    cudaFree(dflag);
+    cudaStreamDestroy(st);
+    if (pivot_flag) *pivot_flag = flag;
   });
 }
 

@@ -583,6 +583,12 @@ struct EngineT final : Engine {
   // iteration, whose next product and orthonormalisation only use the span.
   void orth_chol(DT<T>& Y, int64_t n, int64_t k, int passes = 4) {
     PrecScope fp64(this, 0);
+    if constexpr (!CPLX) {
+      if (cholqr_cluster_supported(n, k)) {
+        cholqr_cluster(Y.p, n, k, passes, 2, ++noise_stream, 1e-14 / std::sqrt(static_cast<double>(n)), d_flag, st);
+        return;
+      }
+    }
     for (int pass = 0; pass < passes; ++pass) {
       int nparts = 0;
       DT<T> parts = gram_parts(Y, n, k, &nparts);

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <string>
 
+#include "counter_rng.cuh"
 #include "kernels.cuh"
 
 namespace tg {
@@ -1164,22 +1165,6 @@ __global__ void __launch_bounds__(256) jacobi_spectrum_kernel(const T* const* ma
   if (threadIdx.x == 0 && sweeps_used) sweeps_used[blockIdx.x] = sweep;
 }
 
-// splitmix64 finaliser on a Weyl sequence; the CPU oracle's counter_normal
-// (oracle/tenes_oracle.py) computes the same numbers.
-__device__ __forceinline__ double counter_uniform(uint64_t idx, uint64_t key) {
-  uint64_t z = idx * 0x9E3779B97F4A7C15ull + key;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  z = z ^ (z >> 31);
-  return (static_cast<double>(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
-}
-
-__device__ __forceinline__ double counter_gauss(uint64_t n, uint64_t key) {
-  const double u1 = counter_uniform(2 * n, key);
-  const double u2 = counter_uniform(2 * n + 1, key);
-  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
-}
-
 template <typename T>
 __global__ void counter_normal_kernel(T* __restrict__ out, int64_t rows, int64_t cols, uint64_t key_re,
                                       uint64_t key_im) {
@@ -1374,10 +1359,10 @@ __global__ void add_noise_kernel(T* __restrict__ x, int64_t len, double scale, u
        n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     T v = x[n];
     if constexpr (is_cplx<T>::value) {
-      v.x += scale * counter_gauss(static_cast<uint64_t>(n), key_re);
-      v.y += scale * counter_gauss(static_cast<uint64_t>(n), key_im);
+      v.x += scale * counter_unit_uniform(static_cast<uint64_t>(n), key_re);
+      v.y += scale * counter_unit_uniform(static_cast<uint64_t>(n), key_im);
     } else {
-      v += scale * counter_gauss(static_cast<uint64_t>(n), key_re);
+      v += scale * counter_unit_uniform(static_cast<uint64_t>(n), key_re);
     }
     x[n] = v;
   }
@@ -2161,9 +2146,7 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
 
 template <typename T>
 void add_noise(T* x, int64_t len, double scale, uint64_t stream, cudaStream_t st) {
-  const uint64_t base = 0xD1B54A32D192ED03ull;  // keys disjoint from the rSVD test matrices
-  const uint64_t k_re = base + (2 * stream) * 0xBF58476D1CE4E5B9ull;
-  const uint64_t k_im = base + (2 * stream + 1) * 0xBF58476D1CE4E5B9ull;
+  const uint64_t k_re = noise_key_re(stream), k_im = noise_key_im(stream);
   add_noise_kernel<T><<<num_blocks(len, 256), 256, 0, st>>>(x, len, scale, k_re, k_im);
   TG_CHECK_LAUNCH();
   count_launch();

@@ -115,8 +115,9 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
 template <typename T>
 int jacobi_svd_max_k();
 
-// x[i] += scale * N(0,1) (counter-based, key derived from `stream`; complex
-// entries get independent real and imaginary parts)
+// x[i] += scale * u_i, u_i counter-based uniform numbers of mean 0 and
+// variance 1 (key derived from `stream`; complex entries get independent real
+// and imaginary parts)
 template <typename T>
 void add_noise(T* x, int64_t len, double scale, uint64_t stream, cudaStream_t st);
 
@@ -132,6 +133,17 @@ void sum_partials(const T* parts, int nparts, int64_t len, T* out, cudaStream_t 
 // flag[0] is set to 1 if a pivot is not positive.  k <= jacobi_svd_max_k<T>().
 template <typename T>
 void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* Rinv, int* flag, cudaStream_t st);
+
+// Shifted CholeskyQR of a real column-major n x k panel Y in place, all
+// `passes` passes in one launch of one thread-block cluster: the first
+// `shifted_passes` add the shift of chol_rinv, and after the first pass the
+// perturbation noise_scale * u of add_noise(stream noise_stream) is added.
+// flag[0] = 1 if a pivot is not positive.  Callable when
+// cholqr_cluster_supported(n, k) (k <= 96 and a device that runs clusters of
+// 8 or 16 CTAs with the kernel's shared memory).
+bool cholqr_cluster_supported(int64_t n, int64_t k);
+void cholqr_cluster(double* Y, int64_t n, int64_t k, int passes, int shifted_passes, uint64_t noise_stream,
+                    double noise_scale, int* flag, cudaStream_t st);
 
 // y += alpha x (alpha real)
 template <typename T>
