@@ -292,18 +292,20 @@ extern "C" tg_status tg_cholqr_host(int64_t n, int64_t k, double* Y, int passes,
     if (!tg::cholqr_cluster_supported(n, k)) tg::fail(TG_E_INPUT, "CholeskyQR panel shape not supported");
     cudaStream_t st;
     TG_CUDA(cudaStreamCreate(&st));
-    double* dY = nullptr;
+    double *dY = nullptr, *dscr = nullptr;
     int* dflag = nullptr;
     TG_CUDA(cudaMalloc(&dY, sizeof(double) * n * k));
+    TG_CUDA(cudaMalloc(&dscr, sizeof(double) * tg::cholqr_scratch_doubles(k)));
     TG_CUDA(cudaMalloc(&dflag, sizeof(int)));
     TG_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), st));
     TG_CUDA(cudaMemcpyAsync(dY, Y, sizeof(double) * n * k, cudaMemcpyHostToDevice, st));
-    tg::cholqr_cluster(dY, n, k, passes, 2, 1, 1e-14 / std::sqrt(static_cast<double>(n)), dflag, st);
+    tg::cholqr_cluster(dY, n, k, passes, 2, 1, 1e-14 / std::sqrt(static_cast<double>(n)), dscr, dflag, st);
     int flag = 0;
     TG_CUDA(cudaMemcpyAsync(Y, dY, sizeof(double) * n * k, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaMemcpyAsync(&flag, dflag, sizeof(int), cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
     cudaFree(dY);
+    cudaFree(dscr);
     cudaFree(dflag);
     cudaStreamDestroy(st);
     if (pivot_flag) *pivot_flag = flag;

@@ -39,6 +39,7 @@ constexpr int CQ_KPMAX = 8 * CQ_NBMAX;
 constexpr int CQ_RB = 176;          // rows of Y staged per chunk of the Gram phase
 constexpr int CQ_LDY = CQ_RB + 4;   // 180 = 4 (mod 16): conflict-free fragment loads
 constexpr int CQ_SLOTS = (CQ_NBMAX * (CQ_NBMAX + 1) / 2 + CQ_WARPS - 1) / CQ_WARPS;
+constexpr int CQ_NU = 3;  // 8-row blocks a warp solves together
 
 __device__ __forceinline__ void dmma_acc(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -180,8 +181,8 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
 }
 
 __global__ void __launch_bounds__(CQ_THREADS, 1)
-    cholqr_cluster_kernel(double* Y, int n, int k, int passes, int shifted, double shift, double noise_scale,
-                          unsigned long long noise_key, int* flag) {
+    cholqr_cluster_kernel(double* Y, double* scratch, int n, int k, int passes, int shifted, double shift,
+                          double noise_scale, unsigned long long noise_key, int* flag) {
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = static_cast<int>(cluster.block_rank());
   const int cs = static_cast<int>(cluster.num_blocks());
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #ifdef TG_CQ_TRACE
   unsigned call = 0;
-  unsigned long long tt[4][8];
+  unsigned long long tt[4][8] = {};
   if (rank == 0 && tid == 0) call = atomicAdd(&g_cq_calls, 1u);
   const bool trace = rank == 0 && tid == 0 && passes == 4 && ((call % 24) == 10 || (call % 24) == 11);
 #define CQ_T(p, i) \
@@ -321,20 +322,29 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
         }
       }
       __syncthreads();
+#ifdef TG_CQ_TRACE
+      if (trace && pass < 4) tt[pass][7] = cq_now();
+#endif
       cholesky_blocked(Rs, kp, ld, dinv, btab, flag);
+      // R' and D to the global scratch, read from L2 by the other CTAs (a
+      // broadcast from one SM's shared memory would serialise on that SM)
+      for (int e = tid; e < total; e += CQ_THREADS) {
+        const int off = entry(e);
+        scratch[off] = Rs[off];
+      }
+      for (int i = tid; i < kp; i += CQ_THREADS) scratch[kp * ld + i] = ds[i];
+      __threadfence();
     }
     cluster.sync();
     CQ_T(pass, 4)
-    // ---- 4. R' and D from CTA 0
+    // ---- 4. R' and D from the scratch (L2 only: the lines change every pass)
     if (rank != 0) {
-      const double* R0 = cluster.map_shared_rank(Rs, 0);
-      const double* d0 = cluster.map_shared_rank(ds, 0);
 #pragma unroll 4
       for (int e = tid; e < total; e += CQ_THREADS) {
         const int off = entry(e);
-        Rs[off] = R0[off];
+        Rs[off] = __ldcg(scratch + off);
       }
-      for (int i = tid; i < kp; i += CQ_THREADS) ds[i] = d0[i];
+      for (int i = tid; i < kp; i += CQ_THREADS) ds[i] = __ldcg(scratch + kp * ld + i);
       __syncthreads();
     }
     CQ_T(pass, 5)
@@ -345,25 +355,25 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       if (!resident) stage(rc, nr);
       const int nrb = nr8 / 8;
       const int g = lane >> 2, t = lane & 3;
-      for (int rb0 = warp; rb0 < nrb; rb0 += 2 * CQ_WARPS) {
-        // row blocks rb0 and rb0 + CQ_WARPS, two independent chains; an absent
-        // second block recomputes the rows of the first and stores nothing.
+      for (int rb0 = warp; rb0 < nrb; rb0 += CQ_NU * CQ_WARPS) {
+        // row blocks rb0 + u CQ_WARPS, u < CQ_NU: independent chains; an
+        // absent block recomputes the rows of the first and stores nothing.
         // The solved blocks X_I are read back from U as A fragments.
-        bool val[2];
-        int rb8[2];
+        bool val[CQ_NU];
+        int rb8[CQ_NU];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < CQ_NU; ++u) {
           val[u] = rb0 + u * CQ_WARPS < nrb;
-          rb8[u] = (val[u] ? rb0 + u * CQ_WARPS : rb0) * 8;
+          rb8[u] = (val[u] ? rb0 + u * CQ_WARPS : rb0) * 8 + g;
         }
 #pragma unroll 1
         for (int J = 0; J < nb; ++J) {
           const int c0 = 8 * J + 2 * t;
-          double a0[2], a1[2], b0[2], b1[2];
+          double a0[CQ_NU], a1[CQ_NU], b0[CQ_NU], b1[CQ_NU];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            a0[u] = U[c0 * CQ_LDY + rb8[u] + g] * ds[c0];
-            a1[u] = U[(c0 + 1) * CQ_LDY + rb8[u] + g] * ds[c0 + 1];
+          for (int u = 0; u < CQ_NU; ++u) {
+            a0[u] = U[c0 * CQ_LDY + rb8[u]] * ds[c0];
+            a1[u] = U[(c0 + 1) * CQ_LDY + rb8[u]] * ds[c0 + 1];
             b0[u] = b1[u] = 0.0;
           }
           // a -= X_I R'_IJ over I < J, even I into a, odd I into b
@@ -376,24 +386,24 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
               const double bva = Rs[ra * ld + 8 * J + g];
               const double bvb = odd ? Rs[rb * ld + 8 * J + g] : 0.0;
 #pragma unroll
-              for (int u = 0; u < 2; ++u) {
-                dmma_acc(a0[u], a1[u], -U[ra * CQ_LDY + rb8[u] + g], bva);
-                if (odd) dmma_acc(b0[u], b1[u], -U[rb * CQ_LDY + rb8[u] + g], bvb);
+              for (int u = 0; u < CQ_NU; ++u) {
+                dmma_acc(a0[u], a1[u], -U[ra * CQ_LDY + rb8[u]], bva);
+                if (odd) dmma_acc(b0[u], b1[u], -U[rb * CQ_LDY + rb8[u]], bvb);
               }
             }
           }
           const double d0 = Rs[(8 * J + t) * ld + 8 * J + g];
           const double d1 = Rs[(8 * J + 4 + t) * ld + 8 * J + g];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
+          for (int u = 0; u < CQ_NU; ++u) {
             double f0, f1;
             acc_to_afrag(a0[u] + b0[u], a1[u] + b1[u], lane, f0, f1);
             double x0 = 0.0, x1 = 0.0;
             dmma_acc(x0, x1, f0, d0);
             dmma_acc(x0, x1, f1, d1);
             if (val[u]) {
-              U[c0 * CQ_LDY + rb8[u] + g] = x0;
-              U[(c0 + 1) * CQ_LDY + rb8[u] + g] = x1;
+              U[c0 * CQ_LDY + rb8[u]] = x0;
+              U[(c0 + 1) * CQ_LDY + rb8[u]] = x1;
             }
           }
           __syncwarp();  // X_J visible to the warp's later A-fragment loads
@@ -418,9 +428,10 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
 #ifdef TG_CQ_TRACE
   if (trace) {
     for (int p = 0; p < 4; ++p)
-      printf("cq n=%d k=%d pass %d: gram %.1f  sync %.1f  reduce %.1f  chol %.1f  copy %.1f  trsm %.1f us\n", n, k, p,
-             (tt[p][1] - tt[p][0]) * 1e-3, (tt[p][2] - tt[p][1]) * 1e-3, (tt[p][3] - tt[p][2]) * 1e-3,
-             (tt[p][4] - tt[p][3]) * 1e-3, (tt[p][5] - tt[p][4]) * 1e-3, (tt[p][6] - tt[p][5]) * 1e-3);
+      printf("cq n=%d k=%d pass %d: gram %.1f  sync %.1f  reduce %.1f  chol %.1f (prep %.1f)  copy %.1f  trsm %.1f us\n",
+             n, k, p, (tt[p][1] - tt[p][0]) * 1e-3, (tt[p][2] - tt[p][1]) * 1e-3, (tt[p][3] - tt[p][2]) * 1e-3,
+             (tt[p][4] - tt[p][3]) * 1e-3, (tt[p][7] - tt[p][3]) * 1e-3, (tt[p][5] - tt[p][4]) * 1e-3,
+             (tt[p][6] - tt[p][5]) * 1e-3);
   }
 #endif
 #undef CQ_T
@@ -474,8 +485,13 @@ bool cholqr_cluster_supported(int64_t n, int64_t k) {
   return k >= 1 && k <= CQ_KPMAX && n >= 1 && n * k < (int64_t(1) << 31) && cholqr_cluster_size() > 0;
 }
 
+int64_t cholqr_scratch_doubles(int64_t k) {
+  const int64_t kp = (k + 7) / 8 * 8;
+  return kp * (kp + ((20 - (kp & 15)) & 15)) + kp;
+}
+
 void cholqr_cluster(double* Y, int64_t n, int64_t k, int passes, int shifted_passes, uint64_t noise_stream,
-                    double noise_scale, int* flag, cudaStream_t st) {
+                    double noise_scale, double* scratch, int* flag, cudaStream_t st) {
   if (!cholqr_cluster_supported(n, k)) fail(TG_E_INPUT, "cholqr_cluster: unsupported panel shape");
   const int cs = cholqr_cluster_size();
   const int kp = static_cast<int>((k + 7) / 8 * 8);
@@ -498,7 +514,7 @@ void cholqr_cluster(double* Y, int64_t n, int64_t k, int passes, int shifted_pas
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    TG_CUDA(cudaLaunchKernelEx(&cfg, cholqr_cluster_kernel, Y, static_cast<int>(n), static_cast<int>(k), passes,
+    TG_CUDA(cudaLaunchKernelEx(&cfg, cholqr_cluster_kernel, Y, scratch, static_cast<int>(n), static_cast<int>(k), passes,
                                shifted_passes, s, noise_scale,
                                static_cast<unsigned long long>(noise_key_re(noise_stream)), flag));
     count_launch();

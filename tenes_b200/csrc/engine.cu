@@ -585,7 +585,9 @@ struct EngineT final : Engine {
     PrecScope fp64(this, 0);
     if constexpr (!CPLX) {
       if (cholqr_cluster_supported(n, k)) {
-        cholqr_cluster(Y.p, n, k, passes, 2, ++noise_stream, 1e-14 / std::sqrt(static_cast<double>(n)), d_flag, st);
+        DT<double> scratch({cholqr_scratch_doubles(k)}, st);
+        cholqr_cluster(Y.p, n, k, passes, 2, ++noise_stream, 1e-14 / std::sqrt(static_cast<double>(n)), scratch.p,
+                       d_flag, st);
         return;
       }
     }

@@ -141,9 +141,11 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
 // flag[0] = 1 if a pivot is not positive.  Callable when
 // cholqr_cluster_supported(n, k) (k <= 96 and a device that runs clusters of
 // 8 or 16 CTAs with the kernel's shared memory).
+// `scratch` holds cholqr_scratch_doubles(k) doubles of device memory.
 bool cholqr_cluster_supported(int64_t n, int64_t k);
+int64_t cholqr_scratch_doubles(int64_t k);
 void cholqr_cluster(double* Y, int64_t n, int64_t k, int passes, int shifted_passes, uint64_t noise_stream,
-                    double noise_scale, int* flag, cudaStream_t st);
+                    double noise_scale, double* scratch, int* flag, cudaStream_t st);
 
 // y += alpha x (alpha real)
 template <typename T>
