@@ -1225,12 +1225,23 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int np = n + (n & 1);
-  const double tol = static_cast<double>(n) * 2.220446049250313e-16;
+  const double tol = static_cast<double>(n) * 2.220446049250313e-16, tol2 = tol * tol;
   const double small2 = tol * tol * block_sumsq<CPLX>(ar, ai, nn);  // rounding-noise columns
   // each column pair is handled by a group of kJG lanes (32 / kJG pairs per warp)
   constexpr int kJG = 16;
   const int grp = lane / kJG, gl = lane % kJG;
   for (int sweep = 0; sweep < 60; ++sweep) {
+    // squared column norms, exact at the start of every sweep and updated with
+    // each rotation (alpha' = alpha - t g, beta' = beta + t g) within it
+    for (int c = warp; c < n; c += nw) {
+      double a = 0;
+      for (int r = lane; r < n; r += 32) {
+        a += ar[c * n + r] * ar[c * n + r];
+        if constexpr (CPLX) a += ai[c * n + r] * ai[c * n + r];
+      }
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+      if (lane == 0) nrm[c] = a;
+    }
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
     for (int rnd = 0; rnd < np - 1; ++rnd) {
@@ -1249,35 +1260,55 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
             q = t;
           }
         }
-        double al = 0, be = 0, gr = 0, gi = 0;
+        double gr = 0, gi = 0, gr2 = 0, gi2 = 0;  // two accumulators: shorter FP64 chains
         if (valid) {
-          for (int r = gl; r < n; r += kJG) {
-            const double pr_ = ar[p * n + r], qr_ = ar[q * n + r];
-            al += pr_ * pr_;
-            be += qr_ * qr_;
-            gr += pr_ * qr_;
+          int r = gl;
+          for (; r + kJG < n; r += 2 * kJG) {
+            const double p0 = ar[p * n + r], q0 = ar[q * n + r];
+            const double p1 = ar[p * n + r + kJG], q1 = ar[q * n + r + kJG];
+            gr += p0 * q0;
+            gr2 += p1 * q1;
             if constexpr (CPLX) {
-              const double pi_ = ai[p * n + r], qi_ = ai[q * n + r];
-              al += pi_ * pi_;
-              be += qi_ * qi_;
-              gr += pi_ * qi_;
-              gi += pr_ * qi_ - pi_ * qr_;
+              const double pi0 = ai[p * n + r], qi0 = ai[q * n + r];
+              const double pi1 = ai[p * n + r + kJG], qi1 = ai[q * n + r + kJG];
+              gr += pi0 * qi0;
+              gr2 += pi1 * qi1;
+              gi += p0 * qi0 - pi0 * q0;
+              gi2 += p1 * qi1 - pi1 * q1;
+            }
+          }
+          if (r < n) {
+            const double p0 = ar[p * n + r], q0 = ar[q * n + r];
+            gr += p0 * q0;
+            if constexpr (CPLX) {
+              const double pi0 = ai[p * n + r], qi0 = ai[q * n + r];
+              gr += pi0 * qi0;
+              gi += p0 * qi0 - pi0 * q0;
             }
           }
         }
+        gr += gr2;
+        gi += gi2;
         for (int o = kJG / 2; o > 0; o >>= 1) {  // reduce within the lane group
-          al += __shfl_xor_sync(0xffffffffu, al, o, kJG);
-          be += __shfl_xor_sync(0xffffffffu, be, o, kJG);
           gr += __shfl_xor_sync(0xffffffffu, gr, o, kJG);
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o, kJG);
         }
+        const double al = valid ? nrm[p] : 0.0, be = valid ? nrm[q] : 0.0;
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
-        if (!valid || g == 0.0 || al <= small2 || be <= small2 || g <= tol * sqrt(al * be)) continue;
+        if (!valid || g == 0.0 || al <= small2 || be <= small2 || g * g <= tol2 * al * be) continue;
+        // b = phase * a_q with a_p . b = g > 0; the rotation that zeroes it has
+        // t = sign(tau) 2g / (|tau| + sqrt(tau^2 + 4 g^2)), tau = beta - alpha
+        // (the smaller root of t^2 + 2 zeta t - 1 = 0, zeta = tau / 2g), in
+        // rsqrt steps only; c = 1 / sqrt(1 + t^2) keeps c^2 + s^2 = 1 to
+        // rounding whatever the accuracy of t
         const double ph_r = CPLX ? gr / g : (gr >= 0 ? 1.0 : -1.0);
         const double ph_i = CPLX ? -gi / g : 0.0;
-        const double zeta = (be - al) / (2.0 * g);
-        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        const double tau = be - al;
+        const double w = fma(tau, tau, 4.0 * g * g);
+        const double den = fabs(tau) + w * rsqrt(w);
+        const double rd = rsqrt(den);
+        const double t = copysign(2.0 * g, tau) * (rd * rd);
+        const double c = rsqrt(fma(t, t, 1.0)), s = c * t;
         for (int r = gl; r < n; r += kJG) {
           {
             const double xpr = ar[p * n + r], xqr = ar[q * n + r];
@@ -1302,7 +1333,11 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
             }
           }
         }
-        if (gl == 0) rotated = 1;
+        if (gl == 0) {
+          nrm[p] = al - t * g;
+          nrm[q] = be + t * g;
+          rotated = 1;
+        }
 #ifdef TG_JACOBI_TRACE
         if (gl == 0) atomicAdd(&trace_rot, 1);
 #endif
@@ -2139,7 +2174,10 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
     attr_bytes = smem;
   }
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
-  jacobi_svd_kernel<T, CPLX><<<1, 1024, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
+  // 16 lanes per column pair, at most 1024 threads
+  const int npairs = static_cast<int>((k + 1) / 2);
+  const int threads = static_cast<int>(std::min<int64_t>(1024, (npairs * 16 + 31) / 32 * 32));
+  jacobi_svd_kernel<T, CPLX><<<1, threads, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
   TG_CHECK_LAUNCH();
   count_launch();
 }
