@@ -1194,8 +1194,15 @@ __global__ void upper_to_rh_kernel(const T* __restrict__ acm, int64_t lda, int64
 }
 
 // One-sided Jacobi SVD with vectors; see jacobi_svd() in kernels.cuh.
-template <typename T, bool CPLX>
-__global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
+// Column pairs of a round-robin schedule are handled by groups of kJG lanes;
+// lane gl of a group holds rows gl + kJG i (i < RPL) of the pair's two
+// columns in registers for the round: one batch of loads, the dot product,
+// the rotation and the update in registers, one batch of stores (the right
+// vectors are loaded only for pairs that rotate).  Squared column norms are
+// exact at the start of every sweep and updated with each rotation
+// (alpha' = alpha - t g, beta' = beta + t g).
+template <typename T, bool CPLX, int kJG, int RPL>
+__global__ void __launch_bounds__(kJG == 16 ? 768 : 1024) jacobi_svd_kernel(const T* __restrict__ A, int n, T* __restrict__ U,
                                                           double* __restrict__ S, T* __restrict__ Wout,
                                                           const T* __restrict__ Winit) {
   extern __shared__ double sm[];
@@ -1210,6 +1217,8 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
 #ifdef TG_JACOBI_TRACE
   __shared__ int trace_rot;
   if (threadIdx.x == 0) trace_rot = 0;
+  unsigned long long trace_t0;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(trace_t0));
 #endif
   for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
     const int r = idx / n, c = idx % n;
@@ -1227,12 +1236,8 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
   const int np = n + (n & 1);
   const double tol = static_cast<double>(n) * 2.220446049250313e-16, tol2 = tol * tol;
   const double small2 = tol * tol * block_sumsq<CPLX>(ar, ai, nn);  // rounding-noise columns
-  // each column pair is handled by a group of kJG lanes (32 / kJG pairs per warp)
-  constexpr int kJG = 16;
   const int grp = lane / kJG, gl = lane % kJG;
   for (int sweep = 0; sweep < 60; ++sweep) {
-    // squared column norms, exact at the start of every sweep and updated with
-    // each rotation (alpha' = alpha - t g, beta' = beta + t g) within it
     for (int c = warp; c < n; c += nw) {
       double a = 0;
       for (int r = lane; r < n; r += 32) {
@@ -1247,7 +1252,12 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
     for (int rnd = 0; rnd < np - 1; ++rnd) {
       for (int base = warp * (32 / kJG); base < np / 2; base += nw * (32 / kJG)) {
         const int pr = base + grp;
-        auto player = [&](int kk) { return kk == 0 ? 0 : ((kk - 1 + rnd) % (np - 1)) + 1; };
+        // position kk of the round-robin circle (0 fixed, the others rotating)
+        auto player = [&](int kk) {
+          if (kk == 0) return 0;
+          const int x = kk - 1 + rnd;  // < 2 (np - 1)
+          return (x >= np - 1 ? x - (np - 1) : x) + 1;
+        };
         int p = 0, q = 0;
         bool valid = pr < np / 2;
         if (valid) {
@@ -1260,35 +1270,33 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
             q = t;
           }
         }
-        double gr = 0, gi = 0, gr2 = 0, gi2 = 0;  // two accumulators: shorter FP64 chains
-        if (valid) {
-          int r = gl;
-          for (; r + kJG < n; r += 2 * kJG) {
-            const double p0 = ar[p * n + r], q0 = ar[q * n + r];
-            const double p1 = ar[p * n + r + kJG], q1 = ar[q * n + r + kJG];
-            gr += p0 * q0;
-            gr2 += p1 * q1;
-            if constexpr (CPLX) {
-              const double pi0 = ai[p * n + r], qi0 = ai[q * n + r];
-              const double pi1 = ai[p * n + r + kJG], qi1 = ai[q * n + r + kJG];
-              gr += pi0 * qi0;
-              gr2 += pi1 * qi1;
-              gi += p0 * qi0 - pi0 * q0;
-              gi2 += p1 * qi1 - pi1 * q1;
-            }
+        double xp[RPL], xq[RPL], yp[CPLX ? RPL : 1], yq[CPLX ? RPL : 1];
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          const int r = gl + i * kJG;
+          const bool ok = valid && r < n;
+          xp[i] = ok ? ar[p * n + r] : 0.0;
+          xq[i] = ok ? ar[q * n + r] : 0.0;
+          if constexpr (CPLX) {
+            yp[i] = ok ? ai[p * n + r] : 0.0;
+            yq[i] = ok ? ai[q * n + r] : 0.0;
           }
-          if (r < n) {
-            const double p0 = ar[p * n + r], q0 = ar[q * n + r];
-            gr += p0 * q0;
-            if constexpr (CPLX) {
-              const double pi0 = ai[p * n + r], qi0 = ai[q * n + r];
-              gr += pi0 * qi0;
-              gi += p0 * qi0 - pi0 * q0;
-            }
+        }
+        double gr = 0, gi = 0, gr2 = 0, gi2 = 0;  // two accumulators: shorter FP64 chains
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          double& a = (i & 1) ? gr2 : gr;
+          a = fma(xp[i], xq[i], a);
+          if constexpr (CPLX) {
+            double& b = (i & 1) ? gi2 : gi;
+            a = fma(yp[i], yq[i], a);
+            b = fma(xp[i], yq[i], b);
+            b = fma(-yp[i], xq[i], b);
           }
         }
         gr += gr2;
         gi += gi2;
+#pragma unroll
         for (int o = kJG / 2; o > 0; o >>= 1) {  // reduce within the lane group
           gr += __shfl_xor_sync(0xffffffffu, gr, o, kJG);
           if constexpr (CPLX) gi += __shfl_xor_sync(0xffffffffu, gi, o, kJG);
@@ -1296,6 +1304,18 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
         const double al = valid ? nrm[p] : 0.0, be = valid ? nrm[q] : 0.0;
         const double g = CPLX ? hypot(gr, gi) : fabs(gr);
         if (!valid || g == 0.0 || al <= small2 || be <= small2 || g * g <= tol2 * al * be) continue;
+        // real: the right vectors of the pair, issued before the rotation
+        // arithmetic; complex: loaded in the update (register budget)
+        double vp[CPLX ? 1 : RPL], vq[CPLX ? 1 : RPL];
+        if constexpr (!CPLX) {
+#pragma unroll
+          for (int i = 0; i < RPL; ++i) {
+            const int r = gl + i * kJG;
+            const bool ok = r < n;
+            vp[i] = ok ? wr[p * n + r] : 0.0;
+            vq[i] = ok ? wr[q * n + r] : 0.0;
+          }
+        }
         // b = phase * a_q with a_p . b = g > 0; the rotation that zeroes it has
         // t = sign(tau) 2g / (|tau| + sqrt(tau^2 + 4 g^2)), tau = beta - alpha
         // (the smaller root of t^2 + 2 zeta t - 1 = 0, zeta = tau / 2g), in
@@ -1309,27 +1329,28 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
         const double rd = rsqrt(den);
         const double t = copysign(2.0 * g, tau) * (rd * rd);
         const double c = rsqrt(fma(t, t, 1.0)), s = c * t;
-        for (int r = gl; r < n; r += kJG) {
-          {
-            const double xpr = ar[p * n + r], xqr = ar[q * n + r];
-            const double xpi = CPLX ? ai[p * n + r] : 0.0, xqi = CPLX ? ai[q * n + r] : 0.0;
-            const double bqr = xqr * ph_r - xqi * ph_i, bqi = xqr * ph_i + xqi * ph_r;
-            ar[p * n + r] = c * xpr - s * bqr;
-            ar[q * n + r] = s * xpr + c * bqr;
+#pragma unroll
+        for (int i = 0; i < RPL; ++i) {
+          const int r = gl + i * kJG;
+          if (r < n) {
             if constexpr (CPLX) {
-              ai[p * n + r] = c * xpi - s * bqi;
-              ai[q * n + r] = s * xpi + c * bqi;
-            }
-          }
-          {
-            const double xpr = wr[p * n + r], xqr = wr[q * n + r];
-            const double xpi = CPLX ? wi[p * n + r] : 0.0, xqi = CPLX ? wi[q * n + r] : 0.0;
-            const double bqr = xqr * ph_r - xqi * ph_i, bqi = xqr * ph_i + xqi * ph_r;
-            wr[p * n + r] = c * xpr - s * bqr;
-            wr[q * n + r] = s * xpr + c * bqr;
-            if constexpr (CPLX) {
-              wi[p * n + r] = c * xpi - s * bqi;
-              wi[q * n + r] = s * xpi + c * bqi;
+              const double bqr = xq[i] * ph_r - yq[i] * ph_i, bqi = xq[i] * ph_i + yq[i] * ph_r;
+              ar[p * n + r] = c * xp[i] - s * bqr;
+              ar[q * n + r] = s * xp[i] + c * bqr;
+              ai[p * n + r] = c * yp[i] - s * bqi;
+              ai[q * n + r] = s * yp[i] + c * bqi;
+              const double vpr = wr[p * n + r], vqr = wr[q * n + r], vpi = wi[p * n + r], vqi = wi[q * n + r];
+              const double dqr = vqr * ph_r - vqi * ph_i, dqi = vqr * ph_i + vqi * ph_r;
+              wr[p * n + r] = c * vpr - s * dqr;
+              wr[q * n + r] = s * vpr + c * dqr;
+              wi[p * n + r] = c * vpi - s * dqi;
+              wi[q * n + r] = s * vpi + c * dqi;
+            } else {
+              const double bq = xq[i] * ph_r, dq = vq[i] * ph_r;
+              ar[p * n + r] = c * xp[i] - s * bq;
+              ar[q * n + r] = s * xp[i] + c * bq;
+              wr[p * n + r] = c * vp[i] - s * dq;
+              wr[q * n + r] = s * vp[i] + c * dq;
             }
           }
         }
@@ -1347,7 +1368,11 @@ __global__ void __launch_bounds__(1024) jacobi_svd_kernel(const T* __restrict__ 
     const int any = rotated;
     __syncthreads();
 #ifdef TG_JACOBI_TRACE  // sweep log for tuning builds (off in the library)
-    if (threadIdx.x == 0) printf("jacobi_svd n=%d sweep=%d rotations=%d\n", n, sweep, trace_rot);
+    if (threadIdx.x == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %globaltimer;" : "=l"(now));
+      printf("jacobi_svd n=%d sweep=%d rotations=%d t=%.1f us\n", n, sweep, trace_rot, (now - trace_t0) * 1e-3);
+    }
     __syncthreads();
     if (threadIdx.x == 0) trace_rot = 0;
 #endif
@@ -2167,17 +2192,22 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
   constexpr bool CPLX = is_cplx<T>::value;
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "jacobi_svd: k out of range");
   const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k) + sizeof(int) * k;
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(jacobi_svd_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    attr_bytes = smem;
-  }
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
-  // 16 lanes per column pair, at most 1024 threads
   const int npairs = static_cast<int>((k + 1) / 2);
-  const int threads = static_cast<int>(std::min<int64_t>(1024, (npairs * 16 + 31) / 32 * 32));
-  jacobi_svd_kernel<T, CPLX><<<1, threads, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
+  // up to 96 columns: 16 lanes a pair, 6 rows a lane; up to 160: 32 lanes, 5 rows
+  auto run = [&](auto kernel, int lanes) {
+    static size_t attr_bytes = 0;
+    if (smem > attr_bytes) {
+      TG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      attr_bytes = smem;
+    }
+    const int threads = static_cast<int>(std::min<int64_t>(1024, (static_cast<int64_t>(npairs) * lanes + 31) / 32 * 32));
+    kernel<<<1, threads, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
+  };
+  if (k <= 96)
+    run(jacobi_svd_kernel<T, CPLX, 16, 6>, 16);
+  else
+    run(jacobi_svd_kernel<T, CPLX, 32, 5>, 32);
   TG_CHECK_LAUNCH();
   count_launch();
 }
