@@ -1873,6 +1873,9 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return;
   if (d.K <= 0) fail(TG_E_INPUT, "gemm: K must be positive");
   constexpr bool CPLX = is_cplx<T>::value;
+  if constexpr (!CPLX) {
+    if (gemm_skinny(A, B, C, d, st)) return;
+  }
   constexpr int NP = CPLX ? 2 : 1;
   const size_t smem = sizeof(double) * 2 * 2 * NP * GBK * GLD;
   static bool attr_set = false;
