@@ -225,13 +225,16 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
     t0 = time.perf_counter()
     e_prev, n, ref_conv, conv = None, 0, None, False
     e = float("nan")
+    per_sweep = []
     while n < max_sweeps:
+        ts = time.perf_counter()
         env.sweep()
         n += 1
         c, _ = env.check_convergence()
         if c and ref_conv is None:
             ref_conv = n
         e = bond_energy(env)
+        per_sweep.append(round(time.perf_counter() - ts, 4))
         if e_prev is not None and abs(e - e_prev) <= tol:
             conv = True
             break
@@ -240,7 +243,7 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
     env.close()
     return {"sweeps": n, "seconds": secs, "converged": conv, "energy_per_site": e,
             "last_delta_e": (abs(e - e_prev) if e_prev is not None else None),
-            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv}
+            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv, "seconds_per_sweep": per_sweep}
 
 
 def run_ours(args, rank, world, local_rank):
