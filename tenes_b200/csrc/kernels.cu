@@ -828,6 +828,90 @@ struct PermParams32 {
   bool conj;
 };
 
+// Permutations that keep the innermost axis: one thread copies a whole run
+// of `run` contiguous elements (16-byte copies when aligned), the run's
+// source offset decoded with multiplicative inverses instead of divisions
+// (Granlund & Montgomery, PLDI 1994: q = (t + ((n - t) >> 1)) >> (l - 1),
+// t = umulhi(m, n), l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1).
+struct PermRunParams {
+  int nouter;  // output axes outside the run, outermost first
+  uint32_t run, nruns;
+  uint32_t nchunks, cmagic, cshift;  // chunks of kRunChunk elements per run, and their inverse
+  uint32_t dims[kMaxRank], magic[kMaxRank], shift[kMaxRank], src_stride[kMaxRank];
+  bool conj, vec;
+};
+constexpr uint32_t kRunChunk = 8;  // elements one thread copies
+
+__device__ __forceinline__ uint32_t div_magic(uint32_t n, uint32_t m, uint32_t l) {
+  if (l == 0) return n;  // d == 1
+  const uint32_t t = __umulhi(m, n);
+  return (t + ((n - t) >> 1)) >> (l - 1);
+}
+
+// Permutations whose new innermost axis a sits directly before the old one
+// b (extent nb < 16) in the input: every (na x nb) block is contiguous in
+// the input and becomes nb runs of na contiguous elements in the output.
+// Consecutive threads take consecutive elements of a block (coalesced
+// reads; the writes fill whole runs); the other axes index the blocks.
+struct PermBlockParams {
+  int nbatch;
+  uint32_t na, nb, blk, out_b, nblocks;
+  uint32_t blk_magic, blk_shift, nb_magic, nb_shift;
+  uint32_t bdims[kMaxRank], bmagic[kMaxRank], bshift[kMaxRank], bin[kMaxRank], bout[kMaxRank];
+  bool conj;
+};
+
+template <typename T>
+__global__ void permute_blocks_kernel(const T* __restrict__ in, T* __restrict__ out, PermBlockParams p) {
+  const uint64_t items = static_cast<uint64_t>(p.nblocks) * p.blk;
+  for (uint64_t it = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; it < items;
+       it += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t u = div_magic(static_cast<uint32_t>(it), p.blk_magic, p.blk_shift);
+    const uint32_t j = static_cast<uint32_t>(it) - u * p.blk;
+    uint32_t rem = u, ibase = 0, obase = 0;
+    for (int i = p.nbatch - 1; i >= 0; --i) {
+      const uint32_t q = div_magic(rem, p.bmagic[i], p.bshift[i]);
+      const uint32_t idx = rem - q * p.bdims[i];
+      ibase += idx * p.bin[i];
+      obase += idx * p.bout[i];
+      rem = q;
+    }
+    const uint32_t ia = div_magic(j, p.nb_magic, p.nb_shift), ib = j - ia * p.nb;
+    const T v = in[ibase + j];
+    out[obase + ib * p.out_b + ia] = p.conj ? conj_of(v) : v;
+  }
+}
+
+template <typename T>
+__global__ void permute_runs_kernel(const T* __restrict__ in, T* __restrict__ out, PermRunParams p) {
+  const uint64_t items = static_cast<uint64_t>(p.nruns) * p.nchunks;
+  for (uint64_t it = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; it < items;
+       it += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    // item = (run u, chunk c): consecutive threads take consecutive chunks of a run
+    const uint32_t u = div_magic(static_cast<uint32_t>(it), p.cmagic, p.cshift);
+    const uint32_t c0 = (static_cast<uint32_t>(it) - u * p.nchunks) * kRunChunk;
+    const uint32_t len = min(kRunChunk, p.run - c0);
+    uint32_t rem = u, off = c0;
+    for (int i = p.nouter - 1; i > 0; --i) {
+      const uint32_t q = div_magic(rem, p.magic[i], p.shift[i]);
+      off += (rem - q * p.dims[i]) * p.src_stride[i];
+      rem = q;
+    }
+    off += rem * p.src_stride[0];
+    const T* src = in + off;
+    T* dst = out + static_cast<size_t>(u) * p.run + c0;
+    if constexpr (!is_cplx<T>::value) {
+      if (p.vec) {  // pairs of doubles (the run and the chunk are even)
+        const double2* s2 = reinterpret_cast<const double2*>(src);
+        double2* d2 = reinterpret_cast<double2*>(dst);
+        for (uint32_t j = 0; j < len / 2; ++j) d2[j] = s2[j];
+        continue;
+      }
+    }
+    for (uint32_t j = 0; j < len; ++j) dst[j] = p.conj ? conj_of(src[j]) : src[j];
+  }
+}
+
 template <typename T>
 __global__ void permute32_kernel(const T* __restrict__ in, T* __restrict__ out, PermParams32 p) {
   for (uint32_t lin = blockIdx.x * blockDim.x + threadIdx.x; lin < p.total; lin += gridDim.x * blockDim.x) {
@@ -2050,6 +2134,77 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
     count_launch();
     return;
   }
+  auto magic_of = [](uint32_t d, uint32_t* mg, uint32_t* sh) {
+    if (d <= 1) {
+      *mg = 0;
+      *sh = 0;
+      return;
+    }
+    uint32_t l = 0;
+    while ((uint64_t{1} << l) < d) ++l;  // ceil(log2 d)
+    *mg = static_cast<uint32_t>((((uint64_t{1} << 32) * ((uint64_t{1} << l) - d)) / d) + 1);
+    *sh = l;
+  };
+  if (m >= 2 && mp[m - 1] == m - 2 && ms[m - 1] < 16 && ms[m - 2] * ms[m - 1] <= 4096) {
+    // the new innermost axis directly before the old one: contiguous blocks
+    const int a = m - 2, b = m - 1;
+    PermBlockParams p{};
+    p.na = static_cast<uint32_t>(ms[a]);
+    p.nb = static_cast<uint32_t>(ms[b]);
+    p.blk = p.na * p.nb;
+    p.out_b = static_cast<uint32_t>(ostr[pos[b]]);
+    p.nblocks = static_cast<uint32_t>(total / p.blk);
+    p.conj = conj;
+    magic_of(p.blk, &p.blk_magic, &p.blk_shift);
+    magic_of(p.nb, &p.nb_magic, &p.nb_shift);
+    int nbd = 0;
+    for (int d = 0; d < m; ++d) {
+      if (d == a || d == b) continue;
+      p.bdims[nbd] = static_cast<uint32_t>(ms[d]);
+      p.bin[nbd] = static_cast<uint32_t>(istr[d]);
+      p.bout[nbd] = static_cast<uint32_t>(ostr[pos[d]]);
+      magic_of(p.bdims[nbd], &p.bmagic[nbd], &p.bshift[nbd]);
+      ++nbd;
+    }
+    p.nbatch = nbd;
+    permute_blocks_kernel<T><<<num_blocks(total, 256, 148 * 16), 256, 0, st>>>(in, out, p);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    return;
+  }
+  if (m >= 2 && mp[m - 1] == m - 1) {  // the innermost axis stays innermost: copy runs
+    PermRunParams p{};
+    p.nouter = m - 1;
+    p.run = static_cast<uint32_t>(ms[m - 1]);
+    p.nruns = static_cast<uint32_t>(total / ms[m - 1]);
+    p.nchunks = (p.run + kRunChunk - 1) / kRunChunk;
+    magic_of(p.nchunks, &p.cmagic, &p.cshift);
+    p.conj = conj;
+    for (int i = 0; i < m - 1; ++i) {
+      p.dims[i] = static_cast<uint32_t>(od[i]);
+      p.src_stride[i] = static_cast<uint32_t>(istr[mp[i]]);
+      magic_of(p.dims[i], &p.magic[i], &p.shift[i]);
+    }
+    // the outer strides are multiples of the run, so an even run keeps every run 16-byte aligned
+    p.vec = !conj && (p.run % 2 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) &&
+            (reinterpret_cast<uintptr_t>(out) % 16 == 0);
+#ifdef TG_PERM_TRACE  // shape log for tuning builds (off in the library)
+    fprintf(stderr, "permute runs: run=%u nruns=%u m=%d\n", p.run, p.nruns, m);
+#endif
+    permute_runs_kernel<T><<<num_blocks(static_cast<int64_t>(p.nruns) * p.nchunks, 256, 148 * 16), 256, 0, st>>>(
+        in, out, p);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    return;
+  }
+#ifdef TG_PERM_TRACE
+  {
+    std::string sh_s, pm_s;
+    for (int i = 0; i < m; ++i) sh_s += std::to_string(ms[i]) + " ";
+    for (int i = 0; i < m; ++i) pm_s += std::to_string(mp[i]) + " ";
+    fprintf(stderr, "permute generic: merged shape [%s] perm [%s]\n", sh_s.c_str(), pm_s.c_str());
+  }
+#endif
   PermParams32 p{};
   p.rank = std::max(m, 1);
   p.conj = conj;
