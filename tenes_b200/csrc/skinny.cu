@@ -64,11 +64,13 @@ __host__ __device__ inline int sk_ld(int x) { return x + ((20 - (x & 15)) & 15);
 // contiguous along K; either way the A-fragment loads are conflict-free.
 constexpr int SK_LDR = SK_R + 4;
 
-template <int STAGES>
+// NB = ceil(n / 8) column blocks, a template parameter so that the MMA
+// loops carry no predicated-off work
+template <int STAGES, int NB>
 __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyParams p) {
   extern __shared__ __align__(16) double sk_smem[];
   const int K = p.K, n = p.n;
-  const int K4 = (K + 3) & ~3, n8 = (n + 7) & ~7, nb = n8 >> 3;
+  const int K4 = (K + 3) & ~3, n8 = NB * 8;
   const bool kmajor = p.sk != 1;  // Big contiguous along its rows
   const int ldb = sk_ld(K4), lds = sk_ld(n8);
   const int stage_len = kmajor ? K4 * SK_LDR : SK_R * ldb;
@@ -162,29 +164,29 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyParams p) {
     SKT(1)
     const double* bst = Bt + stage * stage_len;
     stage = stage + 1 == STAGES ? 0 : stage + 1;
-    double acc[SK_NB][2];
+    double acc[NB][2];
 #pragma unroll
-    for (int c = 0; c < SK_NB; ++c) acc[c][0] = acc[c][1] = 0.0;
+    for (int c = 0; c < NB; ++c) acc[c][0] = acc[c][1] = 0.0;
     const double* ap = kmajor ? bst + t * SK_LDR + 8 * warp + g : bst + (8 * warp + g) * ldb + t;
     const double* sp = S + t * lds + g;
     // the fragments of the next k step are loaded before this step's MMAs
-    double a0 = *ap, b0[SK_NB];
+    double a0 = *ap, b0[NB];
 #pragma unroll
-    for (int c = 0; c < SK_NB; ++c) b0[c] = c < nb ? sp[8 * c] : 0.0;
+    for (int c = 0; c < NB; ++c) b0[c] = sp[8 * c];
+#pragma unroll 2
     for (int k4 = 0; k4 < K4; k4 += 4) {
       const bool more = k4 + 4 < K4;
       ap += astep;
       sp += 4 * lds;
       const double a1 = more ? *ap : 0.0;
-      double b1[SK_NB];
+      double b1[NB];
 #pragma unroll
-      for (int c = 0; c < SK_NB; ++c) b1[c] = (more && c < nb) ? sp[8 * c] : 0.0;
+      for (int c = 0; c < NB; ++c) b1[c] = more ? sp[8 * c] : 0.0;
 #pragma unroll
-      for (int c = 0; c < SK_NB; ++c)
-        if (c < nb) sk_dmma(acc[c][0], acc[c][1], a0, b0[c]);
+      for (int c = 0; c < NB; ++c) sk_dmma(acc[c][0], acc[c][1], a0, b0[c]);
       a0 = a1;
 #pragma unroll
-      for (int c = 0; c < SK_NB; ++c) b0[c] = b1[c];
+      for (int c = 0; c < NB; ++c) b0[c] = b1[c];
     }
     SKT(2)
     __syncthreads();  // every warp done with this stage before it is refilled
@@ -196,15 +198,13 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyParams p) {
     if (r < p.rows) {
       double* crow = p.C + r * p.scr;
 #pragma unroll
-      for (int c = 0; c < SK_NB; ++c) {
-        if (c < nb) {
+      for (int c = 0; c < NB; ++c) {
 #pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int j = 8 * c + 2 * t + e;
-            if (j < n) {
-              double* dst = crow + j * p.scn;
-              *dst = p.accumulate ? *dst + acc[c][e] : acc[c][e];
-            }
+        for (int e = 0; e < 2; ++e) {
+          const int j = 8 * c + 2 * t + e;
+          if (j < n) {
+            double* dst = crow + j * p.scn;
+            *dst = p.accumulate ? *dst + acc[c][e] : acc[c][e];
           }
         }
       }
@@ -225,18 +225,36 @@ size_t skinny_smem(int K, int n, bool kmajor, int stages) {
   return sizeof(double) * (static_cast<size_t>(K4) * sk_ld(n8) + stages * stage);
 }
 
-template <int STAGES>
-void launch_skinny(const SkinnyParams& p, size_t smem, cudaStream_t st) {
+template <int STAGES, int NB>
+void launch_skinny_nb(const SkinnyParams& p, size_t smem, cudaStream_t st) {
   static size_t attr_bytes = 0;
   if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(skinny_kernel<STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TG_CUDA(cudaFuncSetAttribute(skinny_kernel<STAGES, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
     attr_bytes = smem;
   }
   const int64_t ntiles = (p.rows + SK_R - 1) / SK_R;
   const int per_sm = smem <= SK_SMEM_2CTA ? 2 : 1;
   const unsigned grid = static_cast<unsigned>(std::min<int64_t>(ntiles, 148 * per_sm));
-  skinny_kernel<STAGES><<<grid, SK_THREADS, smem, st>>>(p);
+  skinny_kernel<STAGES, NB><<<grid, SK_THREADS, smem, st>>>(p);
+}
+
+template <int STAGES>
+void launch_skinny(const SkinnyParams& p, size_t smem, cudaStream_t st) {
+  switch ((p.n + 7) / 8) {
+    case 1: launch_skinny_nb<STAGES, 1>(p, smem, st); break;
+    case 2: launch_skinny_nb<STAGES, 2>(p, smem, st); break;
+    case 3: launch_skinny_nb<STAGES, 3>(p, smem, st); break;
+    case 4: launch_skinny_nb<STAGES, 4>(p, smem, st); break;
+    case 5: launch_skinny_nb<STAGES, 5>(p, smem, st); break;
+    case 6: launch_skinny_nb<STAGES, 6>(p, smem, st); break;
+    case 7: launch_skinny_nb<STAGES, 7>(p, smem, st); break;
+    case 8: launch_skinny_nb<STAGES, 8>(p, smem, st); break;
+    case 9: launch_skinny_nb<STAGES, 9>(p, smem, st); break;
+    case 10: launch_skinny_nb<STAGES, 10>(p, smem, st); break;
+    case 11: launch_skinny_nb<STAGES, 11>(p, smem, st); break;
+    default: launch_skinny_nb<STAGES, 12>(p, smem, st); break;
+  }
 }
 
 }  // namespace
