@@ -170,12 +170,14 @@ def fp64_peak_tflops(device):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def traffic_from_profile(cfg):
-    """DRAM bytes per DMMA-GEMM launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"gemm_dmma_{cfg}.md")
+def traffic_from_profile(cfg, family):
+    """DRAM bytes per launch of the product family's dominant shape from the
+    committed ncu summary (profiles/roofline_traffic_<cfg>.md, a line
+    `<family>: traffic_bytes_per_launch = X`), if any."""
+    path = os.path.join(ROOT, "profiles", f"roofline_traffic_{cfg}.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"traffic_bytes_per_launch\s*=\s*([0-9.eE+]+)", open(path).read())
+    m = re.search(family + r":\s*traffic_bytes_per_launch\s*=\s*([0-9.eE+]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -362,7 +364,11 @@ def run_ours(args, rank, world, local_rank):
                 "achieved": fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0, "peak": peak,
                 "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (MEASURED_PEAKS.json has no FP64 entry)"}
     roof.update({"unit": "TFLOP/s", "frac": (roof["achieved"] / roof["peak"]) if roof["peak"] else None,
-                 "traffic": traffic_from_profile(args.config), "launches_per_sweep": n_g,
+                 "traffic": traffic_from_profile(args.config, "gemm_tcgen05" if "tcgen05" in roof["kernel"]
+                                                 else "gemm_dmma"),
+                 "traffic_note": "DRAM bytes of one launch of the family's dominant shape (the rSVD range-finder "
+                                 "product 2592 x 82 x 2592), from profiles/roofline_traffic_<config>.md",
+                 "launches_per_sweep": n_g,
                  "avg_launch_us": 1e3 * ms_g / max(n_g, 1), "flops_per_launch": fl_g / max(n_g, 1),
                  "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}})
 
