@@ -62,6 +62,12 @@ struct EngineT final : Engine {
   cudaStream_t main_st = nullptr;
   cudaStream_t row_st[kRowStreams] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kRowStreams] = {};
+  // Row staggering: row r's rSVD waits for row r-1's first range-finder
+  // product, so that the rows' latency-bound orthonormalisations fall on
+  // each other's tensor-core products instead of coinciding.
+  cudaEvent_t ev_stagger[kRowStreams] = {};
+  bool stagger_rec[kRowStreams] = {};
+  int cur_row = -1;
   int slot = 0;  // 0: main stream, 1..kRowStreams: row streams
 
   unsigned long long* d_max = nullptr;  // one per stream slot
@@ -101,6 +107,7 @@ struct EngineT final : Engine {
     for (int r = 0; r < kRowStreams; ++r) {
       TG_CUDA(cudaStreamCreateWithFlags(&row_st[r], cudaStreamNonBlocking));
       TG_CUDA(cudaEventCreateWithFlags(&ev_join[r], cudaEventDisableTiming));
+      TG_CUDA(cudaEventCreateWithFlags(&ev_stagger[r], cudaEventDisableTiming));
     }
     TG_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long) * (kRowStreams + 1)));
@@ -159,6 +166,7 @@ struct EngineT final : Engine {
     for (int r = 0; r < kRowStreams; ++r) {
       if (row_st[r]) cudaStreamDestroy(row_st[r]);
       if (ev_join[r]) cudaEventDestroy(ev_join[r]);
+      if (ev_stagger[r]) cudaEventDestroy(ev_stagger[r]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (st) cudaStreamDestroy(st);
@@ -203,9 +211,12 @@ struct EngineT final : Engine {
     for (int s = 0; s < ns; ++s) TG_CUDA(cudaStreamWaitEvent(row_st[s], ev_fork, 0));
     cudaStream_t saved = st;
     const int saved_slot = slot;
+    const bool stagger = n <= kRowStreams;  // one stream per row
+    for (int r = 0; r < kRowStreams; ++r) stagger_rec[r] = false;
     auto join = [&]() {
       st = saved;
       slot = saved_slot;
+      cur_row = -1;
       for (int s = 0; s < ns; ++s) {
         cudaEventRecord(ev_join[s], row_st[s]);
         cudaStreamWaitEvent(st, ev_join[s], 0);
@@ -215,6 +226,7 @@ struct EngineT final : Engine {
       for (int r = 0; r < n; ++r) {
         st = row_st[r % ns];
         slot = 1 + r % ns;
+        cur_row = stagger ? r : -1;
         body(r);
       }
     } catch (...) {
@@ -223,6 +235,16 @@ struct EngineT final : Engine {
     }
     join();
     TG_CUDA(cudaGetLastError());
+  }
+  // row staggering (see ev_stagger): wait for the previous row's mark / set this row's
+  void stagger_wait() {
+    if (cur_row > 0 && stagger_rec[cur_row - 1]) TG_CUDA(cudaStreamWaitEvent(st, ev_stagger[cur_row - 1], 0));
+  }
+  void stagger_mark() {
+    if (cur_row >= 0 && !stagger_rec[cur_row]) {
+      TG_CUDA(cudaEventRecord(ev_stagger[cur_row], st));
+      stagger_rec[cur_row] = true;
+    }
   }
   // release `v`'s storage in stream order on `st` (after a join)
   void keep(std::vector<DT<T>>& v) {
@@ -624,7 +646,9 @@ struct EngineT final : Engine {
     };
     DT<T> Om({k, ncol}, st);
     counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
+    stagger_wait();
     DT<T> Q = apply_M(Om);
+    stagger_mark();
     orth_chol(Q, nrow, k, P.rsvd_power_iters > 0 ? 2 : 4);
     for (int it = 0; it < P.rsvd_power_iters; ++it) {
       DT<T> Z = apply_MH(Q);
