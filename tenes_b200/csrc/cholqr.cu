@@ -81,14 +81,19 @@ __device__ __forceinline__ unsigned long long cq_now() {
 // redundantly in registers -- each lane holds the whole upper triangle, so a
 // pivot step is rsqrt -> scale -> update with no communication -- and applies
 // the same steps to its own block-row column.  The trailing triangle is then
-// updated on DMMA, one 8 x 8 block per warp task.  dinv[i] = 1/R'_ii.  At the
+// updated on DMMA, two 8 x 8 blocks per warp task.  dinv[i] = 1/R'_ii.  At the
 // end the diagonal blocks are replaced by their inverses (lower parts zero).
 // btab lists the upper 8 x 8 blocks row by row, so the trailing blocks of
 // block J are its suffix starting at (J+1) nb - J (J+1) / 2.
-__device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, double* dinv, const int* btab, int* flag) {
+__device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, double* dinv, const int* btab, int* flag,
+                                                 unsigned long long* tr = nullptr) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int nb = kp / 8, nblk = nb * (nb + 1) / 2;
   const int g = lane >> 2, t = lane & 3;
+#ifdef TG_CQ_TRACE
+  unsigned long long t0 = 0, t1 = 0;
+  if (tr) t0 = clock64();
+#endif
   for (int J = 0; J < nb; ++J) {
     const int j0 = 8 * J, ncol = kp - j0 - 8;
     double a[8][8];
@@ -128,6 +133,13 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
       }
     }
     __syncthreads();  // every warp has loaded the diagonal block
+#ifdef TG_CQ_TRACE
+    if (tr) {
+      t1 = clock64();
+      tr[0] += t1 - t0;
+      t0 = t1;
+    }
+#endif
     if (warp == 0 && lane < 8) {  // lane c writes column c of R'_JJ (no trailing block touches it)
 #pragma unroll
       for (int c = 0; c < 8; ++c)
@@ -158,6 +170,13 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
       }
     }
     __syncthreads();
+#ifdef TG_CQ_TRACE
+    if (tr) {
+      t1 = clock64();
+      tr[1] += t1 - t0;
+      t0 = t1;
+    }
+#endif
   }
   // diagonal blocks -> their inverses: warp J, lane c solves R'_JJ x = e_c
   for (int J = warp; J < nb; J += nw) {
@@ -178,6 +197,12 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
     }
   }
   __syncthreads();
+#ifdef TG_CQ_TRACE
+  if (tr) {
+    t1 = clock64();
+    tr[2] += t1 - t0;
+  }
+#endif
 }
 
 __global__ void __launch_bounds__(CQ_THREADS, 1)
@@ -197,7 +222,7 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #ifdef TG_CQ_TRACE
   unsigned call = 0;
-  unsigned long long tt[4][8] = {};
+  unsigned long long tt[4][12] = {};
   if (rank == 0 && tid == 0) call = atomicAdd(&g_cq_calls, 1u);
   const bool trace = rank == 0 && tid == 0 && passes == 4 && ((call % 24) == 10 || (call % 24) == 11);
 #define CQ_T(p, i) \
@@ -325,7 +350,17 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
 #ifdef TG_CQ_TRACE
       if (trace && pass < 4) tt[pass][7] = cq_now();
 #endif
+#ifdef TG_CQ_TRACE
+      unsigned long long chtr[3] = {0, 0, 0};
+      cholesky_blocked(Rs, kp, ld, dinv, btab, flag, trace ? chtr : nullptr);
+      if (trace && pass < 4) {
+        tt[pass][8] = chtr[0];
+        tt[pass][9] = chtr[1];
+        tt[pass][10] = chtr[2];
+      }
+#else
       cholesky_blocked(Rs, kp, ld, dinv, btab, flag);
+#endif
       // R' and D to the global scratch, read from L2 by the other CTAs (a
       // broadcast from one SM's shared memory would serialise on that SM)
       for (int e = tid; e < total; e += CQ_THREADS) {
@@ -428,10 +463,10 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
 #ifdef TG_CQ_TRACE
   if (trace) {
     for (int p = 0; p < 4; ++p)
-      printf("cq n=%d k=%d pass %d: gram %.1f  sync %.1f  reduce %.1f  chol %.1f (prep %.1f)  copy %.1f  trsm %.1f us\n",
+      printf("cq n=%d k=%d pass %d: gram %.1f  sync %.1f  reduce %.1f  chol %.1f (prep %.1f, diag+row %.1f, trailing %.1f, inverses %.1f kcycles)  copy %.1f  trsm %.1f us\n",
              n, k, p, (tt[p][1] - tt[p][0]) * 1e-3, (tt[p][2] - tt[p][1]) * 1e-3, (tt[p][3] - tt[p][2]) * 1e-3,
-             (tt[p][4] - tt[p][3]) * 1e-3, (tt[p][7] - tt[p][3]) * 1e-3, (tt[p][5] - tt[p][4]) * 1e-3,
-             (tt[p][6] - tt[p][5]) * 1e-3);
+             (tt[p][4] - tt[p][3]) * 1e-3, (tt[p][7] - tt[p][3]) * 1e-3, tt[p][8] * 1e-3, tt[p][9] * 1e-3,
+             tt[p][10] * 1e-3, (tt[p][5] - tt[p][4]) * 1e-3, (tt[p][6] - tt[p][5]) * 1e-3);
   }
 #endif
 #undef CQ_T
