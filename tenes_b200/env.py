@@ -114,10 +114,18 @@ class Environment:
             raise ValueError(f"site {i}: shape {a.shape} != {self.site_shape(i)}")
         check(self.lib.tg_set_site_tensor(self.ctx, i, dptr(a.view(np.float64))))
 
-    def get_site_tensor(self, i: int) -> np.ndarray:
-        a = np.empty(self.site_shape(i), dtype=self.dtype)
+    def get_site_tensor(self, i: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Site tensor i; into `out` (C-contiguous, of the tensor's shape and dtype) when given."""
+        a = self._out(out, self.site_shape(i))
         check(self.lib.tg_get_site_tensor(self.ctx, i, dptr(a.view(np.float64))))
         return a
+
+    def _out(self, out: Optional[np.ndarray], shape) -> np.ndarray:
+        if out is None:
+            return np.empty(shape, dtype=self.dtype)
+        if out.shape != tuple(shape) or out.dtype != self.dtype or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out: needs a C-contiguous {self.dtype} array of shape {tuple(shape)}")
+        return out
 
     def set_lambda(self, i: int, leg: int, lam: np.ndarray) -> None:
         a = np.ascontiguousarray(lam, dtype=np.float64)
@@ -136,8 +144,9 @@ class Environment:
             raise ValueError(f"{ENV_NAMES[which]}[{i}]: shape {a.shape} != {self.env_shape(which, i)}")
         check(self.lib.tg_set_env(self.ctx, which, i, dptr(a.view(np.float64))))
 
-    def get_env(self, which: int, i: int) -> np.ndarray:
-        a = np.empty(self.env_shape(which, i), dtype=self.dtype)
+    def get_env(self, which: int, i: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Environment tensor `which` (ENV_NAMES) of site i; into `out` when given."""
+        a = self._out(out, self.env_shape(which, i))
         check(self.lib.tg_get_env(self.ctx, which, i, dptr(a.view(np.float64))))
         return a
 
