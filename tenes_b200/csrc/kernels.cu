@@ -729,6 +729,12 @@ __global__ void __launch_bounds__(tma::THREADS) gemm_tma_kernel(const __grid_con
     double* out = g.nchunks > 1 ? g.C + static_cast<int64_t>(chunk) * g.M * g.N : g.C;
     const int64_t sm_ = g.nchunks > 1 ? g.N : g.sCm, sn_ = g.nchunks > 1 ? 1 : g.sCn;
     const bool acc = g.nchunks == 1 && g.accumulate;
+    // C contiguous along n: each 32 x 16 block goes through a per-warp
+    // staging tile in the (now idle) ring so that a warp's stores cover two
+    // rows of 16 consecutive columns; contiguous along m (or neither), each
+    // lane stores its own row, which is then the coalesced direction
+    const bool by_rows = sn_ == 1 && sm_ != 1;
+    double* stg = reinterpret_cast<double*>(tma_smem + (ring - raw)) + warp * 32 * 17;
 #pragma unroll
     for (int c0 = 0; c0 < BN; c0 += 16) {
       uint32_t v[16];
@@ -739,7 +745,24 @@ __global__ void __launch_bounds__(tma::THREADS) gemm_tma_kernel(const __grid_con
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (m < g.M) {
+      if (by_rows) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = static_cast<double>(__uint_as_float(v[j]));
+        __syncwarp();
+        const int col = lane & 15;
+        const int64_t n = n0 + c0 + col;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int r = 2 * i + (lane >> 4);
+          const int64_t mr = m0 + warp * 32 + r;
+          if (mr < g.M && n < g.N) {
+            double* c = out + mr * sm_ + n;
+            const double x = stg[r * 17 + col];
+            *c = acc ? *c + x : x;
+          }
+        }
+        __syncwarp();
+      } else if (m < g.M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int64_t n = n0 + c0 + j;
