@@ -874,23 +874,25 @@ __device__ __forceinline__ uint32_t div_magic(uint32_t n, uint32_t m, uint32_t l
 // Permutations whose new innermost axis a sits directly before the old one
 // b (extent nb < 16) in the input: every (na x nb) block is contiguous in
 // the input and becomes nb runs of na contiguous elements in the output.
-// Consecutive threads take consecutive elements of a block (coalesced
-// reads; the writes fill whole runs); the other axes index the blocks.
+// Consecutive threads take consecutive groups of kBlkVec elements of a
+// block (coalesced reads, several loads in flight per thread; the writes
+// fill whole runs); the other axes index the blocks.
+constexpr uint32_t kBlkVec = 4;  // consecutive block elements one thread moves (loads issued together)
 struct PermBlockParams {
   int nbatch;
   uint32_t na, nb, blk, out_b, nblocks;
-  uint32_t blk_magic, blk_shift, nb_magic, nb_shift;
+  uint32_t nq, q_magic, q_shift, nb_magic, nb_shift;  // nq = ceil(blk / kBlkVec) groups per block
   uint32_t bdims[kMaxRank], bmagic[kMaxRank], bshift[kMaxRank], bin[kMaxRank], bout[kMaxRank];
   bool conj;
 };
 
 template <typename T>
 __global__ void permute_blocks_kernel(const T* __restrict__ in, T* __restrict__ out, PermBlockParams p) {
-  const uint64_t items = static_cast<uint64_t>(p.nblocks) * p.blk;
+  const uint64_t items = static_cast<uint64_t>(p.nblocks) * p.nq;
   for (uint64_t it = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; it < items;
        it += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint32_t u = div_magic(static_cast<uint32_t>(it), p.blk_magic, p.blk_shift);
-    const uint32_t j = static_cast<uint32_t>(it) - u * p.blk;
+    const uint32_t u = div_magic(static_cast<uint32_t>(it), p.q_magic, p.q_shift);
+    const uint32_t j0 = (static_cast<uint32_t>(it) - u * p.nq) * kBlkVec;
     uint32_t rem = u, ibase = 0, obase = 0;
     for (int i = p.nbatch - 1; i >= 0; --i) {
       const uint32_t q = div_magic(rem, p.bmagic[i], p.bshift[i]);
@@ -899,9 +901,17 @@ __global__ void permute_blocks_kernel(const T* __restrict__ in, T* __restrict__ 
       obase += idx * p.bout[i];
       rem = q;
     }
-    const uint32_t ia = div_magic(j, p.nb_magic, p.nb_shift), ib = j - ia * p.nb;
-    const T v = in[ibase + j];
-    out[obase + ib * p.out_b + ia] = p.conj ? conj_of(v) : v;
+    T v[kBlkVec];
+#pragma unroll
+    for (uint32_t e = 0; e < kBlkVec; ++e) v[e] = j0 + e < p.blk ? in[ibase + j0 + e] : zero_of<T>();
+#pragma unroll
+    for (uint32_t e = 0; e < kBlkVec; ++e) {
+      const uint32_t j = j0 + e;
+      if (j < p.blk) {
+        const uint32_t ia = div_magic(j, p.nb_magic, p.nb_shift), ib = j - ia * p.nb;
+        out[obase + ib * p.out_b + ia] = p.conj ? conj_of(v[e]) : v[e];
+      }
+    }
   }
 }
 
@@ -2178,7 +2188,8 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
     p.out_b = static_cast<uint32_t>(ostr[pos[b]]);
     p.nblocks = static_cast<uint32_t>(total / p.blk);
     p.conj = conj;
-    magic_of(p.blk, &p.blk_magic, &p.blk_shift);
+    p.nq = (p.blk + kBlkVec - 1) / kBlkVec;
+    magic_of(p.nq, &p.q_magic, &p.q_shift);
     magic_of(p.nb, &p.nb_magic, &p.nb_shift);
     int nbd = 0;
     for (int d = 0; d < m; ++d) {
@@ -2190,7 +2201,8 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
       ++nbd;
     }
     p.nbatch = nbd;
-    permute_blocks_kernel<T><<<num_blocks(total, 256, 148 * 16), 256, 0, st>>>(in, out, p);
+    permute_blocks_kernel<T><<<num_blocks(static_cast<int64_t>(p.nblocks) * p.nq, 256, 148 * 16), 256, 0, st>>>(
+        in, out, p);
     TG_CHECK_LAUNCH();
     count_launch();
     return;
