@@ -791,11 +791,20 @@ __global__ void splitk_reduce_kernel(const T* __restrict__ parts, int nparts, in
   const int64_t len = M * N;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < len;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    // partials summed in order p = 0, 1, ...; up to 16 of them are loaded
+    // together first so that their loads are in flight at once
     double re = 0.0, im = 0.0;
-    for (int p = 0; p < nparts; ++p) {
-      const T v = parts[p * len + i];
-      re += re_of(v);
-      im += im_of(v);
+    for (int p0 = 0; p0 < nparts; p0 += 16) {
+      T v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (p0 + q < nparts) v[q] = parts[(p0 + q) * len + i];
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (p0 + q < nparts) {
+          re += re_of(v[q]);
+          im += im_of(v[q]);
+        }
     }
     const int64_t m = i / N, n = i - m * N;
     T* c = C + m * sCm + n * sCn;

@@ -39,7 +39,7 @@ template <typename T>
 void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st);
 
 // FP64 product with one operand of at most 96 x 96 and the other at least
-// 4096 long (batch 1, a unit stride on the long operand and on C): the
+// 2048 long (batch 1, a unit stride on the long operand and on C): the
 // streaming kernel of skinny.cu.  Returns false, launching nothing, for any
 // other shape.  gemm() tries it first at both precisions (it is exact FP64).
 bool gemm_skinny(const double* A, const double* B, double* C, const GemmDesc& d, cudaStream_t st);

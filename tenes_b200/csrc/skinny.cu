@@ -264,7 +264,7 @@ bool gemm_skinny(const double* A, const double* B, double* C, const GemmDesc& d,
   SkinnyParams p{};
   p.K = static_cast<int>(d.K);
   p.accumulate = d.accumulate;
-  constexpr int64_t kLong = 4096;
+  constexpr int64_t kLong = 2048;
   if (d.N <= SK_NMAX && d.M >= kLong) {  // C = A B, A the long operand
     p.big = A;
     p.rows = d.M;

@@ -29,8 +29,9 @@ def _run(A, B, layout_a, layout_b, layout_c, prec, seed_c=None):
 
 SHAPES = [(128, 128, 16), (200, 37, 100), (36, 1000, 72), (1000, 36, 72), (2592, 82, 2592), (130, 257, 1030),
           (1, 1, 1), (17, 300, 5),
-          # one side <= 96 and the other >= 4096: the streaming kernel for long operands
-          (36, 5000, 72), (5000, 72, 36), (72, 4100, 35), (4099, 17, 96), (96, 4096, 1), (5, 6000, 3)]
+          # one side <= 96 and the other >= 2048: the streaming kernel for long operands
+          (36, 5000, 72), (5000, 72, 36), (72, 4100, 35), (4099, 17, 96), (96, 4096, 1), (5, 6000, 3),
+          (2592, 82, 82), (72, 2592, 72), (2048, 96, 96)]
 
 
 @pytest.mark.parametrize("M,N,K", SHAPES)
