@@ -601,10 +601,11 @@ struct EngineT final : Engine {
   //
   // passes = 4: two shifted and two plain passes, orthonormal to O(u): the
   // final range basis Q and the basis Qz of the Rayleigh-Ritz core.
-  // passes = 1: one shifted pass (and the perturbation), a basis of the same
-  // span whose columns are far from parallel -- enough for the intermediate
-  // bases of the power iteration, whose next product only uses the span and
-  // whose last basis is orthonormalised in full.
+  // passes = 2: the two shifted passes only, a basis of the same span with
+  // condition number ~1e4 -- enough for the intermediate bases of the power
+  // iteration, whose next product and orthonormalisation only use the span.
+  // (One shifted pass is not enough: with weakly converged site tensors the
+  // next panel's Gram matrix then met a non-positive pivot.)
   void orth_chol(DT<T>& Y, int64_t n, int64_t k, int passes = 4) {
     PrecScope fp64(this, 0);
     if constexpr (!CPLX) {
@@ -651,12 +652,12 @@ struct EngineT final : Engine {
     stagger_wait();
     DT<T> Q = apply_M(Om);
     stagger_mark();
-    orth_chol(Q, nrow, k, P.rsvd_power_iters > 0 ? 1 : 4);
+    orth_chol(Q, nrow, k, P.rsvd_power_iters > 0 ? 2 : 4);
     for (int it = 0; it < P.rsvd_power_iters; ++it) {
       DT<T> Z = apply_MH(Q);
-      orth_chol(Z, ncol, k, 1);
+      orth_chol(Z, ncol, k, 2);
       Q = apply_M(Z);
-      orth_chol(Q, nrow, k, it + 1 < P.rsvd_power_iters ? 1 : 4);
+      orth_chol(Q, nrow, k, it + 1 < P.rsvd_power_iters ? 2 : 4);
     }
     // B = Q^H M = Z^H with Z = M^H Q.  With Qz an orthonormal basis of
     // range(Z), B = (Z^H Qz) Qz^H, so the SVD of the k x k matrix T = Z^H Qz,

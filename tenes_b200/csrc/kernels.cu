@@ -1455,6 +1455,7 @@ __global__ void __launch_bounds__(kJG == 16 ? 768 : 1024) jacobi_svd_kernel(cons
         const double rd = rsqrt(den);
         const double t = copysign(2.0 * g, tau) * (rd * rd);
         const double c = rsqrt(fma(t, t, 1.0)), s = c * t;
+        const double sph = s * ph_r, cph = c * ph_r;
 #pragma unroll
         for (int i = 0; i < RPL; ++i) {
           const int r = gl + i * kJG;
@@ -1471,12 +1472,11 @@ __global__ void __launch_bounds__(kJG == 16 ? 768 : 1024) jacobi_svd_kernel(cons
               wr[q * n + r] = s * vpr + c * dqr;
               wi[p * n + r] = c * vpi - s * dqi;
               wi[q * n + r] = s * vpi + c * dqi;
-            } else {
-              const double bq = xq[i] * ph_r, dq = vq[i] * ph_r;
-              ar[p * n + r] = c * xp[i] - s * bq;
-              ar[q * n + r] = s * xp[i] + c * bq;
-              wr[p * n + r] = c * vp[i] - s * dq;
-              wr[q * n + r] = s * vp[i] + c * dq;
+            } else {  // ph_r = +-1 folded into the coefficients (exact)
+              ar[p * n + r] = c * xp[i] - sph * xq[i];
+              ar[q * n + r] = s * xp[i] + cph * xq[i];
+              wr[p * n + r] = c * vp[i] - sph * vq[i];
+              wr[q * n + r] = s * vp[i] + cph * vq[i];
             }
           }
         }
