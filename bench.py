@@ -482,6 +482,91 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# J1-J2 gradient workload: 2x2 cell, d = 2, D = 3, chi = 36, J2 = 0.5, site
+# tensors i.i.d. normal(0, 1), 25 CTMRG sweeps checkpointed every 5
+GRAD = dict(D=3, chi=36, iterations=25, checkpoint_every=5, J1=1.0, J2=0.5, fd_step=1e-5)
+
+
+def grad_problem(seed):
+    from tenes_b200.grad import j1j2_terms
+    rng = np.random.default_rng(seed)
+    D = GRAD["D"]
+    Tn = [rng.standard_normal((D, D, D, D, 2)) for _ in range(4)]
+    return Tn, j1j2_terms(4, GRAD["J1"], GRAD["J2"])
+
+
+def grad_env(Tn, mixed):
+    from tenes_b200.env import CTMParams, Environment
+    D = GRAD["D"]
+    env = Environment(2, 2, [2] * 4, [[D] * 4 for _ in range(4)],
+                      CTMParams(chi=GRAD["chi"], max_ctm_iteration=1, mixed=mixed), False)
+    for i, t in enumerate(Tn):
+        env.set_site_tensor(i, t)
+    return env
+
+
+def run_grad(args):
+    """Gradient evaluations/s of the J1-J2 energy (hand-written adjoint
+    through the sweeps and the projector SVDs), the central-difference check
+    on seeded entries, and the mixed-precision (3xTF32 moves) arm."""
+    from tenes_b200.env import kernel_launch_count
+    Tn, terms = grad_problem(SEED)
+    it, ck = args.grad_iters, GRAD["checkpoint_every"]
+
+    def timed(env, grad=True):
+        t0 = time.perf_counter()
+        out = env.energy_grad(terms, it, ck, grad=grad)
+        return out, time.perf_counter() - t0
+
+    env = grad_env(Tn, False)
+    (E, g), _ = timed(env)  # warm-up
+    l0 = kernel_launch_count()
+    times = []
+    for _ in range(args.steps):
+        (E, g), dt = timed(env)
+        times.append(dt)
+    launches = (kernel_launch_count() - l0) // max(args.steps, 1)
+    _, t_fwd = timed(env, grad=False)
+    gmax = max(float(np.abs(x).max()) for x in g)
+    rng = np.random.default_rng(SEED + 1)
+    errs, h = [], GRAD["fd_step"]
+    for _ in range(args.grad_fd):
+        site = int(rng.integers(4))
+        idx = tuple(int(rng.integers(n)) for n in Tn[site].shape)
+        vals = []
+        for sgn in (1, -1):
+            T = Tn[site].copy()
+            T[idx] += sgn * h
+            env.set_site_tensor(site, T)
+            vals.append(env.energy_grad(terms, it, ck, grad=False)[0])
+        env.set_site_tensor(site, Tn[site])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        errs.append(abs(fd - g[site][idx]) / max(abs(fd), abs(g[site][idx]), 1e-3 * gmax))
+    env.close()
+    envm = grad_env(Tn, True)
+    (Em, gm), _ = timed(envm)
+    tm = []
+    for _ in range(args.steps):
+        (Em, gm), dt = timed(envm)
+        tm.append(dt)
+    envm.close()
+    gv = np.concatenate([x.reshape(-1) for x in g])
+    gmv = np.concatenate([x.reshape(-1) for x in gm])
+    med, medm = float(np.median(times)), float(np.median(tm))
+    return {"metric": "gradient_evaluations_per_s", "value": 1.0 / med, "unit": "evals/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": 1, "ms_per_step": 1e3 * med, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (site tensors i.i.d. normal(0,1), seeded)",
+            "config": {"workload": "j1j2_square_2x2_D3_chi36_J2_0.5_fp64", "D": GRAD["D"], "chi": GRAD["chi"],
+                       "iterations": it, "checkpoint_every": ck, "projector": "full SVD",
+                       "timing": "host wall clock around tg_energy_grad (synchronous call)"},
+            "energy_per_site": E, "seconds_energy_only": t_fwd, "gpu_launches": int(launches),
+            "fd_check": {"entries": args.grad_fd, "step": h, "max_rel_err": max(errs) if errs else None},
+            "mixed": {"value": 1.0 / medm, "unit": "evals/s", "energy_per_site": Em,
+                      "abs_delta_e": abs(Em - E),
+                      "grad_rel_err": float(np.linalg.norm(gmv - gv) / np.linalg.norm(gv))}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -503,8 +588,15 @@ def main():
                     help="CUDA-event profile of the library kernels during the timed sweeps (diagnostic)")
     ap.add_argument("--profile-sweep", action="store_true",
                     help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")
+    ap.add_argument("--grad", action="store_true",
+                    help="gradient evaluations/s of the J1-J2 energy (D=3, chi=36) with the FD check")
+    ap.add_argument("--grad-iters", type=int, default=GRAD["iterations"])
+    ap.add_argument("--grad-fd", type=int, default=32, help="entries checked by central differences")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.grad:
+        print(json.dumps(run_grad(args)), flush=True)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

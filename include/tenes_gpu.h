@@ -174,6 +174,40 @@ tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op);
 tg_status tg_init_tensors(tg_ctx* ctx, int seed, const double* initial_dirs, const int* dir_len,
                           const double* noises);
 
+/* One product term of an energy: <prod ops> on an nrow x ncol window, the
+ * geometry and operator layout of tg_measure_window, divided by the same
+ * window without operators (the norm, shared by all terms of one window as
+ * twosite_obs.cpp:160-181 shares it).  A two-site operator enters as the sum
+ * of the products of its singular components (twosite_obs.cpp:223-243). */
+typedef struct tg_window_term {
+  int source;
+  int nrow, ncol, source_row, source_col;
+  int nops;
+  const int* op_row;
+  const int* op_col;
+  const double* ops; /* nops real d x d operators, concatenated */
+  double coeff;
+} tg_window_term;
+
+/* Energy and its gradient with respect to the site tensors.  No counterpart
+ * in the reference (TeNeS optimises by simple / full update only).
+ *   E = sum_t coeff_t <ops_t> / <1>_t
+ * on the environment reached after `iterations` CTMRG sweeps from the
+ * initial environment of the current site tensors (tg_ctm_init, then
+ * tg_ctm_sweep; full-SVD corner projectors, projector_corner = 1,
+ * use_rsvd = 0; real tensors).  grad (optional, NULL for E only) receives
+ * dE/dTn of every site, concatenated in site order in the layout of
+ * tg_set_site_tensor.  The gradient is a hand-written reverse pass through
+ * the sweeps and the truncated SVDs of the projectors, whose adjoint uses the
+ * Lorentzian-broadened factors (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 +
+ * svd_broadening).  The sweeps are recomputed in segments of
+ * checkpoint_every sweeps, so device memory holds one segment's
+ * intermediates.  With params.mixed the moves' contractions (forward and
+ * adjoint) run as 3xTF32 products; SVDs and the energy stay FP64.  The
+ * context's own environment is left unchanged. */
+tg_status tg_energy_grad(tg_ctx* ctx, int nterms, const tg_window_term* terms, int iterations,
+                         int checkpoint_every, double svd_broadening, double* energy, double* grad);
+
 /* Synchronise the context's stream; report asynchronous CUDA errors. */
 tg_status tg_sync(tg_ctx* ctx);
 

@@ -28,7 +28,7 @@ EXPORTED = [
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
-    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host",
+    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad",
 ]
 
 
@@ -41,6 +41,13 @@ class TGError(RuntimeError):
 class LatticeDesc(C.Structure):
     _fields_ = [("LX", C.c_int), ("LY", C.c_int), ("skew", C.c_int),
                 ("physical_dims", C.POINTER(C.c_int)), ("virtual_dims", C.POINTER(C.c_int))]
+
+
+class WindowTerm(C.Structure):
+    """tg_window_term: one product term of an energy on a window."""
+    _fields_ = [("source", C.c_int), ("nrow", C.c_int), ("ncol", C.c_int), ("source_row", C.c_int),
+                ("source_col", C.c_int), ("nops", C.c_int), ("op_row", C.POINTER(C.c_int)),
+                ("op_col", C.POINTER(C.c_int)), ("ops", C.POINTER(C.c_double)), ("coeff", C.c_double)]
 
 
 class Params(C.Structure):
@@ -104,6 +111,7 @@ def load() -> C.CDLL:
         "tg_gemm_host": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, dp, C.c_int64, C.c_int64, dp, C.c_int64,
                                    C.c_int64, dp, C.c_int64, C.c_int64, C.c_int]),
         "tg_cholqr_host": (C.c_int, [C.c_int64, C.c_int64, dp, C.c_int, P(C.c_int)]),
+        "tg_energy_grad": (C.c_int, [vp, C.c_int, P(WindowTerm), C.c_int, C.c_int, C.c_double, dp, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -20,7 +20,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtenes_gpu.so")
-SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "engine.cu", "api.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "adjoint.cu", "engine.cu", "api.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -216,6 +216,14 @@ tg_status tg_init_tensors(tg_ctx* ctx, int seed, const double* initial_dirs, con
     E(ctx)->init_tensors(seed, initial_dirs, dir_len, noises);
   });
 }
+tg_status tg_energy_grad(tg_ctx* ctx, int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
+                         double svd_broadening, double* energy, double* grad) {
+  return guard([&] {
+    need(terms, "terms");
+    need(energy, "energy");
+    E(ctx)->energy_grad(nterms, terms, iterations, checkpoint_every, svd_broadening, energy, grad);
+  });
+}
 tg_status tg_sync(tg_ctx* ctx) {
   return guard([&] { E(ctx)->sync(); });
 }

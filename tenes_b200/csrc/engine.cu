@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint_device.hpp"
 #include "dtensor.hpp"
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -1931,6 +1932,73 @@ struct EngineT final : Engine {
       upload(Tn[i], reinterpret_cast<const double*>(h.data()));
       rot_ok[i] = false;
       for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+    }
+  }
+
+  // ------------------------------------------------- energy gradient
+  // E = sum_t coeff_t <ops_t>/<1>_t after `iterations` sweeps from the
+  // initial environment, and dE/dTn by the reverse pass of adjoint.hpp
+  void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
+                   double svd_broadening, double* energy, double* grad) override {
+    if constexpr (CPLX) {
+      fail(TG_E_INPUT, "energy gradient: real site tensors only");
+    } else {
+      if (!P.projector_corner || P.use_rsvd)
+        fail(TG_E_INPUT, "energy gradient: full-SVD corner projectors only (projector_corner = 1, use_rsvd = 0)");
+      if (nterms < 1) fail(TG_E_INPUT, "energy gradient: no energy terms");
+      if (!(svd_broadening >= 0.0)) fail(TG_E_INPUT, "energy gradient: svd_broadening must be >= 0");
+      std::vector<ad::WindowTerm> w(static_cast<size_t>(nterms));
+      for (int q = 0; q < nterms; ++q) {
+        const tg_window_term& t = terms[q];
+        check_site(t.source);
+        if (t.nrow < 1 || t.ncol < 1 || t.nrow > 4 || t.ncol > 4) fail(TG_E_INPUT, "window must be 1..4 x 1..4");
+        if (t.source_row < 0 || t.source_row >= t.nrow || t.source_col < 0 || t.source_col >= t.ncol)
+          fail(TG_E_INPUT, "source position outside the window");
+        if (t.nops < 0 || (t.nops > 0 && (!t.op_row || !t.op_col || !t.ops)))
+          fail(TG_E_INPUT, "energy term: operators missing");
+        ad::WindowTerm& a = w[static_cast<size_t>(q)];
+        a.source = t.source;
+        a.nrow = t.nrow;
+        a.ncol = t.ncol;
+        a.source_row = t.source_row;
+        a.source_col = t.source_col;
+        a.coeff = t.coeff;
+        int64_t off = 0;
+        for (int i = 0; i < t.nops; ++i) {
+          const int r = t.op_row[i], c = t.op_col[i];
+          if (r < 0 || r >= t.nrow || c < 0 || c >= t.ncol) fail(TG_E_INPUT, "operator position outside the window");
+          for (int j = 0; j < i; ++j)
+            if (t.op_row[j] == r && t.op_col[j] == c) fail(TG_E_INPUT, "two operators on one window site");
+          const int site = lat.other(t.source, c - t.source_col, t.source_row - r);
+          const int64_t d = lat.pdim[site];
+          a.op_row.push_back(r);
+          a.op_col.push_back(c);
+          a.ops.emplace_back(t.ops + off, t.ops + off + d * d);
+          off += d * d;
+        }
+      }
+      ad::Options o;
+      o.chi = P.chi;
+      o.cutoff = P.inverse_projector_cut;
+      o.eps = svd_broadening;
+      o.iterations = iterations;
+      o.checkpoint_every = checkpoint_every;
+      o.prec_absorb = abs_prec;
+      std::vector<DT<double>> g;
+      const SvdFn fn = [this](DT<double>& A, int64_t m, int64_t n, DT<double>& U, DT<double>& s, DT<double>& VT) {
+        svd(A, m, n, U, s, VT);
+      };
+      const double E = energy_grad_device(st, lat, Tn, w, o, fn, grad ? &g : nullptr);
+      check_infos();
+      *energy = E;
+      if (grad) {
+        int64_t off = 0;
+        for (int i = 0; i < lat.N; ++i) {
+          if (g[static_cast<size_t>(i)].size() != Tn[i].size()) fail(TG_E_RUNTIME, "energy gradient: shape mismatch");
+          download(g[static_cast<size_t>(i)], grad + off);
+          off += Tn[i].size();
+        }
+      }
     }
   }
 

@@ -36,6 +36,8 @@ struct Engine {
   virtual void su_onesite(int site, const double* op) = 0;
   virtual void su_bond(int source, int leg, const double* op) = 0;
   virtual void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) = 0;
+  virtual void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
+                           double svd_broadening, double* energy, double* grad) = 0;
   virtual void sync() = 0;
   virtual void* stream() = 0;
 };

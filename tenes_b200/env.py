@@ -208,6 +208,41 @@ class Environment:
                                          cols, dptr(flat.view(np.float64)), dptr(out)))
         return complex(out[0], out[1])
 
+    def energy_grad(self, terms, iterations: int, checkpoint_every: int = 5, svd_broadening: float = 1e-12,
+                    grad: bool = True):
+        """E = sum_t coeff_t <ops_t>/<1>_t after ``iterations`` CTMRG sweeps from
+        the initial environment of the current site tensors, and dE/dTn per
+        site (None when ``grad`` is False).  ``terms`` are window terms as
+        built by ``tenes_b200.grad`` (dicts with source, nrow, ncol,
+        source_row, source_col, ops {(row, col): d x d real operator}, coeff).
+        The context's environment is left unchanged."""
+        if self.is_complex:
+            raise ValueError("energy_grad: real site tensors only")
+        arr = (_lib.WindowTerm * len(terms))()
+        keep = []
+        for q, t in enumerate(terms):
+            keys = sorted(t["ops"])
+            rows = (C.c_int * max(len(keys), 1))(*[k[0] for k in keys])
+            cols = (C.c_int * max(len(keys), 1))(*[k[1] for k in keys])
+            flat = np.ascontiguousarray(
+                np.concatenate([np.asarray(t["ops"][k], dtype=np.float64).reshape(-1) for k in keys])
+                if keys else np.zeros(1), dtype=np.float64)
+            keep.append((rows, cols, flat))
+            arr[q] = _lib.WindowTerm(t["source"], t["nrow"], t["ncol"], t["source_row"], t["source_col"],
+                                     len(keys), rows, cols, dptr(flat), float(t["coeff"]))
+        E = np.zeros(1)
+        sizes = [int(np.prod(self.site_shape(i))) for i in range(self.N)]
+        g = np.zeros(sum(sizes)) if grad else None
+        check(self.lib.tg_energy_grad(self.ctx, len(terms), arr, int(iterations), int(checkpoint_every),
+                                      float(svd_broadening), dptr(E), dptr(g) if grad else None))
+        if not grad:
+            return float(E[0]), None
+        out, off = [], 0
+        for i, n in enumerate(sizes):
+            out.append(g[off:off + n].reshape(self.site_shape(i)))
+            off += n
+        return float(E[0]), out
+
     def tm_eigenvalues(self, direction: int, fixed: int, num_eigvals: int = 4, maxdim_dense: int = 200,
                        arnoldi_maxdim: int = 50, arnoldi_restartdim: int = 20, arnoldi_maxiter: int = 1,
                        arnoldi_rtol: float = 1e-10) -> np.ndarray:
