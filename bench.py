@@ -518,15 +518,21 @@ def run_grad(args):
         out = env.energy_grad(terms, it, ck, grad=grad)
         return out, time.perf_counter() - t0
 
+    from tenes_b200.env import profile_enable, profile_query, profile_reset
     env = grad_env(Tn, False)
-    (E, g), _ = timed(env)  # warm-up
+    env.energy_grad(terms, 1, ck)  # warm-up (library and solver initialisation)
     l0 = kernel_launch_count()
     times = []
     for _ in range(args.steps):
         (E, g), dt = timed(env)
         times.append(dt)
     launches = (kernel_launch_count() - l0) // max(args.steps, 1)
+    profile_enable(True)
+    profile_reset()
     _, t_fwd = timed(env, grad=False)
+    kinds = ["gemm_dmma", "permute", "normalize", "spectrum", "factorisations", "other", "gemm_tcgen05"]
+    breakdown = {k: round(profile_query(q)[1], 3) for q, k in enumerate(kinds)}
+    profile_enable(False)
     gmax = max(float(np.abs(x).max()) for x in g)
     rng = np.random.default_rng(SEED + 1)
     errs, h = [], GRAD["fd_step"]
@@ -544,7 +550,7 @@ def run_grad(args):
         errs.append(abs(fd - g[site][idx]) / max(abs(fd), abs(g[site][idx]), 1e-3 * gmax))
     env.close()
     envm = grad_env(Tn, True)
-    (Em, gm), _ = timed(envm)
+    envm.energy_grad(terms, 1, ck)
     tm = []
     for _ in range(args.steps):
         (Em, gm), dt = timed(envm)
@@ -561,6 +567,7 @@ def run_grad(args):
                        "iterations": it, "checkpoint_every": ck, "projector": "full SVD",
                        "timing": "host wall clock around tg_energy_grad (synchronous call)"},
             "energy_per_site": E, "seconds_energy_only": t_fwd, "gpu_launches": int(launches),
+            "energy_only_breakdown_ms": breakdown,
             "fd_check": {"entries": args.grad_fd, "step": h, "max_rel_err": max(errs) if errs else None},
             "mixed": {"value": 1.0 / medm, "unit": "evals/s", "energy_per_site": Em,
                       "abs_delta_e": abs(Em - E),

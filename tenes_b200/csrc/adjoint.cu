@@ -165,6 +165,16 @@ __global__ void svd_core_kernel(const double* __restrict__ J, const double* __re
   }
 }
 
+// Ur = U with the columns of vanishing singular values (s_j <= tol s_0)
+// zeroed, VTr = VT with those rows zeroed
+__global__ void svd_rank_mask_kernel(const double* __restrict__ U, const double* __restrict__ VT,
+                                     const double* __restrict__ s, int64_t m, int64_t n, int64_t k, double tol,
+                                     double* __restrict__ Ur, double* __restrict__ VTr) {
+  const double thr = tol * s[0];
+  GRID_STRIDE(i, m * k) { Ur[i] = s[i % k] > thr ? U[i] : 0.0; }
+  GRID_STRIDE(i, k * n) { VTr[i] = s[i / n] > thr ? VT[i] : 0.0; }
+}
+
 // X(rows x k) columns j scaled by sinv_j^2 = 1 / s_j (0 beyond w or where cut)
 __global__ void scale_cols_sq_kernel(double* __restrict__ X, int64_t rows, int64_t k, const double* __restrict__ sinv,
                                      int64_t w) {
@@ -261,6 +271,15 @@ struct DevBackend {
     svd_gs_kernel<<<static_cast<unsigned>(k), 256, 0, st>>>(gUc.p, gVTc.p, U.p, VT.p, sinv.p, m, n, k, w, gs.p);
     TG_CHECK_LAUNCH();
     count_launch(2);
+  }
+  void svd_rank_mask(const Ten& U, const Ten& VT, const Ten& s, double tol, Ten& Ur, Ten& VTr) {
+    const int64_t m = U.dim(0), k = U.dim(1), n = VT.dim(1);
+    Ur = Ten({m, k}, st);
+    VTr = Ten({k, n}, st);
+    svd_rank_mask_kernel<<<blocks_for(std::max(m * k, k * n)), 256, 0, st>>>(U.p, VT.p, s.p, m, n, k, tol, Ur.p,
+                                                                             VTr.p);
+    TG_CHECK_LAUNCH();
+    count_launch();
   }
   Ten svd_core(const Ten& J, const Ten& K, const Ten& s, const Ten& gs, int64_t k, double eps) {
     Ten core({k, k}, st);

@@ -18,8 +18,12 @@
 //               F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps):
 //               gM = U [diag(gs) + (F o (J - J^T)) S + S (F o (K - K^T))] VT
 //                    + (1 - U U^T) gU S^-1 VT + U S^-1 gVT (1 - V V^T),
-//               J = U^T gU, K = V^T gV (the last two terms carry the
-//               truncation to the discarded subspace of a non-square M).
+//               J = U^T gU, K = V^T gV.  U, S, V are the rank-r part of
+//               the SVD (singular values above kRankTol s_0; the rest are
+//               taken as exact zeros), so the last two terms carry the whole
+//               null space and the result does not depend on how a solver
+//               completes the singular vectors of vanishing values (the
+//               zero-padded environments of the first sweeps have many).
 //
 // Memory: the sweeps are cut into segments of `checkpoint_every` sweeps; the
 // forward keeps only the environment at each segment start, and the backward
@@ -67,6 +71,12 @@ struct Options {
   int checkpoint_every = 5;
   int prec_absorb = 0;     // product precision of the moves (0 FP64, 1 3xTF32)
 };
+
+// Singular values at or below kRankTol times the largest count as zero in
+// the SVD adjoint.  Dropping their F terms changes the result by O(s_j / s_i)
+// against the kept values; in exchange the adjoint reads no singular vector
+// whose direction a Jacobi solver fixes only to eps s_0 / s_j.
+constexpr double kRankTol = 1e-10;
 
 inline bool identity_perm(const Axes& p) {
   for (size_t i = 0; i < p.size(); ++i)
@@ -346,22 +356,23 @@ class Tape {
     const Ten gVTc = BK::empty(nd.gVTc) ? bk.zeros({w, n}) : nd.gVTc;
     Ten gU, gVT, gs;
     bk.svd_prep(gUc, gVTc, nd.U, nd.VT, nd.sinv, m, n, k, w, gU, gVT, gs);
-    const Ten J = bk.td(nd.U, gU, {0}, {0}, 0);    // U^T gU  (k x k)
-    const Ten K = bk.td(nd.VT, gVT, {1}, {1}, 0);  // V^T gV  (k x k)
+    // rank-r factors: columns of U / rows of VT of vanishing values zeroed
+    Ten U, VT;
+    bk.svd_rank_mask(nd.U, nd.VT, nd.s, kRankTol, U, VT);
+    const Ten J = bk.td(U, gU, {0}, {0}, 0);    // U^T gU  (k x k)
+    const Ten K = bk.td(VT, gVT, {1}, {1}, 0);  // V^T gV  (k x k)
     const Ten core = bk.svd_core(J, K, nd.s, gs, k, eps);
-    Ten gM = bk.td(bk.td(nd.U, core, {1}, {0}, 0), nd.VT, {1}, {0}, 0);
-    if (m > k) {  // (1 - U U^T) gU S^-1 VT
-      Ten P = bk.td(nd.U, J, {1}, {0}, 0);
-      bk.axpy(P, gU, -1.0);
-      bk.scale_cols_sq(P, nd.sinv, w);
-      bk.axpy(gM, bk.td(P, nd.VT, {1}, {0}, 0), -1.0);
-    }
-    if (n > k) {  // U S^-1 gVT (1 - V V^T)
-      Ten Q = bk.td(bk.td(gVT, nd.VT, {1}, {1}, 0), nd.VT, {1}, {0}, 0);
-      bk.axpy(Q, gVT, -1.0);
-      bk.scale_rows_sq(Q, nd.sinv, w);
-      bk.axpy(gM, bk.td(nd.U, Q, {1}, {0}, 0), -1.0);
-    }
+    Ten gM = bk.td(bk.td(U, core, {1}, {0}, 0), VT, {1}, {0}, 0);
+    // (1 - U U^T) gU S^-1 VT
+    Ten P = bk.td(U, J, {1}, {0}, 0);
+    bk.axpy(P, gU, -1.0);
+    bk.scale_cols_sq(P, nd.sinv, w);
+    bk.axpy(gM, bk.td(P, VT, {1}, {0}, 0), -1.0);
+    // U S^-1 gVT (1 - V V^T)
+    Ten Q = bk.td(bk.td(gVT, VT, {1}, {1}, 0), VT, {1}, {0}, 0);
+    bk.axpy(Q, gVT, -1.0);
+    bk.scale_rows_sq(Q, nd.sinv, w);
+    bk.axpy(gM, bk.td(U, Q, {1}, {0}, 0), -1.0);
     acc(nd.a, gM);
   }
 };

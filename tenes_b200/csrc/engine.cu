@@ -156,6 +156,7 @@ struct EngineT final : Engine {
     spec_old = DT<double>();
     if (st) cudaStreamSynchronize(st);
     cudaDeviceGraphMemTrim(dev);
+    if (gj_params) cusolverDnDestroyGesvdjInfo(gj_params);
     if (sol) cusolverDnDestroy(sol);
     cudaFree(d_max);
     cudaFree(d_info);
@@ -344,6 +345,41 @@ struct EngineT final : Engine {
       // U_A = conj(V_B) = (VT_B)^T read row-major without conj -> conj needed
       // only on the value: VT_B holds V_B^H, whose row-major reading is
       // conj(V_B) already; VT_A = U_B^T has no conjugation.
+    }
+  }
+
+  // The same factors by cuSOLVER's Jacobi SVD (gesvdj, real matrices),
+  // which takes any m, n and runs on the device without the host-side
+  // bidiagonal iteration of gesvd; the energy gradient's projector SVDs use
+  // it.  Singular vectors of vanishing values may be left incomplete, which
+  // the gradient's SVD adjoint does not read.  The column-major view of the
+  // row-major A is A^T = U' S V'^T, so VT = U'^T is U' read row-major and U
+  // is the transpose of V' read row-major.
+  gesvdjInfo_t gj_params = nullptr;
+  void svd_jacobi(DT<T>& A, int64_t m, int64_t n, DT<T>& U, DT<double>& s, DT<T>& VT) {
+    if constexpr (CPLX) {
+      fail(TG_E_RUNTIME, "svd_jacobi: real matrices only");
+    } else {
+      if (!gj_params) {
+        check_sol(cusolverDnCreateGesvdjInfo(&gj_params), "CreateGesvdjInfo");
+        check_sol(cusolverDnXgesvdjSetSortEig(gj_params, 1), "gesvdjSetSortEig");
+      }
+      const int64_t k = std::min(m, n);
+      const int rows = static_cast<int>(n), cols = static_cast<int>(m);
+      ProfScope ps(PK_SOLVER, st, 22.0 * static_cast<double>(m) * n * k, 0.0);
+      s = DT<double>({k}, st);
+      DT<T> Ub({k, n}, st);  // U' (n x k column-major) = VT (k x n row-major)
+      DT<T> Vb({k, m}, st);  // V' (m x k column-major) = U^T (k x m row-major)
+      int lwork = 0;
+      check_sol(cusolverDnDgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p,
+                                             rows, Vb.p, cols, &lwork, gj_params),
+                "Dgesvdj_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
+      check_sol(cusolverDnDgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p, rows, Vb.p,
+                                  cols, work.p, lwork, info_slot(), gj_params),
+                "Dgesvdj");
+      VT = reshape(Ub, {k, n});
+      U = tr(reshape(Vb, {k, m}), {1, 0});
     }
   }
 
@@ -1986,7 +2022,7 @@ struct EngineT final : Engine {
       o.prec_absorb = abs_prec;
       std::vector<DT<double>> g;
       const SvdFn fn = [this](DT<double>& A, int64_t m, int64_t n, DT<double>& U, DT<double>& s, DT<double>& VT) {
-        svd(A, m, n, U, s, VT);
+        svd_jacobi(A, m, n, U, s, VT);
       };
       const double E = energy_grad_device(st, lat, Tn, w, o, fn, grad ? &g : nullptr);
       check_infos();

@@ -96,11 +96,12 @@ class CTMEnergy(torch.autograd.Function):
         want = any(ctx.needs_input_grad[5:])
         E, g = env.energy_grad(terms, iterations, checkpoint_every, broadening, grad=want)
         ctx.grads = [torch.from_numpy(x.copy()) for x in g] if want else None
+        ctx.nsites = len(Tn)
         return torch.tensor(E, dtype=torch.float64)
 
     @staticmethod
     def backward(ctx, gE: torch.Tensor):
-        grads = tuple(gE * g for g in ctx.grads) if ctx.grads is not None else (None,) * 0
+        grads = tuple(gE * g for g in ctx.grads) if ctx.grads is not None else (None,) * ctx.nsites
         return (None, None, None, None, None) + grads
 
 

@@ -10,12 +10,15 @@
 //   per site: D0*D1*D2*D3*pdim values (row-major)
 //   nterms, then per term: source nrow ncol source_row source_col coeff nops,
 //     then per operator: row col d, d*d values
-// Output: "E <energy>" and one line "G <values>" per site.
+// Output: "E <energy>" and one line "G <values>" per site.  With the argument
+// "zero-null" the host SVD leaves the singular vectors of vanishing values
+// as zero vectors.
 #include <cmath>
 #include <cstdio>
 #include <iostream>
 #include <memory>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "adjoint.hpp"
@@ -56,6 +59,10 @@ HT permute(const HT& a, const Axes& perm) {
 
 // one-sided Jacobi SVD of a row-major m x n matrix with m >= n: U (m x n,
 // orthonormal, completed where a singular value vanishes), s descending, VT (n x n)
+// When set, singular vectors of vanishing values are left as zero vectors
+// instead of completing the basis (a solver that does not complete them).
+bool g_zero_null = false;
+
 void jacobi_svd_tall(const std::vector<double>& A, int64_t m, int64_t n, std::vector<double>& U,
                      std::vector<double>& s, std::vector<double>& VT) {
   std::vector<double> W(A), V(static_cast<size_t>(n * n), 0.0);
@@ -123,6 +130,8 @@ void jacobi_svd_tall(const std::vector<double>& A, int64_t m, int64_t n, std::ve
     if (nrm[j] > tiny) {
       for (int64_t i = 0; i < m; ++i) u[i] = W[i * n + j] / nrm[j];
       a = project_out(u);
+    } else if (g_zero_null) {
+      continue;
     } else {
       // a vanishing value: complete the basis with the standard basis vector
       // that keeps the most norm outside the columns so far
@@ -279,6 +288,16 @@ struct HostBackend {
       gs.p()[j] = -0.5 * si * si * si * a;
     }
   }
+  void svd_rank_mask(const Ten& U, const Ten& VT, const Ten& s, double tol, Ten& Ur, Ten& VTr) {
+    const int64_t m = U.sh[0], k = U.sh[1], n = VT.sh[1];
+    Ur = make({m, k});
+    VTr = make({k, n});
+    for (int64_t j = 0; j < k; ++j) {
+      const bool keep = s.p()[j] > tol * s.p()[0];
+      for (int64_t i = 0; i < m; ++i) Ur.p()[i * k + j] = keep ? U.p()[i * k + j] : 0.0;
+      for (int64_t l = 0; l < n; ++l) VTr.p()[j * n + l] = keep ? VT.p()[j * n + l] : 0.0;
+    }
+  }
   Ten svd_core(const Ten& J, const Ten& K, const Ten& s, const Ten& gs, int64_t k, double eps) {
     HT c = make({k, k});
     for (int64_t i = 0; i < k; ++i)
@@ -319,7 +338,8 @@ struct HostBackend {
 
 }  // namespace
 
-int main() {
+int main(int argc, char** argv) {
+  g_zero_null = argc > 1 && std::string(argv[1]) == "zero-null";
   int LX, LY, skew, chi, iters, ckpt;
   double cutoff, eps;
   std::cin >> LX >> LY >> skew >> chi >> iters >> ckpt >> cutoff >> eps;

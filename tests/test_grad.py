@@ -153,7 +153,7 @@ def host_adjoint(tmp_path_factory):
     return out
 
 
-def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12):
+def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12, zero_null=False):
     lines = [f"{lat.LX} {lat.LY} 0 {chi} {iters} {ckpt}", f"{cutoff!r} {eps!r}"]
     for i in range(lat.N_UNIT):
         lines.append(" ".join(str(x) for x in [lat.physical_dims[i]] + list(lat.virtual_dims[i])))
@@ -167,7 +167,8 @@ def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12):
         for k in keys:
             op = np.asarray(t["ops"][k], dtype=np.float64)
             lines.append(f"{k[0]} {k[1]} {op.shape[0]} " + " ".join(repr(float(x)) for x in op.reshape(-1)))
-    res = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True, check=True)
+    res = subprocess.run([exe] + (["zero-null"] if zero_null else []), input="\n".join(lines) + "\n",
+                         capture_output=True, text=True, check=True)
     out = res.stdout.splitlines()
     E = float(out[0].split()[1])
     g = [np.array([float(x) for x in ln.split()[1:]]).reshape(Tn[i].shape) for i, ln in enumerate(out[1:])]
@@ -207,3 +208,17 @@ def test_host_adjoint_checkpoint_interval_is_invisible(host_adjoint):
     for a, b, c in zip(g1, g4, g3):
         np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-15)
         np.testing.assert_allclose(a, c, rtol=1e-12, atol=1e-15)
+
+
+def test_host_adjoint_does_not_use_null_space_vectors(host_adjoint):
+    """chi > D^2 pads the first environments with zeros, so the projector
+    matrices have exactly vanishing singular values; the adjoint must not
+    depend on how the SVD completes their singular vectors."""
+    rng = np.random.default_rng(13)
+    lat = lattice(2, 2, uniform_dims(4, 2))
+    Tn = random_tensors(lat, rng)
+    terms = j1j2_terms(4, 1.0, 0.5)
+    E1, g1 = run_host(host_adjoint, lat, Tn, terms, 6, 2, ckpt=1)
+    E2, g2 = run_host(host_adjoint, lat, Tn, terms, 6, 2, ckpt=1, zero_null=True)
+    assert abs(E1 - E2) <= 1e-12 * abs(E1)
+    assert _rel(g2, g1) <= 1e-9, _rel(g2, g1)
