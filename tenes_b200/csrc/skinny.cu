@@ -23,7 +23,6 @@ namespace {
 constexpr int SK_R = 64;         // rows of Big per tile
 constexpr int SK_THREADS = 256;  // 8 warps, one 8-row block each
 constexpr int SK_NMAX = 96;      // n and K at most this
-constexpr int SK_NB = SK_NMAX / 8;
 constexpr size_t SK_SMEM_2CTA = 113 * 1024;  // two CTAs per SM at or below this
 
 struct SkinnyParams {
