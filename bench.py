@@ -184,14 +184,15 @@ def traffic_from_profile(cfg, family):
 def bond_energy(env):
     """Energy per site: <S.S> over the horizontal and vertical bond of every
     site, each normalised by the same contraction with the identity
-    (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225)."""
+    (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225), both read
+    from the bond's reduced density matrix (one contraction per bond)."""
     from tenes_b200.std_ops import heisenberg_bond, real_if_close
     h = real_if_close(heisenberg_bond(1.0))
-    ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
     tot = 0.0
     for s in range(env.N):
         for dx, dy in ((1, 0), (0, 1)):
-            tot += (env.contract_bond_op12(s, dx, dy, h) / env.contract_bond_op12(s, dx, dy, ident)).real
+            rho = env.contract_bond_rdm(s, dx, dy)
+            tot += (np.sum(h * rho) / np.einsum("abab->", rho)).real
     return tot / env.N
 
 

@@ -139,6 +139,14 @@ tg_status tg_measure_onesite(tg_ctx* ctx, int site, const double* op, double* ou
 tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const double* op,
                                double* out);
 
+/* Two-site reduced density matrix of the nearest-neighbour bond of
+ * tg_measure_bond_op12, unnormalised, legs (source, target, source', target')
+ * (d_s * d_t * d_s * d_t values, interleaved pairs when complex): the op12
+ * value of that call is sum op12 * rdm and the norm sum_ab rdm[a,b,a,b], so
+ * one contraction of the bond serves any number of operators.  The same
+ * contraction sequence as Contract_two_sites_*_op12 (ctm.cpp:213-319). */
+tg_status tg_measure_bond_rdm(tg_ctx* ctx, int source, int dx, int dy, double* out);
+
 /* <prod of one-site ops> on an nrow x ncol window (1..4 each), unnormalised:
  * Contract_RxC_iTPS_CTM (contract_itps_ctm/ctm.cpp:45-87).  The window holds
  * site lat.other(source, c - source_col, source_row - r) at (r, c), row 0 on

@@ -173,6 +173,12 @@ tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const do
     E(ctx)->measure_bond_op12(source, dx, dy, op, out);
   });
 }
+tg_status tg_measure_bond_rdm(tg_ctx* ctx, int source, int dx, int dy, double* out) {
+  return guard([&] {
+    need(out, "out");
+    E(ctx)->measure_bond_rdm(source, dx, dy, out);
+  });
+}
 tg_status tg_measure_window(tg_ctx* ctx, int source, int nrow, int ncol, int source_row, int source_col, int nops,
                             const int* op_row, const int* op_col, const double* ops, double* out) {
   return guard([&] {

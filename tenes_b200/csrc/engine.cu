@@ -1298,10 +1298,11 @@ struct EngineT final : Engine {
     if constexpr (!CPLX) out[1] = 0.0;
   }
 
-  // Contract_two_sites_horizontal_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:213-264)
-  T two_sites_h(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
-                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
-                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+  // Contract_two_sites_horizontal_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:213-264) up to the
+  // operator: X with <op12> = sum op12[a,b,c,d] X[a,c,b,d]
+  DT<T> bond_X_h(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                 const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                 const DT<T>& T1, const DT<T>& T2) {
     DT<T> A = td(eT5, td(C1, td(C4, eT6, {1}, {0}), {0}, {1}), {1}, {1});
     A = td(T1, A, {0, 3}, {5, 2}, true, false);
     A = td(T1, A, {0, 3}, {6, 4});
@@ -1310,14 +1311,20 @@ struct EngineT final : Engine {
     B = td(T2, B, {2, 3}, {5, 2}, true, false);
     B = td(T2, B, {2, 3}, {6, 4});
     B = td(eT2, B, {1, 2, 3}, {7, 1, 4});
-    DT<T> X = td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+    return td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+  }
+  T two_sites_h(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+    const DT<T> X = bond_X_h(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, T1, T2);
     return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
   }
 
-  // Contract_two_sites_vertical_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:266-319)
-  T two_sites_v(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
-                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
-                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+  // Contract_two_sites_vertical_op12_iTPS_CTM (contract_itps_ctm/ctm.cpp:266-319) up to the
+  // operator, as bond_X_h
+  DT<T> bond_X_v(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                 const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                 const DT<T>& T1, const DT<T>& T2) {
     DT<T> A = td(eT6, td(C1, td(C2, eT1, {0}, {1}), {1}, {1}), {1}, {0});
     A = td(T1, A, {0, 1}, {2, 5}, true, false);
     A = td(T1, A, {0, 1}, {4, 6});
@@ -1326,7 +1333,12 @@ struct EngineT final : Engine {
     B = td(T2, B, {0, 3}, {2, 5}, true, false);
     B = td(T2, B, {0, 3}, {4, 6});
     B = td(eT3, B, {1, 2, 3}, {7, 1, 4});
-    DT<T> X = td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+    return td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
+  }
+  T two_sites_v(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
+                const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
+                const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
+    const DT<T> X = bond_X_v(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, T1, T2);
     return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
   }
 
@@ -1367,6 +1379,35 @@ struct EngineT final : Engine {
     }
     std::memcpy(out, &v, sizeof(T));
     if constexpr (!CPLX) out[1] = 0.0;
+  }
+
+  // The two-site reduced density matrix of a nearest-neighbour bond,
+  // unnormalised, legs (source, target, source', target'): every op12 of
+  // twosite_obs.cpp:186-222 measures as sum op12 * rdm, the norm as
+  // sum_ab rdm[a,b,a,b] -- one contraction of the bond for any number of
+  // operators.
+  void measure_bond_rdm(int source, int dx, int dy, double* out) override {
+    require_env();
+    check_site(source);
+    if (std::abs(dx) + std::abs(dy) != 1) fail(TG_E_INPUT, "bond must be a nearest-neighbour bond");
+    DT<T> X;
+    bool source_first;
+    if (dy == 0) {
+      const int source_col = dx >= 0 ? 0 : 1;
+      const int left = lat.other(source, -source_col, 0), right = lat.other(source, 1 - source_col, 0);
+      X = bond_X_h(C[0][left], C[1][right], C[2][right], C[3][left], E[0][left], E[0][right], E[1][right],
+                   E[2][right], E[2][left], E[3][left], Tn[left], Tn[right]);
+      source_first = left == source;
+    } else {
+      const int source_row = dy >= 0 ? 1 : 0;
+      const int top = lat.other(source, 0, source_row), bottom = lat.other(source, 0, source_row - 1);
+      X = bond_X_v(C[0][top], C[1][top], C[2][bottom], C[3][bottom], E[0][top], E[1][top], E[1][bottom],
+                   E[2][bottom], E[3][bottom], E[3][top], Tn[top], Tn[bottom]);
+      source_first = top == source;
+    }
+    // X[a,c,b,d] with (a,c) the first site's legs: rdm_first[a,b,c,d] = X[a,c,b,d]; with the
+    // source second, rdm_source[b,a,d,c] = X[a,c,b,d]
+    download(tr(X, source_first ? V{0, 2, 1, 3} : V{2, 0, 3, 1}), out);
   }
 
   // ------------------------------------------------- N x M window <op...>

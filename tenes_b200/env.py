@@ -192,6 +192,17 @@ class Environment:
         check(self.lib.tg_measure_bond_op12(self.ctx, source, dx, dy, dptr(o.view(np.float64)), dptr(out)))
         return complex(out[0], out[1])
 
+    def contract_bond_rdm(self, source: int, dx: int, dy: int) -> np.ndarray:
+        """Unnormalised two-site reduced density matrix of a nearest-neighbour
+        bond, legs (source, target, source', target'): <op12> = sum(op12 * rdm),
+        norm = einsum('abab', rdm)."""
+        from .input import LatticeSpec
+        target = LatticeSpec(self.LX, self.LY, self.skew, self.pdim, self.vdim, [], []).other(source, dx, dy)
+        shape = (self.pdim[source], self.pdim[target]) * 2
+        out = np.zeros(int(np.prod(shape)) * (2 if self.is_complex else 1))
+        check(self.lib.tg_measure_bond_rdm(self.ctx, source, dx, dy, dptr(out)))
+        return out.view(self.dtype).reshape(shape)
+
     def contract_window(self, source: int, nrow: int, ncol: int, source_row: int, source_col: int,
                         ops: Optional[dict] = None) -> complex:
         """Contract_RxC_iTPS_CTM: <prod ops> on an nrow x ncol window (unnormalised).

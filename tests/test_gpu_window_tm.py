@@ -55,3 +55,39 @@ def test_transfer_matrix_eigenvalues(is_complex, chi):
             xg, eg = O.correlation_length(g, L)
             np.testing.assert_allclose(np.abs(g), np.abs(o), rtol=1e-9 if chi == 8 else 1e-7)
             assert abs(xg - xo) <= (1e-9 if chi == 8 else 1e-7) * abs(xo)
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_bond_rdm_reproduces_op12(is_complex):
+    """tg_measure_bond_rdm: sum(op12 * rdm) equals Contract_two_sites_*_op12 of
+    the oracle (source left / right / top / bottom), einsum('abab', rdm) its norm."""
+    lat, Tn, oe, ge = _setup(is_complex)
+    rng = np.random.default_rng(17)
+    for source in range(lat.N_UNIT):
+        for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+            op = rng.standard_normal((2, 2, 2, 2))
+            if is_complex:
+                op = op + 1j * rng.standard_normal((2, 2, 2, 2))
+            rho = ge.contract_bond_rdm(source, dx, dy)
+            assert rho.shape == (2, 2, 2, 2)
+            g = ge.contract_bond_op12(source, dx, dy, op)
+            assert abs(np.sum(op * rho) - g) <= 1e-11 * abs(g), (source, dx, dy)
+            ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+            n = ge.contract_bond_op12(source, dx, dy, ident)
+            assert abs(np.einsum("abab->", rho) - n) <= 1e-11 * abs(n)
+            # against the oracle directly
+            target = lat.other(source, dx, dy)
+            if dy == 0:
+                left, right = (source, target) if dx > 0 else (target, source)
+                o = op if left == source else op.transpose(1, 0, 3, 2)
+                ref = O.contract_two_sites_horizontal_op12(
+                    oe.C1[left], oe.C2[right], oe.C3[right], oe.C4[left], oe.eTt[left], oe.eTt[right],
+                    oe.eTr[right], oe.eTb[right], oe.eTb[left], oe.eTl[left], Tn[left], Tn[right], o)
+            else:
+                top, bottom = (target, source) if dy > 0 else (source, target)
+                o = op if top == source else op.transpose(1, 0, 3, 2)
+                ref = O.contract_two_sites_vertical_op12(
+                    oe.C1[top], oe.C2[top], oe.C3[bottom], oe.C4[bottom], oe.eTt[top], oe.eTr[top],
+                    oe.eTr[bottom], oe.eTb[bottom], oe.eTl[bottom], oe.eTl[top], Tn[top], Tn[bottom], o)
+            assert abs(np.sum(op * rho) - ref) <= 1e-10 * abs(ref), (source, dx, dy)
+    ge.close()
