@@ -5,6 +5,7 @@ import argparse
 import sys
 
 from .input import InputError
+from .saveload import LoadError
 
 
 def main(argv=None) -> int:
@@ -19,7 +20,7 @@ def main(argv=None) -> int:
     from .itps import run
     try:
         run(a.input, device=a.device, mixed=a.mixed, print_level=0 if a.quiet else 1, outdir=a.outdir)
-    except InputError as e:
+    except (InputError, LoadError) as e:
         print(f"ERROR: {e}", file=sys.stderr)
         return 1
     return 0

@@ -11,6 +11,8 @@ of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 Out of scope (raises InputError): full update (num_step > 0 of
 [parameter.full_update]), finite-temperature mode, the mean-field environment;
 long-range correlation functions ([correlation]) are skipped with a warning.
+Tensor checkpoints (tensor_save / tensor_load) are written and read by
+saveload.py.
 """
 
 from __future__ import annotations
@@ -25,6 +27,7 @@ import numpy as np
 
 from .env import CTMParams, Environment
 from .input import Input, InputError, load_input
+from .saveload import load_tensors, save_tensors
 
 
 def _fmt(x: float) -> str:
@@ -53,7 +56,12 @@ class ITPS:
                        inverse_lambda_cut=p.Inverse_lambda_cut, mixed=mixed)
         self.env = Environment(ls.LX, ls.LY, ls.physical_dims, ls.virtual_dims, cp, not self.is_real,
                                skew=ls.skew, device=device)
-        self.env.init_tensors(p.seed, ls.initial_dirs, ls.noises)
+        if p.tensor_save_dir:  # iTPS.cpp:161-173
+            os.makedirs(p.tensor_save_dir, exist_ok=True)
+        if p.tensor_load_dir:  # initialize_tensors: the checkpoint replaces the random start (tensors.cpp:130-135)
+            load_tensors(self.env, p.tensor_load_dir, p.CHI, print_level)
+        else:
+            self.env.init_tensors(p.seed, ls.initial_dirs, ls.noises)
         if p.Simple_Gauge_Fix:
             raise InputError("simple_update.gauge_fix is not part of this library")
         self.outdir = p.outdir
@@ -463,10 +471,14 @@ def run(path: str, device: int = 0, mixed: bool = False, print_level: int = 1,
     if outdir is not None:
         inp.params.outdir = outdir
     it = ITPS(inp, device=device, mixed=mixed, print_level=print_level)
+    # run_groundstate / run_timeevolution (main.cpp:141-177): the checkpoint
+    # is written after the optimisation, before the measurement
     if inp.params.calcmode == "time_evolution":
         it.time_evolution()
+        save_tensors(it.env, inp.params.tensor_save_dir, inp.params.CHI, print_level)
     else:
         it.optimize()
+        save_tensors(it.env, inp.params.tensor_save_dir, inp.params.CHI, print_level)
         if inp.params.to_measure:
             it.measure()
     it.summary()

@@ -23,6 +23,59 @@ class OracleEnvironment:
         self.env = None
         self.lam = [[np.ones(v[l]) for l in range(4)] for v in virtual_dims]
 
+    # accessors of tenes_b200.env.Environment (checkpoints)
+    @property
+    def pdim(self):
+        return self.lat.physical_dims
+
+    @property
+    def vdim(self):
+        return self.lat.virtual_dims
+
+    def site_shape(self, i):
+        v = self.lat.virtual_dims[i]
+        return (v[0], v[1], v[2], v[3], self.lat.physical_dims[i])
+
+    def env_shape(self, which, i):
+        chi = self.p.CHI
+        if which < 4:
+            return (chi, chi)
+        d = self.lat.virtual_dims[i][{4: 1, 5: 2, 6: 3, 7: 0}[which]]
+        return (chi, chi, d, d)
+
+    def _env_or_zeros(self):
+        if self.env is None:
+            dt = np.complex128 if self.is_complex else np.float64
+            names = ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")
+            self.env = O.Env(*[[np.zeros(self.env_shape(w, i), dtype=dt) for i in range(self.N)]
+                               for w in range(len(names))])
+        return self.env
+
+    def get_site_tensor(self, i):
+        return np.array(self.Tn[i], copy=True)
+
+    def set_site_tensor(self, i, T):
+        if not hasattr(self, "Tn"):
+            self.Tn = [None] * self.N
+        assert tuple(T.shape) == self.site_shape(i)
+        self.Tn[i] = np.array(T, dtype=np.complex128 if self.is_complex else np.float64)
+
+    def get_env(self, which, i):
+        names = ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")
+        return np.array(getattr(self._env_or_zeros(), names[which])[i], copy=True)
+
+    def set_env(self, which, i, T):
+        names = ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")
+        assert tuple(T.shape) == self.env_shape(which, i)
+        getattr(self._env_or_zeros(), names[which])[i] = np.array(T)
+
+    def get_lambda(self, i, leg):
+        return np.array(self.lam[i][leg], copy=True)
+
+    def set_lambda(self, i, leg, lam):
+        assert len(lam) == self.lat.virtual_dims[i][leg]
+        self.lam[i][leg] = np.array(lam, dtype=np.float64)
+
     def init_tensors(self, seed, initial_dirs, noises):
         self.lat.initial_dirs = [list(d) for d in initial_dirs]
         self.lat.noises = list(noises)
