@@ -60,6 +60,15 @@ class TransferMatrixParameters:
 
 
 @dataclass
+class CorrelationParameters:
+    """[correlation] (CorrelationParameter, correlation_function.hpp:33-39;
+    gen_corparam, load_toml.cpp:298-314): r_max and (left, right) one-site
+    operator groups."""
+    r_max: int = 0
+    operators: List[Tuple[int, int]] = field(default_factory=list)
+
+
+@dataclass
 class LatticeSpec:
     """[tensor] section (load_toml.cpp:247-296)."""
     LX: int
@@ -130,6 +139,7 @@ class Input:
     multisite: List[Operator]
     tm_params: TransferMatrixParameters
     is_real: bool
+    corparam: CorrelationParameters = field(default_factory=CorrelationParameters)
 
 
 def _drop_comment(line: str) -> str:
@@ -408,10 +418,19 @@ def load_input_dict(toml: dict) -> Input:
         tm.arnoldi_restartdim = int(cl.get("arnoldi_restartdim", tm.arnoldi_restartdim))
         tm.arnoldi_maxiter = int(cl.get("arnoldi_maxiterations", tm.arnoldi_maxiter))
         tm.arnoldi_rtol = float(cl.get("arnoldi_rtol", tm.arnoldi_rtol))
+    cp = CorrelationParameters()
+    cor = toml.get("correlation")
+    if cor is not None:
+        if "r_max" not in cor:
+            raise InputError("cannot find r_max in correlation")
+        if "operators" not in cor:
+            raise InputError("cannot find operators in correlation")
+        cp.r_max = int(cor["r_max"])
+        cp.operators = [(int(o[0]), int(o[1])) for o in cor["operators"]]
     real = p.is_real
     real = real and _is_real([e.op for e in su], tol) and _is_real([e.op for e in fu], tol)
     real = real and _is_real([o.op for o in one + two + multi], tol)
     if p.is_real and not real:
         raise InputError("TeNeS invoked in real tensor mode (parameter.general.is_real = true) "
                          "but some operators are complex.")
-    return Input(p, lat, su, fu, one, two, multi, tm, real)
+    return Input(p, lat, su, fu, one, two, multi, tm, real, cp)

@@ -9,8 +9,9 @@ density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
 of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 
 Out of scope (raises InputError): full update (num_step > 0 of
-[parameter.full_update]), finite-temperature mode, the mean-field environment;
-long-range correlation functions ([correlation]) are skipped with a warning.
+[parameter.full_update]), finite-temperature mode, the mean-field environment.
+Long-range correlation functions ([correlation]) are measured up to r = 3
+through window contractions, and skipped with a warning beyond that.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
 saveload.py.
 """
@@ -227,6 +228,81 @@ class ITPS:
         self._norm_warnings(list(norms.values()), strict=True)
         return ret
 
+    # ------------------------------------------- long-range correlations
+    # The strip of a correlation at distance r is a 1 x (r+1) (or (r+1) x 1)
+    # window; the window contraction's boundary tensor carries two legs of
+    # dimension D per column, so the strip is held to r <= 3 (the window
+    # limit) and to about 2 GB of boundary tensor.
+    MAX_CORRELATION_R = 3
+    MAX_CORRELATION_BYTES = 2 << 30
+
+    def _site_op_or_none(self, site: int, group: int):
+        for o in self.inp.onesite:
+            if o.source_site == site and o.group == group:
+                return self._op(o.op)
+        return None
+
+    def measure_correlation(self):
+        """measure_correlation_ctm (correlation_function.cpp:42-220): for every
+        site and every (left, right) one-site operator group pair of
+        [correlation], <O_left O_right> / <1> at horizontal and vertical
+        distances 1 .. r_max.  Each value is the window spanning the two sites
+        with the two operators at its ends, over the same window without
+        operators -- the network the reference's StartCorrelation / Transfer /
+        FinishCorrelation strip contracts.  Returns None (with a warning) when
+        the strips are beyond the window contraction's reach."""
+        cp = self.inp.corparam
+        nl = len(self.names1)
+        dmax = max(max(v) for v in self.inp.lattice.virtual_dims)
+        need = 16 * self.p.CHI ** 2 * dmax ** (2 * (cp.r_max + 1))
+        if cp.r_max > self.MAX_CORRELATION_R or need > self.MAX_CORRELATION_BYTES:
+            if self.print_level > 0:
+                print(f"WARNING: long-range correlations up to r_max = {cp.r_max} need strips beyond this "
+                      f"library's window contraction (r <= {self.MAX_CORRELATION_R}, "
+                      f"{self.MAX_CORRELATION_BYTES >> 30} GB); [correlation] skipped", file=sys.stderr)
+            return None
+        r_ops: List[List[int]] = [[] for _ in range(nl)]
+        for lop, rop in cp.operators:
+            if not (0 <= lop < nl and 0 <= rop < nl):
+                raise InputError(f"correlation operator index out of range: ({lop}, {rop})")
+            r_ops[lop].append(rop)
+        out = []
+        for left in range(self.N):
+            for lop in range(nl):
+                if not r_ops[lop]:
+                    continue
+                Ol = self._site_op_or_none(left, lop)
+                if Ol is None:
+                    continue
+                for horizontal in (True, False):
+                    site = left
+                    for r in range(1, cp.r_max + 1):
+                        site = self._other(site, 1, 0) if horizontal else self._other(site, 0, 1)
+                        if horizontal:
+                            geo, pl, pr, dx, dy = (1, r + 1, 0, 0), (0, 0), (0, r), r, 0
+                        else:
+                            geo, pl, pr, dx, dy = (r + 1, 1, r, 0), (r, 0), (0, 0), 0, r
+                        norm = self.env.contract_window(left, *geo)
+                        for rop in r_ops[lop]:
+                            Or = self._site_op_or_none(site, rop)
+                            if Or is None:
+                                continue
+                            v = self.env.contract_window(left, *geo, {pl: Ol, pr: Or}) / norm
+                            out.append((left, dx, dy, lop, rop, v))
+        return out
+
+    def save_correlation(self, cors, time, prefix):
+        """save_correlation (correlation_function.cpp:349-395)."""
+        cols = self._time_header(time) + ["left_op", "left_site", "right_op", "right_dx", "right_dy", "real",
+                                          "imag"]
+        hdr = self._cols(cols)
+        hdr.append("# The names of operators are the following: ")
+        hdr += [f"# {i}: {n}" for i, n in enumerate(self.names1)]
+        with self._open(prefix + "correlation.dat", hdr) as f:
+            for left, dx, dy, lop, rop, v in cors:
+                t = f"{_fmt(time)} " if time is not None else ""
+                f.write(f"{t}{lop} {left} {rop} {dx} {dy} {_fmt(v.real)} {_fmt(v.imag)} \n")
+
     def measure_transfer_matrix(self):
         """measure_transfer_matrix_eigenvalues (correlation_length.cpp:24-55)."""
         tp = self.inp.tm_params
@@ -407,6 +483,10 @@ class ITPS:
         multi = self.measure_multisite()
         if self.inp.multisite:
             self.save_multisite(multi, time, prefix)
+        if self.inp.corparam.r_max > 0:
+            cors = self.measure_correlation()
+            if cors is not None:
+                self.save_correlation(cors, time, prefix)
         if self.inp.tm_params.to_calculate:
             self.save_correlation_length(self.measure_transfer_matrix(), time, prefix)
         energy = self.save_density(vals, two, multi, time, prefix)

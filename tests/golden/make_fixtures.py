@@ -12,7 +12,7 @@ tree at run time:
   (known answer of core::Simple_update_bond, test/simple_update.cpp:28-160)
 * te_tfi_input.toml       <- test/data/TE_TFI.toml (expert input file)
 * te_tfi_expected.json    <- test/data/output_TE_TFI/TE_{density,onesite_obs,
-  twosite_obs,multisite_obs_4,correlation_length}.dat
+  twosite_obs,multisite_obs_4,correlation_length,correlation}.dat
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
 """
@@ -54,7 +54,8 @@ def main(ref):
     exp = {}
     for key, fname in (("density", "TE_density.dat"), ("onesite", "TE_onesite_obs.dat"),
                        ("twosite", "TE_twosite_obs.dat"), ("multisite", "TE_multisite_obs_4.dat"),
-                       ("correlation_length", "TE_correlation_length.dat")):
+                       ("correlation_length", "TE_correlation_length.dat"),
+                       ("correlation", "TE_correlation.dat")):
         exp[key] = _rows(os.path.join(out, fname))
     exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
     with open(os.path.join(HERE, "te_tfi_expected.json"), "w") as f:

@@ -136,7 +136,7 @@ def test_te_tfi_driver_on_oracle(tmp_path, monkeypatch):
     exp = expected()
     for name, key in [("TE_density.dat", "density"), ("TE_onesite_obs.dat", "onesite"),
                       ("TE_twosite_obs.dat", "twosite"), ("TE_multisite_obs_4.dat", "multisite"),
-                      ("TE_correlation_length.dat", "correlation_length")]:
+                      ("TE_correlation_length.dat", "correlation_length"), ("TE_correlation.dat", "correlation")]:
         res = _rows(tmp_path / name)
         ref = exp[key]
         assert len(res) == len(ref), name
