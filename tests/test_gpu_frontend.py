@@ -39,7 +39,8 @@ def te_tfi_run(tmp_path_factory):
 @pytest.mark.parametrize("name,key", [("TE_density.dat", "density"), ("TE_onesite_obs.dat", "onesite"),
                                       ("TE_twosite_obs.dat", "twosite"),
                                       ("TE_multisite_obs_4.dat", "multisite"),
-                                      ("TE_correlation_length.dat", "correlation_length")])
+                                      ("TE_correlation_length.dat", "correlation_length"),
+                                      ("TE_correlation.dat", "correlation")])
 def test_te_tfi_outputs(te_tfi_run, name, key):
     exp = expected()
     tol = exp["tolerance"]
