@@ -15,6 +15,9 @@ are the ones mptensor's ``tensordot`` / ``transpose`` use.
 
 Parity pins (checked in ``tests/test_oracle_golden.py``):
   * ``test/data/simple_update.dat`` (known-answer test of the bond step).
+  * ``test/data/full_update.dat`` (known-answer test of the full-update bond
+    step) and ``test/data/output_AntiferroHeisenberg_real/*`` (simple update,
+    one full-update step, CTMRG, observables).
   * ``test/data/output_TE_TFI/*`` (simple update + CTMRG + one-site, two-site
     and multisite observables, complex tensors, chi = 10).
 The randomized SVD of mptensor (``rsvd``) is not part of the reference tree;
@@ -211,6 +214,12 @@ class Params:
     rsvd_power_iters: int = 2
     rsvd_oversample_abs: Optional[int] = None
     rsvd_seed: int = 0
+    # full update (PEPS_Parameters.cpp:57-62)
+    Inverse_Env_cut: float = 1e-12
+    Full_Inverse_precision: float = 1e-12
+    Full_Convergence_Epsilon: float = 1e-6
+    Full_max_iteration: int = 100
+    Full_Gauge_Fix: bool = True
 
 
 def initialize_tensors(lat: Lattice, seed: int, is_real: bool) -> List[np.ndarray]:
@@ -712,6 +721,217 @@ def calc_ctm_environment(Tn, p: Params, lat: Lattice, env: Optional[Env] = None,
         if on_sweep is not None:
             on_sweep(count, env)
     return env, count, conv, sig_max
+
+
+# ---------------------------------------------------------------------------
+# Full update (src/iTPS/core/full_update.cpp:31-455).  mptensor's matrix
+# factorisations of a tensor over (row legs | column legs) are restated as
+# numpy's on the reshaped matrix: qr -> Q (rows..., k), R (k, cols...);
+# svd -> U (rows..., k), s, VT (k, cols...); eigh -> ascending w,
+# Z (rows..., k); all thin, k = min(rows, cols).
+# ---------------------------------------------------------------------------
+
+
+def _split(A, rows, cols):
+    A = np.transpose(A, list(rows) + list(cols))
+    rs = A.shape[:len(rows)]
+    cs = A.shape[len(rows):]
+    return A.reshape(int(np.prod(rs)), int(np.prod(cs))), rs, cs
+
+
+def _qr_legs(A, rows, cols):
+    M, rs, cs = _split(A, rows, cols)
+    Q, R = np.linalg.qr(M)
+    return Q.reshape(rs + (-1,)), R.reshape((-1,) + cs)
+
+
+def _svd_legs(A, rows, cols):
+    M, rs, cs = _split(A, rows, cols)
+    U, s, VT = np.linalg.svd(M, full_matrices=False)
+    return U.reshape(rs + (-1,)), s, VT.reshape((-1,) + cs)
+
+
+def _eigh_legs(A, rows, cols):
+    M, rs, cs = _split(A, rows, cols)
+    w, Z = np.linalg.eigh(M)
+    return w, Z.reshape(rs + (-1,))
+
+
+def _mulvec(A, v, leg):
+    sh = [1] * A.ndim
+    sh[leg] = -1
+    return A * np.asarray(v).reshape(sh)
+
+
+def _trace(A, B, a, b):
+    return td(A, B, (list(a), list(b)))
+
+
+def create_environment_two_sites(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, Q1, Q2):
+    """Create_Environment_two_sites (core/full_update.cpp:50-83): the bond
+    environment of two double-layer halves, legs (t1, t2, tc1, tc2)."""
+    right = td(td(C2, eT2, ([0], [1])),
+               td(td(td(td(C3, eT4, ([1], [0])), eT3, ([0], [1])), cj(Q2), ([2, 5], [3, 2])), Q2,
+                  ([1, 3], [3, 2])),
+               ([0, 2, 3], [1, 5, 3]))
+    left = td(td(C1, eT1, ([1], [0])),
+              td(td(td(td(C4, eT6, ([1], [0])), eT5, ([0], [1])), cj(Q1), ([2, 5], [0, 2])), Q1,
+                 ([1, 3], [0, 2])),
+              ([0, 2, 3], [0, 4, 2]))
+    return td(right, left, ([0, 1], [0, 1])).transpose(3, 1, 2, 0)
+
+
+def _pinv_t(A, cut):
+    """conj(u s^-1) conj(vt) of A = u s vt, values below cut * s_0 dropped
+    (the pseudo-inverse, transposed, of core/full_update.cpp:158-184)."""
+    u, s, vt = np.linalg.svd(A, full_matrices=False)
+    sinv = np.array([1.0 / x if x / s[0] > cut else 0.0 for x in s])
+    return td(cj(u * sinv[None, :]), cj(vt), ([1], [0]))
+
+
+def _fu_delta(E, Theta, R1, R2):
+    """-2 <R1 R2|E|Theta> + <R1 R2|E|R1 R2> (core/full_update.cpp:238-254)."""
+    ET = td(E, Theta, ([0, 1], [0, 1]))
+    a = _trace(td(ET, cj(R2), ([1, 3], [0, 2])), cj(R1), (0, 1, 2), (0, 2, 1))
+    b = _trace(R1, td(R2, td(E, td(cj(R1), cj(R2), ([1], [1])), ([2, 3], [0, 2])), ([0, 2], [1, 3])),
+               (0, 1, 2), (1, 0, 2))
+    return -2.0 * a + b
+
+
+def _fu_solve(N_mat, W_vec, prec):
+    """R = pinv(N) W (core/full_update.cpp:276-296, 311-329)."""
+    U, s, VT = _svd_legs(N_mat, (1, 3), (0, 2))
+    sinv = np.array([1.0 / x if x / s[0] > prec else 0.0 for x in s])
+    N_inv = td(cj(_mulvec(U, sinv, 2)), cj(VT), ([2], [0]))
+    return td(N_inv, W_vec, ([0, 1], [0, 2]))
+
+
+def full_update_bond_horizontal(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, Tn1, Tn2, op12, p: Params):
+    """Full_update_bond_horizontal (core/full_update.cpp:85-389): returns
+    (Tn1_new, Tn2_new, iterations, converged)."""
+    D_connect = Tn1.shape[2]
+    Q1, R1 = _qr_legs(Tn1, (0, 1, 3), (2, 4))
+    Q2, R2 = _qr_legs(Tn2, (1, 2, 3), (0, 4))
+    envR1, envR2 = R1.shape[0], R2.shape[0]
+    Theta = td(td(R1, R2, ([1], [1])), op12, ([1, 3], [0, 1]))
+    E = create_environment_two_sites(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, Q1, Q2.transpose(3, 0, 1, 2))
+    E = 0.5 * (E + cj(E.transpose(2, 3, 0, 1)))
+    w, Z = _eigh_legs(E, (0, 1), (2, 3))
+    w_max = abs(w[envR1 * envR2 - 1])
+    w = np.array([math.sqrt(x) if x / w_max > p.Inverse_Env_cut else 0.0 for x in w])
+    Z = _mulvec(Z, w, 2)
+    if p.Full_Gauge_Fix:
+        _, LR1 = _qr_legs(Z, (2, 1), (0,))
+        _, LR2 = _qr_legs(Z, (2, 0), (1,))
+        Theta = td(LR1, td(LR2, Theta, ([1], [1])), ([1], [1]))
+        LR1_inv = _pinv_t(LR1, p.Inverse_Env_cut)
+        LR2_inv = _pinv_t(LR2, p.Inverse_Env_cut)
+        Z = td(td(Z, LR1_inv, ([0], [1])), LR2_inv, ([0], [1]))
+        E = td(Z, cj(Z), ([0], [0]))
+    else:
+        E = td(Z, cj(Z), ([2], [2]))
+    # initial guess from the SVD of Theta, truncated to D_connect
+    U, s, VT = _svd_legs(Theta, (0, 2), (1, 3))
+    lam = np.zeros(D_connect)
+    lam[:min(D_connect, len(s))] = s[:D_connect]
+    U = U[:, :, :D_connect]
+    VT = VT[:D_connect]
+    lam = np.sqrt(lam / math.sqrt(float(np.sum(lam * lam))))
+    U = _mulvec(U, lam[:U.shape[2]], 2)
+    VT = _mulvec(VT, lam[:VT.shape[0]], 0)
+    R1 = U.transpose(0, 2, 1)
+    R2 = VT.transpose(1, 0, 2)
+    C_phi = _trace(td(E, Theta, ([0, 1], [0, 1])), cj(Theta), (0, 1, 2, 3), (0, 1, 2, 3))
+    old = _fu_delta(E, Theta, R1, R2)
+    count, conv = 0, False
+    while not conv and count < p.Full_max_iteration:
+        W = td(td(E, Theta, ([0, 1], [0, 1])), cj(R2), ([1, 3], [0, 2]))
+        N = td(td(E, R2, ([1], [0])), cj(R2), ([2, 4], [0, 2]))
+        R1 = _fu_solve(N, W, p.Full_Inverse_precision)
+        W = td(td(E, Theta, ([0, 1], [0, 1])), cj(R1), ([0, 2], [0, 2]))
+        N = td(td(E, R1, ([0], [0])), cj(R1), ([1, 4], [0, 2]))
+        R2 = _fu_solve(N, W, p.Full_Inverse_precision)
+        delta = _fu_delta(E, Theta, R1, R2)
+        if abs(old - delta) / abs(C_phi) < p.Full_Convergence_Epsilon:
+            conv = True
+        old = delta
+        count += 1
+    if p.Full_Gauge_Fix:
+        R1 = td(LR1_inv, R1, ([0], [0]))
+        R2 = td(LR2_inv, R2, ([0], [0]))
+    # balancing and normalisation
+    q1, r1 = _qr_legs(R1, (0, 2), (1,))
+    q2, r2 = _qr_legs(R2, (0, 2), (1,))
+    U, s, VT = np.linalg.svd(td(r1, r2, ([1], [1])), full_matrices=False)
+    n = math.sqrt(float(np.sum(s[:D_connect] ** 2)))
+    s = s.copy()
+    s[:D_connect] = np.sqrt(s[:D_connect] / n)
+    U = U * s[None, :]
+    VT = VT * s[:, None]
+    R1 = td(q1, U, ([2], [0]))
+    R2 = td(q2, VT, ([2], [1]))
+    Tn1_new = td(Q1, R1, ([3], [0])).transpose(0, 1, 4, 2, 3)
+    Tn2_new = td(Q2, R2, ([3], [0])).transpose(4, 0, 1, 2, 3)
+    return Tn1_new, Tn2_new, count, conv
+
+
+_FU_ROT = {0: (2, 3, 0, 1, 4), 1: (3, 0, 1, 2, 4), 2: (0, 1, 2, 3, 4), 3: (1, 2, 3, 0, 4)}
+_FU_BACK = {0: (2, 3, 0, 1, 4), 1: (1, 2, 3, 0, 4), 2: (0, 1, 2, 3, 4), 3: (3, 0, 1, 2, 4)}
+
+
+def full_update_bond(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, Tn1, Tn2, op12, connect1: int, p: Params):
+    """Full_update_bond (core/full_update.cpp:391-455): the bond on leg
+    connect1 of Tn1 rotated onto the horizontal case and back."""
+    r = _FU_ROT[connect1]
+    a, b, _, _ = full_update_bond_horizontal(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6,
+                                             Tn1.transpose(r), Tn2.transpose(r), op12, p)
+    k = _FU_BACK[connect1]
+    return a.transpose(k), b.transpose(k)
+
+
+def full_update_op(env: "Env", Tn, source: int, leg: int, op, p: Params, lat: "Lattice",
+                   fast: bool = True) -> None:
+    """iTPS::full_update(up) (src/iTPS/full_update.cpp:30-149): the bond
+    (source, leg) updated with the environment tensors that face it, then the
+    fast full update's single moves through the two columns (rows) of the bond
+    (or a full CTMRG when ``fast`` is False).  Tn and env are updated in place.
+    A one-site operator (leg < 0) is applied as tensordot(Tn, op, 4, 0)."""
+    if leg < 0:
+        Tn[source] = td(Tn[source], op, ([4], [0]))
+        return
+    tgt = lat.neighbor(source, leg)
+    e = env
+    if leg == 0:
+        args = (e.C4[source], e.C2[tgt], e.C1[tgt], e.C3[source], e.eTb[source], e.eTb[tgt], e.eTl[tgt],
+                e.eTt[tgt], e.eTt[source], e.eTr[source])
+    elif leg == 1:
+        args = (e.C4[source], e.C1[tgt], e.C2[tgt], e.C3[source], e.eTl[source], e.eTl[tgt], e.eTt[tgt],
+                e.eTr[tgt], e.eTr[source], e.eTb[source])
+    elif leg == 2:
+        args = (e.C1[source], e.C2[tgt], e.C3[tgt], e.C4[source], e.eTt[source], e.eTt[tgt], e.eTr[tgt],
+                e.eTb[tgt], e.eTb[source], e.eTl[source])
+    else:
+        args = (e.C2[source], e.C3[tgt], e.C4[tgt], e.C1[source], e.eTr[source], e.eTr[tgt], e.eTb[tgt],
+                e.eTl[tgt], e.eTl[source], e.eTt[source])
+    Tn[source], Tn[tgt] = full_update_bond(*args, Tn[source], Tn[tgt], op, leg, p)
+    if not fast:
+        new, _, _, _ = calc_ctm_environment(Tn, p, lat)
+        for name in ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl"):
+            setattr(env, name, getattr(new, name))
+        return
+    LX = lat.LX
+    if leg == 0:
+        right_move(env, Tn, source % LX, p, lat)
+        left_move(env, Tn, tgt % LX, p, lat)
+    elif leg == 1:
+        bottom_move(env, Tn, source // LX, p, lat)
+        top_move(env, Tn, tgt // LX, p, lat)
+    elif leg == 2:
+        left_move(env, Tn, source % LX, p, lat)
+        right_move(env, Tn, tgt % LX, p, lat)
+    else:
+        top_move(env, Tn, source // LX, p, lat)
+        bottom_move(env, Tn, tgt // LX, p, lat)
 
 
 # ---------------------------------------------------------------------------

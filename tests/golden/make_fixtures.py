@@ -10,9 +10,14 @@ tree at run time:
 
 * simple_update_kat.json  <- test/data/simple_update.dat
   (known answer of core::Simple_update_bond, test/simple_update.cpp:28-160)
+* full_update_kat.json    <- test/data/full_update.dat
+  (known answer of core::Full_update_bond, test/full_update.cpp:28-140)
 * te_tfi_input.toml       <- test/data/TE_TFI.toml (expert input file)
 * te_tfi_expected.json    <- test/data/output_TE_TFI/TE_{density,onesite_obs,
   twosite_obs,multisite_obs_4,correlation_length,correlation}.dat
+* afh_real_input.toml / afh_real_expected.json <- test/data/AntiferroHeisenberg_real.toml and
+  output_AntiferroHeisenberg_real/{density,onesite_obs,twosite_obs,multisite_obs_4,correlation,
+  correlation_length}.dat (simple update + one full-update step + CTMRG)
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
 """
@@ -49,6 +54,12 @@ def main(ref):
     with open(os.path.join(HERE, "simple_update_kat.json"), "w") as f:
         json.dump(kat, f, indent=1)
 
+    vals = [float(x) for x in open(os.path.join(data, "full_update.dat")).read().split()]
+    fu = {"T1": vals[:n], "T2": vals[n:2 * n], "D": 2, "ldof": 2, "chi": 4, "connect": 2, "tol": 1e-8,
+          "source": "test/data/full_update.dat; inputs test/full_update.cpp:36-88"}
+    with open(os.path.join(HERE, "full_update_kat.json"), "w") as f:
+        json.dump(fu, f, indent=1)
+
     shutil.copyfile(os.path.join(data, "TE_TFI.toml"), os.path.join(HERE, "te_tfi_input.toml"))
     out = os.path.join(data, "output_TE_TFI")
     exp = {}
@@ -59,6 +70,24 @@ def main(ref):
         exp[key] = _rows(os.path.join(out, fname))
     exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
     with open(os.path.join(HERE, "te_tfi_expected.json"), "w") as f:
+        json.dump(exp, f)
+
+    # ground state with one full-update step (test/data/AntiferroHeisenberg_real.toml)
+    shutil.copyfile(os.path.join(data, "AntiferroHeisenberg_real.toml"), os.path.join(HERE, "afh_real_input.toml"))
+    out = os.path.join(data, "output_AntiferroHeisenberg_real")
+    exp = {}
+    dens = {}
+    for line in open(os.path.join(out, "density.dat")):
+        if "=" in line:
+            name, vals = line.split("=")
+            dens[name.strip()] = [float(x) for x in vals.split()]
+    exp["density"] = dens
+    for key, fname in (("onesite", "onesite_obs.dat"), ("twosite", "twosite_obs.dat"),
+                       ("multisite", "multisite_obs_4.dat"), ("correlation", "correlation.dat"),
+                       ("correlation_length", "correlation_length.dat")):
+        exp[key] = _rows(os.path.join(out, fname))
+    exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
+    with open(os.path.join(HERE, "afh_real_expected.json"), "w") as f:
         json.dump(exp, f)
 
     with tempfile.TemporaryDirectory() as td:

@@ -3,6 +3,8 @@
 * mt19937 draws from the C++ standard library (oracle/mt19937_draws.cpp).
 * test/data/simple_update.dat: known answer of Simple_update_bond
   (test/simple_update.cpp:28-160, tol 1e-8 with the per-fibre sign gauge).
+* test/data/full_update.dat: known answer of Full_update_bond
+  (test/full_update.cpp:28-140, tol 1e-8 with the per-index sign gauge).
 * test/data/output_TE_TFI: simple update + CTMRG + observables + correlation
   length.  The reference test compares at rtol 1e-3 / atol 1e-4
   (test/fulltest.py.in:141-142); the restatement reproduces it to 1e-10.
@@ -46,6 +48,34 @@ def test_simple_update_known_answer():
                     sign = 1 if a * r > 0 else -1
                 assert r * sign == pytest.approx(a, rel=tol, abs=1e-14)
     np.testing.assert_allclose(lc, kat["lambda"], rtol=tol)
+
+
+def test_full_update_known_answer():
+    """test/full_update.cpp:28-140: all-ones tensors and environment (the
+    corners non-zero on their D x D block only), op12 = delta_{iiii},
+    horizontal bond; the reference's check fixes one sign per physical index
+    and tensor from the first non-zero entry."""
+    kat = json.load(open(os.path.join(GOLDEN, "full_update_kat.json")))
+    D, d, chi = kat["D"], kat["ldof"], kat["chi"]
+    T = np.ones((D, D, D, D, d))
+    C = []
+    for _ in range(4):
+        c = np.zeros((chi, chi))
+        c[:D, :D] = 1.0
+        C.append(c)
+    E = [np.ones((chi, chi, D, D)) for _ in range(6)]
+    op = np.zeros((d, d, d, d))
+    for i in range(d):
+        op[i, i, i, i] = 1.0
+    T1, T2 = O.full_update_bond(*C, *E, T, T.copy(), op, kat["connect"], O.Params())
+    for new, ans in ((T1, kat["T1"]), (T2, kat["T2"])):
+        ans = np.array(ans).reshape(D, D, D, D, d)
+        sign = np.zeros(d)
+        for idx in np.ndindex(new.shape):
+            m = idx[4]
+            if sign[m] == 0 and new[idx] != 0.0:
+                sign[m] = 1 if ans[idx] * new[idx] > 0 else -1
+            assert new[idx] * sign[m] == pytest.approx(ans[idx], rel=kat["tol"], abs=1e-14)
 
 
 def _match(t, rows, key_fn, val_fn, tol=1e-10):
@@ -102,3 +132,50 @@ def test_te_tfi_golden():
         t += inp.params.tau_simple_step[0]
         if step % inp.params.measure_interval[0] == 0:
             measure(t)
+
+
+def test_full_update_pipeline_golden():
+    """test/data/AntiferroHeisenberg_real: 100 simple-update steps, one
+    full-update step (fast full update: single moves after every bond,
+    src/iTPS/full_update.cpp:30-186, preceded by a full CTMRG), then CTMRG
+    and the observables (onesite_obs, twosite_obs, multisite_obs_4 and the
+    energy of density.dat).  The reference checks at rtol 1e-3 / atol 1e-4."""
+    with open(os.path.join(GOLDEN, "afh_real_expected.json")) as f:
+        exp = json.load(f)
+    inp, lat, p, one, two, multi = oracle_setup(os.path.join(GOLDEN, "afh_real_input.toml"))
+    Tn = O.initialize_tensors(lat, inp.params.seed, inp.is_real)
+    lam = [[np.ones(lat.virtual_dims[i][l]) for l in range(4)] for i in range(lat.N_UNIT)]
+    for _ in range(inp.params.num_simple_step[0]):
+        su_step(inp, lat, p, Tn, lam)
+    env, _, _, _ = O.calc_ctm_environment(Tn, p, lat)
+    for _ in range(inp.params.num_full_step[0]):
+        for up in inp.full_updates:
+            if up.group == 0:
+                O.full_update_op(env, Tn, up.source_site, -1 if up.is_onesite() else up.source_leg, up.op, p, lat)
+    env, _, _, _ = O.calc_ctm_environment(Tn, p, lat)
+    n1 = max(o.group for o in one) + 1
+    n2 = max(o.group for o in two) + 1
+    n3 = max(o.group for o in multi) + 1
+    v1, norm = O.measure_onesite(env, Tn, lat, one, n1)
+    v2, _ = O.measure_twosite(env, Tn, lat, two, one, n2)
+    v3 = O.measure_multisite(env, Tn, lat, multi, one, n3)
+    tol = 1e-11  # observed <= 1.4e-14
+    n = 0
+    for r in exp["onesite"]:
+        v = norm[int(r[1])] if int(r[0]) == -1 else v1[int(r[0])][int(r[1])]
+        assert abs(v.real - r[2]) <= tol * max(1.0, abs(r[2])), (r, v)
+        n += 1
+    for r in exp["twosite"]:
+        if int(r[0]) < 0:
+            continue
+        v = v2[int(r[0])][(int(r[1]), int(r[2]), int(r[3]))]
+        assert abs(v.real - r[4]) <= tol * max(1.0, abs(r[4])), (r, v)
+        n += 1
+    for r in exp["multisite"]:
+        v = v3[int(r[0])][(int(r[1]), (int(r[2]), int(r[4]), int(r[6])), (int(r[3]), int(r[5]), int(r[7])))]
+        assert abs(v.real - r[8]) <= tol * max(1.0, abs(r[8])), (r, v)
+        n += 1
+    assert n > 40
+    bond = [o.group for o in two if o.name == "bond_hamiltonian"]
+    E = sum(sum(v2[g].values()).real for g in set(bond)) / lat.N_UNIT
+    assert abs(E - exp["density"]["Energy"][0]) <= tol
