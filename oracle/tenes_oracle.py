@@ -900,6 +900,15 @@ def full_update_op(env: "Env", Tn, source: int, leg: int, op, p: Params, lat: "L
         Tn[source] = td(Tn[source], op, ([4], [0]))
         return
     tgt = lat.neighbor(source, leg)
+    args = full_update_env_args(env, source, leg, lat)
+    Tn[source], Tn[tgt] = full_update_bond(*args, Tn[source], Tn[tgt], op, leg, p)
+    _full_update_moves(env, Tn, source, tgt, leg, p, lat, fast)
+
+
+def full_update_env_args(env: "Env", source: int, leg: int, lat: "Lattice"):
+    """The ten environment tensors facing the bond (source, leg), in the
+    argument order of Full_update_bond (src/iTPS/full_update.cpp:42-116)."""
+    tgt = lat.neighbor(source, leg)
     e = env
     if leg == 0:
         args = (e.C4[source], e.C2[tgt], e.C1[tgt], e.C3[source], e.eTb[source], e.eTb[tgt], e.eTl[tgt],
@@ -913,7 +922,11 @@ def full_update_op(env: "Env", Tn, source: int, leg: int, op, p: Params, lat: "L
     else:
         args = (e.C2[source], e.C3[tgt], e.C4[tgt], e.C1[source], e.eTr[source], e.eTr[tgt], e.eTb[tgt],
                 e.eTl[tgt], e.eTl[source], e.eTt[source])
-    Tn[source], Tn[tgt] = full_update_bond(*args, Tn[source], Tn[tgt], op, leg, p)
+    return args
+
+
+def _full_update_moves(env, Tn, source, tgt, leg, p, lat, fast):
+    """The fast full update's single moves (src/iTPS/full_update.cpp:122-148)."""
     if not fast:
         new, _, _, _ = calc_ctm_environment(Tn, p, lat)
         for name in ("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl"):

@@ -148,7 +148,8 @@ def host_adjoint(tmp_path_factory):
     from tenes_b200.build import cuda_home
     out = str(tmp_path_factory.mktemp("adhost") / "ad_host_check")
     subprocess.check_call([gxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
-                           "-I", os.path.join(ROOT, "tenes_b200", "csrc"), "-I", os.path.join(cuda_home(), "include"),
+                           "-I", os.path.join(ROOT, "tenes_b200", "csrc"), "-I", os.path.join(ROOT, "tests"),
+                           "-I", os.path.join(cuda_home(), "include"),
                            os.path.join(ROOT, "tests", "ad_host_check.cpp"), "-o", out])
     return out
 
