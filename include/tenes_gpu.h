@@ -173,6 +173,30 @@ tg_status tg_tm_eigenvalues(tg_ctx* ctx, int dir, int fixed, int num_eigvals, in
 tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op);
 tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op);
 
+/* Full update of one bond (PEPS_Parameters full-update knobs,
+ * src/iTPS/PEPS_Parameters.cpp:57-62; keys of [parameter.full_update] in
+ * src/iTPS/load_toml.cpp:374-379). */
+typedef struct tg_fu_params {
+  double inverse_env_cut;     /* full_update.env_cutoff (1e-12) */
+  double inverse_precision;   /* full_update.inverse_precision (1e-12) */
+  double convergence_epsilon; /* full_update.convergence_epsilon (1e-6) */
+  int max_iteration;          /* full_update.iteration_max (100) */
+  int gauge_fix;              /* full_update.gauge_fix (1) */
+} tg_fu_params;
+
+/* Fill *p with the reference defaults. */
+void tg_fu_params_default(tg_fu_params* p);
+
+/* core::Full_update_bond (src/iTPS/core/full_update.cpp:31-455) of the bond
+ * between `source` and its neighbour on `source_leg`, in the current
+ * environment (the tensors that face the bond, src/iTPS/full_update.cpp:42-116);
+ * op is (d1, d2, d1, d2).  Replaces the two site tensors and leaves the
+ * environment alone: the fast full update follows with tg_ctm_move on the
+ * two lines of the bond (full_update.cpp:122-148).  *iterations and
+ * *converged (optional) report the least-squares loop.  Real tensors. */
+tg_status tg_fu_bond(tg_ctx* ctx, int source, int source_leg, const double* op, const tg_fu_params* params,
+                     int* iterations, int* converged);
+
 /* iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137): per site,
  * Tn[0,0,0,0,:] = initial state (random when all entries are zero) and every
  * other entry noise * U(-1,1) from std::mt19937(seed) (real part) and

@@ -28,7 +28,7 @@ EXPORTED = [
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
-    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm",
+    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond",
 ]
 
 
@@ -48,6 +48,12 @@ class WindowTerm(C.Structure):
     _fields_ = [("source", C.c_int), ("nrow", C.c_int), ("ncol", C.c_int), ("source_row", C.c_int),
                 ("source_col", C.c_int), ("nops", C.c_int), ("op_row", C.POINTER(C.c_int)),
                 ("op_col", C.POINTER(C.c_int)), ("ops", C.POINTER(C.c_double)), ("coeff", C.c_double)]
+
+
+class FuParams(C.Structure):
+    """tg_fu_params: full-update knobs."""
+    _fields_ = [("inverse_env_cut", C.c_double), ("inverse_precision", C.c_double),
+                ("convergence_epsilon", C.c_double), ("max_iteration", C.c_int), ("gauge_fix", C.c_int)]
 
 
 class Params(C.Structure):
@@ -100,6 +106,8 @@ def load() -> C.CDLL:
         "tg_tm_eigenvalues": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_double, dp, P(C.c_int)]),
         "tg_su_bond": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+        "tg_fu_params_default": (None, [P(FuParams)]),
+        "tg_fu_bond": (C.c_int, [vp, C.c_int, C.c_int, dp, P(FuParams), P(C.c_int), P(C.c_int)]),
         "tg_init_tensors": (C.c_int, [vp, C.c_int, dp, P(C.c_int), dp]),
         "tg_sync": (C.c_int, [vp]),
         "tg_kernel_launch_count": (C.c_uint64, []),

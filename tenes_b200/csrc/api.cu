@@ -230,6 +230,22 @@ tg_status tg_energy_grad(tg_ctx* ctx, int nterms, const tg_window_term* terms, i
     E(ctx)->energy_grad(nterms, terms, iterations, checkpoint_every, svd_broadening, energy, grad);
   });
 }
+void tg_fu_params_default(tg_fu_params* p) {
+  if (!p) return;
+  p->inverse_env_cut = 1e-12;
+  p->inverse_precision = 1e-12;
+  p->convergence_epsilon = 1e-6;
+  p->max_iteration = 100;
+  p->gauge_fix = 1;
+}
+tg_status tg_fu_bond(tg_ctx* ctx, int source, int source_leg, const double* op, const tg_fu_params* params,
+                     int* iterations, int* converged) {
+  return guard([&] {
+    need(op, "op");
+    need(params, "params");
+    E(ctx)->fu_bond(source, source_leg, op, params, iterations, converged);
+  });
+}
 tg_status tg_sync(tg_ctx* ctx) {
   return guard([&] { E(ctx)->sync(); });
 }

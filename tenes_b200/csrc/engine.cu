@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "adjoint_device.hpp"
+#include "full_update.hpp"
 #include "dtensor.hpp"
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -2009,6 +2010,134 @@ struct EngineT final : Engine {
       upload(Tn[i], reinterpret_cast<const double*>(h.data()));
       rot_ok[i] = false;
       for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+    }
+  }
+
+  // ------------------------------------------------------- full update
+  // Eigendecomposition of a real symmetric row-major n x n matrix (cuSOLVER
+  // syevd): ascending w on the host, Z (n x n, column j the eigenvector of
+  // w_j).  A symmetric matrix reads the same in either storage order; the
+  // column-major eigenvectors read row-major are Z^T.
+  void eigh(const DT<T>& A, int64_t n, std::vector<double>& w, DT<T>& Z) {
+    if constexpr (CPLX) {
+      fail(TG_E_RUNTIME, "eigh: real matrices only");
+    } else {
+      DT<T> a = clone(A, st);
+      DT<double> wd({n}, st);
+      const int in = static_cast<int>(n);
+      int lwork = 0;
+      ProfScope ps(PK_SOLVER, st, 9.0 * static_cast<double>(n) * n * n, 0.0);
+      check_sol(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in,
+                                            wd.p, &lwork),
+                "Dsyevd_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
+      check_sol(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in, wd.p, work.p,
+                                 lwork, info_slot()),
+                "Dsyevd");
+      Z = tr(reshape(a, {n, n}), {1, 0});
+      w.resize(static_cast<size_t>(n));
+      TG_CUDA(cudaMemcpyAsync(w.data(), wd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+
+  // Backend of full_update.hpp on this engine's device tensors: products and
+  // permutations through td / tr, QR and SVD through cuSOLVER (qr, svd),
+  // leg scaling through scale_leg, slicing as a product with a 0/1 matrix.
+  struct FuBackend {
+    using Ten = DT<T>;
+    EngineT* e;
+    static const Shape& shape(const Ten& t) { return t.sh; }
+    Ten td(const Ten& a, const Ten& b, const V& x, const V& y, int) { return e->td(a, b, x, y); }
+    Ten tr(const Ten& a, const V& q) { return e->tr(a, q); }
+    Ten reshape(const Ten& a, const Shape& s) { return tg::reshape(a, s); }
+    void axpy(Ten& y, const Ten& x, double alpha) { tg::axpy<T>(y.p, x.p, alpha, y.size(), e->st); }
+    void scale(Ten& x, double alpha) { tg::scale<T>(x.p, x.size(), alpha, e->st); }
+    double scalar(const Ten& t) {
+      const T v = e->scalar(t);
+      if constexpr (CPLX) return v.x;
+      else return v;
+    }
+    void qr_matrix(const Ten& M, Ten& Q, Ten& R) { e->qr(M, M.dim(0), M.dim(1), Q, R); }
+    void svd_matrix(const Ten& M, Ten& U, std::vector<double>& s, Ten& VT) {
+      Ten A = clone(M, e->st);
+      DT<double> sd;
+      e->svd(A, M.dim(0), M.dim(1), U, sd, VT);
+      s.resize(static_cast<size_t>(sd.size()));
+      TG_CUDA(cudaMemcpyAsync(s.data(), sd.p, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, e->st));
+      TG_CUDA(cudaStreamSynchronize(e->st));
+    }
+    void eigh_matrix(const Ten& M, std::vector<double>& w, Ten& Z) { e->eigh(M, M.dim(0), w, Z); }
+    Ten mulvec(const Ten& A, const std::vector<double>& v, int leg) {
+      Ten o = clone(A, e->st);
+      e->mulvec(o, leg, v);
+      return o;
+    }
+    Ten slice(const Ten& A, int leg, int64_t n) {
+      const int64_t dim = A.dim(leg);
+      if (n == dim) return A;
+      std::vector<double> h(static_cast<size_t>(n * dim * NW), 0.0);
+      for (int64_t i = 0; i < n; ++i) h[static_cast<size_t>((i * dim + i) * NW)] = 1.0;
+      const Ten S = e->from_host({n, dim}, h.data());
+      const Ten B = e->td(A, S, {leg}, {1});  // A's other legs, then the n kept entries
+      V perm;
+      const int r = A.rank();
+      for (int i = 0; i < r; ++i) perm.push_back(i < leg ? i : (i == leg ? r - 1 : i - 1));
+      return e->tr(B, perm);
+    }
+  };
+
+  // core::Full_update_bond for the bond (source, leg) with the environment
+  // tensors that face it (src/iTPS/full_update.cpp:42-116); the site tensors
+  // are replaced, the environment is left to the caller's moves
+  void fu_bond(int source, int leg, const double* op, const tg_fu_params* fp, int* iterations,
+               int* converged) override {
+    if constexpr (CPLX) {
+      fail(TG_E_INPUT, "full update: real site tensors only");
+    } else {
+      require_env();
+      check_site(source);
+      if (leg < 0 || leg > 3) fail(TG_E_INPUT, "source_leg must be 0..3");
+      const int t = lat.neighbor(source, leg);
+      auto &C1 = C[0], &C2 = C[1], &C3 = C[2], &C4 = C[3];
+      auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
+      const int s = source;
+      const DT<T>* a[10];
+      if (leg == 0) {
+        const DT<T>* x[10] = {&C4[s], &C2[t], &C1[t], &C3[s], &eTb[s], &eTb[t], &eTl[t], &eTt[t], &eTt[s], &eTr[s]};
+        std::copy(x, x + 10, a);
+      } else if (leg == 1) {
+        const DT<T>* x[10] = {&C4[s], &C1[t], &C2[t], &C3[s], &eTl[s], &eTl[t], &eTt[t], &eTr[t], &eTr[s], &eTb[s]};
+        std::copy(x, x + 10, a);
+      } else if (leg == 2) {
+        const DT<T>* x[10] = {&C1[s], &C2[t], &C3[t], &C4[s], &eTt[s], &eTt[t], &eTr[t], &eTb[t], &eTb[s], &eTl[s]};
+        std::copy(x, x + 10, a);
+      } else {
+        const DT<T>* x[10] = {&C2[s], &C3[t], &C4[t], &C1[s], &eTr[s], &eTr[t], &eTb[t], &eTl[t], &eTl[s], &eTt[s]};
+        std::copy(x, x + 10, a);
+      }
+      const int64_t d1 = lat.pdim[s], d2 = lat.pdim[t];
+      const DT<T> op12 = from_host({d1, d2, d1, d2}, op);
+      PrecScope prec(this, 0);
+      FuBackend bk{this};
+      fu::Params p;
+      p.inverse_env_cut = fp->inverse_env_cut;
+      p.inverse_precision = fp->inverse_precision;
+      p.convergence_epsilon = fp->convergence_epsilon;
+      p.max_iteration = fp->max_iteration;
+      p.gauge_fix = fp->gauge_fix != 0;
+      fu::FullUpdate<FuBackend> f{bk, p};
+      DT<T> n1, n2;
+      const fu::Stats st_ = f.bond(*a[0], *a[1], *a[2], *a[3], *a[4], *a[5], *a[6], *a[7], *a[8], *a[9], Tn[s], Tn[t],
+                                   op12, leg, n1, n2);
+      if (n1.sh != Tn[s].sh || n2.sh != Tn[t].sh)
+        fail(TG_E_RUNTIME, "full update: the updated bond lost rank (site tensor shape changed)");
+      Tn[s] = n1;
+      Tn[t] = n2;
+      rot_ok[s] = rot_ok[t] = false;
+      check_infos();
+      if (iterations) *iterations = st_.iterations;
+      if (converged) *converged = st_.converged ? 1 : 0;
     }
   }
 

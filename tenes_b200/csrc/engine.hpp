@@ -36,6 +36,8 @@ struct Engine {
                               int maxiter, double rtol, double* out, int* nev_out) = 0;
   virtual void su_onesite(int site, const double* op) = 0;
   virtual void su_bond(int source, int leg, const double* op) = 0;
+  virtual void fu_bond(int source, int leg, const double* op, const tg_fu_params* params, int* iterations,
+                       int* converged) = 0;
   virtual void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) = 0;
   virtual void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
                            double svd_broadening, double* energy, double* grad) = 0;

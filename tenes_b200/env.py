@@ -275,6 +275,21 @@ class Environment:
         else:
             check(self.lib.tg_su_bond(self.ctx, source, source_leg, dptr(o.view(np.float64))))
 
+    def full_update_bond(self, source: int, source_leg: int, op: np.ndarray, inverse_env_cut: float = 1e-12,
+                         inverse_precision: float = 1e-12, convergence_epsilon: float = 1e-6,
+                         max_iteration: int = 100, gauge_fix: bool = True) -> Tuple[int, bool]:
+        """core::Full_update_bond of the bond (source, source_leg) in the
+        current environment (src/iTPS/full_update.cpp:30-120); the site
+        tensors are replaced, the environment is not moved.  Returns the
+        least-squares iterations and whether they converged."""
+        o = _lib.as_host(op, self.is_complex)
+        fp = _lib.FuParams(float(inverse_env_cut), float(inverse_precision), float(convergence_epsilon),
+                           int(max_iteration), int(bool(gauge_fix)))
+        it, conv = C.c_int(), C.c_int()
+        check(self.lib.tg_fu_bond(self.ctx, source, source_leg, dptr(o.view(np.float64)), C.byref(fp),
+                                  C.byref(it), C.byref(conv)))
+        return it.value, bool(conv.value)
+
     def init_tensors(self, seed: int, initial_dirs: Sequence[Sequence[float]],
                      noises: Sequence[float]) -> None:
         """iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137)."""

@@ -37,6 +37,12 @@ class PEPSParameters:
     MeanField_Env: bool = False
     num_full_step: List[int] = field(default_factory=lambda: [0])
     tau_full_step: List[float] = field(default_factory=lambda: [0.0])
+    Inverse_Env_cut: float = 1e-12
+    Full_Inverse_precision: float = 1e-12
+    Full_Convergence_Epsilon: float = 1e-6
+    Full_max_iteration: int = 100
+    Full_Gauge_Fix: bool = True
+    Full_Use_FastFullUpdate: bool = True
     seed: int = 11
     is_real: bool = False
     iszero_tol: float = 0.0
@@ -215,6 +221,12 @@ def gen_param(param: dict) -> PEPSParameters:
         # (load_toml.cpp:371); kept as is
         if s is not None and "tau" in s:
             p.tau_full_step = _as_list(s["tau"], float)
+        p.Full_Inverse_precision = float(f.get("inverse_precision", p.Full_Inverse_precision))
+        p.Full_Convergence_Epsilon = float(f.get("convergence_epsilon", p.Full_Convergence_Epsilon))
+        p.Inverse_Env_cut = float(f.get("env_cutoff", p.Inverse_Env_cut))
+        p.Full_max_iteration = int(f.get("iteration_max", p.Full_max_iteration))
+        p.Full_Gauge_Fix = bool(f.get("gauge_fix", p.Full_Gauge_Fix))
+        p.Full_Use_FastFullUpdate = bool(f.get("fastfullupdate", p.Full_Use_FastFullUpdate))
     c = param.get("ctm")
     if c is not None:
         p.CHI = int(c.get("dimension", p.CHI))

@@ -8,8 +8,9 @@ twosite_obs.cpp:288-340, multisite_obs.cpp:250-300, correlation_length.cpp:57-12
 density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
 of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 
-Out of scope (raises InputError): full update (num_step > 0 of
-[parameter.full_update]), finite-temperature mode, the mean-field environment.
+Out of scope (raises InputError): full update of complex tensors and
+full-update time evolution, finite-temperature mode, the mean-field
+environment.
 Long-range correlation functions ([correlation]) are measured up to r = 3
 through window contractions, and skipped with a warning beyond that.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
@@ -73,7 +74,7 @@ class ITPS:
         width = max([len("Energy")] + [len(s) for s in n1 + n2 + nm])
         self.names1, self.names2, self.namesm = ([s.ljust(width) for s in n] for n in (n1, n2, nm))
         self._first: Dict[str, bool] = {}
-        self.t_su = self.t_env = self.t_obs = 0.0
+        self.t_su = self.t_fu = self.t_env = self.t_obs = 0.0
         self.t0 = _time.perf_counter()
         if p.CHI < max(max(v) for v in ls.virtual_dims) ** 2 and print_level > 0:
             print("WARNING: CTM may be too small (chi < D*D) for iTPS", file=sys.stderr)
@@ -106,15 +107,56 @@ class ITPS:
             self.env.simple_update(up.source_site, up.source_leg, self._op(up.op))
 
     def optimize(self) -> None:
-        """optimize() (optimize.cpp:24-37): simple update, then (full update: not built)."""
-        if any(n > 0 for n in self.p.num_full_step):
-            raise InputError("full update is not part of this library (set full_update.num_step = 0)")
+        """optimize() (optimize.cpp:24-37): simple update, then full update."""
+        if self.p.num_full_step[0] > 0 and not self.is_real:
+            raise InputError("full update: real tensors only in this library (parameter.general.is_real = true)")
         t = _time.perf_counter()
         nsteps = self.p.num_simple_step[0]
         for _ in range(nsteps):
             self.simple_update_step(0)
         self.env.sync()
         self.t_su += _time.perf_counter() - t
+        if self.p.num_full_step[0] > 0:
+            self.full_update()
+
+    # ------------------------------------------------------ full update
+    # moves after a bond update of the fast full update: (direction, site
+    # whose column / row) for the source and the target (full_update.cpp:122-148);
+    # directions 0 left, 1 right, 2 top, 3 bottom
+    _FAST_MOVES = {0: ((1, "s", "x"), (0, "t", "x")), 1: ((3, "s", "y"), (2, "t", "y")),
+                   2: ((0, "s", "x"), (1, "t", "x")), 3: ((2, "s", "y"), (3, "t", "y"))}
+
+    def full_update_op(self, up) -> None:
+        """iTPS::full_update(EvolutionOperator) (full_update.cpp:30-149)."""
+        if up.is_onesite():
+            self.env.simple_update(up.source_site, -1, self._op(up.op))
+            return
+        p = self.p
+        it, conv = self.env.full_update_bond(up.source_site, up.source_leg, self._op(up.op),
+                                             p.Inverse_Env_cut, p.Full_Inverse_precision,
+                                             p.Full_Convergence_Epsilon, p.Full_max_iteration, p.Full_Gauge_Fix)
+        if not conv and self.print_level > 0:
+            print(f"warning: Full update iteration was not conveged! count= {it}")
+        if not p.Full_Use_FastFullUpdate:
+            self.update_ctm()
+            return
+        target = self._other(up.source_site, *((-1, 0), (0, 1), (1, 0), (0, -1))[up.source_leg])
+        for direction, who, axis in self._FAST_MOVES[up.source_leg]:
+            site = up.source_site if who == "s" else target
+            line = site % self.LX if axis == "x" else site // self.LX
+            self.env.move(direction, line)
+
+    def full_update(self) -> None:
+        """iTPS::full_update() (full_update.cpp:151-186): a full CTMRG, then
+        every full-update operator of group 0 in input order, num_step times."""
+        t = _time.perf_counter()
+        self.update_ctm()
+        for _ in range(self.p.num_full_step[0]):
+            for up in self.inp.full_updates:
+                if up.group == 0:
+                    self.full_update_op(up)
+        self.env.sync()
+        self.t_fu += _time.perf_counter() - t
 
     # ------------------------------------------------------ environment
     def update_ctm(self) -> Tuple[int, bool, float]:
@@ -538,7 +580,7 @@ class ITPS:
         with open(os.path.join(self.outdir, "time.dat"), "w") as f:
             f.write(f"time all           = {_time.perf_counter() - self.t0}\n")
             f.write(f"time simple update = {self.t_su}\n")
-            f.write(f"time full update   = 0\n")
+            f.write(f"time full update   = {self.t_fu}\n")
             f.write(f"time environment  = {self.t_env}\n")
             f.write(f"time observable    = {self.t_obs}\n")
 

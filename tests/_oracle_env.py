@@ -95,6 +95,25 @@ class OracleEnvironment:
     def sync(self):
         pass
 
+    def full_update_bond(self, source, leg, op, inverse_env_cut=1e-12, inverse_precision=1e-12,
+                         convergence_epsilon=1e-6, max_iteration=100, gauge_fix=True):
+        import dataclasses
+        p = dataclasses.replace(self.p, Inverse_Env_cut=inverse_env_cut, Full_Inverse_precision=inverse_precision,
+                                Full_Convergence_Epsilon=convergence_epsilon, Full_max_iteration=max_iteration,
+                                Full_Gauge_Fix=gauge_fix)
+        tg = self.lat.neighbor(source, leg)
+        args = O.full_update_env_args(self.env, source, leg, self.lat)
+        r = O._FU_ROT[leg]
+        a, b, it, conv = O.full_update_bond_horizontal(*args, self.Tn[source].transpose(r),
+                                                       self.Tn[tg].transpose(r), op, p)
+        k = O._FU_BACK[leg]
+        self.Tn[source], self.Tn[tg] = a.transpose(k), b.transpose(k)
+        return it, conv
+
+    def move(self, direction, line):
+        fn = (O.left_move, O.right_move, O.top_move, O.bottom_move)[direction]
+        fn(self.env, self.Tn, line, self.p, self.lat)
+
     def calc_ctm_environment(self, initialize=True):
         self.env, it, conv, sig = O.calc_ctm_environment(self.Tn, self.p, self.lat)
         return it, conv, sig

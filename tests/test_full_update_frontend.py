@@ -1,0 +1,49 @@
+"""Ground state with a full-update step through the front end
+(optimize.cpp:24-37, full_update.cpp:30-186) over the oracle-backed stand-in
+of the environment, against the reference's AntiferroHeisenberg_real golden
+(100 simple-update steps, one full-update step with the fast full update's
+single moves, CTMRG chi = 5, observables, correlations)."""
+
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _rows(path):
+    out = []
+    for line in open(path):
+        line = line.split("#")[0].strip()
+        if line:
+            out.append([float(w) for w in line.split()])
+    return out
+
+
+def _density(path):
+    d = {}
+    for line in open(path):
+        if "=" in line:
+            name, vals = line.split("=")
+            d[name.strip()] = [float(x) for x in vals.split()]
+    return d
+
+
+def test_afh_full_update_driver_on_oracle(tmp_path, monkeypatch):
+    import tenes_b200.itps as itps
+    from tests._oracle_env import OracleEnvironment
+    monkeypatch.setattr(itps, "Environment", OracleEnvironment)
+    it = itps.run(os.path.join(GOLDEN, "afh_real_input.toml"), print_level=0, outdir=str(tmp_path))
+    exp = json.load(open(os.path.join(GOLDEN, "afh_real_expected.json")))
+    dens = _density(tmp_path / "density.dat")
+    assert set(dens) == set(exp["density"])
+    for k, v in exp["density"].items():
+        np.testing.assert_allclose(dens[k], v, rtol=1e-10, atol=1e-12, err_msg=k)
+    for name, key in (("onesite_obs.dat", "onesite"), ("twosite_obs.dat", "twosite"),
+                      ("multisite_obs_4.dat", "multisite"), ("correlation.dat", "correlation")):
+        res, ref = _rows(tmp_path / name), exp[key]
+        assert len(res) == len(ref), name
+        np.testing.assert_allclose(np.array(res), np.array(ref), rtol=1e-9, atol=1e-11, err_msg=name)
+    assert it.t_fu > 0.0
+    assert "time full update" in open(tmp_path / "time.dat").read()

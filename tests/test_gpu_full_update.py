@@ -1,0 +1,89 @@
+"""Full update on the GPU (tg_fu_bond and the front end's full-update steps).
+
+* tg_fu_bond against the oracle's full_update_bond (pinned to the reference's
+  full_update.dat and AntiferroHeisenberg_real golden) in a CTM environment,
+  for every bond direction: the bond-contracted pair Tn1_new . Tn2_new (free of
+  the gauge on the updated bond) and the least-squares iteration count;
+* the reference's AntiferroHeisenberg_real input through ``python -m
+  tenes_b200`` (simple update, one full-update step with the fast full
+  update's moves, CTMRG, observables) against its golden files, checked the
+  way the reference checks them (test/fulltest.py.in: rtol 1e-3, atol 1e-4)."""
+
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import tenes_oracle as O
+from tenes_b200.std_ops import evolution_twosite, heisenberg_bond
+from tests._helpers import gpu_env, load_env
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(REPO, "tests", "golden")
+BOND = {0: (0, 2), 1: (1, 3), 2: (2, 0), 3: (3, 1)}
+
+
+@pytest.mark.parametrize("leg", [0, 1, 2, 3])
+def test_fu_bond_matches_oracle(leg):
+    rng = np.random.default_rng(31 + leg)
+    lat = O.Lattice(2, 2)
+    lat.physical_dims = [2] * 4
+    lat.virtual_dims = [[2] * 4 for _ in range(4)]
+    Tn = [rng.standard_normal((2, 2, 2, 2, 2)) for _ in range(4)]
+    p = O.Params(CHI=4)
+    env = O.init_env(Tn, p, lat)
+    for _ in range(3):
+        O.sweep(env, Tn, p, lat)
+    op = evolution_twosite(heisenberg_bond(1.0), 0.1).real
+    source = 1
+    tgt = lat.neighbor(source, leg)
+    args = O.full_update_env_args(env, source, leg, lat)
+    r = O._FU_ROT[leg]
+    _, _, it_ref, conv_ref = O.full_update_bond_horizontal(*args, Tn[source].transpose(r), Tn[tgt].transpose(r),
+                                                           op, p)
+    ra, rb = O.full_update_bond(*args, Tn[source], Tn[tgt], op, leg, p)
+    ge = gpu_env(lat, Tn, 4)
+    load_env(ge, env)
+    it, conv = ge.full_update_bond(source, leg, op)
+    a, b = ge.get_site_tensor(source), ge.get_site_tensor(tgt)
+    ge.close()
+    la, lb = BOND[leg]
+    assert (it, conv) == (it_ref, conv_ref)
+    np.testing.assert_allclose(np.tensordot(a, b, ([la], [lb])), np.tensordot(ra, rb, ([la], [lb])),
+                               rtol=1e-8, atol=1e-12)
+
+
+def _rows(path):
+    out = []
+    for line in open(path):
+        line = line.split("#")[0].strip()
+        if line:
+            out.append([float(w) for w in line.split()])
+    return out
+
+
+def test_afh_full_update_golden(tmp_path):
+    r = subprocess.run([sys.executable, "-m", "tenes_b200", os.path.join(GOLDEN, "afh_real_input.toml"),
+                        "--outdir", str(tmp_path), "--quiet"], cwd=REPO, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    exp = json.load(open(os.path.join(GOLDEN, "afh_real_expected.json")))
+    tol = exp["tolerance"]
+    dens = {}
+    for line in open(tmp_path / "density.dat"):
+        if "=" in line:
+            name, vals = line.split("=")
+            dens[name.strip()] = [float(x) for x in vals.split()]
+    assert set(dens) == set(exp["density"])
+    for k, v in exp["density"].items():
+        np.testing.assert_allclose(dens[k], v, rtol=tol["rtol"], atol=tol["atol"], err_msg=k)
+    for name, key in (("onesite_obs.dat", "onesite"), ("twosite_obs.dat", "twosite"),
+                      ("multisite_obs_4.dat", "multisite"), ("correlation.dat", "correlation")):
+        res, ref = _rows(tmp_path / name), exp[key]
+        assert len(res) == len(ref), name
+        np.testing.assert_allclose(np.array(res), np.array(ref), rtol=tol["rtol"], atol=tol["atol"], err_msg=name)
