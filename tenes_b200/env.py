@@ -267,8 +267,24 @@ class Environment:
         return v[0::2] + 1j * v[1::2]
 
     # ------------------------------------------------------- simple update
+    def _check_op(self, source: int, source_leg: int, op: np.ndarray) -> None:
+        """A one-site op must be (d, d) and a bond op (d_s, d_t, d_s, d_t) for the
+        sites' physical dimensions (the library keeps them fixed)."""
+        d = self.pdim[source]
+        if source_leg < 0:
+            want = (d, d)
+        else:
+            from .input import LatticeSpec
+            t = LatticeSpec(self.LX, self.LY, self.skew, self.pdim, self.vdim, [], []).other(
+                source, *((-1, 0), (0, 1), (1, 0), (0, -1))[source_leg])
+            want = (d, self.pdim[t], d, self.pdim[t])
+        if tuple(np.shape(op)) != want:
+            raise ValueError(f"operator of shape {tuple(np.shape(op))} on site {source} leg {source_leg}: "
+                             f"{want} expected")
+
     def simple_update(self, source: int, source_leg: int, op: np.ndarray) -> None:
         """iTPS::simple_update(EvolutionOperator) (src/iTPS/simple_update.cpp:25-46)."""
+        self._check_op(source, source_leg, op)
         o = _lib.as_host(op, self.is_complex)
         if source_leg < 0:
             check(self.lib.tg_su_onesite(self.ctx, source, dptr(o.view(np.float64))))
@@ -282,6 +298,7 @@ class Environment:
         current environment (src/iTPS/full_update.cpp:30-120); the site
         tensors are replaced, the environment is not moved.  Returns the
         least-squares iterations and whether they converged."""
+        self._check_op(source, source_leg, op)
         o = _lib.as_host(op, self.is_complex)
         fp = _lib.FuParams(float(inverse_env_cut), float(inverse_precision), float(convergence_epsilon),
                            int(max_iteration), int(bool(gauge_fix)))

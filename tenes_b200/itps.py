@@ -58,6 +58,17 @@ class ITPS:
                        inverse_lambda_cut=p.Inverse_lambda_cut, mixed=mixed)
         self.env = Environment(ls.LX, ls.LY, ls.physical_dims, ls.virtual_dims, cp, not self.is_real,
                                skew=ls.skew, device=device)
+        for up in list(inp.simple_updates) + list(inp.full_updates):
+            d = ls.physical_dims[up.source_site]
+            if up.is_onesite():
+                ok = up.op.shape == (d, d)
+            else:
+                dt = ls.physical_dims[ls.other(up.source_site, *((-1, 0), (0, 1), (1, 0), (0, -1))[up.source_leg])]
+                ok = up.op.shape == (d, dt, d, dt)
+            if not ok:
+                raise InputError(f"evolution operator on site {up.source_site} has dimensions {list(up.op.shape)}: "
+                                 "operators that change a site's physical dimension along the sequence (as "
+                                 "next-nearest-neighbour gates do) are not supported by this library")
         if p.tensor_save_dir:  # iTPS.cpp:161-173
             os.makedirs(p.tensor_save_dir, exist_ok=True)
         if p.tensor_load_dir:  # initialize_tensors: the checkpoint replaces the random start (tensors.cpp:130-135)

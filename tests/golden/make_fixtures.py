@@ -18,6 +18,8 @@ tree at run time:
 * afh_real_input.toml / afh_real_expected.json <- test/data/AntiferroHeisenberg_real.toml and
   output_AntiferroHeisenberg_real/{density,onesite_obs,twosite_obs,multisite_obs_4,correlation,
   correlation_length}.dat (simple update + one full-update step + CTMRG)
+* {j1j2_afh,honeycomb,honeycomb_skew,afh_complex}_{input.toml,expected.json} <- J1J2_AFH,
+  Honeycomb, Honeycomb_skew and AntiferroHeisenberg_complex in the same form
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
 """
@@ -89,6 +91,28 @@ def main(ref):
     exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
     with open(os.path.join(HERE, "afh_real_expected.json"), "w") as f:
         json.dump(exp, f)
+
+    # further ground states with full-update steps
+    for name, stem in (("J1J2_AFH", "j1j2_afh"), ("Honeycomb", "honeycomb"), ("Honeycomb_skew", "honeycomb_skew"),
+                       ("AntiferroHeisenberg_complex", "afh_complex")):
+        shutil.copyfile(os.path.join(data, name + ".toml"), os.path.join(HERE, stem + "_input.toml"))
+        out = os.path.join(data, "output_" + name)
+        exp = {}
+        dens = {}
+        for line in open(os.path.join(out, "density.dat")):
+            if "=" in line:
+                key, vals = line.split("=")
+                dens[key.strip()] = [float(x) for x in vals.split()]
+        exp["density"] = dens
+        for key, fname in (("onesite", "onesite_obs.dat"), ("twosite", "twosite_obs.dat"),
+                           ("multisite", "multisite_obs_4.dat"), ("correlation", "correlation.dat"),
+                           ("correlation_length", "correlation_length.dat")):
+            path = os.path.join(out, fname)
+            if os.path.exists(path):
+                exp[key] = _rows(path)
+        exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
+        with open(os.path.join(HERE, stem + "_expected.json"), "w") as f:
+            json.dump(exp, f)
 
     with tempfile.TemporaryDirectory() as td:
         exe = os.path.join(td, "mt")

@@ -47,3 +47,17 @@ def test_afh_full_update_driver_on_oracle(tmp_path, monkeypatch):
         np.testing.assert_allclose(np.array(res), np.array(ref), rtol=1e-9, atol=1e-11, err_msg=name)
     assert it.t_fu > 0.0
     assert "time full update" in open(tmp_path / "time.dat").read()
+
+
+def test_dimension_changing_gates_are_an_input_error(tmp_path, monkeypatch):
+    """J1J2_AFH's gates change a site's physical dimension (2 -> 8 -> 2); the
+    library keeps physical dimensions fixed and says so instead of misreading
+    the operators."""
+    import pytest
+
+    import tenes_b200.itps as itps
+    from tenes_b200.input import InputError
+    from tests._oracle_env import OracleEnvironment
+    monkeypatch.setattr(itps, "Environment", OracleEnvironment)
+    with pytest.raises(InputError, match="change a site's physical dimension"):
+        itps.run(os.path.join(GOLDEN, "j1j2_afh_input.toml"), print_level=0, outdir=str(tmp_path))
