@@ -257,6 +257,24 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
             "seconds_per_sweep_sweep_check_energy": per_sweep}
 
 
+def max_over_ranks(ms, device, world):
+    """The largest of the ranks' times (all-reduce MAX over the process
+    group); unchanged for a single rank."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, steps, total_ms):
+    """Whole-job sweeps/s of `world` independent replicas that each ran
+    `steps` sweeps in at most `total_ms`."""
+    return world * steps / (total_ms * 1e-3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -306,14 +324,11 @@ def run_ours(args, rank, world, local_rank):
         timed_breakdown = {PROFILE_KINDS[k]: round(profile_query(k)[1] / args.steps, 3)
                            for k in range(len(PROFILE_KINDS))}
         profile_enable(False)
-    total_ms = sum(times)
+    total_ms = max_over_ranks(sum(times), device, world)
     if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms * 1e-3)
+    value = replica_rate(world, args.steps, total_ms)
 
     # ---- end to end through the C ABI with host buffers (set Tn + env, sweep, get env)
     # page-locked host buffers (allocated and filled outside the timed region)
@@ -352,11 +367,8 @@ def run_ours(args, rank, world, local_rank):
         e.record(stream)
         e.synchronize()
         e2e_ms += s.elapsed_time(e)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "sweeps/s",
+    e2e_ms = max_over_ranks(e2e_ms, device, world)
+    e2e = {"value": replica_rate(world, args.steps, e2e_ms), "unit": "sweeps/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(t.nbytes for ws in host_env for t in ws),
            "host_buffers": "page-locked; per step: 4 site tensors + 32 environment tensors up through "
                            "tg_set_site_tensor / tg_set_env, one tg_ctm_sweep, 32 environment tensors down "
