@@ -147,6 +147,17 @@ tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const do
  * contraction sequence as Contract_two_sites_*_op12 (ctm.cpp:213-319). */
 tg_status tg_measure_bond_rdm(tg_ctx* ctx, int source, int dx, int dy, double* out);
 
+/* Long-range correlations along a strip (StartCorrelation / Transfer /
+ * FinishCorrelation_iTPS_CTM, contract_itps_ctm/correlation.cpp, as
+ * measure_correlation_ctm uses them, correlation_function.cpp:70-212):
+ * <O_left O_right> / <1> with O_left on `left` and O_right on the site r steps
+ * to the right (dir 0) or up (dir 1), for r = 1..r_max.  left_op is d x d for
+ * `left`; right_ops lists, for every site of the unit cell in order, nright
+ * operators of that site's d x d.  out receives (re, im) pairs, r-major:
+ * out[2*((r-1)*nright + q)].  Linear in r_max. */
+tg_status tg_measure_correlation(tg_ctx* ctx, int left, int dir, int r_max, const double* left_op, int nright,
+                                 const double* right_ops, double* out);
+
 /* <prod of one-site ops> on an nrow x ncol window (1..4 each), unnormalised:
  * Contract_RxC_iTPS_CTM (contract_itps_ctm/ctm.cpp:45-87).  The window holds
  * site lat.other(source, c - source_col, source_row - r) at (r, c), row 0 on

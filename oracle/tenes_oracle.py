@@ -1086,6 +1086,73 @@ def contract_window(C: Sequence[np.ndarray], eTt, eTr, eTb, eTl, Tn, op) -> comp
 
 
 # ---------------------------------------------------------------------------
+# Long-range correlations along a strip (contract_itps_ctm/correlation.cpp:
+# StartCorrelation_iTPS_CTM, Transfer_iTPS_CTM, FinishCorrelation_iTPS_CTM;
+# driver correlation_function.cpp:42-220).  The strip state A has legs
+# (e1r, e3r, n1r, n2r).
+# ---------------------------------------------------------------------------
+
+
+def start_correlation(C1, C4, eT1, eT3, eT4, Tn1, op):
+    """StartCorrelation_iTPS_CTM (contract_itps_ctm/correlation.cpp:30-57)."""
+    X = td(eT3, td(C1, td(C4, eT4, ([1], [0])), ([0], [1])), ([1], [1]))
+    X = td(td(cj(Tn1), op, ([4], [1])), X, ([0, 3], [5, 2]))
+    X = td(Tn1, X, ([0, 3, 4], [6, 4, 2]))
+    return td(eT1, X, ([0, 2, 3], [5, 0, 2])).transpose(0, 3, 1, 2)
+
+
+def transfer_correlation(A, eT1, eT3, Tn1):
+    """Transfer_iTPS_CTM (contract_itps_ctm/correlation.cpp:59-77)."""
+    X = td(cj(Tn1), td(A, eT3, ([1], [1])), ([0, 3], [2, 5]))
+    X = td(Tn1, X, ([0, 3, 4], [4, 6, 2]))
+    return td(eT1, X, ([0, 2, 3], [4, 0, 2])).transpose(0, 3, 1, 2)
+
+
+def finish_correlation(A, C2, C3, eT1, eT2, eT3, Tn1, op):
+    """FinishCorrelation_iTPS_CTM (contract_itps_ctm/correlation.cpp:79-104)."""
+    X = td(eT3, td(C2, td(C3, eT2, ([0], [1])), ([1], [1])), ([0], [1]))
+    X = td(cj(Tn1), X, ([2, 3], [5, 2]))
+    X = td(td(A, eT1, ([0], [0])), X, ([0, 2, 3, 5], [3, 0, 5, 1]))
+    X = td(Tn1, X, ([0, 1, 2, 3], [0, 1, 4, 3]))
+    return complex(np.sum(op * X))
+
+
+_VROT = (3, 0, 1, 2, 4)
+
+
+def correlation_strip(env: "Env", Tn, lat: "Lattice", left: int, vertical: bool, r_max: int, left_op,
+                      right_ops):
+    """<O_left O_right> / <1> at distances 1..r_max to the right (vertical:
+    up) of `left`, as correlation_function.cpp:70-212 computes them.
+    right_ops(site) lists the right operators for a site; returns
+    [[value for each right op] for r in 1..r_max]."""
+    e = env
+    eye = lambda s: np.eye(lat.physical_dims[s], dtype=Tn[s].dtype)  # noqa: E731
+    if not vertical:
+        args = (e.C1[left], e.C4[left], e.eTt[left], e.eTb[left], e.eTl[left], Tn[left])
+    else:
+        args = (e.C4[left], e.C3[left], e.eTl[left], e.eTr[left], e.eTb[left], Tn[left].transpose(_VROT))
+    A = start_correlation(*args, left_op)
+    An = start_correlation(*args, eye(left))
+    out = []
+    site = left
+    for _ in range(r_max):
+        site = lat.top(site) if vertical else lat.right(site)
+        if not vertical:
+            fin = (e.C2[site], e.C3[site], e.eTt[site], e.eTr[site], e.eTb[site], Tn[site])
+            tra = (e.eTt[site], e.eTb[site], Tn[site])
+        else:
+            tn = Tn[site].transpose(_VROT)
+            fin = (e.C1[site], e.C2[site], e.eTl[site], e.eTt[site], e.eTr[site], tn)
+            tra = (e.eTl[site], e.eTr[site], tn)
+        norm = finish_correlation(An, *fin, eye(site))
+        out.append([finish_correlation(A, *fin, op) / norm for op in right_ops(site)])
+        A = transfer_correlation(A, *tra)
+        An = transfer_correlation(An, *tra)
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Measurement driver (src/iTPS/onesite_obs.cpp:35-123, twosite_obs.cpp:31-260,
 # multisite_obs.cpp:31-232, density.cpp:30-76)
 # ---------------------------------------------------------------------------

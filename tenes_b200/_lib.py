@@ -28,7 +28,7 @@ EXPORTED = [
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
-    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond",
+    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_measure_correlation",
 ]
 
 
@@ -100,6 +100,7 @@ def load() -> C.CDLL:
         "tg_measure_onesite": (C.c_int, [vp, C.c_int, dp, dp]),
         "tg_measure_bond_op12": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, dp]),
         "tg_measure_bond_rdm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp]),
+        "tg_measure_correlation": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp]),
         "tg_su_onesite": (C.c_int, [vp, C.c_int, dp]),
         "tg_measure_window": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int),
                                         P(C.c_int), dp, dp]),

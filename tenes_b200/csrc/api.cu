@@ -179,6 +179,15 @@ tg_status tg_measure_bond_rdm(tg_ctx* ctx, int source, int dx, int dy, double* o
     E(ctx)->measure_bond_rdm(source, dx, dy, out);
   });
 }
+tg_status tg_measure_correlation(tg_ctx* ctx, int left, int dir, int r_max, const double* left_op, int nright,
+                                 const double* right_ops, double* out) {
+  return guard([&] {
+    need(left_op, "left_op");
+    need(right_ops, "right_ops");
+    need(out, "out");
+    E(ctx)->measure_correlation(left, dir, r_max, left_op, nright, right_ops, out);
+  });
+}
 tg_status tg_measure_window(tg_ctx* ctx, int source, int nrow, int ncol, int source_row, int source_col, int nops,
                             const int* op_row, const int* op_col, const double* ops, double* out) {
   return guard([&] {

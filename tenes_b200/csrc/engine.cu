@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -1409,6 +1410,96 @@ struct EngineT final : Engine {
     // X[a,c,b,d] with (a,c) the first site's legs: rdm_first[a,b,c,d] = X[a,c,b,d]; with the
     // source second, rdm_source[b,a,d,c] = X[a,c,b,d]
     download(tr(X, source_first ? V{0, 2, 1, 3} : V{2, 0, 3, 1}), out);
+  }
+
+  // ------------------------------------------------ correlations (strip)
+  // StartCorrelation_iTPS_CTM (contract_itps_ctm/correlation.cpp:30-57):
+  // the strip state, legs (e1r, e3r, n1r, n2r)
+  DT<T> corr_start(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT3, const DT<T>& eT4,
+                   const DT<T>& Tn1, const DT<T>& op) {
+    DT<T> X = td(eT3, td(C1, td(C4, eT4, {1}, {0}), {0}, {1}), {1}, {1});
+    X = td(td(Tn1, op, {4}, {1}, true, false), X, {0, 3}, {5, 2});
+    X = td(Tn1, X, {0, 3, 4}, {6, 4, 2});
+    return tr(td(eT1, X, {0, 2, 3}, {5, 0, 2}), {0, 3, 1, 2});
+  }
+  // Transfer_iTPS_CTM (correlation.cpp:59-77)
+  DT<T> corr_transfer(const DT<T>& A, const DT<T>& eT1, const DT<T>& eT3, const DT<T>& Tn1) {
+    DT<T> X = td(Tn1, td(A, eT3, {1}, {1}), {0, 3}, {2, 5}, true, false);
+    X = td(Tn1, X, {0, 3, 4}, {4, 6, 2});
+    return tr(td(eT1, X, {0, 2, 3}, {4, 0, 2}), {0, 3, 1, 2});
+  }
+  // FinishCorrelation_iTPS_CTM (correlation.cpp:79-104)
+  T corr_finish(const DT<T>& A, const DT<T>& C2, const DT<T>& C3, const DT<T>& eT1, const DT<T>& eT2,
+                const DT<T>& eT3, const DT<T>& Tn1, const DT<T>& op) {
+    DT<T> X = td(eT3, td(C2, td(C3, eT2, {0}, {1}), {1}, {1}), {0}, {1});
+    X = td(Tn1, X, {2, 3}, {5, 2}, true, false);
+    X = td(td(A, eT1, {0}, {0}), X, {0, 2, 3, 5}, {3, 0, 5, 1});
+    X = td(Tn1, X, {0, 1, 2, 3}, {0, 1, 4, 3});
+    return scalar(td(op, X, {0, 1}, {0, 1}));
+  }
+  static std::complex<double> as_complex(const T& v) {
+    if constexpr (CPLX) return {v.x, v.y};
+    else return {v, 0.0};
+  }
+  DT<T> identity_op(int site) {
+    const int64_t d = lat.pdim[site];
+    std::vector<double> h(static_cast<size_t>(d * d * NW), 0.0);
+    for (int64_t k = 0; k < d; ++k) h[static_cast<size_t>((k * d + k) * NW)] = 1.0;
+    return from_host({d, d}, h.data());
+  }
+
+  // measure_correlation_ctm's strip for one left site and direction
+  // (correlation_function.cpp:70-212): <O_left O_right> / <1> at distances
+  // 1..r_max to the right (dir 0) or up (dir 1).  right_ops holds, site by
+  // site over the unit cell, nright d x d operators of that site.
+  void measure_correlation(int left, int dir, int r_max, const double* left_op, int nright, const double* right_ops,
+                           double* out) override {
+    require_env();
+    check_site(left);
+    if (dir != 0 && dir != 1) fail(TG_E_INPUT, "correlation direction must be 0 (right) or 1 (up)");
+    if (r_max < 1 || nright < 1) fail(TG_E_INPUT, "r_max and the number of right operators must be positive");
+    std::vector<int64_t> off(static_cast<size_t>(lat.N + 1), 0);
+    for (int i = 0; i < lat.N; ++i)
+      off[static_cast<size_t>(i + 1)] = off[static_cast<size_t>(i)] + static_cast<int64_t>(nright) * lat.pdim[i] * lat.pdim[i] * NW;
+    static const V vrot = {3, 0, 1, 2, 4};
+    const int64_t dl = lat.pdim[left];
+    const DT<T> lop = from_host({dl, dl}, left_op);
+    const DT<T> lid = identity_op(left);
+    DT<T> A, An;
+    if (dir == 0) {
+      A = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], Tn[left], lop);
+      An = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], Tn[left], lid);
+    } else {
+      const DT<T> tn = tr(Tn[left], vrot);
+      A = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], tn, lop);
+      An = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], tn, lid);
+    }
+    int site = left;
+    for (int r = 0; r < r_max; ++r) {
+      site = dir == 0 ? lat.right(site) : lat.top(site);
+      const DT<T> tn = dir == 0 ? Tn[site] : tr(Tn[site], vrot);
+      auto fin = [&](const DT<T>& S, const DT<T>& op) {
+        return dir == 0 ? corr_finish(S, C[1][site], C[2][site], E[0][site], E[1][site], E[2][site], tn, op)
+                        : corr_finish(S, C[0][site], C[1][site], E[3][site], E[0][site], E[1][site], tn, op);
+      };
+      const std::complex<double> nrm = as_complex(fin(An, identity_op(site)));
+      const int64_t d = lat.pdim[site];
+      for (int q = 0; q < nright; ++q) {
+        const DT<T> rop = from_host({d, d}, right_ops + off[static_cast<size_t>(site)] + q * d * d * NW);
+        const std::complex<double> v = as_complex(fin(A, rop)) / nrm;
+        out[2 * (r * nright + q)] = v.real();
+        out[2 * (r * nright + q) + 1] = v.imag();
+      }
+      if (r + 1 < r_max) {
+        if (dir == 0) {
+          A = corr_transfer(A, E[0][site], E[2][site], tn);
+          An = corr_transfer(An, E[0][site], E[2][site], tn);
+        } else {
+          A = corr_transfer(A, E[3][site], E[1][site], tn);
+          An = corr_transfer(An, E[3][site], E[1][site], tn);
+        }
+      }
+    }
   }
 
   // ------------------------------------------------- N x M window <op...>

@@ -30,6 +30,8 @@ struct Engine {
   virtual void measure_onesite(int site, const double* op, double* out) = 0;
   virtual void measure_bond_op12(int source, int dx, int dy, const double* op, double* out) = 0;
   virtual void measure_bond_rdm(int source, int dx, int dy, double* out) = 0;
+  virtual void measure_correlation(int left, int dir, int r_max, const double* left_op, int nright,
+                                   const double* right_ops, double* out) = 0;
   virtual void measure_window(int source, int nrow, int ncol, int source_row, int source_col, int nops,
                               const int* op_row, const int* op_col, const double* ops, double* out) = 0;
   virtual void tm_eigenvalues(int dir, int fixed, int num_eigvals, int maxdim_dense, int maxdim, int restartdim,

@@ -203,6 +203,23 @@ class Environment:
         check(self.lib.tg_measure_bond_rdm(self.ctx, source, dx, dy, dptr(out)))
         return out.view(self.dtype).reshape(shape)
 
+    def correlation_strip(self, left: int, vertical: bool, r_max: int, left_op: np.ndarray, right_ops) -> np.ndarray:
+        """<O_left O_right>/<1> at distances 1..r_max to the right (vertical:
+        up) of `left` through the strip contraction (tg_measure_correlation).
+        right_ops(site) -> list of that site's right operators (the same
+        count for every site).  Returns a complex (r_max, nright) array."""
+        lists = [list(right_ops(i)) for i in range(self.N)]
+        nright = len(lists[0])
+        if any(len(l) != nright for l in lists) or nright == 0:
+            raise ValueError("correlation_strip: the same positive number of right operators on every site")
+        flat = np.concatenate([np.ascontiguousarray(o, dtype=self.dtype).reshape(-1) for l in lists for o in l])
+        flat = np.ascontiguousarray(flat, dtype=self.dtype)
+        lop = np.ascontiguousarray(left_op, dtype=self.dtype)
+        out = np.zeros(2 * r_max * nright)
+        check(self.lib.tg_measure_correlation(self.ctx, left, int(bool(vertical)), r_max, dptr(lop.view(np.float64)),
+                                              nright, dptr(flat.view(np.float64)), dptr(out)))
+        return (out[0::2] + 1j * out[1::2]).reshape(r_max, nright)
+
     def contract_window(self, source: int, nrow: int, ncol: int, source_row: int, source_col: int,
                         ops: Optional[dict] = None) -> complex:
         """Contract_RxC_iTPS_CTM: <prod ops> on an nrow x ncol window (unnormalised).

@@ -11,8 +11,8 @@ of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 Out of scope (raises InputError): full update of complex tensors and
 full-update time evolution, finite-temperature mode, the mean-field
 environment.
-Long-range correlation functions ([correlation]) are measured up to r = 3
-through window contractions, and skipped with a warning beyond that.
+Long-range correlation functions ([correlation]) are measured through window
+contractions up to r = 3 and through the strip contraction beyond.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
 saveload.py.
 """
@@ -282,12 +282,11 @@ class ITPS:
         return ret
 
     # ------------------------------------------- long-range correlations
-    # The strip of a correlation at distance r is a 1 x (r+1) (or (r+1) x 1)
-    # window; the window contraction's boundary tensor carries two legs of
-    # dimension D per column, so the strip is held to r <= 3 (the window
-    # limit) and to about 2 GB of boundary tensor.
-    MAX_CORRELATION_R = 3
-    MAX_CORRELATION_BYTES = 2 << 30
+    # Up to r = 3 (and about 2 GB of boundary tensor) a correlation is read
+    # from the window that spans the two sites; longer strips go through the
+    # strip contraction (tg_measure_correlation), linear in r.
+    MAX_WINDOW_R = 3
+    MAX_WINDOW_BYTES = 2 << 30
 
     def _site_op_or_none(self, site: int, group: int):
         for o in self.inp.onesite:
@@ -299,21 +298,15 @@ class ITPS:
         """measure_correlation_ctm (correlation_function.cpp:42-220): for every
         site and every (left, right) one-site operator group pair of
         [correlation], <O_left O_right> / <1> at horizontal and vertical
-        distances 1 .. r_max.  Each value is the window spanning the two sites
-        with the two operators at its ends, over the same window without
-        operators -- the network the reference's StartCorrelation / Transfer /
-        FinishCorrelation strip contracts.  Returns None (with a warning) when
-        the strips are beyond the window contraction's reach."""
+        distances 1 .. r_max, in the reference's order.  Short strips are read
+        from windows (the window over the two sites with the operators at its
+        ends, over the same window without operators); longer ones from the
+        StartCorrelation / Transfer / FinishCorrelation strip."""
         cp = self.inp.corparam
         nl = len(self.names1)
         dmax = max(max(v) for v in self.inp.lattice.virtual_dims)
-        need = 16 * self.p.CHI ** 2 * dmax ** (2 * (cp.r_max + 1))
-        if cp.r_max > self.MAX_CORRELATION_R or need > self.MAX_CORRELATION_BYTES:
-            if self.print_level > 0:
-                print(f"WARNING: long-range correlations up to r_max = {cp.r_max} need strips beyond this "
-                      f"library's window contraction (r <= {self.MAX_CORRELATION_R}, "
-                      f"{self.MAX_CORRELATION_BYTES >> 30} GB); [correlation] skipped", file=sys.stderr)
-            return None
+        use_windows = (cp.r_max <= self.MAX_WINDOW_R
+                       and 16 * self.p.CHI ** 2 * dmax ** (2 * (cp.r_max + 1)) <= self.MAX_WINDOW_BYTES)
         r_ops: List[List[int]] = [[] for _ in range(nl)]
         for lop, rop in cp.operators:
             if not (0 <= lop < nl and 0 <= rop < nl):
@@ -328,21 +321,43 @@ class ITPS:
                 if Ol is None:
                     continue
                 for horizontal in (True, False):
-                    site = left
+                    if use_windows:
+                        vals = self._correlation_windows(left, horizontal, cp.r_max, Ol, r_ops[lop])
+                    else:
+                        def ops_of(site, rops=r_ops[lop]):
+                            d = self.inp.lattice.physical_dims[site]
+                            return [self._site_op_or_none(site, q) if self._site_op_or_none(site, q) is not None
+                                    else np.zeros((d, d)) for q in rops]
+                        strip = self.env.correlation_strip(left, not horizontal, cp.r_max, Ol, ops_of)
+                        vals = []
+                        site = left
+                        for r in range(cp.r_max):
+                            site = self._other(site, 1, 0) if horizontal else self._other(site, 0, 1)
+                            vals.append([strip[r][k] if self._site_op_or_none(site, q) is not None else None
+                                         for k, q in enumerate(r_ops[lop])])
                     for r in range(1, cp.r_max + 1):
-                        site = self._other(site, 1, 0) if horizontal else self._other(site, 0, 1)
-                        if horizontal:
-                            geo, pl, pr, dx, dy = (1, r + 1, 0, 0), (0, 0), (0, r), r, 0
-                        else:
-                            geo, pl, pr, dx, dy = (r + 1, 1, r, 0), (r, 0), (0, 0), 0, r
-                        norm = self.env.contract_window(left, *geo)
-                        for rop in r_ops[lop]:
-                            Or = self._site_op_or_none(site, rop)
-                            if Or is None:
-                                continue
-                            v = self.env.contract_window(left, *geo, {pl: Ol, pr: Or}) / norm
-                            out.append((left, dx, dy, lop, rop, v))
+                        for k, rop in enumerate(r_ops[lop]):
+                            v = vals[r - 1][k]
+                            if v is not None:
+                                out.append((left, r if horizontal else 0, 0 if horizontal else r, lop, rop, v))
         return out
+
+    def _correlation_windows(self, left, horizontal, r_max, Ol, rops):
+        vals = []
+        site = left
+        for r in range(1, r_max + 1):
+            site = self._other(site, 1, 0) if horizontal else self._other(site, 0, 1)
+            if horizontal:
+                geo, pl, pr = (1, r + 1, 0, 0), (0, 0), (0, r)
+            else:
+                geo, pl, pr = (r + 1, 1, r, 0), (r, 0), (0, 0)
+            norm = self.env.contract_window(left, *geo)
+            row = []
+            for rop in rops:
+                Or = self._site_op_or_none(site, rop)
+                row.append(None if Or is None else self.env.contract_window(left, *geo, {pl: Ol, pr: Or}) / norm)
+            vals.append(row)
+        return vals
 
     def save_correlation(self, cors, time, prefix):
         """save_correlation (correlation_function.cpp:349-395)."""
@@ -537,9 +552,7 @@ class ITPS:
         if self.inp.multisite:
             self.save_multisite(multi, time, prefix)
         if self.inp.corparam.r_max > 0:
-            cors = self.measure_correlation()
-            if cors is not None:
-                self.save_correlation(cors, time, prefix)
+            self.save_correlation(self.measure_correlation(), time, prefix)
         if self.inp.tm_params.to_calculate:
             self.save_correlation_length(self.measure_transfer_matrix(), time, prefix)
         energy = self.save_density(vals, two, multi, time, prefix)

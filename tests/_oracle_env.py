@@ -110,6 +110,10 @@ class OracleEnvironment:
         self.Tn[source], self.Tn[tg] = a.transpose(k), b.transpose(k)
         return it, conv
 
+    def correlation_strip(self, left, vertical, r_max, left_op, right_ops):
+        return np.array(O.correlation_strip(self.env, self.Tn, self.lat, left, vertical, r_max, left_op,
+                                            right_ops))
+
     def move(self, direction, line):
         fn = (O.left_move, O.right_move, O.top_move, O.bottom_move)[direction]
         fn(self.env, self.Tn, line, self.p, self.lat)

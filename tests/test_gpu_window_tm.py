@@ -91,3 +91,27 @@ def test_bond_rdm_reproduces_op12(is_complex):
                     oe.eTr[bottom], oe.eTb[bottom], oe.eTl[bottom], oe.eTl[top], Tn[top], Tn[bottom], o)
             assert abs(np.sum(op * rho) - ref) <= 1e-10 * abs(ref), (source, dx, dy)
     ge.close()
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_correlation_strip(is_complex):
+    """tg_measure_correlation (StartCorrelation / Transfer / FinishCorrelation)
+    against the oracle's strip for r = 1..5 in both directions, and against
+    the GPU's own windows for r <= 3."""
+    lat, Tn, oe, ge = _setup(is_complex)
+    ops = [SZ, SX]
+    for left in range(lat.N_UNIT):
+        for vertical in (False, True):
+            strip = ge.correlation_strip(left, vertical, 5, SZ, lambda s: ops)
+            ref = O.correlation_strip(oe, Tn, lat, left, vertical, 5, SZ, lambda s: ops)
+            np.testing.assert_allclose(strip, np.array(ref), rtol=1e-10, atol=1e-13)
+            for r in range(1, 4):
+                if vertical:
+                    geo, pl, pr = (r + 1, 1, r, 0), (r, 0), (0, 0)
+                else:
+                    geo, pl, pr = (1, r + 1, 0, 0), (0, 0), (0, r)
+                n = ge.contract_window(left, *geo)
+                for k, op in enumerate(ops):
+                    w = ge.contract_window(left, *geo, {pl: SZ, pr: op}) / n
+                    assert abs(strip[r - 1][k] - w) <= 1e-10 * max(1.0, abs(w))
+    ge.close()
