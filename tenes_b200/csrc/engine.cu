@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <numeric>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -2105,19 +2106,28 @@ struct EngineT final : Engine {
   }
 
   // ------------------------------------------------------- full update
-  // Eigendecomposition of a real symmetric row-major n x n matrix (cuSOLVER
-  // syevd): ascending w on the host, Z (n x n, column j the eigenvector of
-  // w_j).  A symmetric matrix reads the same in either storage order; the
-  // column-major eigenvectors read row-major are Z^T.
+  // Eigendecomposition of a Hermitian row-major n x n matrix H (cuSOLVER
+  // syevd / heevd): ascending w on the host, Z (n x n, column j the
+  // eigenvector of w_j).  Read column-major the buffer is H^T = conj(H), whose
+  // eigenvectors are conj(z_j); the column-major eigenvectors read row-major
+  // are therefore Z^T (real) or Z^H (complex).
   void eigh(const DT<T>& A, int64_t n, std::vector<double>& w, DT<T>& Z) {
+    DT<T> a = clone(A, st);
+    DT<double> wd({n}, st);
+    const int in = static_cast<int>(n);
+    int lwork = 0;
+    ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 9.0 * static_cast<double>(n) * n * n, 0.0);
     if constexpr (CPLX) {
-      fail(TG_E_RUNTIME, "eigh: real matrices only");
+      auto* ap = reinterpret_cast<cuDoubleComplex*>(a.p);
+      check_sol(cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
+                                            &lwork),
+                "Zheevd_bufferSize");
+      DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
+      check_sol(cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
+                                 reinterpret_cast<cuDoubleComplex*>(work.p), lwork, info_slot()),
+                "Zheevd");
+      Z = transpose<T>(reshape(a, {n, n}), {1, 0}, st, true);
     } else {
-      DT<T> a = clone(A, st);
-      DT<double> wd({n}, st);
-      const int in = static_cast<int>(n);
-      int lwork = 0;
-      ProfScope ps(PK_SOLVER, st, 9.0 * static_cast<double>(n) * n * n, 0.0);
       check_sol(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in,
                                             wd.p, &lwork),
                 "Dsyevd_bufferSize");
@@ -2126,10 +2136,10 @@ struct EngineT final : Engine {
                                  lwork, info_slot()),
                 "Dsyevd");
       Z = tr(reshape(a, {n, n}), {1, 0});
-      w.resize(static_cast<size_t>(n));
-      TG_CUDA(cudaMemcpyAsync(w.data(), wd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-      TG_CUDA(cudaStreamSynchronize(st));
     }
+    w.resize(static_cast<size_t>(n));
+    TG_CUDA(cudaMemcpyAsync(w.data(), wd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
   }
 
   // Backend of full_update.hpp on this engine's device tensors: products and
@@ -2137,16 +2147,26 @@ struct EngineT final : Engine {
   // leg scaling through scale_leg, slicing as a product with a 0/1 matrix.
   struct FuBackend {
     using Ten = DT<T>;
+    using Scalar = std::conditional_t<CPLX, std::complex<double>, double>;
     EngineT* e;
     static const Shape& shape(const Ten& t) { return t.sh; }
+    Ten conj(const Ten& a) {
+      if constexpr (CPLX) {
+        V id(static_cast<size_t>(a.rank()));
+        std::iota(id.begin(), id.end(), 0);
+        return transpose<T>(a, id, e->st, true);
+      } else {
+        return a;
+      }
+    }
     Ten td(const Ten& a, const Ten& b, const V& x, const V& y, int) { return e->td(a, b, x, y); }
     Ten tr(const Ten& a, const V& q) { return e->tr(a, q); }
     Ten reshape(const Ten& a, const Shape& s) { return tg::reshape(a, s); }
     void axpy(Ten& y, const Ten& x, double alpha) { tg::axpy<T>(y.p, x.p, alpha, y.size(), e->st); }
     void scale(Ten& x, double alpha) { tg::scale<T>(x.p, x.size(), alpha, e->st); }
-    double scalar(const Ten& t) {
+    Scalar scalar(const Ten& t) {
       const T v = e->scalar(t);
-      if constexpr (CPLX) return v.x;
+      if constexpr (CPLX) return {v.x, v.y};
       else return v;
     }
     void qr_matrix(const Ten& M, Ten& Q, Ten& R) { e->qr(M, M.dim(0), M.dim(1), Q, R); }
@@ -2183,9 +2203,7 @@ struct EngineT final : Engine {
   // are replaced, the environment is left to the caller's moves
   void fu_bond(int source, int leg, const double* op, const tg_fu_params* fp, int* iterations,
                int* converged) override {
-    if constexpr (CPLX) {
-      fail(TG_E_INPUT, "full update: real site tensors only");
-    } else {
+    {
       require_env();
       check_site(source);
       if (leg < 0 || leg > 3) fail(TG_E_INPUT, "source_leg must be 0..3");

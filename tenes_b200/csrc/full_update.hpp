@@ -1,5 +1,5 @@
 // Full update of one bond (core::Full_update_bond, src/iTPS/core/full_update.cpp:31-455)
-// over a tensor backend BK, real tensors.
+// over a tensor backend BK, real or complex tensors (BK::Scalar).
 //
 // The bond (Tn1 leg 2 -- Tn2 leg 0 after rotation) is updated by:
 //   1. QR splits Tn1 = Q1 R1 over (0,1,3 | 2,4), Tn2 = Q2 R2 over (1,2,3 | 0,4);
@@ -17,14 +17,16 @@
 //   5. the gauge removed, R1, R2 balanced through QR + SVD of r1 r2^T with the
 //      bond weights normalised, and the new tensors put back together.
 //
-// The backend supplies tensordot / transpose / reshape / axpy / scale, leg
-// slicing and scaling by host vectors, and thin matrix QR (Householder, R on
-// LAPACK's sign convention), SVD and Hermitian eigendecomposition (ascending)
-// of row-major matrices.  Tests instantiate it on host tensors; no CUDA code
-// in this header.
+// The backend supplies tensordot / transpose / reshape / conj / axpy / scale,
+// leg slicing and scaling by host vectors, and thin matrix QR, SVD and
+// Hermitian eigendecomposition (ascending) of row-major matrices.  The
+// result does not depend on the sign / phase conventions of these
+// factorisations beyond a gauge on the updated bond.  Tests instantiate it
+// on host tensors; no CUDA code in this header.
 #pragma once
 
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <utility>
 #include <vector>
@@ -52,8 +54,11 @@ struct Stats {
 template <class BK>
 struct FullUpdate {
   using Ten = typename BK::Ten;
+  using S = typename BK::Scalar;  // double or std::complex<double>
   BK& bk;
   Params p;
+
+  Ten cj(const Ten& a) { return bk.conj(a); }
 
   Ten td(const Ten& a, const Ten& b, const Axes& x, const Axes& y) { return bk.td(a, b, x, y, 0); }
   Ten tr(const Ten& a, const Axes& q) { return bk.tr(a, q); }
@@ -102,7 +107,7 @@ struct FullUpdate {
     bk.eigh_matrix(M, w, Z);
     Z = bk.reshape(Z, cat(rs, {static_cast<int64_t>(w.size())}));
   }
-  double trace(const Ten& A, const Ten& B, const Axes& x, const Axes& y) { return bk.scalar(td(A, B, x, y)); }
+  S trace(const Ten& A, const Ten& B, const Axes& x, const Axes& y) { return bk.scalar(td(A, B, x, y)); }
 
   // the transposed pseudo-inverse conj(u s^-1) conj(vt) of A = u s vt (:158-184)
   Ten pinv_t(const Ten& A) {
@@ -111,7 +116,7 @@ struct FullUpdate {
     bk.svd_matrix(A, u, s, vt);
     std::vector<double> si(s.size());
     for (size_t i = 0; i < s.size(); ++i) si[i] = s[i] / s[0] > p.inverse_env_cut ? 1.0 / s[i] : 0.0;
-    return td(bk.mulvec(u, si, 1), vt, {1}, {0});
+    return td(cj(bk.mulvec(u, si, 1)), cj(vt), {1}, {0});
   }
 
   // Create_Environment_two_sites (:50-83), legs (t1, t2, tc1, tc2)
@@ -119,22 +124,22 @@ struct FullUpdate {
                   const Ten& eT3, const Ten& eT4, const Ten& eT5, const Ten& eT6, const Ten& Q1, const Ten& Q2) {
     const Ten right =
         td(td(C2, eT2, {0}, {1}),
-           td(td(td(td(C3, eT4, {1}, {0}), eT3, {0}, {1}), Q2, {2, 5}, {3, 2}), Q2, {1, 3}, {3, 2}), {0, 2, 3},
+           td(td(td(td(C3, eT4, {1}, {0}), eT3, {0}, {1}), cj(Q2), {2, 5}, {3, 2}), Q2, {1, 3}, {3, 2}), {0, 2, 3},
            {1, 5, 3});
     const Ten left =
         td(td(C1, eT1, {1}, {0}),
-           td(td(td(td(C4, eT6, {1}, {0}), eT5, {0}, {1}), Q1, {2, 5}, {0, 2}), Q1, {1, 3}, {0, 2}), {0, 2, 3},
+           td(td(td(td(C4, eT6, {1}, {0}), eT5, {0}, {1}), cj(Q1), {2, 5}, {0, 2}), Q1, {1, 3}, {0, 2}), {0, 2, 3},
            {0, 4, 2});
     return tr(td(right, left, {0, 1}, {0, 1}), {3, 1, 2, 0});
   }
 
   // -2 <R1 R2|E|Theta> + <R1 R2|E|R1 R2> (:238-254)
-  double delta(const Ten& E, const Ten& Theta, const Ten& R1, const Ten& R2) {
+  S delta(const Ten& E, const Ten& Theta, const Ten& R1, const Ten& R2) {
     const Ten ET = td(E, Theta, {0, 1}, {0, 1});
-    const double a = trace(td(ET, R2, {1, 3}, {0, 2}), R1, {0, 1, 2}, {0, 2, 1});
-    const double b =
-        trace(R1, td(R2, td(E, td(R1, R2, {1}, {1}), {2, 3}, {0, 2}), {0, 2}, {1, 3}), {0, 1, 2}, {1, 0, 2});
-    return -2.0 * a + b;
+    const S a = trace(td(ET, cj(R2), {1, 3}, {0, 2}), cj(R1), {0, 1, 2}, {0, 2, 1});
+    const S b = trace(R1, td(R2, td(E, td(cj(R1), cj(R2), {1}, {1}), {2, 3}, {0, 2}), {0, 2}, {1, 3}), {0, 1, 2},
+                      {1, 0, 2});
+    return S(-2.0) * a + b;
   }
   // R = N^+ W with N^+ the pseudo-inverse of the Hermitian normal matrix (:276-296)
   Ten solve(const Ten& N, const Ten& W) {
@@ -143,7 +148,7 @@ struct FullUpdate {
     svd(N, {1, 3}, {0, 2}, U, s, VT);
     std::vector<double> si(s.size());
     for (size_t i = 0; i < s.size(); ++i) si[i] = s[i] / s[0] > p.inverse_precision ? 1.0 / s[i] : 0.0;
-    const Ten Ninv = td(bk.mulvec(U, si, 2), VT, {2}, {0});
+    const Ten Ninv = td(cj(bk.mulvec(U, si, 2)), cj(VT), {2}, {0});
     return td(Ninv, W, {0, 1}, {0, 2});
   }
 
@@ -161,7 +166,7 @@ struct FullUpdate {
     Ten Theta = td(td(R1, R2, {1}, {1}), op12, {1, 3}, {0, 1});
     Ten E = environment(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, Q1, tr(Q2, {3, 0, 1, 2}));
     {  // Hermitise
-      Ten Et = tr(E, {2, 3, 0, 1});
+      Ten Et = cj(tr(E, {2, 3, 0, 1}));
       bk.axpy(Et, E, 1.0);
       bk.scale(Et, 0.5);
       E = Et;
@@ -180,9 +185,9 @@ struct FullUpdate {
       LR1_inv = pinv_t(LR1);
       LR2_inv = pinv_t(LR2);
       Z = td(td(Z, LR1_inv, {0}, {1}), LR2_inv, {0}, {1});
-      E = td(Z, Z, {0}, {0});
+      E = td(Z, cj(Z), {0}, {0});
     } else {
-      E = td(Z, Z, {2}, {2});
+      E = td(Z, cj(Z), {2}, {2});
     }
     // initial guess: SVD of Theta truncated to Dc, weights sqrt(s / |s|)
     Ten U, VT;
@@ -204,17 +209,17 @@ struct FullUpdate {
     VT = bk.mulvec(VT, std::vector<double>(lam.begin(), lam.begin() + kc), 0);
     R1 = tr(U, {0, 2, 1});   // (envR1, Dc, m1)
     R2 = tr(VT, {1, 0, 2});  // (envR2, Dc, m2)
-    const double C_phi = trace(td(E, Theta, {0, 1}, {0, 1}), Theta, {0, 1, 2, 3}, {0, 1, 2, 3});
-    double old = delta(E, Theta, R1, R2);
+    const S C_phi = trace(td(E, Theta, {0, 1}, {0, 1}), cj(Theta), {0, 1, 2, 3}, {0, 1, 2, 3});
+    S old = delta(E, Theta, R1, R2);
     while (!st.converged && st.iterations < p.max_iteration) {
-      Ten W = td(td(E, Theta, {0, 1}, {0, 1}), R2, {1, 3}, {0, 2});
-      Ten N = td(td(E, R2, {1}, {0}), R2, {2, 4}, {0, 2});
+      Ten W = td(td(E, Theta, {0, 1}, {0, 1}), cj(R2), {1, 3}, {0, 2});
+      Ten N = td(td(E, R2, {1}, {0}), cj(R2), {2, 4}, {0, 2});
       R1 = solve(N, W);
-      W = td(td(E, Theta, {0, 1}, {0, 1}), R1, {0, 2}, {0, 2});
-      N = td(td(E, R1, {0}, {0}), R1, {1, 4}, {0, 2});
+      W = td(td(E, Theta, {0, 1}, {0, 1}), cj(R1), {0, 2}, {0, 2});
+      N = td(td(E, R1, {0}, {0}), cj(R1), {1, 4}, {0, 2});
       R2 = solve(N, W);
-      const double d = delta(E, Theta, R1, R2);
-      if (std::fabs(old - d) / std::fabs(C_phi) < p.convergence_epsilon) st.converged = true;
+      const S d = delta(E, Theta, R1, R2);
+      if (std::abs(old - d) / std::abs(C_phi) < p.convergence_epsilon) st.converged = true;
       old = d;
       ++st.iterations;
     }

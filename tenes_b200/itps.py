@@ -8,9 +8,8 @@ twosite_obs.cpp:288-340, multisite_obs.cpp:250-300, correlation_length.cpp:57-12
 density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
 of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 
-Out of scope (raises InputError): full update of complex tensors and
-full-update time evolution, finite-temperature mode, the mean-field
-environment.
+Out of scope (raises InputError): full-update time evolution,
+finite-temperature mode, the mean-field environment.
 Long-range correlation functions ([correlation]) are measured through window
 contractions up to r = 3 and through the strip contraction beyond.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
@@ -119,8 +118,6 @@ class ITPS:
 
     def optimize(self) -> None:
         """optimize() (optimize.cpp:24-37): simple update, then full update."""
-        if self.p.num_full_step[0] > 0 and not self.is_real:
-            raise InputError("full update: real tensors only in this library (parameter.general.is_real = true)")
         t = _time.perf_counter()
         nsteps = self.p.num_simple_step[0]
         for _ in range(nsteps):

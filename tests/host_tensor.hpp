@@ -231,6 +231,8 @@ void jacobi_eigh(const std::vector<double>& A, int64_t n, std::vector<double>& w
 
 struct HostBackend {
   using Ten = HT;
+  using Scalar = double;
+  Ten conj(const Ten& a) { return a; }
   static const Shape& shape(const Ten& t) { return t.sh; }
   static bool empty(const Ten& t) { return !t.d; }
 

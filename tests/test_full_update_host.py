@@ -38,11 +38,15 @@ def fu_exe(tmp_path_factory):
 
 
 def run_host(exe, tensors, connect):
-    parts = []
+    cplx = any(np.iscomplexobj(t) for t in tensors)
+    parts = ["complex" if cplx else "real"]
     for t in tensors:
-        t = np.asarray(t, dtype=np.float64)
-        parts.append(f"{t.ndim} " + " ".join(str(d) for d in t.shape) + " "
-                     + " ".join(repr(float(x)) for x in t.reshape(-1)))
+        t = np.asarray(t, dtype=np.complex128 if cplx else np.float64)
+        if cplx:
+            vals = " ".join(f"{float(x.real)!r} {float(x.imag)!r}" for x in t.reshape(-1))
+        else:
+            vals = " ".join(repr(float(x)) for x in t.reshape(-1))
+        parts.append(f"{t.ndim} " + " ".join(str(d) for d in t.shape) + " " + vals)
     parts.append(str(connect))
     out = subprocess.run([exe], input="\n".join(parts) + "\n", capture_output=True, text=True,
                          check=True).stdout.splitlines()
@@ -52,7 +56,8 @@ def run_host(exe, tensors, connect):
         w = ln.split()
         r = int(w[1])
         shape = tuple(int(x) for x in w[2:2 + r])
-        res.append(np.array([float(x) for x in w[2 + r:]]).reshape(shape))
+        v = np.array([float(x) for x in w[2 + r:]])
+        res.append((v[0::2] + 1j * v[1::2] if cplx else v).reshape(shape))
     return int(st[1]), bool(int(st[2])), res[0], res[1]
 
 
@@ -78,21 +83,25 @@ def test_known_answer_inputs(fu_exe):
     np.testing.assert_allclose(pair(a, b, 2), pair(ra, rb, 2), rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("is_complex", [False, True])
 @pytest.mark.parametrize("leg", [0, 1, 2, 3])
-def test_bond_in_a_ctm_environment(fu_exe, leg):
+def test_bond_in_a_ctm_environment(fu_exe, leg, is_complex):
     """Each bond direction of a 2x2 cell in the environment of a few CTMRG
     sweeps (random D = 2 tensors, chi = 4), with exp(-0.1 H) of the
-    Heisenberg bond."""
-    rng = np.random.default_rng(31 + leg)
+    Heisenberg bond; real and complex tensors."""
+    rng = np.random.default_rng(31 + leg + 10 * is_complex)
     lat = O.Lattice(2, 2)
     lat.physical_dims = [2] * 4
     lat.virtual_dims = [[2] * 4 for _ in range(4)]
     Tn = [rng.standard_normal((2, 2, 2, 2, 2)) for _ in range(4)]
+    if is_complex:
+        Tn = [t + 1j * rng.standard_normal(t.shape) for t in Tn]
     p = O.Params(CHI=4)
     env = O.init_env(Tn, p, lat)
     for _ in range(3):
         O.sweep(env, Tn, p, lat)
-    op = evolution_twosite(heisenberg_bond(1.0), 0.1).real
+    op = evolution_twosite(heisenberg_bond(1.0), 0.1)
+    op = op if is_complex else op.real
     source = 1
     tgt = lat.neighbor(source, leg)
     args = O.full_update_env_args(env, source, leg, lat)
