@@ -18,8 +18,9 @@ tree at run time:
 * afh_real_input.toml / afh_real_expected.json <- test/data/AntiferroHeisenberg_real.toml and
   output_AntiferroHeisenberg_real/{density,onesite_obs,twosite_obs,multisite_obs_4,correlation,
   correlation_length}.dat (simple update + one full-update step + CTMRG)
-* {j1j2_afh,honeycomb,honeycomb_skew,afh_complex}_{input.toml,expected.json} <- J1J2_AFH,
-  Honeycomb, Honeycomb_skew and AntiferroHeisenberg_complex in the same form
+* {j1j2_afh,honeycomb,honeycomb_skew,afh_complex,rsvd}_{input.toml,expected.json} <- J1J2_AFH,
+  Honeycomb, Honeycomb_skew, AntiferroHeisenberg_complex and RSVD (complex, rSVD up/down
+  projectors) in the same form
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
 """
@@ -94,7 +95,7 @@ def main(ref):
 
     # further ground states with full-update steps
     for name, stem in (("J1J2_AFH", "j1j2_afh"), ("Honeycomb", "honeycomb"), ("Honeycomb_skew", "honeycomb_skew"),
-                       ("AntiferroHeisenberg_complex", "afh_complex")):
+                       ("AntiferroHeisenberg_complex", "afh_complex"), ("RSVD", "rsvd")):
         shutil.copyfile(os.path.join(data, name + ".toml"), os.path.join(HERE, stem + "_input.toml"))
         out = os.path.join(data, "output_" + name)
         exp = {}

@@ -1,9 +1,9 @@
 """Ground state with a full-update step through the front end
 (optimize.cpp:24-37, full_update.cpp:30-186) over the oracle-backed stand-in
-of the environment, against the reference's AntiferroHeisenberg_real and
-AntiferroHeisenberg_complex goldens (100 simple-update steps, one full-update
-step with the fast full update's single moves, CTMRG chi = 5, observables,
-correlations)."""
+of the environment, against the reference's AntiferroHeisenberg_real,
+AntiferroHeisenberg_complex and RSVD goldens (100 simple-update steps, one
+full-update step with the fast full update's single moves, CTMRG chi = 5 with
+full-SVD or rSVD projectors, observables, correlations)."""
 
 import json
 import os
@@ -32,7 +32,7 @@ def _density(path):
     return d
 
 
-@pytest.mark.parametrize("stem", ["afh_real", "afh_complex"])
+@pytest.mark.parametrize("stem", ["afh_real", "afh_complex", "rsvd"])
 def test_afh_full_update_driver_on_oracle(tmp_path, monkeypatch, stem):
     import tenes_b200.itps as itps
     from tests._oracle_env import OracleEnvironment

@@ -5,7 +5,7 @@
   environment, for every bond direction and for real and complex tensors: the
   bond-contracted pair Tn1_new . Tn2_new (free of the gauge on the updated
   bond) and the least-squares iteration count;
-* the reference's AntiferroHeisenberg_real and _complex inputs through
+* the reference's AntiferroHeisenberg_real, _complex and RSVD inputs through
   ``python -m tenes_b200`` (simple update, one full-update step with the fast
   full update's moves, CTMRG, observables) against their golden files, checked
   the way the reference checks them (test/fulltest.py.in: rtol 1e-3, atol 1e-4)."""
@@ -72,7 +72,7 @@ def _rows(path):
     return out
 
 
-@pytest.mark.parametrize("stem", ["afh_real", "afh_complex"])
+@pytest.mark.parametrize("stem", ["afh_real", "afh_complex", "rsvd"])
 def test_afh_full_update_golden(tmp_path, stem):
     r = subprocess.run([sys.executable, "-m", "tenes_b200", os.path.join(GOLDEN, f"{stem}_input.toml"),
                         "--outdir", str(tmp_path), "--quiet"], cwd=REPO, capture_output=True, text=True,

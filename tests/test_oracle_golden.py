@@ -137,16 +137,18 @@ def test_te_tfi_golden():
 # observed deviation from the golden files: 1.4e-14 (afh_real), 1.5e-14
 # (afh_complex), 1.2e-12 (honeycomb), 2.3e-6 (j1j2_afh, whose full-update
 # gates change a site's physical dimension 2 -> 8 -> 2 along the sequence),
-# 2.4e-5 (honeycomb_skew, the one skewed cell); all inside the reference's own
-# check (rtol 1e-3, atol 1e-4)
+# 2.4e-5 (honeycomb_skew, the one skewed cell), 7e-15 (rsvd: rSVD up/down
+# projectors at chi = 5, where k = 2 chi covers the rank of the projected
+# matrices, so the random test matrix does not show); all inside the
+# reference's own check (rtol 1e-3, atol 1e-4)
 FU_GOLDEN_TOL = {"afh_real": 1e-11, "afh_complex": 1e-11, "honeycomb": 1e-10, "j1j2_afh": 1e-5,
-                 "honeycomb_skew": 1e-4}
+                 "honeycomb_skew": 1e-4, "rsvd": 1e-11}
 
 
 @pytest.mark.parametrize("stem", sorted(FU_GOLDEN_TOL))
 def test_full_update_pipeline_golden(stem):
     """test/data/{AntiferroHeisenberg_real, J1J2_AFH, Honeycomb,
-    Honeycomb_skew, AntiferroHeisenberg_complex}: simple-update steps,
+    Honeycomb_skew, AntiferroHeisenberg_complex, RSVD}: simple-update steps,
     full-update steps (fast full update: single moves after every bond,
     src/iTPS/full_update.cpp:30-186, preceded by a full CTMRG), then CTMRG
     and the observables (onesite_obs, twosite_obs, multisite_obs_4 and the
