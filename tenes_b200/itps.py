@@ -8,8 +8,8 @@ twosite_obs.cpp:288-340, multisite_obs.cpp:250-300, correlation_length.cpp:57-12
 density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
 of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
 
-Out of scope (raises InputError): full-update time evolution,
-finite-temperature mode, the mean-field environment.
+Out of scope (raises InputError): finite-temperature mode, the mean-field
+environment.
 Long-range correlation functions ([correlation]) are measured through window
 contractions up to r = 3 and through the strip contraction beyond.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
@@ -557,28 +557,32 @@ class ITPS:
         return energy
 
     def time_evolution(self) -> None:
-        """iTPS::time_evolution (time_evolution.cpp:21-90), simple-update based."""
+        """iTPS::time_evolution (time_evolution.cpp:21-90) with the group
+        checks of iTPS.cpp:217-306: simple-update steps when
+        simple_update.num_step > 0, else full-update steps (each followed by
+        the fast full update's moves or a full CTMRG, as in the ground state)."""
         p = self.p
-        if p.num_simple_step[0] <= 0:
-            raise InputError("full-update time evolution is not part of this library")
-        if p.num_full_step[0] > 0:
+        if p.num_simple_step[0] > 0 and p.num_full_step[0] > 0:
             raise InputError("While mode is not ground state calculation,\n"
                              "       simple update and full update are both required.")
-        groups = {u.group for u in self.inp.simple_updates}
+        su = p.num_simple_step[0] > 0
+        kind = "simple" if su else "full"
+        ups = self.inp.simple_updates if su else self.inp.full_updates
+        groups = {u.group for u in ups}
         ngroups = max(groups) + 1 if groups else 1
         for g in range(ngroups):
             if groups and g not in groups:
-                raise InputError(f"no simple update with group number {g}")
+                raise InputError(f"no {kind} update with group number {g}")
 
         def per_group(v: List, what: str) -> List:
             if len(v) == ngroups:
                 return list(v)
             if len(v) == 1:
                 return list(v) * ngroups
-            raise InputError(f"size of {what} {len(v)} is not equal to the number of simple update groups.")
+            raise InputError(f"size of {what} {len(v)} is not equal to the number of {kind} update groups.")
 
-        nss = per_group(p.num_simple_step, "num_step")
-        tau = per_group(p.tau_simple_step, "tau")
+        nss = per_group(p.num_simple_step if su else p.num_full_step, "num_step")
+        tau = per_group(p.tau_simple_step if su else p.tau_full_step, "tau")
         mi = list(p.measure_interval)
         while len(mi) < ngroups:
             mi.append(mi[-1])
@@ -587,9 +591,17 @@ class ITPS:
         for g in range(ngroups):
             for step in range(nss[g]):
                 t0 = _time.perf_counter()
-                self.simple_update_step(g)
+                if su:
+                    self.simple_update_step(g)
+                else:
+                    for up in ups:
+                        if up.group == g:
+                            self.full_update_op(up)
                 self.env.sync()
-                self.t_su += _time.perf_counter() - t0
+                if su:
+                    self.t_su += _time.perf_counter() - t0
+                else:
+                    self.t_fu += _time.perf_counter() - t0
                 t += tau[g]
                 if (step + 1) % mi[g] == 0:
                     self.measure(t, "TE_")
