@@ -99,3 +99,18 @@ def test_afh_full_update_golden(tmp_path, stem):
         res, ref = _rows(tmp_path / name), exp[key]
         assert len(res) == len(ref), name
         np.testing.assert_allclose(np.array(res), np.array(ref), rtol=tol["rtol"], atol=tol["atol"], err_msg=name)
+
+
+def test_full_update_time_evolution_matches_ground_state_steps(tmp_path):
+    """Full-update time evolution on the GPU ends where the ground-state
+    driver with the same full-update steps ends (the CPU test of
+    tests/test_te_full_update.py, on the library)."""
+    import tenes_b200.itps as itps
+    from tests.test_te_full_update import NSTEP, TAU, _input, _rows
+    te = itps.run(_input(tmp_path, "te.toml", "time"), print_level=0, outdir=str(tmp_path / "te"))
+    gs = itps.run(_input(tmp_path, "gs.toml", "ground state"), print_level=0, outdir=str(tmp_path / "gs"))
+    one_te, one_gs = _rows(tmp_path / "te" / "TE_onesite_obs.dat"), _rows(tmp_path / "gs" / "onesite_obs.dat")
+    last = one_te[np.isclose(one_te[:, 0], NSTEP * TAU)][:, 1:]
+    np.testing.assert_allclose(last, one_gs, rtol=0, atol=1e-9)
+    for i in range(4):
+        np.testing.assert_allclose(te.env.get_site_tensor(i), gs.env.get_site_tensor(i), rtol=0, atol=1e-9)
