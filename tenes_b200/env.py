@@ -212,6 +212,13 @@ class Environment:
         nright = len(lists[0])
         if any(len(l) != nright for l in lists) or nright == 0:
             raise ValueError("correlation_strip: the same positive number of right operators on every site")
+        for i, l in enumerate(lists):
+            for o in l:
+                if np.shape(o) != (self.pdim[i],) * 2:
+                    raise ValueError(f"correlation_strip: operator of shape {np.shape(o)} on site {i} "
+                                     f"(physical dimension {self.pdim[i]})")
+        if np.shape(left_op) != (self.pdim[left],) * 2:
+            raise ValueError(f"correlation_strip: left operator of shape {np.shape(left_op)} on site {left}")
         flat = np.concatenate([np.ascontiguousarray(o, dtype=self.dtype).reshape(-1) for l in lists for o in l])
         flat = np.ascontiguousarray(flat, dtype=self.dtype)
         lop = np.ascontiguousarray(left_op, dtype=self.dtype)
