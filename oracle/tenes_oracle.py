@@ -1006,6 +1006,100 @@ def simple_update_bond(Tn1, Tn2, lambda1, lambda2, op12, connect1: int, p: Param
     return Tn1_new, Tn2_new, lam_c
 
 
+# local gauge fixing of the simple update: after the transpose of
+# local_gauge.cpp, leg `connect` of the contracted tensor goes back to its
+# place from the last position (the physical leg is 4th before it)
+_GAUGE_BACK = {0: (4, 0, 1, 2, 3), 1: (0, 4, 1, 2, 3), 2: (0, 1, 4, 2, 3), 3: (0, 1, 2, 4, 3)}
+
+
+def _inv_cut(v, cut):
+    v = np.asarray(v, dtype=float)
+    return np.where(v > cut, 1.0 / np.maximum(v, 1e-300), 0.0)
+
+
+def boundary_tensor(Tn, lam, connect: int, p: Params):
+    """boundary_tensor (src/iTPS/core/local_gauge.cpp:190-224): the site
+    tensor with the weights on its other three legs and the inverse weight on
+    `connect`, contracted with its conjugate over every leg but `connect`:
+    M[a, b] = sum conj(T)[.., a, ..] T[.., b, ..]."""
+    T = Tn
+    for leg in range(4):
+        v = _inv_cut(lam[leg], p.Inverse_lambda_cut) if leg == connect else np.asarray(lam[leg], dtype=float)
+        T = _mulvec(T, v, leg)
+    rest = [l for l in range(5) if l != connect]
+    return td(cj(T), T, (rest, rest))
+
+
+def local_gauge_bond(Tn1, Tn2, lambda1, lambda2, connect1: int, p: Params):
+    """core::fix_local_gauge (src/iTPS/core/local_gauge.cpp:44-158): bring the
+    bond (Tn1 leg connect1, Tn2 leg connect1 + 2) to the gauge in which both
+    boundary tensors are the identity.  Returns Tn1_new, Tn2_new, lambda_c.
+
+    The eigenvalues of the boundary tensors are square-rooted and inverted
+    without a cutoff, and the inverse weight of Tn2 is gated on
+    lambda1[connect2] (local_gauge.cpp:136-142), both as the reference does."""
+    connect2 = (connect1 + 2) % 4
+    M1 = boundary_tensor(Tn1, lambda1, connect1, p)
+    M2 = boundary_tensor(Tn2, lambda2, connect2, p)
+    D1, U1 = np.linalg.eigh(M1)
+    D2, U2 = np.linalg.eigh(M2)
+    D1, D2 = np.sqrt(D1), np.sqrt(D2)
+    U1s = U1 * np.asarray(lambda1[connect1], dtype=float)[:, None] * D1[None, :]
+    U2s = U2 * np.asarray(lambda2[connect2], dtype=float)[:, None] * D2[None, :]
+    W1, lam_c, W2 = np.linalg.svd(td(cj(U1s), cj(U2s), ([0], [0])), full_matrices=False)
+    lam_c = np.sqrt(lam_c / math.sqrt(float(np.sum(lam_c * lam_c))))
+    W1 = W1 / D1[:, None]
+    W2 = W2 / D2[None, :]
+    l1 = np.asarray(lambda1[connect1], dtype=float)
+    inv1 = _inv_cut(l1, p.Inverse_lambda_cut)
+    T1 = td(_mulvec(Tn1, inv1, connect1), U1 @ W1, ([connect1], [0])).transpose(_GAUGE_BACK[connect1])
+    T1 = _mulvec(T1, lam_c, connect1)
+    gate = np.asarray(lambda1[connect2], dtype=float) > p.Inverse_lambda_cut
+    l2 = np.asarray(lambda2[connect2], dtype=float)
+    inv2 = np.where(gate, 1.0 / np.where(gate, l2, 1.0), 0.0)
+    T2 = td(_mulvec(Tn2, inv2, connect2), td(U2, W2, ([1], [1])), ([connect2], [0])).transpose(_GAUGE_BACK[connect2])
+    T2 = _mulvec(T2, lam_c, connect2)
+    return T1, T2, lam_c
+
+
+def gauge_score(Tn, lam, lat: "Lattice", p: Params) -> float:
+    """max |eigenvalue - 1| of every boundary tensor (the convergence check of
+    iTPS::fix_local_gauge, src/iTPS/simple_update.cpp:80-97)."""
+    score = 0.0
+    for site in range(lat.N_UNIT):
+        for leg in range(4):
+            if lat.virtual_dims[site][leg] <= 1:
+                continue
+            w = np.linalg.eigvalsh(boundary_tensor(Tn[site], lam[site], leg, p))
+            score = max(score, float(np.max(np.abs(w - 1.0))))
+    return score
+
+
+def fix_local_gauge(Tn, lam, lat: "Lattice", p: Params, maxiter: int = 100, eps: float = 1e-2):
+    """iTPS::fix_local_gauge (src/iTPS/simple_update.cpp:49-101): sweeps over
+    the bonds (sites of parity +1 then -1; source legs 2 then 1) until every
+    boundary tensor is within eps of the identity, at most maxiter sweeps.
+    Tn and lam are updated in place; returns (sweeps, score)."""
+    score = float("nan")
+    for it in range(maxiter):
+        for parity in (1, -1):
+            for sleg in (2, 1):
+                tleg = (sleg + 2) % 4
+                for s in range(lat.N_UNIT):
+                    if lat.parity(s) != parity or lat.virtual_dims[s][sleg] <= 1:
+                        continue
+                    t = lat.neighbor(s, sleg)
+                    T1, T2, lc = local_gauge_bond(Tn[s], Tn[t], lam[s], lam[t], sleg, p)
+                    lam[s][sleg] = lc
+                    lam[t][tleg] = lc
+                    Tn[s] = T1
+                    Tn[t] = T2
+        score = gauge_score(Tn, lam, lat, p)
+        if score < eps:
+            return it + 1, score
+    return maxiter, score
+
+
 # ---------------------------------------------------------------------------
 # Observables (src/iTPS/core/contract_itps_ctm/ctm.cpp)
 # ---------------------------------------------------------------------------
