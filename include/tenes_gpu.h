@@ -204,9 +204,21 @@ void tg_fu_params_default(tg_fu_params* p);
  * op is (d1, d2, d1, d2).  Replaces the two site tensors and leaves the
  * environment alone: the fast full update follows with tg_ctm_move on the
  * two lines of the bond (full_update.cpp:122-148).  *iterations and
- * *converged (optional) report the least-squares loop.  Real tensors. */
+ * *converged (optional) report the least-squares loop.  Real and complex
+ * tensors. */
 tg_status tg_fu_bond(tg_ctx* ctx, int source, int source_leg, const double* op, const tg_fu_params* params,
                      int* iterations, int* converged);
+
+/* iTPS::fix_local_gauge (src/iTPS/simple_update.cpp:49-101, with
+ * core::fix_local_gauge and boundary_tensor, src/iTPS/core/local_gauge.cpp:44-224):
+ * sweeps over the bonds (sites of parity +1, then -1; source legs 2, then 1;
+ * legs of dimension 1 skipped) that bring each bond to the gauge in which both
+ * boundary tensors are the identity, until the largest |eigenvalue - 1| of the
+ * boundary tensors is below eps, at most maxiter sweeps.  Updates the site
+ * tensors and the simple-update weights (inverse weights cut at the context's
+ * inverse_lambda_cut).  *sweeps and *score (optional) report the sweeps done
+ * and the last score. */
+tg_status tg_su_fix_gauge(tg_ctx* ctx, int maxiter, double eps, int* sweeps, double* score);
 
 /* iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137): per site,
  * Tn[0,0,0,0,:] = initial state (random when all entries are zero) and every

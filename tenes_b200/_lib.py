@@ -28,7 +28,7 @@ EXPORTED = [
     "tg_su_onesite", "tg_su_bond", "tg_init_tensors", "tg_sync", "tg_measure_window",
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
-    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_measure_correlation",
+    "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_su_fix_gauge", "tg_measure_correlation",
 ]
 
 
@@ -109,6 +109,7 @@ def load() -> C.CDLL:
         "tg_su_bond": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "tg_fu_params_default": (None, [P(FuParams)]),
         "tg_fu_bond": (C.c_int, [vp, C.c_int, C.c_int, dp, P(FuParams), P(C.c_int), P(C.c_int)]),
+        "tg_su_fix_gauge": (C.c_int, [vp, C.c_int, C.c_double, P(C.c_int), P(C.c_double)]),
         "tg_init_tensors": (C.c_int, [vp, C.c_int, dp, P(C.c_int), dp]),
         "tg_sync": (C.c_int, [vp]),
         "tg_kernel_launch_count": (C.c_uint64, []),

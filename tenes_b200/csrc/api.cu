@@ -255,6 +255,9 @@ tg_status tg_fu_bond(tg_ctx* ctx, int source, int source_leg, const double* op, 
     E(ctx)->fu_bond(source, source_leg, op, params, iterations, converged);
   });
 }
+tg_status tg_su_fix_gauge(tg_ctx* ctx, int maxiter, double eps, int* sweeps, double* score) {
+  return guard([&] { E(ctx)->su_fix_gauge(maxiter, eps, sweeps, score); });
+}
 tg_status tg_sync(tg_ctx* ctx) {
   return guard([&] { E(ctx)->sync(); });
 }

@@ -20,6 +20,7 @@
 
 #include "adjoint_device.hpp"
 #include "full_update.hpp"
+#include "local_gauge.hpp"
 #include "dtensor.hpp"
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -2248,6 +2249,33 @@ struct EngineT final : Engine {
       if (iterations) *iterations = st_.iterations;
       if (converged) *converged = st_.converged ? 1 : 0;
     }
+  }
+
+  // iTPS::fix_local_gauge (src/iTPS/simple_update.cpp:49-101) over the
+  // engine's site tensors and simple-update weights; the bond step and the
+  // sweep are local_gauge.hpp's, on the same backend as the full update.
+  // Site parity (-1)^(x+y) as SquareLattice builds it (site 0 is +1).
+  void su_fix_gauge(int maxiter, double eps, int* sweeps, double* score) override {
+    if (maxiter < 0) fail(TG_E_INPUT, "gauge_maxiter must be non-negative");
+    PrecScope prec(this, 0);
+    FuBackend bk{this};
+    gauge::LocalGauge<FuBackend> g{bk, P.inverse_lambda_cut};
+    std::vector<DT<T>> tn(Tn.begin(), Tn.end());
+    std::vector<gauge::Weights> lam(lambda.begin(), lambda.end());
+    double sc = 0.0;
+    const int n = g.run(
+        tn, lam, lat.vdim, [&](int s, int leg) { return lat.neighbor(s, leg); },
+        [&](int s) { return ((s % lat.LX) + (s / lat.LX)) % 2 == 0 ? 1 : -1; }, maxiter, eps, &sc);
+    check_infos();
+    for (int i = 0; i < lat.N; ++i) {
+      if (tn[static_cast<size_t>(i)].sh != Tn[static_cast<size_t>(i)].sh)
+        fail(TG_E_RUNTIME, "local gauge fixing changed a site tensor's shape");
+      Tn[static_cast<size_t>(i)] = tn[static_cast<size_t>(i)];
+      lambda[static_cast<size_t>(i)] = lam[static_cast<size_t>(i)];
+      rot_ok[static_cast<size_t>(i)] = false;
+    }
+    if (sweeps) *sweeps = n;
+    if (score) *score = sc;
   }
 
   // ------------------------------------------------- energy gradient

@@ -40,6 +40,7 @@ struct Engine {
   virtual void su_bond(int source, int leg, const double* op) = 0;
   virtual void fu_bond(int source, int leg, const double* op, const tg_fu_params* params, int* iterations,
                        int* converged) = 0;
+  virtual void su_fix_gauge(int maxiter, double eps, int* sweeps, double* score) = 0;
   virtual void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) = 0;
   virtual void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
                            double svd_broadening, double* energy, double* grad) = 0;

@@ -331,6 +331,15 @@ class Environment:
                                   C.byref(it), C.byref(conv)))
         return it.value, bool(conv.value)
 
+    def fix_local_gauge(self, maxiter: int = 100, eps: float = 1e-2) -> Tuple[int, float]:
+        """iTPS::fix_local_gauge (src/iTPS/simple_update.cpp:49-101): sweeps of
+        core::fix_local_gauge over the bonds until every boundary tensor is
+        within eps of the identity (at most maxiter sweeps).  Returns the
+        sweeps done and the last score."""
+        n, sc = C.c_int(), C.c_double()
+        check(self.lib.tg_su_fix_gauge(self.ctx, int(maxiter), float(eps), C.byref(n), C.byref(sc)))
+        return n.value, sc.value
+
     def init_tensors(self, seed: int, initial_dirs: Sequence[Sequence[float]],
                      noises: Sequence[float]) -> None:
         """iTPS::initialize_tensors (src/iTPS/tensors.cpp:38-137)."""

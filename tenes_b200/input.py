@@ -28,6 +28,8 @@ class PEPSParameters:
     measure_interval: List[int] = field(default_factory=lambda: [10])
     Inverse_lambda_cut: float = 1e-12
     Simple_Gauge_Fix: bool = False
+    Simple_Gauge_maxiter: int = 100
+    Simple_Gauge_Convergence_Epsilon: float = 1e-2
     Inverse_projector_cut: float = 1e-12
     CTM_Convergence_Epsilon: float = 1e-6
     Max_CTM_Iteration: int = 100
@@ -213,6 +215,9 @@ def gen_param(param: dict) -> PEPSParameters:
             p.tau_simple_step = _as_list(s["tau"], float)
         p.Inverse_lambda_cut = float(s.get("lambda_cutoff", p.Inverse_lambda_cut))
         p.Simple_Gauge_Fix = bool(s.get("gauge_fix", p.Simple_Gauge_Fix))
+        p.Simple_Gauge_maxiter = int(s.get("gauge_maxiter", p.Simple_Gauge_maxiter))
+        p.Simple_Gauge_Convergence_Epsilon = float(s.get("gauge_convergence_epsilon",
+                                                         p.Simple_Gauge_Convergence_Epsilon))
     f = param.get("full_update")
     if f is not None:
         if "num_step" in f:

@@ -74,8 +74,6 @@ class ITPS:
             load_tensors(self.env, p.tensor_load_dir, p.CHI, print_level)
         else:
             self.env.init_tensors(p.seed, ls.initial_dirs, ls.noises)
-        if p.Simple_Gauge_Fix:
-            raise InputError("simple_update.gauge_fix is not part of this library")
         self.outdir = p.outdir
         os.makedirs(self.outdir, exist_ok=True)
         n1 = self._names(inp.onesite, "onesite", False)
@@ -110,11 +108,14 @@ class ITPS:
 
     # ----------------------------------------------------- simple update
     def simple_update_step(self, group: int = 0) -> None:
-        """One Trotter step: every op of `group` in input order (simple_update.cpp:113-119)."""
+        """One Trotter step: every op of `group` in input order (simple_update.cpp:113-119),
+        then the local gauge fixing when simple_update.gauge_fix is set."""
         for up in self.inp.simple_updates:
             if up.group != group:
                 continue
             self.env.simple_update(up.source_site, up.source_leg, self._op(up.op))
+        if self.p.Simple_Gauge_Fix:  # simple_update.cpp:121-124, time_evolution.cpp:59-62
+            self.env.fix_local_gauge(self.p.Simple_Gauge_maxiter, self.p.Simple_Gauge_Convergence_Epsilon)
 
     def optimize(self) -> None:
         """optimize() (optimize.cpp:24-37): simple update, then full update."""

@@ -81,6 +81,9 @@ class OracleEnvironment:
         self.lat.noises = list(noises)
         self.Tn = O.initialize_tensors(self.lat, seed, not self.is_complex)
 
+    def fix_local_gauge(self, maxiter=100, eps=1e-2):
+        return O.fix_local_gauge(self.Tn, self.lam, self.lat, self.p, maxiter, eps)
+
     def simple_update(self, source, leg, op):
         if leg < 0:
             self.Tn[source] = np.tensordot(self.Tn[source], op, ([4], [0]))

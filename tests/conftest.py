@@ -15,7 +15,7 @@ def pytest_configure(config):
 # The CTMRG path's parity and kernel tests run first; the rows built on top of
 # it (front end, gradients, full update, long-range correlations) follow, so
 # that a stop at the first failure (-x) still reports on the path itself.
-_LATE_FILES = ("test_gpu_frontend.py", "test_gpu_grad.py", "test_gpu_full_update.py")
+_LATE_FILES = ("test_gpu_frontend.py", "test_gpu_grad.py", "test_gpu_full_update.py", "test_gpu_local_gauge.py")
 
 
 def pytest_collection_modifyitems(session, config, items):

@@ -121,3 +121,28 @@ def test_host_template_matches_oracle(gauge_exe, is_complex, maxiter, eps):
     for i in range(lat.N_UNIT):
         for leg in range(4):
             np.testing.assert_allclose(h_lam[i][leg], lam[i][leg], rtol=1e-9, atol=1e-12)
+
+
+def test_front_end_fixes_the_gauge_after_each_step(tmp_path, monkeypatch):
+    """simple_update.gauge_fix = true through the front end (over the
+    oracle-backed environment): every simple-update step ends with the gauge
+    sweeps (simple_update.cpp:121-124), so the final state's boundary tensors
+    are within gauge_convergence_epsilon of the identity."""
+    import re
+
+    import tenes_b200.itps as itps
+    from tests._oracle_env import OracleEnvironment
+    monkeypatch.setattr(itps, "Environment", OracleEnvironment)
+    txt = open(os.path.join(ROOT, "tests", "golden", "te_tfi_input.toml")).read()
+    txt = txt.replace("mode = 'time'", "mode = 'ground state'")
+    txt = re.sub(r"\[parameter.simple_update\]\nnum_step = \d+",
+                 "[parameter.simple_update]\nnum_step = 5\ngauge_fix = true\ngauge_convergence_epsilon = 1e-6",
+                 txt)
+    txt = txt.replace("dimension = 10", "dimension = 4").replace("iteration_max = 10", "iteration_max = 2")
+    txt = txt.replace("noise = 0.0", "noise = 0.05")
+    txt = re.sub(r"\[correlation\].*?(?=\[observable\])", "", txt, flags=re.S)
+    (tmp_path / "in.toml").write_text(txt)
+    it = itps.run(str(tmp_path / "in.toml"), print_level=0, outdir=str(tmp_path / "out"))
+    assert it.p.Simple_Gauge_Fix and it.p.Simple_Gauge_Convergence_Epsilon == 1e-6
+    env = it.env
+    assert O.gauge_score(env.Tn, env.lam, env.lat, env.p) < 1e-6
