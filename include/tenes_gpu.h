@@ -320,14 +320,17 @@ tg_status tg_cholqr_host(int64_t n, int64_t k, double* Y, int passes, int* pivot
  * memory: device_mats is a HOST array of `count` DEVICE pointers (row-major
  * float64, or interleaved complex128 when is_complex), device_out is a device
  * buffer of count*n doubles.  Work is queued on `stream` (a cudaStream_t, NULL
- * for the legacy default stream); the call returns once it is queued.
+ * for the legacy default stream); the call returns once it is queued.  The
+ * pointer table is copied through a pageable staging array inside the call,
+ * so device_mats may be reused (or freed) as soon as the call returns,
+ * whether it is pageable or page-locked.
  *
  * It allocates nothing: the device-side copy of the pointer table goes into a
  * fixed 8 KiB array inside the library (at most 1024 matrices; n <= 160 real,
  * n <= 112 complex; larger requests fail with TG_E_INPUT).  Every GPU that
  * loads the library keeps that array until the process exits.  The first call
- * on each device looks up the array's device address (call it once before
- * any stream capture).  All calls share the array and it keeps the last
+ * on each device looks up the array's device address, so make that first call
+ * before any stream capture.  All calls share the array and it keeps the last
  * call's contents, so calls whose GPU work overlaps race on it: order them
  * on one stream, or synchronise between them. */
 tg_status tg_corner_spectra_noalloc(const void* const* device_mats, int count, int n, int is_complex,

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "counter_rng.cuh"
 #include "kernels.cuh"
@@ -479,16 +480,15 @@ size_t cholqr_smem_bytes(int kp) {
          sizeof(int) * static_cast<size_t>(nb * (nb + 1) / 2);
 }
 
-// cluster size the device runs this kernel with (16, else 8, else 0)
-int cholqr_cluster_size() {
-  static int cs = -1;
-  if (cs >= 0) return cs;
-  cs = 0;
+// cluster size the current device runs this kernel with (16, else 8, else
+// 0).  Both the attributes and the occupancy query belong to the current
+// device's context, so the answer is probed and kept per device.
+int probe_cluster_size() {
   const size_t smem = cholqr_smem_bytes(CQ_KPMAX);
   if (cudaFuncSetAttribute(cholqr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess) {
     cudaGetLastError();
-    return cs;
+    return 0;
   }
   cudaFuncSetAttribute(cholqr_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaGetLastError();
@@ -505,13 +505,24 @@ int cholqr_cluster_size() {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, cholqr_cluster_kernel, &cfg) == cudaSuccess && nclusters > 0) {
-      cs = c;
-      break;
-    }
+    if (cudaOccupancyMaxActiveClusters(&nclusters, cholqr_cluster_kernel, &cfg) == cudaSuccess && nclusters > 0)
+      return c;
     cudaGetLastError();
   }
-  return cs;
+  return 0;
+}
+
+int cholqr_cluster_size() {
+  static std::mutex mu;
+  static int cs[kMaxDevices];
+  static bool probed[kMaxDevices] = {};
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(mu);
+  if (!probed[dev]) {
+    cs[dev] = probe_cluster_size();
+    probed[dev] = true;
+  }
+  return cs[dev];
 }
 
 }  // namespace

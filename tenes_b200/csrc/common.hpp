@@ -45,6 +45,16 @@ inline void check_cuda(cudaError_t e, const char* what, const char* file, int li
 #define TG_CUDA(x) ::tg::check_cuda((x), #x, __FILE__, __LINE__)
 #define TG_CHECK_LAUNCH() ::tg::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
+// Raise the dynamic shared-memory limit of `kernel` on the current device to
+// at least `bytes`.  cudaFuncSetAttribute acts on the current device's
+// context only, so what has been set is remembered per (kernel, device),
+// under a lock shared by all host threads.
+void ensure_dynamic_smem(const void* kernel, size_t bytes);
+
+// Current device ordinal, checked against the per-device tables (64 devices).
+int current_device();
+constexpr int kMaxDevices = 64;
+
 // Number of kernels launched by this library (host-side counter).  Kernels
 // recorded into a CUDA graph are taken back off with uncount_launch and
 // counted again at every launch of the graph.

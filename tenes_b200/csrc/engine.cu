@@ -688,6 +688,15 @@ struct EngineT final : Engine {
       DT<T> t = mm_cm(lth, cm(Ycm.p, nrow, k));
       return mm_cm(lbh, cm(t.p, nmid, k));
     };
+    rsvd_run(apply_M, apply_MH, nrow, ncol, cut, k, Uc, Vc);
+  }
+
+  // The range finder, core SVD and truncation of rsvd_factors for any M
+  // given by its products: apply_M maps a column-major (ncol x k) panel to
+  // M times it (nrow x k, column-major), apply_MH the same for M^H.
+  template <typename FM, typename FMH>
+  void rsvd_run(FM&& apply_M, FMH&& apply_MH, int64_t nrow, int64_t ncol, int cut, int64_t k, DT<T>& Uc,
+                DT<T>& Vc) {
     DT<T> Om({k, ncol}, st);
     counter_normal<T>(Om.p, ncol, k, P.rsvd_seed, 0, st);
     stagger_wait();
@@ -805,14 +814,68 @@ struct EngineT final : Engine {
     }
   }
 
-  // Calc_projector_updown_blocks (ctm.cpp:320-491), full-SVD branch
+  // rSVD branch of Calc_projector_updown_blocks (ctm.cpp:401-439).  The
+  // matrix is M = RT^T LT LB RB over the row legs (t23,e34,tc23) of RT and
+  // the column legs (t23,e34,tc23) of RB -- the product Mult_col_ud applies
+  // (ctm.cpp:129-149) and R1 R2^T of the full-SVD branch -- and it is only
+  // ever applied to panels, four products at a time, never formed.  With the
+  // blocks as matrices (rows / columns = the legs named):
+  //   RTm: (t12,e12,tc12) x (t23,e34,tc23)    LTm: (t12,e12,tc12) x (t41,e78,tc41)
+  //   LBm: (t41,e78,tc41) x (t34,e56,tc34)    RBm: (t34,e56,tc34) x (t23,e34,tc23)
+  // the projectors are PU = LBm RBm V_c and PL = LTm^T RTm conj(U_c), each
+  // reshaped to (t41,e78,tc41,cut) and transposed (1,0,2,3) (ctm.cpp:434-439).
+  void proj_updown_rsvd(const DT<T>& LT, const DT<T>& RT, const DT<T>& RB, const DT<T>& LB, int64_t e34,
+                        int64_t t23, int64_t e78, int64_t t41, DT<T>& PU, DT<T>& PL) {
+    DT<T> RTm = tr(RT, {0, 3, 4, 1, 2, 5});
+    DT<T> LTm = tr(LT, {0, 2, 4, 1, 3, 5});
+    DT<T> LBm = tr(LB, {0, 2, 4, 1, 3, 5});
+    DT<T> RBm = tr(RB, {0, 2, 4, 1, 3, 5});
+    const int64_t na = RT.dim(0) * RT.dim(3) * RT.dim(4), n = RT.dim(1) * RT.dim(2) * RT.dim(5);
+    const int64_t nb = LT.dim(1) * LT.dim(3) * LT.dim(5), nc = LB.dim(1) * LB.dim(3) * LB.dim(5);
+    if (RB.dim(1) * RB.dim(3) * RB.dim(5) != n || LT.dim(0) * LT.dim(2) * LT.dim(4) != na)
+      fail(TG_E_RUNTIME, "proj_updown_rsvd: block shapes do not chain");
+    const MV rtm = rm(RTm.p, na, n), ltm = rm(LTm.p, na, nb), lbm = rm(LBm.p, nb, nc), rbm = rm(RBm.p, nc, n);
+    MV rtm_c = rtm;
+    rtm_c.conj = true;
+    // cut = min(chi, e34 t23^2), k = factor * cut (ctm.cpp:410-414)
+    const int cut = static_cast<int>(std::min<int64_t>(P.chi, e34 * t23 * t23));
+    int64_t k = P.rsvd_oversample_abs >= 0 ? cut + P.rsvd_oversample_abs
+                                           : static_cast<int64_t>(P.rsvd_oversampling_factor * cut);
+    k = std::min<int64_t>(k, n);
+    if (k > jacobi_svd_max_k<T>())
+      fail(TG_E_INPUT, "rSVD sketch size " + std::to_string(k) + " exceeds " +
+                           std::to_string(jacobi_svd_max_k<T>()) +
+                           " (lower rsvd_oversampling_factor or set rsvd_oversample_abs)");
+    auto apply_M = [&](const DT<T>& Xcm) {  // RTm^T (LTm (LBm (RBm X)))
+      DT<T> a = mm_cm(rbm, cm(Xcm.p, n, k));
+      DT<T> b = mm_cm(lbm, cm(a.p, nc, k));
+      a = mm_cm(ltm, cm(b.p, nb, k));
+      return mm_cm(tp(rtm), cm(a.p, na, k));
+    };
+    auto apply_MH = [&](const DT<T>& Ycm) {  // RBm^H (LBm^H (LTm^H (conj(RTm) Y)))
+      DT<T> a = mm_cm(rtm_c, cm(Ycm.p, n, k));
+      DT<T> b = mm_cm(ht(ltm), cm(a.p, na, k));
+      a = mm_cm(ht(lbm), cm(b.p, nb, k));
+      return mm_cm(ht(rbm), cm(a.p, nc, k));
+    };
+    DT<T> Uc, Vc;
+    rsvd_run(apply_M, apply_MH, n, n, cut, k, Uc, Vc);
+    const int64_t w = Uc.dim(1);
+    DT<T> t = mm_rm(rbm, rm(Vc.p, n, w));  // (nc x w)
+    PU = tr(reshape(mm_rm(lbm, rm(t.p, nc, w)), {t41, e78, t41, w}), {1, 0, 2, 3});
+    MV uc = rm(Uc.p, n, w);
+    uc.conj = true;
+    t = mm_rm(rtm, uc);  // (na x w)
+    PL = tr(reshape(mm_rm(tp(ltm), rm(t.p, na, w)), {t41, e78, t41, w}), {1, 0, 2, 3});
+  }
+
+  // Calc_projector_updown_blocks (ctm.cpp:320-491): full-SVD and rSVD branches
   void proj_updown(const DT<T>& C1, const DT<T>& C2, const DT<T>& C3, const DT<T>& C4, const DT<T>& eT1,
                    const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
                    const DT<T>& eT7, const DT<T>& eT8, const DT<T>& T1, const DT<T>& T2, const DT<T>& T3,
                    const DT<T>& T4, DT<T>& PU, DT<T>& PL) {
-    const int64_t e78 = eT7.dim(1);
+    const int64_t e78 = eT7.dim(1), e34 = eT3.dim(1);
     const int64_t t23 = T2.dim(3), t41 = T4.dim(1);
-    (void)t23;
     if (t41 != 1) {
       DT<T> LT = block_LT(C1, eT1, eT8, T1);
       DT<T> X = td(td(td(C2, eT3, {1}, {0}), eT2, {0}, {1}), T2, {2, 5}, {2, 1}, false, true);
@@ -820,7 +883,10 @@ struct EngineT final : Engine {
       X = td(td(td(C3, eT5, {1}, {0}), eT4, {0}, {1}), T3, {2, 5}, {3, 2}, false, true);
       DT<T> RB = td(T3, X, {2, 3, 4}, {3, 1, 6});
       DT<T> LB = block_LB(C4, eT7, eT6, T4);
-      if (t23 != 1 && P.use_rsvd) fail(TG_E_INPUT, "use_rsvd is not available in this build of the FP64 path");
+      if (t23 != 1 && P.use_rsvd) {
+        proj_updown_rsvd(LT, RT, RB, LB, e34, t23, e78, t41, PU, PL);
+        return;
+      }
       DT<T> R1 = td(RT, LT, {0, 3, 4}, {0, 2, 4});
       DT<T> R2 = td(RB, LB, {0, 2, 4}, {1, 3, 5});
       DT<T> M = td(R1, R2, {3, 4, 5}, {3, 4, 5});

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -22,6 +23,25 @@ static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 void uncount_launch(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+int current_device() {
+  int dev = 0;
+  TG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) fail(TG_E_INPUT, "device ordinal out of range: " + std::to_string(dev));
+  return dev;
+}
+
+void ensure_dynamic_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> raised;
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(mu);
+  size_t& cur = raised[{kernel, dev}];
+  if (bytes > cur) {
+    TG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    cur = bytes;
+  }
+}
 
 namespace {
 struct ProfRec {
@@ -1755,11 +1775,7 @@ __global__ void spectrum_distance_kernel(const double* a, const double* c, int c
 template <int BN>
 void launch_tc_bn(dim3 grid, const GemmParams<double>& gp, cudaStream_t st) {
   constexpr int bytes = tc::STAGES * (2 * tc::BM * tc::BK * 4 + 2 * BN * tc::BK * 4);
-  static bool attr_set = false;
-  if (!attr_set) {
-    TG_CUDA(cudaFuncSetAttribute(gemm_tc_tf32x3_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    attr_set = true;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_tc_tf32x3_kernel<BN>), bytes);
   gemm_tc_tf32x3_kernel<BN><<<grid, tc::THREADS, bytes, st>>>(gp);
   TG_CHECK_LAUNCH();
   count_launch();
@@ -1806,11 +1822,7 @@ template <int BN>
 void launch_tma_bn(dim3 grid, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                    const CUtensorMap& bl, const TmaGemm& g, cudaStream_t st) {
   constexpr int bytes = tma::STAGES * (2 * tma::A_TILE + 2 * BN * tma::BK * 4) + 1024;
-  static bool attr_set = false;
-  if (!attr_set) {
-    TG_CUDA(cudaFuncSetAttribute(gemm_tma_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    attr_set = true;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_tma_kernel<BN>), bytes);
   gemm_tma_kernel<BN><<<grid, tma::THREADS, bytes, st>>>(ah, al, bh, bl, g);
   TG_CHECK_LAUNCH();
   count_launch();
@@ -2004,12 +2016,7 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   }
   constexpr int NP = CPLX ? 2 : 1;
   const size_t smem = sizeof(double) * 2 * 2 * NP * GBK * GLD;
-  static bool attr_set = false;
-  if (!attr_set) {
-    TG_CUDA(cudaFuncSetAttribute(gemm_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    attr_set = true;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, CPLX>), smem);
   if (d.batch > 65535) fail(TG_E_INPUT, "gemm: batch too large");
   dim3 grid(static_cast<unsigned>((d.N + GBN - 1) / GBN), static_cast<unsigned>((d.M + GBM - 1) / GBM),
             static_cast<unsigned>(d.batch));
@@ -2326,12 +2333,7 @@ void batched_spectrum(const T* const* mats, int count, int n, double* out, int* 
   if (n > nmax || n < 1)
     fail(TG_E_INPUT, "batched_spectrum: 1 <= chi <= " + std::to_string(nmax) + " required");
   const size_t smem = sizeof(double) * ((CPLX ? 2 : 1) * n * n + n);
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(jacobi_spectrum_kernel<T, CPLX>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    attr_bytes = smem;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(jacobi_spectrum_kernel<T, CPLX>), smem);
   ProfScope ps(PK_SPECTRUM, st, 0.0, sizeof(T) * static_cast<double>(count) * n * n);
   jacobi_spectrum_kernel<T, CPLX><<<count, 256, smem, st>>>(mats, n, out, sweeps_used);
   TG_CHECK_LAUNCH();
@@ -2398,11 +2400,7 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
   const int npairs = static_cast<int>((k + 1) / 2);
   // up to 96 columns: 16 lanes a pair, 6 rows a lane; up to 160: 32 lanes, 5 rows
   auto run = [&](auto kernel, int lanes) {
-    static size_t attr_bytes = 0;
-    if (smem > attr_bytes) {
-      TG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-      attr_bytes = smem;
-    }
+    ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
     const int threads = static_cast<int>(std::min<int64_t>(1024, (static_cast<int64_t>(npairs) * lanes + 31) / 32 * 32));
     kernel<<<1, threads, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
   };
@@ -2435,12 +2433,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   if (k < 1 || k > jacobi_svd_max_k<T>()) fail(TG_E_INPUT, "chol_rinv: k out of range");
   const int64_t kp = (k + 7) / 8 * 8;
   const size_t smem = sizeof(T) * static_cast<size_t>(kp * kp + 8 * kp) + sizeof(double) * static_cast<size_t>(2 * kp);
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(chol_rinv_blocked_kernel<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    attr_bytes = smem;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(chol_rinv_blocked_kernel<T, CPLX>), smem);
   // shifted CholeskyQR (Fukaya et al., SIAM J. Sci. Comput. 42 (2020) A477):
   // s = 11 (m n + n (n+1)) u ||X||_2^2 with ||X||_2^2 <= k for unit columns
   const double u = 1.1102230246251565e-16;

@@ -30,16 +30,13 @@ constexpr int kNoallocMaxMatrices = 1024;
 // call's contents, so calls whose work overlaps on the GPU race on it.
 static __device__ __align__(256) const void* g_noalloc_ptrs[kNoallocMaxMatrices];
 
-constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_symbol_addr[kMaxDevices] = {nullptr};
 
 // Device address of g_noalloc_ptrs on the current device, looked up once per
 // device (the host-side name is only a stand-in, not a device address).
 const void** scratch_address() {
-  int dev = 0;
-  TG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) fail(TG_E_INPUT, "device ordinal out of range");
+  const int dev = current_device();
   std::lock_guard<std::mutex> g(g_mu);
   if (!g_symbol_addr[dev]) {
     void* p = nullptr;
@@ -68,8 +65,14 @@ extern "C" tg_status tg_corner_spectra_noalloc(const void* const* device_mats, i
       if (!device_mats[i]) tg::fail(TG_E_INPUT, "null matrix pointer at index " + std::to_string(i));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const void** table = tg::scratch_address();
-    // the host array is pageable: the copy has consumed it when this returns
-    TG_CUDA(cudaMemcpyAsync(table, device_mats, sizeof(void*) * count, cudaMemcpyHostToDevice, st));
+    // The copy is staged through this stack array, which is pageable: a
+    // host-to-device cudaMemcpyAsync from pageable memory has read its source
+    // when it returns, so the caller may reuse device_mats at once, even when
+    // that array is page-locked (from page-locked memory the copy would read
+    // it later, in stream order).
+    const void* staged[tg::kNoallocMaxMatrices];
+    for (int i = 0; i < count; ++i) staged[i] = device_mats[i];
+    TG_CUDA(cudaMemcpyAsync(table, staged, sizeof(void*) * count, cudaMemcpyHostToDevice, st));
     if (is_complex) {
       tg::batched_spectrum<tg::cplx>(reinterpret_cast<const tg::cplx* const*>(table), count, n, device_out,
                                      nullptr, st);

@@ -226,12 +226,7 @@ size_t skinny_smem(int K, int n, bool kmajor, int stages) {
 
 template <int STAGES, int NB>
 void launch_skinny_nb(const SkinnyParams& p, size_t smem, cudaStream_t st) {
-  static size_t attr_bytes = 0;
-  if (smem > attr_bytes) {
-    TG_CUDA(cudaFuncSetAttribute(skinny_kernel<STAGES, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)));
-    attr_bytes = smem;
-  }
+  ensure_dynamic_smem(reinterpret_cast<const void*>(skinny_kernel<STAGES, NB>), smem);
   const int64_t ntiles = (p.rows + SK_R - 1) / SK_R;
   const int per_sm = smem <= SK_SMEM_2CTA ? 2 : 1;
   const unsigned grid = static_cast<unsigned>(std::min<int64_t>(ntiles, 148 * per_sm));

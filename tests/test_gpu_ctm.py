@@ -162,6 +162,54 @@ def test_rsvd_single_move_matches_oracle(is_complex):
                                        atol=1e-10, err_msg=f"{name}[{i}]")
 
 
+@pytest.mark.parametrize("direction", [0, 1, 2, 3])
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_updown_rsvd_single_move_matches_oracle(direction, is_complex):
+    """One move with the rSVD branch of the up/down projectors
+    (ctm.cpp:401-439; projector_corner = false), from a full-rank environment:
+    the GPU applies M = RT^T LT LB RB as four products per panel, the oracle
+    forms R1 R2^T; both draw the same counter-based test matrix."""
+    lat = make_lattice(2, 2, 2)
+    Tn = random_tensors(lat, 31, is_complex)
+    chi = 8
+    p_full = oracle_params(chi, CTM_Projector_corner=False)
+    oe = O.init_env(Tn, p_full, lat)
+    for _ in range(2):
+        O.sweep(oe, Tn, p_full, lat)
+    p = oracle_params(chi, Use_RSVD=True, CTM_Projector_corner=False, rsvd_power_iters=2, rsvd_oversample_abs=4)
+    ge = gpu_env(lat, Tn, chi, is_complex, use_rsvd=True, projector_corner=False, rsvd_oversample_abs=4,
+                 rsvd_power_iters=2)
+    load_env(ge, oe)
+    move = (O.left_move, O.right_move, O.top_move, O.bottom_move)[direction]
+    move(oe, Tn, 0, p, lat)
+    ge.move(direction, 0)
+    for w, name in enumerate(("C1", "C2", "C3", "C4", "eTt", "eTr", "eTb", "eTl")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(np.abs(ge.get_env(w, i)), np.abs(getattr(oe, name)[i]), rtol=1e-8,
+                                       atol=1e-10, err_msg=f"{name}[{i}]")
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_updown_rsvd_ctm_run_matches_oracle(is_complex):
+    """Whole CTMRG runs with up/down rSVD projectors and the reference's
+    default multiplicative oversampling (k = 2 cut)."""
+    lat = make_lattice(2, 2, 2)
+    Tn = physical_tensors(lat, 2, is_complex=is_complex)
+    chi, iters = 8, 4
+    oe, ocnt, _, _ = O.calc_ctm_environment(
+        Tn, oracle_params(chi, Use_RSVD=True, CTM_Projector_corner=False, Max_CTM_Iteration=iters,
+                          rsvd_power_iters=2), lat)
+    ge = gpu_env(lat, Tn, chi, is_complex, max_ctm_iteration=iters, use_rsvd=True, projector_corner=False,
+                 rsvd_power_iters=2)
+    gcnt, _, _ = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt
+    for w, name in enumerate(("C1", "C2", "C3", "C4")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i]),
+                                       rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
+
+
 @pytest.mark.parametrize("is_complex", [False, True])
 def test_graph_sweeps_equal_eager_sweeps(is_complex):
     """Sweeps replayed from the captured CUDA graph give the same environment as
