@@ -1,16 +1,22 @@
 """CTMRG throughput on B200: sweeps/s of the iTPS corner-transfer-matrix
 environment (one sweep = Left, Right, Top, Bottom moves of
 core::Calc_CTM_Environment, src/iTPS/core/ctm.cpp:1203-1243) and the time to
-a converged environment, mixed precision against the FP64 path.
+a converged environment, FP64 and mixed precision.
 
-Workload (default): spin-1/2 antiferromagnetic Heisenberg model, 2x2 unit
+Workload (default c3): spin-1/2 antiferromagnetic Heisenberg model, 2x2 unit
 cell, D=6, chi=72, site tensors from 300 seeded simple-update steps at
-tau=0.01 run through the library itself, Neel initial state + noise 1e-2
-(seed 11).  Data are synthetic; the reference publishes no benchmark suite.
-`value` is the chosen form: 3xTF32 tcgen05 contractions with FP64 rSVD
-projectors (k = chi+10, q = 2).  `time_to_converge` runs the chosen form, the
-FP64 rSVD path and the FP64 full-SVD path (the reference's default projector)
-from the same tensors until the energy per site moves by <= 1e-7 per sweep.
+tau=0.01 run through the library itself from a Neel initial state + noise
+1e-2 (iTPS::initialize_tensors, seed 11).  Data are synthetic; the reference
+publishes no benchmark suite.
+
+`value` is the FP64 path with rSVD projectors (k = chi+10, q = 2), the same
+arithmetic and the same algorithm as the reference arm (`--impl reference`:
+the FP64 CPU oracle with the same projectors, on all host cores).  Beside it
+the line reports the mixed form (3xTF32 tcgen05 contractions, FP64 projector
+algebra) at the same projectors, the FP64 full-SVD path (the reference's
+default projector), the time to a converged environment of all three, and
+each arm's energy per site against the FP64 oracle run from the same site
+tensors.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -36,15 +42,20 @@ if ROOT not in sys.path:
 
 import numpy as np  # noqa: E402
 
+# name: workload of one 2x2 unit cell
+#   afh: J (SxSx + SySy + SzSz), Neel + noise 1e-2 through initialize_tensors
+#   tfi: -SzSz bonds and a -hx Sx field (one-site evolution operators), site
+#        tensors i.i.d. uniform[-1, 1] from the seed, each scaled to max |entry| = 1
 CONFIGS = {
-    # name: (D, chi, su_steps, description)
-    "c3": (6, 72, 300, "afh_square_2x2_D6_chi72_fp64"),
-    "c2": (4, 32, 200, "afh_square_2x2_D4_chi32_fp64"),
-    "c1": (2, 10, 100, "afh_square_2x2_D2_chi10_fp64"),
+    "c3": dict(model="afh", D=6, chi=72, su_steps=300, name="afh_square_2x2_D6_chi72"),
+    "c2": dict(model="afh", D=4, chi=32, su_steps=200, name="afh_square_2x2_D4_chi32"),
+    "c1": dict(model="tfi", D=2, chi=10, su_steps=1000, name="tfi_square_2x2_D2_chi10_hx1"),
 }
+HX = 1.0
 TAU = 0.01
 SEED = 11
 L2_BYTES = 126 * 1024 * 1024
+RSVD_OVERSAMPLE, RSVD_POWER = 10, 2
 
 
 def log(*a):
@@ -73,30 +84,63 @@ def heisenberg_op():
     return real_if_close(evolution_twosite(heisenberg_bond(1.0), TAU))
 
 
+def su_ops(cfg):
+    """(bond evolution operator, one-site evolution operator or None)."""
+    from tenes_b200.std_ops import evolution_onesite, evolution_twosite, ising_bond, real_if_close, spin_ops
+    if CONFIGS[cfg]["model"] == "afh":
+        return heisenberg_op(), None
+    _, Sx, _ = spin_ops(0.5)
+    return (real_if_close(evolution_twosite(ising_bond(1.0), TAU)),
+            real_if_close(evolution_onesite(-HX * Sx, TAU)))
+
+
+def bond_hamiltonian(cfg):
+    from tenes_b200.std_ops import heisenberg_bond, ising_bond, real_if_close
+    return real_if_close(heisenberg_bond(1.0) if CONFIGS[cfg]["model"] == "afh" else ising_bond(1.0))
+
+
+def uniform_tensors(D, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(4):
+        t = rng.uniform(-1.0, 1.0, (D, D, D, D, 2))
+        out.append(t / np.abs(t).max())
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def ctm_params(cfg, projector, precision="fp64"):
     from tenes_b200.env import CTMParams
-    D, chi, _, _ = CONFIGS[cfg]
+    chi = CONFIGS[cfg]["chi"]
     mixed = precision == "mixed"
     if projector == "rsvd":
         # rSVD projectors, oversampling chi+10, 2 power iterations
-        return CTMParams(chi=chi, max_ctm_iteration=1, use_rsvd=True, rsvd_oversample_abs=10,
-                         rsvd_power_iters=2, mixed=mixed)
+        return CTMParams(chi=chi, max_ctm_iteration=1, use_rsvd=True, rsvd_oversample_abs=RSVD_OVERSAMPLE,
+                         rsvd_power_iters=RSVD_POWER, mixed=mixed)
     return CTMParams(chi=chi, max_ctm_iteration=1, mixed=mixed)
 
 
 def make_env(cfg, seed, device, projector="svd", su_steps=None, precision="fp64"):
     from tenes_b200.env import Environment
-    D, chi, su_default, _ = CONFIGS[cfg]
-    su_steps = su_default if su_steps is None else su_steps
+    c = CONFIGS[cfg]
+    D = c["D"]
+    su_steps = c["su_steps"] if su_steps is None else su_steps
     LX, LY, pd, vd, dirs, noises = lattice_spec(D)
     env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector, precision), False, device=device)
-    env.init_tensors(seed, dirs, noises)
-    op = heisenberg_op()
+    if c["model"] == "afh":
+        env.init_tensors(seed, dirs, noises)
+    else:
+        for i, t in enumerate(uniform_tensors(D, seed)):
+            env.set_site_tensor(i, t)
+    op, op1 = su_ops(cfg)
     t0 = time.perf_counter()
     for _ in range(su_steps):
         for (s, leg) in bonds(LX, LY):
             env.simple_update(s, leg, op)
+        if op1 is not None:
+            for s in range(env.N):
+                env.simple_update(s, -1, op1)
+    env.sync()
     log(f"[bench] {su_steps} simple-update steps in {time.perf_counter() - t0:.1f}s")
     env.init_env()
     return env
@@ -181,18 +225,22 @@ def traffic_from_profile(cfg, family):
     return float(m.group(1)) if m else None
 
 
-def bond_energy(env):
-    """Energy per site: <S.S> over the horizontal and vertical bond of every
-    site, each normalised by the same contraction with the identity
-    (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225), both read
-    from the bond's reduced density matrix (one contraction per bond)."""
-    from tenes_b200.std_ops import heisenberg_bond, real_if_close
-    h = real_if_close(heisenberg_bond(1.0))
+def bond_energy(env, cfg="c3"):
+    """Energy per site: the bond Hamiltonian over the horizontal and vertical
+    bond of every site, each normalised by the same contraction with the
+    identity (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225), both
+    read from the bond's reduced density matrix (one contraction per bond);
+    for the Ising workload plus the field term -hx <Sx> of every site."""
+    h = bond_hamiltonian(cfg)
     tot = 0.0
     for s in range(env.N):
         for dx, dy in ((1, 0), (0, 1)):
             rho = env.contract_bond_rdm(s, dx, dy)
             tot += (np.sum(h * rho) / np.einsum("abab->", rho)).real
+    if CONFIGS[cfg]["model"] == "tfi":
+        sx = np.array([[0.0, 0.5], [0.5, 0.0]])
+        for s in range(env.N):
+            tot -= HX * (env.contract_one_site(s, sx) / env.contract_one_site(s, np.eye(2))).real
     return tot / env.N
 
 
@@ -206,8 +254,7 @@ def prepare_tensors(cfg, seed, device, su_steps=None):
 
 def env_for(cfg, T, device, projector, precision, max_iter=1):
     from tenes_b200.env import Environment
-    D, chi, _, _ = CONFIGS[cfg]
-    LX, LY, pd, vd, _, _ = lattice_spec(D)
+    LX, LY, pd, vd, _, _ = lattice_spec(CONFIGS[cfg]["D"])
     p = ctm_params(cfg, projector, precision)
     p.max_ctm_iteration = max_iter
     env = Environment(LX, LY, pd, vd, p, False, device=device)
@@ -222,13 +269,14 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
     changes by at most `tol` between successive sweeps (energy evaluations
     included in the wall time); the sweep at which the reference's own
     corner-spectrum criterion (eps = 1e-6, ctm.cpp:815-969) first holds is
-    recorded too."""
+    recorded too (the library's check, run after every sweep)."""
     env = env_for(cfg, T, device, projector, precision)
     env.sync()
     t0 = time.perf_counter()
     e_prev, n, ref_conv, conv = None, 0, None, False
     e = float("nan")
     per_sweep = []  # (sweep, convergence check, energy) seconds
+    energies = []
     while n < max_sweeps:
         ts = time.perf_counter()
         env.sweep()
@@ -238,8 +286,9 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
         if c and ref_conv is None:
             ref_conv = n
         te = time.perf_counter()
-        e = bond_energy(env)
+        e = bond_energy(env, cfg)
         tz = time.perf_counter()
+        energies.append(e)
         per_sweep.append([round(tc - ts, 4), round(te - tc, 4), round(tz - te, 4)])
         if e_prev is not None and abs(e - e_prev) <= tol:
             conv = True
@@ -253,7 +302,7 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
     med = statistics.median(sum(x) for x in per_sweep) if per_sweep else 0.0
     return {"sweeps": n, "seconds": secs, "seconds_sweeps_x_median": n * med, "converged": conv,
             "energy_per_site": e, "last_delta_e": (abs(e - e_prev) if e_prev is not None else None),
-            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv,
+            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv, "energy_per_sweep": energies,
             "seconds_per_sweep_sweep_check_energy": per_sweep}
 
 
@@ -275,15 +324,83 @@ def replica_rate(world, steps, total_ms):
     return world * steps / (total_ms * 1e-3)
 
 
+def timed_sweeps(env, steps, warmup, stream, flush):
+    """Device time (ms) of each of `steps` sweeps after `warmup` untimed ones:
+    CUDA events on the context's stream, an L2 flush before each."""
+    import torch
+    for _ in range(warmup):
+        env.sweep()
+    env.sync()
+    times = []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # L2 flush outside the timed window
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        env.sweep()
+        e.record(stream)
+        e.synchronize()
+        times.append(s.elapsed_time(e))
+    return times
+
+
+def sweep_profile(env):
+    """Per-family device time of one instrumented sweep: {family: (launches, ms, flops, bytes)}."""
+    from tenes_b200.env import PROFILE_KINDS, profile_enable, profile_query, profile_reset
+    profile_enable(True)
+    profile_reset()
+    env.sweep()
+    env.sync()
+    fam = {PROFILE_KINDS[k]: profile_query(k) for k in range(len(PROFILE_KINDS))}
+    profile_enable(False)
+    return fam
+
+
+def roofline_fp64(fam, peak_tflops, cfg):
+    """FP64 DMMA products (gemm_kernel, skinny_kernel): compute-bound at
+    intensity >> the FP64 ridge (~6 flop/B), so the roof is the measured DGEMM
+    rate."""
+    n_g, ms_g, fl_g, by_g = fam["gemm_dmma"]
+    ach = fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0
+    return {"bound": "tensor", "kernel": "gemm_kernel + skinny_kernel (FP64 DMMA m8n8k4)",
+            "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s",
+            "frac": ach / peak_tflops if peak_tflops else None,
+            "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (MEASURED_PEAKS.json has no FP64 entry)",
+            "traffic": traffic_from_profile(cfg, "gemm_dmma"),
+            "hbm_gbs_algorithmic": by_g / (ms_g * 1e-3) / 1e9 if ms_g > 0 else 0.0,
+            "launches_per_sweep": n_g, "avg_launch_us": 1e3 * ms_g / max(n_g, 1),
+            "flops_per_launch": fl_g / max(n_g, 1),
+            "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}}
+
+
+def roofline_tcgen05(fam, peaks, cfg):
+    """3xTF32 tcgen05 products with their split pass: the dominant shape (the
+    rSVD range finder, 2592 x 82 x 2592 at c3) has 55 issued flop/B, below
+    the TF32 ridge (~107), so the binding roof is HBM; the tensor-pipe
+    fraction is reported beside it."""
+    n_g, ms_g, fl_g, by_g = fam["gemm_tcgen05"]
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    tf32 = peaks.get("bf16_tflops_sustained", 1411.5) / 2.0
+    gbs = by_g / (ms_g * 1e-3) / 1e9 if ms_g > 0 else 0.0
+    issued = 3.0 * fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0
+    return {"bound": "hbm", "kernel": "gemm_tma_kernel (tcgen05 kind::tf32, 3 products) + split_pack_kernel",
+            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if hbm else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "tensor_tflops_issued": issued, "tensor_peak": tf32, "tensor_frac": issued / tf32,
+            "traffic": traffic_from_profile(cfg, "gemm_tcgen05"),
+            "launches_per_sweep": n_g, "avg_launch_us": 1e3 * ms_g / max(n_g, 1),
+            "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
-    import torch.distributed as dist
-    from tenes_b200.env import (PROFILE_KINDS, kernel_launch_count, profile_enable, profile_query,
-                                profile_reset)
+    from tenes_b200.env import kernel_launch_count
     device = local_rank
     torch.cuda.set_device(device)
-    T = prepare_tensors(args.config, SEED + rank, device, args.su_steps)
-    env = env_for(args.config, T, device, args.projector, args.precision)
+    cfg = args.config
+    T = prepare_tensors(cfg, SEED + rank, device, args.su_steps)
+    env = env_for(cfg, T, device, args.projector, args.precision)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
@@ -296,34 +413,17 @@ def run_ours(args, rank, world, local_rank):
         env.sweep()
         env.sync()
         torch.cuda.profiler.stop()
-    times = []
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize(device)
     clocks = Clocks(device)
     clocks.start()
-    if args.profile_timed:
-        profile_enable(True)
-        profile_reset()
     l0 = kernel_launch_count()
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)  # L2 flush outside the timed window
-        s = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        env.sweep()
-        e.record(stream)
-        e.synchronize()
-        times.append(s.elapsed_time(e))
+    times = timed_sweeps(env, args.steps, 0, stream, flush)
     launches = kernel_launch_count() - l0
     torch.cuda.synchronize(device)
     ck = clocks.stop()
-    timed_breakdown = None
-    if args.profile_timed:
-        timed_breakdown = {PROFILE_KINDS[k]: round(profile_query(k)[1] / args.steps, 3)
-                           for k in range(len(PROFILE_KINDS))}
-        profile_enable(False)
     total_ms = max_over_ranks(sum(times), device, world)
     if world > 1:
         dist.barrier()
@@ -374,54 +474,53 @@ def run_ours(args, rank, world, local_rank):
                            "tg_set_site_tensor / tg_set_env, one tg_ctm_sweep, 32 environment tensors down "
                            "through tg_get_env"}
 
-    # ---- per-family device time of one instrumented sweep (roofline of the dominant product kernel)
-    profile_enable(True)
-    profile_reset()
-    env.sweep()
-    env.sync()
-    fam = {PROFILE_KINDS[k]: profile_query(k) for k in range(len(PROFILE_KINDS))}
-    profile_enable(False)
+    # ---- roofline of this arm's dominant product family (one instrumented sweep)
+    fam = sweep_profile(env)
     env.close()
     peaks = measured_peaks()
-    if fam["gemm_tcgen05"][1] >= fam["gemm_dmma"][1]:
-        n_g, ms_g, fl_g, _ = fam["gemm_tcgen05"]
-        issued = 3.0 * fl_g  # three TF32 products per multiply-add
-        peak = peaks.get("bf16_tflops_sustained", 1411.5) / 2.0
-        roof = {"bound": "tensor", "kernel": "gemm_tma_kernel (tcgen05 kind::tf32, 3 products; split/pack included)",
-                "achieved": issued / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0, "peak": peak,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained / 2 (dense TF32 rate, of measured)",
-                "algorithmic_tflops": fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0}
+    dgemm = fp64_peak_tflops(device)
+    if args.precision == "mixed":
+        roof = roofline_tcgen05(fam, peaks, cfg)
     else:
-        n_g, ms_g, fl_g, _ = fam["gemm_dmma"]
-        peak = fp64_peak_tflops(device) if rank == 0 else None
-        roof = {"bound": "tensor", "kernel": "gemm_kernel (FP64 DMMA m8n8k4)",
-                "achieved": fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0, "peak": peak,
-                "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (MEASURED_PEAKS.json has no FP64 entry)"}
-    roof.update({"unit": "TFLOP/s", "frac": (roof["achieved"] / roof["peak"]) if roof["peak"] else None,
-                 "traffic": traffic_from_profile(args.config, "gemm_tcgen05" if "tcgen05" in roof["kernel"]
-                                                 else "gemm_dmma"),
-                 "traffic_note": "DRAM bytes of one launch of the family's dominant shape (the rSVD range-finder "
-                                 "product 2592 x 82 x 2592), from profiles/roofline_traffic_<config>.md",
-                 "launches_per_sweep": n_g,
-                 "avg_launch_us": 1e3 * ms_g / max(n_g, 1), "flops_per_launch": fl_g / max(n_g, 1),
-                 "sweep_breakdown_ms": {k: round(v[1], 3) for k, v in fam.items()}})
+        roof = roofline_fp64(fam, dgemm, cfg)
 
-    # ---- time to a converged environment: the chosen form against the FP64 plain path
+    # ---- the other arms from the same tensors (device-timed sweeps, same flush)
+    arms = {}
+    if not args.quick:
+        for tag, proj, prec, k in (("mixed_rsvd", "rsvd", "mixed", args.steps), ("fp64_rsvd", "rsvd", "fp64",
+                                   args.steps), ("fp64_full_svd", "svd", "fp64", min(args.steps, 3))):
+            if proj == args.projector and prec == args.precision:
+                arms[tag] = {"sweeps_per_s": value / world, "ms_per_sweep": ms_per_step, "headline": True}
+                continue
+            e2 = env_for(cfg, T, device, proj, prec)
+            st2 = torch.cuda.ExternalStream(e2.stream_handle(), device=device)
+            tt = timed_sweeps(e2, k, 3 if proj == "rsvd" else 1, st2, flush)
+            f2 = sweep_profile(e2)
+            e2.close()
+            arms[tag] = {"sweeps_per_s": 1e3 * len(tt) / sum(tt), "ms_per_sweep": sum(tt) / len(tt),
+                         "sweeps_timed": len(tt),
+                         "roofline": roofline_tcgen05(f2, peaks, cfg) if prec == "mixed"
+                         else roofline_fp64(f2, dgemm, cfg)}
+        if "mixed_rsvd" in arms and "fp64_rsvd" in arms:
+            arms["speedup_mixed_vs_fp64_same_projector"] = (arms["mixed_rsvd"]["sweeps_per_s"]
+                                                            / arms["fp64_rsvd"]["sweeps_per_s"])
+
+    # ---- time to a converged environment: mixed and FP64 at the same projector, and FP64 full SVD
     conv = None
     if args.converge != "none":
         conv = {"criterion": "|E/site(sweep t) - E/site(sweep t-1)| <= 1e-7 (energy evaluations timed too)"}
-        conv["mixed_rsvd"] = converge(args.config, T, device, "rsvd", "mixed")
-        conv["fp64_rsvd"] = converge(args.config, T, device, "rsvd", "fp64")
+        conv["mixed_rsvd"] = converge(cfg, T, device, "rsvd", "mixed")
+        conv["fp64_rsvd"] = converge(cfg, T, device, "rsvd", "fp64")
         if args.converge == "full":
-            conv["fp64_full_svd"] = converge(args.config, T, device, "svd", "fp64", max_sweeps=30)
-        base = conv.get("fp64_full_svd") or conv["fp64_rsvd"]
+            conv["fp64_full_svd"] = converge(cfg, T, device, "svd", "fp64", max_sweeps=30)
+        conv["speedup_mixed_vs_fp64_rsvd"] = conv["fp64_rsvd"]["seconds"] / conv["mixed_rsvd"]["seconds"]
         conv["speedup_mixed_vs_fp64_full_svd"] = (conv["fp64_full_svd"]["seconds"] / conv["mixed_rsvd"]["seconds"]
                                                   if "fp64_full_svd" in conv else None)
-        conv["speedup_mixed_vs_fp64_rsvd"] = conv["fp64_rsvd"]["seconds"] / conv["mixed_rsvd"]["seconds"]
-        conv["abs_delta_e_mixed_vs_fp64"] = abs(conv["mixed_rsvd"]["energy_per_site"] - base["energy_per_site"])
-    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roof,
+        conv["abs_delta_e_mixed_vs_fp64_rsvd"] = abs(conv["mixed_rsvd"]["energy_per_site"]
+                                                     - conv["fp64_rsvd"]["energy_per_site"])
+    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roof, "arms": arms,
             "clocks": ck, "gpu_launches": launches, "sweep_ms": [round(t, 3) for t in times],
-            "timed_breakdown_ms": timed_breakdown, "converge": conv}
+            "converge": conv, "tensors": T}
 
 
 def measured_peaks():
@@ -434,64 +533,148 @@ def measured_peaks():
 
 
 # -------------------------------------------------------- CPU oracle (reference arm)
-def oracle_sample(cfg, rank=0):
-    """Time one Left_move of the CPU oracle on the same workload; one sweep is
-    4*LX... = 8 moves of this size for a 2x2 cell."""
+def oracle_lattice(cfg):
     from oracle import tenes_oracle as O
-    D, chi, su_steps, _ = CONFIGS[cfg]
-    LX, LY, pd, vd, dirs, noises = lattice_spec(D)
+    LX, LY, pd, vd, dirs, noises = lattice_spec(CONFIGS[cfg]["D"])
     lat = O.Lattice(LX, LY)
     lat.physical_dims = pd
     lat.virtual_dims = vd
     lat.initial_dirs = dirs
     lat.noises = noises
-    Tn = O.initialize_tensors(lat, SEED + rank, True)
+    return lat
+
+
+def oracle_params(cfg, projector="rsvd"):
+    from oracle import tenes_oracle as O
+    chi = CONFIGS[cfg]["chi"]
+    if projector == "rsvd":
+        return O.Params(CHI=chi, Use_RSVD=True, rsvd_oversample_abs=RSVD_OVERSAMPLE, rsvd_power_iters=RSVD_POWER)
+    return O.Params(CHI=chi)
+
+
+def oracle_tensors(cfg, seed):
+    """The workload's site tensors by the CPU oracle: its own seeded start and
+    simple update (the same algorithm as the library's)."""
+    from oracle import tenes_oracle as O
+    c = CONFIGS[cfg]
+    D = c["D"]
+    lat = oracle_lattice(cfg)
+    Tn = O.initialize_tensors(lat, seed, True) if c["model"] == "afh" else uniform_tensors(D, seed)
     lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
-    p = O.Params(CHI=chi)
-    op = heisenberg_op()
-    for _ in range(su_steps):
-        for (s, leg) in bonds(LX, LY):
+    p = O.Params()
+    op, op1 = su_ops(cfg)
+    for _ in range(c["su_steps"]):
+        for (s, leg) in bonds(lat.LX, lat.LY):
             tg = lat.neighbor(s, leg)
             a, b, lc = O.simple_update_bond(Tn[s], Tn[tg], lam[s], lam[tg], op, leg, p)
             lam[s][leg] = lc
             lam[tg][(leg + 2) % 4] = lc
             Tn[s], Tn[tg] = a, b
-    env = O.init_env(Tn, p, lat)
-    return lat, Tn, p, env
+        if op1 is not None:
+            for s in range(lat.N_UNIT):
+                Tn[s] = np.tensordot(Tn[s], op1, ([4], [0]))
+    return lat, Tn
 
 
-def time_oracle_move(lat, Tn, p, env):
+def oracle_moves(lat):
+    """The moves of one sweep in the order of ctm.cpp:1205-1228 (as O.sweep)."""
     from oracle import tenes_oracle as O
-    t0 = time.perf_counter()
-    O.left_move(env, Tn, 0, p, lat)
-    return time.perf_counter() - t0
+    LX, LY = lat.LX_noskew, lat.LY_noskew
+    mv = [(O.left_move, ix) for ix in range(LX)]
+    mv += [(O.right_move, (ix + 1 + LX) % LX) for ix in range(0, -LX, -1)]
+    mv += [(O.top_move, (iy + 1 + LY) % LY) for iy in range(0, -LY, -1)]
+    mv += [(O.bottom_move, iy) for iy in range(LY)]
+    return mv
 
 
-def moves_per_sweep(lat):
-    return 2 * lat.LX_noskew + 2 * lat.LY_noskew
+def oracle_energy(cfg, oe, Tn, lat):
+    """Energy per site of the oracle's environment (op12 contractions / norm,
+    twosite_obs.cpp; the Ising field through the one-site contraction)."""
+    from oracle import tenes_oracle as O
+    h = bond_hamiltonian(cfg)
+    one = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    tot = 0.0
+    for i in range(lat.N_UNIT):
+        j = lat.right(i)
+        a = (oe.C1[i], oe.C2[j], oe.C3[j], oe.C4[i], oe.eTt[i], oe.eTt[j], oe.eTr[j], oe.eTb[j], oe.eTb[i],
+             oe.eTl[i], Tn[i], Tn[j])
+        tot += (O.contract_two_sites_horizontal_op12(*a, h) / O.contract_two_sites_horizontal_op12(*a, one)).real
+        j = lat.top(i)
+        a = (oe.C1[j], oe.C2[j], oe.C3[i], oe.C4[i], oe.eTt[j], oe.eTr[j], oe.eTr[i], oe.eTb[i], oe.eTl[i],
+             oe.eTl[j], Tn[j], Tn[i])
+        tot += (O.contract_two_sites_vertical_op12(*a, h) / O.contract_two_sites_vertical_op12(*a, one)).real
+    if CONFIGS[cfg]["model"] == "tfi":
+        sx = np.array([[0.0, 0.5], [0.5, 0.0]])
+        for i in range(lat.N_UNIT):
+            a = (oe.C1[i], oe.C2[i], oe.C3[i], oe.C4[i], oe.eTt[i], oe.eTr[i], oe.eTb[i], oe.eTl[i], Tn[i])
+            tot -= HX * (O.contract_one_site(*a, sx) / O.contract_one_site(*a, np.eye(2))).real
+    return tot / lat.N_UNIT
+
+
+def oracle_check(cfg, T, sweeps):
+    """The FP64 CPU oracle with the headline's projectors (rSVD, k = chi+10,
+    q = 2) from the GPU's own site tensors: `sweeps` sweeps, each move timed
+    (the first sweep is the CPU baseline sample), then the energy per site."""
+    from oracle import tenes_oracle as O
+    lat = oracle_lattice(cfg)
+    p = oracle_params(cfg)
+    oe = O.init_env(T, p, lat)
+    move_s = []
+    for _ in range(sweeps):
+        for fn, line in oracle_moves(lat):
+            t0 = time.perf_counter()
+            fn(oe, T, line, p, lat)
+            move_s.append(time.perf_counter() - t0)
+    return move_s, oracle_energy(cfg, oe, T, lat)
+
+
+def config_block(args, world):
+    """The `config` object, identical in both arms for the same flags."""
+    c = CONFIGS[args.config]
+    return {"workload": f"{c['name']}_{args.precision}_{args.projector}", "precision": args.precision,
+            "D": c["D"], "chi": c["chi"], "unit_cell": "2x2", "su_steps": c["su_steps"],
+            "projector": ("full SVD (reference default)" if args.projector == "svd"
+                          else f"rSVD k=chi+{RSVD_OVERSAMPLE}, q={RSVD_POWER}"),
+            "parallelism": f"replicas{world}",
+            "l2": "GPU arm: flushed between timed sweeps (252 MB write outside the timed window)"}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the FP64 CPU oracle (numpy, all host cores through
+    BLAS/LAPACK) on the same workload and projectors.  Each step is one move;
+    the steps walk through the moves of consecutive sweeps in the order of
+    ctm.cpp:1205-1228, so every move of a sweep is timed and the sweeps/s is
+    (steps / moves per sweep) / time."""
     if rank != 0:
         return None
-    lat, Tn, p, env = oracle_sample(args.config)
+    from oracle import tenes_oracle as O
+    lat, Tn = oracle_tensors(args.config, SEED)
+    p = oracle_params(args.config, args.projector)
+    env = O.init_env(Tn, p, lat)
+    moves = oracle_moves(lat)
+    k = 0
     for _ in range(args.warmup):
-        time_oracle_move(lat, Tn, p, env)
+        fn, line = moves[k % len(moves)]
+        fn(env, Tn, line, p, lat)
+        k += 1
     tot = 0.0
     for _ in range(args.steps):
-        tot += time_oracle_move(lat, Tn, p, env)
-    per_sweep = tot / args.steps * moves_per_sweep(lat)
-    v = 1.0 / per_sweep
+        fn, line = moves[k % len(moves)]
+        t0 = time.perf_counter()
+        fn(env, Tn, line, p, lat)
+        tot += time.perf_counter() - t0
+        k += 1
+    v = (args.steps / len(moves)) / tot
     cores = os.cpu_count()
-    D, chi, _, name = CONFIGS[args.config]
     return {"metric": "ctmrg_sweeps_per_s", "value": v, "unit": "sweeps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_sweep * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": name, "D": D, "chi": chi, "unit_cell": "2x2", "projector": "full SVD"},
+            "data": "synthetic (seeded simple-update tensors of the workload's shapes)", "impl": "reference",
+            "config": config_block(args, world),
+            "step": f"one CTMRG move (1/{len(moves)} of a sweep), moves of consecutive sweeps in sweep order",
             "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": cores, "kind": "port",
-                             "sample": "one Left_move (2 projector rows, full SVD) of the CPU oracle per step, "
-                                       f"x{moves_per_sweep(lat)} moves per sweep"},
+                             "sample": f"{args.steps} consecutive moves of the FP64 CPU oracle "
+                                       f"({args.steps / len(moves):.2f} sweeps) after {args.warmup} warm-up moves"},
             "e2e": {"value": v, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -596,16 +779,15 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--projector", default="rsvd", choices=["svd", "rsvd"],
                     help="svd: full SVD (reference default); rsvd: k = chi+10, 2 power iterations")
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: 3xTF32 tcgen05 contractions, FP64 projector algebra")
     ap.add_argument("--converge", default="full", choices=["full", "fast", "none"],
                     help="time-to-converge arms: full = mixed rSVD, FP64 rSVD and FP64 full SVD; "
                          "fast = without the FP64 full-SVD arm")
+    ap.add_argument("--quick", action="store_true", help="headline and e2e only (no other arms)")
     ap.add_argument("--su-steps", type=int, default=None,
                     help="override the simple-update steps that prepare the tensors (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-timed", action="store_true",
-                    help="CUDA-event profile of the library kernels during the timed sweeps (diagnostic)")
     ap.add_argument("--profile-sweep", action="store_true",
                     help="wrap one extra sweep in cudaProfilerStart/Stop (for ncu)")
     ap.add_argument("--grad", action="store_true",
@@ -636,31 +818,42 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     res = run_ours(args, rank, world, local_rank)
     if rank == 0:
-        D, chi, su, name = CONFIGS[args.config]
+        c = CONFIGS[args.config]
         cpu = None
+        oracle = None
         if not args.no_cpu_baseline:
-            lat, Tn, p, env = oracle_sample(args.config)
-            t = time_oracle_move(lat, Tn, p, env)
-            v = 1.0 / (t * moves_per_sweep(lat))
-            cpu = {"value": v, "unit": "sweeps/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"one Left_move of the CPU oracle (numpy FP64, full SVD), x{moves_per_sweep(lat)} "
-                             "moves per sweep"}
+            # The oracle from the GPU's own site tensors, as many sweeps as the
+            # FP64 rSVD arm took to converge: its first sweep is the CPU
+            # baseline sample, its energy pins every arm's energy.
+            n_sw = (res["converge"]["fp64_rsvd"]["sweeps"] if res["converge"] else 1) if args.config == "c3" \
+                else (res["converge"]["fp64_rsvd"]["sweeps"] if res["converge"] else 3)
+            move_s, e_or = oracle_check(args.config, res["tensors"], n_sw)
+            per = len(oracle_moves(oracle_lattice(args.config)))
+            first = sum(move_s[:per])
+            cpu = {"value": 1.0 / first, "unit": "sweeps/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"the first of {n_sw} consecutive sweeps ({per} moves) of the FP64 CPU oracle with "
+                             f"the same projectors (rSVD k=chi+{RSVD_OVERSAMPLE}, q={RSVD_POWER}) from the same "
+                             "site tensors"}
+            oracle = {"sweeps": n_sw, "energy_per_site": e_or, "seconds_per_sweep": sum(move_s) / n_sw}
+            if res["converge"]:
+                for tag in ("mixed_rsvd", "fp64_rsvd", "fp64_full_svd"):
+                    arm = res["converge"].get(tag)
+                    if arm and len(arm["energy_per_sweep"]) >= n_sw:
+                        oracle[f"abs_delta_e_{tag}_at_sweep_{n_sw}"] = abs(arm["energy_per_sweep"][n_sw - 1] - e_or)
         line = {"metric": "ctmrg_sweeps_per_s", "value": res["value"], "unit": "sweeps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64",
                 "data": "synthetic (seeded simple-update tensors of the workload's shapes)",
-                "config": {"workload": f"{name}_{args.precision}_{args.projector}", "precision": args.precision,
-                           "D": D, "chi": chi, "unit_cell": "2x2", "su_steps": su,
-                           "projector": ("full SVD (reference default)" if args.projector == "svd"
-                                         else "rSVD k=chi+10, q=2"), "parallelism": f"replicas{world}",
-                           "l2": "flushed between timed sweeps (252 MB write outside the timed window)"},
+                "config": config_block(args, world),
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"], "sweep_ms": res["sweep_ms"]}
+        if res["arms"]:
+            line["arms"] = res["arms"]
         if res["converge"] is not None:
             line["time_to_converge"] = res["converge"]
-        if res["timed_breakdown_ms"] is not None:
-            line["timed_breakdown_ms"] = res["timed_breakdown_ms"]
+        if oracle is not None:
+            line["fp64_oracle_check"] = oracle
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

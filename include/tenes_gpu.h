@@ -75,6 +75,13 @@ typedef struct tg_params {
   int cuda_graph;                   /* 1 (default): with rSVD corner projectors, replay each CTMRG
                                        sweep from a captured CUDA graph (same kernels, same results);
                                        0: launch every kernel from the host. */
+  int svd_solver;                   /* solver of the full-SVD projectors (use_rsvd = 0,
+                                       ctm.cpp:267-302, 441-475): 0 (default) the leading singular
+                                       triplets the truncation keeps, by block subspace iteration
+                                       with Rayleigh-Ritz checks run until every kept triplet's
+                                       residual is <= 1e-13 s_0 (a dense SVD when that cannot be
+                                       reached); 1: the dense SVD (cuSOLVER gesvd) of the whole
+                                       matrix.  Both give the reference's truncated factors. */
 } tg_params;
 
 /* Fill *p with the reference defaults. */
@@ -119,6 +126,13 @@ tg_status tg_ctm_sweep(tg_ctx* ctx);
 /* Check_Convergence_CTM (ctm.cpp:815-969) against the corners saved by the
  * previous call (or by tg_ctm_init); saves the current corners. */
 tg_status tg_ctm_check_convergence(tg_ctx* ctx, int* converged, double* sig_max);
+
+/* Counters of the exact truncated SVD behind the full-SVD projectors
+ * (svd_solver = 0; the dense SVD of ctm.cpp:273-302 and 441-475 restated as
+ * block subspace iteration): out[0] solves, out[1] subspace iterations,
+ * out[2] Rayleigh-Ritz checks, out[3] solves handed to the dense SVD.
+ * Cumulative over the context's life. */
+tg_status tg_projector_svd_stats(tg_ctx* ctx, int64_t* out);
 
 /* core::Calc_CTM_Environment (ctm.cpp:971-1253): optional init, then sweeps
  * until converged or max_ctm_iteration.  Returns TG_OK also when not

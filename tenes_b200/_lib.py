@@ -29,6 +29,7 @@ EXPORTED = [
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
     "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_su_fix_gauge", "tg_measure_correlation",
+    "tg_projector_svd_stats",
 ]
 
 
@@ -62,7 +63,8 @@ class Params(C.Structure):
                 ("projector_corner", C.c_int), ("use_rsvd", C.c_int),
                 ("rsvd_oversampling_factor", C.c_double), ("rsvd_oversample_abs", C.c_int),
                 ("rsvd_power_iters", C.c_int), ("rsvd_seed", C.c_uint64),
-                ("inverse_lambda_cut", C.c_double), ("mixed", C.c_int), ("cuda_graph", C.c_int)]
+                ("inverse_lambda_cut", C.c_double), ("mixed", C.c_int), ("cuda_graph", C.c_int),
+                ("svd_solver", C.c_int)]
 
 
 _lib = None
@@ -95,6 +97,7 @@ def load() -> C.CDLL:
         "tg_ctm_move": (C.c_int, [vp, C.c_int, C.c_int]),
         "tg_ctm_sweep": (C.c_int, [vp]),
         "tg_ctm_check_convergence": (C.c_int, [vp, P(C.c_int), dp]),
+        "tg_projector_svd_stats": (C.c_int, [vp, P(C.c_int64)]),
         "tg_ctm_run": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int), dp]),
         "tg_corner_spectrum": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "tg_measure_onesite": (C.c_int, [vp, C.c_int, dp, dp]),

@@ -69,6 +69,7 @@ void tg_params_default(tg_params* p) {
   p->inverse_lambda_cut = 1e-12;
   p->mixed = 0;
   p->cuda_graph = 1;
+  p->svd_solver = 0;
 }
 
 const char* tg_last_error(void) { return g_last_error.c_str(); }
@@ -149,6 +150,12 @@ tg_status tg_ctm_sweep(tg_ctx* ctx) {
 }
 tg_status tg_ctm_check_convergence(tg_ctx* ctx, int* converged, double* sig_max) {
   return guard([&] { E(ctx)->check_convergence(converged, sig_max); });
+}
+tg_status tg_projector_svd_stats(tg_ctx* ctx, int64_t* out) {
+  return guard([&] {
+    need(out, "out");
+    E(ctx)->svd_stats(out);
+  });
 }
 tg_status tg_ctm_run(tg_ctx* ctx, int initialize, int* iterations, int* converged, double* sig_max) {
   return guard([&] { E(ctx)->ctm_run(initialize, iterations, converged, sig_max); });

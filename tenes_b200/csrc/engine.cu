@@ -734,9 +734,143 @@ struct EngineT final : Engine {
     scale_cols<T>(V.p, k, ncol, w, sinv.p, false, Vc.p, st);
   }
 
+  // ------------------------------------------------ exact truncated SVD
+  // The full-SVD projectors (ctm.cpp:273-302, 441-475) keep at most chi
+  // singular triplets of an n x n matrix (n = chi D^2: 2592 at D = 6,
+  // chi = 72), so the dense SVD of the whole matrix is not needed.  The kept
+  // triplets come from block subspace iteration on M (alternating products
+  // with M and M^H, i.e. orthogonal iteration on M^H M: Golub & Van Loan,
+  // Matrix Computations, 4th ed., sec. 8.2.4) on a block of b > chi
+  // columns, orthonormalised by the rSVD's shifted CholeskyQR.  A two-sided
+  // Rayleigh-Ritz step -- the SVD of the b x b matrix T = Q^H M Qz, Qz an
+  // orthonormal basis of M^H Q, by the one-CTA Jacobi kernel -- gives
+  // approximate triplets (s_i, u_i = Q t_i, v_i = Qz w_i) for which
+  // M^H u_i = s_i v_i holds exactly; they are accepted once every triplet
+  // the truncation keeps also has || M v_i - s_i u_i || <= kExactTol s_0,
+  // which bounds the angle between each kept vector and the exact one by
+  // that residual over the gap to the rest of the spectrum.  The result
+  // therefore matches the dense SVD's truncated factors to that accuracy.
+  // The start block holds the basis that the same projector (move, line,
+  // row) ended with in the previous sweep -- an almost converged guess once
+  // the environment settles -- completed with counter-based Gaussian
+  // columns.  If the residuals are not below the tolerance after
+  // kExactMaxIters iterations (a flat spectrum at the block edge), the
+  // dense SVD is used instead.
+  static constexpr double kExactTol = 1e-13;
+  static constexpr int kExactMaxIters = 80;
+  std::map<int, DT<T>> warm_v;   // right basis (ncol x b, column-major) per projector
+  int proj_key = -1;             // set by the moves before each projector
+  int64_t exact_solves = 0, exact_iters = 0, exact_checks = 0, exact_dense = 0;
+
+  int exact_block(int64_t kmax) const {
+    const int bmax = CPLX ? 84 : 96;  // CholeskyQR / Jacobi core sizes (one cluster, one CTA)
+    const int64_t w = std::min<int64_t>(P.chi, kmax);
+    if (kmax <= bmax) return static_cast<int>(kmax);  // the block spans the smaller dimension
+    const int64_t b = std::min<int64_t>(bmax, std::max<int64_t>(w + 16, w + w / 3));
+    return b >= w + 8 ? static_cast<int>(b) : -1;
+  }
+
+  // Truncated factors of M (views m = M, mh = M^H, nrow x ncol) as rsvd_run
+  // returns them: Uc (nrow x w) and Vc (ncol x w), row-major, scaled by
+  // 1/sqrt(s), zero past the cut.  Returns false when the dense SVD must be
+  // used (block too small for chi, or no convergence).
+  bool exact_factors(const MV& m, const MV& mh, int64_t nrow, int64_t ncol, DT<T>& Uc, DT<T>& Vc) {
+    const int64_t kmax = std::min(nrow, ncol);
+    const int b = exact_block(kmax);
+    if (b < 1) return false;
+    PrecScope fp64(this, 0);
+    const int w = static_cast<int>(std::min<int64_t>(P.chi, kmax));
+    ++exact_solves;
+    DT<T> Om({b, ncol}, st);  // column-major ncol x b
+    int w0 = 0;
+    auto hit = warm_v.find(proj_key);
+    if (proj_key >= 0 && hit != warm_v.end() && hit->second.size() == static_cast<int64_t>(b) * ncol) {
+      w0 = w;
+      TG_CUDA(cudaMemcpyAsync(Om.p, hit->second.p, sizeof(T) * w0 * ncol, cudaMemcpyDeviceToDevice, st));
+    }
+    if (b > w0) counter_normal<T>(Om.p + static_cast<int64_t>(w0) * ncol, ncol, b - w0, P.rsvd_seed, 7, st);
+    DT<T> Q = mm_cm(m, cm(Om.p, ncol, b));  // nrow x b, column-major
+    int next_check = (w0 > 0 || b == kmax) ? 1 : 3;
+    orth_chol(Q, nrow, b, next_check == 1 ? 4 : 2);
+    std::vector<double> hs(static_cast<size_t>(b)), hr(static_cast<size_t>(w));
+    int prev_it = 0;
+    double prev_ratio = 0.0;
+    for (int it = 1; it <= kExactMaxIters; ++it) {
+      ++exact_iters;
+      DT<T> Z = mm_cm(mh, cm(Q.p, nrow, b));  // M^H Q: ncol x b
+      if (it < next_check) {
+        orth_chol(Z, ncol, b, 2);
+        Q = mm_cm(m, cm(Z.p, ncol, b));
+        orth_chol(Q, nrow, b, it + 1 == next_check ? 4 : 2);
+        continue;
+      }
+      ++exact_checks;
+      DT<T> Qz = clone(Z, st);
+      orth_chol(Qz, ncol, b, 4);
+      DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, b)), cm(Qz.p, ncol, b));  // Q^H M Qz (b x b row-major)
+      DT<T> Ur({b, b}, st), Wr({b, b}, st);
+      DT<double> s({b}, st);
+      jacobi_svd<T>(Tm.p, b, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
+      DT<T> Y = mm_cm(m, cm(Qz.p, ncol, b));        // M Qz: nrow x b
+      DT<T> MV1 = mm_cm(cm(Y.p, nrow, b), rm(Wr.p, b, b));  // M v_i
+      DT<T> U1 = mm_cm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // u_i
+      DT<double> r({w}, st);
+      ritz_residual<T>(MV1.p, U1.p, s.p, nrow, w, r.p, st);
+      TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * b, cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaMemcpyAsync(hr.data(), r.p, sizeof(double) * w, cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaStreamSynchronize(st));
+      // the kept triplets: the truncation rule of ctm.cpp:277-288
+      int cut = w;
+      for (int i = 0; i < w; ++i)
+        if (!(hs[static_cast<size_t>(i)] > P.inverse_projector_cut * hs[0])) {
+          cut = i;
+          break;
+        }
+      double worst = 0.0;
+      for (int i = 0; i < cut; ++i) worst = std::max(worst, hr[static_cast<size_t>(i)]);
+      const double ratio = hs[0] > 0.0 ? worst / (kExactTol * hs[0]) : 0.0;
+      if (ratio <= 1.0 || b == kmax) {
+        DT<T> U = mm_rm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // nrow x b row-major
+        DT<T> V = mm_rm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));  // ncol x b row-major
+        DT<double> sinv({w}, st);
+        truncation(s.p, b, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut + slot, st);
+        Uc = DT<T>({nrow, w}, st);
+        scale_cols<T>(U.p, b, nrow, w, sinv.p, false, Uc.p, st);
+        Vc = DT<T>({ncol, w}, st);
+        scale_cols<T>(V.p, b, ncol, w, sinv.p, false, Vc.p, st);
+        if (proj_key >= 0) warm_v[proj_key] = mm_cm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));
+        return true;
+      }
+      // a stalled decay (a flat spectrum at the block edge): the dense SVD
+      if (prev_it > 0 && it > 12 && ratio > 0.5 * prev_ratio) break;
+      // iterations to the next check, from the decay seen between the last two
+      int gap = 3;
+      if (prev_it > 0 && ratio < prev_ratio) {
+        const double f = std::pow(ratio / prev_ratio, 1.0 / (it - prev_it));
+        gap = static_cast<int>(std::ceil(std::log(ratio) / -std::log(f)));
+        gap = std::min(16, std::max(1, gap));
+      }
+      prev_it = it;
+      prev_ratio = ratio;
+      next_check = it + gap;
+      Q = std::move(Y);
+      orth_chol(Q, nrow, b, next_check == it + 1 ? 4 : 2);
+    }
+    ++exact_dense;
+    return false;
+  }
+
   // Truncated projectors from M (nrow x ncol, consumed):
   // U_c (nrow x w), VT_c (w x ncol) scaled by 1/sqrt(s), w = min(k, chi)
   void truncated_factors(DT<T>& M, int64_t nrow, int64_t ncol, DT<T>& Uc, DT<T>& VTc) {
+    if (P.svd_solver == 0) {
+      const MV m = rm(M.p, nrow, ncol);
+      DT<T> Vc;
+      if (exact_factors(m, ht(m), nrow, ncol, Uc, Vc)) {
+        VTc = transpose<T>(Vc, {1, 0}, st, true);  // VT_c = V_c^H (w x ncol)
+        return;
+      }
+    }
     DT<T> U, VT;
     DT<double> s;
     svd(M, nrow, ncol, U, s, VT);
@@ -958,6 +1092,7 @@ struct EngineT final : Engine {
     const bool par = rows_parallel();
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
+      proj_key = (0 * 4096 + ix) * 4096 + iy;
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       if (P.projector_corner)
         proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
@@ -994,6 +1129,7 @@ struct EngineT final : Engine {
     prepare_rotations();  // before the rows fork
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
+      proj_key = (1 * 4096 + ix) * 4096 + iy;
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       if (P.projector_corner)
         proj_left_block(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], rot(k, 0), rot(j, 0), PUs[iy], PLs[iy]);
@@ -1030,6 +1166,7 @@ struct EngineT final : Engine {
     prepare_rotations();
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
+      proj_key = (2 * 4096 + iy) * 4096 + ix;
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       if (P.projector_corner)
         proj_left_block(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], rot(j, 1), rot(i, 1), PUs[ix], PLs[ix]);
@@ -1066,6 +1203,7 @@ struct EngineT final : Engine {
     prepare_rotations();
     std::vector<DT<T>> PUs(LX), PLs(LX);
     for_rows(LX, par, [&](int ix) {
+      proj_key = (3 * 4096 + iy) * 4096 + ix;
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       if (P.projector_corner)
         proj_left_block(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], rot(l, 2), rot(k, 2), PUs[ix], PLs[ix]);
@@ -2444,6 +2582,13 @@ struct EngineT final : Engine {
     spec_old_ok = false;
   }
   void get_env(int which, int site, double* host) override { download(env_ref(which, site), host); }
+  void svd_stats(int64_t* out) override {
+    out[0] = exact_solves;
+    out[1] = exact_iters;
+    out[2] = exact_checks;
+    out[3] = exact_dense;
+  }
+
   void sync() override {
     check_infos();
     TG_CUDA(cudaStreamSynchronize(st));

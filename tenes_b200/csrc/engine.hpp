@@ -44,6 +44,9 @@ struct Engine {
   virtual void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) = 0;
   virtual void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
                            double svd_broadening, double* energy, double* grad) = 0;
+  // counters of the exact truncated SVD of the full-SVD projectors:
+  // solves, subspace iterations, Rayleigh-Ritz checks, dense fallbacks
+  virtual void svd_stats(int64_t* out) = 0;
   virtual void sync() = 0;
   virtual void* stream() = 0;
 };

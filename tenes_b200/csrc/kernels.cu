@@ -1142,6 +1142,35 @@ __global__ void scale_cols_kernel(const T* __restrict__ U, int64_t ldu, int64_t 
   }
 }
 
+// r[j] = || P1[:, j] - s[j] P2[:, j] ||_2, one block per column j of the
+// column-major n-row panels P1, P2 (column j at j*n); fixed reduction order.
+__device__ __forceinline__ double abs2_of(double x) { return x * x; }
+__device__ __forceinline__ double abs2_of(cplx x) { return x.x * x.x + x.y * x.y; }
+__device__ __forceinline__ double sub_scaled_abs2(double a, double s, double b) { return abs2_of(a - s * b); }
+__device__ __forceinline__ double sub_scaled_abs2(cplx a, double s, cplx b) {
+  return abs2_of(make_double2(a.x - s * b.x, a.y - s * b.y));
+}
+
+template <typename T>
+__global__ void ritz_residual_kernel(const T* __restrict__ P1, const T* __restrict__ P2,
+                                     const double* __restrict__ s, int64_t n, double* __restrict__ r) {
+  const int j = blockIdx.x;
+  const T* a = P1 + static_cast<int64_t>(j) * n;
+  const T* b = P2 + static_cast<int64_t>(j) * n;
+  const double sj = s[j];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += sub_scaled_abs2(a[i], sj, b[i]);
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) r[j] = sqrt(v);
+  }
+}
+
 template <typename T>
 __global__ void scale_rows_kernel(const T* __restrict__ VT, int64_t ldv, int64_t cols, int kc,
                                   const double* __restrict__ sinv, bool conj, T* __restrict__ out) {
@@ -2317,6 +2346,14 @@ void scale_rows(const T* VT, int64_t ldv, int64_t cols, int kc, const double* si
 }
 
 template <typename T>
+void ritz_residual(const T* P1, const T* P2, const double* s, int64_t n, int w, double* r, cudaStream_t st) {
+  if (w < 1) return;
+  ritz_residual_kernel<T><<<w, 256, 0, st>>>(P1, P2, s, n, r);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
 void identity(T* out, int64_t e, cudaStream_t st) {
   identity_kernel<T><<<num_blocks(e * e, 256), 256, 0, st>>>(out, e);
   TG_CHECK_LAUNCH();
@@ -2462,6 +2499,7 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   template void scale_rows<T>(const T*, int64_t, int64_t, int, const double*, bool, T*,          \
                               cudaStream_t);                                                     \
   template void identity<T>(T*, int64_t, cudaStream_t);                                          \
+  template void ritz_residual<T>(const T*, const T*, const double*, int64_t, int, double*, cudaStream_t); \
   template void batched_spectrum<T>(const T* const*, int, int, double*, int*, cudaStream_t);     \
   template void scale<T>(T*, int64_t, double, cudaStream_t);                                     \
   template void axpy<T>(T*, const T*, double, int64_t, cudaStream_t);                            \

@@ -81,6 +81,11 @@ template <typename T>
 void scale_rows(const T* VT, int64_t ldv, int64_t cols, int kc, const double* sinv, bool conj,
                 T* out, cudaStream_t st);
 
+// Residuals of a Rayleigh-Ritz check: r[j] = || P1[:, j] - s[j] P2[:, j] ||_2
+// for j < w, with P1, P2 column-major n-row panels (column j at j*n).
+template <typename T>
+void ritz_residual(const T* P1, const T* P2, const double* s, int64_t n, int w, double* r, cudaStream_t st);
+
 // Identity projector reshaped to (e, 1, 1, e) (ctm.cpp:303-317).
 template <typename T>
 void identity(T* out, int64_t e, cudaStream_t st);

@@ -44,6 +44,7 @@ class CTMParams:
     inverse_lambda_cut: float = 1e-12
     mixed: bool = False
     cuda_graph: bool = True
+    svd_solver: int = 0
 
     def to_c(self) -> _lib.Params:
         p = _lib.Params()
@@ -173,6 +174,12 @@ class Environment:
         sig = C.c_double()
         check(self.lib.tg_ctm_run(self.ctx, int(initialize), C.byref(it), C.byref(conv), C.byref(sig)))
         return it.value, bool(conv.value), sig.value
+
+    def projector_svd_stats(self) -> dict:
+        """Counters of the exact truncated SVD of the full-SVD projectors."""
+        out = (C.c_int64 * 4)()
+        check(self.lib.tg_projector_svd_stats(self.ctx, out))
+        return {"solves": out[0], "iterations": out[1], "checks": out[2], "dense": out[3]}
 
     def corner_spectrum(self, which: int, i: int) -> np.ndarray:
         a = np.empty(self.params.chi, dtype=np.float64)

@@ -15,7 +15,8 @@ def pytest_configure(config):
 # The CTMRG path's parity and kernel tests run first; the rows built on top of
 # it (front end, gradients, full update, long-range correlations) follow, so
 # that a stop at the first failure (-x) still reports on the path itself.
-_LATE_FILES = ("test_gpu_frontend.py", "test_gpu_grad.py", "test_gpu_full_update.py", "test_gpu_local_gauge.py")
+_LATE_FILES = ("test_gpu_frontend.py", "test_gpu_grad.py", "test_gpu_full_update.py", "test_gpu_local_gauge.py",
+               "test_gpu_configs.py")
 
 
 def pytest_collection_modifyitems(session, config, items):
@@ -24,6 +25,8 @@ def pytest_collection_modifyitems(session, config, items):
         if name in _LATE_FILES:
             return 1 + _LATE_FILES.index(name)
         if item.name.startswith("test_correlation_strip"):
-            return 1 + len(_LATE_FILES)
+            return len(_LATE_FILES)
+        if name == "test_zz_no_alloc.py":
+            return 2 + len(_LATE_FILES)
         return 0
     items.sort(key=rank)  # stable: file and definition order within a rank
