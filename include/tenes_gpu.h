@@ -84,6 +84,23 @@ typedef struct tg_params {
                                        matrix.  Both give the reference's truncated factors. */
 } tg_params;
 
+/* One `tenes input.toml` run, as the reference's process-level entry point
+ *   extern "C" int tenes_itps_main(const char*, MPI_Comm, int)
+ * (src/iTPS/main.hpp:26-28, main.cpp:33-39) without the communicator (one
+ * GPU, device 0 unless CUDA_VISIBLE_DEVICES says otherwise): reads the expert
+ * input file, runs the simple / full update or the time evolution, the CTMRG
+ * environment and the measurements, and writes the reference's output files
+ * into the input's outdir (parameters.dat, density.dat, onesite_obs.dat,
+ * twosite_obs.dat, multisite_obs_*.dat, correlation*.dat, time.dat, or their
+ * TE_ forms).  Where the reference throws, this returns a status:
+ * TG_E_INPUT (bad or unsupported input, missing file), TG_E_LOAD (tensor
+ * checkpoint), TG_E_RUNTIME, TG_E_CUDA; the message is in tg_last_error().
+ * The run is the library's Python front end (tenes_b200.itps), embedded:
+ * from a process without Python the first call loads libpython
+ * (TENES_GPU_LIBPYTHON overrides which; TENES_GPU_PYTHON_SITE the packages
+ * directory).  Calls are serialised. */
+int tenes_gpu_main(const char* input_toml, int print_level);
+
 /* Fill *p with the reference defaults. */
 void tg_params_default(tg_params* p);
 

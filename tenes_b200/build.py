@@ -20,7 +20,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtenes_gpu.so")
-SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "adjoint.cu", "engine.cu", "api.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "adjoint.cu", "engine.cu", "api.cu", "noalloc.cu",
+           "main_entry.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -32,6 +33,18 @@ def cuda_home() -> str:
     if nvcc:
         return os.path.dirname(os.path.dirname(os.path.realpath(nvcc)))
     raise RuntimeError("nvcc not found")
+
+
+def python_defines():
+    """Where tenes_gpu_main finds the Python runtime and the packages of the
+    front end (numpy, scipy) when the calling process has no interpreter:
+    this interpreter's shared libpython and site-packages."""
+    import sysconfig
+    lib = os.path.join(sysconfig.get_config_var("LIBDIR") or "", sysconfig.get_config_var("INSTSONAME") or "")
+    if not os.path.exists(lib):
+        lib = "libpython3.so"
+    site = sysconfig.get_paths()["purelib"]
+    return [f'-DTG_PY_LIB="{lib}"', f'-DTG_PY_SITE="{site}"']
 
 
 def _newer(target: str, deps) -> bool:
@@ -52,17 +65,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
               "-I", CSRC, "--expt-relaxed-constexpr"] + ARCH
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
-        if force or _newer(o, [s] + headers):
-            cmd = [nvcc, "-c", s, "-o", o] + common
+        if force or _newer(o, [s, __file__] + headers):
+            cmd = [nvcc, "-c", s, "-o", o] + common + (python_defines() if src.endswith(".cpp") else [])
             if verbose:
                 print(" ".join(cmd))
             subprocess.check_call(cmd)
     libdir = os.path.join(cuda, "lib64")
     if force or _newer(LIB, objs):
         cmd = [nvcc, "-shared", "-o", LIB] + objs + ARCH + [
-            "-L", libdir, "-lcusolver", "-lcublas", "-Xlinker", "-rpath=" + libdir]
+            "-L", libdir, "-lcusolver", "-lcublas", "-ldl", "-Xlinker", "-rpath=" + libdir]
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)

@@ -158,6 +158,7 @@ struct EngineT final : Engine {
     for (auto& v : C) v.clear();
     for (auto& v : E) v.clear();
     spec_old = DT<double>();
+    warm_v.clear();  // every device tensor is freed on `st`, so before it is destroyed below
     if (st) cudaStreamSynchronize(st);
     cudaDeviceGraphMemTrim(dev);
     if (gj_params) cusolverDnDestroyGesvdjInfo(gj_params);

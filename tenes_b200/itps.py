@@ -35,6 +35,60 @@ def _fmt(x: float) -> str:
     return f"{x:.17e}"
 
 
+def _g(x) -> str:
+    """A number as C++'s default ostream formatting prints it (%g, 6 digits)."""
+    return format(x, "g") if isinstance(x, float) else str(int(x))
+
+
+def write_parameters(path: str, p, lattice) -> None:
+    """parameters.dat: PEPS_Parameters::save (PEPS_Parameters.cpp:220-300),
+    SquareLattice::save appended (SquareLattice.cpp:139-150) and the start
+    time (iTPS.cpp:145-150), line for line.  The reference's switch over the
+    calculation mode falls through from "time evolution" into "finite
+    temperature" (no break, PEPS_Parameters.cpp:282-287), so a time-evolution
+    run lists both; the file keeps that."""
+    import datetime
+    b = lambda v: "true" if v else "false"  # noqa: E731
+    lst = lambda v: "[" + ", ".join(_g(x) for x in v) + "]"  # noqa: E731
+    mode = {"ground_state": "ground state\n", "time_evolution": "time evolution\nfinite temperature\n",
+            "finite_temperature": "finite temperature\n"}[p.calcmode]
+    lines = [
+        f"simple_num_step = {lst(p.num_simple_step)}",
+        f"simple_tau = {lst([float(x) for x in p.tau_simple_step])}",
+        f"simple_inverse_lambda_cutoff = {_g(float(p.Inverse_lambda_cut))}",
+        f"simple_gauge_fix = {int(bool(p.Simple_Gauge_Fix))}",
+        f"simple_gauge_maxiter = {int(p.Simple_Gauge_maxiter)}",
+        f"simple_gauge_convergence_epsilon = {_g(float(p.Simple_Gauge_Convergence_Epsilon))}",
+        "",
+        f"full_num_step = {lst(p.num_full_step)}",
+        f"full_inverse_projector_cutoff = {_g(float(p.Inverse_projector_cut))}",
+        f"full_inverse_precision = {_g(float(p.Full_Inverse_precision))}",
+        f"full_convergence_epsilon = {_g(float(p.Full_Convergence_Epsilon))}",
+        f"full_iteration_max = {int(p.Full_max_iteration)}",
+        f"full_gauge_fix = {b(p.Full_Gauge_Fix)}",
+        f"full_fastfullupdate = {b(p.Full_Use_FastFullUpdate)}",
+        "",
+        f"ctm_dimension = {int(p.CHI)}",
+        f"ctm_inverse_projector_cutoff = {_g(float(p.Inverse_Env_cut))}",
+        f"ctm_convergence_epsilon = {_g(float(p.CTM_Convergence_Epsilon))}",
+        f"ctm_iteration_max = {int(p.Max_CTM_Iteration)}",
+        f"ctm_projector_corner = {b(p.CTM_Projector_corner)}",
+        f"use_rsvd = {b(p.Use_RSVD)}",
+        f"rsvd_oversampling_factor = {_g(float(p.RSVD_Oversampling_factor))}",
+        f"meanfield_env = {b(p.MeanField_Env)}",
+        "",
+    ]
+    text = "\n".join(lines) + "\n" + "mode = " + mode + "simple\n"
+    text += (f"Lcor = {int(getattr(p, 'Lcor', 0))}\nseed = {int(p.seed)}\nis_real = {int(bool(p.is_real))}\n"
+             f"iszero_tol = {_g(float(p.iszero_tol))}\nmeasure = {int(bool(p.to_measure))}\n"
+             f"tensor_load_dir = {p.tensor_load_dir}\ntensor_save_dir = {p.tensor_save_dir}\n"
+             f"outdir = {p.outdir}\n")
+    text += f"\nLsub = [ {lattice.LX} , {lattice.LY} ]\nskew = {lattice.skew}\n"
+    text += f"\nstart_datetime =  {datetime.datetime.now().astimezone().isoformat(timespec='seconds')}\n"
+    with open(path, "w") as f:
+        f.write(text)
+
+
 class ITPS:
     """iTPS<tensor> (src/iTPS/iTPS.hpp:97-234) over a device-resident Environment."""
 
@@ -76,6 +130,7 @@ class ITPS:
             self.env.init_tensors(p.seed, ls.initial_dirs, ls.noises)
         self.outdir = p.outdir
         os.makedirs(self.outdir, exist_ok=True)
+        write_parameters(os.path.join(self.outdir, "parameters.dat"), p, ls)
         n1 = self._names(inp.onesite, "onesite", False)
         n2 = self._names(inp.twosite, "twosite", False)
         nm = self._names(inp.multisite, "multisite", True)
@@ -617,6 +672,31 @@ class ITPS:
             f.write(f"time full update   = {self.t_fu}\n")
             f.write(f"time environment  = {self.t_env}\n")
             f.write(f"time observable    = {self.t_obs}\n")
+
+
+def run_status(path: str, print_level: int = 1, device: int = 0) -> Tuple[int, str]:
+    """The body of the C entry point tenes_gpu_main: run() with every error
+    turned into a tg_status code and a message, nothing raised (the
+    reference's tenes_itps_main lets its exceptions propagate,
+    src/iTPS/main.cpp:33-39; a C caller cannot catch them)."""
+    from ._lib import TG_E_INPUT, TG_E_LOAD, TG_E_RUNTIME, TGError
+    from .saveload import LoadError
+    try:
+        run(path, device=device, print_level=print_level)
+        return 0, ""
+    except InputError as e:
+        code, msg = TG_E_INPUT, f"input error: {e}"
+    except LoadError as e:
+        code, msg = TG_E_LOAD, f"load error: {e}"
+    except TGError as e:
+        code, msg = e.code, str(e)
+    except (OSError, FileNotFoundError) as e:
+        code, msg = TG_E_INPUT, f"input error: {e}"
+    except Exception as e:  # noqa: BLE001 -- every failure becomes a status code
+        code, msg = TG_E_RUNTIME, f"{type(e).__name__}: {e}"
+    if print_level > 0:
+        print(f"ERROR: {msg}", file=sys.stderr)
+    return code, msg
 
 
 def run(path: str, device: int = 0, mixed: bool = False, print_level: int = 1,

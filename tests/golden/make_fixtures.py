@@ -23,6 +23,11 @@ tree at run time:
   projectors) in the same form
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
+* parameters_dat.json     <- output_*/parameters.dat of the ground-state and
+  time-evolution goldens (PEPS_Parameters::save + SquareLattice::save + the
+  start time), the run-dependent start_datetime value removed
+
+The path of the TeNeS source tree is a required argument.
 """
 
 import json
@@ -115,6 +120,18 @@ def main(ref):
         with open(os.path.join(HERE, stem + "_expected.json"), "w") as f:
             json.dump(exp, f)
 
+    pdat = {}
+    for name, stem in (("TE_TFI", "te_tfi"), ("AntiferroHeisenberg_real", "afh_real"),
+                       ("AntiferroHeisenberg_complex", "afh_complex"), ("RSVD", "rsvd"),
+                       ("Honeycomb", "honeycomb"), ("Honeycomb_skew", "honeycomb_skew"),
+                       ("J1J2_AFH", "j1j2_afh")):
+        text = open(os.path.join(data, "output_" + name, "parameters.dat")).read()
+        pdat[stem] = "".join(line for line in text.splitlines(keepends=True)
+                             if not line.startswith("start_datetime"))
+    with open(os.path.join(HERE, "parameters_dat.json"), "w") as f:
+        json.dump({"files": pdat, "source": "test/data/output_*/parameters.dat, start_datetime line removed"}, f,
+                  indent=1)
+
     with tempfile.TemporaryDirectory() as td:
         exe = os.path.join(td, "mt")
         subprocess.check_call(["g++", "-O2", "-o", exe, os.path.join(REPO, "oracle", "mt19937_draws.cpp")])
@@ -127,4 +144,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <path of the TeNeS source tree>")
+    main(sys.argv[1])

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_symbols():
     txt = open(os.path.join(ROOT, "include", "tenes_gpu.h")).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(tg_[a-z0-9_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b((?:tg|tenes_gpu)_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_library_exports_every_declared_symbol():
