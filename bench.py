@@ -141,9 +141,46 @@ def make_env(cfg, seed, device, projector="svd", su_steps=None, precision="fp64"
             for s in range(env.N):
                 env.simple_update(s, -1, op1)
     env.sync()
-    log(f"[bench] {su_steps} simple-update steps in {time.perf_counter() - t0:.1f}s")
+    env.su_seconds = time.perf_counter() - t0
+    log(f"[bench] {su_steps} simple-update steps in {env.su_seconds:.2f}s")
     env.init_env()
     return env
+
+
+def su_rate_gpu(cfg, seed, device, steps=None):
+    """Simple-update steps/s of the library (one step = every bond of the
+    cell, plus the one-site operators of the Ising field), host wall clock
+    around a synchronised loop from the seeded start."""
+    env = make_env(cfg, seed, device, "svd", steps, "fp64")
+    n = CONFIGS[cfg]["su_steps"] if steps is None else steps
+    rate = n / env.su_seconds
+    env.close()
+    return rate
+
+
+def su_rate_oracle(cfg, seed, steps):
+    """The same for the CPU oracle (core::Simple_update_bond restated), on a
+    sample of `steps` steps."""
+    from oracle import tenes_oracle as O
+    c = CONFIGS[cfg]
+    D = c["D"]
+    lat = oracle_lattice(cfg)
+    Tn = O.initialize_tensors(lat, seed, True) if c["model"] == "afh" else uniform_tensors(D, seed)
+    lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
+    p = O.Params()
+    op, op1 = su_ops(cfg)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for (s, leg) in bonds(lat.LX, lat.LY):
+            tg = lat.neighbor(s, leg)
+            a, b, lc = O.simple_update_bond(Tn[s], Tn[tg], lam[s], lam[tg], op, leg, p)
+            lam[s][leg] = lc
+            lam[tg][(leg + 2) % 4] = lc
+            Tn[s], Tn[tg] = a, b
+        if op1 is not None:
+            for s in range(lat.N_UNIT):
+                Tn[s] = np.tensordot(Tn[s], op1, ([4], [0]))
+    return steps / (time.perf_counter() - t0)
 
 
 class Clocks:
@@ -245,11 +282,14 @@ def bond_energy(env, cfg="c3"):
 
 
 def prepare_tensors(cfg, seed, device, su_steps=None):
-    """Site tensors from the seeded simple update, run by the library."""
+    """Site tensors from the seeded simple update, run by the library, and
+    the simple update's steps/s."""
     env = make_env(cfg, seed, device, "svd", su_steps, "fp64")
     T = [env.get_site_tensor(i) for i in range(env.N)]
+    n = CONFIGS[cfg]["su_steps"] if su_steps is None else su_steps
+    rate = n / env.su_seconds if env.su_seconds > 0 else None
     env.close()
-    return T
+    return T, rate
 
 
 def env_for(cfg, T, device, projector, precision, max_iter=1):
@@ -399,7 +439,10 @@ def run_ours(args, rank, world, local_rank):
     device = local_rank
     torch.cuda.set_device(device)
     cfg = args.config
-    T = prepare_tensors(cfg, SEED + rank, device, args.su_steps)
+    T, su_rate = prepare_tensors(cfg, SEED + rank, device, args.su_steps)
+    su = {cfg: {"gpu_steps_per_s": su_rate}}
+    if not args.quick and cfg != "c1":
+        su["c1"] = {"gpu_steps_per_s": su_rate_gpu("c1", SEED + rank, device)}
     env = env_for(cfg, T, device, args.projector, args.precision)
     stream = torch.cuda.ExternalStream(env.stream_handle(), device=device)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
@@ -520,7 +563,7 @@ def run_ours(args, rank, world, local_rank):
                                                      - conv["fp64_rsvd"]["energy_per_site"])
     return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "roofline": roof, "arms": arms,
             "clocks": ck, "gpu_launches": launches, "sweep_ms": [round(t, 3) for t in times],
-            "converge": conv, "tensors": T}
+            "converge": conv, "tensors": T, "simple_update": su}
 
 
 def measured_peaks():
@@ -854,6 +897,18 @@ def main():
             line["time_to_converge"] = res["converge"]
         if oracle is not None:
             line["fp64_oracle_check"] = oracle
+        su = res["simple_update"]
+        if not args.no_cpu_baseline:
+            for c in su:
+                # a bounded CPU sample: 1000 bond updates or so
+                n = max(2, 1000 // (2 * 4 + (4 if CONFIGS[c]["model"] == "tfi" else 0)))
+                su[c]["cpu_oracle_steps_per_s"] = su_rate_oracle(c, SEED, n)
+                su[c]["cpu_oracle_sample_steps"] = n
+                if su[c]["gpu_steps_per_s"]:
+                    su[c]["speedup_gpu_vs_cpu_oracle"] = su[c]["gpu_steps_per_s"] / su[c]["cpu_oracle_steps_per_s"]
+        line["simple_update"] = {"step": "every bond of the 2x2 cell once (8 bond updates; the Ising workload also "
+                                         "applies its 4 one-site field operators), tau = 0.01",
+                                 "cpu_cores": os.cpu_count(), **su}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

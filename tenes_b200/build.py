@@ -20,8 +20,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtenes_gpu.so")
-SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "adjoint.cu", "engine.cu", "api.cu", "noalloc.cu",
-           "main_entry.cpp"]
+SOURCES = ["kernels.cu", "cholqr.cu", "skinny.cu", "su_fused.cu", "adjoint.cu", "engine.cu", "api.cu",
+           "noalloc.cu", "main_entry.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -82,6 +82,14 @@ struct EngineT final : Engine {
   int* d_flag = nullptr;  // set by device kernels on a numerical failure
   uint64_t noise_stream = 0;  // key sequence of the orthonormalisation perturbations
   int* d_cut = nullptr;
+  // Simple-update weights on the device, [(site * 4 + leg) * lam_ld + j]: the
+  // fused bond kernel reads and writes them there; `lambda` (host) is the
+  // copy the other paths use.  Either side may be the newer one.
+  double* d_lam = nullptr;
+  int lam_ld = 1;
+  bool lam_dev_stale = true, lam_host_stale = false;
+  int* d_su_flag = nullptr;
+  std::map<std::vector<double>, DT<T>> op_cache;  // evolution operators already on the device
   const T** d_ptrs = nullptr;
   const T** h_ptrs = nullptr;  // pinned
   double* h_sig = nullptr;     // pinned
@@ -121,6 +129,11 @@ struct EngineT final : Engine {
     TG_CUDA(cudaMalloc(&d_flag, sizeof(int)));
     TG_CUDA(cudaMemset(d_flag, 0, sizeof(int)));
     TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * (kRowStreams + 1)));
+    for (int i = 0; i < lat.N; ++i)
+      for (int l = 0; l < 4; ++l) lam_ld = std::max(lam_ld, lat.vdim[i][l]);
+    TG_CUDA(cudaMalloc(&d_lam, sizeof(double) * 4 * lat.N * lam_ld));
+    TG_CUDA(cudaMalloc(&d_su_flag, sizeof(int)));
+    TG_CUDA(cudaMemset(d_su_flag, 0, sizeof(int)));
     TG_CUDA(cudaMalloc(&d_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_ptrs, sizeof(T*) * 4 * lat.N));
     TG_CUDA(cudaMallocHost(&h_sig, sizeof(double) * 4 * lat.N));
@@ -159,6 +172,7 @@ struct EngineT final : Engine {
     for (auto& v : E) v.clear();
     spec_old = DT<double>();
     warm_v.clear();  // every device tensor is freed on `st`, so before it is destroyed below
+    op_cache.clear();
     if (st) cudaStreamSynchronize(st);
     cudaDeviceGraphMemTrim(dev);
     if (gj_params) cusolverDnDestroyGesvdjInfo(gj_params);
@@ -167,6 +181,8 @@ struct EngineT final : Engine {
     cudaFree(d_info);
     cudaFree(d_flag);
     cudaFree(d_cut);
+    cudaFree(d_lam);
+    cudaFree(d_su_flag);
     cudaFree(d_ptrs);
     cudaFreeHost(h_ptrs);
     cudaFreeHost(h_sig);
@@ -401,6 +417,12 @@ struct EngineT final : Engine {
     if (flag) {
       TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
       fail(TG_E_RUNTIME, "CholeskyQR orthonormalisation met a non-positive pivot (rank-deficient panel)");
+    }
+    TG_CUDA(cudaMemcpyAsync(&flag, d_su_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    if (flag) {
+      TG_CUDA(cudaMemsetAsync(d_su_flag, 0, sizeof(int), st));
+      fail(TG_E_RUNTIME, "simple update: the SVD of Theta did not converge (bond left unchanged)");
     }
     if (P.mixed && tc_fault_take())
       fail(TG_E_RUNTIME, "tensor-core product stopped waiting for its MMAs (results discarded)");
@@ -763,10 +785,15 @@ struct EngineT final : Engine {
   int proj_key = -1;             // set by the moves before each projector
   int64_t exact_solves = 0, exact_iters = 0, exact_checks = 0, exact_dense = 0;
 
+  // block size of the subspace iteration, or -1 where the dense SVD is the
+  // better choice: a matrix whose smaller dimension a block would span gains
+  // nothing from the iteration (and its first-sweep panels can be almost
+  // entirely null space), and chi too close to the largest block leaves no
+  // room for oversampling
   int exact_block(int64_t kmax) const {
     const int bmax = CPLX ? 84 : 96;  // CholeskyQR / Jacobi core sizes (one cluster, one CTA)
     const int64_t w = std::min<int64_t>(P.chi, kmax);
-    if (kmax <= bmax) return static_cast<int>(kmax);  // the block spans the smaller dimension
+    if (kmax <= bmax) return -1;
     const int64_t b = std::min<int64_t>(bmax, std::max<int64_t>(w + 16, w + w / 3));
     return b >= w + 8 ? static_cast<int>(b) : -1;
   }
@@ -817,9 +844,15 @@ struct EngineT final : Engine {
       DT<T> U1 = mm_cm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // u_i
       DT<double> r({w}, st);
       ritz_residual<T>(MV1.p, U1.p, s.p, nrow, w, r.p, st);
+      int pivot_flag = 0;
       TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * b, cudaMemcpyDeviceToHost, st));
       TG_CUDA(cudaMemcpyAsync(hr.data(), r.p, sizeof(double) * w, cudaMemcpyDeviceToHost, st));
+      TG_CUDA(cudaMemcpyAsync(&pivot_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
       TG_CUDA(cudaStreamSynchronize(st));
+      if (pivot_flag) {  // an orthonormalisation met a non-positive pivot: the dense SVD instead
+        TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+        break;
+      }
       // the kept triplets: the truncation rule of ctm.cpp:277-288
       int cut = w;
       for (int i = 0; i < w; ++i)
@@ -2183,12 +2216,72 @@ struct EngineT final : Engine {
     scale_leg<T>(t.p, outer, t.dim(ax), inner, dv.p, st);
   }
 
+  // the weights: device table <-> host vectors, whichever is newer
+  void lam_to_device() {
+    if (!lam_dev_stale) return;
+    std::vector<double> h(static_cast<size_t>(4 * lat.N * lam_ld), 0.0);
+    for (int i = 0; i < lat.N; ++i)
+      for (int l = 0; l < 4; ++l)
+        std::copy(lambda[i][l].begin(), lambda[i][l].end(), h.begin() + (i * 4 + l) * lam_ld);
+    TG_CUDA(cudaMemcpyAsync(d_lam, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    lam_dev_stale = false;
+  }
+  void lam_to_host() {
+    if (!lam_host_stale) return;
+    std::vector<double> h(static_cast<size_t>(4 * lat.N * lam_ld));
+    TG_CUDA(cudaMemcpyAsync(h.data(), d_lam, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    check_infos();
+    for (int i = 0; i < lat.N; ++i)
+      for (int l = 0; l < 4; ++l)
+        std::copy(h.begin() + (i * 4 + l) * lam_ld, h.begin() + (i * 4 + l) * lam_ld + lambda[i][l].size(),
+                  lambda[i][l].begin());
+    lam_host_stale = false;
+  }
+  const DT<T>& device_op(const double* op, int64_t n) {
+    std::vector<double> key(op, op + n * NW);
+    auto it = op_cache.find(key);
+    if (it != op_cache.end()) return it->second;
+    if (op_cache.size() >= 256) op_cache.clear();
+    DT<T> d = from_host({n}, op);
+    return op_cache.emplace(std::move(key), std::move(d)).first->second;
+  }
+
   // core::Simple_update_bond (core/simple_update.cpp:50-198)
   void su_bond(int source, int connect1, const double* op) override {
     check_site(source);
     if (connect1 < 0 || connect1 > 3) fail(TG_E_INPUT, "source_leg must be 0..3");
     const int target = lat.neighbor(source, connect1);
     const int connect2 = (connect1 + 2) % 4;
+    {
+      // the whole step in one thread block (su_fused.cu), in place
+      SuBondArgs a{};
+      for (int q = 0; q < 5; ++q) {
+        a.dims1[q] = static_cast<int>(Tn[source].dim(q));
+        a.dims2[q] = static_cast<int>(Tn[target].dim(q));
+      }
+      if (su_bond_fused_supported<T>(a.dims1, a.dims2, connect1, lam_ld)) {
+        lam_to_device();
+        const int64_t nop = static_cast<int64_t>(a.dims1[4]) * a.dims2[4] * a.dims1[4] * a.dims2[4];
+        a.tn1 = Tn[source].p;
+        a.tn2 = Tn[target].p;
+        a.lam = d_lam;
+        a.lam_ld = lam_ld;
+        a.site1 = source;
+        a.site2 = target;
+        a.connect1 = connect1;
+        a.op = device_op(op, nop).p;
+        a.lambda_cut = P.inverse_lambda_cut;
+        a.flag = d_su_flag;
+        su_bond_fused<T>(a, st);
+        lam_host_stale = true;
+        rot_ok[source] = rot_ok[target] = false;
+        return;
+      }
+    }
+    lam_to_host();
+    lam_dev_stale = true;
     static const int outer[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
     static const int to_last[4][5] = {{1, 2, 3, 0, 4}, {0, 2, 3, 1, 4}, {0, 1, 3, 2, 4}, {0, 1, 2, 3, 4}};
     static const int back1[4][5] = {{4, 0, 1, 2, 3}, {0, 4, 1, 2, 3}, {0, 1, 4, 2, 3}, {0, 1, 2, 4, 3}};
@@ -2309,6 +2402,8 @@ struct EngineT final : Engine {
       rot_ok[i] = false;
       for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
     }
+    lam_host_stale = false;  // the reset host weights are the current ones
+    lam_dev_stale = true;
   }
 
   // ------------------------------------------------------- full update
@@ -2463,6 +2558,8 @@ struct EngineT final : Engine {
   void su_fix_gauge(int maxiter, double eps, int* sweeps, double* score) override {
     if (maxiter < 0) fail(TG_E_INPUT, "gauge_maxiter must be non-negative");
     PrecScope prec(this, 0);
+    lam_to_host();
+    lam_dev_stale = true;
     FuBackend bk{this};
     gauge::LocalGauge<FuBackend> g{bk, P.inverse_lambda_cut};
     std::vector<DT<T>> tn(Tn.begin(), Tn.end());
@@ -2563,12 +2660,15 @@ struct EngineT final : Engine {
   void set_lambda(int site, int leg, const double* host) override {
     check_site(site);
     if (leg < 0 || leg > 3) fail(TG_E_INPUT, "leg must be 0..3");
+    lam_to_host();
     auto& l = lambda[site][leg];
     std::copy(host, host + l.size(), l.begin());
+    lam_dev_stale = true;
   }
   void get_lambda(int site, int leg, double* host) override {
     check_site(site);
     if (leg < 0 || leg > 3) fail(TG_E_INPUT, "leg must be 0..3");
+    lam_to_host();
     const auto& l = lambda[site][leg];
     std::copy(l.begin(), l.end(), host);
   }

@@ -86,6 +86,27 @@ void scale_rows(const T* VT, int64_t ldv, int64_t cols, int kc, const double* si
 template <typename T>
 void ritz_residual(const T* P1, const T* P2, const double* s, int64_t n, int w, double* r, cudaStream_t st);
 
+// One simple-update bond step (core::Simple_update_bond) in one thread
+// block, in place on the two site tensors; the weights of every (site, leg)
+// are read from and the new bond weights written to the device table
+// lam[(site * 4 + leg) * lam_ld + j].  *flag is set to 1 (tensors and
+// weights left unchanged) if Theta's Jacobi SVD does not converge.
+struct SuBondArgs {
+  void* tn1;
+  void* tn2;
+  double* lam;
+  int lam_ld;
+  int site1, site2, connect1;
+  int dims1[5], dims2[5];  // (l, u, r, b, p) of the two tensors
+  const void* op;          // op12 (d1, d2, d1, d2), row-major
+  double lambda_cut;       // Inverse_lambda_cut
+  int* flag;
+};
+template <typename T>
+bool su_bond_fused_supported(const int* dims1, const int* dims2, int connect1, int lam_ld);
+template <typename T>
+void su_bond_fused(const SuBondArgs& a, cudaStream_t st);
+
 // Identity projector reshaped to (e, 1, 1, e) (ctm.cpp:303-317).
 template <typename T>
 void identity(T* out, int64_t e, cudaStream_t st);
