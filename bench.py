@@ -813,6 +813,26 @@ def run_grad(args):
                       "grad_rel_err": float(np.linalg.norm(gmv - gv) / np.linalg.norm(gv))}}
 
 
+def run_gemm(spec):
+    """One contraction kernel alone, through tg_bench_gemm: spec = M N K
+    [layout] [prec] [iters]; layout 0: A row-major (M, K), B row-major (K, N);
+    1: B column-major (the rSVD panel products); prec 0: FP64 DMMA, 1: 3xTF32
+    on tcgen05.  Prints the average device time of one product and its
+    algorithmic rate (2 M N K flop)."""
+    import ctypes as C
+    from tenes_b200 import _lib
+    a = [int(x) for x in spec]
+    M, N, K = a[:3]
+    layout = a[3] if len(a) > 3 else 0
+    prec = a[4] if len(a) > 4 else 0
+    iters = a[5] if len(a) > 5 else 10
+    lib = _lib.load()
+    ms = C.c_double()
+    _lib.check(lib.tg_bench_gemm(M, N, K, layout, prec, iters, C.byref(ms)))
+    tf = 2.0 * M * N * K / (ms.value * 1e-3) / 1e12
+    print(f"M={M} N={N} K={K} layout={layout} prec={prec}: {ms.value * 1e3:.1f} us  {tf:.1f} TFLOP/s", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -837,7 +857,12 @@ def main():
                     help="gradient evaluations/s of the J1-J2 energy (D=3, chi=36) with the FD check")
     ap.add_argument("--grad-iters", type=int, default=GRAD["iterations"])
     ap.add_argument("--grad-fd", type=int, default=32, help="entries checked by central differences")
+    ap.add_argument("--gemm", nargs="+", metavar="M N K [layout prec iters]",
+                    help="time one contraction kernel alone (tg_bench_gemm) and exit")
     args = ap.parse_args()
+    if args.gemm:
+        run_gemm(args.gemm)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.grad:
         print(json.dumps(run_grad(args)), flush=True)

@@ -67,14 +67,6 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-#ifdef TG_CQ_TRACE
-__device__ unsigned g_cq_calls = 0;
-__device__ __forceinline__ unsigned long long cq_now() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-#endif
 
 // Upper Cholesky factor of the kp x kp matrix A (row stride ld, upper
 // triangle referenced) in place, blocked by 8.  For block J every warp that
@@ -86,15 +78,10 @@ __device__ __forceinline__ unsigned long long cq_now() {
 // end the diagonal blocks are replaced by their inverses (lower parts zero).
 // btab lists the upper 8 x 8 blocks row by row, so the trailing blocks of
 // block J are its suffix starting at (J+1) nb - J (J+1) / 2.
-__device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, double* dinv, const int* btab, int* flag,
-                                                 unsigned long long* tr = nullptr) {
+__device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, double* dinv, const int* btab, int* flag) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int nb = kp / 8, nblk = nb * (nb + 1) / 2;
   const int g = lane >> 2, t = lane & 3;
-#ifdef TG_CQ_TRACE
-  unsigned long long t0 = 0, t1 = 0;
-  if (tr) t0 = clock64();
-#endif
   for (int J = 0; J < nb; ++J) {
     const int j0 = 8 * J, ncol = kp - j0 - 8;
     double a[8][8];
@@ -134,13 +121,6 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
       }
     }
     __syncthreads();  // every warp has loaded the diagonal block
-#ifdef TG_CQ_TRACE
-    if (tr) {
-      t1 = clock64();
-      tr[0] += t1 - t0;
-      t0 = t1;
-    }
-#endif
     if (warp == 0 && lane < 8) {  // lane c writes column c of R'_JJ (no trailing block touches it)
 #pragma unroll
       for (int c = 0; c < 8; ++c)
@@ -171,13 +151,6 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
       }
     }
     __syncthreads();
-#ifdef TG_CQ_TRACE
-    if (tr) {
-      t1 = clock64();
-      tr[1] += t1 - t0;
-      t0 = t1;
-    }
-#endif
   }
   // diagonal blocks -> their inverses: warp J, lane c solves R'_JJ x = e_c
   for (int J = warp; J < nb; J += nw) {
@@ -198,12 +171,6 @@ __device__ __forceinline__ void cholesky_blocked(double* A, int kp, int ld, doub
     }
   }
   __syncthreads();
-#ifdef TG_CQ_TRACE
-  if (tr) {
-    t1 = clock64();
-    tr[2] += t1 - t0;
-  }
-#endif
 }
 
 __global__ void __launch_bounds__(CQ_THREADS, 1)
@@ -221,16 +188,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
   int* btab = reinterpret_cast<int*>(dinv + kp);  // (bi << 8) | bj of the upper 8 x 8 blocks
   const int nblk = nb * (nb + 1) / 2, total = nblk * 64;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-#ifdef TG_CQ_TRACE
-  unsigned call = 0;
-  unsigned long long tt[4][12] = {};
-  if (rank == 0 && tid == 0) call = atomicAdd(&g_cq_calls, 1u);
-  const bool trace = rank == 0 && tid == 0 && passes == 4 && ((call % 24) == 10 || (call % 24) == 11);
-#define CQ_T(p, i) \
-  if (trace && (p) < 4) tt[p][i] = cq_now();
-#else
-#define CQ_T(p, i)
-#endif
   if (tid == 0) {
     int q = 0;
     for (int bi = 0; bi < nb; ++bi)
@@ -269,7 +226,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
   if (resident && nch == 1) stage(r0, r1 - r0);
 
   for (int pass = 0; pass < passes; ++pass) {
-    CQ_T(pass, 0)
     // ---- 1. Gram partial of rows [r0, r1)
     double acc[CQ_SLOTS][2];
 #pragma unroll
@@ -292,7 +248,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       }
       if (!resident) __syncthreads();  // before the next chunk is staged
     }
-    CQ_T(pass, 1)
     // CTA 0's R' of the previous pass is read by the others until here
     if (pass > 0) cluster.sync();
 #pragma unroll
@@ -306,7 +261,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       }
     }
     cluster.sync();
-    CQ_T(pass, 2)
     // ---- 2. sum slice [e0, e1) of the entries over the cluster, in rank order
     {
       const int e0 = rank * per, e1 = min(total, e0 + per);
@@ -320,7 +274,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       }
     }
     cluster.sync();
-    CQ_T(pass, 3)
     // ---- 3. CTA 0: gather, equilibrate, shift, factor
     if (rank == 0) {
 #pragma unroll 4
@@ -348,20 +301,7 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
         }
       }
       __syncthreads();
-#ifdef TG_CQ_TRACE
-      if (trace && pass < 4) tt[pass][7] = cq_now();
-#endif
-#ifdef TG_CQ_TRACE
-      unsigned long long chtr[3] = {0, 0, 0};
-      cholesky_blocked(Rs, kp, ld, dinv, btab, flag, trace ? chtr : nullptr);
-      if (trace && pass < 4) {
-        tt[pass][8] = chtr[0];
-        tt[pass][9] = chtr[1];
-        tt[pass][10] = chtr[2];
-      }
-#else
       cholesky_blocked(Rs, kp, ld, dinv, btab, flag);
-#endif
       // R' and D to the global scratch, read from L2 by the other CTAs (a
       // broadcast from one SM's shared memory would serialise on that SM)
       for (int e = tid; e < total; e += CQ_THREADS) {
@@ -372,7 +312,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       __threadfence();
     }
     cluster.sync();
-    CQ_T(pass, 4)
     // ---- 4. R' and D from the scratch (L2 only: the lines change every pass)
     if (rank != 0) {
 #pragma unroll 4
@@ -383,7 +322,6 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
       for (int i = tid; i < kp; i += CQ_THREADS) ds[i] = __ldcg(scratch + kp * ld + i);
       __syncthreads();
     }
-    CQ_T(pass, 5)
     // ---- 5. X R' = Y D on 8-row blocks, X written over the rows in U
     const bool noisy = (pass == 0 && noise_scale != 0.0);
     for (int ch = 0; ch < nch; ++ch) {
@@ -458,18 +396,8 @@ __global__ void __launch_bounds__(CQ_THREADS, 1)
         if (!resident) __syncthreads();
       }
     }
-    CQ_T(pass, 6)
   }
   cluster.sync();  // CTA 0's shared memory is read by the others until here
-#ifdef TG_CQ_TRACE
-  if (trace) {
-    for (int p = 0; p < 4; ++p)
-      printf("cq n=%d k=%d pass %d: gram %.1f  sync %.1f  reduce %.1f  chol %.1f (prep %.1f, diag+row %.1f, trailing %.1f, inverses %.1f kcycles)  copy %.1f  trsm %.1f us\n",
-             n, k, p, (tt[p][1] - tt[p][0]) * 1e-3, (tt[p][2] - tt[p][1]) * 1e-3, (tt[p][3] - tt[p][2]) * 1e-3,
-             (tt[p][4] - tt[p][3]) * 1e-3, (tt[p][7] - tt[p][3]) * 1e-3, tt[p][8] * 1e-3, tt[p][9] * 1e-3,
-             tt[p][10] * 1e-3, (tt[p][5] - tt[p][4]) * 1e-3, (tt[p][6] - tt[p][5]) * 1e-3);
-  }
-#endif
 #undef CQ_T
 }
 

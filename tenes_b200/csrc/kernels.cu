@@ -1389,12 +1389,6 @@ __global__ void __launch_bounds__(kJG == 16 ? 768 : 1024) jacobi_svd_kernel(cons
   double* nrm = sm + (CPLX ? 4 : 2) * nn;     // n
   int* pos = reinterpret_cast<int*>(nrm + n);  // n
   __shared__ int rotated;
-#ifdef TG_JACOBI_TRACE
-  __shared__ int trace_rot;
-  if (threadIdx.x == 0) trace_rot = 0;
-  unsigned long long trace_t0;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(trace_t0));
-#endif
   for (int idx = threadIdx.x; idx < nn; idx += blockDim.x) {
     const int r = idx / n, c = idx % n;
     const T v = A[idx];
@@ -1534,23 +1528,11 @@ __global__ void __launch_bounds__(kJG == 16 ? 768 : 1024) jacobi_svd_kernel(cons
           nrm[q] = be + t * g;
           rotated = 1;
         }
-#ifdef TG_JACOBI_TRACE
-        if (gl == 0) atomicAdd(&trace_rot, 1);
-#endif
       }
       __syncthreads();
     }
     const int any = rotated;
     __syncthreads();
-#ifdef TG_JACOBI_TRACE  // sweep log for tuning builds (off in the library)
-    if (threadIdx.x == 0) {
-      unsigned long long now;
-      asm volatile("mov.u64 %0, %globaltimer;" : "=l"(now));
-      printf("jacobi_svd n=%d sweep=%d rotations=%d t=%.1f us\n", n, sweep, trace_rot, (now - trace_t0) * 1e-3);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) trace_rot = 0;
-#endif
     if (!any) break;
   }
   for (int c = warp; c < n; c += nw) {
@@ -2069,11 +2051,6 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   // up to two CTAs per SM (the kernel's occupancy), K chunks of at least 128
   if (d.batch == 1 && tiles < 148 && d.K >= 256)
     split = std::min<int64_t>(std::max<int64_t>(1, 296 / tiles), (d.K + 127) / 128);
-#ifdef TG_GEMM_TRACE  // shape log for tuning builds (off in the library)
-  fprintf(stderr, "gemm M=%lld N=%lld K=%lld batch=%lld sAm=%lld sAk=%lld sBk=%lld sBn=%lld split=%lld prec=%d\n",
-          (long long)d.M, (long long)d.N, (long long)d.K, (long long)d.batch, (long long)d.sAm, (long long)d.sAk,
-          (long long)d.sBk, (long long)d.sBn, (long long)split, d.prec);
-#endif
   if (split <= 1) {
     launch(grid, GemmParams<T>{A, B, C, d});
     TG_CHECK_LAUNCH();
@@ -2268,23 +2245,12 @@ void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>&
     // the outer strides are multiples of the run, so an even run keeps every run 16-byte aligned
     p.vec = !conj && (p.run % 2 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) &&
             (reinterpret_cast<uintptr_t>(out) % 16 == 0);
-#ifdef TG_PERM_TRACE  // shape log for tuning builds (off in the library)
-    fprintf(stderr, "permute runs: run=%u nruns=%u m=%d\n", p.run, p.nruns, m);
-#endif
     permute_runs_kernel<T><<<num_blocks(static_cast<int64_t>(p.nruns) * p.nchunks, 256, 148 * 16), 256, 0, st>>>(
         in, out, p);
     TG_CHECK_LAUNCH();
     count_launch();
     return;
   }
-#ifdef TG_PERM_TRACE
-  {
-    std::string sh_s, pm_s;
-    for (int i = 0; i < m; ++i) sh_s += std::to_string(ms[i]) + " ";
-    for (int i = 0; i < m; ++i) pm_s += std::to_string(mp[i]) + " ";
-    fprintf(stderr, "permute generic: merged shape [%s] perm [%s]\n", sh_s.c_str(), pm_s.c_str());
-  }
-#endif
   PermParams32 p{};
   p.rank = std::max(m, 1);
   p.conj = conj;
