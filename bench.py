@@ -50,8 +50,14 @@ CONFIGS = {
     "c3": dict(model="afh", D=6, chi=72, su_steps=300, name="afh_square_2x2_D6_chi72"),
     "c2": dict(model="afh", D=4, chi=32, su_steps=200, name="afh_square_2x2_D4_chi32"),
     "c1": dict(model="tfi", D=2, chi=10, su_steps=1000, name="tfi_square_2x2_D2_chi10_hx1"),
+    # Kitaev honeycomb on the brick wall, 4x4, complex, per-bond D from {3, 4, 5} (seeded), one vertical
+    # leg of every site of dimension 1, chi = 48; site tensors i.i.d. uniform[-1, 1] (real and imaginary
+    # parts); 40 CTMRG sweeps; energy per site and plaquette flux
+    "c5": dict(model="kitaev", D=5, dims=(3, 4, 5), chi=48, su_steps=0, sweeps=40,
+               name="kitaev_brickwall_4x4_D345_chi48_h0.05"),
 }
 HX = 1.0
+KITAEV_H = 0.05  # [111] field: -h (Sx + Sy + Sz) on every site
 TAU = 0.01
 SEED = 11
 L2_BYTES = 126 * 1024 * 1024
@@ -72,6 +78,92 @@ def lattice_spec(D):
     dirs = [[1.0, 0.0] if ((i % LX) + (i // LX)) % 2 == 0 else [0.0, 1.0] for i in range(N)]
     noises = [1e-2] * N
     return LX, LY, pd, vd, dirs, noises
+
+
+def brick_wall_dims(LX=4, LY=4, seed=5, dims=(3, 4, 5)):
+    """Virtual dimensions [site][left, up, right, bottom] of the honeycomb
+    lattice on the brick wall: every horizontal bond present, a vertical bond
+    only above the sites of odd x + y (the others have an up leg of dimension
+    1, so their left / right moves take the identity projector,
+    ctm.cpp:303-317); each present bond's dimension drawn from `dims`."""
+    rng = np.random.default_rng(seed)
+    N = LX * LY
+    right = lambda i: (i % LX + 1) % LX + (i // LX) * LX  # noqa: E731
+    top = lambda i: i % LX + ((i // LX + 1) % LY) * LX  # noqa: E731
+    vd = [[0] * 4 for _ in range(N)]
+    for i in range(N):
+        vd[i][2] = vd[right(i)][0] = int(rng.choice(dims))
+    for i in range(N):
+        x, y = i % LX, i // LX
+        vd[i][1] = vd[top(i)][3] = int(rng.choice(dims)) if (x + y) % 2 == 1 else 1
+    return vd
+
+
+def cell(cfg):
+    """(LX, LY, physical dims, virtual dims, initial directions, noises, complex) of a workload."""
+    c = CONFIGS[cfg]
+    if c["model"] == "kitaev":
+        vd = brick_wall_dims(dims=c["dims"])
+        return 4, 4, [2] * 16, vd, [[0.0, 0.0] for _ in range(16)], [0.0] * 16, True
+    LX, LY, pd, vd, dirs, noises = lattice_spec(c["D"])
+    return LX, LY, pd, vd, dirs, noises, False
+
+
+def random_complex_tensors(vd, seed):
+    """Site tensors with real and imaginary parts i.i.d. uniform[-1, 1]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for v in vd:
+        sh = (v[0], v[1], v[2], v[3], 2)
+        out.append(rng.uniform(-1.0, 1.0, sh) + 1j * rng.uniform(-1.0, 1.0, sh))
+    return out
+
+
+def kitaev_bond_list(vd, LX=4, LY=4):
+    """(site, dx, dy, Pauli-pair index) of every Kitaev bond: x and y bonds
+    alternate along the rows (x to the right of an even-parity site), z bonds
+    on the present vertical legs; the bond term is -K S^a S^a with K = 1."""
+    out = []
+    for i in range(LX * LY):
+        x, y = i % LX, i // LX
+        out.append((i, 1, 0, 0 if (x + y) % 2 == 0 else 1))
+        if vd[i][1] > 1:
+            out.append((i, 0, 1, 2))
+    return out
+
+
+def spin_half():
+    sx = np.array([[0.0, 0.5], [0.5, 0.0]], dtype=complex)
+    sy = np.array([[0.0, -0.5j], [0.5j, 0.0]])
+    sz = np.array([[0.5, 0.0], [0.0, -0.5]], dtype=complex)
+    return sx, sy, sz
+
+
+def hexagons(LX=4, LY=4):
+    """Bottom-left sites of the hexagons of the cell (odd x + y) and the Pauli
+    operator of each of the six sites on the 2 x 3 window -- the one of the
+    site's bond that leaves the hexagon: bottom row x, z, y; top row y, z, x."""
+    S = spin_half()
+    ops = {(1, 0): 2 * S[0], (1, 1): 2 * S[2], (1, 2): 2 * S[1], (0, 0): 2 * S[1], (0, 1): 2 * S[2], (0, 2): 2 * S[0]}
+    return [i for i in range(LX * LY) if ((i % LX) + (i // LX)) % 2 == 1], ops
+
+
+def kitaev_observables(env, vd):
+    """Energy per site (-K S^a S^a on every bond from the bond's reduced
+    density matrix, -h (Sx + Sy + Sz) on every site) and the mean plaquette
+    flux W_p = <prod_j sigma_j> over the cell's hexagons (2 x 3 windows)."""
+    S = spin_half()
+    tot = 0.0
+    for (s, dx, dy, a) in kitaev_bond_list(vd):
+        rho = env.contract_bond_rdm(s, dx, dy)
+        h = -np.einsum("ac,bd->abcd", S[a], S[a])
+        tot += (np.sum(h * rho) / np.einsum("abab->", rho)).real
+    f = S[0] + S[1] + S[2]
+    for s in range(env.N):
+        tot -= KITAEV_H * (env.contract_one_site(s, f) / env.contract_one_site(s, np.eye(2))).real
+    starts, ops = hexagons()
+    flux = [(env.contract_window(s, 2, 3, 1, 0, ops) / env.contract_window(s, 2, 3, 1, 0)).real for s in starts]
+    return tot / env.N, float(np.mean(flux))
 
 
 def bonds(LX, LY):
@@ -125,14 +217,17 @@ def make_env(cfg, seed, device, projector="svd", su_steps=None, precision="fp64"
     c = CONFIGS[cfg]
     D = c["D"]
     su_steps = c["su_steps"] if su_steps is None else su_steps
-    LX, LY, pd, vd, dirs, noises = lattice_spec(D)
-    env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector, precision), False, device=device)
+    LX, LY, pd, vd, dirs, noises, cx = cell(cfg)
+    env = Environment(LX, LY, pd, vd, ctm_params(cfg, projector, precision), cx, device=device)
     if c["model"] == "afh":
         env.init_tensors(seed, dirs, noises)
+    elif c["model"] == "kitaev":
+        for i, t in enumerate(random_complex_tensors(vd, seed)):
+            env.set_site_tensor(i, t)
     else:
         for i, t in enumerate(uniform_tensors(D, seed)):
             env.set_site_tensor(i, t)
-    op, op1 = su_ops(cfg)
+    op, op1 = su_ops(cfg) if su_steps else (None, None)
     t0 = time.perf_counter()
     for _ in range(su_steps):
         for (s, leg) in bonds(LX, LY):
@@ -165,6 +260,8 @@ def su_rate_oracle(cfg, seed, steps):
     c = CONFIGS[cfg]
     D = c["D"]
     lat = oracle_lattice(cfg)
+    if c["model"] == "kitaev":
+        return lat, random_complex_tensors(lat.virtual_dims, seed)
     Tn = O.initialize_tensors(lat, seed, True) if c["model"] == "afh" else uniform_tensors(D, seed)
     lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
     p = O.Params()
@@ -268,6 +365,8 @@ def bond_energy(env, cfg="c3"):
     identity (Contract_two_sites_*_op12 / norm, twosite_obs.cpp:180-225), both
     read from the bond's reduced density matrix (one contraction per bond);
     for the Ising workload plus the field term -hx <Sx> of every site."""
+    if CONFIGS[cfg]["model"] == "kitaev":
+        return kitaev_observables(env, cell(cfg)[3])[0]
     h = bond_hamiltonian(cfg)
     tot = 0.0
     for s in range(env.N):
@@ -294,10 +393,10 @@ def prepare_tensors(cfg, seed, device, su_steps=None):
 
 def env_for(cfg, T, device, projector, precision, max_iter=1):
     from tenes_b200.env import Environment
-    LX, LY, pd, vd, _, _ = lattice_spec(CONFIGS[cfg]["D"])
+    LX, LY, pd, vd, _, _, cx = cell(cfg)
     p = ctm_params(cfg, projector, precision)
     p.max_ctm_iteration = max_iter
-    env = Environment(LX, LY, pd, vd, p, False, device=device)
+    env = Environment(LX, LY, pd, vd, p, cx, device=device)
     for i, t in enumerate(T):
         env.set_site_tensor(i, t)
     env.init_env()
@@ -307,13 +406,14 @@ def env_for(cfg, T, device, projector, precision, max_iter=1):
 def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
     """Time to a converged environment: sweeps until the energy per site
     changes by at most `tol` between successive sweeps (energy evaluations
-    included in the wall time); the sweep at which the reference's own
-    corner-spectrum criterion (eps = 1e-6, ctm.cpp:815-969) first holds is
-    recorded too (the library's check, run after every sweep)."""
+    included in the wall time).  The sweeps go on, up to `max_sweeps`, until
+    the reference's own corner-spectrum criterion (eps = 1e-6,
+    ctm.cpp:815-969; the library's check after every sweep) holds as well,
+    and the sweep and time at which each criterion first held are reported."""
     env = env_for(cfg, T, device, projector, precision)
     env.sync()
     t0 = time.perf_counter()
-    e_prev, n, ref_conv, conv = None, 0, None, False
+    e_prev, n, ref_conv, ref_secs, conv, secs, n_conv, e_conv = None, 0, None, None, False, None, None, None
     e = float("nan")
     per_sweep = []  # (sweep, convergence check, energy) seconds
     energies = []
@@ -323,27 +423,30 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
         n += 1
         tc = time.perf_counter()
         c, _ = env.check_convergence()
-        if c and ref_conv is None:
-            ref_conv = n
         te = time.perf_counter()
         e = bond_energy(env, cfg)
         tz = time.perf_counter()
         energies.append(e)
         per_sweep.append([round(tc - ts, 4), round(te - tc, 4), round(tz - te, 4)])
-        if e_prev is not None and abs(e - e_prev) <= tol:
-            conv = True
+        if c and ref_conv is None:
+            ref_conv, ref_secs = n, tz - t0
+        if not conv and e_prev is not None and abs(e - e_prev) <= tol:
+            conv, secs, n_conv, e_conv = True, tz - t0, n, e
+        if conv and ref_conv is not None:
             break
         e_prev = e
-    secs = time.perf_counter() - t0
+    if not conv:
+        secs, n_conv, e_conv = time.perf_counter() - t0, n, e
     env.close()
     # host-side stalls (capture, allocator, other jobs on a shared machine) show
     # up as outliers of single sweeps; sweeps x the median sweep is the steady
     # rate's estimate of the same wall time
-    med = statistics.median(sum(x) for x in per_sweep) if per_sweep else 0.0
-    return {"sweeps": n, "seconds": secs, "seconds_sweeps_x_median": n * med, "converged": conv,
-            "energy_per_site": e, "last_delta_e": (abs(e - e_prev) if e_prev is not None else None),
-            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv, "energy_per_sweep": energies,
-            "seconds_per_sweep_sweep_check_energy": per_sweep}
+    med = statistics.median(sum(x) for x in per_sweep[:n_conv]) if per_sweep else 0.0
+    return {"sweeps": n_conv, "seconds": secs, "seconds_sweeps_x_median": n_conv * med, "converged": conv,
+            "energy_per_site": e_conv,
+            "last_delta_e": abs(energies[n_conv - 1] - energies[n_conv - 2]) if n_conv >= 2 else None,
+            "sweeps_to_corner_spectrum_eps_1e-6": ref_conv, "seconds_to_corner_spectrum_eps_1e-6": ref_secs,
+            "sweeps_run": n, "energy_per_sweep": energies, "seconds_per_sweep_sweep_check_energy": per_sweep}
 
 
 def max_over_ranks(ms, device, world):
@@ -578,7 +681,7 @@ def measured_peaks():
 # -------------------------------------------------------- CPU oracle (reference arm)
 def oracle_lattice(cfg):
     from oracle import tenes_oracle as O
-    LX, LY, pd, vd, dirs, noises = lattice_spec(CONFIGS[cfg]["D"])
+    LX, LY, pd, vd, dirs, noises, _ = cell(cfg)
     lat = O.Lattice(LX, LY)
     lat.physical_dims = pd
     lat.virtual_dims = vd
@@ -674,8 +777,11 @@ def oracle_check(cfg, T, sweeps):
 def config_block(args, world):
     """The `config` object, identical in both arms for the same flags."""
     c = CONFIGS[args.config]
+    kit = c["model"] == "kitaev"
     return {"workload": f"{c['name']}_{args.precision}_{args.projector}", "precision": args.precision,
-            "D": c["D"], "chi": c["chi"], "unit_cell": "2x2", "su_steps": c["su_steps"],
+            "D": "per bond from {3, 4, 5}, seeded; one vertical leg of 1 per site" if kit else c["D"],
+            "chi": c["chi"], "unit_cell": "4x4" if kit else "2x2", "su_steps": c["su_steps"],
+            "tensors": "complex128" if kit else "float64",
             "projector": ("full SVD (reference default)" if args.projector == "svd"
                           else f"rSVD k=chi+{RSVD_OVERSAMPLE}, q={RSVD_POWER}"),
             "parallelism": f"replicas{world}",

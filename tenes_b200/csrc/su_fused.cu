@@ -68,6 +68,13 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 __device__ __forceinline__ double warp_sum_t(double v) { return warp_sum(v); }
 __device__ __forceinline__ cplx warp_sum_t(cplx v) { return make_double2(warp_sum(v.x), warp_sum(v.y)); }
+// sum over the 16 lanes of a half-warp (every lane of the warp takes part)
+__device__ __forceinline__ double half_sum(double v) {
+  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double half_sum_t(double v) { return half_sum(v); }
+__device__ __forceinline__ cplx half_sum_t(cplx v) { return make_double2(half_sum(v.x), half_sum(v.y)); }
 
 // sum over the block, result returned to every thread (red: >= SU_WARPS doubles)
 __device__ double block_sum(double v, double* red) {
@@ -271,50 +278,60 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondArgs a) {
   for (int q = tid; q < acp * acp; q += SU_THREADS) JV[q] = from_re<T>(q % acp == q / acp ? 1.0 : 0.0);
   __syncthreads();
 
-  // one-sided Jacobi on the columns of JA (round-robin pairs, one warp a pair)
+  // one-sided Jacobi on the columns of JA (round-robin pairs, one half-warp a
+  // pair, so that the 16 half-warps of the block take up to 16 pairs of a round
+  // at once)
   const int lane = tid & 31, warp = tid >> 5;
+  const int hl = lane & 15, hw = tid >> 4;  // lane in the half-warp, half-warp index
   int sweep = 0;
   for (; sweep < SU_MAX_SWEEPS; ++sweep) {
     if (tid == 0) rotated = 0;
     __syncthreads();
     for (int rnd = 0; rnd < acp - 1; ++rnd) {
-      for (int pr = warp; pr < acp / 2; pr += SU_WARPS) {
+      // every half-warp runs the same number of passes, so that the shuffles
+      // below always have their full half-warp
+      for (int base = 0; base < acp / 2; base += 2 * SU_WARPS) {
+        const int pr = base + hw;
+        const bool live = pr < acp / 2;
         // circle method: slot 0 fixed, slots 1..acp-1 rotate
-        const int sa = pr, sb = acp - 1 - pr;
-        const int p = sa == 0 ? 0 : 1 + (sa - 1 + rnd) % (acp - 1);
-        const int q = 1 + (sb - 1 + rnd) % (acp - 1);
+        const int sa = live ? pr : 0, sb = acp - 1 - sa;
+        int p = sa == 0 ? 0 : 1 + (sa - 1 + rnd) % (acp - 1);
+        int q = 1 + (sb - 1 + rnd) % (acp - 1);
         T* cp = JA + static_cast<size_t>(p) * ar;
         T* cq = JA + static_cast<size_t>(q) * ar;
         double al = 0.0, be = 0.0;
         T ga = zero<T>();
-        for (int i = lane; i < ar; i += 32) {
-          al += abs2(cp[i]);
-          be += abs2(cq[i]);
-          ga = add(ga, mul(cj(cp[i]), cq[i]));
-        }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        ga = warp_sum_t(ga);
-        const double g = sqrt(abs2(ga));
-        if (g > 1e-15 * sqrt(al * be) && g > 0.0) {
-          const double zeta = (be - al) / (2.0 * g);
+        if (live)
+          for (int i = hl; i < ar; i += 16) {
+            al += abs2(cp[i]);
+            be += abs2(cq[i]);
+            ga = add(ga, mul(cj(cp[i]), cq[i]));
+          }
+        al = half_sum(al);
+        be = half_sum(be);
+        ga = half_sum_t(ga);
+        const double g2 = abs2(ga);
+        // rotate unless |g| <= 1e-15 sqrt(al be) (tested squared: no root on the common path)
+        if (live && g2 > 1e-30 * al * be && g2 > 0.0) {
+          const double rg = rsqrt(g2);                  // 1 / |g|
+          const double zeta = 0.5 * (be - al) * rg;      // (be - al) / (2 |g|)
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
-          const T e = phase(ga);  // g = |g| e
+          const double c = rsqrt(1.0 + t * t), sn = c * t;
+          const T e = scl(ga, rg);                       // g = |g| e
           const T se = scl(e, sn), sec = scl(cj(e), sn);
-          for (int i = lane; i < ar; i += 32) {
+          for (int i = hl; i < ar; i += 16) {
             const T x = cp[i], y = cq[i];
             cp[i] = sub(scl(x, c), mul(sec, y));
             cq[i] = add(mul(se, x), scl(y, c));
           }
           T* vp = JV + static_cast<size_t>(p) * acp;
           T* vq = JV + static_cast<size_t>(q) * acp;
-          for (int i = lane; i < acp; i += 32) {
+          for (int i = hl; i < acp; i += 16) {
             const T x = vp[i], y = vq[i];
             vp[i] = sub(scl(x, c), mul(sec, y));
             vq[i] = add(mul(se, x), scl(y, c));
           }
-          if (lane == 0) rotated = 1;
+          if (hl == 0) rotated = 1;
         }
       }
       __syncthreads();
