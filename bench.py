@@ -260,8 +260,6 @@ def su_rate_oracle(cfg, seed, steps):
     c = CONFIGS[cfg]
     D = c["D"]
     lat = oracle_lattice(cfg)
-    if c["model"] == "kitaev":
-        return lat, random_complex_tensors(lat.virtual_dims, seed)
     Tn = O.initialize_tensors(lat, seed, True) if c["model"] == "afh" else uniform_tensors(D, seed)
     lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
     p = O.Params()
@@ -449,6 +447,23 @@ def converge(cfg, T, device, projector, precision, tol=1e-7, max_sweeps=40):
             "sweeps_run": n, "energy_per_sweep": energies, "seconds_per_sweep_sweep_check_energy": per_sweep}
 
 
+def kitaev_run(cfg, T, device, projector, precision="fp64"):
+    """The Kitaev workload's run: a fixed number of sweeps from the initial
+    environment, timed on the host around synchronised sweeps, then the energy
+    per site and the mean plaquette flux."""
+    n = CONFIGS[cfg]["sweeps"]
+    env = env_for(cfg, T, device, projector, precision)
+    env.sync()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        env.sweep()
+    env.sync()
+    secs = time.perf_counter() - t0
+    e, w = kitaev_observables(env, cell(cfg)[3])
+    env.close()
+    return {"sweeps": n, "seconds": secs, "sweeps_per_s": n / secs, "energy_per_site": e, "plaquette_flux": w}
+
+
 def max_over_ranks(ms, device, world):
     """The largest of the ranks' times (all-reduce MAX over the process
     group); unchanged for a single rank."""
@@ -542,8 +557,9 @@ def run_ours(args, rank, world, local_rank):
     device = local_rank
     torch.cuda.set_device(device)
     cfg = args.config
+    kit = CONFIGS[cfg]["model"] == "kitaev"
     T, su_rate = prepare_tensors(cfg, SEED + rank, device, args.su_steps)
-    su = {cfg: {"gpu_steps_per_s": su_rate}}
+    su = {} if kit else {cfg: {"gpu_steps_per_s": su_rate}}
     if not args.quick and cfg != "c1":
         su["c1"] = {"gpu_steps_per_s": su_rate_gpu("c1", SEED + rank, device)}
     env = env_for(cfg, T, device, args.projector, args.precision)
@@ -635,6 +651,8 @@ def run_ours(args, rank, world, local_rank):
     if not args.quick:
         for tag, proj, prec, k in (("mixed_rsvd", "rsvd", "mixed", args.steps), ("fp64_rsvd", "rsvd", "fp64",
                                    args.steps), ("fp64_full_svd", "svd", "fp64", min(args.steps, 3))):
+            if kit and prec == "mixed":
+                continue  # the tensor-core form takes real tensors only
             if proj == args.projector and prec == args.precision:
                 arms[tag] = {"sweeps_per_s": value / world, "ms_per_sweep": ms_per_step, "headline": True}
                 continue
@@ -653,7 +671,12 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- time to a converged environment: mixed and FP64 at the same projector, and FP64 full SVD
     conv = None
-    if args.converge != "none":
+    if args.converge != "none" and kit:
+        conv = {"criterion": f"{CONFIGS[cfg]['sweeps']} sweeps from the initial environment (fixed count)",
+                "fp64_rsvd": kitaev_run(cfg, T, device, "rsvd")}
+        if args.converge == "full":
+            conv["fp64_full_svd"] = kitaev_run(cfg, T, device, "svd")
+    elif args.converge != "none":
         conv = {"criterion": "|E/site(sweep t) - E/site(sweep t-1)| <= 1e-7 (energy evaluations timed too)"}
         conv["mixed_rsvd"] = converge(cfg, T, device, "rsvd", "mixed")
         conv["fp64_rsvd"] = converge(cfg, T, device, "rsvd", "fp64")
@@ -705,6 +728,8 @@ def oracle_tensors(cfg, seed):
     c = CONFIGS[cfg]
     D = c["D"]
     lat = oracle_lattice(cfg)
+    if c["model"] == "kitaev":
+        return lat, random_complex_tensors(lat.virtual_dims, seed)
     Tn = O.initialize_tensors(lat, seed, True) if c["model"] == "afh" else uniform_tensors(D, seed)
     lam = [[np.ones(D) for _ in range(4)] for _ in range(lat.N_UNIT)]
     p = O.Params()
@@ -733,10 +758,47 @@ def oracle_moves(lat):
     return mv
 
 
+def oracle_kitaev(oe, Tn, lat):
+    """Energy per site and mean plaquette flux of the oracle's environment
+    (the same terms and windows as kitaev_observables)."""
+    from oracle import tenes_oracle as O
+    S = spin_half()
+    one = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    tot = 0.0
+    for (s, dx, dy, a) in kitaev_bond_list(lat.virtual_dims):
+        h = -np.einsum("ac,bd->abcd", S[a], S[a])
+        if dy == 0:
+            l, r = s, lat.other(s, 1, 0)
+            arg = (oe.C1[l], oe.C2[r], oe.C3[r], oe.C4[l], oe.eTt[l], oe.eTt[r], oe.eTr[r], oe.eTb[r], oe.eTb[l],
+                   oe.eTl[l], Tn[l], Tn[r])
+            tot += (O.contract_two_sites_horizontal_op12(*arg, h)
+                    / O.contract_two_sites_horizontal_op12(*arg, one)).real
+        else:
+            t, b = lat.other(s, 0, 1), s
+            arg = (oe.C1[t], oe.C2[t], oe.C3[b], oe.C4[b], oe.eTt[t], oe.eTr[t], oe.eTr[b], oe.eTb[b], oe.eTl[b],
+                   oe.eTl[t], Tn[t], Tn[b])
+            tot += (O.contract_two_sites_vertical_op12(*arg, h.transpose(1, 0, 3, 2))
+                    / O.contract_two_sites_vertical_op12(*arg, one)).real
+    f = S[0] + S[1] + S[2]
+    for i in range(lat.N_UNIT):
+        a = (oe.C1[i], oe.C2[i], oe.C3[i], oe.C4[i], oe.eTt[i], oe.eTr[i], oe.eTb[i], oe.eTl[i], Tn[i])
+        tot -= KITAEV_H * (O.contract_one_site(*a, f) / O.contract_one_site(*a, np.eye(2))).real
+    starts, ops = hexagons()
+    flux = []
+    for s in starts:
+        _, Cs, eTt, eTr, eTb, eTl, T = O._window(oe, Tn, lat, s, 0, 1, 2, 3)
+        grid = [[ops.get((r, c), np.eye(2)) for c in range(3)] for r in range(2)]
+        flux.append((O.contract_window(Cs, eTt, eTr, eTb, eTl, T, grid)
+                     / O.contract_window(Cs, eTt, eTr, eTb, eTl, T, [[np.eye(2)] * 3 for _ in range(2)])).real)
+    return tot / lat.N_UNIT, float(np.mean(flux))
+
+
 def oracle_energy(cfg, oe, Tn, lat):
     """Energy per site of the oracle's environment (op12 contractions / norm,
     twosite_obs.cpp; the Ising field through the one-site contraction)."""
     from oracle import tenes_oracle as O
+    if CONFIGS[cfg]["model"] == "kitaev":
+        return oracle_kitaev(oe, Tn, lat)[0]
     h = bond_hamiltonian(cfg)
     one = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
     tot = 0.0
@@ -771,7 +833,16 @@ def oracle_check(cfg, T, sweeps):
             t0 = time.perf_counter()
             fn(oe, T, line, p, lat)
             move_s.append(time.perf_counter() - t0)
-    return move_s, oracle_energy(cfg, oe, T, lat)
+    if CONFIGS[cfg]["model"] == "kitaev":
+        e, w = oracle_kitaev(oe, T, lat)
+        return move_s, e, w
+    return move_s, oracle_energy(cfg, oe, T, lat), None
+
+
+def data_note(cfg):
+    if CONFIGS[cfg]["model"] == "kitaev":
+        return "synthetic (site tensors with i.i.d. uniform[-1, 1] real and imaginary parts, seeded)"
+    return "synthetic (seeded simple-update tensors of the workload's shapes)"
 
 
 def config_block(args, world):
@@ -818,7 +889,7 @@ def run_reference(args, rank, world):
     return {"metric": "ctmrg_sweeps_per_s", "value": v, "unit": "sweeps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded simple-update tensors of the workload's shapes)", "impl": "reference",
+            "data": data_note(args.config), "impl": "reference",
             "config": config_block(args, world),
             "step": f"one CTMRG move (1/{len(moves)} of a sweep), moves of consecutive sweeps in sweep order",
             "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": cores, "kind": "port",
@@ -999,9 +1070,8 @@ def main():
             # The oracle from the GPU's own site tensors, as many sweeps as the
             # FP64 rSVD arm took to converge: its first sweep is the CPU
             # baseline sample, its energy pins every arm's energy.
-            n_sw = (res["converge"]["fp64_rsvd"]["sweeps"] if res["converge"] else 1) if args.config == "c3" \
-                else (res["converge"]["fp64_rsvd"]["sweeps"] if res["converge"] else 3)
-            move_s, e_or = oracle_check(args.config, res["tensors"], n_sw)
+            n_sw = res["converge"]["fp64_rsvd"]["sweeps"] if res["converge"] else 1
+            move_s, e_or, w_or = oracle_check(args.config, res["tensors"], n_sw)
             per = len(oracle_moves(oracle_lattice(args.config)))
             first = sum(move_s[:per])
             cpu = {"value": 1.0 / first, "unit": "sweeps/s", "cores": os.cpu_count(), "kind": "port",
@@ -1009,7 +1079,12 @@ def main():
                              f"the same projectors (rSVD k=chi+{RSVD_OVERSAMPLE}, q={RSVD_POWER}) from the same "
                              "site tensors"}
             oracle = {"sweeps": n_sw, "energy_per_site": e_or, "seconds_per_sweep": sum(move_s) / n_sw}
-            if res["converge"]:
+            if w_or is not None and res["converge"]:
+                arm = res["converge"]["fp64_rsvd"]
+                oracle["plaquette_flux"] = w_or
+                oracle["abs_delta_e_fp64_rsvd"] = abs(arm["energy_per_site"] - e_or)
+                oracle["abs_delta_flux_fp64_rsvd"] = abs(arm["plaquette_flux"] - w_or)
+            elif res["converge"]:
                 for tag in ("mixed_rsvd", "fp64_rsvd", "fp64_full_svd"):
                     arm = res["converge"].get(tag)
                     if arm and len(arm["energy_per_sweep"]) >= n_sw:
@@ -1018,7 +1093,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64",
-                "data": "synthetic (seeded simple-update tensors of the workload's shapes)",
+                "data": data_note(args.config),
                 "config": config_block(args, world),
                 "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res["e2e"],
                 "clocks": res["clocks"], "gpu_launches": res["gpu_launches"], "sweep_ms": res["sweep_ms"]}
@@ -1029,7 +1104,7 @@ def main():
         if oracle is not None:
             line["fp64_oracle_check"] = oracle
         su = res["simple_update"]
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and su:
             for c in su:
                 # a bounded CPU sample: 1000 bond updates or so
                 n = max(2, 1000 // (2 * 4 + (4 if CONFIGS[c]["model"] == "tfi" else 0)))
@@ -1037,9 +1112,10 @@ def main():
                 su[c]["cpu_oracle_sample_steps"] = n
                 if su[c]["gpu_steps_per_s"]:
                     su[c]["speedup_gpu_vs_cpu_oracle"] = su[c]["gpu_steps_per_s"] / su[c]["cpu_oracle_steps_per_s"]
-        line["simple_update"] = {"step": "every bond of the 2x2 cell once (8 bond updates; the Ising workload also "
-                                         "applies its 4 one-site field operators), tau = 0.01",
-                                 "cpu_cores": os.cpu_count(), **su}
+        if su:
+            line["simple_update"] = {"step": "every bond of the 2x2 cell once (8 bond updates; the Ising workload also "
+                                             "applies its 4 one-site field operators), tau = 0.01",
+                                     "cpu_cores": os.cpu_count(), **su}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -88,3 +88,43 @@ def test_kitaev_brick_wall_complex_4x4():
              / O.contract_one_site(e.C1[i], e.C2[i], e.C3[i], e.C4[i], e.eTt[i], e.eTr[i], e.eTb[i], e.eTl[i],
                                    Tn[i], np.eye(2)))
         assert abs(g - o) <= 1e-9 * max(abs(o), 1e-3)
+
+
+def test_kitaev_c5_shapes_ctm_energy_and_flux():
+    """The Kitaev workload at its own shapes: 4x4 brick wall, per-bond D drawn
+    from {3, 4, 5} by the seed, chi = 48, complex site tensors with i.i.d.
+    uniform[-1, 1] parts; three CTMRG iterations with the reference's full-SVD
+    corner projectors on both sides, then the corner spectra, every Kitaev bond
+    term and the plaquette flux W_p = <prod sigma> of the cell's eight
+    hexagons (2 x 3 windows), GPU against the oracle."""
+    import bench
+    vd = bench.brick_wall_dims(dims=(3, 4, 5))
+    lat = O.Lattice(4, 4)
+    lat.physical_dims = [2] * 16
+    lat.virtual_dims = vd
+    Tn = bench.random_complex_tensors(vd, 11)
+    chi, iters = 48, 3
+    oe, ocnt, _, _ = O.calc_ctm_environment(Tn, oracle_params(chi, Max_CTM_Iteration=iters), lat)
+    ge = gpu_env(lat, Tn, chi, True, max_ctm_iteration=iters)
+    gcnt, _, _ = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt
+    for w, name in enumerate(("C1", "C2", "C3", "C4")):
+        for i in range(lat.N_UNIT):
+            g, o = ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i])
+            g = g[:len(o)] if len(g) > len(o) else g
+            err = np.linalg.norm(g - o[:len(g)]) / np.linalg.norm(o)
+            assert err <= 1e-9, (name, i, err)
+    ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    for (s, dx, dy, op) in kitaev_bonds(lat):
+        g = ge.contract_bond_op12(s, dx, dy, op) / ge.contract_bond_op12(s, dx, dy, ident)
+        o = oracle_bond(oe, Tn, lat, s, dx, dy, op) / oracle_bond(oe, Tn, lat, s, dx, dy, ident)
+        assert abs(g - o) <= 1e-9 * max(abs(o), 1e-3), (s, dx, dy, g, o)
+    starts, ops = bench.hexagons()
+    for s in starts:
+        _, Cs, eTt, eTr, eTb, eTl, T = O._window(oe, Tn, lat, s, 0, 1, 2, 3)
+        grid = [[ops.get((r, c), np.eye(2)) for c in range(3)] for r in range(2)]
+        o = (O.contract_window(Cs, eTt, eTr, eTb, eTl, T, grid)
+             / O.contract_window(Cs, eTt, eTr, eTb, eTl, T, [[np.eye(2)] * 3 for _ in range(2)]))
+        g = ge.contract_window(s, 2, 3, 1, 0, ops) / ge.contract_window(s, 2, 3, 1, 0)
+        assert abs(g - o) <= 1e-9 * max(abs(o), 1e-3), (s, g, o)
+    ge.close()
