@@ -31,7 +31,9 @@ SHAPES = [(128, 128, 16), (200, 37, 100), (36, 1000, 72), (1000, 36, 72), (2592,
           (1, 1, 1), (17, 300, 5),
           # one side <= 96 and the other >= 2048: the streaming kernel for long operands
           (36, 5000, 72), (5000, 72, 36), (72, 4100, 35), (4099, 17, 96), (96, 4096, 1), (5, 6000, 3),
-          (2592, 82, 82), (72, 2592, 72), (2048, 96, 96)]
+          (2592, 82, 82), (72, 2592, 72), (2048, 96, 96),
+          # FP64: a 96-wide column tile where it pads N less than 64-wide ones, with and without split-K
+          (300, 90, 500), (700, 95, 16), (1500, 72, 200), (4000, 72, 64), (130, 250, 2000)]
 
 
 @pytest.mark.parametrize("M,N,K", SHAPES)
