@@ -214,6 +214,13 @@ tg_status tg_tm_eigenvalues(tg_ctx* ctx, int dir, int fixed, int num_eigvals, in
  * `source` and its neighbour on `source_leg`; op is (d1, d2, d1, d2). */
 tg_status tg_su_onesite(tg_ctx* ctx, int site, const double* op);
 tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op);
+/* A sequence of simple-update steps applied in its order, as n calls of
+ * tg_su_onesite (source_legs[i] < 0) and tg_su_bond would apply them -- one
+ * Trotter step of iTPS::simple_update over the evolution operators
+ * (src/iTPS/simple_update.cpp:113-119).  Consecutive bond steps on pairwise
+ * disjoint site pairs commute exactly, so each run of them is one launch with
+ * one thread block a bond.  ops[i] points at operator i. */
+tg_status tg_su_bonds(tg_ctx* ctx, int n, const int* sources, const int* source_legs, const double* const* ops);
 
 /* Full update of one bond (PEPS_Parameters full-update knobs,
  * src/iTPS/PEPS_Parameters.cpp:57-62; keys of [parameter.full_update] in

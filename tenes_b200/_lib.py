@@ -29,7 +29,7 @@ EXPORTED = [
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
     "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_su_fix_gauge", "tg_measure_correlation",
-    "tg_projector_svd_stats", "tenes_gpu_main",
+    "tg_projector_svd_stats", "tenes_gpu_main", "tg_su_bonds",
 ]
 
 
@@ -99,6 +99,7 @@ def load() -> C.CDLL:
         "tg_ctm_check_convergence": (C.c_int, [vp, P(C.c_int), dp]),
         "tg_projector_svd_stats": (C.c_int, [vp, P(C.c_int64)]),
         "tenes_gpu_main": (C.c_int, [C.c_char_p, C.c_int]),
+        "tg_su_bonds": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int), P(C.c_void_p)]),
         "tg_ctm_run": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int), dp]),
         "tg_corner_spectrum": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "tg_measure_onesite": (C.c_int, [vp, C.c_int, dp, dp]),

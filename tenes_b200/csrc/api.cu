@@ -229,6 +229,16 @@ tg_status tg_su_bond(tg_ctx* ctx, int source, int source_leg, const double* op) 
     E(ctx)->su_bond(source, source_leg, op);
   });
 }
+tg_status tg_su_bonds(tg_ctx* ctx, int n, const int* sources, const int* source_legs, const double* const* ops) {
+  return guard([&] {
+    if (n > 0) {
+      need(sources, "sources");
+      need(source_legs, "source_legs");
+      need(ops, "ops");
+    }
+    E(ctx)->su_bonds(n, sources, source_legs, ops);
+  });
+}
 tg_status tg_init_tensors(tg_ctx* ctx, int seed, const double* initial_dirs, const int* dir_len,
                           const double* noises) {
   return guard([&] {

@@ -2239,13 +2239,82 @@ struct EngineT final : Engine {
                   lambda[i][l].begin());
     lam_host_stale = false;
   }
+  // the device copy of an evolution operator; the cache is emptied only
+  // between launches (trim_op_cache), never while a batch holds its pointers
   const DT<T>& device_op(const double* op, int64_t n) {
     std::vector<double> key(op, op + n * NW);
     auto it = op_cache.find(key);
     if (it != op_cache.end()) return it->second;
-    if (op_cache.size() >= 256) op_cache.clear();
     DT<T> d = from_host({n}, op);
     return op_cache.emplace(std::move(key), std::move(d)).first->second;
+  }
+  void trim_op_cache(size_t incoming) {
+    if (op_cache.size() + incoming > 256) op_cache.clear();
+  }
+  // the arguments of the fused bond step, or false when its shapes need the
+  // multi-launch path
+  bool fused_args(int source, int connect1, const double* op, SuBondArgs& a) {
+    const int target = lat.neighbor(source, connect1);
+    for (int q = 0; q < 5; ++q) {
+      a.dims1[q] = static_cast<int>(Tn[source].dim(q));
+      a.dims2[q] = static_cast<int>(Tn[target].dim(q));
+    }
+    if (!su_bond_fused_supported<T>(a.dims1, a.dims2, connect1, lam_ld)) return false;
+    const int64_t nop = static_cast<int64_t>(a.dims1[4]) * a.dims2[4] * a.dims1[4] * a.dims2[4];
+    a.tn1 = Tn[source].p;
+    a.tn2 = Tn[target].p;
+    a.lam = d_lam;
+    a.lam_ld = lam_ld;
+    a.site1 = source;
+    a.site2 = target;
+    a.connect1 = connect1;
+    a.op = device_op(op, nop).p;
+    a.lambda_cut = P.inverse_lambda_cut;
+    a.flag = d_su_flag;
+    return true;
+  }
+
+  // A sequence of simple-update steps in its order (legs[i] < 0: one-site).
+  // Consecutive bond steps on pairwise disjoint site pairs commute -- none
+  // reads a tensor or a weight that another writes -- so each run of them
+  // goes to the device as one launch of one block per bond.
+  void su_bonds(int n, const int* sources, const int* legs, const double* const* ops) override {
+    if (n < 0) fail(TG_E_INPUT, "negative count");
+    trim_op_cache(static_cast<size_t>(n));
+    std::vector<SuBondArgs> group;
+    std::vector<char> busy(static_cast<size_t>(lat.N), 0);
+    auto flush = [&]() {
+      if (group.empty()) return;
+      lam_to_device();
+      su_bonds_fused<T>(group.data(), static_cast<int>(group.size()), st);
+      lam_host_stale = true;
+      group.clear();
+      std::fill(busy.begin(), busy.end(), 0);
+    };
+    for (int i = 0; i < n; ++i) {
+      check_site(sources[i]);
+      if (!ops || !ops[i]) fail(TG_E_INPUT, "null operator");
+      if (legs[i] < 0) {
+        flush();
+        su_onesite(sources[i], ops[i]);
+        continue;
+      }
+      if (legs[i] > 3) fail(TG_E_INPUT, "source_leg must be -1..3");
+      const int target = lat.neighbor(sources[i], legs[i]);
+      SuBondArgs a{};
+      if (!fused_args(sources[i], legs[i], ops[i], a)) {
+        flush();
+        su_bond(sources[i], legs[i], ops[i]);
+        continue;
+      }
+      if (busy[static_cast<size_t>(sources[i])] || busy[static_cast<size_t>(target)] ||
+          static_cast<int>(group.size()) == kSuBatchMax)
+        flush();
+      group.push_back(a);
+      busy[static_cast<size_t>(sources[i])] = busy[static_cast<size_t>(target)] = 1;
+      rot_ok[sources[i]] = rot_ok[target] = false;
+    }
+    flush();
   }
 
   // core::Simple_update_bond (core/simple_update.cpp:50-198)
@@ -2257,23 +2326,9 @@ struct EngineT final : Engine {
     {
       // the whole step in one thread block (su_fused.cu), in place
       SuBondArgs a{};
-      for (int q = 0; q < 5; ++q) {
-        a.dims1[q] = static_cast<int>(Tn[source].dim(q));
-        a.dims2[q] = static_cast<int>(Tn[target].dim(q));
-      }
-      if (su_bond_fused_supported<T>(a.dims1, a.dims2, connect1, lam_ld)) {
+      trim_op_cache(1);
+      if (fused_args(source, connect1, op, a)) {
         lam_to_device();
-        const int64_t nop = static_cast<int64_t>(a.dims1[4]) * a.dims2[4] * a.dims1[4] * a.dims2[4];
-        a.tn1 = Tn[source].p;
-        a.tn2 = Tn[target].p;
-        a.lam = d_lam;
-        a.lam_ld = lam_ld;
-        a.site1 = source;
-        a.site2 = target;
-        a.connect1 = connect1;
-        a.op = device_op(op, nop).p;
-        a.lambda_cut = P.inverse_lambda_cut;
-        a.flag = d_su_flag;
         su_bond_fused<T>(a, st);
         lam_host_stale = true;
         rot_ok[source] = rot_ok[target] = false;

@@ -38,6 +38,7 @@ struct Engine {
                               int maxiter, double rtol, double* out, int* nev_out) = 0;
   virtual void su_onesite(int site, const double* op) = 0;
   virtual void su_bond(int source, int leg, const double* op) = 0;
+  virtual void su_bonds(int n, const int* sources, const int* legs, const double* const* ops) = 0;
   virtual void fu_bond(int source, int leg, const double* op, const tg_fu_params* params, int* iterations,
                        int* converged) = 0;
   virtual void su_fix_gauge(int maxiter, double eps, int* sweeps, double* score) = 0;

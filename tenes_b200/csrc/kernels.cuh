@@ -106,6 +106,14 @@ template <typename T>
 bool su_bond_fused_supported(const int* dims1, const int* dims2, int connect1, int lam_ld);
 template <typename T>
 void su_bond_fused(const SuBondArgs& a, cudaStream_t st);
+// Bond steps on pairwise disjoint site pairs (they commute: none reads a
+// weight or a tensor another writes), one thread block each, in one launch.
+constexpr int kSuBatchMax = 16;
+struct SuBondBatch {
+  SuBondArgs a[kSuBatchMax];
+};
+template <typename T>
+void su_bonds_fused(const SuBondArgs* a, int n, cudaStream_t st);
 
 // Identity projector reshaped to (e, 1, 1, e) (ctm.cpp:303-317).
 template <typename T>

@@ -197,7 +197,8 @@ __device__ __forceinline__ double outer_weight(const Side& s, const double* w, i
 }
 
 template <typename T>
-__global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondArgs a) {
+__global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) {
+  const SuBondArgs& a = batch.a[blockIdx.x];
   extern __shared__ __align__(16) double smem_d[];
   __shared__ double red[SU_WARPS];
   __shared__ int rotated;
@@ -460,20 +461,33 @@ bool su_bond_fused_supported(const int* dims1, const int* dims2, int connect1, i
 }
 
 template <typename T>
-void su_bond_fused(const SuBondArgs& a, cudaStream_t st) {
-  if (!su_bond_fused_supported<T>(a.dims1, a.dims2, a.connect1, a.lam_ld))
-    fail(TG_E_INPUT, "su_bond_fused: shapes not supported");
-  const size_t smem = su_smem_bytes<T>(a.dims1, a.dims2, a.connect1, a.lam_ld);
+void su_bonds_fused(const SuBondArgs* a, int n, cudaStream_t st) {
+  if (n < 1 || n > kSuBatchMax) fail(TG_E_INPUT, "su_bonds_fused: 1.." + std::to_string(kSuBatchMax) + " bonds");
+  SuBondBatch batch{};
+  size_t smem = 0;
+  for (int b = 0; b < n; ++b) {
+    if (!su_bond_fused_supported<T>(a[b].dims1, a[b].dims2, a[b].connect1, a[b].lam_ld))
+      fail(TG_E_INPUT, "su_bonds_fused: shapes not supported");
+    smem = std::max(smem, su_smem_bytes<T>(a[b].dims1, a[b].dims2, a[b].connect1, a[b].lam_ld));
+    batch.a[b] = a[b];
+  }
   ensure_dynamic_smem(reinterpret_cast<const void*>(su_bond_kernel<T>), smem);
   ProfScope ps(PK_SOLVER, st, 0.0, 0.0);
-  su_bond_kernel<T><<<1, SU_THREADS, smem, st>>>(a);
+  su_bond_kernel<T><<<n, SU_THREADS, smem, st>>>(batch);
   TG_CHECK_LAUNCH();
   count_launch();
+}
+
+template <typename T>
+void su_bond_fused(const SuBondArgs& a, cudaStream_t st) {
+  su_bonds_fused<T>(&a, 1, st);
 }
 
 template bool su_bond_fused_supported<double>(const int*, const int*, int, int);
 template bool su_bond_fused_supported<cplx>(const int*, const int*, int, int);
 template void su_bond_fused<double>(const SuBondArgs&, cudaStream_t);
 template void su_bond_fused<cplx>(const SuBondArgs&, cudaStream_t);
+template void su_bonds_fused<double>(const SuBondArgs*, int, cudaStream_t);
+template void su_bonds_fused<cplx>(const SuBondArgs*, int, cudaStream_t);
 
 }  // namespace tg

@@ -322,6 +322,23 @@ class Environment:
         else:
             check(self.lib.tg_su_bond(self.ctx, source, source_leg, dptr(o.view(np.float64))))
 
+    def simple_update_many(self, steps) -> None:
+        """A sequence of (source, source_leg, op) simple-update steps in its
+        order, in one library call (tg_su_bonds): runs of bond steps on
+        disjoint site pairs go to the device together."""
+        steps = list(steps)
+        if not steps:
+            return
+        hosts = []
+        for source, leg, op in steps:
+            self._check_op(source, leg, op)
+            hosts.append(np.ascontiguousarray(_lib.as_host(op, self.is_complex)))
+        n = len(steps)
+        src = (C.c_int * n)(*[int(x[0]) for x in steps])
+        legs = (C.c_int * n)(*[int(x[1]) if x[1] >= 0 else -1 for x in steps])
+        ptrs = (C.c_void_p * n)(*[h.ctypes.data for h in hosts])
+        check(self.lib.tg_su_bonds(self.ctx, n, src, legs, ptrs))
+
     def full_update_bond(self, source: int, source_leg: int, op: np.ndarray, inverse_env_cut: float = 1e-12,
                          inverse_precision: float = 1e-12, convergence_epsilon: float = 1e-6,
                          max_iteration: int = 100, gauge_fix: bool = True) -> Tuple[int, bool]:

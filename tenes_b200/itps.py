@@ -165,10 +165,8 @@ class ITPS:
     def simple_update_step(self, group: int = 0) -> None:
         """One Trotter step: every op of `group` in input order (simple_update.cpp:113-119),
         then the local gauge fixing when simple_update.gauge_fix is set."""
-        for up in self.inp.simple_updates:
-            if up.group != group:
-                continue
-            self.env.simple_update(up.source_site, up.source_leg, self._op(up.op))
+        self.env.simple_update_many((up.source_site, up.source_leg, self._op(up.op))
+                                    for up in self.inp.simple_updates if up.group == group)
         if self.p.Simple_Gauge_Fix:  # simple_update.cpp:121-124, time_evolution.cpp:59-62
             self.env.fix_local_gauge(self.p.Simple_Gauge_maxiter, self.p.Simple_Gauge_Convergence_Epsilon)
 

@@ -95,6 +95,10 @@ class OracleEnvironment:
         self.lam[tg][(leg + 2) % 4] = lc
         self.Tn[source], self.Tn[tg] = a, b
 
+    def simple_update_many(self, steps):
+        for source, leg, op in steps:
+            self.simple_update(source, leg, op)
+
     def sync(self):
         pass
 

@@ -101,3 +101,32 @@ def test_te_tfi_golden_on_gpu():
         t += inp.params.tau_simple_step[0]
         if step % inp.params.measure_interval[0] == 0:
             measure(t)
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_batched_steps_equal_single_steps(is_complex):
+    """tg_su_bonds (runs of site-disjoint bond steps as one launch) gives the
+    same tensors and weights, bit for bit, as the same steps one call at a
+    time, one-site operators in between included; a 2x2 and a 4x2 cell."""
+    from tenes_b200.std_ops import evolution_onesite, evolution_twosite, heisenberg_bond, spin_ops
+    _, Sx, _ = spin_ops(0.5)
+    bond = evolution_twosite(heisenberg_bond(1.0), 0.05)
+    site = evolution_onesite(-0.3 * Sx, 0.05)
+    if not is_complex:
+        bond, site = bond.real, site.real
+    for LX, LY in ((2, 2), (4, 2)):
+        lat = make_lattice(LX, LY, 3)
+        Tn = random_tensors(lat, 21, is_complex)
+        steps = [(s, 2, bond) for s in range(lat.N_UNIT)] + [(s, 1, bond) for s in range(lat.N_UNIT)]
+        steps += [(s, -1, site) for s in range(lat.N_UNIT)]
+        one, many = gpu_env(lat, Tn, 4, is_complex), gpu_env(lat, Tn, 4, is_complex)
+        for _ in range(3):
+            for s, leg, op in steps:
+                one.simple_update(s, leg, op)
+            many.simple_update_many(steps)
+        for i in range(lat.N_UNIT):
+            assert np.array_equal(one.get_site_tensor(i), many.get_site_tensor(i)), i
+            for leg in range(4):
+                assert np.array_equal(one.get_lambda(i, leg), many.get_lambda(i, leg)), (i, leg)
+        one.close()
+        many.close()
