@@ -166,16 +166,11 @@ struct GemmParams {
   GemmDesc d;
 };
 
-// WN warps along N (2: 64-wide CTA tile, 128 threads; 3: 96-wide, 192 threads,
-// for the rSVD panels whose 82 or 72 columns fill a 96-wide tile better than
-// two 64-wide ones)
-template <typename T, bool CPLX, int WN>
-__global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
   constexpr int NP = CPLX ? 2 : 1;  // planes
-  constexpr int NT = 64 * WN, BN = 32 * WN, GLDB = BN + GPAD;
-  constexpr int AT = (GBM * GBK + NT - 1) / NT, BT = (BN * GBK + NT - 1) / NT;  // loads a thread
   extern __shared__ double smem[];
-  // layout: As[stage][plane][GBK][GLD], Bs[stage][plane][GBK][GLDB]
+  // layout: As[stage][plane][GBK][GLD], Bs[stage][plane][GBK][GLD]
   double* As = smem;
   double* Bs = smem + 2 * NP * GBK * GLD;
   const GemmDesc& d = p.d;
@@ -184,7 +179,7 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
   const T* B = p.B + bz * d.bB;
   T* C = p.C + bz * d.bC;
   const int64_t m0 = static_cast<int64_t>(blockIdx.y) * GBM;
-  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * BN;
+  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * GBN;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -195,13 +190,11 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
   // split-K launches: the last chunk may be shorter
   const int64_t Kz = (d.klast > 0 && blockIdx.z == gridDim.z - 1) ? d.klast : d.K;
 
-  T ra[AT], rb[BT];
-  // the 64-wide tile: one combined loop (AT = BT, no remainder)
-  constexpr bool EVEN = AT == BT && AT * NT == GBM * GBK && BT * NT == BN * GBK;
+  T ra[8], rb[8];
   auto load_tiles = [&](int64_t k0) {
 #pragma unroll
-    for (int i = 0; i < AT; ++i) {
-      const int idx = tid + i * NT;
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
       int mm, kk;
       if (a_kc) {
         kk = idx % GBK;
@@ -211,44 +204,25 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
         kk = idx / GBM;
       }
       const int64_t gm = m0 + mm, gk = k0 + kk;
-      if constexpr (EVEN)
-        ra[i] = (gm < d.M && gk < Kz) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
-      else
-        ra[i] = (idx < GBM * GBK && gm < d.M && gk < Kz) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
-      if constexpr (EVEN) {
-        int nn, kb;
-        if (b_nc) {
-          nn = idx % BN;
-          kb = idx / BN;
-        } else {
-          kb = idx % GBK;
-          nn = idx / GBK;
-        }
-        const int64_t gn = n0 + nn, gkb = k0 + kb;
-        rb[i] = (gn < d.N && gkb < Kz) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
+      ra[i] = (gm < d.M && gk < Kz) ? A[gm * d.sAm + gk * d.sAk] : zero_of<T>();
+      int nn, kb;
+      if (b_nc) {
+        nn = idx % GBN;
+        kb = idx / GBN;
+      } else {
+        kb = idx % GBK;
+        nn = idx / GBK;
       }
-    }
-    if constexpr (!EVEN) {
-#pragma unroll
-      for (int i = 0; i < BT; ++i) {
-        const int idx = tid + i * NT;
-        int nn, kb;
-        if (b_nc) {
-          nn = idx % BN;
-          kb = idx / BN;
-        } else {
-          kb = idx % GBK;
-          nn = idx / GBK;
-        }
-        const int64_t gn = n0 + nn, gkb = k0 + kb;
-        rb[i] = (idx < BN * GBK && gn < d.N && gkb < Kz) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
-      }
+      const int64_t gn = n0 + nn, gkb = k0 + kb;
+      rb[i] = (gn < d.N && gkb < Kz) ? B[gkb * d.sBk + gn * d.sBn] : zero_of<T>();
     }
   };
   auto store_tiles = [&](int stage) {
     double* as = As + stage * NP * GBK * GLD;
-    double* bs = Bs + stage * NP * GBK * GLDB;
-    auto put_a = [&](int i, int idx) {
+    double* bs = Bs + stage * NP * GBK * GLD;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = tid + i * 128;
       int mm, kk;
       if (a_kc) {
         kk = idx % GBK;
@@ -259,51 +233,16 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
       }
       as[kk * GLD + mm] = re_of(ra[i]);
       if constexpr (CPLX) as[GBK * GLD + kk * GLD + mm] = d.conjA ? -im_of(ra[i]) : im_of(ra[i]);
-    };
-    auto put_b = [&](int i, int idx) {
       int nn, kb;
       if (b_nc) {
-        nn = idx % BN;
-        kb = idx / BN;
+        nn = idx % GBN;
+        kb = idx / GBN;
       } else {
         kb = idx % GBK;
         nn = idx / GBK;
       }
-      bs[kb * GLDB + nn] = re_of(rb[i]);
-      if constexpr (CPLX) bs[GBK * GLDB + kb * GLDB + nn] = d.conjB ? -im_of(rb[i]) : im_of(rb[i]);
-    };
-    if constexpr (EVEN) {
-#pragma unroll
-      for (int i = 0; i < AT; ++i) {
-        const int idx = tid + i * NT;
-        int mm, kk;
-        if (a_kc) {
-          kk = idx % GBK;
-          mm = idx / GBK;
-        } else {
-          mm = idx % GBM;
-          kk = idx / GBM;
-        }
-        as[kk * GLD + mm] = re_of(ra[i]);
-        if constexpr (CPLX) as[GBK * GLD + kk * GLD + mm] = d.conjA ? -im_of(ra[i]) : im_of(ra[i]);
-        int nn, kb;
-        if (b_nc) {
-          nn = idx % BN;
-          kb = idx / BN;
-        } else {
-          kb = idx % GBK;
-          nn = idx / GBK;
-        }
-        bs[kb * GLDB + nn] = re_of(rb[i]);
-        if constexpr (CPLX) bs[GBK * GLDB + kb * GLDB + nn] = d.conjB ? -im_of(rb[i]) : im_of(rb[i]);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < AT; ++i)
-        if (tid + i * NT < GBM * GBK) put_a(i, tid + i * NT);
-#pragma unroll
-      for (int i = 0; i < BT; ++i)
-        if (tid + i * NT < BN * GBK) put_b(i, tid + i * NT);
+      bs[kb * GLD + nn] = re_of(rb[i]);
+      if constexpr (CPLX) bs[GBK * GLD + kb * GLD + nn] = d.conjB ? -im_of(rb[i]) : im_of(rb[i]);
     }
   };
 
@@ -328,7 +267,7 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
     const int stage = static_cast<int>(kt & 1);
     if (kt + 1 < nk) load_tiles((kt + 1) * GBK);
     const double* as = As + stage * NP * GBK * GLD;
-    const double* bs = Bs + stage * NP * GBK * GLDB;
+    const double* bs = Bs + stage * NP * GBK * GLD;
 #pragma unroll
     for (int k4 = 0; k4 < GBK; k4 += 4) {
       const int kr = k4 + (lane & 3);
@@ -336,10 +275,10 @@ __global__ void __launch_bounds__(64 * WN) gemm_kernel(GemmParams<T> p) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         a_r[i] = as[kr * GLD + wm + i * 8 + (lane >> 2)];
-        b_r[i] = bs[kr * GLDB + wn + i * 8 + (lane >> 2)];
+        b_r[i] = bs[kr * GLD + wn + i * 8 + (lane >> 2)];
         if constexpr (CPLX) {
           a_i[i] = as[GBK * GLD + kr * GLD + wm + i * 8 + (lane >> 2)];
-          b_i[i] = bs[GBK * GLDB + kr * GLDB + wn + i * 8 + (lane >> 2)];
+          b_i[i] = bs[GBK * GLD + kr * GLD + wn + i * 8 + (lane >> 2)];
         }
       }
 #pragma unroll
@@ -2087,18 +2026,21 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
     if (gemm_skinny(A, B, C, d, st)) return;
   }
   constexpr int NP = CPLX ? 2 : 1;
-  // a 96-wide tile where it pads N less than 64-wide ones (real products)
-  const bool wide = !CPLX && d.prec == 0 && (d.N + 95) / 96 * 96 < (d.N + 63) / 64 * 64;
-  const int bn = wide ? 96 : 64;
-  const size_t smem = sizeof(double) * 2 * NP * GBK * (GLD + bn + GPAD);
-  if constexpr (!CPLX) {
-    if (wide) ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, false, 3>), smem);
-  }
-  if (!wide) ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, CPLX, 2>), smem);
+  const size_t smem = sizeof(double) * 2 * 2 * NP * GBK * GLD;
+  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, CPLX>), smem);
   if (d.batch > 65535) fail(TG_E_INPUT, "gemm: batch too large");
-  dim3 grid(static_cast<unsigned>((d.N + bn - 1) / bn), static_cast<unsigned>((d.M + GBM - 1) / GBM),
+  // products taller than the grid's 65535 row tiles run as row chunks
+  constexpr int64_t kRowsPerLaunch = int64_t(65535) * GBM;
+  if (d.M > kRowsPerLaunch) {
+    for (int64_t m0 = 0; m0 < d.M; m0 += kRowsPerLaunch) {
+      GemmDesc part = d;
+      part.M = std::min(kRowsPerLaunch, d.M - m0);
+      gemm<T>(A + m0 * d.sAm, B, C + m0 * d.sCm, part, st);
+    }
+    return;
+  }
+  dim3 grid(static_cast<unsigned>((d.N + GBN - 1) / GBN), static_cast<unsigned>((d.M + GBM - 1) / GBM),
             static_cast<unsigned>(d.batch));
-  if (grid.y > 65535) fail(TG_E_INPUT, "gemm: M too large");
   const double macs = static_cast<double>(d.M) * d.N * d.K * d.batch;
   ProfScope ps(d.prec == 1 ? PK_GEMM_TC : PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
                sizeof(T) * static_cast<double>(d.batch) * (d.M * d.K + d.K * d.N + d.M * d.N));
@@ -2112,31 +2054,12 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
       return;
     }
   }
-  auto launch = [&](dim3 gr, const GemmParams<T>& gp) {
-    if constexpr (!CPLX) {
-      if (wide) {
-        gemm_kernel<T, false, 3><<<gr, 192, smem, st>>>(gp);
-        return;
-      }
-    }
-    gemm_kernel<T, CPLX, 2><<<gr, 128, smem, st>>>(gp);
-  };
+  auto launch = [&](dim3 gr, const GemmParams<T>& gp) { gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp); };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
-  // K cut into chunks of at least 128 so that the CTAs fill whole waves best
-  // (two 128-thread CTAs an SM, one 192-thread CTA), at most 8 chunks
-  if (d.batch == 1 && tiles < 148 && d.K >= 256) {
-    const int64_t slots = wide ? 148 : 296, smax = std::min<int64_t>(8, (d.K + 127) / 128);
-    double best = 0.0;
-    for (int64_t sp = 1; sp <= smax; ++sp) {
-      const int64_t ctas = tiles * sp;
-      const double fill = static_cast<double>(ctas) / (static_cast<double>((ctas + slots - 1) / slots) * slots);
-      if (fill > best + 1e-9) {
-        best = fill;
-        split = sp;
-      }
-    }
-  }
+  // up to two CTAs per SM (the kernel's occupancy), K chunks of at least 128
+  if (d.batch == 1 && tiles < 148 && d.K >= 256)
+    split = std::min<int64_t>(std::max<int64_t>(1, 296 / tiles), (d.K + 127) / 128);
   if (split <= 1) {
     launch(grid, GemmParams<T>{A, B, C, d});
     TG_CHECK_LAUNCH();

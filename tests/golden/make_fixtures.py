@@ -23,6 +23,8 @@ tree at run time:
   projectors) in the same form
 * mt19937_seed11.json     <- draws of std::mt19937 + uniform_real_distribution
   produced by oracle/mt19937_draws.cpp compiled with the system g++
+* restart_{0,1}_input.toml <- test/data/restart_{0,1}.toml (the reference's restart test,
+  test/restart.py.in: save tensors, then load them)
 * parameters_dat.json     <- output_*/parameters.dat of the ground-state and
   time-evolution goldens (PEPS_Parameters::save + SquareLattice::save + the
   start time), the run-dependent start_datetime value removed
@@ -119,6 +121,9 @@ def main(ref):
         exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
         with open(os.path.join(HERE, stem + "_expected.json"), "w") as f:
             json.dump(exp, f)
+
+    for k in (0, 1):
+        shutil.copyfile(os.path.join(data, f"restart_{k}.toml"), os.path.join(HERE, f"restart_{k}_input.toml"))
 
     pdat = {}
     for name, stem in (("TE_TFI", "te_tfi"), ("AntiferroHeisenberg_real", "afh_real"),

@@ -3,6 +3,7 @@
 own runs (test/fulltest.py.in:55-88, rtol 1e-3, atol 1e-4) against the
 committed TE_* output fixtures."""
 import os
+import shutil
 import subprocess
 import sys
 
@@ -14,6 +15,13 @@ from tests._te_tfi import GOLDEN, expected
 pytestmark = pytest.mark.gpu
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _env():
+    """The child runs the repository's package from any directory."""
+    e = dict(os.environ)
+    e["PYTHONPATH"] = REPO + os.pathsep + e.get("PYTHONPATH", "")
+    return e
 
 
 def _read(path):
@@ -58,3 +66,33 @@ def test_te_tfi_time_dat(te_tfi_run):
     lines = open(os.path.join(te_tfi_run, "time.dat")).read().splitlines()
     assert [l.split("=")[0].strip() for l in lines] == [
         "time all", "time simple update", "time full update", "time environment", "time observable"]
+
+
+def _density(path):
+    out = []
+    for line in open(path):
+        w = line.split()
+        out.append(complex(float(w[2]), float(w[3])))
+    return out
+
+
+def test_restart_from_saved_tensors(tmp_path):
+    """The reference's restart test (test/restart.py.in) on the GPU front end:
+    restart_0 runs 10 simple-update steps and saves the tensors, restart_1
+    loads them and runs on; density, one-site and two-site observables of the
+    two runs agree within the reference test's tolerances (rtol 1e-3, atol
+    1e-4)."""
+    for k in (0, 1):
+        shutil.copyfile(os.path.join(GOLDEN, f"restart_{k}_input.toml"), tmp_path / f"restart_{k}.toml")
+        r = subprocess.run([sys.executable, "-m", "tenes_b200", f"restart_{k}.toml", "--quiet"], cwd=tmp_path,
+                           capture_output=True, text=True, timeout=900, env=_env())
+        assert r.returncode == 0, r.stderr[-3000:]
+    assert (tmp_path / "tensor" / "params.dat").exists()
+    ref, res = tmp_path / "output_restart_0", tmp_path / "output_restart_1"
+    a, b = _density(res / "density.dat"), _density(ref / "density.dat")
+    assert len(a) == len(b)
+    np.testing.assert_allclose(a, b, rtol=1e-3, atol=1e-4)
+    for name in ("onesite_obs.dat", "twosite_obs.dat"):
+        x, y = _read(res / name), _read(ref / name)
+        assert len(x) == len(y), name
+        np.testing.assert_allclose(np.array(x), np.array(y), rtol=1e-3, atol=1e-4, err_msg=name)
