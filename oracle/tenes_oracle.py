@@ -1537,16 +1537,20 @@ class TMParams:
     arnoldi_rtol: float = 1e-10
 
 
-def tm_eigenvalues(env: Env, lat: Lattice, direction: int, fixed: int, tp: TMParams) -> np.ndarray:
-    """TransferMatrix::eigenvalues (transfer_matrix.cpp:84-142)."""
+def tm_eigenvalues(env: Env, lat: Lattice, direction: int, fixed: int, tp: TMParams,
+                   matvec: Optional[Callable] = None) -> np.ndarray:
+    """TransferMatrix::eigenvalues (transfer_matrix.cpp:84-142).  matvec
+    (env, lat, fixed, v) replaces the double-layer matvec of the direction
+    (the iTPO environment's rank-3 edges have their own)."""
     if direction == 0:
         s0 = lat.index(0, fixed)
         N = env.eTt[s0].shape[0] * env.eTb[lat.top(s0)].shape[1]
-        mv = lambda v: tm_matvec_horizontal(env, lat, fixed, v)  # noqa: E731
+        f = matvec or tm_matvec_horizontal
     else:
         s0 = lat.index(fixed, 0)
         N = env.eTl[s0].shape[0] * env.eTr[lat.left(s0)].shape[1]
-        mv = lambda v: tm_matvec_vertical(env, lat, fixed, v)  # noqa: E731
+        f = matvec or tm_matvec_vertical
+    mv = lambda v: f(env, lat, fixed, v)  # noqa: E731
     nev = min(tp.num_eigvals, N)
     if N == 1:
         return np.array([1.0 + 0j])

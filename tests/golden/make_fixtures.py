@@ -25,6 +25,9 @@ tree at run time:
   produced by oracle/mt19937_draws.cpp compiled with the system g++
 * restart_{0,1}_input.toml <- test/data/restart_{0,1}.toml (the reference's restart test,
   test/restart.py.in: save tensors, then load them)
+* ft_{tfi_square,kitaev}_{input.toml,expected.json} <- FT_TFI_square and FT_Kitaev
+  (finite temperature: density simple update, single-layer CTMRG, FT_{density,onesite_obs,
+  twosite_obs,correlation_length,correlation}.dat)
 * parameters_dat.json     <- output_*/parameters.dat of the ground-state and
   time-evolution goldens (PEPS_Parameters::save + SquareLattice::save + the
   start time), the run-dependent start_datetime value removed
@@ -124,6 +127,19 @@ def main(ref):
 
     for k in (0, 1):
         shutil.copyfile(os.path.join(data, f"restart_{k}.toml"), os.path.join(HERE, f"restart_{k}_input.toml"))
+
+    # finite temperature (iTPO): density simple update + single-layer CTMRG
+    for name, stem in (("FT_TFI_square", "ft_tfi_square"), ("FT_Kitaev", "ft_kitaev")):
+        shutil.copyfile(os.path.join(data, name + ".toml"), os.path.join(HERE, stem + "_input.toml"))
+        out = os.path.join(data, "output_" + name)
+        exp = {}
+        for key, fname in (("density", "FT_density.dat"), ("onesite", "FT_onesite_obs.dat"),
+                           ("twosite", "FT_twosite_obs.dat"), ("correlation_length", "FT_correlation_length.dat"),
+                           ("correlation", "FT_correlation.dat")):
+            exp[key] = _rows(os.path.join(out, fname))
+        exp["tolerance"] = {"rtol": 1e-3, "atol": 1e-4, "source": "test/fulltest.py.in:141-142"}
+        with open(os.path.join(HERE, stem + "_expected.json"), "w") as f:
+            json.dump(exp, f)
 
     pdat = {}
     for name, stem in (("TE_TFI", "te_tfi"), ("AntiferroHeisenberg_real", "afh_real"),
