@@ -82,6 +82,17 @@ typedef struct tg_params {
                                        residual is <= 1e-13 s_0 (a dense SVD when that cannot be
                                        reached); 1: the dense SVD (cuSOLVER gesvd) of the whole
                                        matrix.  Both give the reference's truncated factors. */
+  int density;                      /* 1: the context holds an iTPO, the density operator of the
+                                       finite-temperature mode (iTPS::finite_temperature,
+                                       finite_temperature.cpp:22-86).  Site tensors are
+                                       (D0,D1,D2,D3,d,d) (physical_dims hold d); the simple update
+                                       applies kron(op, conj(op)) (simple_update.cpp:141-178); the
+                                       CTMRG is the single-layer one of ctm_single.cpp on
+                                       sum_p Tn[...,p,p], with edge tensors (chi,chi,D,1); the
+                                       measurements are the density contractions of
+                                       contract_density_ctm/ (sum_{p,q} op[p,q] Tn[...,p,q]).  Needs
+                                       chi >= every bond dimension; no full update or gradient.
+                                       0 (default): an iTPS. */
 } tg_params;
 
 /* One `tenes input.toml` run, as the reference's process-level entry point
@@ -165,7 +176,13 @@ tg_status tg_corner_spectrum(tg_ctx* ctx, int which, int site, double* host);
  * One site: Contract_one_site_iTPS_CTM (contract_itps_ctm/ctm.cpp:89-113),
  *   op is d x d, applied as sum_{p,q} Tn[..p] op[p,q] conj(Tn[..q]).
  * Nearest-neighbour op12 (d1,d2,d1,d2): Contract_two_sites_{horizontal,vertical}_op12
- *   (ctm.cpp:213-319); source/target as in twosite_obs.cpp:189-222. */
+ *   (ctm.cpp:213-319); source/target as in twosite_obs.cpp:189-222.
+ * For an iTPO (params.density) the same calls are the density contractions
+ * (contract_density_ctm/ctm.cpp:89-274): sum_{p,q} op[p,q] Tn[...,p,q] for
+ * one site, sum op12[p1,p2,q1,q2] over the two density tensors for a bond;
+ * tg_measure_window, tg_measure_correlation and the transfer matrix likewise
+ * (Contract_RxC_density_CTM, *Correlation_density_CTM, the rank-3 matvecs of
+ * transfer_matrix.cpp:187-308). */
 tg_status tg_measure_onesite(tg_ctx* ctx, int site, const double* op, double* out);
 tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const double* op,
                                double* out);
@@ -175,7 +192,10 @@ tg_status tg_measure_bond_op12(tg_ctx* ctx, int source, int dx, int dy, const do
  * (d_s * d_t * d_s * d_t values, interleaved pairs when complex): the op12
  * value of that call is sum op12 * rdm and the norm sum_ab rdm[a,b,a,b], so
  * one contraction of the bond serves any number of operators.  The same
- * contraction sequence as Contract_two_sites_*_op12 (ctm.cpp:213-319). */
+ * contraction sequence as Contract_two_sites_*_op12 (ctm.cpp:213-319).
+ * For an iTPO the values are R[(p_s*d_s + q_s), (p_t*d_t + q_t)], the
+ * environment of the two density tensors: <op12> = sum op12[p_s,p_t,q_s,q_t] R
+ * and the norm sum_ab R[(a,a),(b,b)]. */
 tg_status tg_measure_bond_rdm(tg_ctx* ctx, int source, int dx, int dy, double* out);
 
 /* Long-range correlations along a strip (StartCorrelation / Transfer /

@@ -659,3 +659,34 @@ def measure_multisite(e: Env, Tn, lat: O.Lattice, ops, onesite, ngroups: int):
         ret[o.group][(o.source, o.dxs, o.dys)] = o.coeff * _window_value(C, eTt, eTr, eTb, eTl, Tn, idx,
                                                                            opw) / norms[key]
     return ret
+
+
+def contract_op12(e: Env, Tn, lat: O.Lattice, source: int, dx: int, dy: int, op) -> complex:
+    """<op12> of a nearest-neighbour bond with the source/target rule of
+    twosite_obs.cpp:186-222, as the sum over the SVD split of op12 of
+    one-site-operator windows (equal to Contract_two_sites_*_op12_density_CTM
+    up to rounding)."""
+    ncol, nrow = abs(dx) + 1, abs(dy) + 1
+    source_col, target_col = (0, ncol - 1) if dx >= 0 else (ncol - 1, 0)
+    source_row, target_row = (nrow - 1, 0) if dy >= 0 else (0, nrow - 1)
+    idx, C, eTt, eTr, eTb, eTl = _window(e, lat, source, source_col, source_row, nrow, ncol)
+    sh = op.shape
+    U, s, VT = np.linalg.svd(op.transpose(0, 2, 1, 3).reshape(sh[0] * sh[2], -1), full_matrices=False)
+    U = U.reshape(sh[0], sh[2], -1)
+    VT = VT.reshape(-1, sh[1], sh[3])
+    value = 0.0
+    for si in range(len(s)):
+        opw = [[np.eye(Tn[idx[r][c]].shape[4]) for c in range(ncol)] for r in range(nrow)]
+        opw[source_row][source_col] = U[:, :, si]
+        opw[target_row][target_col] = VT[si]
+        value += _window_value(C, eTt, eTr, eTb, eTl, Tn, idx, opw) * s[si]
+    return complex(value)
+
+
+def window_value(e: Env, Tn, lat: O.Lattice, source: int, nrow: int, ncol: int, source_row: int,
+                 source_col: int, ops) -> complex:
+    """Contract_density_CTM over the nrow x ncol window whose source sits at
+    (source_row, source_col); ops maps (row, col) to a one-site operator."""
+    idx, C, eTt, eTr, eTb, eTl = _window(e, lat, source, source_col, source_row, nrow, ncol)
+    opw = [[ops.get((r, c), np.eye(Tn[idx[r][c]].shape[4])) for c in range(ncol)] for r in range(nrow)]
+    return _window_value(C, eTt, eTr, eTb, eTl, Tn, idx, opw)

@@ -64,7 +64,7 @@ class Params(C.Structure):
                 ("rsvd_oversampling_factor", C.c_double), ("rsvd_oversample_abs", C.c_int),
                 ("rsvd_power_iters", C.c_int), ("rsvd_seed", C.c_uint64),
                 ("inverse_lambda_cut", C.c_double), ("mixed", C.c_int), ("cuda_graph", C.c_int),
-                ("svd_solver", C.c_int)]
+                ("svd_solver", C.c_int), ("density", C.c_int)]
 
 
 _lib = None

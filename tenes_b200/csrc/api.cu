@@ -70,6 +70,7 @@ void tg_params_default(tg_params* p) {
   p->mixed = 0;
   p->cuda_graph = 1;
   p->svd_solver = 0;
+  p->density = 0;
 }
 
 const char* tg_last_error(void) { return g_last_error.c_str(); }

@@ -51,6 +51,16 @@ struct EngineT final : Engine {
   std::vector<DT<T>> Tn;
   std::vector<std::array<DT<T>, 3>> Trot;  // right (2,3,0,1,4), top (1,2,3,0,4), bottom (3,0,1,2,4)
   std::vector<bool> rot_ok;
+  // iTPO (tg_params.density): Tn[i] holds the density tensor
+  // (D,D,D,D,d,d) as (D,D,D,D,d*d); the CTMRG runs on the single-layer
+  // network of Ts[i] = sum_p Tn[i][...,p,p] (Make_single_tensor_density,
+  // ctm_single.cpp:43-50), stored (D,D,D,D,1).  Every double-layer
+  // contraction of the engine then serves as the single-layer one with the
+  // all-ones (1,1,1,1,1) tensor `bra1` in place of conj(Tn): the edges are
+  // (chi,chi,D,1) and every "bra" leg has dimension 1.
+  bool density = false;
+  std::vector<DT<T>> Ts;
+  DT<T> bra1, one1;  // (1,1,1,1,1) ones; the 1 x 1 operator [[1]]
   std::array<std::vector<DT<T>>, 4> C;  // C1..C4
   std::array<std::vector<DT<T>>, 4> E;  // eTt, eTr, eTb, eTl
   std::vector<std::array<std::vector<double>, 4>> lambda;
@@ -105,8 +115,17 @@ struct EngineT final : Engine {
     }
     lat.check_dims();
     if (P.chi < 1) fail(TG_E_INPUT, "chi must be positive");
+    if (P.density) {
+      // the single-layer environment starts at the bond dimensions
+      // (ctm_single.cpp:752-960) and is kept padded to chi
+      for (int i = 0; i < lat.N; ++i)
+        for (int l = 0; l < 4; ++l)
+          if (lat.vdim[i][l] > P.chi)
+            fail(TG_E_INPUT, "an iTPO environment needs chi >= every bond dimension");
+    }
     if (P.rsvd_oversampling_factor < 1.0) fail(TG_E_INPUT, "rsvd_oversampling_factor must be >= 1.0");
     if (P.mixed && CPLX) fail(TG_E_INPUT, "mixed precision is available for real tensors only");
+    density = P.density != 0;
     abs_prec = P.mixed ? 1 : 0;
     TG_CUDA(cudaSetDevice(dev));
     TG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -143,8 +162,19 @@ struct EngineT final : Engine {
     lambda.resize(lat.N);
     for (int i = 0; i < lat.N; ++i) {
       const auto& v = lat.vdim[i];
-      Tn[i] = zeros<T>({v[0], v[1], v[2], v[3], lat.pdim[i]}, st);
+      Tn[i] = zeros<T>({v[0], v[1], v[2], v[3], tdim(i)}, st);
       for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+    }
+    if (density) {
+      Ts.resize(lat.N);
+      for (int i = 0; i < lat.N; ++i) {
+        const auto& v = lat.vdim[i];
+        Ts[i] = zeros<T>({v[0], v[1], v[2], v[3], 1}, st);
+      }
+      std::vector<double> h(NW, 0.0);
+      h[0] = 1.0;
+      bra1 = from_host({1, 1, 1, 1, 1}, h.data());
+      one1 = from_host({1, 1}, h.data());
     }
     const int64_t chi = P.chi;
     for (int k = 0; k < 4; ++k) {
@@ -154,11 +184,12 @@ struct EngineT final : Engine {
     for (int i = 0; i < lat.N; ++i) {
       for (int k = 0; k < 4; ++k) C[k][i] = zeros<T>({chi, chi}, st);
       // eTt: vdim[1], eTr: vdim[2], eTb: vdim[3], eTl: vdim[0] (tensors.cpp:57-60)
+      // (iTPO: the bra leg of dimension 1, tensors.cpp:155-158)
       const int64_t dt = lat.vdim[i][1], dr = lat.vdim[i][2], db = lat.vdim[i][3], dl = lat.vdim[i][0];
-      E[0][i] = zeros<T>({chi, chi, dt, dt}, st);
-      E[1][i] = zeros<T>({chi, chi, dr, dr}, st);
-      E[2][i] = zeros<T>({chi, chi, db, db}, st);
-      E[3][i] = zeros<T>({chi, chi, dl, dl}, st);
+      E[0][i] = zeros<T>({chi, chi, dt, density ? 1 : dt}, st);
+      E[1][i] = zeros<T>({chi, chi, dr, density ? 1 : dr}, st);
+      E[2][i] = zeros<T>({chi, chi, db, density ? 1 : db}, st);
+      E[3][i] = zeros<T>({chi, chi, dl, density ? 1 : dl}, st);
     }
     TG_CUDA(cudaStreamSynchronize(st));
   }
@@ -168,6 +199,9 @@ struct EngineT final : Engine {
     // release device tensors before the stream goes away
     Tn.clear();
     Trot.clear();
+    Ts.clear();
+    bra1 = DT<T>();
+    one1 = DT<T>();
     for (auto& v : C) v.clear();
     for (auto& v : E) v.clear();
     spec_old = DT<double>();
@@ -300,21 +334,50 @@ struct EngineT final : Engine {
     if (site < 0 || site >= lat.N) fail(TG_E_INPUT, "site index out of range: " + std::to_string(site));
   }
 
+  // last leg of a site tensor: d, or d*d for an iTPO
+  int64_t tdim(int site) const {
+    const int64_t d = lat.pdim[site];
+    return density ? d * d : d;
+  }
+  // the conjugated layer of a double-layer contraction: the tensor itself,
+  // or the all-ones unit tensor of the single-layer network
+  const DT<T>& bra(const DT<T>& t) const { return density ? bra1 : t; }
+
+  // an iTPO site tensor with the operator op (d x d, on the device) traced
+  // in: sum_{p,q} op[p,q] Tn[...,p,q] as (D,D,D,D,1) -- the operator legs
+  // of contract_density_ctm/ctm.cpp:103 and correlation.cpp:46; with op the
+  // identity, Make_single_tensor_density (ctm_single.cpp:43-50)
+  DT<T> traced(int site, const DT<T>& op) {
+    const int64_t dd = tdim(site);
+    if (op.size() != dd) fail(TG_E_INPUT, "operator size does not match the site");
+    return td(Tn[site], reshape(op, {dd, 1}), {4}, {0});
+  }
+  void traced_into(int site, const DT<T>& op, DT<T>& out) {
+    const DT<T> t = traced(site, op);
+    TG_CUDA(cudaMemcpyAsync(out.p, t.p, sizeof(T) * t.size(), cudaMemcpyDeviceToDevice, st));
+  }
+
+  // the tensor the CTMRG moves absorb at a site (Tn, or the iTPO's Ts) and
+  // its rotations for the right / top / bottom moves, refreshed whenever Tn
+  // has changed
   const DT<T>& rot(int site, int which) {
     if (!rot_ok[site]) {
+      if (density) traced_into(site, identity_op(site), Ts[site]);
+      const DT<T>& src = density ? Ts[site] : Tn[site];
       static const std::vector<int> perms[3] = {{2, 3, 0, 1, 4}, {1, 2, 3, 0, 4}, {3, 0, 1, 2, 4}};
       for (int w = 0; w < 3; ++w) {
         if (Trot[site][w].empty()) {
           Shape s(5);
-          for (int a = 0; a < 5; ++a) s[a] = Tn[site].dim(perms[w][a]);
+          for (int a = 0; a < 5; ++a) s[a] = src.dim(perms[w][a]);
           Trot[site][w] = DT<T>(s, st);  // allocated once, rewritten when Tn changes
         }
-        permute<T>(Tn[site].p, Trot[site][w].p, Tn[site].sh, perms[w], false, st);
+        permute<T>(src.p, Trot[site][w].p, src.sh, perms[w], false, st);
       }
       rot_ok[site] = true;
     }
     return Trot[site][which];
   }
+  const DT<T>& mt(int site) { return density ? Ts[site] : Tn[site]; }
   void prepare_rotations() {
     for (int i = 0; i < lat.N; ++i) rot(i, 0);
   }
@@ -496,12 +559,12 @@ struct EngineT final : Engine {
   // ------------------------------------------------------------ CTM pieces
   // LT = Tn1*(((C1*eT1)*eT8)*conj(Tn1)), legs (t12,t41,e12,e78,tc12,tc41)  (ctm.cpp:207-212)
   DT<T> block_LT(const DT<T>& C1, const DT<T>& eT1, const DT<T>& eT8, const DT<T>& T1) {
-    DT<T> X = td(td(td(C1, eT1, {1}, {0}), eT8, {0}, {1}), T1, {2, 5}, {1, 0}, false, true);
+    DT<T> X = td(td(td(C1, eT1, {1}, {0}), eT8, {0}, {1}), bra(T1), {2, 5}, {1, 0}, false, true);
     return td(T1, X, {0, 1, 4}, {3, 1, 6});
   }
   // LB = Tn4*(((C4*eT7)*eT6)*conj(Tn4)), legs (t41,t34,e78,e56,tc41,tc34)  (ctm.cpp:222-227)
   DT<T> block_LB(const DT<T>& C4, const DT<T>& eT7, const DT<T>& eT6, const DT<T>& T4) {
-    DT<T> X = td(td(td(C4, eT7, {1}, {0}), eT6, {0}, {1}), T4, {2, 5}, {0, 3}, false, true);
+    DT<T> X = td(td(td(C4, eT7, {1}, {0}), eT6, {0}, {1}), bra(T4), {2, 5}, {0, 3}, false, true);
     return td(T4, X, {0, 3, 4}, {1, 3, 6});
   }
 
@@ -924,12 +987,14 @@ struct EngineT final : Engine {
                        DT<T>& PL) {
     const int64_t e12 = eT1.dim(1), e56 = eT6.dim(0), e78 = eT8.dim(0);
     const int64_t t12 = T1.dim(2), t41 = T1.dim(3), t34 = T4.dim(2);
+    // the bra's bond dimensions: t.. again, or 1 in the single-layer network of an iTPO
+    const int64_t b12 = bra(T1).dim(2), b41 = bra(T1).dim(3), b34 = bra(T4).dim(2);
     if (t41 != 1) {
       // LT as the matrix [(t12,e12,tc12), (t41,e78,tc41)], LB as [(t41,e78,tc41), (t34,e56,tc34)]:
       // M = LTm LBm is tensordot(LT, LB, Axes(1,3,5), Axes(0,2,4)) of ctm.cpp:273
       DT<T> LTm = tr(block_LT(C1, eT1, eT8, T1), {0, 2, 4, 1, 3, 5});
       DT<T> LBm = tr(block_LB(C4, eT7, eT6, T4), {0, 2, 4, 1, 3, 5});
-      const int64_t nrow = t12 * e12 * t12, nmid = t41 * e78 * t41, ncol = t34 * e56 * t34;
+      const int64_t nrow = t12 * e12 * b12, nmid = t41 * e78 * b41, ncol = t34 * e56 * b34;
       MV lt = rm(LTm.p, nrow, nmid), lb = rm(LBm.p, nmid, ncol);
       MV lth = ht(lt), lbh = ht(lb);
       // 3xTF32: LT, LB and their transposes are the left operands of every
@@ -950,7 +1015,8 @@ struct EngineT final : Engine {
       DT<T> Uc, Vrow;  // Uc: nrow x w;  PU = LBm * Vc where Vc = (VT_c)^H
       MV vc{nullptr, 0, 0, 0, 0, false};
       if ((t12 != 1 && t34 != 1) && P.use_rsvd) {
-        // cut = min(chi, e78 t41^2, e12 t12^2, e56 t34^2), k = factor * cut (ctm.cpp:242-244)
+        // cut = min(chi, e78 t41^2, e12 t12^2, e56 t34^2), k = factor * cut (ctm.cpp:242-244;
+        // single layer: e78 t41, ..., ctm_single.cpp:200-203)
         const int cut = static_cast<int>(std::min<int64_t>(std::min<int64_t>(P.chi, nmid), std::min(nrow, ncol)));
         int64_t k = P.rsvd_oversample_abs >= 0 ? cut + P.rsvd_oversample_abs
                                                : static_cast<int64_t>(P.rsvd_oversampling_factor * cut);
@@ -968,13 +1034,13 @@ struct EngineT final : Engine {
       }
       const int64_t w = Uc.dim(1);
       // PU = tensordot(LB, conj(VT_c), Axes(1,3,5), Axes(1,2,3)).transpose(1,0,2,3)  (ctm.cpp:263-266)
-      PU = tr(reshape(mm_rm(lb, vc), {t41, e78, t41, w}), {1, 0, 2, 3});
+      PU = tr(reshape(mm_rm(lb, vc), {t41, e78, b41, w}), {1, 0, 2, 3});
       // PL = tensordot(LT, conj(U_c), Axes(0,2,4), Axes(0,1,2)).transpose(1,0,2,3)
       MV uc = rm(Uc.p, nrow, w);
       uc.conj = true;
       MV ltt = tp(lt);
       ltt.split = lth.split;  // real operands: transpose = conjugate transpose
-      PL = tr(reshape(mm_rm(ltt, uc), {t41, e78, t41, w}), {1, 0, 2, 3});
+      PL = tr(reshape(mm_rm(ltt, uc), {t41, e78, b41, w}), {1, 0, 2, 3});
     } else {
       PU = DT<T>({e78, 1, 1, e78}, st);
       identity<T>(PU.p, e78, st);
@@ -993,7 +1059,7 @@ struct EngineT final : Engine {
   // the projectors are PU = LBm RBm V_c and PL = LTm^T RTm conj(U_c), each
   // reshaped to (t41,e78,tc41,cut) and transposed (1,0,2,3) (ctm.cpp:434-439).
   void proj_updown_rsvd(const DT<T>& LT, const DT<T>& RT, const DT<T>& RB, const DT<T>& LB, int64_t e34,
-                        int64_t t23, int64_t e78, int64_t t41, DT<T>& PU, DT<T>& PL) {
+                        int64_t t23, int64_t b23, int64_t e78, int64_t t41, int64_t b41, DT<T>& PU, DT<T>& PL) {
     DT<T> RTm = tr(RT, {0, 3, 4, 1, 2, 5});
     DT<T> LTm = tr(LT, {0, 2, 4, 1, 3, 5});
     DT<T> LBm = tr(LB, {0, 2, 4, 1, 3, 5});
@@ -1005,8 +1071,9 @@ struct EngineT final : Engine {
     const MV rtm = rm(RTm.p, na, n), ltm = rm(LTm.p, na, nb), lbm = rm(LBm.p, nb, nc), rbm = rm(RBm.p, nc, n);
     MV rtm_c = rtm;
     rtm_c.conj = true;
-    // cut = min(chi, e34 t23^2), k = factor * cut (ctm.cpp:410-414)
-    const int cut = static_cast<int>(std::min<int64_t>(P.chi, e34 * t23 * t23));
+    // cut = min(chi, e34 t23^2), k = factor * cut (ctm.cpp:410-414; single layer:
+    // e34 t23, ctm_single.cpp:362-365)
+    const int cut = static_cast<int>(std::min<int64_t>(P.chi, e34 * t23 * b23));
     int64_t k = P.rsvd_oversample_abs >= 0 ? cut + P.rsvd_oversample_abs
                                            : static_cast<int64_t>(P.rsvd_oversampling_factor * cut);
     k = std::min<int64_t>(k, n);
@@ -1030,11 +1097,11 @@ struct EngineT final : Engine {
     rsvd_run(apply_M, apply_MH, n, n, cut, k, Uc, Vc);
     const int64_t w = Uc.dim(1);
     DT<T> t = mm_rm(rbm, rm(Vc.p, n, w));  // (nc x w)
-    PU = tr(reshape(mm_rm(lbm, rm(t.p, nc, w)), {t41, e78, t41, w}), {1, 0, 2, 3});
+    PU = tr(reshape(mm_rm(lbm, rm(t.p, nc, w)), {t41, e78, b41, w}), {1, 0, 2, 3});
     MV uc = rm(Uc.p, n, w);
     uc.conj = true;
     t = mm_rm(rtm, uc);  // (na x w)
-    PL = tr(reshape(mm_rm(tp(ltm), rm(t.p, na, w)), {t41, e78, t41, w}), {1, 0, 2, 3});
+    PL = tr(reshape(mm_rm(tp(ltm), rm(t.p, na, w)), {t41, e78, b41, w}), {1, 0, 2, 3});
   }
 
   // Calc_projector_updown_blocks (ctm.cpp:320-491): full-SVD and rSVD branches
@@ -1046,13 +1113,13 @@ struct EngineT final : Engine {
     const int64_t t23 = T2.dim(3), t41 = T4.dim(1);
     if (t41 != 1) {
       DT<T> LT = block_LT(C1, eT1, eT8, T1);
-      DT<T> X = td(td(td(C2, eT3, {1}, {0}), eT2, {0}, {1}), T2, {2, 5}, {2, 1}, false, true);
+      DT<T> X = td(td(td(C2, eT3, {1}, {0}), eT2, {0}, {1}), bra(T2), {2, 5}, {2, 1}, false, true);
       DT<T> RT = td(T2, X, {1, 2, 4}, {3, 1, 6});
-      X = td(td(td(C3, eT5, {1}, {0}), eT4, {0}, {1}), T3, {2, 5}, {3, 2}, false, true);
+      X = td(td(td(C3, eT5, {1}, {0}), eT4, {0}, {1}), bra(T3), {2, 5}, {3, 2}, false, true);
       DT<T> RB = td(T3, X, {2, 3, 4}, {3, 1, 6});
       DT<T> LB = block_LB(C4, eT7, eT6, T4);
       if (t23 != 1 && P.use_rsvd) {
-        proj_updown_rsvd(LT, RT, RB, LB, e34, t23, e78, t41, PU, PL);
+        proj_updown_rsvd(LT, RT, RB, LB, e34, t23, bra(T2).dim(3), e78, t41, bra(T4).dim(1), PU, PL);
         return;
       }
       DT<T> R1 = td(RT, LT, {0, 3, 4}, {0, 2, 4});
@@ -1084,7 +1151,7 @@ struct EngineT final : Engine {
 
   // Calc_Next_eT (ctm.cpp:520-552), written into the storage of `out`
   void next_et(const DT<T>& eT8, const DT<T>& T1, const DT<T>& PU, const DT<T>& PL, DT<T>& out) {
-    DT<T> X = td(T1, td(eT8, PL, {1}, {0}), {0, 1}, {2, 4}, true, false);
+    DT<T> X = td(bra(T1), td(eT8, PL, {1}, {0}), {0, 1}, {2, 4}, true, false);
     X = td(T1, X, {0, 1, 4}, {4, 5, 2});
     normalize_into(tr(td(X, PU, {1, 3, 4}, {1, 2, 0}), {3, 2, 0, 1}), out);
   }
@@ -1124,15 +1191,16 @@ struct EngineT final : Engine {
     auto &eTt = E[0], &eTr = E[1], &eTb = E[2], &eTl = E[3];
     const int LY = lat.LY_noskew;
     const bool par = rows_parallel();
+    if (density) prepare_rotations();  // Ts, before the rows fork
     std::vector<DT<T>> PUs(LY), PLs(LY);
     for_rows(LY, par, [&](int iy) {
       proj_key = (0 * 4096 + ix) * 4096 + iy;
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       if (P.projector_corner)
-        proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l], PUs[iy], PLs[iy]);
+        proj_left_block(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], mt(i), mt(l), PUs[iy], PLs[iy]);
       else
         proj_updown(C1[i], C2[j], C3[k], C4[l], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i],
-                    Tn[i], Tn[j], Tn[k], Tn[l], PUs[iy], PLs[iy]);
+                    mt(i), mt(j), mt(k), mt(l), PUs[iy], PLs[iy]);
     });
     std::vector<EtJob> jobs;
     for (int iy = 0; iy < LY; ++iy) {
@@ -1148,7 +1216,7 @@ struct EngineT final : Engine {
       next_ctm(C1[i], C4[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
       for (size_t q = iy; q < fin.size(); q += LY) {
         const EtJob& b = fin[q];
-        next_et(eTl[b.src], Tn[b.site], PUs[b.pu], PLs[b.pl], eTl[b.out]);
+        next_et(eTl[b.src], mt(b.site), PUs[b.pu], PLs[b.pl], eTl[b.out]);
       }
     });
     keep(PUs);
@@ -1276,7 +1344,45 @@ struct EngineT final : Engine {
     fit_chi<T>(X.p, d1, d2, rest, out.p, chi, st);
   }
 
+  // Calc_CTM_Environment_density's initialisation (ctm_single.cpp:752-960):
+  // every corner / edge is the neighbouring site's Ts summed over its outer
+  // legs (a contraction with all-ones vectors).  The reference keeps these
+  // at their natural size; here they are zero-padded to chi, which changes
+  // no contraction and no kept singular value.
+  void ctm_init_density() {
+    prepare_rotations();  // Ts
+    auto sum_leg = [&](const DT<T>& A, int leg) {
+      const int64_t n = A.dim(leg);
+      std::vector<double> h(static_cast<size_t>(n * NW), 0.0);
+      for (int64_t k = 0; k < n; ++k) h[static_cast<size_t>(k * NW)] = 1.0;
+      return td(A, from_host({n}, h.data()), {leg}, {0});
+    };
+    auto put = [&](const DT<T>& X, DT<T>& out) {  // X (d1, d2, rest...) into (chi, chi, rest...)
+      int64_t rest = 1;
+      for (int a = 2; a < X.rank(); ++a) rest *= X.dim(a);
+      fit_chi<T>(X.p, X.dim(0), X.dim(1), rest, out.p, P.chi, st);
+    };
+    for (int i = 0; i < lat.N; ++i) {
+      put(tr(sum_leg(sum_leg(Ts[lat.top(lat.left(i))], 0), 0), {1, 0, 2}), C[0][i]);       // (b, r)
+      put(sum_leg(sum_leg(Ts[lat.top(lat.right(i))], 1), 1), C[1][i]);                     // (l, b)
+      put(tr(sum_leg(sum_leg(Ts[lat.bottom(lat.right(i))], 2), 2), {1, 0, 2}), C[2][i]);   // (t, l)
+      put(tr(sum_leg(sum_leg(Ts[lat.bottom(lat.left(i))], 0), 2), {1, 0, 2}), C[3][i]);    // (r, t)
+      put(sum_leg(Ts[lat.top(i)], 1), E[0][i]);                                            // (l, r, b)
+      put(tr(sum_leg(Ts[lat.right(i)], 2), {1, 2, 0, 3}), E[1][i]);                        // (t, b, l)
+      put(tr(sum_leg(Ts[lat.bottom(i)], 3), {2, 0, 1, 3}), E[2][i]);                       // (r, l, t)
+      put(tr(sum_leg(Ts[lat.left(i)], 0), {2, 0, 1, 3}), E[3][i]);                         // (b, t, r)
+    }
+    env_ready = true;
+    spec_old = spectra();
+    spec_old_ok = true;
+    TG_CUDA(cudaStreamSynchronize(st));
+  }
+
   void ctm_init() override {
+    if (density) {
+      ctm_init_density();
+      return;
+    }
     for (int i = 0; i < lat.N; ++i) {
       int num = lat.top(lat.left(i));
       const DT<T>* t = &Tn[num];
@@ -1365,6 +1471,7 @@ struct EngineT final : Engine {
     for (int i = 0; i < lat.N; ++i) {
       a.push_back(Tn[i].p);
       for (int w = 0; w < 3; ++w) a.push_back(rot(i, w).p);
+      if (density) a.push_back(Ts[i].p);
       for (int k = 0; k < 4; ++k) {
         a.push_back(C[k][i].p);
         a.push_back(E[k][i].p);
@@ -1519,12 +1626,17 @@ struct EngineT final : Engine {
 
   // ---------------------------------------------------------- observables
   // Contract_one_site_iTPS_CTM (contract_itps_ctm/ctm.cpp:89-113)
+  // (iTPO: Contract_one_site_density_CTM, contract_density_ctm/ctm.cpp:89-116,
+  // as the single-layer network of the site tensor with op traced in)
   T one_site(int i, const DT<T>& op) {
+    if (density) return one_site_t(i, traced(i, op), one1);
+    return one_site_t(i, Tn[i], op);
+  }
+  T one_site_t(int i, const DT<T>& T1, const DT<T>& op) {
     const DT<T>&C1 = C[0][i], &C2 = C[1][i], &C3 = C[2][i], &C4 = C[3][i];
     const DT<T>&eT1 = E[0][i], &eT2 = E[1][i], &eT3 = E[2][i], &eT4 = E[3][i];
-    const DT<T>& T1 = Tn[i];
     DT<T> X = td(td(C2, td(C3, eT2, {0}, {1}), {1}, {1}), td(C1, eT1, {1}, {0}), {0}, {1});
-    DT<T> Y = td(td(td(C4, eT4, {1}, {0}), eT3, {0}, {1}), T1, {2, 5}, {0, 3}, false, true);
+    DT<T> Y = td(td(td(C4, eT4, {1}, {0}), eT3, {0}, {1}), bra(T1), {2, 5}, {0, 3}, false, true);
     DT<T> Z = td(X, Y, {0, 2, 3, 5}, {2, 5, 0, 4});
     DT<T> W = td(Z, T1, {0, 1, 2, 3}, {2, 1, 0, 3});
     return scalar(td(W, op, {0, 1}, {1, 0}));
@@ -1546,11 +1658,11 @@ struct EngineT final : Engine {
                  const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
                  const DT<T>& T1, const DT<T>& T2) {
     DT<T> A = td(eT5, td(C1, td(C4, eT6, {1}, {0}), {0}, {1}), {1}, {1});
-    A = td(T1, A, {0, 3}, {5, 2}, true, false);
+    A = td(bra(T1), A, {0, 3}, {5, 2}, true, false);
     A = td(T1, A, {0, 3}, {6, 4});
     A = td(eT1, A, {0, 2, 3}, {7, 0, 3});
     DT<T> B = td(eT4, td(C2, td(C3, eT3, {0}, {1}), {1}, {1}), {0}, {1});
-    B = td(T2, B, {2, 3}, {5, 2}, true, false);
+    B = td(bra(T2), B, {2, 3}, {5, 2}, true, false);
     B = td(T2, B, {2, 3}, {6, 4});
     B = td(eT2, B, {1, 2, 3}, {7, 1, 4});
     return td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
@@ -1559,6 +1671,7 @@ struct EngineT final : Engine {
                 const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
                 const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
     const DT<T> X = bond_X_h(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, T1, T2);
+    if (density) return density_op12(X, op12);
     return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
   }
 
@@ -1568,11 +1681,11 @@ struct EngineT final : Engine {
                  const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
                  const DT<T>& T1, const DT<T>& T2) {
     DT<T> A = td(eT6, td(C1, td(C2, eT1, {0}, {1}), {1}, {1}), {1}, {0});
-    A = td(T1, A, {0, 1}, {2, 5}, true, false);
+    A = td(bra(T1), A, {0, 1}, {2, 5}, true, false);
     A = td(T1, A, {0, 1}, {4, 6});
     A = td(eT2, A, {0, 2, 3}, {7, 0, 3});
     DT<T> B = td(eT5, td(C3, td(C4, eT4, {0}, {1}), {1}, {1}), {0}, {1});
-    B = td(T2, B, {0, 3}, {2, 5}, true, false);
+    B = td(bra(T2), B, {0, 3}, {2, 5}, true, false);
     B = td(T2, B, {0, 3}, {4, 6});
     B = td(eT3, B, {1, 2, 3}, {7, 1, 4});
     return td(A, B, {0, 1, 3, 5}, {0, 1, 3, 5});
@@ -1581,7 +1694,20 @@ struct EngineT final : Engine {
                 const DT<T>& eT2, const DT<T>& eT3, const DT<T>& eT4, const DT<T>& eT5, const DT<T>& eT6,
                 const DT<T>& T1, const DT<T>& T2, const DT<T>& op12) {
     const DT<T> X = bond_X_v(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, T1, T2);
+    if (density) return density_op12(X, op12);
     return scalar(td(op12, X, {0, 1, 2, 3}, {0, 2, 1, 3}));
+  }
+
+  // An iTPO bond: with the single-layer bra the X of bond_X_h / bond_X_v
+  // keeps each site's merged physical pair (p,q) open (its other leg has
+  // dimension 1), so X read as R[(p1,q1), (p2,q2)] is the environment of the
+  // two density tensors and <op12> = sum op12[p1,p2,q1,q2] R -- the
+  // contraction of Contract_two_sites_{horizontal,vertical}_op12_density_CTM
+  // (contract_density_ctm/ctm.cpp:196-274)
+  T density_op12(const DT<T>& X, const DT<T>& op12) {
+    const int64_t n1 = op12.dim(0) * op12.dim(2), n2 = op12.dim(1) * op12.dim(3);
+    if (X.dim(0) * X.dim(1) != n1 || X.dim(2) * X.dim(3) != n2) fail(TG_E_INPUT, "op12 does not match the bond");
+    return scalar(td(reshape(X, {n1, n2}), reshape(tr(op12, {0, 2, 1, 3}), {n1, n2}), {0, 1}, {0, 1}));
   }
 
   // twosite_obs.cpp:186-222: nearest-neighbour op12 with the source/target
@@ -1649,6 +1775,12 @@ struct EngineT final : Engine {
     }
     // X[a,c,b,d] with (a,c) the first site's legs: rdm_first[a,b,c,d] = X[a,c,b,d]; with the
     // source second, rdm_source[b,a,d,c] = X[a,c,b,d]
+    if (density) {
+      // an iTPO: R[(p_s,q_s), (p_t,q_t)], <op12> = sum op12[p_s,p_t,q_s,q_t] R (density_op12)
+      const DT<T> R = reshape(X, {X.dim(0) * X.dim(1), X.dim(2) * X.dim(3)});
+      download(source_first ? R : tr(R, {1, 0}), out);
+      return;
+    }
     download(tr(X, source_first ? V{0, 2, 1, 3} : V{2, 0, 3, 1}), out);
   }
 
@@ -1658,13 +1790,13 @@ struct EngineT final : Engine {
   DT<T> corr_start(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT3, const DT<T>& eT4,
                    const DT<T>& Tn1, const DT<T>& op) {
     DT<T> X = td(eT3, td(C1, td(C4, eT4, {1}, {0}), {0}, {1}), {1}, {1});
-    X = td(td(Tn1, op, {4}, {1}, true, false), X, {0, 3}, {5, 2});
+    X = td(td(bra(Tn1), op, {4}, {1}, true, false), X, {0, 3}, {5, 2});
     X = td(Tn1, X, {0, 3, 4}, {6, 4, 2});
     return tr(td(eT1, X, {0, 2, 3}, {5, 0, 2}), {0, 3, 1, 2});
   }
   // Transfer_iTPS_CTM (correlation.cpp:59-77)
   DT<T> corr_transfer(const DT<T>& A, const DT<T>& eT1, const DT<T>& eT3, const DT<T>& Tn1) {
-    DT<T> X = td(Tn1, td(A, eT3, {1}, {1}), {0, 3}, {2, 5}, true, false);
+    DT<T> X = td(bra(Tn1), td(A, eT3, {1}, {1}), {0, 3}, {2, 5}, true, false);
     X = td(Tn1, X, {0, 3, 4}, {4, 6, 2});
     return tr(td(eT1, X, {0, 2, 3}, {4, 0, 2}), {0, 3, 1, 2});
   }
@@ -1672,7 +1804,7 @@ struct EngineT final : Engine {
   T corr_finish(const DT<T>& A, const DT<T>& C2, const DT<T>& C3, const DT<T>& eT1, const DT<T>& eT2,
                 const DT<T>& eT3, const DT<T>& Tn1, const DT<T>& op) {
     DT<T> X = td(eT3, td(C2, td(C3, eT2, {0}, {1}), {1}, {1}), {0}, {1});
-    X = td(Tn1, X, {2, 3}, {5, 2}, true, false);
+    X = td(bra(Tn1), X, {2, 3}, {5, 2}, true, false);
     X = td(td(A, eT1, {0}, {0}), X, {0, 2, 3, 5}, {3, 0, 5, 1});
     X = td(Tn1, X, {0, 1, 2, 3}, {0, 1, 4, 3});
     return scalar(td(op, X, {0, 1}, {0, 1}));
@@ -1702,25 +1834,40 @@ struct EngineT final : Engine {
     for (int i = 0; i < lat.N; ++i)
       off[static_cast<size_t>(i + 1)] = off[static_cast<size_t>(i)] + static_cast<int64_t>(nright) * lat.pdim[i] * lat.pdim[i] * NW;
     static const V vrot = {3, 0, 1, 2, 4};
+    if (density) prepare_rotations();  // Ts
+    // the site tensor an operator enters with, rotated for the vertical
+    // strip: Tn with op, or for an iTPO the traced tensor with [[1]]
+    // (StartCorrelation / FinishCorrelation_density_CTM, correlation.cpp:33-98)
+    auto with_op = [&](int site, const DT<T>& op, DT<T>& k, DT<T>& o) {
+      k = density ? traced(site, op) : Tn[site];
+      if (dir == 1) k = tr(k, vrot);
+      o = density ? one1 : op;
+    };
+    // the tensor a transfer step absorbs (Transfer_density_CTM takes Ts)
+    auto plain = [&](int site) { return dir == 0 ? mt(site) : tr(mt(site), vrot); };
     const int64_t dl = lat.pdim[left];
     const DT<T> lop = from_host({dl, dl}, left_op);
     const DT<T> lid = identity_op(left);
-    DT<T> A, An;
+    DT<T> A, An, k, o;
     if (dir == 0) {
-      A = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], Tn[left], lop);
-      An = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], Tn[left], lid);
+      with_op(left, lop, k, o);
+      A = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], k, o);
+      with_op(left, lid, k, o);
+      An = corr_start(C[0][left], C[3][left], E[0][left], E[2][left], E[3][left], k, o);
     } else {
-      const DT<T> tn = tr(Tn[left], vrot);
-      A = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], tn, lop);
-      An = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], tn, lid);
+      with_op(left, lop, k, o);
+      A = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], k, o);
+      with_op(left, lid, k, o);
+      An = corr_start(C[3][left], C[2][left], E[3][left], E[1][left], E[2][left], k, o);
     }
     int site = left;
     for (int r = 0; r < r_max; ++r) {
       site = dir == 0 ? lat.right(site) : lat.top(site);
-      const DT<T> tn = dir == 0 ? Tn[site] : tr(Tn[site], vrot);
       auto fin = [&](const DT<T>& S, const DT<T>& op) {
-        return dir == 0 ? corr_finish(S, C[1][site], C[2][site], E[0][site], E[1][site], E[2][site], tn, op)
-                        : corr_finish(S, C[0][site], C[1][site], E[3][site], E[0][site], E[1][site], tn, op);
+        DT<T> kk, oo;
+        with_op(site, op, kk, oo);
+        return dir == 0 ? corr_finish(S, C[1][site], C[2][site], E[0][site], E[1][site], E[2][site], kk, oo)
+                        : corr_finish(S, C[0][site], C[1][site], E[3][site], E[0][site], E[1][site], kk, oo);
       };
       const std::complex<double> nrm = as_complex(fin(An, identity_op(site)));
       const int64_t d = lat.pdim[site];
@@ -1731,6 +1878,7 @@ struct EngineT final : Engine {
         out[2 * (r * nright + q) + 1] = v.imag();
       }
       if (r + 1 < r_max) {
+        const DT<T> tn = plain(site);
         if (dir == 0) {
           A = corr_transfer(A, E[0][site], E[2][site], tn);
           An = corr_transfer(An, E[0][site], E[2][site], tn);
@@ -1780,15 +1928,16 @@ struct EngineT final : Engine {
     for (int r = 0; r < nrow; ++r) {
       B = td(E[3][idx[r][0]], B, {1}, {0});  // (a', y, yb, k0, kb0, ..., r)
       for (int c = 0; c < ncol; ++c) {
-        const DT<T>& Tc = Tn[idx[r][c]];
+        // an iTPO site enters with its operator (or the identity) traced in
+        const DT<T>& o = ops[static_cast<size_t>(r * ncol + c)];
+        const DT<T> Tk = density ? traced(idx[r][c], o.empty() ? identity_op(idx[r][c]) : o) : Tn[idx[r][c]];
         const int pos = 1 + 2 * c;
         B = tr(B, moved_to_end(B.rank(), pos, 4));  // (..., y, yb, k, kb)
         int n = B.rank();
-        B = td(B, Tc, {n - 4, n - 2}, {0, 1});  // (..., yb, kb, y', z, p)
-        const DT<T>& o = ops[static_cast<size_t>(r * ncol + c)];
-        if (!o.empty()) B = td(B, o, {B.rank() - 1}, {0});
+        B = td(B, Tk, {n - 4, n - 2}, {0, 1});  // (..., yb, kb, y', z, p)
+        if (!o.empty() && !density) B = td(B, o, {B.rank() - 1}, {0});
         n = B.rank();
-        B = td(B, Tc, {n - 5, n - 4, n - 1}, {0, 1, 4}, false, true);  // (..., y', z, yb', zb)
+        B = td(B, bra(Tk), {n - 5, n - 4, n - 1}, {0, 1, 4}, false, true);  // (..., y', z, yb', zb)
         n = B.rank();
         V p;
         for (int i = 0; i < n - 4; ++i) p.push_back(i);
@@ -2193,11 +2342,68 @@ struct EngineT final : Engine {
   // -------------------------------------------------------- simple update
   void su_onesite(int site, const double* op) override {
     check_site(site);
-    const int64_t d = lat.pdim[site];
+    if (density) {
+      const std::vector<double> k = density_site_op(op, lat.pdim[site]);
+      su_onesite_raw(site, k.data());
+    } else {
+      su_onesite_raw(site, op);
+    }
+  }
+  // Tn = tensordot(Tn, op, Axes(4), Axes(0)) (simple_update.cpp:27-30) with
+  // op of the stored last leg
+  void su_onesite_raw(int site, const double* op) {
+    const int64_t d = tdim(site);
     DT<T> o = from_host({d, d}, op);
     Tn[site] = td(Tn[site], o, {4}, {0});
     rot_ok[site] = false;
     TG_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // iTPS::simple_update_density (simple_update.cpp:141-178) on the merged
+  // physical pair (p,q) -> p*d+q.  A one-site operator makes
+  // Tn'[..,a,c] = sum_{p,q} Tn[..,p,q] op[p,a] conj(op[c,q]); a bond
+  // operator acts as mptensor::kron(op, conj(op)), whose legs are
+  // (i*d + j) of op's i and conj(op)'s j.
+  std::vector<double> density_site_op(const double* op, int64_t d) const {
+    std::vector<double> out(static_cast<size_t>(d * d * d * d * NW), 0.0);
+    for (int64_t p = 0; p < d; ++p)
+      for (int64_t q = 0; q < d; ++q)
+        for (int64_t a = 0; a < d; ++a)
+          for (int64_t c = 0; c < d; ++c) {
+            const double* x = op + (p * d + a) * NW;
+            const double* y = op + (c * d + q) * NW;
+            const size_t o = static_cast<size_t>(((p * d + q) * d * d + (a * d + c)) * NW);
+            cmul_conj(x, y, out.data() + o);
+          }
+    return out;
+  }
+  std::vector<double> density_bond_op(const double* op, int64_t d1, int64_t d2) const {
+    const int64_t n = d1 * d2 * d1 * d2;
+    std::vector<double> out(static_cast<size_t>(n * n * NW), 0.0);
+    const int64_t dim[4] = {d1, d2, d1, d2};
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t j = 0; j < n; ++j) {
+        int64_t ii = i, jj = j, idx = 0;
+        int64_t a[4], b[4];
+        for (int l = 3; l >= 0; --l) {
+          a[l] = ii % dim[l];
+          ii /= dim[l];
+          b[l] = jj % dim[l];
+          jj /= dim[l];
+        }
+        for (int l = 0; l < 4; ++l) idx = idx * dim[l] * dim[l] + a[l] * dim[l] + b[l];
+        cmul_conj(op + i * NW, op + j * NW, out.data() + idx * NW);
+      }
+    return out;
+  }
+  // out = x * conj(y) for NW doubles per value
+  static void cmul_conj(const double* x, const double* y, double* out) {
+    if constexpr (CPLX) {
+      out[0] = x[0] * y[0] + x[1] * y[1];
+      out[1] = x[1] * y[0] - x[0] * y[1];
+    } else {
+      out[0] = x[0] * y[0];
+    }
   }
 
   DT<double> dvec(const std::vector<double>& h) {
@@ -2280,6 +2486,22 @@ struct EngineT final : Engine {
   // goes to the device as one launch of one block per bond.
   void su_bonds(int n, const int* sources, const int* legs, const double* const* ops) override {
     if (n < 0) fail(TG_E_INPUT, "negative count");
+    std::vector<std::vector<double>> conv;  // an iTPO's operators on the merged physical legs
+    std::vector<const double*> cops;
+    if (density) {
+      conv.resize(static_cast<size_t>(n));
+      cops.resize(static_cast<size_t>(n));
+      for (int i = 0; i < n; ++i) {
+        check_site(sources[i]);
+        if (!ops || !ops[i]) fail(TG_E_INPUT, "null operator");
+        if (legs[i] > 3) fail(TG_E_INPUT, "source_leg must be -1..3");
+        conv[i] = legs[i] < 0 ? density_site_op(ops[i], lat.pdim[sources[i]])
+                              : density_bond_op(ops[i], lat.pdim[sources[i]],
+                                                lat.pdim[lat.neighbor(sources[i], legs[i])]);
+        cops[i] = conv[i].data();
+      }
+      ops = cops.data();
+    }
     trim_op_cache(static_cast<size_t>(n));
     std::vector<SuBondArgs> group;
     std::vector<char> busy(static_cast<size_t>(lat.N), 0);
@@ -2296,7 +2518,7 @@ struct EngineT final : Engine {
       if (!ops || !ops[i]) fail(TG_E_INPUT, "null operator");
       if (legs[i] < 0) {
         flush();
-        su_onesite(sources[i], ops[i]);
+        su_onesite_raw(sources[i], ops[i]);
         continue;
       }
       if (legs[i] > 3) fail(TG_E_INPUT, "source_leg must be -1..3");
@@ -2304,7 +2526,7 @@ struct EngineT final : Engine {
       SuBondArgs a{};
       if (!fused_args(sources[i], legs[i], ops[i], a)) {
         flush();
-        su_bond(sources[i], legs[i], ops[i]);
+        su_bond_raw(sources[i], legs[i], ops[i]);
         continue;
       }
       if (busy[static_cast<size_t>(sources[i])] || busy[static_cast<size_t>(target)] ||
@@ -2317,10 +2539,20 @@ struct EngineT final : Engine {
     flush();
   }
 
-  // core::Simple_update_bond (core/simple_update.cpp:50-198)
   void su_bond(int source, int connect1, const double* op) override {
     check_site(source);
     if (connect1 < 0 || connect1 > 3) fail(TG_E_INPUT, "source_leg must be 0..3");
+    if (density) {
+      const std::vector<double> k =
+          density_bond_op(op, lat.pdim[source], lat.pdim[lat.neighbor(source, connect1)]);
+      su_bond_raw(source, connect1, k.data());
+    } else {
+      su_bond_raw(source, connect1, op);
+    }
+  }
+  // core::Simple_update_bond (core/simple_update.cpp:50-198) with op on the
+  // stored last legs
+  void su_bond_raw(int source, int connect1, const double* op) {
     const int target = lat.neighbor(source, connect1);
     const int connect2 = (connect1 + 2) % 4;
     {
@@ -2406,6 +2638,23 @@ struct EngineT final : Engine {
   // drawn in first-leg-fastest order from mt19937(seed) (real part) and
   // mt19937(seed*11+137) (imaginary part); lambdas reset to one.
   void init_tensors(int seed, const double* dirs, const int* dir_len, const double* noises) override {
+    if (density) {
+      // iTPS::initialize_tensors_density (tensors.cpp:140-208): the identity
+      // operator, Tn[0,0,0,0,p,p] = 1, on every site; seed, directions and
+      // noise are not used
+      for (int i = 0; i < lat.N; ++i) {
+        const auto& v = lat.vdim[i];
+        const int64_t d = lat.pdim[i];
+        std::vector<double> h(static_cast<size_t>(Tn[i].size() * NW), 0.0);
+        for (int64_t p = 0; p < d; ++p) h[static_cast<size_t>((p * d + p) * NW)] = 1.0;
+        upload(Tn[i], h.data());
+        rot_ok[i] = false;
+        for (int l = 0; l < 4; ++l) lambda[i][l].assign(v[l], 1.0);
+      }
+      lam_host_stale = false;
+      lam_dev_stale = true;
+      return;
+    }
     std::mt19937 gen(static_cast<unsigned>(seed));
     std::mt19937 gen_im(static_cast<unsigned>(seed * 11 + 137));
     std::uniform_real_distribution<double> dist(-1.0, 1.0);
@@ -2559,6 +2808,7 @@ struct EngineT final : Engine {
   // are replaced, the environment is left to the caller's moves
   void fu_bond(int source, int leg, const double* op, const tg_fu_params* fp, int* iterations,
                int* converged) override {
+    if (density) fail(TG_E_INPUT, "the full update is not defined for an iTPO (finite_temperature.cpp runs the simple update only)");
     {
       require_env();
       check_site(source);
@@ -2640,6 +2890,7 @@ struct EngineT final : Engine {
   // initial environment, and dE/dTn by the reverse pass of adjoint.hpp
   void energy_grad(int nterms, const tg_window_term* terms, int iterations, int checkpoint_every,
                    double svd_broadening, double* energy, double* grad) override {
+    if (density) fail(TG_E_INPUT, "the energy gradient is defined for an iTPS only");
     if constexpr (CPLX) {
       fail(TG_E_INPUT, "energy gradient: real site tensors only");
     } else {

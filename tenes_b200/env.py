@@ -45,6 +45,9 @@ class CTMParams:
     mixed: bool = False
     cuda_graph: bool = True
     svd_solver: int = 0
+    # an iTPO (finite-temperature density operator): site tensors
+    # (D,D,D,D,d,d), single-layer CTMRG, density contractions
+    density: bool = False
 
     def to_c(self) -> _lib.Params:
         p = _lib.Params()
@@ -99,6 +102,8 @@ class Environment:
     # ------------------------------------------------------------- tensors
     def site_shape(self, i: int) -> Tuple[int, ...]:
         v = self.vdim[i]
+        if self.params.density:
+            return (v[0], v[1], v[2], v[3], self.pdim[i], self.pdim[i])
         return (v[0], v[1], v[2], v[3], self.pdim[i])
 
     def env_shape(self, which: int, i: int) -> Tuple[int, ...]:
@@ -107,7 +112,7 @@ class Environment:
             return (chi, chi)
         leg = {4: 1, 5: 2, 6: 3, 7: 0}[which]
         d = self.vdim[i][leg]
-        return (chi, chi, d, d)
+        return (chi, chi, d, 1 if self.params.density else d)
 
     def set_site_tensor(self, i: int, T: np.ndarray) -> None:
         a = _lib.as_host(T, self.is_complex)
@@ -208,6 +213,10 @@ class Environment:
         shape = (self.pdim[source], self.pdim[target]) * 2
         out = np.zeros(int(np.prod(shape)) * (2 if self.is_complex else 1))
         check(self.lib.tg_measure_bond_rdm(self.ctx, source, dx, dy, dptr(out)))
+        if self.params.density:
+            # R[(p_s,q_s),(p_t,q_t)] -> rdm[p_s,p_t,q_s,q_t], the same contraction rule
+            ds, dt = self.pdim[source], self.pdim[target]
+            return out.view(self.dtype).reshape(ds, ds, dt, dt).transpose(0, 2, 1, 3).copy()
         return out.view(self.dtype).reshape(shape)
 
     def correlation_strip(self, left: int, vertical: bool, r_max: int, left_op: np.ndarray, right_ops) -> np.ndarray:

@@ -1,15 +1,18 @@
-"""Drop-in driver for TeNeS's iTPS ground-state / time-evolution runs on the
-GPU path: ``python -m tenes_b200 input.toml`` in place of ``tenes input.toml``.
+"""Drop-in driver for TeNeS's iTPS ground-state, time-evolution and
+finite-temperature runs on the GPU path: ``python -m tenes_b200 input.toml``
+in place of ``tenes input.toml``.
 
 Mirrors the reference's driver (src/iTPS/main.cpp:141-199, iTPS.cpp,
 optimize.cpp:24-37, simple_update.cpp:103-138, time_evolution.cpp:21-90,
-measure.cpp:30-79) and its output files (onesite_obs.cpp:125-200,
-twosite_obs.cpp:288-340, multisite_obs.cpp:250-300, correlation_length.cpp:57-125,
-density.cpp:30-228, measure.cpp:81-107).  All tensor work goes through the C ABI
-of libtenes_gpu; this layer holds the reference's host-side bookkeeping only.
+finite_temperature.cpp:22-86, measure.cpp:30-144) and its output files
+(onesite_obs.cpp:125-200, twosite_obs.cpp:288-340, multisite_obs.cpp:250-300,
+correlation_length.cpp:57-125, density.cpp:30-228, measure.cpp:81-107).  All
+tensor work goes through the C ABI of libtenes_gpu; this layer holds the
+reference's host-side bookkeeping only.  In finite-temperature mode the
+context holds the density operator (tg_params.density) and the same
+measurement calls are the density contractions.
 
-Out of scope (raises InputError): finite-temperature mode, the mean-field
-environment.
+Out of scope (raises InputError): the mean-field environment.
 Long-range correlation functions ([correlation]) are measured through window
 contractions up to r = 3 and through the strip contraction beyond.
 Tensor checkpoints (tensor_save / tensor_load) are written and read by
@@ -94,8 +97,7 @@ class ITPS:
 
     def __init__(self, inp: Input, device: int = 0, mixed: bool = False, print_level: int = 1):
         p = inp.params
-        if p.calcmode == "finite_temperature":
-            raise InputError("finite-temperature (iTPO) mode is not part of this library")
+        self.density = p.calcmode == "finite_temperature"  # an iTPO (iTPS.cpp:176-180)
         if p.MeanField_Env:
             raise InputError("the mean-field environment is not part of this library")
         self.inp = inp
@@ -108,7 +110,7 @@ class ITPS:
                        ctm_convergence_epsilon=p.CTM_Convergence_Epsilon,
                        max_ctm_iteration=p.Max_CTM_Iteration, projector_corner=p.CTM_Projector_corner,
                        use_rsvd=p.Use_RSVD, rsvd_oversampling_factor=p.RSVD_Oversampling_factor,
-                       inverse_lambda_cut=p.Inverse_lambda_cut, mixed=mixed)
+                       inverse_lambda_cut=p.Inverse_lambda_cut, mixed=mixed, density=self.density)
         self.env = Environment(ls.LX, ls.LY, ls.physical_dims, ls.virtual_dims, cp, not self.is_real,
                                skew=ls.skew, device=device)
         for up in list(inp.simple_updates) + list(inp.full_updates):
@@ -139,7 +141,11 @@ class ITPS:
         self._first: Dict[str, bool] = {}
         self.t_su = self.t_fu = self.t_env = self.t_obs = 0.0
         self.t0 = _time.perf_counter()
-        if p.CHI < max(max(v) for v in ls.virtual_dims) ** 2 and print_level > 0:
+        dmax = max(max(v) for v in ls.virtual_dims)  # iTPS.cpp:120-136
+        if self.density:
+            if p.CHI < dmax and print_level > 0:
+                print("WARNING: CTM may be too small (chi < D) for iTPO (finite_temperature mode)", file=sys.stderr)
+        elif p.CHI < dmax ** 2 and print_level > 0:
             print("WARNING: CTM may be too small (chi < D*D) for iTPS", file=sys.stderr)
 
     @staticmethod
@@ -604,7 +610,9 @@ class ITPS:
             self.save_multisite(multi, time, prefix)
         if self.inp.corparam.r_max > 0:
             self.save_correlation(self.measure_correlation(), time, prefix)
-        if self.inp.tm_params.to_calculate:
+        # measure_density skips the transfer matrix at beta = 0, where it is
+        # degenerate (measure.cpp:133-139)
+        if self.inp.tm_params.to_calculate and not (self.density and time == 0.0):
             self.save_correlation_length(self.measure_transfer_matrix(), time, prefix)
         energy = self.save_density(vals, two, multi, time, prefix)
         self.t_obs += _time.perf_counter() - t
@@ -662,6 +670,45 @@ class ITPS:
             if nss[g] % mi[g] != 0:
                 self.measure(t, "TE_")
 
+    def finite_temperature(self) -> None:
+        """iTPS::finite_temperature (finite_temperature.cpp:22-86): imaginary-time
+        simple-update steps on the density operator, beta += 2 tau per step,
+        measure_density (measure.cpp:110-144) at beta = 0, every
+        measure_interval steps and after the last step of a group."""
+        p = self.p
+        ups = self.inp.simple_updates
+        groups = {u.group for u in ups}
+        ngroups = max(groups) + 1 if groups else 1
+        for g in range(ngroups):
+            if groups and g not in groups:
+                raise InputError(f"no simple update with group number {g}")
+
+        def per_group(v: List, what: str) -> List:
+            if len(v) == ngroups:
+                return list(v)
+            if len(v) == 1:
+                return list(v) * ngroups
+            raise InputError(f"size of {what} {len(v)} is not equal to the number of simple update groups.")
+
+        nss = per_group(p.num_simple_step, "num_step")
+        tau = per_group(p.tau_simple_step, "tau")
+        mi = list(p.measure_interval)
+        while len(mi) < ngroups:
+            mi.append(mi[-1])
+        beta = 0.0
+        self.measure(beta, "FT_")
+        for g in range(ngroups):
+            for step in range(nss[g]):
+                t0 = _time.perf_counter()
+                self.simple_update_step(g)
+                self.env.sync()
+                self.t_su += _time.perf_counter() - t0
+                beta += 2.0 * tau[g]
+                if mi[g] > 0 and (step + 1) % mi[g] == 0:
+                    self.measure(beta, "FT_")
+            if mi[g] == 0 or nss[g] % mi[g] != 0:
+                self.measure(beta, "FT_")
+
     def summary(self) -> None:
         """summary() (measure.cpp:81-107): time.dat."""
         with open(os.path.join(self.outdir, "time.dat"), "w") as f:
@@ -709,6 +756,9 @@ def run(path: str, device: int = 0, mixed: bool = False, print_level: int = 1,
     # is written after the optimisation, before the measurement
     if inp.params.calcmode == "time_evolution":
         it.time_evolution()
+        save_tensors(it.env, inp.params.tensor_save_dir, inp.params.CHI, print_level)
+    elif inp.params.calcmode == "finite_temperature":  # run_finitetemperature (main.cpp:180-198)
+        it.finite_temperature()
         save_tensors(it.env, inp.params.tensor_save_dir, inp.params.CHI, print_level)
     else:
         it.optimize()

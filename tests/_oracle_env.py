@@ -4,6 +4,7 @@ Test infrastructure only: it lets the front-end's driver loop and writers run
 here (no GPU) against the golden output files.  The product never imports it."""
 import numpy as np
 
+from oracle import tenes_density as D
 from oracle import tenes_oracle as O
 
 
@@ -22,6 +23,8 @@ class OracleEnvironment:
                           Inverse_lambda_cut=params.inverse_lambda_cut)
         self.env = None
         self.lam = [[np.ones(v[l]) for l in range(4)] for v in virtual_dims]
+        # an iTPO (finite temperature) runs through oracle/tenes_density.py
+        self.density = bool(getattr(params, "density", False))
 
     # accessors of tenes_b200.env.Environment (checkpoints)
     @property
@@ -34,7 +37,8 @@ class OracleEnvironment:
 
     def site_shape(self, i):
         v = self.lat.virtual_dims[i]
-        return (v[0], v[1], v[2], v[3], self.lat.physical_dims[i])
+        d = self.lat.physical_dims[i]
+        return (v[0], v[1], v[2], v[3], d, d) if self.density else (v[0], v[1], v[2], v[3], d)
 
     def env_shape(self, which, i):
         chi = self.p.CHI
@@ -79,12 +83,28 @@ class OracleEnvironment:
     def init_tensors(self, seed, initial_dirs, noises):
         self.lat.initial_dirs = [list(d) for d in initial_dirs]
         self.lat.noises = list(noises)
+        if self.density:
+            self.Tn = D.initial_density(self.lat, not self.is_complex)
+            return
         self.Tn = O.initialize_tensors(self.lat, seed, not self.is_complex)
 
     def fix_local_gauge(self, maxiter=100, eps=1e-2):
+        if self.density:
+            flat = [t.reshape(t.shape[:4] + (-1,)) for t in self.Tn]
+            r = O.fix_local_gauge(flat, self.lam, self.lat, self.p, maxiter, eps)
+            self.Tn = [f.reshape(t.shape) for f, t in zip(flat, self.Tn)]
+            return r
         return O.fix_local_gauge(self.Tn, self.lam, self.lat, self.p, maxiter, eps)
 
     def simple_update(self, source, leg, op):
+        if self.density:
+            class _Up:
+                pass
+            up = _Up()
+            up.source_site, up.source_leg, up.op = source, leg, op
+            up.is_onesite = lambda: leg < 0
+            D.su_density(self.Tn, self.lam, self.lat, up, self.p)
+            return
         if leg < 0:
             self.Tn[source] = np.tensordot(self.Tn[source], op, ([4], [0]))
             return
@@ -118,6 +138,9 @@ class OracleEnvironment:
         return it, conv
 
     def correlation_strip(self, left, vertical, r_max, left_op, right_ops):
+        if self.density:
+            return np.array(D.correlation_strip(self.env, self.Tn, self.lat, left, vertical, r_max, left_op,
+                                                right_ops))
         return np.array(O.correlation_strip(self.env, self.Tn, self.lat, left, vertical, r_max, left_op,
                                             right_ops))
 
@@ -126,16 +149,20 @@ class OracleEnvironment:
         fn(self.env, self.Tn, line, self.p, self.lat)
 
     def calc_ctm_environment(self, initialize=True):
-        self.env, it, conv, sig = O.calc_ctm_environment(self.Tn, self.p, self.lat)
+        calc = D.calc_ctm_environment if self.density else O.calc_ctm_environment
+        self.env, it, conv, sig = calc(self.Tn, self.p, self.lat)
         return it, conv, sig
 
     def contract_one_site(self, i, op):
         e = self.env
-        return complex(O.contract_one_site(e.C1[i], e.C2[i], e.C3[i], e.C4[i], e.eTt[i], e.eTr[i], e.eTb[i],
+        f = D.contract_one_site if self.density else O.contract_one_site
+        return complex(f(e.C1[i], e.C2[i], e.C3[i], e.C4[i], e.eTt[i], e.eTr[i], e.eTb[i],
                                            e.eTl[i], self.Tn[i], op))
 
     def contract_bond_op12(self, source, dx, dy, op):
         e, lat, Tn = self.env, self.lat, self.Tn
+        if self.density:
+            return D.contract_op12(e, Tn, lat, source, dx, dy, op)
         if dy == 0:
             sc = 0 if dx >= 0 else 1
             l, r = lat.other(source, -sc, 0), lat.other(source, 1 - sc, 0)
@@ -152,6 +179,8 @@ class OracleEnvironment:
 
     def contract_window(self, source, nrow, ncol, source_row, source_col, ops=None):
         ops = ops or {}
+        if self.density:
+            return D.window_value(self.env, self.Tn, self.lat, source, nrow, ncol, source_row, source_col, ops)
         idx, Cs, eTt, eTr, eTb, eTl, T = O._window(self.env, self.Tn, self.lat, source, source_col, source_row,
                                                     nrow, ncol)
         grid = [[ops.get((r, c), np.eye(self.lat.physical_dims[idx[r][c]])) for c in range(ncol)]
@@ -162,4 +191,6 @@ class OracleEnvironment:
                        arnoldi_restartdim=20, arnoldi_maxiter=1, arnoldi_rtol=1e-10):
         tp = O.TMParams(num_eigvals, maxdim_dense, arnoldi_maxdim, arnoldi_restartdim, arnoldi_maxiter,
                         arnoldi_rtol)
+        if self.density:
+            return D.tm_eigenvalues(self.env, self.lat, direction, fixed, tp)
         return O.tm_eigenvalues(self.env, self.lat, direction, fixed, tp)

@@ -151,3 +151,31 @@ def test_te_tfi_driver_on_oracle(tmp_path, monkeypatch):
                 assert all(np.isinf(rf[4:])), rf
             n = min(len(rs), len(rf))
             np.testing.assert_allclose(rs[:n], rf[:n], rtol=1e-9, atol=1e-11, err_msg=name)
+
+
+@pytest.mark.parametrize("stem,tol,tol_xi", [("ft_tfi_square", 5e-5, 5e-4), ("ft_kitaev", 1e-10, 1e-4)])
+def test_finite_temperature_driver_on_oracle(tmp_path, monkeypatch, stem, tol, tol_xi):
+    """The finite-temperature front end (iTPS::finite_temperature: beta
+    stepping, measure_density with the transfer matrix skipped at beta = 0,
+    the FT_ writers) over the oracle-backed stand-in reproduces the
+    reference's FT_TFI_square and FT_Kitaev output files; the tolerance is
+    the oracle's own distance to them (tests/test_oracle_density.py)."""
+    import tenes_b200.itps as itps
+    from tests._oracle_env import OracleEnvironment
+    from tests._ft import expected
+
+    monkeypatch.setattr(itps, "Environment", OracleEnvironment)
+    itps.run(os.path.join(GOLDEN, stem + "_input.toml"), print_level=0, outdir=str(tmp_path))
+    exp = expected(stem)
+    for name, key in [("FT_density.dat", "density"), ("FT_onesite_obs.dat", "onesite"),
+                      ("FT_twosite_obs.dat", "twosite"), ("FT_correlation_length.dat", "correlation_length"),
+                      ("FT_correlation.dat", "correlation")]:
+        res = _rows(tmp_path / name)
+        ref = exp[key]
+        assert len(res) == len(ref), name
+        for rs, rf in zip(res, ref):
+            assert len(rs) == len(rf), name
+            t = tol_xi if key == "correlation_length" else tol
+            np.testing.assert_allclose(rs, rf, rtol=t, atol=t, err_msg=name)
+    head = open(tmp_path / "FT_density.dat").read().splitlines()
+    assert head[1] == "# $1: inverse temperature"

@@ -78,21 +78,34 @@ def _density(path):
 
 def test_restart_from_saved_tensors(tmp_path):
     """The reference's restart test (test/restart.py.in) on the GPU front end:
-    restart_0 runs 10 simple-update steps and saves the tensors, restart_1
-    loads them and runs on; density, one-site and two-site observables of the
-    two runs agree within the reference test's tolerances (rtol 1e-3, atol
-    1e-4)."""
+    restart_0 runs 10 simple-update steps and saves the tensors and weights,
+    restart_1 loads them and runs 10 more.  Both inputs write into
+    output_restart_0 (the reference's test then compares that directory with
+    itself), so the first run's output is moved aside; the continued run must
+    reproduce one uninterrupted run of 20 steps from the same start, and its
+    observables must have moved away from the first run's."""
     for k in (0, 1):
         shutil.copyfile(os.path.join(GOLDEN, f"restart_{k}_input.toml"), tmp_path / f"restart_{k}.toml")
-        r = subprocess.run([sys.executable, "-m", "tenes_b200", f"restart_{k}.toml", "--quiet"], cwd=tmp_path,
+    txt = open(os.path.join(GOLDEN, "restart_0_input.toml")).read()
+    assert "num_step = 10" in txt and "tensor_save = 'tensor'" in txt
+    txt = txt.replace("num_step = 10", "num_step = 20", 1).replace("tensor_save = 'tensor'", "")
+    (tmp_path / "twenty.toml").write_text(txt.replace("output = 'output_restart_0'", "output = 'output_twenty'"))
+
+    def run(name):
+        r = subprocess.run([sys.executable, "-m", "tenes_b200", name, "--quiet"], cwd=tmp_path,
                            capture_output=True, text=True, timeout=900, env=_env())
         assert r.returncode == 0, r.stderr[-3000:]
+    run("restart_0.toml")
     assert (tmp_path / "tensor" / "params.dat").exists()
-    ref, res = tmp_path / "output_restart_0", tmp_path / "output_restart_1"
+    shutil.move(str(tmp_path / "output_restart_0"), str(tmp_path / "first"))
+    run("restart_1.toml")
+    run("twenty.toml")
+    res, ref, first = tmp_path / "output_restart_0", tmp_path / "output_twenty", tmp_path / "first"
     a, b = _density(res / "density.dat"), _density(ref / "density.dat")
     assert len(a) == len(b)
-    np.testing.assert_allclose(a, b, rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12)
+    assert np.max(np.abs(np.array(a) - np.array(_density(first / "density.dat")))) > 1e-6
     for name in ("onesite_obs.dat", "twosite_obs.dat"):
         x, y = _read(res / name), _read(ref / name)
         assert len(x) == len(y), name
-        np.testing.assert_allclose(np.array(x), np.array(y), rtol=1e-3, atol=1e-4, err_msg=name)
+        np.testing.assert_allclose(np.array(x), np.array(y), rtol=1e-9, atol=1e-12, err_msg=name)

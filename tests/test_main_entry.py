@@ -40,16 +40,17 @@ def _run(host, cwd, *inputs, print_level=0, timeout=900):
 
 
 def test_missing_and_bad_inputs_are_input_errors(host, tmp_path):
-    bad = tmp_path / "ft.toml"
-    text = open(os.path.join(GOLDEN, "te_tfi_input.toml")).read().replace("mode = 'time'",
-                                                                          "mode = 'finite temperature'")
+    bad = tmp_path / "mf.toml"
+    text = open(os.path.join(GOLDEN, "te_tfi_input.toml")).read().replace("meanfield_env = false",
+                                                                          "meanfield_env = true")
+    assert "meanfield_env = true" in text
     bad.write_text(text)
     r = _run(host, tmp_path, str(tmp_path / "absent.toml"), str(bad), "")
     statuses = [int(x) for x in re.findall(r"^status (\d+)$", r.stdout, re.M)]
     assert statuses == [TG_E_INPUT] * 3, r.stdout + r.stderr
     msgs = re.findall(r"^message (.*)$", r.stdout, re.M)
     assert "absent.toml" in msgs[0]
-    assert "finite-temperature" in msgs[1]
+    assert "mean-field" in msgs[1]
     assert "empty" in msgs[2]
     assert r.returncode == TG_E_INPUT
 
