@@ -1161,10 +1161,9 @@ struct EngineT final : Engine {
   // Each move has the two passes of Left_move (ctm.cpp:562-616): all the
   // projectors of the line, then the new corners and edges of the next line.
   // The reference writes into copies (C1_bak, ...) and copies back; here the
-  // results go straight into the environment storage, which is safe because
-  // every row reads the current line and writes the next one (for a line
-  // count of 1 both are the same line, and then every tensor is read and
-  // written by one row only).  The reference computes every new edge tensor
+  // results go straight into the environment storage, and pass 2 reads from
+  // copies only where the current and the next line share sites (a skewed
+  // cell, pass_inputs).  The reference computes every new edge tensor
   // twice -- row iy's eT[k] and row iy-1's eT[j] are the same Calc_Next_eT
   // of the same inputs -- so each distinct (output, inputs) job runs once;
   // when two jobs write one output the later one wins, as in the reference.
@@ -1184,6 +1183,23 @@ struct EngineT final : Engine {
       if (!superseded && !repeated) out.push_back(jobs[a]);
     }
     return out;
+  }
+
+  // Pass 2 of a move writes the corners and edges of the next line while it
+  // reads those of the current one.  Where a site is in both -- on a skewed
+  // cell a row's next line is another row's current one -- every read must
+  // see the tensor as it was before the pass, the reference's C1_bak /
+  // C4_bak / eTl_bak (ctm.cpp:595-601): the family is then read from copies
+  // made before the rows start.  Elsewhere nothing is copied.
+  const std::vector<DT<T>>& pass_inputs(const std::vector<DT<T>>& fam, const std::vector<int>& reads,
+                                        const std::vector<int>& writes, std::vector<DT<T>>& copy) {
+    bool shared = false;
+    for (int w : writes)
+      for (int r : reads) shared = shared || w == r;
+    if (!shared) return fam;
+    copy.resize(fam.size());
+    for (size_t i = 0; i < fam.size(); ++i) copy[i] = clone(fam[i], st);
+    return copy;
   }
 
   void left_move(int ix) {
@@ -1210,17 +1226,30 @@ struct EngineT final : Engine {
       jobs.push_back({k, l, l, dn, iy});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
+    std::vector<int> ra, wa, rb, wb, re, we;
+    for (int iy = 0; iy < LY; ++iy) {
+      const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
+      ra.push_back(i), wa.push_back(j), rb.push_back(l), wb.push_back(k);
+    }
+    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
+    std::vector<DT<T>> ca, cb, ce;
+    const auto& C1in = pass_inputs(C1, ra, wa, ca);
+    const auto& C4in = pass_inputs(C4, rb, wb, cb);
+    const auto& eTlin = pass_inputs(eTl, re, we, ce);
     for_rows(LY, par, [&](int iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C1[i], C4[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
+      next_ctm(C1in[i], C4in[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
       for (size_t q = iy; q < fin.size(); q += LY) {
         const EtJob& b = fin[q];
-        next_et(eTl[b.src], mt(b.site), PUs[b.pu], PLs[b.pl], eTl[b.out]);
+        next_et(eTlin[b.src], mt(b.site), PUs[b.pu], PLs[b.pl], eTl[b.out]);
       }
     });
     keep(PUs);
     keep(PLs);
+    keep(ca);
+    keep(cb);
+    keep(ce);
   }
 
   void right_move(int ix) {
@@ -1247,17 +1276,30 @@ struct EngineT final : Engine {
       jobs.push_back({i, j, j, up, iy});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
+    std::vector<int> ra, wa, rb, wb, re, we;
+    for (int iy = 0; iy < LY; ++iy) {
+      const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
+      ra.push_back(k), wa.push_back(l), rb.push_back(j), wb.push_back(i);
+    }
+    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
+    std::vector<DT<T>> ca, cb, ce;
+    const auto& C3in = pass_inputs(C3, ra, wa, ca);
+    const auto& C2in = pass_inputs(C2, rb, wb, cb);
+    const auto& eTrin = pass_inputs(eTr, re, we, ce);
     for_rows(LY, par, [&](int iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C3[k], C2[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
+      next_ctm(C3in[k], C2in[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
       for (size_t q = iy; q < fin.size(); q += LY) {
         const EtJob& b = fin[q];
-        next_et(eTr[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
+        next_et(eTrin[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
       }
     });
     keep(PUs);
     keep(PLs);
+    keep(ca);
+    keep(cb);
+    keep(ce);
   }
 
   void top_move(int iy) {
@@ -1284,17 +1326,30 @@ struct EngineT final : Engine {
       jobs.push_back({l, i, i, lf, ix});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
+    std::vector<int> ra, wa, rb, wb, re, we;
+    for (int ix = 0; ix < LX; ++ix) {
+      const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
+      ra.push_back(j), wa.push_back(k), rb.push_back(i), wb.push_back(l);
+    }
+    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
+    std::vector<DT<T>> ca, cb, ce;
+    const auto& C2in = pass_inputs(C2, ra, wa, ca);
+    const auto& C1in = pass_inputs(C1, rb, wb, cb);
+    const auto& eTtin = pass_inputs(eTt, re, we, ce);
     for_rows(LX, par, [&](int ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C2[j], C1[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
+      next_ctm(C2in[j], C1in[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
       for (size_t q = ix; q < fin.size(); q += LX) {
         const EtJob& b = fin[q];
-        next_et(eTt[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
+        next_et(eTtin[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
       }
     });
     keep(PUs);
     keep(PLs);
+    keep(ca);
+    keep(cb);
+    keep(ce);
   }
 
   void bottom_move(int iy) {
@@ -1321,17 +1376,30 @@ struct EngineT final : Engine {
       jobs.push_back({j, k, k, rt, ix});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
+    std::vector<int> ra, wa, rb, wb, re, we;
+    for (int ix = 0; ix < LX; ++ix) {
+      const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
+      ra.push_back(l), wa.push_back(i), rb.push_back(k), wb.push_back(j);
+    }
+    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
+    std::vector<DT<T>> ca, cb, ce;
+    const auto& C4in = pass_inputs(C4, ra, wa, ca);
+    const auto& C3in = pass_inputs(C3, rb, wb, cb);
+    const auto& eTbin = pass_inputs(eTb, re, we, ce);
     for_rows(LX, par, [&](int ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C4[l], C3[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
+      next_ctm(C4in[l], C3in[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
       for (size_t q = ix; q < fin.size(); q += LX) {
         const EtJob& b = fin[q];
-        next_et(eTb[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
+        next_et(eTbin[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
       }
     });
     keep(PUs);
     keep(PLs);
+    keep(ca);
+    keep(cb);
+    keep(ce);
   }
 
   // ------------------------------------------------------ initialisation

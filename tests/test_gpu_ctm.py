@@ -243,3 +243,39 @@ def test_graph_sweeps_equal_eager_sweeps(is_complex):
                 e.set_site_tensor(0, Tn[1] if Tn[1].shape == Tn[0].shape else Tn[0])
                 for _ in range(3):
                     e.sweep()
+
+
+@pytest.mark.parametrize("LX,LY,skew", [(2, 1, 1), (3, 2, 1), (2, 2, 1)])
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_skewed_cell_ctm_run_matches_oracle(LX, LY, skew, is_complex):
+    """Skewed unit cells, where a move's current and next lines share sites
+    (the second pass must read the corners and edges as they were before it,
+    the reference's C1_bak / eTl_bak, ctm.cpp:595-601): a whole run against the
+    oracle, corner spectra, one-site values and both transfer-matrix
+    spectra, whose sub-leading eigenvalues see every edge tensor."""
+    lat = make_lattice(LX, LY, 2, skew=skew)
+    Tn = random_tensors(lat, 7 + LX + LY, is_complex)
+    chi, iters = 8, 4
+    oe, ocnt, _, _ = O.calc_ctm_environment(Tn, oracle_params(chi, Max_CTM_Iteration=iters), lat)
+    ge = gpu_env(lat, Tn, chi, is_complex, max_ctm_iteration=iters)
+    gcnt, _, _ = ge.calc_ctm_environment(True)
+    assert gcnt == ocnt
+    for w, name in enumerate(("C1", "C2", "C3", "C4")):
+        for i in range(lat.N_UNIT):
+            np.testing.assert_allclose(ge.corner_spectrum(w, i), O.corner_spectrum(getattr(oe, name)[i]),
+                                       rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(_observables_gpu(ge, lat), _observables_oracle(oe, Tn, lat), rtol=TOL, atol=1e-12)
+    # The vertical transfer matrix of a skewed cell continues at column
+    # x + skew after the top row (transfer_matrix.cpp:281, 302), while the
+    # site above that row is in column x - skew (SquareLattice.cpp:95-100);
+    # unless the two coincide (2 skew = 0 mod LX) it chains edge tensors that
+    # share no bond, and its spectrum depends on the projectors' singular-
+    # vector phases -- in the reference as much as here -- so only the
+    # well-defined cases are compared.
+    dirs = (0, 1) if (2 * skew) % LX == 0 else (0,)
+    for d in dirs:
+        fixed = 0
+        o = O.tm_eigenvalues(oe, lat, d, fixed, O.TMParams())
+        g = ge.tm_eigenvalues(d, fixed)
+        np.testing.assert_allclose(np.abs(g), np.abs(o), rtol=1e-8, atol=1e-14)
+    ge.close()
