@@ -19,6 +19,8 @@ each arm's energy per site against the FP64 oracle run from the same site
 tensors.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --ft     # iTPO: single-layer CTMRG, density simple update, FT_TFI_square run
+    python bench.py --grad   # energy gradient of the J1-J2 model (adjoint CTMRG)
 
 N>1 runs N independent replicas (one per GPU, different seeds; the CTMRG of
 one unit cell does not shard) and reports the summed sweeps/s.
@@ -1003,6 +1005,152 @@ def run_grad(args):
                       "grad_rel_err": float(np.linalg.norm(gmv - gv) / np.linalg.norm(gv))}}
 
 
+# iTPO workload (finite temperature, ctm_single.cpp): TFI on the square
+# lattice, bond -SzSz, field -hx Sx on the bonds' sites, density operator of
+# a 2x2 cell from the identity at beta = 0 through FT["su_steps"] density
+# simple-update steps at tau (beta = 2 tau per step).
+FT = dict(D=8, chi=64, su_steps=200, tau=0.01, hx=1.0)
+
+
+def ft_problem():
+    """(lattice spec, Trotter step as (source, leg, op) triples, bond
+    Hamiltonian) of the iTPO workload."""
+    from tenes_b200.std_ops import evolution_onesite, evolution_twosite, ising_bond, real_if_close, spin_ops
+    _, Sx, _ = spin_ops(0.5)
+    op = real_if_close(evolution_twosite(ising_bond(1.0), FT["tau"]))
+    op1 = real_if_close(evolution_onesite(-FT["hx"] * Sx, FT["tau"]))
+    step = [(s, leg, op) for (s, leg) in bonds(2, 2)] + [(s, -1, op1) for s in range(4)]
+    h = real_if_close(ising_bond(1.0))
+    return step, h, Sx
+
+
+def ft_env(device, T=None):
+    from tenes_b200.env import CTMParams, Environment
+    p = CTMParams(chi=FT["chi"], max_ctm_iteration=1, density=True)
+    env = Environment(2, 2, [2] * 4, [[FT["D"]] * 4] * 4, p, False, device=device)
+    if T is None:
+        env.init_tensors(SEED, [[0.0]] * 4, [0.0] * 4)
+    else:
+        for i, t in enumerate(T):
+            env.set_site_tensor(i, t)
+    return env
+
+
+def ft_energy(env, h, Sx):
+    """E/site = <bond terms> + <-hx Sx> through the density contractions."""
+    ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    e = 0.0
+    for s in range(4):
+        for dx, dy in ((1, 0), (0, 1)):
+            e += (env.contract_bond_op12(s, dx, dy, h) / env.contract_bond_op12(s, dx, dy, ident)).real
+        e -= FT["hx"] * (env.contract_one_site(s, Sx) / env.contract_one_site(s, np.eye(2))).real
+    return e / 4
+
+
+def run_ft(args):
+    """Single-layer (iTPO) CTMRG sweeps/s at D=8, chi=64 with the
+    reference-default full-SVD corner projectors, the density simple update's
+    steps/s, the energy per site against the oracle, and the whole
+    FT_TFI_square run (500 steps, 6 measurements) end to end through the
+    front end."""
+    import torch
+    from oracle import tenes_density as Dn
+    from oracle import tenes_oracle as O
+    from tenes_b200.env import kernel_launch_count
+    device = 0
+    step, h, Sx = ft_problem()
+    env = ft_env(device)
+    t0 = time.perf_counter()
+    for _ in range(FT["su_steps"]):
+        env.simple_update_many(step)
+    env.sync()
+    su_s = time.perf_counter() - t0
+    T = [env.get_site_tensor(i) for i in range(4)]
+    env.init_env()
+    stream = torch.cuda.ExternalStream(env.stream_handle())
+    flush = torch.empty(int(256e6) // 4, dtype=torch.float32, device=f"cuda:{device}")
+    l0 = kernel_launch_count()
+    times = timed_sweeps(env, args.steps, args.warmup, stream, flush)
+    launches = (kernel_launch_count() - l0) // max(args.steps + args.warmup, 1)
+    n_sw = args.warmup + args.steps
+    e_gpu = ft_energy(env, h, Sx)
+    env.close()
+    # the oracle: same tensors, the same number of sweeps; the first sweep is the CPU sample
+    lat = O.Lattice(2, 2)
+    lat.physical_dims = [2] * 4
+    lat.virtual_dims = [[FT["D"]] * 4] * 4
+    p = O.Params(CHI=FT["chi"], Max_CTM_Iteration=1)
+    Ts = [Dn.single_tensor(t) for t in T]
+    oe = Dn.init_env(Ts, lat)
+    sw = []
+    for _ in range(n_sw):
+        t1 = time.perf_counter()
+        Dn.sweep(oe, Ts, p, lat)
+        sw.append(time.perf_counter() - t1)
+    ident = np.einsum("ac,bd->abcd", np.eye(2), np.eye(2))
+    e_or = 0.0
+    for s in range(4):
+        for dx, dy in ((1, 0), (0, 1)):
+            e_or += (Dn.contract_op12(oe, T, lat, s, dx, dy, h) / Dn.contract_op12(oe, T, lat, s, dx, dy, ident)).real
+        e = oe
+        n1 = Dn.contract_one_site(e.C1[s], e.C2[s], e.C3[s], e.C4[s], e.eTt[s], e.eTr[s], e.eTb[s], e.eTl[s], T[s],
+                                  np.eye(2))
+        v1 = Dn.contract_one_site(e.C1[s], e.C2[s], e.C3[s], e.C4[s], e.eTt[s], e.eTr[s], e.eTb[s], e.eTl[s], T[s],
+                                  Sx)
+        e_or -= FT["hx"] * (v1 / n1).real
+    e_or /= 4
+    # density simple update on the CPU oracle: a sample of the same steps
+    Tn_o = [t.copy() for t in T]
+    lam = [[np.ones(FT["D"]) for _ in range(4)] for _ in range(4)]
+
+    class Up:
+        def __init__(self, s, l, o):
+            self.source_site, self.source_leg, self.op = s, l, o
+
+        def is_onesite(self):
+            return self.source_leg < 0
+    ups = [Up(s, l, o) for (s, l, o) in step]
+    n_cpu = 5
+    t1 = time.perf_counter()
+    for _ in range(n_cpu):
+        for up in ups:
+            Dn.su_density(Tn_o, lam, lat, up, p)
+    su_cpu = n_cpu / (time.perf_counter() - t1)
+    # the reference's own FT_TFI_square input end to end, GPU front end and the oracle driver
+    import shutil
+    import tenes_b200.itps as itps
+    from tests import _ft  # noqa: F401 -- the oracle's driver loop
+    with tempfile.TemporaryDirectory() as td:
+        shutil.copyfile(os.path.join(ROOT, "tests", "golden", "ft_tfi_square_input.toml"),
+                        os.path.join(td, "in.toml"))
+        t1 = time.perf_counter()
+        itps.run(os.path.join(td, "in.toml"), print_level=0, outdir=os.path.join(td, "out"))
+        run_gpu = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    _ft.run("ft_tfi_square", lambda beta, inp, lat_, p_, one, two, multi, Tn: _ft.measure(inp, lat_, p_, one, two,
+                                                                                            multi, Tn))
+    run_cpu = time.perf_counter() - t1
+    med = float(np.median(times))
+    return {"metric": "itpo_ctmrg_sweeps_per_s", "value": 1e3 / med, "unit": "sweeps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": med, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the density operator after the seeded finite-temperature simple update)",
+            "config": {"workload": f"itpo_tfi_square_2x2_D{FT['D']}_chi{FT['chi']}_beta{2 * FT['tau'] * FT['su_steps']:g}",
+                       "projector": "full SVD corner (reference default)",
+                       "l2": "flushed between timed sweeps (256 MB write outside the timed window)"},
+            "sweep_ms": [round(t, 3) for t in times], "gpu_launches": int(launches),
+            "cpu_baseline": {"value": 1.0 / sw[0], "unit": "sweeps/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "the first of the oracle's single-layer sweeps from the same tensors"},
+            "energy_per_site": e_gpu, "oracle_energy_per_site": e_or, "abs_delta_e": abs(e_gpu - e_or),
+            "sweeps_compared": n_sw,
+            "density_simple_update": {"gpu_steps_per_s": FT["su_steps"] / su_s, "cpu_oracle_steps_per_s": su_cpu,
+                                      "step": "8 bond + 4 one-site density updates (kron(op, conj(op)))"},
+            "ft_tfi_square_run": {"gpu_seconds": run_gpu, "cpu_oracle_seconds": run_cpu,
+                                  "what": "the reference's FT_TFI_square input: 500 density simple-update steps "
+                                          "and 6 measurements (CTMRG chi=10, observables, correlations, "
+                                          "correlation length)"}}
+
+
 def run_gemm(spec):
     """One contraction kernel alone, through tg_bench_gemm: spec = M N K
     [layout] [prec] [iters]; layout 0: A row-major (M, K), B row-major (K, N);
@@ -1047,6 +1195,9 @@ def main():
                     help="gradient evaluations/s of the J1-J2 energy (D=3, chi=36) with the FD check")
     ap.add_argument("--grad-iters", type=int, default=GRAD["iterations"])
     ap.add_argument("--grad-fd", type=int, default=32, help="entries checked by central differences")
+    ap.add_argument("--ft", action="store_true",
+                    help="iTPO (finite temperature): single-layer CTMRG sweeps/s at D=8, chi=64, the density "
+                         "simple update and the FT_TFI_square run")
     ap.add_argument("--gemm", nargs="+", metavar="M N K [layout prec iters]",
                     help="time one contraction kernel alone (tg_bench_gemm) and exit")
     args = ap.parse_args()
@@ -1056,6 +1207,9 @@ def main():
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.grad:
         print(json.dumps(run_grad(args)), flush=True)
+        return
+    if args.ft:
+        print(json.dumps(run_ft(args)), flush=True)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

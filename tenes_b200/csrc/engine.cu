@@ -872,86 +872,102 @@ struct EngineT final : Engine {
     PrecScope fp64(this, 0);
     const int w = static_cast<int>(std::min<int64_t>(P.chi, kmax));
     ++exact_solves;
-    DT<T> Om({b, ncol}, st);  // column-major ncol x b
-    int w0 = 0;
-    auto hit = warm_v.find(proj_key);
-    if (proj_key >= 0 && hit != warm_v.end() && hit->second.size() == static_cast<int64_t>(b) * ncol) {
-      w0 = w;
-      TG_CUDA(cudaMemcpyAsync(Om.p, hit->second.p, sizeof(T) * w0 * ncol, cudaMemcpyDeviceToDevice, st));
-    }
-    if (b > w0) counter_normal<T>(Om.p + static_cast<int64_t>(w0) * ncol, ncol, b - w0, P.rsvd_seed, 7, st);
-    DT<T> Q = mm_cm(m, cm(Om.p, ncol, b));  // nrow x b, column-major
-    int next_check = (w0 > 0 || b == kmax) ? 1 : 3;
-    orth_chol(Q, nrow, b, next_check == 1 ? 4 : 2);
-    std::vector<double> hs(static_cast<size_t>(b)), hr(static_cast<size_t>(w));
-    int prev_it = 0;
-    double prev_ratio = 0.0;
-    for (int it = 1; it <= kExactMaxIters; ++it) {
-      ++exact_iters;
-      DT<T> Z = mm_cm(mh, cm(Q.p, nrow, b));  // M^H Q: ncol x b
-      if (it < next_check) {
-        orth_chol(Z, ncol, b, 2);
-        Q = mm_cm(m, cm(Z.p, ncol, b));
-        orth_chol(Q, nrow, b, it + 1 == next_check ? 4 : 2);
-        continue;
+    // Attempt 0 orthonormalises by shifted CholeskyQR.  A matrix of rank below
+    // the block (the padded environments of an iTPO, whose single-layer
+    // matrices are narrow) can leave a Gram matrix that no shift makes
+    // positive: the solve then starts again with Householder QR, which
+    // yields orthonormal columns for any panel, before giving up for the
+    // dense SVD.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const bool householder = attempt == 1;
+      auto orth = [&](DT<T>& X, int64_t n, int passes) {
+        if (householder) orth_cm(X, n, b);
+        else orth_chol(X, n, b, passes);
+      };
+      DT<T> Om({b, ncol}, st);  // column-major ncol x b
+      int w0 = 0;
+      auto hit = warm_v.find(proj_key);
+      if (proj_key >= 0 && hit != warm_v.end() && hit->second.size() == static_cast<int64_t>(b) * ncol) {
+        w0 = w;
+        TG_CUDA(cudaMemcpyAsync(Om.p, hit->second.p, sizeof(T) * w0 * ncol, cudaMemcpyDeviceToDevice, st));
       }
-      ++exact_checks;
-      DT<T> Qz = clone(Z, st);
-      orth_chol(Qz, ncol, b, 4);
-      DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, b)), cm(Qz.p, ncol, b));  // Q^H M Qz (b x b row-major)
-      DT<T> Ur({b, b}, st), Wr({b, b}, st);
-      DT<double> s({b}, st);
-      jacobi_svd<T>(Tm.p, b, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
-      DT<T> Y = mm_cm(m, cm(Qz.p, ncol, b));        // M Qz: nrow x b
-      DT<T> MV1 = mm_cm(cm(Y.p, nrow, b), rm(Wr.p, b, b));  // M v_i
-      DT<T> U1 = mm_cm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // u_i
-      DT<double> r({w}, st);
-      ritz_residual<T>(MV1.p, U1.p, s.p, nrow, w, r.p, st);
-      int pivot_flag = 0;
-      TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * b, cudaMemcpyDeviceToHost, st));
-      TG_CUDA(cudaMemcpyAsync(hr.data(), r.p, sizeof(double) * w, cudaMemcpyDeviceToHost, st));
-      TG_CUDA(cudaMemcpyAsync(&pivot_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-      TG_CUDA(cudaStreamSynchronize(st));
-      if (pivot_flag) {  // an orthonormalisation met a non-positive pivot: the dense SVD instead
-        TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
-        break;
-      }
-      // the kept triplets: the truncation rule of ctm.cpp:277-288
-      int cut = w;
-      for (int i = 0; i < w; ++i)
-        if (!(hs[static_cast<size_t>(i)] > P.inverse_projector_cut * hs[0])) {
-          cut = i;
+      if (b > w0) counter_normal<T>(Om.p + static_cast<int64_t>(w0) * ncol, ncol, b - w0, P.rsvd_seed, 7, st);
+      DT<T> Q = mm_cm(m, cm(Om.p, ncol, b));  // nrow x b, column-major
+      int next_check = (w0 > 0 || b == kmax) ? 1 : 3;
+      orth(Q, nrow, next_check == 1 ? 4 : 2);
+      std::vector<double> hs(static_cast<size_t>(b)), hr(static_cast<size_t>(w));
+      int prev_it = 0;
+      double prev_ratio = 0.0;
+      bool pivot_failed = false;
+      for (int it = 1; it <= kExactMaxIters; ++it) {
+        ++exact_iters;
+        DT<T> Z = mm_cm(mh, cm(Q.p, nrow, b));  // M^H Q: ncol x b
+        if (it < next_check) {
+          orth(Z, ncol, 2);
+          Q = mm_cm(m, cm(Z.p, ncol, b));
+          orth(Q, nrow, it + 1 == next_check ? 4 : 2);
+          continue;
+        }
+        ++exact_checks;
+        DT<T> Qz = clone(Z, st);
+        orth(Qz, ncol, 4);
+        DT<T> Tm = mm_rm(ht(cm(Z.p, ncol, b)), cm(Qz.p, ncol, b));  // Q^H M Qz (b x b row-major)
+        DT<T> Ur({b, b}, st), Wr({b, b}, st);
+        DT<double> s({b}, st);
+        jacobi_svd<T>(Tm.p, b, Ur.p, s.p, Wr.p, st);  // T Wr = Ur S
+        DT<T> Y = mm_cm(m, cm(Qz.p, ncol, b));        // M Qz: nrow x b
+        DT<T> MV1 = mm_cm(cm(Y.p, nrow, b), rm(Wr.p, b, b));  // M v_i
+        DT<T> U1 = mm_cm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // u_i
+        DT<double> r({w}, st);
+        ritz_residual<T>(MV1.p, U1.p, s.p, nrow, w, r.p, st);
+        int pivot_flag = 0;
+        TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * b, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaMemcpyAsync(hr.data(), r.p, sizeof(double) * w, cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaMemcpyAsync(&pivot_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaStreamSynchronize(st));
+        if (pivot_flag) {  // an orthonormalisation met a non-positive pivot
+          TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+          pivot_failed = true;
           break;
         }
-      double worst = 0.0;
-      for (int i = 0; i < cut; ++i) worst = std::max(worst, hr[static_cast<size_t>(i)]);
-      const double ratio = hs[0] > 0.0 ? worst / (kExactTol * hs[0]) : 0.0;
-      if (ratio <= 1.0 || b == kmax) {
-        DT<T> U = mm_rm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // nrow x b row-major
-        DT<T> V = mm_rm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));  // ncol x b row-major
-        DT<double> sinv({w}, st);
-        truncation(s.p, b, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut + slot, st);
-        Uc = DT<T>({nrow, w}, st);
-        scale_cols<T>(U.p, b, nrow, w, sinv.p, false, Uc.p, st);
-        Vc = DT<T>({ncol, w}, st);
-        scale_cols<T>(V.p, b, ncol, w, sinv.p, false, Vc.p, st);
-        if (proj_key >= 0) warm_v[proj_key] = mm_cm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));
-        return true;
+        // the kept triplets: the truncation rule of ctm.cpp:277-288
+        int cut = w;
+        for (int i = 0; i < w; ++i)
+          if (!(hs[static_cast<size_t>(i)] > P.inverse_projector_cut * hs[0])) {
+            cut = i;
+            break;
+          }
+        double worst = 0.0;
+        for (int i = 0; i < cut; ++i) worst = std::max(worst, hr[static_cast<size_t>(i)]);
+        const double ratio = hs[0] > 0.0 ? worst / (kExactTol * hs[0]) : 0.0;
+        if (ratio <= 1.0 || b == kmax) {
+          DT<T> U = mm_rm(cm(Q.p, nrow, b), rm(Ur.p, b, b));   // nrow x b row-major
+          DT<T> V = mm_rm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));  // ncol x b row-major
+          DT<double> sinv({w}, st);
+          truncation(s.p, b, P.chi, P.inverse_projector_cut, sinv.p, w, d_cut + slot, st);
+          Uc = DT<T>({nrow, w}, st);
+          scale_cols<T>(U.p, b, nrow, w, sinv.p, false, Uc.p, st);
+          Vc = DT<T>({ncol, w}, st);
+          scale_cols<T>(V.p, b, ncol, w, sinv.p, false, Vc.p, st);
+          if (proj_key >= 0) warm_v[proj_key] = mm_cm(cm(Qz.p, ncol, b), rm(Wr.p, b, b));
+          return true;
+        }
+        // a stalled decay (a flat spectrum at the block edge): the dense SVD
+        if (prev_it > 0 && it > 12 && ratio > 0.5 * prev_ratio) break;
+        // iterations to the next check, from the decay seen between the last two
+        int gap = 3;
+        if (prev_it > 0 && ratio < prev_ratio) {
+          const double f = std::pow(ratio / prev_ratio, 1.0 / (it - prev_it));
+          gap = static_cast<int>(std::ceil(std::log(ratio) / -std::log(f)));
+          gap = std::min(16, std::max(1, gap));
+        }
+        prev_it = it;
+        prev_ratio = ratio;
+        next_check = it + gap;
+        Q = std::move(Y);
+        orth(Q, nrow, next_check == it + 1 ? 4 : 2);
       }
-      // a stalled decay (a flat spectrum at the block edge): the dense SVD
-      if (prev_it > 0 && it > 12 && ratio > 0.5 * prev_ratio) break;
-      // iterations to the next check, from the decay seen between the last two
-      int gap = 3;
-      if (prev_it > 0 && ratio < prev_ratio) {
-        const double f = std::pow(ratio / prev_ratio, 1.0 / (it - prev_it));
-        gap = static_cast<int>(std::ceil(std::log(ratio) / -std::log(f)));
-        gap = std::min(16, std::max(1, gap));
-      }
-      prev_it = it;
-      prev_ratio = ratio;
-      next_check = it + gap;
-      Q = std::move(Y);
-      orth_chol(Q, nrow, b, next_check == it + 1 ? 4 : 2);
+      if (!pivot_failed) break;
     }
     ++exact_dense;
     return false;

@@ -27,8 +27,10 @@
 namespace tg {
 namespace {
 
-constexpr int SU_THREADS = 256;
-constexpr int SU_WARPS = SU_THREADS / 32;
+// the block is SU_MAX_THREADS threads at most; the kernel runs with 256, 512 or
+// 1024 of them, enough half-warps for every column pair of a Jacobi round
+constexpr int SU_MAX_THREADS = 1024;
+constexpr int SU_MAX_WARPS = SU_MAX_THREADS / 32;
 constexpr int SU_MAX_SWEEPS = 40;
 
 __device__ __forceinline__ double cj(double x) { return x; }
@@ -76,14 +78,14 @@ __device__ __forceinline__ double half_sum(double v) {
 __device__ __forceinline__ double half_sum_t(double v) { return half_sum(v); }
 __device__ __forceinline__ cplx half_sum_t(cplx v) { return make_double2(half_sum(v.x), half_sum(v.y)); }
 
-// sum over the block, result returned to every thread (red: >= SU_WARPS doubles)
+// sum over the block, result returned to every thread (red: >= one double a warp)
 __device__ double block_sum(double v, double* red) {
   v = warp_sum(v);
   __syncthreads();
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
   double t = 0.0;
-  for (int w = 0; w < SU_WARPS; ++w) t += red[w];
+  for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += red[w];
   return t;
 }
 
@@ -97,7 +99,7 @@ __device__ void householder_qr(T* A, int m, int n, T* rdiag, double* uu, double*
   for (int j = 0; j < k; ++j) {
     T* x = A + static_cast<size_t>(j) * m;
     double part = 0.0;
-    for (int i = j + static_cast<int>(threadIdx.x); i < m; i += SU_THREADS) part += abs2(x[i]);
+    for (int i = j + static_cast<int>(threadIdx.x); i < m; i += static_cast<int>(blockDim.x)) part += abs2(x[i]);
     const double nrm2 = block_sum(part, red);
     const T x0 = x[j];
     const double xn = sqrt(nrm2), ax0 = sqrt(abs2(x0));
@@ -119,7 +121,7 @@ __device__ void householder_qr(T* A, int m, int n, T* rdiag, double* uu, double*
     }
     __syncthreads();
     const double f2 = 2.0 / uu[j];
-    for (int c = j + 1 + warp; c < n; c += SU_WARPS) {
+    for (int c = j + 1 + warp; c < n; c += static_cast<int>(blockDim.x >> 5)) {
       T* y = A + static_cast<size_t>(c) * m;
       T d = zero<T>();
       for (int i = j + lane; i < m; i += 32) d = add(d, mul(cj(x[i]), y[i]));
@@ -138,7 +140,7 @@ __device__ void apply_q(const T* A, int m, int k, const double* uu, T* Y, int ny
     if (uu[j] != 0.0) {
       const T* x = A + static_cast<size_t>(j) * m;
       const double f2 = 2.0 / uu[j];
-      for (int c = warp; c < ny; c += SU_WARPS) {
+      for (int c = warp; c < ny; c += static_cast<int>(blockDim.x >> 5)) {
         T* y = Y + static_cast<size_t>(c) * m;
         T d = zero<T>();
         for (int i = j + lane; i < m; i += 32) d = add(d, mul(cj(x[i]), y[i]));
@@ -196,11 +198,11 @@ __device__ __forceinline__ double outer_weight(const Side& s, const double* w, i
   return w[i0] * w[ld + i1] * w[2 * ld + i2];
 }
 
-template <typename T>
-__global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) {
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) su_bond_kernel(SuBondBatch batch) {
   const SuBondArgs& a = batch.a[blockIdx.x];
   extern __shared__ __align__(16) double smem_d[];
-  __shared__ double red[SU_WARPS];
+  __shared__ double red[SU_MAX_WARPS];
   __shared__ int rotated;
   Side s1, s2;
   make_side(a.dims1, a.connect1, s1);
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
   const int tid = threadIdx.x;
 
   // weights of the outer legs and their cut inverses (simple_update.cpp:63-81)
-  for (int q = tid; q < 3 * ld; q += SU_THREADS) {
+  for (int q = tid; q < 3 * ld; q += static_cast<int>(blockDim.x)) {
     const int leg = q / ld, j = q % ld;
     const double l1 = j < s1.d[s1.outer[leg]] ? a.lam[(a.site1 * 4 + s1.outer[leg]) * ld + j] : 0.0;
     const double l2 = j < s2.d[s2.outer[leg]] ? a.lam[(a.site2 * 4 + s2.outer[leg]) * ld + j] : 0.0;
@@ -241,14 +243,14 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
     w2[q] = l2;
     w2[3 * ld + q] = l2 > a.lambda_cut ? 1.0 / l2 : 0.0;
   }
-  for (int q = tid; q < d1 * d2 * d1 * d2; q += SU_THREADS) opl[q] = static_cast<const T*>(a.op)[q];
+  for (int q = tid; q < d1 * d2 * d1 * d2; q += static_cast<int>(blockDim.x)) opl[q] = static_cast<const T*>(a.op)[q];
   __syncthreads();
   // A = (outer | bond, physical) with the outer weights multiplied in, column-major
-  for (int q = tid; q < s1.m * s1.n; q += SU_THREADS) {
+  for (int q = tid; q < s1.m * s1.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s1.m, c = q / s1.m;
     A1[q] = scl(tn1[tensor_index(s1, r, c / d1, c % d1)], outer_weight(s1, w1, ld, r));
   }
-  for (int q = tid; q < s2.m * s2.n; q += SU_THREADS) {
+  for (int q = tid; q < s2.m * s2.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s2.m, c = q / s2.m;
     A2[q] = scl(tn2[tensor_index(s2, r, c / d2, c % d2)], outer_weight(s2, w2, ld, r));
   }
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
 
   // Theta[(c1, p1'), (c2, p2')] = sum_{b, p1, p2} R1[c1, (b, p1)] R2[c2, (b, p2)] op[p1, p2, p1', p2'],
   // stored as the Jacobi matrix (Theta, or Theta^H when it is wide), column-major
-  for (int q = tid; q < ar * acp; q += SU_THREADS) {
+  for (int q = tid; q < ar * acp; q += static_cast<int>(blockDim.x)) {
     const int i = q % ar, j = q / ar;
     T v = zero<T>();
     if (j < ac) {
@@ -276,7 +278,7 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
     }
     JA[q] = v;
   }
-  for (int q = tid; q < acp * acp; q += SU_THREADS) JV[q] = from_re<T>(q % acp == q / acp ? 1.0 : 0.0);
+  for (int q = tid; q < acp * acp; q += static_cast<int>(blockDim.x)) JV[q] = from_re<T>(q % acp == q / acp ? 1.0 : 0.0);
   __syncthreads();
 
   // one-sided Jacobi on the columns of JA (round-robin pairs, one half-warp a
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
     for (int rnd = 0; rnd < acp - 1; ++rnd) {
       // every half-warp runs the same number of passes, so that the shuffles
       // below always have their full half-warp
-      for (int base = 0; base < acp / 2; base += 2 * SU_WARPS) {
+      for (int base = 0; base < acp / 2; base += 2 * static_cast<int>(blockDim.x >> 5)) {
         const int pr = base + hw;
         const bool live = pr < acp / 2;
         // circle method: slot 0 fixed, slots 1..acp-1 rotate
@@ -346,14 +348,14 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
     return;
   }
   // singular values, descending (ties by column index)
-  for (int j = warp; j < acp; j += SU_WARPS) {
+  for (int j = warp; j < acp; j += static_cast<int>(blockDim.x >> 5)) {
     double v = 0.0;
     for (int i = lane; i < ar; i += 32) v += abs2(JA[static_cast<size_t>(j) * ar + i]);
     v = warp_sum(v);
     if (lane == 0) sig[j] = sqrt(v);
   }
   __syncthreads();
-  for (int j = tid; j < acp; j += SU_THREADS) {
+  for (int j = tid; j < acp; j += static_cast<int>(blockDim.x)) {
     int rank = 0;
     for (int i = 0; i < acp; ++i) rank += (sig[i] > sig[j] || (sig[i] == sig[j] && i < j)) ? 1 : 0;
     order[rank] = j;
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
   T* out1 = static_cast<T*>(a.tn1);
   T* out2 = static_cast<T*>(a.tn2);
   // new Tn1: Q1 [X1; 0], X1[c1, p1' dc + i] = U[(c1, p1'), i] lambda_c[i]  (Uc, simple_update.cpp:154, 157-175)
-  for (int q = tid; q < s1.m * s1.n; q += SU_THREADS) {
+  for (int q = tid; q < s1.m * s1.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s1.m, c = q / s1.m;
     T v = zero<T>();
     if (r < s1.k) {
@@ -393,14 +395,14 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
   }
   __syncthreads();
   apply_q(A1, s1.m, s1.k, uu1, Y, s1.n);
-  for (int q = tid; q < s1.m * s1.n; q += SU_THREADS) {
+  for (int q = tid; q < s1.m * s1.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s1.m, c = q / s1.m;
     const int p = c / dc, i = c % dc;
     out1[tensor_index(s1, r, i, p)] = scl(Y[q], outer_weight(s1, w1 + 3 * ld, ld, r));
   }
   __syncthreads();
   // new Tn2: Q2 [X2; 0], X2[c2, i d2 + p2'] = lambda_c[i] conj(V[(c2, p2'), i])  (VTc, :155, 177-197)
-  for (int q = tid; q < s2.m * s2.n; q += SU_THREADS) {
+  for (int q = tid; q < s2.m * s2.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s2.m, c = q / s2.m;
     T v = zero<T>();
     if (r < s2.k) {
@@ -411,12 +413,12 @@ __global__ void __launch_bounds__(SU_THREADS) su_bond_kernel(SuBondBatch batch) 
   }
   __syncthreads();
   apply_q(A2, s2.m, s2.k, uu2, Y, s2.n);
-  for (int q = tid; q < s2.m * s2.n; q += SU_THREADS) {
+  for (int q = tid; q < s2.m * s2.n; q += static_cast<int>(blockDim.x)) {
     const int r = q % s2.m, c = q / s2.m;
     const int i = c / d2, p = c % d2;
     out2[tensor_index(s2, r, i, p)] = scl(Y[q], outer_weight(s2, w2 + 3 * ld, ld, r));
   }
-  for (int i = tid; i < dc; i += SU_THREADS) {
+  for (int i = tid; i < dc; i += static_cast<int>(blockDim.x)) {
     a.lam[(a.site1 * 4 + s1.connect) * ld + i] = lc[i];
     a.lam[(a.site2 * 4 + s2.connect) * ld + i] = lc[i];
   }
@@ -431,6 +433,13 @@ HostSide host_side(const int* dims, int connect) {
     if (a != connect) s.m *= dims[a];
   s.k = std::min(s.m, s.n);
   return s;
+}
+
+// column pairs of one Jacobi round of the bond's Theta
+int su_pairs(const int* dims1, const int* dims2, int connect1) {
+  const HostSide s1 = host_side(dims1, connect1), s2 = host_side(dims2, (connect1 + 2) % 4);
+  const int ac = std::min(s1.k * dims1[4], s2.k * dims2[4]);
+  return (ac + (ac & 1)) / 2;
 }
 
 template <typename T>
@@ -471,9 +480,20 @@ void su_bonds_fused(const SuBondArgs* a, int n, cudaStream_t st) {
     smem = std::max(smem, su_smem_bytes<T>(a[b].dims1, a[b].dims2, a[b].connect1, a[b].lam_ld));
     batch.a[b] = a[b];
   }
-  ensure_dynamic_smem(reinterpret_cast<const void*>(su_bond_kernel<T>), smem);
+  // enough half-warps for all column pairs of a Jacobi round at once
+  int pairs = 0;
+  for (int b = 0; b < n; ++b) pairs = std::max(pairs, su_pairs(a[b].dims1, a[b].dims2, a[b].connect1));
   ProfScope ps(PK_SOLVER, st, 0.0, 0.0);
-  su_bond_kernel<T><<<n, SU_THREADS, smem, st>>>(batch);
+  if (pairs <= 16) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(su_bond_kernel<T, 256>), smem);
+    su_bond_kernel<T, 256><<<n, 256, smem, st>>>(batch);
+  } else if (pairs <= 32) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(su_bond_kernel<T, 512>), smem);
+    su_bond_kernel<T, 512><<<n, 512, smem, st>>>(batch);
+  } else {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(su_bond_kernel<T, SU_MAX_THREADS>), smem);
+    su_bond_kernel<T, SU_MAX_THREADS><<<n, SU_MAX_THREADS, smem, st>>>(batch);
+  }
   TG_CHECK_LAUNCH();
   count_launch();
 }
