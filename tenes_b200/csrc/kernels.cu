@@ -327,6 +327,124 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmParams<T> p) {
 }
 
 // ---------------------------------------------------------------------------
+// Narrow FP64 GEMM (real operands, 64 < N <= 96): one column tile of 8 NF columns
+// covers the whole of N, so N pads to the next multiple of 8 instead of 64
+// -- the rSVD panels (N = k = chi + 10, 82 at chi = 72) waste 7% of the
+// DMMAs instead of 36%.  CTA tile 64 x 8NF x 16, 4 warps of 16 rows x 8NF
+// (2 x NF m8n8k4 fragments each).  The tiles move global -> shared with
+// 8-byte cp.async (zero-filled outside the matrix) through a 3-stage ring,
+// one barrier per k tile, so no registers hold staged elements.
+// ---------------------------------------------------------------------------
+constexpr int NSTAGE = 3;
+
+__device__ __forceinline__ void cp_async8_zfill(double* dst, const double* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int n = valid ? 8 : 0;  // src-size 0: the 8 destination bytes are zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int NF>
+__global__ void __launch_bounds__(128) gemm_narrow_kernel(GemmParams<double> p) {
+  constexpr int BN = 8 * NF;
+  constexpr int LDB = BN + 4;  // LDB = 4 or 12 mod 16: conflict-free fragment reads
+  constexpr int ASZ = GBK * GLD, BSZ = GBK * LDB;
+  extern __shared__ double smem[];
+  double* As = smem;                 // [NSTAGE][GBK][GLD]
+  double* Bs = smem + NSTAGE * ASZ;  // [NSTAGE][GBK][LDB]
+  const GemmDesc& d = p.d;
+  const int64_t bz = blockIdx.z;
+  const double* A = p.A + bz * d.bA;
+  const double* B = p.B + bz * d.bB;
+  double* C = p.C + bz * d.bC;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * GBM;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wm = (tid >> 5) * 16;
+  const bool a_kc = (d.sAk == 1);
+  const bool b_nc = (d.sBn == 1);
+  const int64_t Kz = (d.klast > 0 && blockIdx.z == gridDim.z - 1) ? d.klast : d.K;
+  const int64_t nk = (Kz + GBK - 1) / GBK;
+
+  auto issue = [&](int64_t kt) {
+    if (kt < nk) {
+      const int64_t k0 = kt * GBK;
+      double* as = As + (kt % NSTAGE) * ASZ;
+      double* bs = Bs + (kt % NSTAGE) * BSZ;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int idx = tid + i * 128;
+        const int mm = a_kc ? idx / GBK : idx % GBM;
+        const int kk = a_kc ? idx % GBK : idx / GBM;
+        const int64_t gm = m0 + mm, gk = k0 + kk;
+        const bool ok = gm < d.M && gk < Kz;
+        cp_async8_zfill(as + kk * GLD + mm, ok ? A + gm * d.sAm + gk * d.sAk : A, ok);
+      }
+#pragma unroll
+      for (int i = 0; i < NF; ++i) {
+        const int idx = tid + i * 128;
+        const int nn = b_nc ? idx % BN : idx / GBK;
+        const int kb = b_nc ? idx / BN : idx % GBK;
+        const int64_t gk = k0 + kb;
+        const bool ok = nn < d.N && gk < Kz;
+        cp_async8_zfill(bs + kb * LDB + nn, ok ? B + gk * d.sBk + nn * d.sBn : B, ok);
+      }
+    }
+    cp_async_commit();  // an empty group past the last tile keeps the group count uniform
+  };
+
+  double acc[2][NF][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+  for (int s0 = 0; s0 < NSTAGE - 1; ++s0) issue(s0);
+  for (int64_t kt = 0; kt < nk; ++kt) {
+    cp_async_wait<NSTAGE - 2>();  // this thread's copies of tile kt have landed
+    __syncthreads();              // ... everyone's; and tile kt-1's stage is free again
+    issue(kt + NSTAGE - 1);
+    const double* as = As + (kt % NSTAGE) * ASZ;
+    const double* bs = Bs + (kt % NSTAGE) * BSZ;
+#pragma unroll
+    for (int k4 = 0; k4 < GBK; k4 += 4) {
+      const int kr = k4 + (lane & 3);
+      double a[2], b[NF];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) a[i] = as[kr * GLD + wm + i * 8 + (lane >> 2)];
+#pragma unroll
+      for (int j = 0; j < NF; ++j) b[j] = bs[kr * LDB + j * 8 + (lane >> 2)];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < NF; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t gm = m0 + wm + i * 8 + (lane >> 2);
+        const int64_t gn = j * 8 + 2 * (lane & 3) + h;
+        if (gm < d.M && gn < d.N) {
+          double* c = C + gm * d.sCm + gn * d.sCn;
+          double v = acc[i][j][h];
+          if (d.accumulate) v += *c;
+          *c = v;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
 // Mixed precision: 3xTF32 product on the 5th-generation tensor cores
 // (tcgen05.mma kind::tf32, accumulator in tensor memory).
 //
@@ -2017,6 +2135,34 @@ bool tc_fault_take() {
   return f != 0;
 }
 
+// Column-tile width of the narrow FP64 product for this shape, in fragments
+// of 8 columns, or 0 for the 64 x 64 tile: real FP64 products with
+// 64 < N <= 96, which two 64-wide tiles pad by 33-100%.  (At N <= 64 the
+// narrow tile saved nothing measurable: 16.5 us either way at 20000 x 36 x
+// 72, and 20.6 against 18.6 us at 1024 x 42 x 1024, whose short split-K
+// chunks favour register staging.)
+template <typename T>
+int narrow_nf(const GemmDesc& d) {
+  if (is_cplx<T>::value || d.prec != 0 || d.N <= GBN || d.N > 96) return 0;
+  return static_cast<int>((d.N + 7) / 8);
+}
+
+template <int NF>
+void launch_narrow_nf(dim3 gr, size_t smem, cudaStream_t st, const GemmParams<double>& gp) {
+  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_narrow_kernel<NF>), smem);
+  gemm_narrow_kernel<NF><<<gr, 128, smem, st>>>(gp);
+}
+
+void launch_narrow(int nf, dim3 gr, size_t smem, cudaStream_t st, const GemmParams<double>& gp) {
+  switch (nf) {
+    case 9: launch_narrow_nf<9>(gr, smem, st, gp); break;
+    case 10: launch_narrow_nf<10>(gr, smem, st, gp); break;
+    case 11: launch_narrow_nf<11>(gr, smem, st, gp); break;
+    case 12: launch_narrow_nf<12>(gr, smem, st, gp); break;
+    default: fail(TG_E_RUNTIME, "gemm: no narrow tile of " + std::to_string(nf) + " fragments");
+  }
+}
+
 template <typename T>
 void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return;
@@ -2026,8 +2172,11 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
     if (gemm_skinny(A, B, C, d, st)) return;
   }
   constexpr int NP = CPLX ? 2 : 1;
-  const size_t smem = sizeof(double) * 2 * 2 * NP * GBK * GLD;
-  ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, CPLX>), smem);
+  // the narrow tile (one column tile of 8 nf columns) where N pads to fewer columns than 64-wide tiles
+  const int nf = narrow_nf<T>(d);
+  const size_t smem = nf > 0 ? sizeof(double) * NSTAGE * GBK * (GLD + 8 * nf + 4)
+                             : sizeof(double) * 2 * 2 * NP * GBK * GLD;
+  if (nf == 0) ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_kernel<T, CPLX>), smem);
   if (d.batch > 65535) fail(TG_E_INPUT, "gemm: batch too large");
   // products taller than the grid's 65535 row tiles run as row chunks
   constexpr int64_t kRowsPerLaunch = int64_t(65535) * GBM;
@@ -2039,8 +2188,8 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
     }
     return;
   }
-  dim3 grid(static_cast<unsigned>((d.N + GBN - 1) / GBN), static_cast<unsigned>((d.M + GBM - 1) / GBM),
-            static_cast<unsigned>(d.batch));
+  dim3 grid(nf > 0 ? 1u : static_cast<unsigned>((d.N + GBN - 1) / GBN),
+            static_cast<unsigned>((d.M + GBM - 1) / GBM), static_cast<unsigned>(d.batch));
   const double macs = static_cast<double>(d.M) * d.N * d.K * d.batch;
   ProfScope ps(d.prec == 1 ? PK_GEMM_TC : PK_GEMM, st, (CPLX ? 8.0 : 2.0) * macs,
                sizeof(T) * static_cast<double>(d.batch) * (d.M * d.K + d.K * d.N + d.M * d.N));
@@ -2054,7 +2203,15 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
       return;
     }
   }
-  auto launch = [&](dim3 gr, const GemmParams<T>& gp) { gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp); };
+  auto launch = [&](dim3 gr, const GemmParams<T>& gp) {
+    if constexpr (!CPLX) {
+      if (nf > 0) {
+        launch_narrow(nf, gr, smem, st, gp);
+        return;
+      }
+    }
+    gemm_kernel<T, CPLX><<<gr, 128, smem, st>>>(gp);
+  };
   const int64_t tiles = static_cast<int64_t>(grid.x) * grid.y * grid.z;
   int64_t split = 1;
   // up to two CTAs per SM (the kernel's occupancy), K chunks of at least 128

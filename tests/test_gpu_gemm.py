@@ -32,8 +32,10 @@ SHAPES = [(128, 128, 16), (200, 37, 100), (36, 1000, 72), (1000, 36, 72), (2592,
           # one side <= 96 and the other >= 2048: the streaming kernel for long operands
           (36, 5000, 72), (5000, 72, 36), (72, 4100, 35), (4099, 17, 96), (96, 4096, 1), (5, 6000, 3),
           (2592, 82, 82), (72, 2592, 72), (2048, 96, 96),
-          # FP64: a 96-wide column tile where it pads N less than 64-wide ones, with and without split-K
-          (300, 90, 500), (700, 95, 16), (1500, 72, 200), (4000, 72, 64), (130, 250, 2000)]
+          # FP64: one narrow column tile (64 < N <= 96, a multiple of 8 columns), with and without
+          # split-K; N <= 64 stays on 64-wide tiles
+          (300, 90, 500), (700, 95, 16), (1500, 72, 200), (4000, 72, 64), (130, 250, 2000),
+          (500, 36, 700), (3000, 20, 300), (257, 5, 1000), (129, 41, 2100), (64, 88, 3000), (2592, 82, 2600)]
 
 
 @pytest.mark.parametrize("M,N,K", SHAPES)
