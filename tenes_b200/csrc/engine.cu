@@ -46,7 +46,7 @@ struct EngineT final : Engine {
   tg_params P;
   int dev = 0;
   cudaStream_t st = nullptr;
-  cusolverDnHandle_t sol = nullptr;
+  cusolverDnHandle_t sol = nullptr;  // slot 0 (the main stream); see hsol()
 
   std::vector<DT<T>> Tn;
   std::vector<std::array<DT<T>, 3>> Trot;  // right (2,3,0,1,4), top (1,2,3,0,4), bottom (3,0,1,2,4)
@@ -85,11 +85,21 @@ struct EngineT final : Engine {
   int cur_row = -1;
   int slot = 0;  // 0: main stream, 1..kRowStreams: row streams
 
+  // cuSOLVER handles, one per stream slot (created on first use), so that
+  // rows factorising on their own streams share no handle state
+  cusolverDnHandle_t sol_slot[kRowStreams + 1] = {};
+  cusolverDnHandle_t hsol() {
+    cusolverDnHandle_t& h = sol_slot[slot];
+    if (!h) check_sol(cusolverDnCreate(&h), "cusolverDnCreate");
+    check_sol(cusolverDnSetStream(h, st), "cusolverDnSetStream");
+    return h;
+  }
+
   unsigned long long* d_max = nullptr;  // one per stream slot
   static constexpr int kInfoSlots = 4096;
   int* d_info = nullptr;  // one slot per cuSOLVER call, checked at sync points
   int info_used = 0;
-  int* d_flag = nullptr;  // set by device kernels on a numerical failure
+  int* d_flag = nullptr;  // one per stream slot: set by device kernels on a numerical failure
   uint64_t noise_stream = 0;  // key sequence of the orthonormalisation perturbations
   int* d_cut = nullptr;
   // Simple-update weights on the device, [(site * 4 + leg) * lam_ld + j]: the
@@ -135,6 +145,7 @@ struct EngineT final : Engine {
     TG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     check_sol(cusolverDnCreate(&sol), "cusolverDnCreate");
     check_sol(cusolverDnSetStream(sol, st), "cusolverDnSetStream");
+    sol_slot[0] = sol;
     main_st = st;
     for (int r = 0; r < kRowStreams; ++r) {
       TG_CUDA(cudaStreamCreateWithFlags(&row_st[r], cudaStreamNonBlocking));
@@ -145,8 +156,8 @@ struct EngineT final : Engine {
     TG_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long) * (kRowStreams + 1)));
     TG_CUDA(cudaMalloc(&d_info, sizeof(int) * kInfoSlots));
     TG_CUDA(cudaMemset(d_info, 0, sizeof(int) * kInfoSlots));
-    TG_CUDA(cudaMalloc(&d_flag, sizeof(int)));
-    TG_CUDA(cudaMemset(d_flag, 0, sizeof(int)));
+    TG_CUDA(cudaMalloc(&d_flag, sizeof(int) * (kRowStreams + 1)));
+    TG_CUDA(cudaMemset(d_flag, 0, sizeof(int) * (kRowStreams + 1)));
     TG_CUDA(cudaMalloc(&d_cut, sizeof(int) * (kRowStreams + 1)));
     for (int i = 0; i < lat.N; ++i)
       for (int l = 0; l < 4; ++l) lam_ld = std::max(lam_ld, lat.vdim[i][l]);
@@ -210,6 +221,8 @@ struct EngineT final : Engine {
     if (st) cudaStreamSynchronize(st);
     cudaDeviceGraphMemTrim(dev);
     if (gj_params) cusolverDnDestroyGesvdjInfo(gj_params);
+    for (int r = 1; r <= kRowStreams; ++r)
+      if (sol_slot[r]) cusolverDnDestroy(sol_slot[r]);
     if (sol) cusolverDnDestroy(sol);
     cudaFree(d_max);
     cudaFree(d_info);
@@ -308,7 +321,11 @@ struct EngineT final : Engine {
     for (auto& t : v)
       if (t.mem) t.mem->st = st;
   }
-  bool rows_parallel() const { return graph_capable(); }
+  // Rows run on their own streams except under the per-kernel profiler,
+  // whose attribution wants one launch at a time.  (Rows with full-SVD
+  // projectors synchronise with the host at every residual check, so they
+  // overlap only with the rows that follow them.)
+  bool rows_parallel() const { return !profile_enabled(); }
 
   void upload(DT<T>& t, const double* host) {
     TG_CUDA(cudaMemcpyAsync(t.p, host, sizeof(T) * t.size(), cudaMemcpyHostToDevice, st));
@@ -408,18 +425,18 @@ struct EngineT final : Engine {
     DT<T> VTb({k, k}, st);  // VT_B: k x k column-major == U_A row-major (m x k)
     int lwork = 0;
     if constexpr (CPLX) {
-      check_sol(cusolverDnZgesvd_bufferSize(sol, rows, cols, &lwork), "Zgesvd_bufferSize");
+      check_sol(cusolverDnZgesvd_bufferSize(hsol(), rows, cols, &lwork), "Zgesvd_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
       DT<double> rwork({std::max<int64_t>(5 * k, 1)}, st);
-      check_sol(cusolverDnZgesvd(sol, 'S', 'S', rows, cols, reinterpret_cast<cuDoubleComplex*>(A.p), rows, s.p,
+      check_sol(cusolverDnZgesvd(hsol(), 'S', 'S', rows, cols, reinterpret_cast<cuDoubleComplex*>(A.p), rows, s.p,
                                  reinterpret_cast<cuDoubleComplex*>(Ub.p), rows,
                                  reinterpret_cast<cuDoubleComplex*>(VTb.p), cols,
                                  reinterpret_cast<cuDoubleComplex*>(work.p), lwork, rwork.p, info_slot()),
                 "Zgesvd");
     } else {
-      check_sol(cusolverDnDgesvd_bufferSize(sol, rows, cols, &lwork), "Dgesvd_bufferSize");
+      check_sol(cusolverDnDgesvd_bufferSize(hsol(), rows, cols, &lwork), "Dgesvd_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
-      check_sol(cusolverDnDgesvd(sol, 'S', 'S', rows, cols, A.p, rows, s.p, Ub.p, rows, VTb.p, cols, work.p,
+      check_sol(cusolverDnDgesvd(hsol(), 'S', 'S', rows, cols, A.p, rows, s.p, Ub.p, rows, VTb.p, cols, work.p,
                                  lwork, nullptr, info_slot()),
                 "Dgesvd");
     }
@@ -455,11 +472,11 @@ struct EngineT final : Engine {
       DT<T> Ub({k, n}, st);  // U' (n x k column-major) = VT (k x n row-major)
       DT<T> Vb({k, m}, st);  // V' (m x k column-major) = U^T (k x m row-major)
       int lwork = 0;
-      check_sol(cusolverDnDgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p,
+      check_sol(cusolverDnDgesvdj_bufferSize(hsol(), CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p,
                                              rows, Vb.p, cols, &lwork, gj_params),
                 "Dgesvdj_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
-      check_sol(cusolverDnDgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p, rows, Vb.p,
+      check_sol(cusolverDnDgesvdj(hsol(), CUSOLVER_EIG_MODE_VECTOR, 1, rows, cols, A.p, rows, s.p, Ub.p, rows, Vb.p,
                                   cols, work.p, lwork, info_slot(), gj_params),
                 "Dgesvdj");
       VT = reshape(Ub, {k, n});
@@ -474,11 +491,13 @@ struct EngineT final : Engine {
   // Every cuSOLVER call reports into its own device slot; a non-zero value
   // (illegal argument or non-convergence) is turned into an error here.
   void check_infos() {
-    int flag = 0;
-    TG_CUDA(cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int flags[kRowStreams + 1] = {};
+    TG_CUDA(cudaMemcpyAsync(flags, d_flag, sizeof(flags), cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
+    int flag = 0;
+    for (int f : flags) flag |= f;
     if (flag) {
-      TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+      TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(flags), st));
       fail(TG_E_RUNTIME, "CholeskyQR orthonormalisation met a non-positive pivot (rank-deficient panel)");
     }
     TG_CUDA(cudaMemcpyAsync(&flag, d_su_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -514,23 +533,23 @@ struct EngineT final : Engine {
     if constexpr (CPLX) {
       auto* a = reinterpret_cast<cuDoubleComplex*>(Ac.p);
       auto* t = reinterpret_cast<cuDoubleComplex*>(tau.p);
-      check_sol(cusolverDnZgeqrf_bufferSize(sol, im, in, a, im, &lwork), "Zgeqrf_bufferSize");
-      check_sol(cusolverDnZungqr_bufferSize(sol, im, ik, ik, a, im, t, &lwork2), "Zungqr_bufferSize");
+      check_sol(cusolverDnZgeqrf_bufferSize(hsol(), im, in, a, im, &lwork), "Zgeqrf_bufferSize");
+      check_sol(cusolverDnZungqr_bufferSize(hsol(), im, ik, ik, a, im, t, &lwork2), "Zungqr_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
       auto* w = reinterpret_cast<cuDoubleComplex*>(work.p);
-      check_sol(cusolverDnZgeqrf(sol, im, in, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zgeqrf");
+      check_sol(cusolverDnZgeqrf(hsol(), im, in, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zgeqrf");
       // R: upper k x n of the factored matrix (column-major (m, n))
       R = DT<T>({n, k}, st);  // fill as row-major (n, k) == column-major (k, n)
       extract_r(Ac, m, n, k, R);
-      check_sol(cusolverDnZungqr(sol, im, ik, ik, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zungqr");
+      check_sol(cusolverDnZungqr(hsol(), im, ik, ik, a, im, t, w, std::max(lwork, lwork2), info_slot()), "Zungqr");
     } else {
-      check_sol(cusolverDnDgeqrf_bufferSize(sol, im, in, Ac.p, im, &lwork), "Dgeqrf_bufferSize");
-      check_sol(cusolverDnDorgqr_bufferSize(sol, im, ik, ik, Ac.p, im, tau.p, &lwork2), "Dorgqr_bufferSize");
+      check_sol(cusolverDnDgeqrf_bufferSize(hsol(), im, in, Ac.p, im, &lwork), "Dgeqrf_bufferSize");
+      check_sol(cusolverDnDorgqr_bufferSize(hsol(), im, ik, ik, Ac.p, im, tau.p, &lwork2), "Dorgqr_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(std::max(lwork, lwork2), 1))}, st);
-      check_sol(cusolverDnDgeqrf(sol, im, in, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()), "Dgeqrf");
+      check_sol(cusolverDnDgeqrf(hsol(), im, in, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()), "Dgeqrf");
       R = DT<T>({n, k}, st);
       extract_r(Ac, m, n, k, R);
-      check_sol(cusolverDnDorgqr(sol, im, ik, ik, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()),
+      check_sol(cusolverDnDorgqr(hsol(), im, ik, ik, Ac.p, im, tau.p, work.p, std::max(lwork, lwork2), info_slot()),
                 "Dorgqr");
     }
     // Q: first k columns of the column-major (m, *) buffer -> row-major (m, k)
@@ -641,15 +660,15 @@ struct EngineT final : Engine {
     ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 2.0 * n * k * k, 0.0);
     if constexpr (CPLX) {
       auto* a = reinterpret_cast<cuDoubleComplex*>(Y.p);
-      check_sol(cusolverDnZgeqrf_bufferSize(sol, in, ik, a, in, &lwork), "Zgeqrf_bufferSize");
+      check_sol(cusolverDnZgeqrf_bufferSize(hsol(), in, ik, a, in, &lwork), "Zgeqrf_bufferSize");
       DT<T> work({std::max<int64_t>(lwork, 1)}, st);
-      check_sol(cusolverDnZgeqrf(sol, in, ik, a, in, reinterpret_cast<cuDoubleComplex*>(tau.p),
+      check_sol(cusolverDnZgeqrf(hsol(), in, ik, a, in, reinterpret_cast<cuDoubleComplex*>(tau.p),
                                  reinterpret_cast<cuDoubleComplex*>(work.p), lwork, info_slot()),
                 "Zgeqrf");
     } else {
-      check_sol(cusolverDnDgeqrf_bufferSize(sol, in, ik, Y.p, in, &lwork), "Dgeqrf_bufferSize");
+      check_sol(cusolverDnDgeqrf_bufferSize(hsol(), in, ik, Y.p, in, &lwork), "Dgeqrf_bufferSize");
       DT<T> work({std::max<int64_t>(lwork, 1)}, st);
-      check_sol(cusolverDnDgeqrf(sol, in, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dgeqrf");
+      check_sol(cusolverDnDgeqrf(hsol(), in, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dgeqrf");
     }
     return tau;
   }
@@ -661,15 +680,15 @@ struct EngineT final : Engine {
     if constexpr (CPLX) {
       auto* a = reinterpret_cast<cuDoubleComplex*>(Y.p);
       auto* t = reinterpret_cast<const cuDoubleComplex*>(tau.p);
-      check_sol(cusolverDnZungqr_bufferSize(sol, in, ik, ik, a, in, t, &lwork), "Zungqr_bufferSize");
+      check_sol(cusolverDnZungqr_bufferSize(hsol(), in, ik, ik, a, in, t, &lwork), "Zungqr_bufferSize");
       DT<T> work({std::max<int64_t>(lwork, 1)}, st);
-      check_sol(cusolverDnZungqr(sol, in, ik, ik, a, in, t, reinterpret_cast<cuDoubleComplex*>(work.p), lwork,
+      check_sol(cusolverDnZungqr(hsol(), in, ik, ik, a, in, t, reinterpret_cast<cuDoubleComplex*>(work.p), lwork,
                                  info_slot()),
                 "Zungqr");
     } else {
-      check_sol(cusolverDnDorgqr_bufferSize(sol, in, ik, ik, Y.p, in, tau.p, &lwork), "Dorgqr_bufferSize");
+      check_sol(cusolverDnDorgqr_bufferSize(hsol(), in, ik, ik, Y.p, in, tau.p, &lwork), "Dorgqr_bufferSize");
       DT<T> work({std::max<int64_t>(lwork, 1)}, st);
-      check_sol(cusolverDnDorgqr(sol, in, ik, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dorgqr");
+      check_sol(cusolverDnDorgqr(hsol(), in, ik, ik, Y.p, in, tau.p, work.p, lwork, info_slot()), "Dorgqr");
     }
   }
   void orth_cm(DT<T>& Y, int64_t n, int64_t k) {
@@ -739,7 +758,7 @@ struct EngineT final : Engine {
       if (cholqr_cluster_supported(n, k)) {
         DT<double> scratch({cholqr_scratch_doubles(k)}, st);
         cholqr_cluster(Y.p, n, k, passes, 2, ++noise_stream, 1e-14 / std::sqrt(static_cast<double>(n)), scratch.p,
-                       d_flag, st);
+                       d_flag + slot, st);
         return;
       }
     }
@@ -749,7 +768,7 @@ struct EngineT final : Engine {
       DT<T> G({k, k}, st);
       sum_partials<T>(parts.p, nparts, k * k, G.p, st);
       DT<T> Ri({k, k}, st);
-      chol_rinv<T>(G.p, 1, k, n, pass <= 1 ? 1 : 0, Ri.p, d_flag, st);
+      chol_rinv<T>(G.p, 1, k, n, pass <= 1 ? 1 : 0, Ri.p, d_flag + slot, st);
       Y = mm_cm(cm(Y.p, n, k), rm(Ri.p, k, k));
       if (pass == 0) add_noise<T>(Y.p, n * k, 1e-14 / std::sqrt(static_cast<double>(n)), ++noise_stream, st);
     }
@@ -923,10 +942,10 @@ struct EngineT final : Engine {
         int pivot_flag = 0;
         TG_CUDA(cudaMemcpyAsync(hs.data(), s.p, sizeof(double) * b, cudaMemcpyDeviceToHost, st));
         TG_CUDA(cudaMemcpyAsync(hr.data(), r.p, sizeof(double) * w, cudaMemcpyDeviceToHost, st));
-        TG_CUDA(cudaMemcpyAsync(&pivot_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TG_CUDA(cudaMemcpyAsync(&pivot_flag, d_flag + slot, sizeof(int), cudaMemcpyDeviceToHost, st));
         TG_CUDA(cudaStreamSynchronize(st));
         if (pivot_flag) {  // an orthonormalisation met a non-positive pivot
-          TG_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), st));
+          TG_CUDA(cudaMemsetAsync(d_flag + slot, 0, sizeof(int), st));
           pivot_failed = true;
           break;
         }
@@ -2091,14 +2110,14 @@ struct EngineT final : Engine {
     check_sol(cusolverDnCreateParams(&prm), "cusolverDnCreateParams");
     size_t dws = 0, hws = 0;
     const cusolverEigMode_t jr = vr_last ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
-    check_sol(cusolverDnXgeev_bufferSize(sol, prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F,
+    check_sol(cusolverDnXgeev_bufferSize(hsol(), prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F,
                                          W.p, CUDA_C_64F, nullptr, 1, CUDA_C_64F, VR.p, vr_last ? n : 1,
                                          CUDA_C_64F, &dws, &hws),
               "Xgeev_bufferSize");
     DT<unsigned char> dw({static_cast<int64_t>(std::max<size_t>(dws, 1))}, st);
     std::vector<unsigned char> hw(std::max<size_t>(hws, 1));
     ProfScope ps(PK_SOLVER, st, 10.0 * n * n * n, 0.0);
-    check_sol(cusolverDnXgeev(sol, prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F, W.p,
+    check_sol(cusolverDnXgeev(hsol(), prm, CUSOLVER_EIG_MODE_NOVECTOR, jr, n, CUDA_C_64F, A.p, n, CUDA_C_64F, W.p,
                               CUDA_C_64F, nullptr, 1, CUDA_C_64F, VR.p, vr_last ? n : 1, CUDA_C_64F, dw.p, dws,
                               hw.data(), hws, info_slot()),
               "Xgeev");
@@ -2358,13 +2377,13 @@ struct EngineT final : Engine {
     auto* ap = reinterpret_cast<cuDoubleComplex*>(A.p);
     auto* tp = reinterpret_cast<cuDoubleComplex*>(tau.p);
     const int ik = static_cast<int>(k);
-    check_sol(cusolverDnZgeqrf_bufferSize(sol, ik, ik, ap, ik, &lw1), "Zgeqrf_bufferSize");
-    check_sol(cusolverDnZungqr_bufferSize(sol, ik, ik, ik, ap, ik, tp, &lw2), "Zungqr_bufferSize");
+    check_sol(cusolverDnZgeqrf_bufferSize(hsol(), ik, ik, ap, ik, &lw1), "Zgeqrf_bufferSize");
+    check_sol(cusolverDnZungqr_bufferSize(hsol(), ik, ik, ik, ap, ik, tp, &lw2), "Zungqr_bufferSize");
     const int lw = std::max(std::max(lw1, lw2), 1);
     DT<cplx> work({lw}, st);
     auto* wp = reinterpret_cast<cuDoubleComplex*>(work.p);
-    check_sol(cusolverDnZgeqrf(sol, ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zgeqrf");
-    check_sol(cusolverDnZungqr(sol, ik, ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zungqr");
+    check_sol(cusolverDnZgeqrf(hsol(), ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zgeqrf");
+    check_sol(cusolverDnZungqr(hsol(), ik, ik, ik, ap, ik, tp, wp, lw, info_slot()), "Zungqr");
     TG_CUDA(cudaMemcpyAsync(a.data(), A.p, sizeof(cplx) * k * k, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaStreamSynchronize(st));
     check_infos();
@@ -2808,20 +2827,20 @@ struct EngineT final : Engine {
     ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 9.0 * static_cast<double>(n) * n * n, 0.0);
     if constexpr (CPLX) {
       auto* ap = reinterpret_cast<cuDoubleComplex*>(a.p);
-      check_sol(cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
+      check_sol(cusolverDnZheevd_bufferSize(hsol(), CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
                                             &lwork),
                 "Zheevd_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
-      check_sol(cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
+      check_sol(cusolverDnZheevd(hsol(), CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, ap, in, wd.p,
                                  reinterpret_cast<cuDoubleComplex*>(work.p), lwork, info_slot()),
                 "Zheevd");
       Z = transpose<T>(reshape(a, {n, n}), {1, 0}, st, true);
     } else {
-      check_sol(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in,
+      check_sol(cusolverDnDsyevd_bufferSize(hsol(), CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in,
                                             wd.p, &lwork),
                 "Dsyevd_bufferSize");
       DT<T> work({static_cast<int64_t>(std::max(lwork, 1))}, st);
-      check_sol(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in, wd.p, work.p,
+      check_sol(cusolverDnDsyevd(hsol(), CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, in, a.p, in, wd.p, work.p,
                                  lwork, info_slot()),
                 "Dsyevd");
       Z = tr(reshape(a, {n, n}), {1, 0});
