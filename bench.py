@@ -517,12 +517,13 @@ def sweep_profile(env):
 
 
 def roofline_fp64(fam, peak_tflops, cfg):
-    """FP64 DMMA products (gemm_kernel, skinny_kernel): compute-bound at
-    intensity >> the FP64 ridge (~6 flop/B), so the roof is the measured DGEMM
-    rate."""
+    """FP64 DMMA products (gemm_kernel, gemm_narrow_kernel, gemm_group_kernel,
+    skinny_kernel): compute-bound at intensity >> the FP64 ridge (~6 flop/B),
+    so the roof is the measured DGEMM rate."""
     n_g, ms_g, fl_g, by_g = fam["gemm_dmma"]
     ach = fl_g / (ms_g * 1e-3) / 1e12 if ms_g > 0 else 0.0
-    return {"bound": "tensor", "kernel": "gemm_kernel + skinny_kernel (FP64 DMMA m8n8k4)",
+    return {"bound": "tensor", "kernel": "gemm_kernel + gemm_narrow_kernel + gemm_group_kernel + skinny_kernel "
+                                         "(FP64 DMMA m8n8k4)",
             "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s",
             "frac": ach / peak_tflops if peak_tflops else None,
             "peak_source": "measured in-run: cuBLAS DGEMM 8192^3 FP64 (MEASURED_PEAKS.json has no FP64 entry)",

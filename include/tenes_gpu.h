@@ -343,6 +343,22 @@ tg_status tg_profile_enable(int on);
 tg_status tg_profile_reset(void);
 tg_status tg_profile_query(int kind, uint64_t* launches, double* ms, double* flops, double* bytes);
 
+/* n independent products C_i = op(A_i) op(B_i) through the library's grouped
+ * persistent contraction kernel (the one a move's absorptions run as), with
+ * host buffers: A holds every A_i (M_i x K_i) back to back, B every B_i
+ * (K_i x N_i), C receives every C_i (M_i x N_i, row-major); mnk = (M_i, N_i,
+ * K_i) triples.  flags[i] (or all 0 if flags is NULL): bit 0 A_i stored
+ * column-major, bit 1 B_i stored column-major, bit 2 conj(A_i), bit 3
+ * conj(B_i) (complex only).  is_complex: elements are (re, im) pairs of
+ * doubles, the products run as 3M.  For tests of the kernels; not part of
+ * the CTMRG path. */
+tg_status tg_gemm_group_host(int n, const int64_t* mnk, const int* flags, int is_complex, const double* A,
+                             const double* B, double* C);
+/* The grouped kernel's tile autotuner so far (process-wide): the number of
+ * group shapes it has timed, and for each of the first nwins tile variants
+ * (0: 64-row tiles, 1: 32-row tiles) how many of them it chose. */
+tg_status tg_gemm_group_stats(int64_t* tuned, int64_t* wins, int nwins);
+
 /* Microbenchmark of the library's contraction kernel: average device time of
  * one M x N x K real product (prec 0: FP64 DMMA, 1: 3xTF32), B row-major
  * (layout 0) or column-major (layout 1).  Allocates its own buffers; not part

@@ -29,7 +29,7 @@ EXPORTED = [
     "tg_tm_eigenvalues", "tg_kernel_launch_count", "tg_ctx_stream",
     "tg_profile_enable", "tg_profile_reset", "tg_profile_query", "tg_corner_spectra_noalloc",
     "tg_bench_gemm", "tg_gemm_host", "tg_cholqr_host", "tg_energy_grad", "tg_measure_bond_rdm", "tg_fu_params_default", "tg_fu_bond", "tg_su_fix_gauge", "tg_measure_correlation",
-    "tg_projector_svd_stats", "tenes_gpu_main", "tg_su_bonds",
+    "tg_projector_svd_stats", "tenes_gpu_main", "tg_su_bonds", "tg_gemm_group_host", "tg_gemm_group_stats",
 ]
 
 
@@ -127,6 +127,8 @@ def load() -> C.CDLL:
         "tg_gemm_host": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, dp, C.c_int64, C.c_int64, dp, C.c_int64,
                                    C.c_int64, dp, C.c_int64, C.c_int64, C.c_int]),
         "tg_cholqr_host": (C.c_int, [C.c_int64, C.c_int64, dp, C.c_int, P(C.c_int)]),
+        "tg_gemm_group_host": (C.c_int, [C.c_int, P(C.c_int64), P(C.c_int), C.c_int, dp, dp, dp]),
+        "tg_gemm_group_stats": (C.c_int, [P(C.c_int64), P(C.c_int64), C.c_int]),
         "tg_energy_grad": (C.c_int, [vp, C.c_int, P(WindowTerm), C.c_int, C.c_int, C.c_double, dp, dp]),
     }
     for name, (res, args) in sig.items():

@@ -346,6 +346,66 @@ extern "C" tg_status tg_gemm_host(int64_t M, int64_t N, int64_t K, const double*
   });
 }
 
+extern "C" tg_status tg_gemm_group_host(int n, const int64_t* mnk, const int* flags, int is_complex,
+                                        const double* A, const double* B, double* C) {
+  return guard([&] {
+    if (n < 1 || !mnk || !A || !B || !C) tg::fail(TG_E_INPUT, "bad grouped gemm arguments");
+    const int64_t w = is_complex ? 2 : 1;  // doubles per element
+    std::vector<tg::GroupItem> items(static_cast<size_t>(n));
+    std::vector<int64_t> oa(static_cast<size_t>(n)), ob(oa), oc(oa);  // element offsets
+    int64_t na = 0, nb = 0, nc = 0;
+    for (int i = 0; i < n; ++i) {
+      const int64_t M = mnk[3 * i], N = mnk[3 * i + 1], K = mnk[3 * i + 2];
+      if (M < 1 || N < 1 || K < 1) tg::fail(TG_E_INPUT, "grouped gemm: every M, N, K must be positive");
+      const int f = flags ? flags[i] : 0;
+      if ((f & ~15) || (!is_complex && (f & 12))) tg::fail(TG_E_INPUT, "grouped gemm: bad flags");
+      tg::GroupItem& it = items[static_cast<size_t>(i)];
+      it.M = M;
+      it.N = N;
+      it.K = K;
+      it.sAm = (f & 1) ? 1 : K;
+      it.sAk = (f & 1) ? M : 1;
+      it.sBk = (f & 2) ? 1 : N;
+      it.sBn = (f & 2) ? K : 1;
+      it.sCm = N;
+      it.sCn = 1;
+      it.conjA = (f & 4) != 0;
+      it.conjB = (f & 8) != 0;
+      oa[static_cast<size_t>(i)] = na;
+      ob[static_cast<size_t>(i)] = nb;
+      oc[static_cast<size_t>(i)] = nc;
+      na += M * K;
+      nb += K * N;
+      nc += M * N;
+    }
+    cudaStream_t st;
+    TG_CUDA(cudaStreamCreate(&st));
+    double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    TG_CUDA(cudaMalloc(&dA, sizeof(double) * w * na));
+    TG_CUDA(cudaMalloc(&dB, sizeof(double) * w * nb));
+    TG_CUDA(cudaMalloc(&dC, sizeof(double) * w * nc));
+    TG_CUDA(cudaMemcpyAsync(dA, A, sizeof(double) * w * na, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(dB, B, sizeof(double) * w * nb, cudaMemcpyHostToDevice, st));
+    for (size_t i = 0; i < items.size(); ++i) {
+      items[i].A = dA + w * oa[i];
+      items[i].B = dB + w * ob[i];
+      items[i].C = dC + w * oc[i];
+    }
+    if (is_complex) tg::gemm_group<tg::cplx>(items.data(), n, st);
+    else tg::gemm_group<double>(items.data(), n, st);
+    TG_CUDA(cudaMemcpyAsync(C, dC, sizeof(double) * w * nc, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaStreamDestroy(st);
+  });
+}
+
+extern "C" tg_status tg_gemm_group_stats(int64_t* tuned, int64_t* wins, int nwins) {
+  return guard([&] { tg::gemm_group_stats(tuned, wins, nwins); });
+}
+
 extern "C" tg_status tg_cholqr_host(int64_t n, int64_t k, double* Y, int passes, int* pivot_flag) {
   return guard([&] {
     if (n < 1 || k < 1 || k > n || passes < 1 || !Y) tg::fail(TG_E_INPUT, "bad CholeskyQR arguments");

@@ -94,12 +94,19 @@ DT<T> reshape(const DT<T>& a, const Shape& s) {
   return t;
 }
 
-// tensordot(A, B, axA, axB): result legs = free legs of A (in order) then
-// free legs of B (in order).  conjA / conjB conjugate the operands.
+// A tensordot reduced to one matrix product: the operands as used (the
+// inputs themselves, or permuted copies where no strided matrix view
+// exists), the allocated result and the product's descriptor.
 template <typename T>
-DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
-                const std::vector<int>& axB, cudaStream_t st, bool conjA = false,
-                bool conjB = false, int prec = 0) {
+struct TdPlan {
+  DT<T> A, B, C;
+  GemmDesc g{};
+};
+
+template <typename T>
+TdPlan<T> plan_tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
+                         const std::vector<int>& axB, cudaStream_t st, bool conjA = false,
+                         bool conjB = false, int prec = 0) {
   if (axA.size() != axB.size()) fail(TG_E_INPUT, "tensordot: axes length mismatch");
   std::vector<int> freeA, freeB;
   for (int i = 0; i < A.rank(); ++i)
@@ -120,7 +127,8 @@ DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
     if (A.dim(axA[i]) != B.dim(axB[i])) fail(TG_E_INPUT, "tensordot: contracted dims differ");
     K *= A.dim(axA[i]);
   }
-  GemmDesc g{};
+  TdPlan<T> pl;
+  GemmDesc& g = pl.g;
   g.M = M;
   g.N = N;
   g.K = K;
@@ -130,7 +138,7 @@ DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
   g.accumulate = false;
   g.prec = prec;
   // A as (M, K) or (K, M)
-  DT<T> Ause = A;
+  pl.A = A;
   std::vector<int> pa(freeA);
   pa.insert(pa.end(), axA.begin(), axA.end());
   std::vector<int> pa2(axA);
@@ -142,11 +150,11 @@ DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
     g.sAm = 1;
     g.sAk = M;
   } else {
-    Ause = transpose(A, pa, st);
+    pl.A = transpose(A, pa, st);
     g.sAm = K;
     g.sAk = 1;
   }
-  DT<T> Buse = B;
+  pl.B = B;
   std::vector<int> pb(axB);
   pb.insert(pb.end(), freeB.begin(), freeB.end());
   std::vector<int> pb2(freeB);
@@ -158,19 +166,59 @@ DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
     g.sBk = 1;
     g.sBn = K;
   } else {
-    Buse = transpose(B, pb, st);
+    pl.B = transpose(B, pb, st);
     g.sBk = N;
     g.sBn = 1;
   }
   g.sCm = N;
   g.sCn = 1;
-  DT<T> C(out, st);
-  if (K == 0) {
-    TG_CUDA(cudaMemsetAsync(C.p, 0, sizeof(T) * static_cast<size_t>(C.size()), st));
-    return C;
+  pl.C = DT<T>(out, st);
+  if (K == 0) TG_CUDA(cudaMemsetAsync(pl.C.p, 0, sizeof(T) * static_cast<size_t>(pl.C.size()), st));
+  return pl;
+}
+
+// tensordot(A, B, axA, axB): result legs = free legs of A (in order) then
+// free legs of B (in order).  conjA / conjB conjugate the operands.
+template <typename T>
+DT<T> tensordot(const DT<T>& A, const DT<T>& B, const std::vector<int>& axA,
+                const std::vector<int>& axB, cudaStream_t st, bool conjA = false,
+                bool conjB = false, int prec = 0) {
+  TdPlan<T> pl = plan_tensordot(A, B, axA, axB, st, conjA, conjB, prec);
+  if (pl.g.K > 0) gemm<T>(pl.A.p, pl.B.p, pl.C.p, pl.g, st);
+  return std::move(pl.C);
+}
+
+// Independent tensordots as one grouped product launch (FP64; see
+// gemm_group): plan them all -- the permuted copies of their operands --
+// then contract every one in one persistent launch.
+template <typename T>
+std::vector<DT<T>> tensordot_group(const std::vector<TdPlan<T>>& plans, cudaStream_t st) {
+  std::vector<GroupItem> items;
+  for (const TdPlan<T>& pl : plans) {
+    if (pl.g.K == 0 || pl.g.M == 0 || pl.g.N == 0) continue;
+    if (pl.g.prec != 0) fail(TG_E_RUNTIME, "tensordot_group: FP64 products only");
+    GroupItem it;
+    it.A = pl.A.p;
+    it.B = pl.B.p;
+    it.C = pl.C.p;
+    it.M = pl.g.M;
+    it.N = pl.g.N;
+    it.K = pl.g.K;
+    it.sAm = pl.g.sAm;
+    it.sAk = pl.g.sAk;
+    it.sBk = pl.g.sBk;
+    it.sBn = pl.g.sBn;
+    it.sCm = pl.g.sCm;
+    it.sCn = pl.g.sCn;
+    it.conjA = pl.g.conjA;
+    it.conjB = pl.g.conjB;
+    items.push_back(it);
   }
-  gemm<T>(Ause.p, Buse.p, C.p, g, st);
-  return C;
+  if (!items.empty()) gemm_group<T>(items.data(), static_cast<int>(items.size()), st);
+  std::vector<DT<T>> out;
+  out.reserve(plans.size());
+  for (const TdPlan<T>& pl : plans) out.push_back(pl.C);
+  return out;
 }
 
 }  // namespace tg

@@ -76,7 +76,7 @@ struct EngineT final : Engine {
   static constexpr int kRowStreams = 4;
   cudaStream_t main_st = nullptr;
   cudaStream_t row_st[kRowStreams] = {};
-  cudaEvent_t ev_fork = nullptr, ev_join[kRowStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kRowStreams] = {}, ev_mid[kRowStreams] = {};
   // Row staggering: row r's rSVD waits for row r-1's first range-finder
   // product, so that the rows' latency-bound orthonormalisations fall on
   // each other's tensor-core products instead of coinciding.
@@ -150,6 +150,7 @@ struct EngineT final : Engine {
     for (int r = 0; r < kRowStreams; ++r) {
       TG_CUDA(cudaStreamCreateWithFlags(&row_st[r], cudaStreamNonBlocking));
       TG_CUDA(cudaEventCreateWithFlags(&ev_join[r], cudaEventDisableTiming));
+      TG_CUDA(cudaEventCreateWithFlags(&ev_mid[r], cudaEventDisableTiming));
       TG_CUDA(cudaEventCreateWithFlags(&ev_stagger[r], cudaEventDisableTiming));
     }
     TG_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -236,6 +237,7 @@ struct EngineT final : Engine {
     for (int r = 0; r < kRowStreams; ++r) {
       if (row_st[r]) cudaStreamDestroy(row_st[r]);
       if (ev_join[r]) cudaEventDestroy(ev_join[r]);
+      if (ev_mid[r]) cudaEventDestroy(ev_mid[r]);
       if (ev_stagger[r]) cudaEventDestroy(ev_stagger[r]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -1176,32 +1178,138 @@ struct EngineT final : Engine {
     }
   }
 
-  // Calc_Next_CTM (ctm.cpp:493-518); the results are written into the
-  // storage of C1o / C4o
-  void next_ctm(const DT<T>& C1, const DT<T>& C4, const DT<T>& eT1, const DT<T>& eT6, const DT<T>& PU,
-                const DT<T>& PL, DT<T>& C1o, DT<T>& C4o) {
-    normalize_into(td(PU, td(C1, eT1, {1}, {0}), {0, 1, 2}, {0, 2, 3}), C1o);
-    normalize_into(td(td(eT6, C4, {1}, {0}), PL, {3, 1, 2}, {0, 1, 2}), C4o);
+  // Pass 2 of a move, every line at once: Calc_Next_CTM (ctm.cpp:493-518,
+  // the new corners, normalised by their largest element) and Calc_Next_eT
+  // (ctm.cpp:520-552, the new edges) for all rows, stage by stage, each stage's products over all
+  // rows in ONE grouped persistent launch (gemm_group; the 3xTF32 form runs
+  // them one by one).  Stage 1 reads every corner and edge tensor the pass
+  // needs; the new ones are written at the ends of stages 2 and 4, so no
+  // row reads a tensor another row has already replaced -- on a skewed cell,
+  // where one row's next line is another row's current one, this is what
+  // the reference's C1_bak / C4_bak / eTl_bak copies (ctm.cpp:595-601)
+  // provide.
+  struct CtmAbs {
+    const DT<T>*C1, *C4, *eT1, *eT6, *PU, *PL;
+    DT<T>*C1o, *C4o;
+  };
+  struct EtAbs {
+    const DT<T>*eT8, *T1, *PU, *PL;
+    DT<T>* out;
+  };
+  // One stage of absorb: the tensordots `specs`, independent of each other.
+  // The operand permutations run on the row streams; FP64 products without
+  // a specialised kernel (gemm_specialised) then run as one grouped launch on
+  // `st`, while the others -- and every 3xTF32 product -- run one by one on
+  // the row streams, overlapping it.
+  struct TdSpec {
+    DT<T> a, b;
+    V x, y;
+    bool ca;
+  };
+  std::vector<DT<T>> td_stage(std::vector<TdSpec>& specs) {
+    const int n = static_cast<int>(specs.size());
+    std::vector<TdPlan<T>> plans(static_cast<size_t>(n));
+    std::vector<char> alone(static_cast<size_t>(n), 0);
+    const bool par = rows_parallel() && n > 1;
+    const int ns = par ? std::min(n, kRowStreams) : 0;
+    cudaStream_t home = st;
+    if (par) {
+      TG_CUDA(cudaEventRecord(ev_fork, home));
+      for (int r = 0; r < ns; ++r) TG_CUDA(cudaStreamWaitEvent(row_st[r], ev_fork, 0));
+    }
+    auto on = [&](int q) { return par ? row_st[q % ns] : home; };
+    auto make = [&](int q) {
+      TdSpec& sp = specs[static_cast<size_t>(q)];
+      plans[static_cast<size_t>(q)] = plan_tensordot<T>(sp.a, sp.b, sp.x, sp.y, on(q), sp.ca, false, cur_prec);
+      const GemmDesc& g = plans[static_cast<size_t>(q)].g;
+      alone[static_cast<size_t>(q)] = cur_prec != 0 || gemm_specialised<T>(g);
+    };
+    auto own = [&](int q) {
+      TdPlan<T>& pl = plans[static_cast<size_t>(q)];
+      if (pl.g.K > 0) gemm<T>(pl.A.p, pl.B.p, pl.C.p, pl.g, on(q));
+    };
+    // the grouped products' operands first on every row stream, then the lone products
+    for (int q = 0; q < n; ++q) make(q);
+    std::vector<TdPlan<T>> grouped;
+    for (int q = 0; q < n; ++q)
+      if (!alone[static_cast<size_t>(q)]) grouped.push_back(plans[static_cast<size_t>(q)]);
+    if (par)
+      for (int r = 0; r < ns; ++r) TG_CUDA(cudaEventRecord(ev_mid[r], row_st[r]));
+    for (int q = 0; q < n; ++q)
+      if (alone[static_cast<size_t>(q)]) own(q);
+    if (!grouped.empty()) {
+      if (par)
+        for (int r = 0; r < ns; ++r) TG_CUDA(cudaStreamWaitEvent(home, ev_mid[r], 0));
+      tensordot_group<T>(grouped, home);
+    }
+    if (par)
+      for (int r = 0; r < ns; ++r) {
+        TG_CUDA(cudaEventRecord(ev_join[r], row_st[r]));
+        TG_CUDA(cudaStreamWaitEvent(home, ev_join[r], 0));
+      }
+    std::vector<DT<T>> out;
+    for (TdPlan<T>& pl : plans) {
+      // tensors made on a row stream: released on `st`, after the join
+      for (DT<T>* t : {&pl.A, &pl.B, &pl.C})
+        if (t->mem) t->mem->st = home;
+      out.push_back(pl.C);
+    }
+    return out;
   }
 
-  // Calc_Next_eT (ctm.cpp:520-552), written into the storage of `out`
-  void next_et(const DT<T>& eT8, const DT<T>& T1, const DT<T>& PU, const DT<T>& PL, DT<T>& out) {
-    DT<T> X = td(bra(T1), td(eT8, PL, {1}, {0}), {0, 1}, {2, 4}, true, false);
-    X = td(T1, X, {0, 1, 4}, {4, 5, 2});
-    normalize_into(tr(td(X, PU, {1, 3, 4}, {1, 2, 0}), {3, 2, 0, 1}), out);
+  void absorb(const std::vector<CtmAbs>& cj, const std::vector<EtAbs>& ej) {
+    std::vector<TdSpec> ps;
+    auto plan = [&](const DT<T>& a, const DT<T>& b, const V& x, const V& y, bool ca = false) {
+      ps.push_back({a, b, x, y, ca});
+    };
+    auto run = [&](std::vector<TdSpec>& sp) {
+      std::vector<DT<T>> out = td_stage(sp);
+      sp.clear();
+      return out;
+    };
+    const size_t nc = cj.size(), ne = ej.size();
+    // stage 1: C1 eT1, eT6 C4 (next_ctm), eT8 PL (next_et)
+    for (const CtmAbs& c : cj) {
+      plan(*c.C1, *c.eT1, {1}, {0});
+      plan(*c.eT6, *c.C4, {1}, {0});
+    }
+    for (const EtAbs& e : ej) plan(*e.eT8, *e.PL, {1}, {0});
+    std::vector<DT<T>> r1 = run(ps);
+    // stage 2: the new corners, and the bra layer of the new edges
+    for (size_t q = 0; q < nc; ++q) {
+      plan(*cj[q].PU, r1[2 * q], {0, 1, 2}, {0, 2, 3});
+      plan(r1[2 * q + 1], *cj[q].PL, {3, 1, 2}, {0, 1, 2});
+    }
+    for (size_t q = 0; q < ne; ++q) plan(bra(*ej[q].T1), r1[2 * nc + q], {0, 1}, {2, 4}, true);
+    std::vector<DT<T>> r2 = run(ps);
+    r1.clear();
+    for (size_t q = 0; q < nc; ++q) {
+      normalize_into(r2[2 * q], *cj[q].C1o);
+      normalize_into(r2[2 * q + 1], *cj[q].C4o);
+    }
+    if (ne == 0) return;
+    // stage 3: the ket layer
+    for (size_t q = 0; q < ne; ++q) plan(*ej[q].T1, r2[2 * nc + q], {0, 1, 4}, {4, 5, 2});
+    std::vector<DT<T>> r3 = run(ps);
+    r2.clear();
+    // stage 4: PU closes the new edges
+    for (size_t q = 0; q < ne; ++q) plan(r3[q], *ej[q].PU, {1, 3, 4}, {1, 2, 0});
+    std::vector<DT<T>> r4 = run(ps);
+    r3.clear();
+    for (size_t q = 0; q < ne; ++q) normalize_into(tr(r4[q], {3, 2, 0, 1}), *ej[q].out);
   }
 
   // ------------------------------------------------------------- the moves
   //
   // Each move has the two passes of Left_move (ctm.cpp:562-616): all the
-  // projectors of the line, then the new corners and edges of the next line.
-  // The reference writes into copies (C1_bak, ...) and copies back; here the
-  // results go straight into the environment storage, and pass 2 reads from
-  // copies only where the current and the next line share sites (a skewed
-  // cell, pass_inputs).  The reference computes every new edge tensor
-  // twice -- row iy's eT[k] and row iy-1's eT[j] are the same Calc_Next_eT
-  // of the same inputs -- so each distinct (output, inputs) job runs once;
-  // when two jobs write one output the later one wins, as in the reference.
+  // projectors of the line (rows on their own streams), then the new corners
+  // and edges of the next line (absorb, all rows at once).  The reference
+  // writes into copies (C1_bak, ...) and copies back; here the results go
+  // straight into the environment storage.  The reference computes every new
+  // edge tensor twice -- row iy's eT[k] and row iy-1's eT[j] are the same
+  // Calc_Next_eT of the same inputs -- so each distinct (output, inputs) job
+  // runs once; when two jobs write one output the later one wins, as in the
+  // reference.
   struct EtJob {
     int out, src, site, pu, pl;
     bool same_inputs(const EtJob& o) const { return src == o.src && site == o.site && pu == o.pu && pl == o.pl; }
@@ -1218,23 +1326,6 @@ struct EngineT final : Engine {
       if (!superseded && !repeated) out.push_back(jobs[a]);
     }
     return out;
-  }
-
-  // Pass 2 of a move writes the corners and edges of the next line while it
-  // reads those of the current one.  Where a site is in both -- on a skewed
-  // cell a row's next line is another row's current one -- every read must
-  // see the tensor as it was before the pass, the reference's C1_bak /
-  // C4_bak / eTl_bak (ctm.cpp:595-601): the family is then read from copies
-  // made before the rows start.  Elsewhere nothing is copied.
-  const std::vector<DT<T>>& pass_inputs(const std::vector<DT<T>>& fam, const std::vector<int>& reads,
-                                        const std::vector<int>& writes, std::vector<DT<T>>& copy) {
-    bool shared = false;
-    for (int w : writes)
-      for (int r : reads) shared = shared || w == r;
-    if (!shared) return fam;
-    copy.resize(fam.size());
-    for (size_t i = 0; i < fam.size(); ++i) copy[i] = clone(fam[i], st);
-    return copy;
   }
 
   void left_move(int ix) {
@@ -1261,30 +1352,17 @@ struct EngineT final : Engine {
       jobs.push_back({k, l, l, dn, iy});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
-    std::vector<int> ra, wa, rb, wb, re, we;
+    std::vector<CtmAbs> cj;
+    std::vector<EtAbs> ej;
     for (int iy = 0; iy < LY; ++iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
-      ra.push_back(i), wa.push_back(j), rb.push_back(l), wb.push_back(k);
-    }
-    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
-    std::vector<DT<T>> ca, cb, ce;
-    const auto& C1in = pass_inputs(C1, ra, wa, ca);
-    const auto& C4in = pass_inputs(C4, rb, wb, cb);
-    const auto& eTlin = pass_inputs(eTl, re, we, ce);
-    for_rows(LY, par, [&](int iy) {
-      const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C1in[i], C4in[l], eTt[i], eTb[l], PUs[up], PLs[dn], C1[j], C4[k]);
-      for (size_t q = iy; q < fin.size(); q += LY) {
-        const EtJob& b = fin[q];
-        next_et(eTlin[b.src], mt(b.site), PUs[b.pu], PLs[b.pl], eTl[b.out]);
-      }
-    });
+      cj.push_back({&C1[i], &C4[l], &eTt[i], &eTb[l], &PUs[up], &PLs[dn], &C1[j], &C4[k]});
+    }
+    for (const EtJob& b : fin) ej.push_back({&eTl[b.src], &mt(b.site), &PUs[b.pu], &PLs[b.pl], &eTl[b.out]});
+    absorb(cj, ej);
     keep(PUs);
     keep(PLs);
-    keep(ca);
-    keep(cb);
-    keep(ce);
   }
 
   void right_move(int ix) {
@@ -1311,30 +1389,17 @@ struct EngineT final : Engine {
       jobs.push_back({i, j, j, up, iy});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
-    std::vector<int> ra, wa, rb, wb, re, we;
+    std::vector<CtmAbs> cj;
+    std::vector<EtAbs> ej;
     for (int iy = 0; iy < LY; ++iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
-      ra.push_back(k), wa.push_back(l), rb.push_back(j), wb.push_back(i);
-    }
-    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
-    std::vector<DT<T>> ca, cb, ce;
-    const auto& C3in = pass_inputs(C3, ra, wa, ca);
-    const auto& C2in = pass_inputs(C2, rb, wb, cb);
-    const auto& eTrin = pass_inputs(eTr, re, we, ce);
-    for_rows(LY, par, [&](int iy) {
-      const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
       const int up = (iy + 1) % LY, dn = (iy - 1 + LY) % LY;
-      next_ctm(C3in[k], C2in[j], eTb[k], eTt[j], PUs[dn], PLs[up], C3[l], C2[i]);
-      for (size_t q = iy; q < fin.size(); q += LY) {
-        const EtJob& b = fin[q];
-        next_et(eTrin[b.src], rot(b.site, 0), PUs[b.pu], PLs[b.pl], eTr[b.out]);
-      }
-    });
+      cj.push_back({&C3[k], &C2[j], &eTb[k], &eTt[j], &PUs[dn], &PLs[up], &C3[l], &C2[i]});
+    }
+    for (const EtJob& b : fin) ej.push_back({&eTr[b.src], &rot(b.site, 0), &PUs[b.pu], &PLs[b.pl], &eTr[b.out]});
+    absorb(cj, ej);
     keep(PUs);
     keep(PLs);
-    keep(ca);
-    keep(cb);
-    keep(ce);
   }
 
   void top_move(int iy) {
@@ -1361,30 +1426,17 @@ struct EngineT final : Engine {
       jobs.push_back({l, i, i, lf, ix});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
-    std::vector<int> ra, wa, rb, wb, re, we;
+    std::vector<CtmAbs> cj;
+    std::vector<EtAbs> ej;
     for (int ix = 0; ix < LX; ++ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
-      ra.push_back(j), wa.push_back(k), rb.push_back(i), wb.push_back(l);
-    }
-    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
-    std::vector<DT<T>> ca, cb, ce;
-    const auto& C2in = pass_inputs(C2, ra, wa, ca);
-    const auto& C1in = pass_inputs(C1, rb, wb, cb);
-    const auto& eTtin = pass_inputs(eTt, re, we, ce);
-    for_rows(LX, par, [&](int ix) {
-      const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C2in[j], C1in[i], eTr[j], eTl[i], PUs[rt], PLs[lf], C2[k], C1[l]);
-      for (size_t q = ix; q < fin.size(); q += LX) {
-        const EtJob& b = fin[q];
-        next_et(eTtin[b.src], rot(b.site, 1), PUs[b.pu], PLs[b.pl], eTt[b.out]);
-      }
-    });
+      cj.push_back({&C2[j], &C1[i], &eTr[j], &eTl[i], &PUs[rt], &PLs[lf], &C2[k], &C1[l]});
+    }
+    for (const EtJob& b : fin) ej.push_back({&eTt[b.src], &rot(b.site, 1), &PUs[b.pu], &PLs[b.pl], &eTt[b.out]});
+    absorb(cj, ej);
     keep(PUs);
     keep(PLs);
-    keep(ca);
-    keep(cb);
-    keep(ce);
   }
 
   void bottom_move(int iy) {
@@ -1411,30 +1463,17 @@ struct EngineT final : Engine {
       jobs.push_back({j, k, k, rt, ix});
     }
     const std::vector<EtJob> fin = final_jobs(jobs);
-    std::vector<int> ra, wa, rb, wb, re, we;
+    std::vector<CtmAbs> cj;
+    std::vector<EtAbs> ej;
     for (int ix = 0; ix < LX; ++ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
-      ra.push_back(l), wa.push_back(i), rb.push_back(k), wb.push_back(j);
-    }
-    for (const EtJob& b : fin) re.push_back(b.src), we.push_back(b.out);
-    std::vector<DT<T>> ca, cb, ce;
-    const auto& C4in = pass_inputs(C4, ra, wa, ca);
-    const auto& C3in = pass_inputs(C3, rb, wb, cb);
-    const auto& eTbin = pass_inputs(eTb, re, we, ce);
-    for_rows(LX, par, [&](int ix) {
-      const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
       const int rt = (ix + 1) % LX, lf = (ix - 1 + LX) % LX;
-      next_ctm(C4in[l], C3in[k], eTl[l], eTr[k], PUs[lf], PLs[rt], C4[i], C3[j]);
-      for (size_t q = ix; q < fin.size(); q += LX) {
-        const EtJob& b = fin[q];
-        next_et(eTbin[b.src], rot(b.site, 2), PUs[b.pu], PLs[b.pl], eTb[b.out]);
-      }
-    });
+      cj.push_back({&C4[l], &C3[k], &eTl[l], &eTr[k], &PUs[lf], &PLs[rt], &C4[i], &C3[j]});
+    }
+    for (const EtJob& b : fin) ej.push_back({&eTb[b.src], &rot(b.site, 2), &PUs[b.pu], &PLs[b.pl], &eTb[b.out]});
+    absorb(cj, ej);
     keep(PUs);
     keep(PLs);
-    keep(ca);
-    keep(cb);
-    keep(ce);
   }
 
   // ------------------------------------------------------ initialisation

@@ -445,6 +445,212 @@ __global__ void __launch_bounds__(128) gemm_narrow_kernel(GemmParams<double> p) 
 }
 
 // ---------------------------------------------------------------------------
+// Grouped persistent product (gemm_group in kernels.cuh).  The problem table
+// travels as a __grid_constant__ kernel parameter (no copy, no memcpy node in
+// a captured graph); tile t of the group belongs to the problem whose tile0
+// is the last one <= t.  CTA tile (16 WFM) x (16 WFN) x 16, 4 warps of
+// (8 WFM) x (8 WFN), operands staged global -> shared by cp.async through a
+// 3-stage ring (zero-filled outside the matrix).  Complex operands stay
+// interleaved in shared memory; each fragment load forms re, im and re + im.
+// ---------------------------------------------------------------------------
+struct GroupTab {
+  struct P {
+    const void* A;
+    const void* B;
+    void* C;
+    void* part;  // split-K: nsplit partial products (M x N, row-major) instead of C
+    int64_t M, N, K, sAm, sAk, sBk, sBn, sCm, sCn;
+    int64_t kchunk;  // K of one split chunk (a multiple of 16)
+    int tn, tiles;   // column tiles, output tiles
+    int tile0;       // first work item (tile x chunk) of the problem
+    int nsplit;
+    int conjA, conjB;
+  } p[kGroupMax];
+  int count, total;
+};
+// the partial sums of the split problems of a group, added in chunk order
+struct GroupRed {
+  struct R {
+    const void* part;
+    void* C;
+    int64_t M, N, sCm, sCn, elem0;
+    int nsplit;
+  } r[kGroupMax];
+  int count;
+  int64_t total;
+};
+
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src, bool valid) {
+  if constexpr (is_cplx<T>::value) cp_async16_zfill(dst, src, valid);
+  else cp_async8_zfill(dst, src, valid);
+}
+
+template <typename T, int WFM, int WFN>
+__global__ void __launch_bounds__(128) gemm_group_kernel(const __grid_constant__ GroupTab tab) {
+  constexpr bool CPLX = is_cplx<T>::value;
+  constexpr int BM = 16 * WFM, BN = 16 * WFN;
+  // row pitches: fragment reads conflict-free (8-byte: 4 mod 16; 16-byte: 2 mod 8)
+  constexpr int LDA = BM + (CPLX ? 2 : 4), LDB = BN + (CPLX ? 2 : 4);
+  constexpr int ASZ = GBK * LDA, BSZ = GBK * LDB;
+  extern __shared__ __align__(16) double smem_g[];
+  T* As = reinterpret_cast<T*>(smem_g);  // [NSTAGE][GBK][LDA]
+  T* Bs = As + NSTAGE * ASZ;             // [NSTAGE][GBK][LDB]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * (8 * WFM), wn = (warp >> 1) * (8 * WFN);
+  constexpr int NACC = CPLX ? 3 : 1;
+
+  for (int t = blockIdx.x; t < tab.total; t += gridDim.x) {
+    int pi = 0;
+    while (pi + 1 < tab.count && t >= tab.p[pi + 1].tile0) ++pi;
+    const GroupTab::P& P = tab.p[pi];
+    const int lt = (t - P.tile0) % P.tiles, z = (t - P.tile0) / P.tiles;  // tile, K chunk
+    const int64_t m0 = static_cast<int64_t>(lt / P.tn) * BM, n0 = static_cast<int64_t>(lt % P.tn) * BN;
+    const int64_t M = P.M, N = P.N;
+    const int64_t kb0 = z * P.kchunk;
+    const int64_t K = std::min(P.K - kb0, P.kchunk);  // this chunk's K
+    const T* A = static_cast<const T*>(P.A) + kb0 * P.sAk;
+    const T* B = static_cast<const T*>(P.B) + kb0 * P.sBk;
+    const bool split = P.nsplit > 1;
+    T* C = split ? static_cast<T*>(P.part) + z * M * N : static_cast<T*>(P.C);
+    const int64_t sCm = split ? N : P.sCm, sCn = split ? 1 : P.sCn;
+    const bool a_kc = P.sAk == 1, b_nc = P.sBn == 1;
+    const int64_t nk = (K + GBK - 1) / GBK;
+
+    auto issue = [&](int64_t kt) {
+      if (kt < nk) {
+        const int64_t k0 = kt * GBK;
+        T* as = As + (kt % NSTAGE) * ASZ;
+        T* bs = Bs + (kt % NSTAGE) * BSZ;
+#pragma unroll
+        for (int i = 0; i < BM / 8; ++i) {
+          const int idx = tid + i * 128;
+          const int mm = a_kc ? idx / GBK : idx % BM;
+          const int kk = a_kc ? idx % GBK : idx / BM;
+          const int64_t gm = m0 + mm, gk = k0 + kk;
+          const bool ok = gm < M && gk < K;
+          cp_async_elem<T>(as + kk * LDA + mm, ok ? A + gm * P.sAm + gk * P.sAk : A, ok);
+        }
+#pragma unroll
+        for (int i = 0; i < BN / 8; ++i) {
+          const int idx = tid + i * 128;
+          const int nn = b_nc ? idx % BN : idx / GBK;
+          const int kb = b_nc ? idx / BN : idx % GBK;
+          const int64_t gn = n0 + nn, gk = k0 + kb;
+          const bool ok = gn < N && gk < K;
+          cp_async_elem<T>(bs + kb * LDB + nn, ok ? B + gk * P.sBk + gn * P.sBn : B, ok);
+        }
+      }
+      cp_async_commit();
+    };
+
+    double acc[NACC][WFM][WFN][2];
+#pragma unroll
+    for (int c = 0; c < NACC; ++c)
+#pragma unroll
+      for (int i = 0; i < WFM; ++i)
+#pragma unroll
+        for (int j = 0; j < WFN; ++j) acc[c][i][j][0] = acc[c][i][j][1] = 0.0;
+    const double sa = P.conjA ? -1.0 : 1.0, sb = P.conjB ? -1.0 : 1.0;
+
+#pragma unroll
+    for (int s0 = 0; s0 < NSTAGE - 1; ++s0) issue(s0);
+    for (int64_t kt = 0; kt < nk; ++kt) {
+      cp_async_wait<NSTAGE - 2>();
+      __syncthreads();
+      issue(kt + NSTAGE - 1);
+      const T* as = As + (kt % NSTAGE) * ASZ;
+      const T* bs = Bs + (kt % NSTAGE) * BSZ;
+#pragma unroll
+      for (int k4 = 0; k4 < GBK; k4 += 4) {
+        const int kr = k4 + (lane & 3);
+        if constexpr (CPLX) {
+          double ar[WFM], ai[WFM], br[WFN], bi[WFN];
+#pragma unroll
+          for (int i = 0; i < WFM; ++i) {
+            const cplx v = as[kr * LDA + wm + i * 8 + (lane >> 2)];
+            ar[i] = v.x;
+            ai[i] = sa * v.y;
+          }
+#pragma unroll
+          for (int j = 0; j < WFN; ++j) {
+            const cplx v = bs[kr * LDB + wn + j * 8 + (lane >> 2)];
+            br[j] = v.x;
+            bi[j] = sb * v.y;
+          }
+#pragma unroll
+          for (int i = 0; i < WFM; ++i)
+#pragma unroll
+            for (int j = 0; j < WFN; ++j) {
+              dmma(acc[0][i][j][0], acc[0][i][j][1], ar[i], br[j]);
+              dmma(acc[1][i][j][0], acc[1][i][j][1], ai[i], bi[j]);
+              dmma(acc[2][i][j][0], acc[2][i][j][1], ar[i] + ai[i], br[j] + bi[j]);
+            }
+        } else {
+          double a[WFM], b[WFN];
+#pragma unroll
+          for (int i = 0; i < WFM; ++i) a[i] = as[kr * LDA + wm + i * 8 + (lane >> 2)];
+#pragma unroll
+          for (int j = 0; j < WFN; ++j) b[j] = bs[kr * LDB + wn + j * 8 + (lane >> 2)];
+#pragma unroll
+          for (int i = 0; i < WFM; ++i)
+#pragma unroll
+            for (int j = 0; j < WFN; ++j) dmma(acc[0][i][j][0], acc[0][i][j][1], a[i], b[j]);
+        }
+      }
+    }
+    cp_async_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < WFM; ++i)
+#pragma unroll
+      for (int j = 0; j < WFN; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t gm = m0 + wm + i * 8 + (lane >> 2);
+          const int64_t gn = n0 + wn + j * 8 + 2 * (lane & 3) + h;
+          if (gm < M && gn < N) {
+            T* c = C + gm * sCm + gn * sCn;
+            if constexpr (CPLX) {
+              const double p1 = acc[0][i][j][h], p2 = acc[1][i][j][h], p3 = acc[2][i][j][h];
+              *c = make_double2(p1 - p2, p3 - p1 - p2);
+            } else {
+              *c = acc[0][i][j][h];
+            }
+          }
+        }
+    __syncthreads();  // the next tile's first copies reuse the stages
+  }
+}
+
+template <typename T>
+__global__ void group_reduce_kernel(const __grid_constant__ GroupRed red) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < red.total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int ri = 0;
+    while (ri + 1 < red.count && i >= red.r[ri + 1].elem0) ++ri;
+    const GroupRed::R& R = red.r[ri];
+    const int64_t e = i - R.elem0, len = R.M * R.N;
+    const T* part = static_cast<const T*>(R.part);
+    double re = 0.0, im = 0.0;
+    for (int z = 0; z < R.nsplit; ++z) {
+      const T v = part[z * len + e];
+      re += re_of(v);
+      im += im_of(v);
+    }
+    const int64_t m = e / R.N, n = e - m * R.N;
+    T* c = static_cast<T*>(R.C) + m * R.sCm + n * R.sCn;
+    if constexpr (is_cplx<T>::value) *c = make_double2(re, im);
+    else *c = re;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Mixed precision: 3xTF32 product on the 5th-generation tensor cores
 // (tcgen05.mma kind::tf32, accumulator in tensor memory).
 //
@@ -2249,6 +2455,234 @@ void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st) {
   TG_CUDA(cudaFreeAsync(buf, st));
 }
 
+// ---- grouped products: launch of one tile variant, autotuner, entry point
+namespace {
+constexpr int kGroupVariants = 2;  // real: 64 x 64, 32 x 64; complex: 64 x 32, 32 x 32
+
+template <typename T, int WFM, int WFN>
+void launch_group_v(const GroupTab& tab, cudaStream_t st) {
+  constexpr bool CPLX = is_cplx<T>::value;
+  constexpr int BM = 16 * WFM, BN = 16 * WFN;
+  constexpr int LDA = BM + (CPLX ? 2 : 4), LDB = BN + (CPLX ? 2 : 4);
+  const size_t smem = sizeof(T) * NSTAGE * GBK * (LDA + LDB);
+  const void* fn = reinterpret_cast<const void*>(gemm_group_kernel<T, WFM, WFN>);
+  ensure_dynamic_smem(fn, smem);
+  // resident CTAs per SM and SM count, per device
+  static std::mutex mu;
+  static std::map<int, int> slots;
+  const int dev = current_device();
+  int cap = 0;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = slots.find(dev);
+    if (it == slots.end()) {
+      int occ = 0, sms = 0;
+      TG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gemm_group_kernel<T, WFM, WFN>, 128, smem));
+      TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      it = slots.emplace(dev, std::max(1, occ) * std::max(1, sms)).first;
+    }
+    cap = it->second;
+  }
+  const int grid = std::min(tab.total, cap);
+  gemm_group_kernel<T, WFM, WFN><<<grid, 128, smem, st>>>(tab);
+  TG_CHECK_LAUNCH();
+  count_launch();
+}
+
+template <typename T>
+constexpr int group_bm(int v) { return v == 0 ? 64 : 32; }
+template <typename T>
+constexpr int group_bn(int) { return is_cplx<T>::value ? 32 : 64; }
+
+template <typename T>
+void launch_group(int v, const GroupTab& tab, cudaStream_t st) {
+  if constexpr (is_cplx<T>::value) {
+    if (v == 0) launch_group_v<T, 4, 2>(tab, st);
+    else launch_group_v<T, 2, 2>(tab, st);
+  } else {
+    if (v == 0) launch_group_v<T, 4, 4>(tab, st);
+    else launch_group_v<T, 2, 4>(tab, st);
+  }
+}
+
+// Work items of a group: every output tile of every problem, problems with
+// long K and few tiles cut into K chunks (split-K, summed afterwards in chunk
+// order) so that the group's work spreads over about four items per SM.  The
+// chunks are sized from 64 x 64 tiles whatever the variant, so every variant
+// sums each output element in the same order.  part_off receives each
+// problem's offset into the partial-product buffer; returns its size in
+// elements.
+template <typename T>
+int64_t fill_tab(const GroupItem* items, int n, int v, GroupTab& tab, std::vector<int64_t>& part_off) {
+  const int bm = group_bm<T>(v), bn = group_bn<T>(v);
+  double work = 0.0;  // k tiles over all 64 x 64 output tiles
+  for (int i = 0; i < n; ++i) {
+    const GroupItem& it = items[i];
+    work += static_cast<double>((it.M + 63) / 64 * ((it.N + 63) / 64)) * ((it.K + GBK - 1) / GBK);
+  }
+  part_off.assign(static_cast<size_t>(n), -1);
+  const int64_t chunk_kt = std::max<int64_t>(8, static_cast<int64_t>(std::ceil(work / (4.0 * 148))));
+  tab.count = 0;
+  tab.total = 0;
+  int64_t part = 0;
+  for (int i = 0; i < n; ++i) {
+    const GroupItem& it = items[i];
+    GroupTab::P& p = tab.p[tab.count++];
+    p.A = it.A;
+    p.B = it.B;
+    p.C = it.C;
+    p.part = nullptr;
+    p.M = it.M;
+    p.N = it.N;
+    p.K = it.K;
+    p.sAm = it.sAm;
+    p.sAk = it.sAk;
+    p.sBk = it.sBk;
+    p.sBn = it.sBn;
+    p.sCm = it.sCm;
+    p.sCn = it.sCn;
+    p.conjA = it.conjA;
+    p.conjB = it.conjB;
+    p.tn = static_cast<int>((it.N + bn - 1) / bn);
+    const int64_t tiles = (it.M + bm - 1) / bm * p.tn;
+    const int64_t kt = (it.K + GBK - 1) / GBK;
+    int64_t ns = (kt + chunk_kt - 1) / chunk_kt;
+    const int64_t ckt = (kt + ns - 1) / ns;  // k tiles of one chunk
+    ns = (kt + ckt - 1) / ckt;
+    p.kchunk = ckt * GBK;
+    p.nsplit = static_cast<int>(ns);
+    p.tiles = static_cast<int>(tiles);
+    p.tile0 = tab.total;
+    if (ns > 1) {
+      part_off[static_cast<size_t>(i)] = part;
+      part += ns * it.M * it.N;
+    }
+    if (tab.total + tiles * ns > INT32_MAX / 2) fail(TG_E_INPUT, "gemm_group: too many tiles");
+    tab.total += static_cast<int>(tiles * ns);
+  }
+  return part;
+}
+
+// Runs variant v of the group: the product launch, then (if any problem was
+// split) the reduction of the partial products into C.
+template <typename T>
+void run_group(const GroupItem* items, int n, int v, cudaStream_t st) {
+  GroupTab tab;
+  std::vector<int64_t> off;
+  const int64_t part = fill_tab<T>(items, n, v, tab, off);
+  void* buf = nullptr;
+  if (part > 0) {
+    TG_CUDA(cudaMallocAsync(&buf, sizeof(T) * part, st));
+    for (int i = 0; i < tab.count; ++i)
+      if (off[static_cast<size_t>(i)] >= 0) tab.p[i].part = static_cast<T*>(buf) + off[static_cast<size_t>(i)];
+  }
+  launch_group<T>(v, tab, st);
+  if (part > 0) {
+    GroupRed red;
+    red.count = 0;
+    red.total = 0;
+    for (int i = 0; i < tab.count; ++i) {
+      const GroupTab::P& p = tab.p[i];
+      if (p.nsplit <= 1) continue;
+      GroupRed::R& r = red.r[red.count++];
+      r.part = p.part;
+      r.C = p.C;
+      r.M = p.M;
+      r.N = p.N;
+      r.sCm = p.sCm;
+      r.sCn = p.sCn;
+      r.nsplit = p.nsplit;
+      r.elem0 = red.total;
+      red.total += p.M * p.N;
+    }
+    group_reduce_kernel<T><<<num_blocks(red.total, 256), 256, 0, st>>>(red);
+    TG_CHECK_LAUNCH();
+    count_launch();
+    TG_CUDA(cudaFreeAsync(buf, st));
+  }
+}
+
+std::mutex g_tune_mu;
+std::map<std::vector<int64_t>, int> g_tuned;  // group shape -> variant
+int64_t g_tune_count = 0, g_tune_wins[kGroupVariants] = {};
+}  // namespace
+
+void gemm_group_stats(int64_t* tuned, int64_t* wins, int nwins) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  if (tuned) *tuned = g_tune_count;
+  for (int v = 0; v < nwins && v < kGroupVariants; ++v) wins[v] = g_tune_wins[v];
+}
+
+template <typename T>
+bool gemm_specialised(const GemmDesc& d) {
+  if (is_cplx<T>::value || d.prec != 0 || d.batch != 1) return false;
+  const bool skinny = d.K <= 96 && ((d.N <= 96 && d.M >= 2048) || (d.M <= 96 && d.N >= 2048));
+  return skinny || narrow_nf<T>(d) > 0;
+}
+
+template <typename T>
+void gemm_group(const GroupItem* items, int n, cudaStream_t st) {
+  std::vector<GroupItem> live;
+  for (int i = 0; i < n; ++i) {
+    const GroupItem& it = items[i];
+    if (it.M <= 0 || it.N <= 0) continue;
+    if (it.K <= 0) fail(TG_E_INPUT, "gemm_group: K must be positive");
+    if ((it.sAm != 1 && it.sAk != 1) || (it.sBk != 1 && it.sBn != 1))
+      fail(TG_E_INPUT, "gemm_group: every operand needs a unit stride");
+    live.push_back(it);
+  }
+  for (size_t off = 0; off < live.size(); off += kGroupMax) {
+    const int cnt = static_cast<int>(std::min<size_t>(kGroupMax, live.size() - off));
+    const GroupItem* its = live.data() + off;
+    double flops = 0.0, bytes = 0.0;
+    std::vector<int64_t> key{current_device(), is_cplx<T>::value ? 1 : 0};
+    for (int i = 0; i < cnt; ++i) {
+      const GroupItem& it = its[i];
+      flops += (is_cplx<T>::value ? 8.0 : 2.0) * static_cast<double>(it.M) * it.N * it.K;
+      bytes += sizeof(T) * static_cast<double>(it.M * it.K + it.K * it.N + it.M * it.N);
+      key.insert(key.end(), {it.M, it.N, it.K, it.sAk == 1, it.sBn == 1, it.sCn == 1});
+    }
+    ProfScope ps(PK_GEMM, st, flops, bytes);
+    int v = -1;
+    {
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      auto f = g_tuned.find(key);
+      if (f != g_tuned.end()) v = f->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (v < 0 && cs == cudaStreamCaptureStatusNone && !profile_enabled()) {
+      // the autotuner: every variant once to warm up, then once timed (all
+      // variants write the same result)
+      float best = 0.0f;
+      cudaEvent_t e0, e1;
+      TG_CUDA(cudaEventCreate(&e0));
+      TG_CUDA(cudaEventCreate(&e1));
+      for (int c = 0; c < kGroupVariants; ++c) {
+        run_group<T>(its, cnt, c, st);
+        TG_CUDA(cudaEventRecord(e0, st));
+        run_group<T>(its, cnt, c, st);
+        TG_CUDA(cudaEventRecord(e1, st));
+        TG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        TG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (v < 0 || ms < best) {
+          v = c;
+          best = ms;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      g_tuned[key] = v;
+      ++g_tune_count;
+      ++g_tune_wins[v];
+    }
+    if (v < 0) v = 0;  // inside a capture before any eager call: the 64-row tile
+    run_group<T>(its, cnt, v, st);
+  }
+}
+
 template <typename T>
 void permute(const T* in, T* out, const Shape& in_shape, const std::vector<int>& perm, bool conj,
              cudaStream_t st) {
@@ -2622,6 +3056,8 @@ void chol_rinv(const T* parts, int nparts, int64_t k, int64_t n, int shift, T* R
   template int jacobi_svd_max_k<T>();                                                            \
   template void jacobi_svd<T>(const T*, int64_t, T*, double*, T*, cudaStream_t, const T*);       \
   template void gemm<T>(const T*, const T*, T*, const GemmDesc&, cudaStream_t);                  \
+  template void gemm_group<T>(const GroupItem*, int, cudaStream_t);                             \
+  template bool gemm_specialised<T>(const GemmDesc&);                                            \
   template void permute<T>(const T*, T*, const Shape&, const std::vector<int>&, bool,            \
                            cudaStream_t);                                                        \
   template void normalize_max_abs<T>(const T*, T*, int64_t, unsigned long long*, cudaStream_t);            \

@@ -38,6 +38,38 @@ struct GemmDesc {
 template <typename T>
 void gemm(const T* A, const T* B, T* C, const GemmDesc& d, cudaStream_t st);
 
+// Grouped FP64 products: up to kGroupMax independent C_p = op(A_p) op(B_p)
+// (batch 1, C overwritten) in ONE persistent launch whose CTAs take the
+// output tiles of every problem in turn, so the products of all rows of a
+// move share one wave instead of running one launch each.  Problems with
+// long K and few output tiles are cut into K chunks whose partial products a
+// second launch sums in chunk order.  Strides as in
+// GemmDesc (one of each operand's strides 1).  Complex products run as three
+// real DMMA products per tile (3M: Re = ArBr - AiBi, Im = (Ar+Ai)(Br+Bi) -
+// ArBr - AiBi).  The tile shape is chosen per group by timing the candidate
+// shapes once on the group's own operands (outside stream capture; cached
+// per device and group shape); every candidate accumulates each output
+// element in the same order, so the choice never changes a result.
+constexpr int kGroupMax = 24;
+struct GroupItem {
+  const void* A = nullptr;
+  const void* B = nullptr;
+  void* C = nullptr;
+  int64_t M = 0, N = 0, K = 0;
+  int64_t sAm = 0, sAk = 0, sBk = 0, sBn = 0, sCm = 0, sCn = 0;
+  bool conjA = false, conjB = false;
+};
+template <typename T>
+void gemm_group(const GroupItem* items, int n, cudaStream_t st);
+// autotuner record: groups tuned so far and, per tile variant, how often it won
+void gemm_group_stats(int64_t* tuned, int64_t* wins, int nwins);
+// True for a product that gemm() runs on a specialised kernel a grouped
+// launch would do worse than: real FP64 shapes of the streaming kernel
+// (skinny.cu: K <= 96, one side <= 96 and the other >= 2048) or of the
+// narrow tile (64 < N <= 96).
+template <typename T>
+bool gemm_specialised(const GemmDesc& d);
+
 // FP64 product with one operand of at most 96 x 96 and the other at least
 // 2048 long (batch 1, a unit stride on the long operand and on C): the
 // streaming kernel of skinny.cu.  Returns false, launching nothing, for any
