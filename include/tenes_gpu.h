@@ -307,13 +307,15 @@ typedef struct tg_window_term {
  *   E = sum_t coeff_t <ops_t> / <1>_t
  * on the environment reached after `iterations` CTMRG sweeps from the
  * initial environment of the current site tensors (tg_ctm_init, then
- * tg_ctm_sweep; full-SVD corner projectors, projector_corner = 1,
- * use_rsvd = 0; real tensors).  grad (optional, NULL for E only) receives
+ * tg_ctm_sweep; full-SVD projectors, corner or up/down
+ * (projector_corner), use_rsvd = 0; real tensors).  grad (optional, NULL
+ * for E only) receives
  * dE/dTn of every site, concatenated in site order in the layout of
  * tg_set_site_tensor.  The gradient is a hand-written reverse pass through
  * the sweeps and the truncated SVDs of the projectors, whose adjoint uses the
  * Lorentzian-broadened factors (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 +
- * svd_broadening).  The sweeps are recomputed in segments of
+ * svd_broadening (s_i^2 + s_j^2)^2), broadened relative to each pair's
+ * scale.  The sweeps are recomputed in segments of
  * checkpoint_every sweeps, so device memory holds one segment's
  * intermediates.  With params.mixed the moves' contractions (forward and
  * adjoint) run as 3xTF32 products; SVDs and the energy stay FP64.  The

@@ -1,12 +1,13 @@
 """FP64 host autograd reference of the CTMRG energy gradient -- TEST INFRASTRUCTURE ONLY.
 
 A torch (float64, CPU) restatement of the oracle's CTMRG forward for real
-site tensors with full-SVD corner projectors:
+site tensors with full-SVD projectors, corner or up/down:
 
   * environment initialisation  (src/iTPS/core/ctm.cpp:984-1193,
     ``tenes_oracle.init_env``),
   * the four moves              (ctm.cpp:562-813, ``tenes_oracle.left_move`` ...),
   * the corner projectors       (ctm.cpp:174-318 without the rSVD branch),
+  * the up/down projectors      (ctm.cpp:320-491 without the rSVD branch),
   * Calc_Next_CTM / Calc_Next_eT (ctm.cpp:493-552),
   * the N x M window contraction (contract_itps_ctm/ctm.cpp:45-87,
     ``tenes_oracle.contract_window``),
@@ -36,7 +37,8 @@ def td(a, b, x, y):
 def svd_backward(U, s, Vh, gU, gs, gVh, eps):
     """dL/dM of M = U diag(s) Vh (thin, real) from dL/dU, dL/ds, dL/dVh.
 
-    F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps), F_ii = 0;
+    F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps (s_i^2 + s_j^2)^2), F_ii = 0
+    (broadened relative to the pair's own scale);
     core = diag(gs) + (F o (J - J^T)) S + S (F o (K - K^T)), J = U^T gU, K = V^T gV;
     gM = U core Vh + (1 - U U^T) gU S^-1 Vh + U S^-1 gVh (1 - V V^T)."""
     m, k = U.shape
@@ -47,7 +49,9 @@ def svd_backward(U, s, Vh, gU, gs, gVh, eps):
     J = U.T @ gU
     K = Vh @ gVh.T
     d = s[None, :] ** 2 - s[:, None] ** 2
-    F = d / (d * d + eps)
+    q = s[None, :] ** 2 + s[:, None] ** 2
+    den = d * d + eps * q * q
+    F = torch.where(den > 0, d / torch.where(den > 0, den, torch.ones_like(den)), torch.zeros_like(den))
     F.fill_diagonal_(0.0)
     core = torch.diag(gs) + (F * (J - J.T)) * s[None, :] + s[:, None] * (F * (K - K.T))
     gM = U @ core @ Vh
@@ -108,6 +112,32 @@ def projector(C1, C4, eT1, eT6, eT7, eT8, T1, T4, chi, cutoff, eps):
     return PU, PL
 
 
+def projector_ud(C1, C2, C3, C4, eT1, eT2, eT3, eT4, eT5, eT6, eT7, eT8, T1, T2, T3, T4, chi, cutoff, eps):
+    """Calc_projector_updown_blocks, full-SVD branch (ctm.cpp:320-491;
+    ``tenes_oracle.calc_projector_updown_blocks``)."""
+    e78 = eT7.shape[1]
+    t41 = T4.shape[1]
+    if t41 == 1:
+        eye = torch.eye(e78, dtype=C1.dtype)
+        return eye.reshape(e78, 1, 1, e78), eye.reshape(e78, 1, 1, e78)
+    LT = _block_LT(C1, eT1, eT8, T1)
+    RT = td(T2, td(td(td(C2, eT3, [1], [0]), eT2, [0], [1]), T2, [2, 5], [2, 1]), [1, 2, 4], [3, 1, 6])
+    RB = td(T3, td(td(td(C3, eT5, [1], [0]), eT4, [0], [1]), T3, [2, 5], [3, 2]), [2, 3, 4], [3, 1, 6])
+    LB = _block_LB(C4, eT7, eT6, T4)
+    R1 = td(RT, LT, [0, 3, 4], [0, 2, 4])
+    R2 = td(RB, LB, [0, 2, 4], [1, 3, 5])
+    M = td(R1, R2, [3, 4, 5], [3, 4, 5])
+    sh = M.shape
+    U, s, Vh = TruncSVD.apply(M.reshape(sh[0] * sh[1] * sh[2], -1), eps)
+    cut, _ = O._truncation(s.detach().numpy(), min(len(s), chi), cutoff)
+    sc = s[:cut] ** -0.5
+    Uc = (U[:, :cut] * sc[None, :]).reshape(sh[0], sh[1], sh[2], cut)
+    Vc = (Vh[:cut] * sc[:, None]).reshape(cut, sh[3], sh[4], sh[5])
+    PU = td(R2, Vc, [0, 1, 2], [1, 2, 3]).permute(1, 0, 2, 3)
+    PL = td(R1, Uc, [0, 1, 2], [0, 1, 2]).permute(1, 0, 2, 3)
+    return PU, PL
+
+
 def _normalized(t):
     return t / t.abs().max()
 
@@ -165,20 +195,28 @@ def init_env(Tn, chi, lat: O.Lattice):
 _RIGHT, _TOP, _BOTTOM = (2, 3, 0, 1, 4), (1, 2, 3, 0, 4), (3, 0, 1, 2, 4)
 
 
-def sweep(env, Tn, chi, lat: O.Lattice, cutoff=1e-12, eps=1e-12):
+def sweep(env, Tn, chi, lat: O.Lattice, cutoff=1e-12, eps=1e-12, corner=True):
     """One CTMRG iteration (ctm.cpp:1205-1228) with the index rules of the
-    oracle's left/right/top/bottom moves (ctm.cpp:562-813)."""
+    oracle's left/right/top/bottom moves (ctm.cpp:562-813); corner=False
+    takes the up/down projectors."""
     C1, C2, C3, C4 = env["C1"], env["C2"], env["C3"], env["C4"]
     eTt, eTr, eTb, eTl = env["eTt"], env["eTr"], env["eTb"], env["eTl"]
     LX, LY = lat.LX_noskew, lat.LY_noskew
-    P = lambda *a: projector(*a, chi, cutoff, eps)  # noqa: E731
     R = lambda t, p: t.permute(*p)  # noqa: E731
+
+    def P(*a, ud):
+        """the corner projector of `a`, or with corner=False the up/down one of `ud`"""
+        if corner:
+            return projector(*a, chi, cutoff, eps)
+        return projector_ud(*ud, chi, cutoff, eps)
 
     for ix in range(LX):  # Left_move
         PU, PL = [None] * LY, [None] * LY
         for iy in range(LY):
             i = lat.index(ix, iy); j = lat.right(i); k = lat.bottom(j); l = lat.left(k)  # noqa: E702
-            PU[iy], PL[iy] = P(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l])
+            PU[iy], PL[iy] = P(C1[i], C4[l], eTt[i], eTb[l], eTl[l], eTl[i], Tn[i], Tn[l],
+                               ud=(C1[i], C2[j], C3[k], C4[l], eTt[i], eTt[j], eTr[j], eTr[k], eTb[k], eTb[l],
+                                   eTl[l], eTl[i], Tn[i], Tn[j], Tn[k], Tn[l]))
         C1b, C4b, eTlb = list(C1), list(C4), list(eTl)
         for iy in range(LY):
             i = lat.index(ix, iy); j = lat.right(i); k = lat.bottom(j); l = lat.left(k)  # noqa: E702
@@ -191,7 +229,10 @@ def sweep(env, Tn, chi, lat: O.Lattice, cutoff=1e-12, eps=1e-12):
         PU, PL = [None] * LY, [None] * LY
         for iy in range(LY):
             k = lat.index(ix, iy); l = lat.left(k); i = lat.top(l); j = lat.right(i)  # noqa: E702
-            PU[iy], PL[iy] = P(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], R(Tn[k], _RIGHT), R(Tn[j], _RIGHT))
+            PU[iy], PL[iy] = P(C3[k], C2[j], eTb[k], eTt[j], eTr[j], eTr[k], R(Tn[k], _RIGHT), R(Tn[j], _RIGHT),
+                               ud=(C3[k], C4[l], C1[i], C2[j], eTb[k], eTb[l], eTl[l], eTl[i], eTt[i], eTt[j],
+                                   eTr[j], eTr[k], R(Tn[k], _RIGHT), R(Tn[l], _RIGHT), R(Tn[i], _RIGHT),
+                                   R(Tn[j], _RIGHT)))
         C2b, C3b, eTrb = list(C2), list(C3), list(eTr)
         for iy in range(LY):
             k = lat.index(ix, iy); l = lat.left(k); i = lat.top(l); j = lat.right(i)  # noqa: E702
@@ -204,7 +245,9 @@ def sweep(env, Tn, chi, lat: O.Lattice, cutoff=1e-12, eps=1e-12):
         PU, PL = [None] * LX, [None] * LX
         for ix in range(LX):
             j = lat.index(ix, iy); k = lat.bottom(j); l = lat.left(k); i = lat.top(l)  # noqa: E702
-            PU[ix], PL[ix] = P(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], R(Tn[j], _TOP), R(Tn[i], _TOP))
+            PU[ix], PL[ix] = P(C2[j], C1[i], eTr[j], eTl[i], eTt[i], eTt[j], R(Tn[j], _TOP), R(Tn[i], _TOP),
+                               ud=(C2[j], C3[k], C4[l], C1[i], eTr[j], eTr[k], eTb[k], eTb[l], eTl[l], eTl[i],
+                                   eTt[i], eTt[j], R(Tn[j], _TOP), R(Tn[k], _TOP), R(Tn[l], _TOP), R(Tn[i], _TOP)))
         C1b, C2b, eTtb = list(C1), list(C2), list(eTt)
         for ix in range(LX):
             j = lat.index(ix, iy); k = lat.bottom(j); l = lat.left(k); i = lat.top(l)  # noqa: E702
@@ -216,7 +259,10 @@ def sweep(env, Tn, chi, lat: O.Lattice, cutoff=1e-12, eps=1e-12):
         PU, PL = [None] * LX, [None] * LX
         for ix in range(LX):
             l = lat.index(ix, iy); i = lat.top(l); j = lat.right(i); k = lat.bottom(j)  # noqa: E702
-            PU[ix], PL[ix] = P(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], R(Tn[l], _BOTTOM), R(Tn[k], _BOTTOM))
+            PU[ix], PL[ix] = P(C4[l], C3[k], eTl[l], eTr[k], eTb[k], eTb[l], R(Tn[l], _BOTTOM), R(Tn[k], _BOTTOM),
+                               ud=(C4[l], C1[i], C2[j], C3[k], eTl[l], eTl[i], eTt[i], eTt[j], eTr[j], eTr[k],
+                                   eTb[k], eTb[l], R(Tn[l], _BOTTOM), R(Tn[i], _BOTTOM), R(Tn[j], _BOTTOM),
+                                   R(Tn[k], _BOTTOM)))
         C3b, C4b, eTbb = list(C3), list(C4), list(eTb)
         for ix in range(LX):
             l = lat.index(ix, iy); i = lat.top(l); j = lat.right(i); k = lat.bottom(j)  # noqa: E702
@@ -276,13 +322,13 @@ def window_value(env, Tn, lat: O.Lattice, term) -> torch.Tensor:
 
 
 def energy(Tn: Sequence[torch.Tensor], terms, chi: int, iterations: int, lat: O.Lattice,
-           cutoff: float = 1e-12, eps: float = 1e-12) -> torch.Tensor:
+           cutoff: float = 1e-12, eps: float = 1e-12, corner: bool = True) -> torch.Tensor:
     """E = sum_t coeff_t <ops_t> / <1>_t after ``iterations`` CTMRG sweeps from
     the initial environment of Tn (the norm of a window shared by every term on
     the same window, as twosite_obs.cpp:160-181 caches it)."""
     env = init_env(Tn, chi, lat)
     for _ in range(iterations):
-        sweep(env, Tn, chi, lat, cutoff, eps)
+        sweep(env, Tn, chi, lat, cutoff, eps, corner)
     norms: Dict[Tuple[int, ...], torch.Tensor] = {}
     E = torch.zeros((), dtype=torch.float64)
     for t in terms:
@@ -294,8 +340,8 @@ def energy(Tn: Sequence[torch.Tensor], terms, chi: int, iterations: int, lat: O.
 
 
 def energy_and_grad(Tn_np: Sequence, terms, chi: int, iterations: int, lat: O.Lattice,
-                    cutoff: float = 1e-12, eps: float = 1e-12) -> Tuple[float, List]:
+                    cutoff: float = 1e-12, eps: float = 1e-12, corner: bool = True) -> Tuple[float, List]:
     Tn = [torch.tensor(t, dtype=torch.float64, requires_grad=True) for t in Tn_np]
-    E = energy(Tn, terms, chi, iterations, lat, cutoff, eps)
+    E = energy(Tn, terms, chi, iterations, lat, cutoff, eps, corner)
     g = torch.autograd.grad(E, Tn)
     return float(E.detach()), [x.numpy() for x in g]

@@ -148,7 +148,9 @@ __global__ void svd_gs_kernel(const double* __restrict__ gUc, const double* __re
 }
 
 // core_ij = delta_ij gs_i + F_ij (J_ij - J_ji) s_j + s_i F_ij (K_ij - K_ji),
-// F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps), F_ii = 0
+// F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps (s_i^2 + s_j^2)^2), F_ii = 0
+// (the broadening relative to the pair's own scale, so that it acts on
+// near-degenerate pairs only, whatever the matrix's norm)
 __global__ void svd_core_kernel(const double* __restrict__ J, const double* __restrict__ K,
                                 const double* __restrict__ s, const double* __restrict__ gs, int64_t k, double eps,
                                 double* __restrict__ core) {
@@ -157,8 +159,9 @@ __global__ void svd_core_kernel(const double* __restrict__ J, const double* __re
     if (i == j) {
       core[idx] = gs[i];
     } else {
-      const double d = s[j] * s[j] - s[i] * s[i];
-      const double F = d / (d * d + eps);
+      const double d = s[j] * s[j] - s[i] * s[i], q = s[j] * s[j] + s[i] * s[i];
+      const double den = d * d + eps * q * q;
+      const double F = den > 0.0 ? d / den : 0.0;
       const int64_t t = j * k + i;
       core[idx] = F * (J[idx] - J[t]) * s[j] + s[i] * F * (K[idx] - K[t]);
     }

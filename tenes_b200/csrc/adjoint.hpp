@@ -15,7 +15,10 @@
 //   slice       ctm.cpp:998-1012);
 //   truncated   Uc = U_w diag(s^-1/2), VTc = diag(s^-1/2) VT_w (ctm.cpp:245-302);
 //   SVD         adjoint of the thin SVD M = U S VT with Lorentzian-broadened
-//               F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps):
+//               F_ij = (s_j^2 - s_i^2) / ((s_j^2 - s_i^2)^2 + eps (s_i^2 + s_j^2)^2)
+//               (broadened relative to the pair's scale: an absolute eps
+//               distorted every pair of small kept values once the matrix's
+//               norm was small, e.g. the up/down projectors' M = R1 R2):
 //               gM = U [diag(gs) + (F o (J - J^T)) S + S (F o (K - K^T))] VT
 //                    + (1 - U U^T) gU S^-1 VT + U S^-1 gVT (1 - V V^T),
 //               J = U^T gU, K = V^T gV.  U, S, V are the rank-r part of
@@ -70,6 +73,7 @@ struct Options {
   int iterations = 0;      // CTMRG sweeps after the initialisation
   int checkpoint_every = 5;
   int prec_absorb = 0;     // product precision of the moves (0 FP64, 1 3xTF32)
+  bool projector_corner = true;  // Calc_projector_left_block, else Calc_projector_updown_blocks
 };
 
 // Singular values at or below kRankTol times the largest count as zero in
@@ -378,7 +382,8 @@ class Tape {
 };
 
 // The CTMRG forward of ctm.cpp on a tape: environment initialisation, the
-// four moves with full-SVD corner projectors, and window contractions.
+// four moves with full-SVD corner or up/down projectors, and window
+// contractions.
 // Environment tensors are zero-padded to chi as in the library's environment.
 template <class BK>
 struct CtmTape {
@@ -484,6 +489,38 @@ struct CtmTape {
     PU = t.tr(t.reshape(t.td(LBm, f.second, {1}, {1}, p), {t41, e78, t41, w}), {1, 0, 2, 3});
     PL = t.tr(t.reshape(t.td(LTm, f.first, {0}, {0}, p), {t41, e78, t41, w}), {1, 0, 2, 3});
   }
+  // Calc_projector_updown_blocks, full-SVD branch (ctm.cpp:320-491): the
+  // four corner blocks, R1 = RT LT and R2 = RB LB, the truncated SVD of
+  // M = R1 R2 (its row legs are R1's first three, its column legs R2's),
+  // PU = R2 conj(VT_c)^T and PL = R1 conj(U_c), legs (e78, t41, tc41, w)
+  void projector_ud(int C1, int C2, int C3, int C4, int eT1, int eT2, int eT3, int eT4, int eT5, int eT6, int eT7,
+                    int eT8, int T1, int T2, int T3, int T4, int& PU, int& PL) {
+    const int p = o.prec_absorb;
+    const int64_t e78 = t.dim(eT7, 1), t41 = t.dim(T4, 1);
+    if (t41 == 1) {  // identity projector (ctm.cpp:479-490)
+      PU = PL = t.leaf(t.bk.identity_projector(e78), false);
+      return;
+    }
+    const int LT = block_LT(C1, eT1, eT8, T1);
+    const int RT = t.td(T2, t.td(t.td(t.td(C2, eT3, {1}, {0}, p), eT2, {0}, {1}, p), T2, {2, 5}, {2, 1}, p),
+                        {1, 2, 4}, {3, 1, 6}, p);
+    const int RB = t.td(T3, t.td(t.td(t.td(C3, eT5, {1}, {0}, p), eT4, {0}, {1}, p), T3, {2, 5}, {3, 2}, p),
+                        {2, 3, 4}, {3, 1, 6}, p);
+    const int LB = block_LB(C4, eT7, eT6, T4);
+    const int R1 = t.td(RT, LT, {0, 3, 4}, {0, 2, 4}, p);
+    const int R2 = t.td(RB, LB, {0, 2, 4}, {1, 3, 5}, p);
+    const int64_t nrow = t.dim(R1, 0) * t.dim(R1, 1) * t.dim(R1, 2);
+    const int64_t ncol = t.dim(R2, 0) * t.dim(R2, 1) * t.dim(R2, 2);
+    const int64_t a3 = t.dim(R1, 3), a4 = t.dim(R1, 4), a5 = t.dim(R1, 5);
+    const int64_t b3 = t.dim(R2, 3), b4 = t.dim(R2, 4), b5 = t.dim(R2, 5);
+    const int R1m = t.reshape(R1, {nrow, a3 * a4 * a5});
+    const int R2m = t.reshape(R2, {ncol, b3 * b4 * b5});
+    const int M = t.td(R1m, R2m, {1}, {1}, p);
+    const std::pair<int, int> f = t.svd(M, o.chi, o.cutoff);
+    const int64_t w = t.dim(f.first, 1);
+    PU = t.tr(t.reshape(t.td(R2m, f.second, {0}, {1}, p), {b3, b4, b5, w}), {1, 0, 2, 3});
+    PL = t.tr(t.reshape(t.td(R1m, f.first, {0}, {0}, p), {a3, a4, a5, w}), {1, 0, 2, 3});
+  }
   // Calc_Next_CTM (ctm.cpp:493-518)
   std::pair<int, int> next_ctm(int C1, int C4, int eT1, int eT6, int PU, int PL) {
     const int p = o.prec_absorb;
@@ -514,9 +551,11 @@ struct CtmTape {
     std::vector<int> PU(L), PL(L);
     for (int iy = 0; iy < L; ++iy) {
       const int i = lat.index(ix, iy), j = lat.right(i), k = lat.bottom(j), l = lat.left(k);
-      (void)j;
-      (void)k;
-      projector(C[0][i], C[3][l], E[0][i], E[2][l], E[3][l], E[3][i], Tn[i], Tn[l], PU[iy], PL[iy]);
+      if (o.projector_corner)
+        projector(C[0][i], C[3][l], E[0][i], E[2][l], E[3][l], E[3][i], Tn[i], Tn[l], PU[iy], PL[iy]);
+      else
+        projector_ud(C[0][i], C[1][j], C[2][k], C[3][l], E[0][i], E[0][j], E[1][j], E[1][k], E[2][k], E[2][l],
+                     E[3][l], E[3][i], Tn[i], Tn[j], Tn[k], Tn[l], PU[iy], PL[iy]);
     }
     const auto C0 = C, E0 = E;
     et_memo.clear();
@@ -535,7 +574,11 @@ struct CtmTape {
     std::vector<int> PU(L), PL(L);
     for (int iy = 0; iy < L; ++iy) {
       const int k = lat.index(ix, iy), l = lat.left(k), i = lat.top(l), j = lat.right(i);
-      projector(C[2][k], C[1][j], E[2][k], E[0][j], E[1][j], E[1][k], rot(k, 0), rot(j, 0), PU[iy], PL[iy]);
+      if (o.projector_corner)
+        projector(C[2][k], C[1][j], E[2][k], E[0][j], E[1][j], E[1][k], rot(k, 0), rot(j, 0), PU[iy], PL[iy]);
+      else
+        projector_ud(C[2][k], C[3][l], C[0][i], C[1][j], E[2][k], E[2][l], E[3][l], E[3][i], E[0][i], E[0][j],
+                     E[1][j], E[1][k], rot(k, 0), rot(l, 0), rot(i, 0), rot(j, 0), PU[iy], PL[iy]);
     }
     const auto C0 = C, E0 = E;
     et_memo.clear();
@@ -554,7 +597,11 @@ struct CtmTape {
     std::vector<int> PU(L), PL(L);
     for (int ix = 0; ix < L; ++ix) {
       const int j = lat.index(ix, iy), k = lat.bottom(j), l = lat.left(k), i = lat.top(l);
-      projector(C[1][j], C[0][i], E[1][j], E[3][i], E[0][i], E[0][j], rot(j, 1), rot(i, 1), PU[ix], PL[ix]);
+      if (o.projector_corner)
+        projector(C[1][j], C[0][i], E[1][j], E[3][i], E[0][i], E[0][j], rot(j, 1), rot(i, 1), PU[ix], PL[ix]);
+      else
+        projector_ud(C[1][j], C[2][k], C[3][l], C[0][i], E[1][j], E[1][k], E[2][k], E[2][l], E[3][l], E[3][i],
+                     E[0][i], E[0][j], rot(j, 1), rot(k, 1), rot(l, 1), rot(i, 1), PU[ix], PL[ix]);
     }
     const auto C0 = C, E0 = E;
     et_memo.clear();
@@ -573,7 +620,11 @@ struct CtmTape {
     std::vector<int> PU(L), PL(L);
     for (int ix = 0; ix < L; ++ix) {
       const int l = lat.index(ix, iy), i = lat.top(l), j = lat.right(i), k = lat.bottom(j);
-      projector(C[3][l], C[2][k], E[3][l], E[1][k], E[2][k], E[2][l], rot(l, 2), rot(k, 2), PU[ix], PL[ix]);
+      if (o.projector_corner)
+        projector(C[3][l], C[2][k], E[3][l], E[1][k], E[2][k], E[2][l], rot(l, 2), rot(k, 2), PU[ix], PL[ix]);
+      else
+        projector_ud(C[3][l], C[0][i], C[1][j], C[2][k], E[3][l], E[3][i], E[0][i], E[0][j], E[1][j], E[1][k],
+                     E[2][k], E[2][l], rot(l, 2), rot(i, 2), rot(j, 2), rot(k, 2), PU[ix], PL[ix]);
     }
     const auto C0 = C, E0 = E;
     et_memo.clear();

@@ -3036,8 +3036,7 @@ struct EngineT final : Engine {
     if constexpr (CPLX) {
       fail(TG_E_INPUT, "energy gradient: real site tensors only");
     } else {
-      if (!P.projector_corner || P.use_rsvd)
-        fail(TG_E_INPUT, "energy gradient: full-SVD corner projectors only (projector_corner = 1, use_rsvd = 0)");
+      if (P.use_rsvd) fail(TG_E_INPUT, "energy gradient: full-SVD projectors only (use_rsvd = 0)");
       if (nterms < 1) fail(TG_E_INPUT, "energy gradient: no energy terms");
       if (!(svd_broadening >= 0.0)) fail(TG_E_INPUT, "energy gradient: svd_broadening must be >= 0");
       std::vector<ad::WindowTerm> w(static_cast<size_t>(nterms));
@@ -3077,6 +3076,7 @@ struct EngineT final : Engine {
       o.iterations = iterations;
       o.checkpoint_every = checkpoint_every;
       o.prec_absorb = abs_prec;
+      o.projector_corner = P.projector_corner != 0;
       std::vector<DT<double>> g;
       const SvdFn fn = [this](DT<double>& A, int64_t m, int64_t n, DT<double>& U, DT<double>& s, DT<double>& VT) {
         svd_jacobi(A, m, n, U, s, VT);

@@ -26,7 +26,11 @@
 
 
 int main(int argc, char** argv) {
-  g_zero_null = argc > 1 && std::string(argv[1]) == "zero-null";
+  bool updown = false;
+  for (int a = 1; a < argc; ++a) {
+    if (std::string(argv[a]) == "zero-null") g_zero_null = true;
+    if (std::string(argv[a]) == "updown") updown = true;
+  }
   int LX, LY, skew, chi, iters, ckpt;
   double cutoff, eps;
   std::cin >> LX >> LY >> skew >> chi >> iters >> ckpt >> cutoff >> eps;
@@ -67,6 +71,7 @@ int main(int argc, char** argv) {
   o.eps = eps;
   o.iterations = iters;
   o.checkpoint_every = ckpt;
+  o.projector_corner = !updown;
   HostBackend bk;
   std::vector<HT> g;
   const double E = tg::ad::energy_grad(bk, lat, Tn, terms, o, &g);

@@ -389,7 +389,9 @@ struct HostBackend {
           continue;
         }
         const double d = s.p()[j] * s.p()[j] - s.p()[i] * s.p()[i];
-        const double F = d / (d * d + eps);
+        const double q = s.p()[j] * s.p()[j] + s.p()[i] * s.p()[i];
+        const double den = d * d + eps * q * q;
+        const double F = den > 0.0 ? d / den : 0.0;
         c.p()[i * k + j] = F * (J.p()[i * k + j] - J.p()[j * k + i]) * s.p()[j] +
                            s.p()[i] * F * (K.p()[i * k + j] - K.p()[j * k + i]);
       }

@@ -2,8 +2,8 @@
 
 * its forward energy equals the library's own sweep + window measurement;
 * its gradient equals the FP64 host autograd reference (oracle/ctm_autograd.py)
-  at small sizes, with uniform and uneven bond dimensions and with the
-  environment zero-padded to chi;
+  at small sizes, with uniform and uneven bond dimensions, with the
+  environment zero-padded to chi, for corner and up/down projectors;
 * the checkpoint interval changes nothing;
 * central finite differences at the J1-J2 gradient workload's shapes
   (D = 3, chi = 36, 2 x 2, J2 = 0.5, normal(0,1) tensors);
@@ -23,9 +23,9 @@ from tenes_b200.grad import CTMEnergy, j1j2_terms, optimize_lbfgs
 pytestmark = pytest.mark.gpu
 
 
-def make(lat, Tn, chi, mixed=False):
+def make(lat, Tn, chi, mixed=False, corner=True):
     env = Environment(lat.LX, lat.LY, lat.physical_dims, lat.virtual_dims,
-                      CTMParams(chi=chi, max_ctm_iteration=1, mixed=mixed), False)
+                      CTMParams(chi=chi, max_ctm_iteration=1, mixed=mixed, projector_corner=corner), False)
     for i, t in enumerate(Tn):
         env.set_site_tensor(i, t)
     return env
@@ -43,12 +43,13 @@ def window_energy(env, terms):
     return E
 
 
-def test_energy_equals_sweeps_and_measurement():
+@pytest.mark.parametrize("corner", [True, False])
+def test_energy_equals_sweeps_and_measurement(corner):
     rng = np.random.default_rng(1)
     lat = lattice(2, 2, uniform_dims(4, 3))
     Tn = random_tensors(lat, rng)
     terms = j1j2_terms(4, 1.0, 0.5)
-    env = make(lat, Tn, 12)
+    env = make(lat, Tn, 12, corner=corner)
     E, g = env.energy_grad(terms, 3, grad=False)
     assert g is None
     env.init_env()
@@ -59,8 +60,10 @@ def test_energy_equals_sweeps_and_measurement():
     assert abs(E - E2) <= 1e-10 * abs(E2), (E, E2)
 
 
-@pytest.mark.parametrize("uneven,chi", [(False, 4), (False, 5), (True, 5)])
-def test_gradient_matches_host_reference(uneven, chi):
+@pytest.mark.parametrize("uneven,chi,corner", [(False, 4, True), (False, 5, True), (True, 5, True),
+                                               (False, 5, False), (True, 5, False)])
+def test_gradient_matches_host_reference(uneven, chi, corner):
+    """corner=False: the up/down projectors (ctm.cpp:320-491, full SVD)."""
     rng = np.random.default_rng(21 + chi + 7 * uneven)
     lat = lattice(2, 2, uniform_dims(4, 2))
     if uneven:
@@ -68,8 +71,8 @@ def test_gradient_matches_host_reference(uneven, chi):
     Tn = random_tensors(lat, rng)
     terms = j1j2_terms(4, 1.0, 0.5)
     iters = 3
-    E_ref, g_ref = R.energy_and_grad(Tn, terms, chi, iters, lat)
-    env = make(lat, Tn, chi)
+    E_ref, g_ref = R.energy_and_grad(Tn, terms, chi, iters, lat, corner=corner)
+    env = make(lat, Tn, chi, corner=corner)
     E, g = env.energy_grad(terms, iters, checkpoint_every=2)
     env.close()
     assert abs(E - E_ref) <= 1e-10 * abs(E_ref)
@@ -94,6 +97,34 @@ def _c4_problem(iters):
     lat = lattice(2, 2, uniform_dims(4, 3))
     Tn = random_tensors(lat, rng)
     return lat, Tn, j1j2_terms(4, 1.0, 0.5)
+
+
+def test_updown_gradient_matches_finite_differences():
+    """The up/down projectors' adjoint against central differences (step
+    1e-5) on 6 seeded entries: D = 2, chi = 8, 4 sweeps."""
+    iters = 4
+    rng = np.random.default_rng(77)
+    lat = lattice(2, 2, uniform_dims(4, 2))
+    Tn = random_tensors(lat, rng)
+    terms = j1j2_terms(4, 1.0, 0.5)
+    env = make(lat, Tn, 8, corner=False)
+    E, g = env.energy_grad(terms, iters, checkpoint_every=2)
+    gmax = max(np.abs(x).max() for x in g)
+    h = 1e-5
+    for _ in range(6):
+        site = int(rng.integers(4))
+        idx = tuple(int(rng.integers(n)) for n in Tn[site].shape)
+        vals = []
+        for s in (+1, -1):
+            T = [t.copy() for t in Tn]
+            T[site][idx] += s * h
+            for i, t in enumerate(T):
+                env.set_site_tensor(i, t)
+            vals.append(env.energy_grad(terms, iters, grad=False)[0])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - g[site][idx]) <= 1e-6 * max(abs(fd), abs(g[site][idx]), 1e-3 * gmax), \
+            (site, idx, fd, g[site][idx])
+    env.close()
 
 
 def test_finite_differences_at_the_gradient_workload_shapes():

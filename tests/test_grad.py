@@ -89,8 +89,8 @@ def test_two_site_terms_reproduce_the_operator():
     assert window_geometry(-1, 1) == (2, 2, 1, 1, 0, 0)
 
 
-def _oracle_energy(Tn, terms, chi, iters, lat):
-    p = O.Params(CHI=chi)
+def _oracle_energy(Tn, terms, chi, iters, lat, corner=True):
+    p = O.Params(CHI=chi, CTM_Projector_corner=corner)
     env = O.init_env(Tn, p, lat)
     for _ in range(iters):
         O.sweep(env, Tn, p, lat)
@@ -111,30 +111,36 @@ def _oracle_energy(Tn, terms, chi, iters, lat):
     return E
 
 
-def test_reference_forward_matches_oracle():
+@pytest.mark.parametrize("corner", [True, False])
+def test_reference_forward_matches_oracle(corner):
     rng = np.random.default_rng(3)
     lat = lattice(2, 2, uniform_dims(4, 2))
     Tn = random_tensors(lat, rng)
     terms = j1j2_terms(4, 1.0, 0.5)
-    E0 = _oracle_energy(Tn, terms, 4, 2, lat)
+    E0 = _oracle_energy(Tn, terms, 4, 2, lat, corner)
     with torch.no_grad():
-        E1 = float(R.energy([torch.tensor(t) for t in Tn], terms, 4, 2, lat))
+        E1 = float(R.energy([torch.tensor(t) for t in Tn], terms, 4, 2, lat, corner=corner))
     assert abs(E1 - E0) <= 1e-11 * abs(E0)
 
 
-def test_reference_gradient_matches_finite_differences():
+@pytest.mark.parametrize("corner,chi", [(True, 4), (False, 4), (True, 8), (False, 8)])
+def test_reference_gradient_matches_finite_differences(corner, chi):
+    """chi = 8 > D^2: zero-padded first environments and, for the up/down
+    projectors, matrices M = R1 R2 of small norm whose kept singular values
+    span six decades -- the case an absolute Lorentzian broadening got wrong
+    by up to 1.5% and the pair-relative one gets right."""
     rng = np.random.default_rng(5)
     lat = lattice(2, 2, uniform_dims(4, 2))
     Tn = random_tensors(lat, rng)
     terms = j1j2_terms(4, 1.0, 0.5)
-    E, g = R.energy_and_grad(Tn, terms, 4, 2, lat)
+    E, g = R.energy_and_grad(Tn, terms, chi, 2, lat, corner=corner)
     h = 1e-5
     for site, idx in [(0, (0, 1, 0, 1, 0)), (1, (1, 1, 1, 0, 1)), (2, (0, 0, 1, 1, 1)), (3, (1, 0, 0, 0, 0))]:
         def f(delta):
             T = [t.copy() for t in Tn]
             T[site][idx] += delta
             with torch.no_grad():
-                return float(R.energy([torch.tensor(t) for t in T], terms, 4, 2, lat))
+                return float(R.energy([torch.tensor(t) for t in T], terms, chi, 2, lat, corner=corner))
         fd = (f(h) - f(-h)) / (2 * h)
         assert abs(fd - g[site][idx]) <= 1e-6 * max(abs(fd), 1e-3), (site, idx, fd, g[site][idx])
 
@@ -154,7 +160,7 @@ def host_adjoint(tmp_path_factory):
     return out
 
 
-def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12, zero_null=False):
+def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12, zero_null=False, corner=True):
     lines = [f"{lat.LX} {lat.LY} 0 {chi} {iters} {ckpt}", f"{cutoff!r} {eps!r}"]
     for i in range(lat.N_UNIT):
         lines.append(" ".join(str(x) for x in [lat.physical_dims[i]] + list(lat.virtual_dims[i])))
@@ -168,7 +174,8 @@ def run_host(exe, lat, Tn, terms, chi, iters, ckpt, cutoff=1e-12, eps=1e-12, zer
         for k in keys:
             op = np.asarray(t["ops"][k], dtype=np.float64)
             lines.append(f"{k[0]} {k[1]} {op.shape[0]} " + " ".join(repr(float(x)) for x in op.reshape(-1)))
-    res = subprocess.run([exe] + (["zero-null"] if zero_null else []), input="\n".join(lines) + "\n",
+    res = subprocess.run([exe] + (["zero-null"] if zero_null else []) + ([] if corner else ["updown"]),
+                         input="\n".join(lines) + "\n",
                          capture_output=True, text=True, check=True)
     out = res.stdout.splitlines()
     E = float(out[0].split()[1])
@@ -182,8 +189,9 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("corner", [True, False])
 @pytest.mark.parametrize("uneven", [False, True])
-def test_host_adjoint_matches_reference(host_adjoint, uneven):
+def test_host_adjoint_matches_reference(host_adjoint, uneven, corner):
     rng = np.random.default_rng(11 if uneven else 7)
     lat = lattice(2, 2, uniform_dims(4, 2))
     if uneven:
@@ -191,8 +199,8 @@ def test_host_adjoint_matches_reference(host_adjoint, uneven):
     Tn = random_tensors(lat, rng)
     terms = j1j2_terms(4, 1.0, 0.5)
     chi, iters = 5, 3
-    E_ref, g_ref = R.energy_and_grad(Tn, terms, chi, iters, lat)
-    E, g = run_host(host_adjoint, lat, Tn, terms, chi, iters, ckpt=2)
+    E_ref, g_ref = R.energy_and_grad(Tn, terms, chi, iters, lat, corner=corner)
+    E, g = run_host(host_adjoint, lat, Tn, terms, chi, iters, ckpt=2, corner=corner)
     assert abs(E - E_ref) <= 1e-10 * abs(E_ref)
     assert _rel(g, g_ref) <= 1e-8, _rel(g, g_ref)
 
