@@ -994,6 +994,42 @@ struct EngineT final : Engine {
     return false;
   }
 
+  // The SVD of a strongly rectangular M (nrow x ncol, row-major; the long
+  // side at least 4 times the short one k, and k within the one-CTA Jacobi
+  // kernel's limit) by R-SVD: a Householder QR of the tall one of M^H / M,
+  // the Jacobi SVD of the k x k factor, and two products back -- in place of
+  // cuSOLVER's gesvd, whose bidiagonalisation of the whole matrix is a chain
+  // of hundreds of small launches (about 3 ms a call at 48 x 1200 complex:
+  // the projectors of a line with a D = 1 leg are that narrow).  Outputs as
+  // svd(): U (nrow x k), s (k, descending), VT (k x ncol), row-major.
+  // Returns false (computing nothing) for other shapes, which keep gesvd.
+  bool small_side_svd(const DT<T>& Min, int64_t nrow, int64_t ncol, DT<T>& U, DT<double>& s, DT<T>& VT) {
+    const int64_t k = std::min(nrow, ncol);
+    if (k < 2 || k > jacobi_svd_max_k<T>() || std::max(nrow, ncol) < 4 * k) return false;
+    const DT<T> M = reshape(Min, {nrow, ncol});
+    PrecScope fp64(this, 0);  // every product of the factorisation in FP64
+    DT<T> Ub({k, k}, st), Wb({k, k}, st);
+    s = DT<double>({k}, st);
+    if (ncol >= nrow) {
+      // Q R = M^H (ncol x k); B = M Q = R^H (k x k); B = Ub S Wb^H; M = Ub S (Q Wb)^H
+      DT<T> Q = transpose<T>(M, {0, 1}, st, true);  // column-major view: M^H
+      orth_cm(Q, ncol, k);
+      DT<T> B = mm_rm(rm(M.p, nrow, ncol), cm(Q.p, ncol, k));
+      jacobi_svd<T>(B.p, k, Ub.p, s.p, Wb.p, st);  // B Wb = Ub S
+      U = Ub;
+      VT = transpose<T>(mm_rm(cm(Q.p, ncol, k), rm(Wb.p, k, k)), {1, 0}, st, true);
+    } else {
+      // Q R = M (nrow x k); B = Q^H M = R (k x k); B = Ub S Wb^H; M = (Q Ub) S Wb^H
+      DT<T> Q = transpose<T>(M, {1, 0}, st);  // column-major view: M
+      orth_cm(Q, nrow, k);
+      DT<T> B = mm_rm(ht(cm(Q.p, nrow, k)), rm(M.p, nrow, ncol));
+      jacobi_svd<T>(B.p, k, Ub.p, s.p, Wb.p, st);
+      U = mm_rm(cm(Q.p, nrow, k), rm(Ub.p, k, k));
+      VT = transpose<T>(Wb, {1, 0}, st, true);
+    }
+    return true;
+  }
+
   // Truncated projectors from M (nrow x ncol, consumed):
   // U_c (nrow x w), VT_c (w x ncol) scaled by 1/sqrt(s), w = min(k, chi)
   void truncated_factors(DT<T>& M, int64_t nrow, int64_t ncol, DT<T>& Uc, DT<T>& VTc) {
@@ -1007,7 +1043,7 @@ struct EngineT final : Engine {
     }
     DT<T> U, VT;
     DT<double> s;
-    svd(M, nrow, ncol, U, s, VT);
+    if (!small_side_svd(M, nrow, ncol, U, s, VT)) svd(M, nrow, ncol, U, s, VT);
     const int64_t k = std::min(nrow, ncol);
     const int w = static_cast<int>(std::min<int64_t>(k, P.chi));
     DT<double> sinv({w}, st);
