@@ -3001,13 +3001,19 @@ void jacobi_svd(const T* A, int64_t k, T* U, double* S, T* W, cudaStream_t st, c
   const size_t smem = sizeof(double) * ((CPLX ? 4 : 2) * k * k + k) + sizeof(int) * k;
   ProfScope ps(PK_SOLVER, st, (CPLX ? 4.0 : 1.0) * 10.0 * static_cast<double>(k) * k * k, 0.0);
   const int npairs = static_cast<int>((k + 1) / 2);
-  // up to 96 columns: 16 lanes a pair, 6 rows a lane; up to 160: 32 lanes, 5 rows
+  // up to 96 columns: 16 lanes a pair, 3, 4 or 6 rows a lane; up to 160: 32 lanes, 5 rows
   auto run = [&](auto kernel, int lanes) {
     ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), smem);
     const int threads = static_cast<int>(std::min<int64_t>(1024, (static_cast<int64_t>(npairs) * lanes + 31) / 32 * 32));
     kernel<<<1, threads, smem, st>>>(A, static_cast<int>(k), U, S, W, Winit);
   };
-  if (k <= 96)
+  // rows a lane holds: the fewest that cover k (masked rows add exact zeros,
+  // so the sums -- and the result -- are those of any larger choice)
+  if (k <= 48)
+    run(jacobi_svd_kernel<T, CPLX, 16, 3>, 16);
+  else if (k <= 64)
+    run(jacobi_svd_kernel<T, CPLX, 16, 4>, 16);
+  else if (k <= 96)
     run(jacobi_svd_kernel<T, CPLX, 16, 6>, 16);
   else
     run(jacobi_svd_kernel<T, CPLX, 32, 5>, 32);
